@@ -1,0 +1,142 @@
+// Shared device and host helpers of the B200 SIMPLEC hot path: the grid
+// layout (one index space for every location type), the context with its
+// stream and scratch, error reporting and the warp reductions.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "../../include/gust_b200.h"
+
+namespace gb {
+
+// ---------------------------------------------------------------- layout ---
+
+//! Element offset of point (i, j, k) of any location type.
+__host__ __device__ __forceinline__ int64_t at(const gb_grid& g, int i, int j, int k)
+{
+    return static_cast<int64_t>(i + g.ng) + static_cast<int64_t>(j + g.ng) * g.sy
+         + static_cast<int64_t>(k + g.ng) * g.sz;
+}
+
+__host__ __device__ __forceinline__ int64_t volume(const gb_grid& g)
+{
+    return g.sz * static_cast<int64_t>(g.nz + 1 + 2 * g.ng);
+}
+
+//! Valid extents of a location: cells, plus one point in each nodal direction.
+__host__ __device__ __forceinline__ int ext_x(const gb_grid& g, int loc) { return g.nx + (loc & 1); }
+__host__ __device__ __forceinline__ int ext_y(const gb_grid& g, int loc) { return g.ny + ((loc >> 1) & 1); }
+__host__ __device__ __forceinline__ int ext_z(const gb_grid& g, int loc) { return g.nz + ((loc >> 2) & 1); }
+
+//! The periodic image of a lateral index outside the valid range [0, n_valid),
+//! or -1 (outside a non-periodic face: the caller reads zero). n is the number
+//! of cells, the period.
+__host__ __device__ __forceinline__ int lateral_image(int i, int n_valid, int n, bool periodic)
+{
+    if (i >= 0 && i < n_valid) { return i; }
+    if (!periodic) { return -1; }
+    return (i < 0) ? i + n : i - n;
+}
+
+// ---------------------------------------------------------- reductions ---
+
+__device__ __forceinline__ double warp_max(double v)
+{
+    for (int o = 16; o > 0; o >>= 1) { v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o)); }
+    return v;
+}
+__device__ __forceinline__ float warp_max(float v)
+{
+    for (int o = 16; o > 0; o >>= 1) { v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o)); }
+    return v;
+}
+__device__ __forceinline__ double warp_sum(double v)
+{
+    for (int o = 16; o > 0; o >>= 1) { v += __shfl_xor_sync(0xffffffffu, v, o); }
+    return v;
+}
+
+//! atomic max of a non-negative value (NaN propagates: its bits order above
+//! every finite value and inf). Slot holds the value's bit pattern.
+__device__ __forceinline__ void atomic_max_nonneg(unsigned long long* slot, double v)
+{
+    if (v != v) { atomicMax(slot, 0x7ff8000000000000ull); return; }
+    atomicMax(slot, static_cast<unsigned long long>(__double_as_longlong(v)));
+}
+__device__ __forceinline__ void atomic_max_nonneg(unsigned long long* slot, float v)
+{
+    atomic_max_nonneg(slot, static_cast<double>(v));
+}
+
+// ---------------------------------------------------------------- errors ---
+
+void set_error(const char* fmt, ...);
+void clear_error();
+
+//! Record a CUDA error (if any) of the last launch or call; returns the status.
+gb_status check_cuda(const char* op);
+
+}  // namespace gb
+
+// ------------------------------------------------------------- context ---
+
+struct gb_ctx {
+    cudaStream_t stream{nullptr};
+    int device{0};
+    int num_sms{148};
+    int64_t launches{0};
+    //! Scratch slots, grown on demand (device memory).
+    std::vector<void*> slot_ptr;
+    std::vector<size_t> slot_bytes;
+    //! Device and pinned-host result words (reductions read back).
+    unsigned long long* d_words{nullptr};
+    unsigned long long* h_words{nullptr};
+    static constexpr int n_words = 64;
+    //! Per-kernel-family timing (CUDA events on the stream around each launch),
+    //! on while profiling is enabled.
+    bool profiling{false};
+    struct Span { int family; cudaEvent_t start, stop; };
+    std::vector<Span> spans;
+    std::vector<cudaEvent_t> event_pool;
+};
+
+namespace gb {
+
+//! Scratch slot `slot` of at least `bytes` (contents undefined); nullptr and
+//! GB_OOM recorded on failure.
+void* scratch(gb_ctx* ctx, int slot, size_t bytes);
+
+//! Open / close a timed span of a kernel family (no-ops unless profiling).
+void span_begin(gb_ctx* ctx, int family);
+void span_end(gb_ctx* ctx);
+
+//! RAII span around the launches of one kernel family.
+struct Span {
+    gb_ctx* ctx;
+    Span(gb_ctx* c, int family) : ctx(c) { span_begin(c, family); }
+    ~Span() { span_end(ctx); }
+};
+
+//! Device pointer of result word n of the context.
+inline unsigned long long* dword(gb_ctx* ctx, int n) { return ctx->d_words + n; }
+
+//! Copy `count` result words to the host (synchronises the stream).
+gb_status read_words(gb_ctx* ctx, int first, int count, unsigned long long* out);
+
+gb_status check_grid(const char* op, const gb_grid* g);
+gb_status check_loc(const char* op, int loc);
+
+inline double bits_to_double(unsigned long long b)
+{
+    double d;
+    static_assert(sizeof(d) == sizeof(b), "");
+    __builtin_memcpy(&d, &b, sizeof(d));
+    return d;
+}
+
+}  // namespace gb

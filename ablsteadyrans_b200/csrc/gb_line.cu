@@ -1,0 +1,267 @@
+// z-line relaxation: the exact tridiagonal solve of every (i, j) column with
+// the x/y neighbour terms of the lagged iterate on the right-hand side
+// (gust::solve_column, Source/LineSolve_K.H:22-45), swept `sweeps` times as a
+// z-line Jacobi iteration (gust::zline_jacobi, Source/Predictor.cpp:87-127).
+//
+// B200 mapping: one thread per column, a warp over 32 consecutive i of one j,
+// so every k step of the Thomas recurrences reads and writes coalesced rows of
+// each k-plane. The recurrence scratch c', e' lives in shared memory (one
+// column per thread, [k][thread] so a warp's accesses are consecutive) when
+// the column fits, else in a global scratch array that stays in L2 for the
+// tile sizes here. The max |change| of the last sweep is a warp-shuffle max
+// and one atomic per warp. Iterates ping-pong between the caller's delta and
+// one scratch array so the last sweep lands in delta.
+#include "gb_line.cuh"
+
+#include <algorithm>
+
+namespace gb {
+
+namespace {
+
+template <typename T>
+struct LineArgs {
+    gb_grid g;
+    int ni, nj, nk;
+    const T* __restrict__ A;
+    int64_t cs;  // component stride of A
+    const T* __restrict__ ap;
+    const T* __restrict__ rhs;
+    const T* __restrict__ dold;  // lagged iterate (ghosts unread: images by index)
+    T* __restrict__ dnew;
+    T* __restrict__ cbuf;  // global scratch (SMEM == false)
+    T* __restrict__ ebuf;
+    int first;  // dold == 0: no neighbour terms, change against 0
+    unsigned long long* change;  // max |dnew - dold| (nullptr: not wanted)
+};
+
+template <typename T, bool SMEM>
+__global__ void __launch_bounds__(128) zline_sweep_kernel(LineArgs<T> a)
+{
+    extern __shared__ unsigned char smem_raw[];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const bool active = (i < a.ni) && (j < a.nj);
+    T chg = T(0);
+    if (active) {
+        const gb_grid& g = a.g;
+        const int im = lateral_image(i - 1, a.ni, g.nx, g.periodic_x != 0);
+        const int ip = lateral_image(i + 1, a.ni, g.nx, g.periodic_x != 0);
+        const int jm = lateral_image(j - 1, a.nj, g.ny, g.periodic_y != 0);
+        const int jp = lateral_image(j + 1, a.nj, g.ny, g.periodic_y != 0);
+        const int64_t o0 = at(g, i, j, 0);
+        const int64_t oxm = (im >= 0) ? at(g, im, j, 0) : -1;
+        const int64_t oxp = (ip >= 0) ? at(g, ip, j, 0) : -1;
+        const int64_t oym = (jm >= 0) ? at(g, i, jm, 0) : -1;
+        const int64_t oyp = (jp >= 0) ? at(g, i, jp, 0) : -1;
+        const T* __restrict__ axm = a.A + GB_COEF_XM * a.cs;
+        const T* __restrict__ axp = a.A + GB_COEF_XP * a.cs;
+        const T* __restrict__ aym = a.A + GB_COEF_YM * a.cs;
+        const T* __restrict__ ayp = a.A + GB_COEF_YP * a.cs;
+        const T* __restrict__ azm = a.A + GB_COEF_ZM * a.cs;
+        const T* __restrict__ azp = a.A + GB_COEF_ZP * a.cs;
+        const int nthr = blockDim.x * blockDim.y;
+        const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+        T* cs = SMEM ? reinterpret_cast<T*>(smem_raw) + tid : a.cbuf + o0;
+        T* es = SMEM ? reinterpret_cast<T*>(smem_raw) + static_cast<int64_t>(a.nk) * nthr + tid : a.ebuf + o0;
+        const int64_t sstep = SMEM ? nthr : g.sz;
+        T cprev = T(0), eprev = T(0);
+        int64_t ko = 0, ks = 0;
+#pragma unroll 4
+        for (int k = 0; k < a.nk; ++k, ko += g.sz, ks += sstep) {
+            const int64_t o = o0 + ko;
+            T rk = a.rhs[o];
+            if (!a.first) {
+                const T dxm = (oxm >= 0) ? a.dold[oxm + ko] : T(0);
+                const T dxp = (oxp >= 0) ? a.dold[oxp + ko] : T(0);
+                const T dym = (oym >= 0) ? a.dold[oym + ko] : T(0);
+                const T dyp = (oyp >= 0) ? a.dold[oyp + ko] : T(0);
+                rk = rk + axm[o] * dxm + axp[o] * dxp + aym[o] * dym + ayp[o] * dyp;
+            }
+            const T lower = -azm[o], upper = -azp[o];
+            const T m = (k == 0) ? a.ap[o] : a.ap[o] - lower * cprev;
+            cprev = upper / m;
+            eprev = ((k == 0) ? rk : rk - lower * eprev) / m;
+            cs[ks] = cprev;
+            es[ks] = eprev;
+        }
+        // Back substitution from the top of the column.
+        T x = eprev;
+        ks -= sstep;
+        ko -= g.sz;
+        a.dnew[o0 + ko] = x;
+        if (a.change) { chg = fabs(x - (a.first ? T(0) : a.dold[o0 + ko])); }
+        for (int k = a.nk - 2; k >= 0; --k) {
+            ks -= sstep;
+            ko -= g.sz;
+            x = es[ks] - cs[ks] * x;
+            a.dnew[o0 + ko] = x;
+            if (a.change) {
+                const T d = fabs(x - (a.first ? T(0) : a.dold[o0 + ko]));
+                chg = (d > chg || d != d) ? d : chg;
+            }
+        }
+    }
+    if (a.change != nullptr) {
+        chg = warp_max(chg);
+        if ((threadIdx.x & 31) == 0) { atomic_max_nonneg(a.change, chg); }
+    }
+}
+
+//! The two copies of a periodic seam face take the low copy's value.
+template <typename T>
+__global__ void seam_sync_kernel(gb_grid g, int loc, T* __restrict__ f)
+{
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    const int ni = ext_x(g, loc), nj = ext_y(g, loc), nk = ext_z(g, loc);
+    const bool sx = (loc & 1) && g.periodic_x, sy = ((loc >> 1) & 1) && g.periodic_y;
+    if (sx) {
+        if (n < nj * nk) {
+            const int j = n % nj, k = n / nj;
+            f[at(g, g.nx, j, k)] = f[at(g, 0, j, k)];
+        }
+    }
+    if (sy) {
+        if (n < ni * nk) {
+            const int i = n % ni, k = n / ni;
+            f[at(g, i, g.ny, k)] = f[at(g, i, 0, k)];
+        }
+    }
+}
+
+}  // namespace
+
+template <typename T>
+void seam_sync(gb_ctx* ctx, const gb_grid& g, int loc, T* f)
+{
+    const bool sx = (loc & 1) && g.periodic_x, sy = ((loc >> 1) & 1) && g.periodic_y;
+    if (!sx && !sy) { return; }
+    const int n = std::max(ext_y(g, loc), ext_x(g, loc)) * ext_z(g, loc);
+    seam_sync_kernel<T><<<(n + 255) / 256, 256, 0, ctx->stream>>>(g, loc, f);
+    ++ctx->launches;
+}
+
+template <typename T>
+size_t line_smem_bytes(int nk)
+{
+    return static_cast<size_t>(2) * nk * 64 * sizeof(T);
+}
+
+template <typename T>
+gb_status zline_sweeps(gb_ctx* ctx, const gb_grid& g, int loc, const T* A, const T* ap, const T* rhs, int sweeps,
+                       T* delta, unsigned long long* change_word, LineScratch scratch_kind)
+{
+    const int ni = ext_x(g, loc), nj = ext_y(g, loc), nk = ext_z(g, loc);
+    const int64_t vol = volume(g);
+    // Ping-pong: sweep s writes buf[(sweeps - 1 - s) & 1], so the last sweep lands in delta.
+    T* tmp = static_cast<T*>(scratch(ctx, kSlotLineNext, sizeof(T) * vol));
+    if (tmp == nullptr) { return GB_OOM; }
+    const size_t smem = line_smem_bytes<T>(nk);
+    bool use_smem = (scratch_kind == LineScratch::shared) || (scratch_kind == LineScratch::automatic && smem <= 160 * 1024);
+    T* cbuf = nullptr;
+    T* ebuf = nullptr;
+    if (!use_smem) {
+        cbuf = static_cast<T*>(scratch(ctx, kSlotLineC, sizeof(T) * vol));
+        ebuf = static_cast<T*>(scratch(ctx, kSlotLineE, sizeof(T) * vol));
+        if (cbuf == nullptr || ebuf == nullptr) { return GB_OOM; }
+    } else {
+        static bool attr_set[2] = {false, false};
+        const int ti = sizeof(T) == 8 ? 1 : 0;
+        if (!attr_set[ti]) {
+            cudaFuncSetAttribute(zline_sweep_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+            attr_set[ti] = true;
+        }
+    }
+    T* buf[2] = {delta, tmp};
+    if (change_word != nullptr) { cudaMemsetAsync(change_word, 0, sizeof(unsigned long long), ctx->stream); }
+    for (int s = 0; s < sweeps; ++s) {
+        LineArgs<T> a;
+        a.g = g;
+        a.ni = ni;
+        a.nj = nj;
+        a.nk = nk;
+        a.A = A;
+        a.cs = vol;
+        a.ap = ap;
+        a.rhs = rhs;
+        a.dold = buf[(sweeps - s) & 1];
+        a.dnew = buf[(sweeps - 1 - s) & 1];
+        a.cbuf = cbuf;
+        a.ebuf = ebuf;
+        a.first = (s == 0) ? 1 : 0;
+        a.change = (s == sweeps - 1) ? change_word : nullptr;
+        Span span(ctx, GB_KERNEL_LINE_SWEEP);
+        if (use_smem) {
+            const dim3 block(32, 2);
+            const dim3 grid((ni + 31) / 32, (nj + 1) / 2);
+            zline_sweep_kernel<T, true><<<grid, block, smem, ctx->stream>>>(a);
+        } else {
+            const dim3 block(32, 4);
+            const dim3 grid((ni + 31) / 32, (nj + 3) / 4);
+            zline_sweep_kernel<T, false><<<grid, block, 0, ctx->stream>>>(a);
+        }
+        ++ctx->launches;
+    }
+    seam_sync<T>(ctx, g, loc, delta);
+    return check_cuda("zline_jacobi");
+}
+
+template gb_status zline_sweeps<double>(gb_ctx*, const gb_grid&, int, const double*, const double*, const double*, int,
+                                        double*, unsigned long long*, LineScratch);
+template gb_status zline_sweeps<float>(gb_ctx*, const gb_grid&, int, const float*, const float*, const float*, int,
+                                       float*, unsigned long long*, LineScratch);
+template void seam_sync<double>(gb_ctx*, const gb_grid&, int, double*);
+template void seam_sync<float>(gb_ctx*, const gb_grid&, int, float*);
+
+}  // namespace gb
+
+namespace {
+
+template <typename T>
+gb_status zline_jacobi_api(gb_ctx* ctx, const gb_grid* g, int32_t loc, const T* A, const T* ap, const T* rhs,
+                           int32_t sweeps, T* delta, T* change)
+{
+    gb::clear_error();
+    const char* op = "zline_jacobi";
+    if (ctx == nullptr) {
+        gb::set_error("gust: %s: ctx is null", op);
+        return GB_BAD_ARG;
+    }
+    gb_status st = gb::check_grid(op, g);
+    if (st != GB_OK) { return st; }
+    if ((st = gb::check_loc(op, loc)) != GB_OK) { return st; }
+    if (sweeps < 1) {
+        gb::set_error("gust: zline_jacobi: sweeps must be >= 1 (got %d)", sweeps);
+        return GB_BAD_ARG;
+    }
+    if (A == nullptr || ap == nullptr || rhs == nullptr || delta == nullptr) {
+        gb::set_error("gust: zline_jacobi: A, ap, rhs and delta must be device arrays of the grid");
+        return GB_BAD_ARG;
+    }
+    // delta.setVal(0): the ghosts outside the domain stay 0 (the couplings are folded).
+    cudaMemsetAsync(delta, 0, sizeof(T) * gb::volume(*g), ctx->stream);
+    st = gb::zline_sweeps<T>(ctx, *g, loc, A, ap, rhs, sweeps, delta, gb::dword(ctx, 0), gb::LineScratch::automatic);
+    if (st != GB_OK) { return st; }
+    unsigned long long w = 0;
+    if ((st = gb::read_words(ctx, 0, 1, &w)) != GB_OK) { return st; }
+    if (change != nullptr) { *change = static_cast<T>(gb::bits_to_double(w)); }
+    return GB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+gb_status gb_zline_jacobi(gb_ctx* ctx, const gb_grid* g, int32_t loc, const double* A, const double* ap,
+                          const double* rhs, int32_t sweeps, double* delta, double* change)
+{
+    return zline_jacobi_api<double>(ctx, g, loc, A, ap, rhs, sweeps, delta, change);
+}
+
+gb_status gb_zline_jacobi_f32(gb_ctx* ctx, const gb_grid* g, int32_t loc, const float* A, const float* ap,
+                              const float* rhs, int32_t sweeps, float* delta, float* change)
+{
+    return zline_jacobi_api<float>(ctx, g, loc, A, ap, rhs, sweeps, delta, change);
+}
+
+}  // extern "C"

@@ -1,0 +1,31 @@
+// z-line relaxation entry points shared by the C ABI, the momentum predictor,
+// the scalar sweeps and the multigrid smoother.
+#pragma once
+
+#include "gb_common.cuh"
+
+namespace gb {
+
+//! Scratch slots of a context (each call family owns its slots).
+enum ScratchSlot : int {
+    kSlotLineNext = 0,
+    kSlotLineC,
+    kSlotLineE,
+    kSlotFirstFree
+};
+
+enum class LineScratch { automatic, shared, global };
+
+//! `sweeps` z-line Jacobi sweeps into delta (which must hold 0 on entry,
+//! ghosts included). change_word (device, may be null) receives the bit
+//! pattern of max |change over the last sweep|. No host synchronisation.
+template <typename T>
+gb_status zline_sweeps(gb_ctx* ctx, const gb_grid& g, int loc, const T* A, const T* ap, const T* rhs, int sweeps,
+                       T* delta, unsigned long long* change_word, LineScratch scratch_kind);
+
+//! OverrideSync of a field at loc: the high copy of a periodic seam takes the
+//! low copy's value.
+template <typename T>
+void seam_sync(gb_ctx* ctx, const gb_grid& g, int loc, T* f);
+
+}  // namespace gb

@@ -1,0 +1,121 @@
+/*
+ * gust_b200.h -- C ABI of the B200-native SIMPLEC hot path of GUST
+ * (hgopalan/ablsteadyrans): z-line relaxation, the terrain-following
+ * pressure-correction Poisson solve and the control-volume residual stencils.
+ *
+ * Conventions
+ *  - Plain C, POD arguments only. Field pointers are DEVICE pointers to arrays
+ *    laid out by gb_grid (below); scalars and result structs live on the host.
+ *  - Every call returns a gb_status and never aborts the process. On an error
+ *    gb_last_error() returns a message naming the argument or the inputs key,
+ *    in the reference's "gust: <op>: <what>" form.
+ *  - Work is ordered on the stream of the gb_ctx passed in. A call that
+ *    returns a host scalar (a norm, a change) synchronises that stream.
+ *  - Location codes follow the reference's bit mask (Stencil_K.H): bit d set
+ *    means nodal in direction d.
+ *
+ * Data layout (one layout per grid, for every location type):
+ *   every array of a grid is (nz+1+2ng) k-planes of (ny+1+2ng) rows of
+ *   pitch_x elements, i fastest, then j, then k ("k-plane-major SoA"). Point
+ *   (i, j, k) of any location type (cell, face, node) sits at element
+ *       (i + ng) + (j + ng) * sy + (k + ng) * sz,
+ *   so cell, face and node arrays share one index space and one stencil
+ *   arithmetic, as AMReX's Array4 does for one box. Multi-component arrays
+ *   (the implicit coefficients) store component c at c * gb_grid_volume(g).
+ */
+#ifndef GUST_B200_H_
+#define GUST_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum gb_status {
+    GB_OK = 0,
+    GB_BAD_ARG = 1,        /* an argument or an inputs value out of range */
+    GB_NONFINITE = 2,      /* a NaN or inf in an input or a result */
+    GB_NOT_CONVERGED = 3,  /* an iterative solve hit its iteration limit */
+    GB_TIMEOUT = 4,        /* a bounded device-side wait gave up */
+    GB_OOM = 5,            /* device memory could not be allocated */
+    GB_CUDA = 6            /* a CUDA runtime error */
+} gb_status;
+
+/* Location of a field's points (the reference's Loc, CVFluxes.H:20). */
+enum { GB_LOC_CELL = 0, GB_LOC_XFACE = 1, GB_LOC_YFACE = 2, GB_LOC_ZFACE = 4, GB_LOC_NODE = 7 };
+
+/* Components of the implicit coefficients (ImplicitOperator.H:57). */
+enum { GB_COEF_P = 0, GB_COEF_XM, GB_COEF_XP, GB_COEF_YM, GB_COEF_YP, GB_COEF_ZM, GB_COEF_ZP, GB_N_COEFS };
+
+typedef struct gb_grid {
+    int32_t nx, ny, nz;        /* cells */
+    int32_t ng;                /* ghost layers every array holds (>= 2) */
+    int32_t periodic_x;        /* 1: periodic in x (amrex::Geometry::isPeriodic(0)) */
+    int32_t periodic_y;
+    int64_t sy, sz;            /* element strides of j and k; the i stride is 1 */
+    double dx, dy, dzeta;      /* computational cell sizes, geom.CellSize() */
+} gb_grid;
+
+/* Fill g for nx x ny x nz cells with ng ghost layers and the default pitch. */
+gb_status gb_grid_init(gb_grid* g, int32_t nx, int32_t ny, int32_t nz, int32_t ng, double dx, double dy,
+                       double dzeta, int32_t periodic_x, int32_t periodic_y);
+/* Elements of one array of the grid (one component). */
+int64_t gb_grid_volume(const gb_grid* g);
+
+/* ---- context ------------------------------------------------------------ */
+typedef struct gb_ctx gb_ctx;
+
+/* A context on the current CUDA device, ordering its work on `stream` (a
+ * cudaStream_t; NULL = the legacy default stream). It owns the scratch the
+ * calls below need (grown on demand, freed by gb_ctx_destroy). One context per
+ * host thread. */
+gb_status gb_ctx_create(void* stream, gb_ctx** out);
+gb_status gb_ctx_destroy(gb_ctx* ctx);
+/* Kernel launches this context has issued (all calls), for launch accounting. */
+int64_t gb_ctx_launches(const gb_ctx* ctx);
+/* Kernel families timed by the context's profiler. */
+enum {
+    GB_KERNEL_LINE_SWEEP = 0,   /* z-line Thomas sweep (one launch per sweep) */
+    GB_KERNEL_POISSON_APPLY,    /* terrain Poisson operator apply / residual */
+    GB_KERNEL_MG_SMOOTH,        /* multigrid z-line smoother */
+    GB_KERNEL_MG_TRANSFER,      /* restriction / prolongation */
+    GB_KERNEL_RESIDUAL,         /* control-volume residual stencils */
+    GB_KERNEL_MASSFLUX,         /* mass-flux / divergence kernels */
+    GB_KERNEL_COEFS,            /* implicit coefficients and row folds */
+    GB_KERNEL_VECTOR,           /* vector ops and reductions */
+    GB_KERNEL_BC,               /* ghost fills */
+    GB_N_KERNEL_FAMILIES
+};
+/* Profiling: with enable = 1 every launch of a timed family is bracketed by
+ * CUDA events on the context's stream (enable clears earlier spans).
+ * gb_ctx_profile_read sums the recorded spans of one family. */
+gb_status gb_ctx_profile(gb_ctx* ctx, int32_t enable);
+gb_status gb_ctx_profile_read(gb_ctx* ctx, int32_t family, double* total_ms, int64_t* spans);
+/* The last error message of the calling thread ("" after success). */
+const char* gb_last_error(void);
+
+/* ---- z-line relaxation -------------------------------------------------- */
+
+/* The z-line Jacobi solve, replacing gust::zline_jacobi (Source/Predictor.H:267-268,
+ * Source/Predictor.cpp:87-127; column kernel gust::solve_column,
+ * Source/LineSolve_K.H:22-45): `sweeps` sweeps of the system with the
+ * off-diagonal coefficients of A (GB_N_COEFS components at loc) and the
+ * diagonal ap, right-hand side rhs, into delta (set to 0 first, x/y neighbours
+ * lagged, periodic images through the grid, zero outside the domain). Every
+ * (i, j) column is solved exactly for (-a_zm, ap, -a_zp) by the Thomas
+ * recurrences. *change receives max |change over the last sweep|. The two
+ * copies of a periodic seam face are made identical afterwards (OverrideSync:
+ * the low copy wins). */
+gb_status gb_zline_jacobi(gb_ctx* ctx, const gb_grid* g, int32_t loc, const double* A, const double* ap,
+                          const double* rhs, int32_t sweeps, double* delta, double* change);
+/* The same in FP32 (the inner solver of the mixed-precision defect correction). */
+gb_status gb_zline_jacobi_f32(gb_ctx* ctx, const gb_grid* g, int32_t loc, const float* A, const float* ap,
+                              const float* rhs, int32_t sweeps, float* delta, float* change);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GUST_B200_H_ */

@@ -1,0 +1,22 @@
+import os
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA device (B200) and the built libgustb200.so")
+
+
+@pytest.fixture(scope="session")
+def ctx():
+    import torch
+    from ablsteadyrans_b200 import Context
+    torch.cuda.init()
+    c = Context()
+    yield c
+    c.close()

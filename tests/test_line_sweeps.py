@@ -1,0 +1,121 @@
+"""z-line relaxation (gust::zline_jacobi, Source/Predictor.cpp:87-127; column
+kernel Source/LineSolve_K.H:22-45).
+
+CPU tests pin the oracle to the reference's own known answers
+(test_Predictor.cpp:378-442: the sweeps converge to the dense solve, the error
+falls with the sweep count; test_LineSweeps.cpp: M-matrix systems at every
+location, periodic seams). GPU tests compare the CUDA path through the C ABI
+with the oracle on the same seeded systems: FP64 to 1e-12 relative (one
+sweep and several), FP32 to 2e-5 relative.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from helpers import LOCS, Grid, dense_line_system_solve, random_system, rel_err, to_dev, to_host
+
+CASES = [
+    # nx, ny, nz, periodic_x, periodic_y
+    (5, 4, 6, False, False),
+    (6, 5, 7, True, True),
+    (4, 7, 5, True, False),
+    (1, 1, 12, True, True),
+]
+
+
+@pytest.mark.parametrize("loc", LOCS)
+@pytest.mark.parametrize("case", CASES)
+def test_oracle_converges_to_dense_solve(loc, case):
+    nx, ny, nz, px, py = case
+    g = Grid(nx, ny, nz, 30.0, 30.0, 10.0, px, py)
+    A, ap, rhs = random_system(g, loc, seed=7 + loc, extra=0.3)
+    exact = dense_line_system_solve(g, loc, A, ap, rhs)
+    scale = np.abs(exact).max()
+    v = g.valid(loc)
+    # the error falls with the sweeps (every 4 sweeps in the max norm: a random
+    # M-matrix's Jacobi error need not fall at every single sweep)
+    prev = np.inf
+    for sweeps in (1, 4, 16):
+        d = g.np_zeros()
+        oracle.zline_jacobi(g, loc, A, ap, rhs, sweeps, d)
+        err = np.abs(d - exact)[v].max() / scale
+        if prev > 1e-14:
+            assert err < prev, (sweeps, err, prev)
+        prev = err
+    d = g.np_zeros()
+    change = oracle.zline_jacobi(g, loc, A, ap, rhs, 400, d)
+    assert np.abs(d - exact)[v].max() / scale < 1e-12
+    assert change / scale < 1e-12
+    # the ghosts below the ground and above the top stay 0
+    assert np.all(d[: g.ng] == 0) and np.all(d[g.ng + g.extents(loc)[2]:] == 0)
+
+
+def test_oracle_single_sweep_is_the_column_solve():
+    """One sweep from delta = 0 is the exact tridiagonal solve of each column."""
+    g = Grid(3, 2, 9, 25.0, 25.0, 5.0, False, False)
+    A, ap, rhs = random_system(g, 0, seed=3)
+    d = g.np_zeros()
+    change = oracle.zline_jacobi(g, 0, A, ap, rhs, 1, d)
+    G = g.ng
+    for j in range(2):
+        for i in range(3):
+            nk = 9
+            M = np.zeros((nk, nk))
+            for k in range(nk):
+                M[k, k] = ap[k + G, j + G, i + G]
+                if k > 0:
+                    M[k, k - 1] = -A[5, k + G, j + G, i + G]
+                if k < nk - 1:
+                    M[k, k + 1] = -A[6, k + G, j + G, i + G]
+            x = np.linalg.solve(M, rhs[G:G + nk, j + G, i + G])
+            np.testing.assert_allclose(d[G:G + nk, j + G, i + G], x, rtol=1e-13, atol=1e-14)
+    assert change == pytest.approx(np.abs(d).max(), rel=0, abs=0)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("loc", LOCS)
+@pytest.mark.parametrize("case", CASES + [(37, 29, 17, True, False), (64, 48, 48, False, True)])
+@pytest.mark.parametrize("sweeps", [1, 2, 5])
+def test_gpu_zline_jacobi_matches_oracle_fp64(ctx, loc, case, sweeps):
+    import torch
+    import ablsteadyrans_b200 as gb
+    nx, ny, nz, px, py = case
+    g = Grid(nx, ny, nz, 30.0, 30.0, 10.0, px, py)
+    A, ap, rhs = random_system(g, loc, seed=11 + 3 * loc + sweeps, extra=0.2, xscale=3.0)
+    d_ref = g.np_zeros()
+    ch_ref = oracle.zline_jacobi(g, loc, A, ap, rhs, sweeps, d_ref)
+    dA, dap, drhs = to_dev(A), to_dev(ap), to_dev(rhs)
+    dd = torch.full(g.shape, 7.0, dtype=torch.float64, device="cuda")  # overwritten: delta starts at 0
+    ch = gb.zline_jacobi(ctx, g, loc, dA, dap, drhs, sweeps, dd)
+    d = to_host(dd)
+    assert rel_err(d, d_ref, g.valid(loc)) < 1e-12
+    assert abs(ch - ch_ref) <= 1e-12 * max(abs(ch_ref), 1e-300)
+    # ghosts outside the domain are 0
+    G = g.ng
+    assert np.all(d[:G] == 0)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("loc", LOCS)
+def test_gpu_zline_jacobi_fp32(ctx, loc):
+    import torch
+    import ablsteadyrans_b200 as gb
+    g = Grid(40, 33, 24, 30.0, 30.0, 10.0, True, False)
+    A, ap, rhs = random_system(g, loc, seed=99 + loc, extra=0.5)
+    d_ref = g.np_zeros()
+    oracle.zline_jacobi(g, loc, A, ap, rhs, 3, d_ref)
+    dd = torch.zeros(g.shape, dtype=torch.float32, device="cuda")
+    gb.zline_jacobi(ctx, g, loc, to_dev(A, torch.float32), to_dev(ap, torch.float32), to_dev(rhs, torch.float32), 3, dd)
+    assert rel_err(to_host(dd), d_ref, g.valid(loc)) < 2e-5
+
+
+@pytest.mark.gpu
+def test_gpu_zline_jacobi_refusals(ctx):
+    import torch
+    import ablsteadyrans_b200 as gb
+    g = Grid(4, 4, 4, 1.0, 1.0, 1.0)
+    z = torch.zeros((7,) + g.shape, dtype=torch.float64, device="cuda")
+    with pytest.raises(gb.GustError, match="sweeps must be >= 1"):
+        gb.zline_jacobi(ctx, g, 0, z, z[0], z[0], 0, z[1])
+    with pytest.raises(gb.GustError, match="loc must be"):
+        gb.zline_jacobi(ctx, g, 3, z, z[0], z[0], 1, z[1])
