@@ -73,6 +73,26 @@ __device__ __forceinline__ void atomic_max_nonneg(unsigned long long* slot, floa
     atomic_max_nonneg(slot, static_cast<double>(v));
 }
 
+// ------------------------------------------------------ asynchronous copy ---
+
+//! Asynchronous global -> shared copy of one element (cp.async, LDGSTS):
+//! the copy completes in the background; cp_async_wait<N>() waits until at
+//! most N of this thread's committed groups are still in flight.
+template <typename T>
+__device__ __forceinline__ void cp_async_elem(T* smem_dst, const T* gmem_src)
+{
+    static_assert(sizeof(T) == 4 || sizeof(T) == 8, "4- or 8-byte elements");
+    const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
+    if constexpr (sizeof(T) == 8) {
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem_src) : "memory");
+    } else {
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem_src) : "memory");
+    }
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
 // ---------------------------------------------------------------- errors ---
 
 void set_error(const char* fmt, ...);

@@ -14,7 +14,7 @@ enum ScratchSlot : int {
     kSlotFirstFree
 };
 
-enum class LineScratch { automatic, shared, global };
+enum class LineScratch { automatic, pipelined, shared, global };
 
 //! `sweeps` z-line Jacobi sweeps into delta (which must hold 0 on entry,
 //! ghosts included). change_word (device, may be null) receives the bit

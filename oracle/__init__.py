@@ -48,6 +48,28 @@ def _declare(L):
     L.og_override_sync.argtypes = [G, i32, P]
     L.og_zline_jacobi.argtypes = [G, i32, P, P, P, i32, P]
     L.og_zline_jacobi.restype = f64
+    # mesh and Poisson layer
+    I = ctypes.POINTER(ctypes.c_int)
+    L.og_btf_heights.argtypes = [G, P, P, P]
+    L.og_metrics.argtypes = [G, P, P, P, P, P, P]
+    L.og_poisson_fill_ghosts.argtypes = [G, I, P, i32]
+    L.og_poisson_zero_flux_faces.argtypes = [G, I]
+    L.og_poisson_zero_flux_faces.restype = i32
+    L.og_poisson_apply.argtypes = [G, I, P, P, P, P, P, P, P]
+    L.og_poisson_fluxes.argtypes = [G, I, P, P, P, P, P, P, P, P]
+    L.og_face_divergence.argtypes = [G, P, P, P, P, P, P, P, P]
+    L.og_weighted_mean.argtypes = [G, P, P]
+    L.og_weighted_mean.restype = f64
+    L.og_mg_create.argtypes = [G, I, P, P, P, P, P, i32, i32, i32, i32, i32]
+    L.og_mg_create.restype = P
+    L.og_mg_destroy.argtypes = [P]
+    L.og_mg_levels.argtypes = [P]
+    L.og_mg_levels.restype = i32
+    L.og_mg_vcycle.argtypes = [P, P, P]
+    L.og_poisson_solve.argtypes = [P, P, P, f64, f64, i32, i32, i32, ctypes.POINTER(f64)]
+    L.og_poisson_solve.restype = i32
+    L.og_line_tridiag.argtypes = [G, I, i32, P, P, P, P, P, i32, i32, i32, ctypes.POINTER(f64),
+                                  ctypes.POINTER(f64), ctypes.POINTER(f64)]
 
 
 def _p(a):
@@ -72,3 +94,90 @@ def fill_periodic(grid, loc, f, layers=1):
 def zline_jacobi(grid, loc, A, ap, rhs, sweeps, delta):
     """Source/Predictor.cpp:87-127 restated; returns the last sweep's change."""
     return float(lib().og_zline_jacobi(ctypes.byref(grid.c), loc, _p(A), _p(ap), _p(rhs), int(sweeps), _p(delta)))
+
+
+# ------------------------------------------------------------ mesh / Poisson
+PERIODIC, NEUMANN, DIRICHLET = 0, 1, 2
+
+
+def _bc(bc):
+    arr = (ctypes.c_int * 6)(*[int(b) for b in bc])
+    return arr
+
+
+def btf_heights(grid, zlevels, ground):
+    """BTF node heights (ERF_TerrainMetrics.cpp BTF, Source/Mesh.cpp fill_ghost_columns).
+    ground: (ny+3, nx+3) heights of node columns i, j in [-1, n+1]."""
+    z = grid.np_zeros()
+    zl = np.ascontiguousarray(zlevels, dtype=np.float64)
+    gr = np.ascontiguousarray(ground, dtype=np.float64)
+    lib().og_btf_heights(ctypes.byref(grid.c), _p(zl), _p(gr), _p(z))
+    return z
+
+
+def metrics(grid, z):
+    """detJ, ax, ay, az, z_cc (ERF_TerrainMetrics.cpp:680-808)."""
+    out = [grid.np_zeros() for _ in range(5)]
+    lib().og_metrics(ctypes.byref(grid.c), _p(z), *[_p(a) for a in out])
+    return out
+
+
+def poisson_fill_ghosts(grid, bc, phi, ground_even=True):
+    lib().og_poisson_fill_ghosts(ctypes.byref(grid.c), _bc(bc), _p(phi), int(ground_even))
+
+
+def poisson_apply(grid, bc, AX, AY, AZ, J, z, phi):
+    y = grid.np_zeros()
+    lib().og_poisson_apply(ctypes.byref(grid.c), _bc(bc), _p(AX), _p(AY), _p(AZ), _p(J), _p(z), _p(phi), _p(y))
+    return y
+
+
+def poisson_fluxes(grid, bc, z, phi, bx=None, by=None, bz=None):
+    f = [grid.np_zeros() for _ in range(3)]
+    lib().og_poisson_fluxes(ctypes.byref(grid.c), _bc(bc), _p(z), _p(phi), _p(bx), _p(by), _p(bz), *[_p(a) for a in f])
+    return f
+
+
+def face_divergence(grid, ax, ay, az, J, fx, fy, fz):
+    d = grid.np_zeros()
+    lib().og_face_divergence(ctypes.byref(grid.c), _p(ax), _p(ay), _p(az), _p(J), _p(fx), _p(fy), _p(fz), _p(d))
+    return d
+
+
+def weighted_mean(grid, f, J):
+    return float(lib().og_weighted_mean(ctypes.byref(grid.c), _p(f), _p(J)))
+
+
+class Multigrid:
+    """This project's multigrid (poisson.c): levels, one V-cycle, the solve."""
+
+    def __init__(self, grid, bc, z, J, AX, AY, AZ, max_levels=12, min_coarse=2, nu1=1, nu2=1, nu_coarse=8):
+        self.grid = grid
+        self._keep = [np.ascontiguousarray(a) for a in (z, J, AX, AY, AZ)]
+        self._h = lib().og_mg_create(ctypes.byref(grid.c), _bc(bc), *[_p(a) for a in self._keep],
+                                     max_levels, min_coarse, nu1, nu2, nu_coarse)
+
+    @property
+    def levels(self):
+        return int(lib().og_mg_levels(self._h))
+
+    def vcycle(self, r):
+        e = self.grid.np_zeros()
+        lib().og_mg_vcycle(self._h, _p(np.ascontiguousarray(r)), _p(e))
+        return e
+
+    def solve(self, rhs, reltol=1e-10, abstol=0.0, max_iter=200, restart=30, precond=True):
+        """Returns (phi, iterations, initial residual, final residual, removed mean);
+        rhs is modified (its J-weighted mean removed when singular)."""
+        phi = self.grid.np_zeros()
+        res = (ctypes.c_double * 3)()
+        it = lib().og_poisson_solve(self._h, _p(rhs), _p(phi), reltol, abstol, max_iter, restart, int(precond), res)
+        return phi, int(it), res[0], res[1], res[2]
+
+    def close(self):
+        if self._h:
+            lib().og_mg_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()

@@ -100,3 +100,58 @@ def rel_err(a, b, v=None):
         a, b = a[v], b[v]
     scale = max(np.abs(b).max(), 1e-300)
     return float(np.abs(a - b).max() / scale)
+
+
+# ------------------------------------------------------------------ Poisson
+GOLDEN = __import__("os").path.join(__import__("os").path.dirname(__import__("os").path.abspath(__file__)), "golden")
+PERIODIC, NEUMANN, DIRICHLET = 0, 1, 2
+
+
+def askervein_case():
+    """The reference's Poisson_Askervein projection (Tests/Supporting_Files/Tools/
+    poisson_projection.cpp): BTF mesh on ERF's Askervein terrain (fixture), the
+    fixed wind u = 8 (1 + 0.2 sin(2 pi y/Ly)), v = 2.4 cos(2 pi x/Lx) (0 on the y
+    walls), w = 0; x low Neumann, x high Dirichlet, y Neumann, ground Neumann,
+    top Dirichlet."""
+    import oracle
+    d = np.load(__import__("os").path.join(GOLDEN, "poisson_askervein.npz"))
+    nx, ny, nz = 30, 30, 18
+    plo, phi_hi = d["prob_lo"], d["prob_hi"]
+    g = Grid(nx, ny, nz, (phi_hi[0] - plo[0]) / nx, (phi_hi[1] - plo[1]) / ny, (phi_hi[2] - plo[2]) / nz)
+    z = oracle.btf_heights(g, d["zlevels"], d["ground"])
+    J, ax, ay, az, zcc = oracle.metrics(g, z)
+    Lx, Ly = phi_hi[0] - plo[0], phi_hi[1] - plo[1]
+    U = [g.np_zeros() for _ in range(3)]
+    G = g.ng
+    for k in range(nz):
+        for j in range(ny):
+            y = plo[1] + (j + 0.5) * g.dy
+            U[0][k + G, j + G, G:G + nx + 1] = 8.0 * (1 + 0.2 * np.sin(2 * np.pi * (y - plo[1]) / Ly))
+        for j in range(ny + 1):
+            x = plo[0] + (np.arange(nx) + 0.5) * g.dx
+            wall = (j == 0) or (j == ny)
+            U[1][k + G, j + G, G:G + nx] = 0.0 if wall else 2.4 * np.cos(2 * np.pi * (x - plo[0]) / Lx)
+    bc = (NEUMANN, NEUMANN, NEUMANN, DIRICHLET, NEUMANN, DIRICHLET)
+    return dict(grid=g, z=z, J=J, ax=ax, ay=ay, az=az, U=U, bc=bc, phi_gold=d["phi"],
+                info=__import__("json").loads(str(d["info"])))
+
+
+def smooth_terrain_case(nx, ny, nz, periodic_x, periodic_y, hill=80.0, dx=40.0, seed=0):
+    """A BTF mesh over a smooth Gaussian hill (periodic images or clamped
+    ghost columns as the reference builds them), stretched layers to 1500 m."""
+    import oracle
+    g = Grid(nx, ny, nz, dx, dx, 1500.0 / nz, periodic_x, periodic_y)
+    r = 1500.0 ** (1.0 / nz)
+    zl = np.concatenate([[0.0], np.cumsum(2.0 * 1.06 ** np.arange(nz))])
+    zl = zl * (1500.0 / zl[-1])
+    ground = np.zeros((ny + 3, nx + 3))
+    cx, cy = nx * dx / 2, ny * dx / 2
+    for j in range(-1, ny + 2):
+        for i in range(-1, nx + 2):
+            ii = (i % nx) if periodic_x else min(max(i, 0), nx)
+            jj = (j % ny) if periodic_y else min(max(j, 0), ny)
+            x, y = ii * dx - cx, jj * dx - cy
+            ground[j + 1, i + 1] = hill * np.exp(-(x * x + y * y) / (0.2 * (nx * dx) ** 2))
+    z = oracle.btf_heights(g, zl, ground)
+    J, ax, ay, az, zcc = oracle.metrics(g, z)
+    return g, z, J, ax, ay, az, zcc
