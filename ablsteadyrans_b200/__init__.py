@@ -26,6 +26,7 @@ _lib = None
 GB_OK = 0
 KERNEL_LINE_SWEEP, KERNEL_POISSON_APPLY, KERNEL_MG_SMOOTH, KERNEL_MG_TRANSFER, KERNEL_RESIDUAL, \
     KERNEL_MASSFLUX, KERNEL_COEFS, KERNEL_VECTOR, KERNEL_BC = range(9)
+TUNE_LINE_VARIANT, TUNE_LINE_BLOCK, TUNE_MG_SMOOTH_BLOCK = range(3)
 STATUS_NAMES = {0: "OK", 1: "BAD_ARG", 2: "NONFINITE", 3: "NOT_CONVERGED", 4: "TIMEOUT", 5: "OOM", 6: "CUDA"}
 
 
@@ -61,6 +62,7 @@ def _declare(L):
     L.gb_ctx_destroy.argtypes = [P]
     L.gb_ctx_launches.argtypes = [P]
     L.gb_ctx_launches.restype = i64
+    L.gb_ctx_tune.argtypes = [P, i32, i32]
     L.gb_ctx_profile.argtypes = [P, i32]
     L.gb_ctx_profile_read.argtypes = [P, i32, ctypes.POINTER(f64), ctypes.POINTER(i64)]
     L.gb_zline_jacobi.argtypes = [P, G, i32, P, P, P, i32, P, ctypes.POINTER(f64)]
@@ -95,6 +97,9 @@ class Context:
 
     def launches(self):
         return int(lib().gb_ctx_launches(self._h))
+
+    def tune(self, key, value):
+        check(lib().gb_ctx_tune(self._h, int(key), int(value)))
 
     def profile(self, enable):
         check(lib().gb_ctx_profile(self._h, int(bool(enable))))
@@ -133,3 +138,128 @@ def zline_jacobi(ctx, grid, loc, A, ap, rhs, sweeps, delta):
         check(L.gb_zline_jacobi_f32(ctx.handle, ctypes.byref(grid.c), loc, _ptr(A), _ptr(ap), _ptr(rhs), sweeps,
                                     _ptr(delta), ctypes.byref(out)))
     return float(out.value)
+
+
+# ------------------------------------------------------------------- mesh ---
+POISSON_PERIODIC, POISSON_NEUMANN, POISSON_DIRICHLET = 0, 1, 2
+
+
+class PoissonOptions(ctypes.Structure):
+    """gb_poisson_opts: the solver.poisson_* inputs plus the multigrid settings."""
+    _fields_ = [("reltol", ctypes.c_double), ("abstol", ctypes.c_double), ("max_iter", ctypes.c_int32),
+                ("restart", ctypes.c_int32), ("precision", ctypes.c_int32), ("nu1", ctypes.c_int32),
+                ("nu2", ctypes.c_int32), ("nu_coarse", ctypes.c_int32), ("max_levels", ctypes.c_int32),
+                ("min_coarse", ctypes.c_int32)]
+
+    @classmethod
+    def default(cls, **kw):
+        o = cls()
+        check(lib().gb_poisson_options_default(ctypes.byref(o)))
+        for k, v in kw.items():
+            setattr(o, k, v)
+        return o
+
+
+class PoissonResult(ctypes.Structure):
+    _fields_ = [("iterations", ctypes.c_int32), ("singular", ctypes.c_int32), ("initial_residual", ctypes.c_double),
+                ("final_residual", ctypes.c_double), ("removed_mean", ctypes.c_double)]
+
+
+def _declare_poisson(L):
+    P = ctypes.c_void_p
+    G = ctypes.POINTER(GbGrid)
+    L.gb_mesh_metrics.argtypes = [P, G, P, P, P, P, P, P]
+    L.gb_face_divergence.argtypes = [P, G, P, P, P, P, P, P, P, P]
+    L.gb_poisson_options_default.argtypes = [ctypes.POINTER(PoissonOptions)]
+    L.gb_poisson_create.argtypes = [P, G, ctypes.POINTER(ctypes.c_int32), P, P, ctypes.POINTER(PoissonOptions),
+                                    ctypes.POINTER(P)]
+    L.gb_poisson_destroy.argtypes = [P]
+    L.gb_poisson_set_coeffs.argtypes = [P, P, P, P, P, P, P]
+    L.gb_poisson_apply.argtypes = [P, P, P]
+    L.gb_poisson_vcycle.argtypes = [P, P, P]
+    L.gb_poisson_solve.argtypes = [P, P, P, ctypes.POINTER(PoissonResult)]
+    L.gb_poisson_fluxes.argtypes = [P, P, P, P, P, P, P, P]
+
+
+_declare_hooks = [_declare_poisson]
+
+
+def _lib_full():
+    L = lib()
+    if not getattr(L, "_gb_full", False):
+        for h in _declare_hooks:
+            h(L)
+        L._gb_full = True
+    return L
+
+
+def _zeros(grid, dtype=None):
+    import torch
+    return torch.zeros(grid.shape, dtype=dtype or torch.float64, device="cuda")
+
+
+def mesh_metrics(ctx, grid, z_nd):
+    """detJ, ax, ay, az, z_cc of the terrain-following mesh (Mesh::make_metrics,
+    Source/Mesh.cpp:147-152 -> ERF_TerrainMetrics.cpp:680-808)."""
+    out = [_zeros(grid) for _ in range(5)]
+    check(_lib_full().gb_mesh_metrics(ctx.handle, ctypes.byref(grid.c), _ptr(z_nd), *[_ptr(t) for t in out]))
+    return out
+
+
+def face_divergence(ctx, grid, ax, ay, az, J, fx, fy, fz, out=None):
+    """gust::face_divergence (Source/Poisson.cpp:733-764)."""
+    div = out if out is not None else _zeros(grid)
+    check(_lib_full().gb_face_divergence(ctx.handle, ctypes.byref(grid.c), _ptr(ax), _ptr(ay), _ptr(az), _ptr(J),
+                                         _ptr(fx), _ptr(fy), _ptr(fz), _ptr(div)))
+    return div
+
+
+class PoissonSolver:
+    """gust::PoissonSolver (Source/Poisson.H:135-161) on the GPU: the terrain
+    operator with face coefficients, multigrid-preconditioned FGMRES, fluxes.
+    z_nd and detJ are kept by reference (the mesh must outlive the solver)."""
+
+    def __init__(self, ctx, grid, z_nd, detJ, bc, options=None):
+        self.ctx = ctx
+        self.grid = grid
+        self._mesh = (z_nd, detJ)
+        self.options = options or PoissonOptions.default()
+        self._h = ctypes.c_void_p()
+        bcs = (ctypes.c_int32 * 6)(*[int(b) for b in bc])
+        check(_lib_full().gb_poisson_create(ctx.handle, ctypes.byref(grid.c), bcs, _ptr(z_nd), _ptr(detJ),
+                                            ctypes.byref(self.options), ctypes.byref(self._h)))
+
+    def set_coeffs(self, ax, ay, az, bx=None, by=None, bz=None):
+        self._coeffs = (ax, ay, az, bx, by, bz)
+        check(_lib_full().gb_poisson_set_coeffs(self._h, _ptr(ax), _ptr(ay), _ptr(az), _ptr(bx), _ptr(by), _ptr(bz)))
+
+    def apply(self, phi, out=None):
+        y = out if out is not None else _zeros(self.grid)
+        check(_lib_full().gb_poisson_apply(self._h, _ptr(phi), _ptr(y)))
+        return y
+
+    def vcycle(self, r, out=None):
+        e = out if out is not None else _zeros(self.grid)
+        check(_lib_full().gb_poisson_vcycle(self._h, _ptr(r), _ptr(e)))
+        return e
+
+    def solve(self, rhs, phi):
+        res = PoissonResult()
+        check(_lib_full().gb_poisson_solve(self._h, _ptr(rhs), _ptr(phi), ctypes.byref(res)))
+        return res
+
+    def fluxes(self, phi, bx=None, by=None, bz=None, out=None):
+        f = out if out is not None else [_zeros(self.grid) for _ in range(3)]
+        check(_lib_full().gb_poisson_fluxes(self._h, _ptr(phi), _ptr(bx), _ptr(by), _ptr(bz), *[_ptr(t) for t in f]))
+        return f
+
+    def close(self):
+        if self._h:
+            check(_lib_full().gb_poisson_destroy(self._h))
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -123,6 +123,8 @@ struct gb_ctx {
     struct Span { int family; cudaEvent_t start, stop; };
     std::vector<Span> spans;
     std::vector<cudaEvent_t> event_pool;
+    //! Tuning knobs (GB_TUNE_*), 0 = default.
+    int tune[GB_N_TUNE] = {};
 };
 
 namespace gb {

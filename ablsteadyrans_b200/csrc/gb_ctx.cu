@@ -192,6 +192,17 @@ gb_status gb_ctx_destroy(gb_ctx* ctx)
 
 int64_t gb_ctx_launches(const gb_ctx* ctx) { return ctx == nullptr ? 0 : ctx->launches; }
 
+gb_status gb_ctx_tune(gb_ctx* ctx, int32_t key, int32_t value)
+{
+    gb::clear_error();
+    if (ctx == nullptr || key < 0 || key >= GB_N_TUNE) {
+        gb::set_error("gust: gb_ctx_tune: unknown context or key %d", key);
+        return GB_BAD_ARG;
+    }
+    ctx->tune[key] = value;
+    return GB_OK;
+}
+
 gb_status gb_ctx_profile(gb_ctx* ctx, int32_t enable)
 {
     gb::clear_error();

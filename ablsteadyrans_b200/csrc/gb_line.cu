@@ -261,14 +261,18 @@ gb_status zline_sweeps(gb_ctx* ctx, const gb_grid& g, int loc, const T* A, const
     T* tmp = static_cast<T*>(scratch(ctx, kSlotLineNext, sizeof(T) * vol));
     if (tmp == nullptr) { return GB_OOM; }
     const size_t smem = line_smem_bytes<T>(nk);
-    if (scratch_kind == LineScratch::automatic) { scratch_kind = LineScratch::pipelined; }
+    if (scratch_kind == LineScratch::automatic) {
+        const int v = ctx->tune[GB_TUNE_LINE_VARIANT];
+        scratch_kind = (v == 2) ? LineScratch::shared : (v == 3) ? LineScratch::global : LineScratch::pipelined;
+    }
     const bool pipelined = (scratch_kind == LineScratch::pipelined);
     bool use_smem = (scratch_kind == LineScratch::shared);
     T* cbuf = nullptr;
     T* ebuf = nullptr;
     // The pipelined kernel: one warp per block, R levels in flight (4 in FP64, 8 in FP32).
     constexpr int R = (sizeof(T) == 8) ? 4 : 8;
-    const int pipe_thr = 32;
+    const int pipe_thr = (ctx->tune[GB_TUNE_LINE_BLOCK] == 64 || ctx->tune[GB_TUNE_LINE_BLOCK] == 128)
+                           ? ctx->tune[GB_TUNE_LINE_BLOCK] : 32;
     const size_t pipe_smem_first = static_cast<size_t>(R * 4 + 2 * nk) * pipe_thr * sizeof(T);
     const size_t pipe_smem = static_cast<size_t>(R * 12 + 2 * nk) * pipe_thr * sizeof(T);
     if (pipelined) {

@@ -1,0 +1,957 @@
+// The pressure-correction Poisson layer on the GPU: mesh metrics, the
+// terrain operator (FP64 and FP32), fluxes, divergence, the multigrid
+// hierarchy (z-line zebra relaxation, x-y 2:1 coarsening, coarsest-level
+// relaxation) and the FP64 flexible GMRES it preconditions.
+//
+// Reference: gust::PoissonSolver (Source/Poisson.H:135-161, Source/Poisson.cpp:
+// 421-623), ERF's TerrainPoisson (extern_erf/ERF_TerrainPoisson.cpp:74-264),
+// the metrics (extern_erf/ERF_TerrainMetrics.cpp:680-808). The multigrid is
+// this project's own (the reference's default, AMReX MLTerrainPoisson, is not
+// in the reference's tree); it is restated by the oracle operation for
+// operation, so one V-cycle agrees with the oracle's to rounding.
+#include "gb_poisson.cuh"
+#include "gb_poisson_api.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+namespace gb {
+
+namespace {
+
+constexpr int kBlock = 256;
+
+inline int nblocks(int64_t n, int b = kBlock) { return static_cast<int>((n + b - 1) / b); }
+
+// ------------------------------------------------------------- metrics ---
+
+__global__ void k_metrics(gb_grid g, const double* __restrict__ z, double* __restrict__ J, double* __restrict__ ax,
+                          double* __restrict__ ay, double* __restrict__ zcc)
+{
+    // one thread per (i, j, k) in i, j in [-1, n+1], k in [-1, nz]
+    const int ni = g.nx + 3, nj = g.ny + 3, nk = g.nz + 2;
+    const int64_t n = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (n >= static_cast<int64_t>(ni) * nj * nk) { return; }
+    const int i = static_cast<int>(n % ni) - 1;
+    const int j = static_cast<int>((n / ni) % nj) - 1;
+    const int k = static_cast<int>(n / (static_cast<int64_t>(ni) * nj)) - 1;
+    const double dzi = 1.0 / g.dzeta;
+#define Z(a, b, c) z[at(g, a, b, c)]
+    if (k >= 0 && i <= g.nx && j <= g.ny) {
+        J[at(g, i, j, k)] = 0.25 * dzi
+            * (Z(i, j, k + 1) + Z(i + 1, j, k + 1) + Z(i, j + 1, k + 1) + Z(i + 1, j + 1, k + 1) - Z(i, j, k)
+               - Z(i + 1, j, k) - Z(i, j + 1, k) - Z(i + 1, j + 1, k));
+    }
+    if (k >= 0 && j <= g.ny) {
+        ax[at(g, i, j, k)] = 0.5 * dzi * (Z(i, j, k + 1) + Z(i, j + 1, k + 1) - Z(i, j, k) - Z(i, j + 1, k));
+    }
+    if (k >= 0 && i <= g.nx) {
+        ay[at(g, i, j, k)] = 0.5 * dzi * (Z(i, j, k + 1) + Z(i + 1, j, k + 1) - Z(i, j, k) - Z(i + 1, j, k));
+    }
+    if (i <= g.nx && j <= g.ny) {
+        zcc[at(g, i, j, k)] = 0.125 * (Z(i, j, k) + Z(i + 1, j, k) + Z(i, j + 1, k) + Z(i + 1, j + 1, k) + Z(i, j, k + 1)
+                                       + Z(i + 1, j, k + 1) + Z(i, j + 1, k + 1) + Z(i + 1, j + 1, k + 1));
+    }
+#undef Z
+}
+
+__global__ void k_fill(double* __restrict__ a, int64_t n, double v)
+{
+    const int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (t < n) { a[t] = v; }
+}
+
+// ------------------------------------------------------- valid-cell maps ---
+
+__device__ __forceinline__ bool cell_of(const gb_grid& g, int64_t n, int& i, int& j, int& k)
+{
+    if (n >= static_cast<int64_t>(g.nx) * g.ny * g.nz) { return false; }
+    i = static_cast<int>(n % g.nx);
+    j = static_cast<int>((n / g.nx) % g.ny);
+    k = static_cast<int>(n / (static_cast<int64_t>(g.nx) * g.ny));
+    return true;
+}
+
+// ------------------------------------------------------- operator apply ---
+
+//! y = A x, or with rhs given y = rhs - A x (the residual).
+template <typename T>
+__global__ void k_apply(gb_grid g, PBC b, const T* __restrict__ x, const T* __restrict__ AX, const T* __restrict__ AY,
+                        const T* __restrict__ AZ, const T* __restrict__ J, const T* __restrict__ z,
+                        const T* __restrict__ rhs, T* __restrict__ y)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = blockIdx.z;
+    if (i >= g.nx || j >= g.ny) { return; }
+    const T v = adotx<T>(g, b, i, j, k, x, x, AX, AY, AZ, J, z);
+    const int64_t o = at(g, i, j, k);
+    y[o] = rhs ? rhs[o] - v : v;
+}
+
+// ---------------------------------------------------------------- fluxes ---
+
+template <typename T>
+__device__ __forceinline__ T flux_x(const gb_grid& g, const PBC& b, int i, int j, int k, const T* x, const T* zp)
+{
+    const T dxinv = static_cast<T>(1.0 / g.dx), h = T(0.5), q = T(0.25);
+#define X(a, bb, c) ldc<T>(x, x, g, b, a, bb, c)
+#define Z(a, bb, c) zp[at(g, a, bb, c)]
+    T px_lo = (X(i, j, k) - X(i - 1, j, k)) * dxinv;
+    T pz_lo_md_hi = h * (X(i, j, k + 1) + X(i - 1, j, k + 1) - X(i, j, k) - X(i - 1, j, k));
+    T h_xi = q * (Z(i + 1, j, k + 1) - Z(i - 1, j, k + 1) + Z(i + 1, j + 1, k + 1) - Z(i - 1, j + 1, k + 1)) * dxinv;
+    T h_zeta = q * (Z(i, j, k + 2) - Z(i, j, k) + Z(i, j + 1, k + 2) - Z(i, j + 1, k));
+    pz_lo_md_hi *= h_xi / h_zeta;
+    T pz_lo_md_lo = h * (X(i, j, k) + X(i - 1, j, k) - X(i, j, k - 1) - X(i - 1, j, k - 1));
+    h_xi = q * (Z(i + 1, j, k) - Z(i - 1, j, k) + Z(i + 1, j + 1, k) - Z(i - 1, j + 1, k)) * dxinv;
+    h_zeta = q * (Z(i, j, k + 1) - Z(i, j, k - 1) + Z(i, j + 1, k + 1) - Z(i, j + 1, k - 1));
+    pz_lo_md_lo *= h_xi / h_zeta;
+    px_lo -= h * (pz_lo_md_hi + pz_lo_md_lo);
+    return -px_lo;
+#undef X
+#undef Z
+}
+
+template <typename T>
+__device__ __forceinline__ T flux_y(const gb_grid& g, const PBC& b, int i, int j, int k, const T* x, const T* zp)
+{
+    const T dyinv = static_cast<T>(1.0 / g.dy), h = T(0.5), q = T(0.25);
+#define X(a, bb, c) ldc<T>(x, x, g, b, a, bb, c)
+#define Z(a, bb, c) zp[at(g, a, bb, c)]
+    T py_lo = (X(i, j, k) - X(i, j - 1, k)) * dyinv;
+    T pz_md_lo_hi = h * (X(i, j, k + 1) + X(i, j - 1, k + 1) - X(i, j, k) - X(i, j - 1, k));
+    T h_eta = q * (Z(i, j + 1, k + 1) - Z(i, j - 1, k + 1) + Z(i + 1, j + 1, k + 1) - Z(i + 1, j - 1, k + 1)) * dyinv;
+    T h_zeta = q * (Z(i, j, k + 2) - Z(i, j, k) + Z(i + 1, j, k + 2) - Z(i + 1, j, k));
+    pz_md_lo_hi *= h_eta / h_zeta;
+    T pz_md_lo_lo = h * (X(i, j, k) + X(i, j - 1, k) - X(i, j, k - 1) - X(i, j - 1, k - 1));
+    h_eta = q * (Z(i, j + 1, k) - Z(i, j - 1, k) + Z(i + 1, j + 1, k) - Z(i + 1, j - 1, k)) * dyinv;
+    h_zeta = q * (Z(i, j, k + 1) - Z(i, j, k - 1) + Z(i + 1, j, k + 1) - Z(i + 1, j, k - 1));
+    pz_md_lo_lo *= h_eta / h_zeta;
+    py_lo -= h * (pz_md_lo_hi + pz_md_lo_lo);
+    return -py_lo;
+#undef X
+#undef Z
+}
+
+template <typename T>
+__device__ __forceinline__ T flux_z(const gb_grid& g, const PBC& b, int i, int j, int k, const T* x, const T* zp)
+{
+    const T dxinv = static_cast<T>(1.0 / g.dx), dyinv = static_cast<T>(1.0 / g.dy), h = T(0.5), q = T(0.25);
+#define X(a, bb, c) ldc<T>(x, x, g, b, a, bb, c)
+#define Z(a, bb, c) zp[at(g, a, bb, c)]
+    T h_xi, h_eta, h_zeta;
+    T pz_lo = X(i, j, k) - X(i, j, k - 1);
+    const T hzi = T(8) / ((Z(i, j, k + 1) + Z(i + 1, j, k + 1) + Z(i, j + 1, k + 1) + Z(i + 1, j + 1, k + 1))
+                          - (Z(i, j, k - 1) + Z(i + 1, j, k - 1) + Z(i, j + 1, k - 1) + Z(i + 1, j + 1, k - 1)));
+    pz_lo *= hzi;
+    const T px_hi_md_lo = h * (X(i + 1, j, k) - X(i, j, k) + X(i + 1, j, k - 1) - X(i, j, k - 1)) * dxinv;
+    const T px_lo_md_lo = h * (X(i, j, k) - X(i - 1, j, k) + X(i, j, k - 1) - X(i - 1, j, k - 1)) * dxinv;
+    const T py_md_hi_lo = h * (X(i, j + 1, k) - X(i, j, k) + X(i, j + 1, k - 1) - X(i, j, k - 1)) * dyinv;
+    const T py_md_lo_lo = h * (X(i, j, k) - X(i, j - 1, k) + X(i, j, k - 1) - X(i, j - 1, k - 1)) * dyinv;
+    T pz_hi_md_lo = h * (X(i + 1, j, k) + X(i, j, k) - X(i + 1, j, k - 1) - X(i, j, k - 1));
+    h_xi = q * (Z(i + 2, j, k) - Z(i, j, k) + Z(i + 2, j + 1, k) - Z(i, j + 1, k)) * dxinv;
+    h_zeta = q * (Z(i + 1, j, k + 1) - Z(i + 1, j, k - 1) + Z(i + 1, j + 1, k + 1) - Z(i + 1, j + 1, k - 1));
+    pz_hi_md_lo *= h_xi / h_zeta;
+    T pz_lo_md_lo = h * (X(i, j, k) + X(i - 1, j, k) - X(i, j, k - 1) - X(i - 1, j, k - 1));
+    h_xi = q * (Z(i + 1, j, k) - Z(i - 1, j, k) + Z(i + 1, j + 1, k) - Z(i - 1, j + 1, k)) * dxinv;
+    h_zeta = q * (Z(i, j, k + 1) - Z(i, j, k - 1) + Z(i, j + 1, k + 1) - Z(i, j + 1, k - 1));
+    pz_lo_md_lo *= h_xi / h_zeta;
+    T pz_md_hi_lo = h * (X(i, j + 1, k) + X(i, j, k) - X(i, j + 1, k - 1) - X(i, j, k - 1));
+    h_eta = q * (Z(i, j + 2, k) - Z(i, j, k) + Z(i + 1, j + 2, k) - Z(i + 1, j, k)) * dyinv;
+    h_zeta = q * (Z(i, j + 1, k + 1) - Z(i, j + 1, k - 1) + Z(i + 1, j + 1, k + 1) - Z(i + 1, j + 1, k - 1));
+    pz_md_hi_lo *= h_eta / h_zeta;
+    T pz_md_lo_lo = h * (X(i, j, k) + X(i, j - 1, k) - X(i, j, k - 1) - X(i, j - 1, k - 1));
+    h_eta = q * (Z(i, j + 1, k) - Z(i, j - 1, k) + Z(i + 1, j + 1, k) - Z(i + 1, j - 1, k)) * dyinv;
+    h_zeta = q * (Z(i, j, k + 1) - Z(i, j, k - 1) + Z(i + 1, j, k + 1) - Z(i + 1, j, k - 1));
+    pz_md_lo_lo *= h_eta / h_zeta;
+    const T h_xi_on_zlo = h * (Z(i + 1, j + 1, k) + Z(i + 1, j, k) - Z(i, j + 1, k) - Z(i, j, k)) * dxinv;
+    const T h_eta_on_zlo = h * (Z(i + 1, j + 1, k) + Z(i, j + 1, k) - Z(i + 1, j, k) - Z(i, j, k)) * dyinv;
+    pz_lo -= h * h_xi_on_zlo * ((px_hi_md_lo + px_lo_md_lo) - (pz_hi_md_lo + pz_lo_md_lo));
+    pz_lo -= h * h_eta_on_zlo * ((py_md_hi_lo + py_md_lo_lo) - (pz_md_hi_lo + pz_md_lo_lo));
+    if (k == 0) { pz_lo = T(0); }
+    return -pz_lo;
+#undef X
+#undef Z
+}
+
+//! The face fluxes -grad phi with the zero-flux faces masked, times beta
+//! (null: 1). One thread per node column (i, j) slot and level k.
+__global__ void k_fluxes(gb_grid g, PBC b, const double* __restrict__ phi, const double* __restrict__ z,
+                         const double* __restrict__ bx, const double* __restrict__ by, const double* __restrict__ bz,
+                         double* __restrict__ fx, double* __restrict__ fy, double* __restrict__ fz)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = blockIdx.z;
+    if (i > g.nx || j > g.ny) { return; }
+    if (j < g.ny && k < g.nz) {
+        double f = flux_x<double>(g, b, i, j, k, phi, z);
+        if (((b.zf & TP_XLO) && i == 0) || ((b.zf & TP_XHI) && i == g.nx)) { f = 0; }
+        const int64_t o = at(g, i, j, k);
+        fx[o] = bx ? f * bx[o] : f;
+    }
+    if (i < g.nx && k < g.nz) {
+        double f = flux_y<double>(g, b, i, j, k, phi, z);
+        if (((b.zf & TP_YLO) && j == 0) || ((b.zf & TP_YHI) && j == g.ny)) { f = 0; }
+        const int64_t o = at(g, i, j, k);
+        fy[o] = by ? f * by[o] : f;
+    }
+    if (i < g.nx && j < g.ny) {
+        double f = flux_z<double>(g, b, i, j, k, phi, z);
+        if ((b.zf & TP_ZHI) && k == g.nz) { f = 0; }
+        const int64_t o = at(g, i, j, k);
+        fz[o] = bz ? f * bz[o] : f;
+    }
+}
+
+__global__ void k_face_divergence(gb_grid g, const double* __restrict__ ax, const double* __restrict__ ay,
+                                  const double* __restrict__ az, const double* __restrict__ J,
+                                  const double* __restrict__ fx, const double* __restrict__ fy,
+                                  const double* __restrict__ fz, double* __restrict__ div)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = blockIdx.z;
+    if (i >= g.nx || j >= g.ny) { return; }
+    const double dxinv = 1.0 / g.dx, dyinv = 1.0 / g.dy, dzinv = 1.0 / g.dzeta;
+    const int64_t o = at(g, i, j, k);
+    const int64_t ox = at(g, i + 1, j, k), oy = at(g, i, j + 1, k), oz = at(g, i, j, k + 1);
+    div[o] = ((ax[ox] * fx[ox] - ax[o] * fx[o]) * dxinv + (ay[oy] * fy[oy] - ay[o] * fy[o]) * dyinv
+              + (az[oz] * fz[oz] - az[o] * fz[o]) * dzinv)
+           / J[o];
+}
+
+// ------------------------------------------------------------- multigrid ---
+
+//! Coarse node heights by injection (the fine column under each coarse node
+//! column; ghost columns the periodic image or the clamped edge).
+__global__ void k_coarse_z(gb_grid gc, double* __restrict__ zc, gb_grid gf, const double* __restrict__ zf)
+{
+    const int ni = gc.nx + 3, nj = gc.ny + 3, nk = gc.nz + 3;
+    const int64_t n = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (n >= static_cast<int64_t>(ni) * nj * nk) { return; }
+    int I = static_cast<int>(n % ni) - 1;
+    int J2 = static_cast<int>((n / ni) % nj) - 1;
+    const int k = static_cast<int>(n / (static_cast<int64_t>(ni) * nj)) - 1;
+    int si = I, sj = J2;
+    if (si < 0 || si > gc.nx) { si = gc.periodic_x ? ((si < 0) ? si + gc.nx : si - gc.nx) : ((si < 0) ? 0 : gc.nx); }
+    if (sj < 0 || sj > gc.ny) { sj = gc.periodic_y ? ((sj < 0) ? sj + gc.ny : sj - gc.ny) : ((sj < 0) ? 0 : gc.ny); }
+    zc[at(gc, I, J2, k)] = zf[at(gf, 2 * si, 2 * sj, k)];
+}
+
+//! Coarse premultiplied areas: the means of the fine faces a coarse face covers.
+__global__ void k_coarse_areas(gb_grid gc, double* __restrict__ AXc, double* __restrict__ AYc,
+                               double* __restrict__ AZc, gb_grid gf, const double* __restrict__ AXf,
+                               const double* __restrict__ AYf, const double* __restrict__ AZf)
+{
+    const int I = blockIdx.x * blockDim.x + threadIdx.x;
+    const int J2 = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = blockIdx.z;
+    if (I > gc.nx || J2 > gc.ny) { return; }
+    if (J2 < gc.ny && k < gc.nz) {
+        AXc[at(gc, I, J2, k)] = 0.5 * (AXf[at(gf, 2 * I, 2 * J2, k)] + AXf[at(gf, 2 * I, 2 * J2 + 1, k)]);
+    }
+    if (I < gc.nx && k < gc.nz) {
+        AYc[at(gc, I, J2, k)] = 0.5 * (AYf[at(gf, 2 * I, 2 * J2, k)] + AYf[at(gf, 2 * I + 1, 2 * J2, k)]);
+    }
+    if (I < gc.nx && J2 < gc.ny) {
+        AZc[at(gc, I, J2, k)] = 0.25 * (AZf[at(gf, 2 * I, 2 * J2, k)] + AZf[at(gf, 2 * I + 1, 2 * J2, k)]
+                                        + AZf[at(gf, 2 * I, 2 * J2 + 1, k)] + AZf[at(gf, 2 * I + 1, 2 * J2 + 1, k)]);
+    }
+}
+
+//! One colour of the zebra z-line relaxation: on every column with (i + j) & 1
+//! == color, r = b - A x over the column, T the principal tridiagonal, and
+//! x += T^{-1} r (Thomas; c', e' in shared memory [k][thread]).
+template <typename T>
+__global__ void __launch_bounds__(64) k_smooth_color(gb_grid g, PBC b, int color, T* __restrict__ x,
+                                                     const T* __restrict__ wrap, const T* __restrict__ bv,
+                                                     const T* __restrict__ AX, const T* __restrict__ AY,
+                                                     const T* __restrict__ AZ, const T* __restrict__ J,
+                                                     const T* __restrict__ z)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int tid = threadIdx.x;
+    const int nthr = blockDim.x;
+    const int j = blockIdx.y;
+    const int i = 2 * (blockIdx.x * blockDim.x + threadIdx.x) + ((j + color) & 1);
+    if (i >= g.nx) { return; }
+    T* cs = reinterpret_cast<T*>(smem_raw);
+    T* es = cs + static_cast<int64_t>(g.nz) * nthr;
+    T cp = T(0), ep = T(0);
+    for (int k = 0; k < g.nz; ++k) {
+        const T r = bv[at(g, i, j, k)] - adotx<T>(g, b, i, j, k, x, wrap, AX, AY, AZ, J, z);
+        T D, C, U;
+        line_tridiag<T>(g, b, AX, AY, AZ, J, z, i, j, k, D, C, U);
+        const T m = (k == 0) ? C : C - D * cp;
+        cp = U / m;
+        ep = ((k == 0) ? r : r - D * ep) / m;
+        cs[k * nthr + tid] = cp;
+        es[k * nthr + tid] = ep;
+    }
+    T xk = ep;
+    x[at(g, i, j, g.nz - 1)] += xk;
+    for (int k = g.nz - 2; k >= 0; --k) {
+        xk = es[k * nthr + tid] - cs[k * nthr + tid] * xk;
+        x[at(g, i, j, k)] += xk;
+    }
+}
+
+template <typename T>
+__global__ void k_restrict(gb_grid gf, const T* __restrict__ Jf, const T* __restrict__ rf, gb_grid gc,
+                           const T* __restrict__ Jc, T* __restrict__ bc)
+{
+    const int I = blockIdx.x * blockDim.x + threadIdx.x;
+    const int J2 = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = blockIdx.z;
+    if (I >= gc.nx || J2 >= gc.ny) { return; }
+    const int i = 2 * I, j = 2 * J2;
+    const T s = (Jf[at(gf, i, j, k)] * rf[at(gf, i, j, k)] + Jf[at(gf, i + 1, j, k)] * rf[at(gf, i + 1, j, k)])
+              + (Jf[at(gf, i, j + 1, k)] * rf[at(gf, i, j + 1, k)] + Jf[at(gf, i + 1, j + 1, k)] * rf[at(gf, i + 1, j + 1, k)]);
+    bc[at(gc, I, J2, k)] = s / (T(4) * Jc[at(gc, I, J2, k)]);
+}
+
+template <typename T>
+__global__ void k_prolong_add(gb_grid gc, PBC bcb, const T* __restrict__ xc, gb_grid gf, T* __restrict__ xf)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = blockIdx.z;
+    if (i >= gf.nx || j >= gf.ny) { return; }
+    const int I = i >> 1, J2 = j >> 1;
+    const int si = (i & 1) ? 1 : -1, sj = (j & 1) ? 1 : -1;
+    const T v = (T(9) * ldc<T>(xc, xc, gc, bcb, I, J2, k) + T(3) * ldc<T>(xc, xc, gc, bcb, I + si, J2, k))
+              + (T(3) * ldc<T>(xc, xc, gc, bcb, I, J2 + sj, k) + T(1) * ldc<T>(xc, xc, gc, bcb, I + si, J2 + sj, k));
+    xf[at(gf, i, j, k)] += v * T(0.0625);
+}
+
+// --------------------------------------------------------- vector ops ---
+
+template <typename TD, typename TS>
+__global__ void k_copy_valid(gb_grid g, TD* __restrict__ dst, const TS* __restrict__ src)
+{
+    int i, j, k;
+    const int64_t n = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (!cell_of(g, n, i, j, k)) { return; }
+    const int64_t o = at(g, i, j, k);
+    dst[o] = static_cast<TD>(src[o]);
+}
+
+template <typename T>
+__global__ void k_convert_all(T* __restrict__ dst, const double* __restrict__ src, int64_t n)
+{
+    const int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (t < n) { dst[t] = static_cast<T>(src[t]); }
+}
+
+//! Partial sums of sum_q over rows... : per block, sum of a*b over the valid
+//! cells (deterministic tree), one partial per (block, vector q).
+__global__ void k_multidot(gb_grid g, const double* __restrict__ w, const double* __restrict__ V, int64_t vstride,
+                           int nq, double* __restrict__ partial)
+{
+    __shared__ double red[kBlock / 32];
+    const int q = blockIdx.y;
+    const double* v = (q < 0) ? w : V + vstride * q;
+    double s = 0;
+    const int64_t ncell = static_cast<int64_t>(g.nx) * g.ny * g.nz;
+    for (int64_t n = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; n < ncell;
+         n += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        int i, j, k;
+        cell_of(g, n, i, j, k);
+        const int64_t o = at(g, i, j, k);
+        s += w[o] * v[o];
+    }
+    s = warp_sum(s);
+    if ((threadIdx.x & 31) == 0) { red[threadIdx.x >> 5] = s; }
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double t = (threadIdx.x < kBlock / 32) ? red[threadIdx.x] : 0.0;
+        t = warp_sum(t);
+        if (threadIdx.x == 0) { partial[static_cast<int64_t>(q) * gridDim.x + blockIdx.x] = t; }
+    }
+}
+
+__global__ void k_reduce_partials(const double* __restrict__ partial, int nblk, int nq, double* __restrict__ out)
+{
+    const int q = blockIdx.x;
+    __shared__ double red[32];
+    double s = 0;
+    for (int n = threadIdx.x; n < nblk; n += blockDim.x) { s += partial[static_cast<int64_t>(q) * nblk + n]; }
+    s = warp_sum(s);
+    if ((threadIdx.x & 31) == 0) { red[threadIdx.x >> 5] = s; }
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double t = (threadIdx.x < static_cast<int>(blockDim.x >> 5)) ? red[threadIdx.x] : 0.0;
+        t = warp_sum(t);
+        if (threadIdx.x == 0) { out[q] = t; }
+    }
+}
+
+//! w -= sum_q h[q] V_q (valid cells).
+__global__ void k_subtract_projection(gb_grid g, double* __restrict__ w, const double* __restrict__ V, int64_t vstride,
+                                      int nq, const double* __restrict__ h)
+{
+    int i, j, k;
+    const int64_t n = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (!cell_of(g, n, i, j, k)) { return; }
+    const int64_t o = at(g, i, j, k);
+    double s = w[o];
+    for (int q = 0; q < nq; ++q) { s -= h[q] * V[vstride * q + o]; }
+    w[o] = s;
+}
+
+//! y = a x + b y (valid cells); with x null y = b y.
+__global__ void k_axpby(gb_grid g, double a, const double* __restrict__ x, double b, double* __restrict__ y)
+{
+    int i, j, k;
+    const int64_t n = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (!cell_of(g, n, i, j, k)) { return; }
+    const int64_t o = at(g, i, j, k);
+    y[o] = (x ? a * x[o] : 0.0) + b * y[o];
+}
+
+//! phi += sum_q y[q] Z_q
+__global__ void k_add_combination(gb_grid g, double* __restrict__ phi, const double* __restrict__ Z, int64_t vstride,
+                                  int nq, const double* __restrict__ y)
+{
+    int i, j, k;
+    const int64_t n = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (!cell_of(g, n, i, j, k)) { return; }
+    const int64_t o = at(g, i, j, k);
+    double s = phi[o];
+    for (int q = 0; q < nq; ++q) { s += y[q] * Z[vstride * q + o]; }
+    phi[o] = s;
+}
+
+__global__ void k_add_const(gb_grid g, double* __restrict__ f, const double* __restrict__ c, double sign)
+{
+    int i, j, k;
+    const int64_t n = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (!cell_of(g, n, i, j, k)) { return; }
+    f[at(g, i, j, k)] += sign * c[0];
+}
+
+}  // namespace
+
+// ================================================================ host ===
+
+namespace {
+
+dim3 cols_grid(const gb_grid& g, int nk, int extra = 0)
+{
+    return dim3((g.nx + extra + 31) / 32, (g.ny + extra + 3) / 4, nk);
+}
+const dim3 kColsBlock(32, 4, 1);
+
+template <typename T>
+T* dalloc(std::vector<void*>& owned, int64_t n)
+{
+    void* p = nullptr;
+    if (cudaMalloc(&p, sizeof(T) * std::max<int64_t>(n, 1)) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    cudaMemset(p, 0, sizeof(T) * std::max<int64_t>(n, 1));
+    owned.push_back(p);
+    return static_cast<T*>(p);
+}
+
+gb_grid coarse_grid(const gb_grid& f)
+{
+    gb_grid c = f;
+    c.nx = f.nx / 2;
+    c.ny = f.ny / 2;
+    c.dx = 2 * f.dx;
+    c.dy = 2 * f.dy;
+    c.sy = c.nx + 1 + 2 * c.ng;
+    c.sz = c.sy * (c.ny + 1 + 2 * c.ng);
+    return c;
+}
+
+}  // namespace
+
+template <typename T>
+void PoissonLevels<T>::release()
+{
+    for (void* p : owned) { cudaFree(p); }
+    owned.clear();
+}
+
+}  // namespace gb
+
+gb_poisson::~gb_poisson()
+{
+    for (void* p : owned) { cudaFree(p); }
+    dl.release();
+    fl.release();
+}
+
+namespace gb {
+
+namespace {
+
+template <typename T>
+void mg_smooth(gb_poisson* P, PoissonLevels<T>& L, int l)
+{
+    gb_ctx* ctx = P->ctx;
+    const gb_grid& g = L.g[l];
+    const PBC& b = L.b[l];
+    const bool odd_wrap = (g.periodic_x && (g.nx & 1)) || (g.periodic_y && (g.ny & 1));
+    const int nthr = 64;
+    const size_t smem = static_cast<size_t>(2) * g.nz * nthr * sizeof(T);
+    for (int color = 0; color < 2; ++color) {
+        const T* wrap = L.x[l];
+        if (odd_wrap) {
+            cudaMemcpyAsync(L.snap[l], L.x[l], sizeof(T) * volume(g), cudaMemcpyDeviceToDevice, ctx->stream);
+            wrap = L.snap[l];
+        }
+        const dim3 grid(((g.nx + 1) / 2 + nthr - 1) / nthr, g.ny);
+        Span span(ctx, GB_KERNEL_MG_SMOOTH);
+        k_smooth_color<T><<<grid, nthr, smem, ctx->stream>>>(g, b, color, L.x[l], wrap, L.bv[l], L.AX[l], L.AY[l],
+                                                            L.AZ[l], L.J[l], L.z[l]);
+        ++ctx->launches;
+    }
+}
+
+template <typename T>
+void mg_residual(gb_poisson* P, PoissonLevels<T>& L, int l)
+{
+    gb_ctx* ctx = P->ctx;
+    const gb_grid& g = L.g[l];
+    Span span(ctx, GB_KERNEL_POISSON_APPLY);
+    k_apply<T><<<cols_grid(g, g.nz), kColsBlock, 0, ctx->stream>>>(g, L.b[l], L.x[l], L.AX[l], L.AY[l], L.AZ[l],
+                                                                   L.J[l], L.z[l], L.bv[l], L.r[l]);
+    ++ctx->launches;
+}
+
+template <typename T>
+void vcycle(gb_poisson* P, PoissonLevels<T>& L, int l)
+{
+    gb_ctx* ctx = P->ctx;
+    if (l == P->nlev - 1) {
+        for (int s = 0; s < P->opt.nu_coarse; ++s) { mg_smooth(P, L, l); }
+        return;
+    }
+    for (int s = 0; s < P->opt.nu1; ++s) { mg_smooth(P, L, l); }
+    mg_residual(P, L, l);
+    const gb_grid& gf = L.g[l];
+    const gb_grid& gc = L.g[l + 1];
+    {
+        Span span(ctx, GB_KERNEL_MG_TRANSFER);
+        k_restrict<T><<<cols_grid(gc, gc.nz), kColsBlock, 0, ctx->stream>>>(gf, L.J[l], L.r[l], gc, L.J[l + 1],
+                                                                            L.bv[l + 1]);
+        ++ctx->launches;
+    }
+    cudaMemsetAsync(L.x[l + 1], 0, sizeof(T) * volume(gc), ctx->stream);
+    vcycle(P, L, l + 1);
+    {
+        Span span(ctx, GB_KERNEL_MG_TRANSFER);
+        k_prolong_add<T><<<cols_grid(gf, gf.nz), kColsBlock, 0, ctx->stream>>>(gc, L.b[l + 1], L.x[l + 1], gf, L.x[l]);
+        ++ctx->launches;
+    }
+    for (int s = 0; s < P->opt.nu2; ++s) { mg_smooth(P, L, l); }
+}
+
+//! e = one V-cycle for A e = r (FP64 vectors at the fine level).
+void precondition(gb_poisson* P, const double* r, double* e)
+{
+    gb_ctx* ctx = P->ctx;
+    const gb_grid& g = P->g;
+    const int64_t ncell = static_cast<int64_t>(g.nx) * g.ny * g.nz;
+    if (P->opt.precision == 1) {
+        auto& L = P->fl;
+        k_copy_valid<float, double><<<nblocks(ncell), kBlock, 0, ctx->stream>>>(g, L.bv[0], r);
+        cudaMemsetAsync(L.x[0], 0, sizeof(float) * volume(g), ctx->stream);
+        ctx->launches += 1;
+        vcycle(P, L, 0);
+        cudaMemsetAsync(e, 0, sizeof(double) * volume(g), ctx->stream);
+        k_copy_valid<double, float><<<nblocks(ncell), kBlock, 0, ctx->stream>>>(g, e, L.x[0]);
+        ctx->launches += 1;
+    } else {
+        auto& L = P->dl;
+        cudaMemcpyAsync(L.bv[0], r, sizeof(double) * volume(g), cudaMemcpyDeviceToDevice, ctx->stream);
+        cudaMemsetAsync(L.x[0], 0, sizeof(double) * volume(g), ctx->stream);
+        vcycle(P, L, 0);
+        cudaMemcpyAsync(e, L.x[0], sizeof(double) * volume(g), cudaMemcpyDeviceToDevice, ctx->stream);
+    }
+}
+
+void apply_fine(gb_poisson* P, const double* x, const double* rhs, double* y)
+{
+    gb_ctx* ctx = P->ctx;
+    const gb_grid& g = P->g;
+    Span span(ctx, GB_KERNEL_POISSON_APPLY);
+    k_apply<double><<<cols_grid(g, g.nz), kColsBlock, 0, ctx->stream>>>(g, P->dl.b[0], x, P->dl.AX[0], P->dl.AY[0],
+                                                                        P->dl.AZ[0], P->dl.J[0], P->dl.z[0], rhs, y);
+    ++ctx->launches;
+}
+
+//! Dots <w, V_q> for q < nq (or <a, b> with V = b, nq = 1) into P->h_dots (host), deterministic.
+gb_status multidot(gb_poisson* P, const double* w, const double* V, int64_t vstride, int nq, double* host_out)
+{
+    gb_ctx* ctx = P->ctx;
+    const gb_grid& g = P->g;
+    const int nblk = P->dot_blocks;
+    {
+        Span span(ctx, GB_KERNEL_VECTOR);
+        k_multidot<<<dim3(nblk, nq), kBlock, 0, ctx->stream>>>(g, w, V, vstride, nq, P->d_partial);
+        k_reduce_partials<<<nq, 256, 0, ctx->stream>>>(P->d_partial, nblk, nq, P->d_dots);
+        ctx->launches += 2;
+    }
+    cudaMemcpyAsync(P->h_dots, P->d_dots, sizeof(double) * nq, cudaMemcpyDeviceToHost, ctx->stream);
+    if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) { return check_cuda("poisson dot"); }
+    std::copy(P->h_dots, P->h_dots + nq, host_out);
+    return GB_OK;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------ creation ---
+
+gb_status poisson_build(gb_poisson* P)
+{
+    gb_ctx* ctx = P->ctx;
+    // levels (FP64 geometry for every level, the FP32 copies when asked)
+    std::vector<gb_grid> grids{P->g};
+    while (static_cast<int>(grids.size()) < P->opt.max_levels) {
+        const gb_grid& c = grids.back();
+        const bool can = (c.nx % 2 == 0) && (c.ny % 2 == 0) && (c.nx / 2 >= P->opt.min_coarse) && (c.ny / 2 >= P->opt.min_coarse);
+        if (!can) { break; }
+        grids.push_back(coarse_grid(c));
+    }
+    P->nlev = static_cast<int>(grids.size());
+    auto& D = P->dl;
+    for (int l = 0; l < P->nlev; ++l) {
+        const gb_grid& g = grids[l];
+        D.g[l] = g;
+        D.b[l] = make_pbc(g, P->bc, true);
+        const int64_t vol = volume(g);
+        if (l == 0) {
+            D.z[l] = const_cast<double*>(P->z_fine);
+            D.J[l] = const_cast<double*>(P->J_fine);
+        } else {
+            D.z[l] = dalloc<double>(D.owned, vol);
+            D.J[l] = dalloc<double>(D.owned, vol);
+        }
+        D.AX[l] = dalloc<double>(D.owned, vol);
+        D.AY[l] = dalloc<double>(D.owned, vol);
+        D.AZ[l] = dalloc<double>(D.owned, vol);
+        D.x[l] = dalloc<double>(D.owned, vol);
+        D.bv[l] = dalloc<double>(D.owned, vol);
+        D.r[l] = dalloc<double>(D.owned, vol);
+        D.snap[l] = dalloc<double>(D.owned, vol);
+        if (!D.AX[l] || !D.AY[l] || !D.AZ[l] || !D.x[l] || !D.bv[l] || !D.r[l] || !D.snap[l] || (l > 0 && (!D.z[l] || !D.J[l]))) {
+            set_error("gust: PoissonSolver: cannot allocate the multigrid levels");
+            return GB_OOM;
+        }
+        if (l > 0) {
+            const gb_grid& gf = grids[l - 1];
+            const int64_t nz3 = static_cast<int64_t>(g.nx + 3) * (g.ny + 3) * (g.nz + 3);
+            k_coarse_z<<<nblocks(nz3), kBlock, 0, ctx->stream>>>(g, D.z[l], gf, D.z[l - 1]);
+            double* ax = dalloc<double>(D.owned, vol);
+            double* ay = dalloc<double>(D.owned, vol);
+            double* zcc = dalloc<double>(D.owned, vol);
+            const int64_t nm = static_cast<int64_t>(g.nx + 3) * (g.ny + 3) * (g.nz + 2);
+            k_metrics<<<nblocks(nm), kBlock, 0, ctx->stream>>>(g, D.z[l], D.J[l], ax, ay, zcc);
+            ctx->launches += 2;
+        }
+    }
+    if (P->opt.precision == 1) {
+        auto& F = P->fl;
+        for (int l = 0; l < P->nlev; ++l) {
+            const gb_grid& g = grids[l];
+            F.g[l] = g;
+            F.b[l] = D.b[l];
+            const int64_t vol = volume(g);
+            F.z[l] = dalloc<float>(F.owned, vol);
+            F.J[l] = dalloc<float>(F.owned, vol);
+            F.AX[l] = dalloc<float>(F.owned, vol);
+            F.AY[l] = dalloc<float>(F.owned, vol);
+            F.AZ[l] = dalloc<float>(F.owned, vol);
+            F.x[l] = dalloc<float>(F.owned, vol);
+            F.bv[l] = dalloc<float>(F.owned, vol);
+            F.r[l] = dalloc<float>(F.owned, vol);
+            F.snap[l] = dalloc<float>(F.owned, vol);
+            if (!F.z[l] || !F.J[l] || !F.AX[l] || !F.AY[l] || !F.AZ[l] || !F.x[l] || !F.bv[l] || !F.r[l] || !F.snap[l]) {
+                set_error("gust: PoissonSolver: cannot allocate the FP32 multigrid levels");
+                return GB_OOM;
+            }
+            k_convert_all<float><<<nblocks(vol), kBlock, 0, ctx->stream>>>(F.z[l], D.z[l], vol);
+            k_convert_all<float><<<nblocks(vol), kBlock, 0, ctx->stream>>>(F.J[l], D.J[l], vol);
+            ctx->launches += 2;
+        }
+    }
+    // Krylov workspace
+    const int64_t vol = volume(P->g);
+    const int m = P->opt.restart;
+    P->vstride = vol;
+    P->V = dalloc<double>(P->owned, vol * (m + 1));
+    P->Zv = dalloc<double>(P->owned, vol * m);
+    P->w = dalloc<double>(P->owned, vol);
+    P->t = dalloc<double>(P->owned, vol);
+    P->dot_blocks = std::min(4 * ctx->num_sms, nblocks(static_cast<int64_t>(P->g.nx) * P->g.ny * P->g.nz));
+    P->d_partial = dalloc<double>(P->owned, static_cast<int64_t>(P->dot_blocks) * (m + 2));
+    P->d_dots = dalloc<double>(P->owned, m + 2);
+    P->d_coef = dalloc<double>(P->owned, m + 2);
+    if (!P->V || !P->Zv || !P->w || !P->t || !P->d_partial || !P->d_dots || !P->d_coef) {
+        set_error("gust: PoissonSolver: cannot allocate the Krylov workspace");
+        return GB_OOM;
+    }
+    if (cudaMallocHost(&P->h_dots, sizeof(double) * (m + 2)) != cudaSuccess) {
+        cudaGetLastError();
+        set_error("gust: PoissonSolver: cannot allocate pinned host words");
+        return GB_OOM;
+    }
+    return check_cuda("PoissonSolver");
+}
+
+gb_status poisson_set_coeffs(gb_poisson* P, const double* ax, const double* ay, const double* az, const double* bx,
+                             const double* by, const double* bz)
+{
+    gb_ctx* ctx = P->ctx;
+    auto& D = P->dl;
+    const gb_grid& g = P->g;
+    const int64_t vol = volume(g);
+    // premultiplied areas a beta (Source/Poisson.cpp:442-447)
+    const double* a[3] = {ax, ay, az};
+    const double* b[3] = {bx, by, bz};
+    double* out[3] = {D.AX[0], D.AY[0], D.AZ[0]};
+    for (int d = 0; d < 3; ++d) {
+        cudaMemcpyAsync(out[d], a[d], sizeof(double) * vol, cudaMemcpyDeviceToDevice, ctx->stream);
+        if (b[d]) { multiply_inplace(ctx, out[d], b[d], vol); }
+    }
+    for (int l = 1; l < P->nlev; ++l) {
+        const gb_grid& gc = D.g[l];
+        k_coarse_areas<<<cols_grid(gc, gc.nz + 1, 1), kColsBlock, 0, ctx->stream>>>(
+            gc, D.AX[l], D.AY[l], D.AZ[l], D.g[l - 1], D.AX[l - 1], D.AY[l - 1], D.AZ[l - 1]);
+        ++ctx->launches;
+    }
+    if (P->opt.precision == 1) {
+        auto& F = P->fl;
+        for (int l = 0; l < P->nlev; ++l) {
+            const int64_t v = volume(F.g[l]);
+            k_convert_all<float><<<nblocks(v), kBlock, 0, ctx->stream>>>(F.AX[l], D.AX[l], v);
+            k_convert_all<float><<<nblocks(v), kBlock, 0, ctx->stream>>>(F.AY[l], D.AY[l], v);
+            k_convert_all<float><<<nblocks(v), kBlock, 0, ctx->stream>>>(F.AZ[l], D.AZ[l], v);
+            ctx->launches += 3;
+        }
+    }
+    P->coeffs_set = true;
+    return check_cuda("PoissonSolver::set_coeffs");
+}
+
+__global__ void k_multiply(double* __restrict__ a, const double* __restrict__ b, int64_t n)
+{
+    const int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (t < n) { a[t] *= b[t]; }
+}
+
+void multiply_inplace(gb_ctx* ctx, double* a, const double* b, int64_t n)
+{
+    k_multiply<<<nblocks(n), kBlock, 0, ctx->stream>>>(a, b, n);
+    ++ctx->launches;
+}
+
+gb_status poisson_apply(gb_poisson* P, const double* phi, double* y)
+{
+    apply_fine(P, phi, nullptr, y);
+    return check_cuda("PoissonSolver::apply");
+}
+
+gb_status poisson_vcycle(gb_poisson* P, const double* r, double* e)
+{
+    precondition(P, r, e);
+    return check_cuda("PoissonSolver::vcycle");
+}
+
+gb_status poisson_fluxes(gb_poisson* P, const double* phi, const double* bx, const double* by, const double* bz,
+                         double* fx, double* fy, double* fz)
+{
+    gb_ctx* ctx = P->ctx;
+    const gb_grid& g = P->g;
+    Span span(ctx, GB_KERNEL_POISSON_APPLY);
+    k_fluxes<<<cols_grid(g, g.nz + 1, 1), kColsBlock, 0, ctx->stream>>>(g, P->dl.b[0], phi, P->dl.z[0], bx, by, bz, fx,
+                                                                        fy, fz);
+    ++ctx->launches;
+    return check_cuda("PoissonSolver::fluxes");
+}
+
+//! J-weighted mean of the valid cells of f into d_coef[slot] (device) and host.
+gb_status weighted_mean(gb_poisson* P, const double* f, double* host_mean, int slot)
+{
+    double num = 0, den = 0;
+    gb_status st = multidot(P, P->dl.J[0], f, 0, 1, &num);
+    if (st != GB_OK) { return st; }
+    if (P->J_sum == 0) {
+        // sum of J: <J, 1> via a ones vector in t
+        gb_ctx* ctx = P->ctx;
+        const int64_t vol = volume(P->g);
+        k_fill<<<nblocks(vol), kBlock, 0, ctx->stream>>>(P->t, vol, 1.0);
+        ++ctx->launches;
+        if ((st = multidot(P, P->dl.J[0], P->t, 0, 1, &den)) != GB_OK) { return st; }
+        P->J_sum = den;
+    }
+    *host_mean = num / P->J_sum;
+    cudaMemcpyAsync(P->d_coef + slot, host_mean, sizeof(double), cudaMemcpyHostToDevice, P->ctx->stream);
+    return GB_OK;
+}
+
+gb_status poisson_solve(gb_poisson* P, double* rhs, double* phi, gb_poisson_result* res)
+{
+    gb_ctx* ctx = P->ctx;
+    const gb_grid& g = P->g;
+    const int64_t ncell = static_cast<int64_t>(g.nx) * g.ny * g.nz;
+    const int64_t vol = volume(g);
+    const int m = P->opt.restart;
+    *res = gb_poisson_result{};
+    bool singular = true;
+    for (int f = 0; f < 6; ++f) {
+        if (P->bc[f] == PF_DIRICHLET) { singular = false; }
+    }
+    res->singular = singular ? 1 : 0;
+    gb_status st;
+    if (singular) {
+        double mean = 0;
+        if ((st = weighted_mean(P, rhs, &mean, m + 1)) != GB_OK) { return st; }
+        res->removed_mean = mean;
+        k_add_const<<<nblocks(ncell), kBlock, 0, ctx->stream>>>(g, rhs, P->d_coef + m + 1, -1.0);
+        ++ctx->launches;
+    }
+    cudaMemsetAsync(phi, 0, sizeof(double) * vol, ctx->stream);
+    double bn2 = 0;
+    if ((st = multidot(P, rhs, rhs, 0, 1, &bn2)) != GB_OK) { return st; }
+    const double bnorm = std::sqrt(bn2);
+    res->initial_residual = bnorm;
+    const double tol = std::max(P->opt.reltol * bnorm, P->opt.abstol);
+    std::vector<double> H(static_cast<size_t>(m + 1) * m), cs(m), sn(m), s(m + 1), y(m), h(m + 1), h2(m + 1);
+    int it = 0;
+    bool converged = !(bnorm > tol);
+    while (!converged && it < P->opt.max_iter) {
+        apply_fine(P, phi, rhs, P->w);  // w = rhs - A phi
+        double b2 = 0;
+        if ((st = multidot(P, P->w, P->w, 0, 1, &b2)) != GB_OK) { return st; }
+        const double beta = std::sqrt(b2);
+        if (!(beta > tol)) {
+            converged = true;
+            break;
+        }
+        if (!std::isfinite(beta)) {
+            set_error("gust: the Poisson solve produced a non-finite residual");
+            return GB_NONFINITE;
+        }
+        cudaMemsetAsync(P->V, 0, sizeof(double) * vol, ctx->stream);
+        k_axpby<<<nblocks(ncell), kBlock, 0, ctx->stream>>>(g, 1.0 / beta, P->w, 0.0, P->V);
+        ++ctx->launches;
+        std::fill(s.begin(), s.end(), 0.0);
+        std::fill(H.begin(), H.end(), 0.0);
+        s[0] = beta;
+        int jj = 0;
+        for (; jj < m && it < P->opt.max_iter; ++jj) {
+            ++it;
+            double* vj = P->V + vol * jj;
+            double* zj = P->Zv + vol * jj;
+            precondition(P, vj, zj);
+            apply_fine(P, zj, nullptr, P->w);
+            // classical Gram-Schmidt, twice (batched dots: one kernel, one sync per pass)
+            std::fill(h.begin(), h.end(), 0.0);
+            for (int pass = 0; pass < 2; ++pass) {
+                if ((st = multidot(P, P->w, P->V, vol, jj + 1, h2.data())) != GB_OK) { return st; }
+                cudaMemcpyAsync(P->d_coef, h2.data(), sizeof(double) * (jj + 1), cudaMemcpyHostToDevice, ctx->stream);
+                k_subtract_projection<<<nblocks(ncell), kBlock, 0, ctx->stream>>>(g, P->w, P->V, vol, jj + 1, P->d_coef);
+                ++ctx->launches;
+                for (int q = 0; q <= jj; ++q) { h[q] += h2[q]; }
+            }
+            double hn2 = 0;
+            if ((st = multidot(P, P->w, P->w, 0, 1, &hn2)) != GB_OK) { return st; }
+            const double hn = std::sqrt(hn2);
+            double* vn = P->V + vol * (jj + 1);
+            cudaMemsetAsync(vn, 0, sizeof(double) * vol, ctx->stream);
+            if (hn > 0) {
+                k_axpby<<<nblocks(ncell), kBlock, 0, ctx->stream>>>(g, 1.0 / hn, P->w, 0.0, vn);
+                ++ctx->launches;
+            }
+            for (int q = 0; q <= jj; ++q) { H[q * m + jj] = h[q]; }
+            H[(jj + 1) * m + jj] = hn;
+            for (int q = 0; q < jj; ++q) {
+                const double a = H[q * m + jj], b2q = H[(q + 1) * m + jj];
+                H[q * m + jj] = cs[q] * a + sn[q] * b2q;
+                H[(q + 1) * m + jj] = -sn[q] * a + cs[q] * b2q;
+            }
+            const double a = H[jj * m + jj], b2j = H[(jj + 1) * m + jj];
+            const double rr = std::sqrt(a * a + b2j * b2j);
+            cs[jj] = (rr > 0) ? a / rr : 1.0;
+            sn[jj] = (rr > 0) ? b2j / rr : 0.0;
+            H[jj * m + jj] = rr;
+            H[(jj + 1) * m + jj] = 0;
+            s[jj + 1] = -sn[jj] * s[jj];
+            s[jj] = cs[jj] * s[jj];
+            if (std::fabs(s[jj + 1]) <= tol) {
+                ++jj;
+                break;
+            }
+        }
+        for (int q = jj - 1; q >= 0; --q) {
+            double acc = s[q];
+            for (int p = q + 1; p < jj; ++p) { acc -= H[q * m + p] * y[p]; }
+            y[q] = acc / H[q * m + q];
+        }
+        cudaMemcpyAsync(P->d_coef, y.data(), sizeof(double) * jj, cudaMemcpyHostToDevice, ctx->stream);
+        k_add_combination<<<nblocks(ncell), kBlock, 0, ctx->stream>>>(g, phi, P->Zv, vol, jj, P->d_coef);
+        ++ctx->launches;
+        if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) { return check_cuda("poisson solve"); }
+    }
+    if (singular) {
+        double mean = 0;
+        if ((st = weighted_mean(P, phi, &mean, m + 1)) != GB_OK) { return st; }
+        k_add_const<<<nblocks(ncell), kBlock, 0, ctx->stream>>>(g, phi, P->d_coef + m + 1, -1.0);
+        ++ctx->launches;
+    }
+    apply_fine(P, phi, rhs, P->w);
+    double r2 = 0;
+    if ((st = multidot(P, P->w, P->w, 0, 1, &r2)) != GB_OK) { return st; }
+    res->final_residual = std::sqrt(r2);
+    res->iterations = it;
+    if (!std::isfinite(res->final_residual)) {
+        set_error("gust: the Poisson solve returned non-finite values");
+        return GB_NONFINITE;
+    }
+    if (!(res->final_residual <= tol * (1 + 1e-7)) && !converged) {
+        set_error("gust: the Poisson solve did not converge in solver.poisson_max_iter = %d iterations (residual %g of "
+                  "%g; solver.poisson_reltol = %g, solver.poisson_abstol = %g)",
+                  P->opt.max_iter, res->final_residual, res->initial_residual, P->opt.reltol, P->opt.abstol);
+        return GB_NOT_CONVERGED;
+    }
+    return check_cuda("PoissonSolver::solve");
+}
+
+// ------------------------------------------------------ free functions ---
+
+gb_status mesh_metrics(gb_ctx* ctx, const gb_grid& g, const double* z, double* J, double* ax, double* ay, double* az,
+                       double* zcc)
+{
+    const int64_t vol = volume(g);
+    cudaMemsetAsync(J, 0, sizeof(double) * vol, ctx->stream);
+    cudaMemsetAsync(ax, 0, sizeof(double) * vol, ctx->stream);
+    cudaMemsetAsync(ay, 0, sizeof(double) * vol, ctx->stream);
+    cudaMemsetAsync(zcc, 0, sizeof(double) * vol, ctx->stream);
+    k_fill<<<nblocks(vol), kBlock, 0, ctx->stream>>>(az, vol, 1.0);
+    const int64_t nm = static_cast<int64_t>(g.nx + 3) * (g.ny + 3) * (g.nz + 2);
+    k_metrics<<<nblocks(nm), kBlock, 0, ctx->stream>>>(g, z, J, ax, ay, zcc);
+    ctx->launches += 2;
+    return check_cuda("mesh_metrics");
+}
+
+gb_status face_divergence(gb_ctx* ctx, const gb_grid& g, const double* ax, const double* ay, const double* az,
+                          const double* J, const double* fx, const double* fy, const double* fz, double* div)
+{
+    Span span(ctx, GB_KERNEL_MASSFLUX);
+    k_face_divergence<<<cols_grid(g, g.nz), kColsBlock, 0, ctx->stream>>>(g, ax, ay, az, J, fx, fy, fz, div);
+    ++ctx->launches;
+    return check_cuda("face_divergence");
+}
+
+template struct PoissonLevels<double>;
+template struct PoissonLevels<float>;
+
+}  // namespace gb

@@ -1,0 +1,76 @@
+// Host-side state of the Poisson layer (the C ABI's gb_poisson handle).
+#pragma once
+
+#include "gb_poisson.cuh"
+
+#include <vector>
+
+namespace gb {
+
+constexpr int kMaxLevels = 16;
+
+//! The multigrid hierarchy in one arithmetic type.
+template <typename T>
+struct PoissonLevels {
+    gb_grid g[kMaxLevels];
+    PBC b[kMaxLevels];
+    T* z[kMaxLevels] = {};
+    T* J[kMaxLevels] = {};
+    T* AX[kMaxLevels] = {};
+    T* AY[kMaxLevels] = {};
+    T* AZ[kMaxLevels] = {};
+    T* x[kMaxLevels] = {};
+    T* bv[kMaxLevels] = {};
+    T* r[kMaxLevels] = {};
+    T* snap[kMaxLevels] = {};
+    std::vector<void*> owned;
+    void release();
+};
+
+}  // namespace gb
+
+struct gb_poisson {
+    gb_ctx* ctx{nullptr};
+    gb_grid g{};
+    int bc[6]{};
+    gb_poisson_opts opt{};
+    const double* z_fine{nullptr};  // the caller's node heights (kept by reference)
+    const double* J_fine{nullptr};
+    int nlev{0};
+    gb::PoissonLevels<double> dl;  // FP64 hierarchy (geometry and coefficients of every level)
+    gb::PoissonLevels<float> fl;   // FP32 copies (precision == 1)
+    bool coeffs_set{false};
+    // Krylov workspace
+    int64_t vstride{0};
+    double* V{nullptr};
+    double* Zv{nullptr};
+    double* w{nullptr};
+    double* t{nullptr};
+    int dot_blocks{0};
+    double* d_partial{nullptr};
+    double* d_dots{nullptr};
+    double* d_coef{nullptr};
+    double* h_dots{nullptr};
+    double J_sum{0};
+    std::vector<void*> owned;
+    ~gb_poisson();
+};
+
+namespace gb {
+
+gb_status poisson_build(gb_poisson* P);
+gb_status poisson_set_coeffs(gb_poisson* P, const double* ax, const double* ay, const double* az, const double* bx,
+                             const double* by, const double* bz);
+gb_status poisson_apply(gb_poisson* P, const double* phi, double* y);
+gb_status poisson_vcycle(gb_poisson* P, const double* r, double* e);
+gb_status poisson_fluxes(gb_poisson* P, const double* phi, const double* bx, const double* by, const double* bz,
+                         double* fx, double* fy, double* fz);
+gb_status poisson_solve(gb_poisson* P, double* rhs, double* phi, gb_poisson_result* res);
+gb_status weighted_mean(gb_poisson* P, const double* f, double* host_mean, int slot);
+gb_status mesh_metrics(gb_ctx* ctx, const gb_grid& g, const double* z, double* J, double* ax, double* ay, double* az,
+                       double* zcc);
+gb_status face_divergence(gb_ctx* ctx, const gb_grid& g, const double* ax, const double* ay, const double* az,
+                          const double* J, const double* fx, const double* fy, const double* fz, double* div);
+void multiply_inplace(gb_ctx* ctx, double* a, const double* b, int64_t n);
+
+}  // namespace gb

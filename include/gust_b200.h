@@ -93,6 +93,14 @@ enum {
  * gb_ctx_profile_read sums the recorded spans of one family. */
 gb_status gb_ctx_profile(gb_ctx* ctx, int32_t enable);
 gb_status gb_ctx_profile_read(gb_ctx* ctx, int32_t family, double* total_ms, int64_t* spans);
+/* Tuning knobs of a context (the in-project autotuner sets them per shape). */
+enum {
+    GB_TUNE_LINE_VARIANT = 0,   /* z-line sweep kernel: 0 auto, 1 pipelined (cp.async ring), 2 shared, 3 global scratch */
+    GB_TUNE_LINE_BLOCK,         /* threads per block of the pipelined sweep (32, 64 or 128; 0 = default) */
+    GB_TUNE_MG_SMOOTH_BLOCK,    /* threads per block of the multigrid smoother (32 or 64; 0 = default) */
+    GB_N_TUNE
+};
+gb_status gb_ctx_tune(gb_ctx* ctx, int32_t key, int32_t value);
 /* The last error message of the calling thread ("" after success). */
 const char* gb_last_error(void);
 
@@ -113,6 +121,86 @@ gb_status gb_zline_jacobi(gb_ctx* ctx, const gb_grid* g, int32_t loc, const doub
 /* The same in FP32 (the inner solver of the mixed-precision defect correction). */
 gb_status gb_zline_jacobi_f32(gb_ctx* ctx, const gb_grid* g, int32_t loc, const float* A, const float* ap,
                               const float* rhs, int32_t sweeps, float* delta, float* change);
+
+/* ---- mesh --------------------------------------------------------------- */
+
+/* The metric terms of the terrain-following mesh from the node heights z
+ * (nodal, one ghost layer filled), replacing make_J / make_areas / make_zcc
+ * (extern_erf/ERF_TerrainMetrics.cpp:680-808, called from Source/Mesh.cpp:
+ * make_metrics): detJ and z_cc at cells, ax, ay at x-, y-faces, az = 1, on the
+ * valid points and one ghost layer (0 below the ground). */
+gb_status gb_mesh_metrics(gb_ctx* ctx, const gb_grid* g, const double* z_nd, double* detJ, double* ax, double* ay,
+                          double* az, double* z_cc);
+
+/* ---- Poisson layer ------------------------------------------------------ */
+
+/* Boundary types of the Poisson problem per domain face, indexed xlo, ylo,
+ * zlo, xhi, yhi, zhi (gust::PoissonBC, Source/Poisson.H:24-35). */
+enum { GB_POISSON_PERIODIC = 0, GB_POISSON_NEUMANN = 1, GB_POISSON_DIRICHLET = 2 };
+
+typedef struct gb_poisson_opts {
+    double reltol;       /* solver.poisson_reltol (SIMPLEC: simplec.pressure_reltol) */
+    double abstol;       /* solver.poisson_abstol */
+    int32_t max_iter;    /* solver.poisson_max_iter */
+    int32_t restart;     /* solver.poisson_restart */
+    int32_t precision;   /* 0: FP64 multigrid, 1: FP32 multigrid inside the FP64 Krylov solve */
+    int32_t nu1, nu2;    /* pre- and post-smoothing z-line zebra relaxations per level */
+    int32_t nu_coarse;   /* relaxations on the coarsest level */
+    int32_t max_levels;  /* multigrid levels (x-y 2:1 coarsening) */
+    int32_t min_coarse;  /* smallest coarse extent in x and y */
+} gb_poisson_opts;
+
+typedef struct gb_poisson_result {
+    int32_t iterations;
+    int32_t singular;          /* no Dirichlet face: the J-weighted mean was removed */
+    double initial_residual;   /* 2-norm of the (mean-free) right-hand side */
+    double final_residual;     /* true residual 2-norm, recomputed */
+    double removed_mean;       /* gust::PoissonResult::removed_mean */
+} gb_poisson_result;
+
+typedef struct gb_poisson gb_poisson;
+
+/* The reference's defaults (Source/Poisson.H:41-75: reltol 1e-10, max_iter 200,
+ * restart 50) with this project's multigrid settings. */
+gb_status gb_poisson_options_default(gb_poisson_opts* opt);
+
+/* gust::PoissonSolver (Source/Poisson.H:135-161) for the mesh (z_nd, detJ:
+ * device arrays kept by reference, as the reference's solver keeps the mesh)
+ * and the boundary types bc[6]. Builds the multigrid hierarchy. */
+gb_status gb_poisson_create(gb_ctx* ctx, const gb_grid* g, const int32_t* bc, const double* z_nd, const double* detJ,
+                            const gb_poisson_opts* opt, gb_poisson** out);
+gb_status gb_poisson_destroy(gb_poisson* p);
+
+/* The face coefficients (gust::FaceCoeffs without z_cross): the operator takes
+ * the premultiplied areas a * beta (Source/Poisson.cpp:442-447; beta null = 1). */
+gb_status gb_poisson_set_coeffs(gb_poisson* p, const double* ax, const double* ay, const double* az, const double* bx,
+                                const double* by, const double* bz);
+
+/* A phi (PoissonSolver::apply / TerrainPoisson::apply with the zero-flux faces,
+ * extern_erf/ERF_TerrainPoisson.cpp:74-101). Ghosts of phi are not read from
+ * memory: they are resolved by index for the boundary types. */
+gb_status gb_poisson_apply(gb_poisson* p, const double* phi, double* Aphi);
+
+/* One multigrid V-cycle for A e = r from e = 0 (the preconditioner). */
+gb_status gb_poisson_vcycle(gb_poisson* p, const double* r, double* e);
+
+/* PoissonSolver::solve (Source/Poisson.cpp:540-623): removes the J-weighted
+ * mean of rhs when singular (rhs is modified), solves A phi = rhs by flexible
+ * GMRES(restart) preconditioned by one V-cycle to max(reltol ||rhs||, abstol),
+ * removes phi's mean when singular, reports the true residual.
+ * GB_NOT_CONVERGED names solver.poisson_max_iter. */
+gb_status gb_poisson_solve(gb_poisson* p, double* rhs, double* phi, gb_poisson_result* res);
+
+/* The coefficient-weighted face fluxes F = -beta grad phi with the terrain
+ * cross terms and the zero-flux faces (TerrainPoisson::getFluxes,
+ * extern_erf/ERF_TerrainPoisson.cpp:212-264, times beta; beta null = 1). */
+gb_status gb_poisson_fluxes(gb_poisson* p, const double* phi, const double* bx, const double* by, const double* bz,
+                            double* fx, double* fy, double* fz);
+
+/* face_divergence (Source/Poisson.H:206-209, Source/Poisson.cpp:733-764):
+ * (1/J) [d_xi (a_x F_x) + d_eta (a_y F_y) + d_zeta (a_z F_z)]. */
+gb_status gb_face_divergence(gb_ctx* ctx, const gb_grid* g, const double* ax, const double* ay, const double* az,
+                             const double* detJ, const double* fx, const double* fy, const double* fz, double* div);
 
 #ifdef __cplusplus
 }

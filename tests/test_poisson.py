@@ -89,3 +89,124 @@ def test_oracle_singular_problem_removes_the_mean():
     assert mean == pytest.approx(oracle.weighted_mean(g, b, J), rel=1e-12)
     assert abs(oracle.weighted_mean(g, phi, J)) < 1e-12 * np.abs(phi).max()
     assert it > 0 and r1 <= 1e-10 * r0 * 1.01
+
+
+# ------------------------------------------------------------------ GPU parity
+def _gpu_case(g, z, J, ax, ay, az):
+    import ablsteadyrans_b200 as gb
+    return [to_dev(a) for a in (z, J, ax, ay, az)]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("per", [(False, False), (True, True), (True, False)])
+def test_gpu_metrics_bit_exact(ctx, per):
+    import ablsteadyrans_b200 as gb
+    g, z, J, ax, ay, az, zcc = smooth_terrain_case(20, 14, 9, *per, hill=150.0)
+    out = gb.mesh_metrics(ctx, g, to_dev(z))
+    for ref, dev in zip((J, ax, ay, az, zcc), out):
+        assert np.array_equal(to_host(dev), ref)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("per", [(False, False), (True, True), (False, True)])
+def test_gpu_apply_and_fluxes_match_oracle(ctx, per):
+    import ablsteadyrans_b200 as gb
+    g, z, J, ax, ay, az, _ = smooth_terrain_case(24, 18, 12, *per, hill=150.0)
+    bc = (PERIODIC if per[0] else NEUMANN, PERIODIC if per[1] else NEUMANN, NEUMANN,
+          PERIODIC if per[0] else DIRICHLET, PERIODIC if per[1] else DIRICHLET, DIRICHLET)
+    rng = np.random.default_rng(9)
+    beta = [g.np_zeros() + rng.uniform(0.5, 2.0, g.shape) for _ in range(3)]
+    AX, AY, AZ = ax * beta[0], ay * beta[1], az * beta[2]
+    phi = g.np_zeros()
+    phi[g.valid(0)] = rng.standard_normal(phi[g.valid(0)].shape)
+    y_ref = oracle.poisson_apply(g, bc, AX, AY, AZ, J, z, phi.copy())
+    F_ref = oracle.poisson_fluxes(g, bc, z, phi.copy(), *beta)
+    dz, dJ, dax, day, daz = _gpu_case(g, z, J, ax, ay, az)
+    ps = gb.PoissonSolver(ctx, g, dz, dJ, bc)
+    db = [to_dev(b) for b in beta]
+    ps.set_coeffs(dax, day, daz, *db)
+    y = to_host(ps.apply(to_dev(phi)))
+    assert rel_err(y, y_ref, g.valid(0)) < 1e-12
+    F = [to_host(f) for f in ps.fluxes(to_dev(phi), *db)]
+    for loc, f, fr in zip((1, 2, 4), F, F_ref):
+        assert rel_err(f, fr, g.valid(loc)) < 1e-12
+    d = to_host(gb.face_divergence(ctx, g, dax, day, daz, dJ, *[to_dev(f) for f in F_ref]))
+    d_ref = oracle.face_divergence(g, ax, ay, az, J, *F_ref)
+    assert rel_err(d, d_ref, g.valid(0)) < 1e-12
+    ps.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("per", [(True, True), (False, False), (True, False)])
+def test_gpu_vcycle_matches_oracle_fp64(ctx, per):
+    """One V-cycle of the FP64 multigrid agrees with the oracle's to 1e-12."""
+    import ablsteadyrans_b200 as gb
+    g, z, J, ax, ay, az, _ = smooth_terrain_case(32, 24, 16, *per, hill=150.0)
+    bc = (PERIODIC if per[0] else NEUMANN, PERIODIC if per[1] else NEUMANN, NEUMANN,
+          PERIODIC if per[0] else DIRICHLET, PERIODIC if per[1] else NEUMANN, DIRICHLET)
+    rng = np.random.default_rng(3)
+    r = g.np_zeros()
+    r[g.valid(0)] = rng.standard_normal(r[g.valid(0)].shape)
+    mg = oracle.Multigrid(g, bc, z, J, ax, ay, az, max_levels=12, min_coarse=2, nu1=1, nu2=1, nu_coarse=8)
+    e_ref = mg.vcycle(r)
+    dz, dJ, dax, day, daz = _gpu_case(g, z, J, ax, ay, az)
+    opts = gb.PoissonOptions.default(precision=0, nu1=1, nu2=1, nu_coarse=8, max_levels=12, min_coarse=2)
+    ps = gb.PoissonSolver(ctx, g, dz, dJ, bc, opts)
+    ps.set_coeffs(dax, day, daz)
+    e = to_host(ps.vcycle(to_dev(r)))
+    assert rel_err(e, e_ref, g.valid(0)) < 1e-12
+    ps.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", [0, 1])
+def test_gpu_askervein_solve_matches_reference_gold(ctx, precision):
+    """The GPU solve of the reference's Poisson_Askervein projection matches the
+    gold potential at the reference's 1e-8 relative, in FP64 and with the FP32
+    multigrid inside the FP64 Krylov solve."""
+    import ablsteadyrans_b200 as gb
+    c = askervein_case()
+    g = c["grid"]
+    dz, dJ, dax, day, daz = _gpu_case(g, c["z"], c["J"], c["ax"], c["ay"], c["az"])
+    rhs = gb.face_divergence(ctx, g, dax, day, daz, dJ, *[to_dev(u) for u in c["U"]])
+    ps = gb.PoissonSolver(ctx, g, dz, dJ, c["bc"], gb.PoissonOptions.default(reltol=1e-12, precision=precision))
+    ps.set_coeffs(dax, day, daz)
+    phi = to_dev(g.np_zeros())
+    res = ps.solve(rhs, phi)
+    assert res.iterations > 0 and not res.singular
+    assert res.final_residual <= 1e-12 * res.initial_residual * 1.01
+    err = np.abs(to_host(phi)[g.valid(0)] - c["phi_gold"]).max() / np.abs(c["phi_gold"]).max()
+    assert err < 1e-8, err
+    ps.close()
+
+
+@pytest.mark.gpu
+def test_gpu_singular_solve_removes_the_mean(ctx):
+    import ablsteadyrans_b200 as gb
+    g, z, J, ax, ay, az, _ = smooth_terrain_case(32, 32, 16, True, True)
+    bc = (PERIODIC, PERIODIC, NEUMANN, PERIODIC, PERIODIC, NEUMANN)
+    rng = np.random.default_rng(5)
+    b = g.np_zeros()
+    b[g.valid(0)] = rng.standard_normal(b[g.valid(0)].shape) + 0.25
+    mg = oracle.Multigrid(g, bc, z, J, ax, ay, az)
+    phi_ref, *_ , mean_ref = mg.solve(b.copy(), reltol=1e-12)
+    dz, dJ, dax, day, daz = _gpu_case(g, z, J, ax, ay, az)
+    ps = gb.PoissonSolver(ctx, g, dz, dJ, bc, gb.PoissonOptions.default(reltol=1e-12))
+    ps.set_coeffs(dax, day, daz)
+    phi = to_dev(g.np_zeros())
+    res = ps.solve(to_dev(b), phi)
+    assert res.singular and res.removed_mean == pytest.approx(mean_ref, rel=1e-12)
+    assert rel_err(to_host(phi), phi_ref, g.valid(0)) < 1e-9
+    ps.close()
+
+
+@pytest.mark.gpu
+def test_gpu_poisson_refusals(ctx):
+    import ablsteadyrans_b200 as gb
+    g, z, J, ax, ay, az, _ = smooth_terrain_case(8, 8, 6, True, False)
+    dz, dJ = to_dev(z), to_dev(J)
+    with pytest.raises(gb.GustError, match="periodic exactly when"):
+        gb.PoissonSolver(ctx, g, dz, dJ, (NEUMANN, NEUMANN, NEUMANN, NEUMANN, NEUMANN, NEUMANN))
+    with pytest.raises(gb.GustError, match="solver.poisson_reltol"):
+        gb.PoissonSolver(ctx, g, dz, dJ, (PERIODIC, NEUMANN, NEUMANN, PERIODIC, NEUMANN, DIRICHLET),
+                         gb.PoissonOptions.default(reltol=2.0))
