@@ -17,6 +17,10 @@ import os
 
 import numpy as np
 
+from . import abi as _abi
+from .abi import (BC, Diffusivities, IterInfo, MeshFields, Physics, SimplecOptions, State,  # noqa: F401
+                  FACE_INFLOW, FACE_NO_SLIP_WALL, FACE_OUTFLOW, FACE_PERIODIC, FACE_SLIP_WALL, LIMITER_UPWIND,
+                  LIMITER_VAN_ALBADA, LIMITER_VAN_LEER)
 from .grid import Grid, GbGrid, LOC_CELL, LOC_XFACE, LOC_YFACE, LOC_ZFACE, LOC_NODE, N_COEFS  # noqa: F401
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
@@ -144,12 +148,8 @@ def zline_jacobi(ctx, grid, loc, A, ap, rhs, sweeps, delta):
 POISSON_PERIODIC, POISSON_NEUMANN, POISSON_DIRICHLET = 0, 1, 2
 
 
-class PoissonOptions(ctypes.Structure):
-    """gb_poisson_opts: the solver.poisson_* inputs plus the multigrid settings."""
-    _fields_ = [("reltol", ctypes.c_double), ("abstol", ctypes.c_double), ("max_iter", ctypes.c_int32),
-                ("restart", ctypes.c_int32), ("precision", ctypes.c_int32), ("nu1", ctypes.c_int32),
-                ("nu2", ctypes.c_int32), ("nu_coarse", ctypes.c_int32), ("max_levels", ctypes.c_int32),
-                ("min_coarse", ctypes.c_int32)]
+class PoissonOptions(_abi.PoissonOptions):
+    """gb_poisson_opts (include/gust_b200.h), with the library's defaults."""
 
     @classmethod
     def default(cls, **kw):

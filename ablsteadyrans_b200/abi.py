@@ -1,0 +1,137 @@
+"""ctypes mirrors of the C ABI's plain structs (include/gust_b200.h) and
+constructors with the reference's defaults. No library is needed to use them."""
+import ctypes
+
+import numpy as np
+
+from .grid import GbGrid  # noqa: F401
+
+FACE_PERIODIC, FACE_INFLOW, FACE_OUTFLOW, FACE_SLIP_WALL, FACE_NO_SLIP_WALL = range(5)
+LIMITER_VAN_LEER, LIMITER_VAN_ALBADA, LIMITER_UPWIND = range(3)
+MAX_PROFILE = 32
+
+
+class PoissonOptions(ctypes.Structure):
+    """gb_poisson_opts: the solver.poisson_* inputs plus the multigrid settings."""
+    _fields_ = [("reltol", ctypes.c_double), ("abstol", ctypes.c_double), ("max_iter", ctypes.c_int32),
+                ("restart", ctypes.c_int32), ("precision", ctypes.c_int32), ("nu1", ctypes.c_int32),
+                ("nu2", ctypes.c_int32), ("nu_coarse", ctypes.c_int32), ("max_levels", ctypes.c_int32),
+                ("min_coarse", ctypes.c_int32)]
+
+    @classmethod
+    def defaults(cls, **kw):
+        """The reference's solver.poisson_* defaults (Source/Poisson.H:41-75) and
+        this project's multigrid settings."""
+        o = cls(reltol=1e-10, abstol=0.0, max_iter=200, restart=50, precision=0, nu1=1, nu2=1, nu_coarse=8,
+                max_levels=12, min_coarse=2)
+        for k, v in kw.items():
+            setattr(o, k, v)
+        return o
+
+
+class BC(ctypes.Structure):
+    """gb_bc: bc.* (Source/BoundaryConditions.H:99-143) with the log-law inflow."""
+    _fields_ = [("face", ctypes.c_int32 * 6), ("wall_velocity", (ctypes.c_double * 3) * 6),
+                ("zhi_theta_grad", ctypes.c_double), ("inflow_ustar", ctypes.c_double),
+                ("inflow_z0", ctypes.c_double), ("inflow_direction", ctypes.c_double), ("kappa", ctypes.c_double),
+                ("Cmu0", ctypes.c_double), ("inflow_inv_lmax", ctypes.c_double), ("theta_ref_n", ctypes.c_int32),
+                ("theta_ref_z", ctypes.c_double * MAX_PROFILE), ("theta_ref_theta", ctypes.c_double * MAX_PROFILE)]
+
+    @classmethod
+    def make(cls, faces, theta_ref=((0.0,), (300.0,)), ustar=0.4, z0=0.1, direction=0.0, kappa=0.41, Cmu0=0.5562,
+             l_max=30.0, zhi_theta_grad=0.0, wall_velocity=None):
+        b = cls()
+        for n, f in enumerate(faces):
+            b.face[n] = int(f)
+        if wall_velocity:
+            for n, vel in wall_velocity.items():
+                for c in range(3):
+                    b.wall_velocity[n][c] = float(vel[c])
+        b.zhi_theta_grad = zhi_theta_grad
+        b.inflow_ustar, b.inflow_z0, b.inflow_direction = ustar, z0, direction
+        b.kappa, b.Cmu0 = kappa, Cmu0
+        b.inflow_inv_lmax = 0.0 if not l_max else 1.0 / l_max
+        zs, ts = theta_ref
+        b.theta_ref_n = len(zs)
+        for n, (zz, tt) in enumerate(zip(zs, ts)):
+            b.theta_ref_z[n] = zz
+            b.theta_ref_theta[n] = tt
+        return b
+
+
+class Physics(ctypes.Structure):
+    """gb_physics: forcing.*, convection.* and the residual scales."""
+    _fields_ = [("gravity", ctypes.c_double), ("theta0", ctypes.c_double), ("coriolis", ctypes.c_int32),
+                ("coriolis_3d", ctypes.c_int32), ("geostrophic", ctypes.c_int32), ("latitude", ctypes.c_double),
+                ("rotation_period", ctypes.c_double), ("ug", ctypes.c_double), ("vg", ctypes.c_double),
+                ("pressure_gradient", ctypes.c_double * 3), ("limiter", ctypes.c_int32),
+                ("smooth_eps_velocity", ctypes.c_double), ("smooth_eps_theta", ctypes.c_double),
+                ("log_mean", ctypes.c_int32), ("scale_velocity", ctypes.c_double), ("scale_theta", ctypes.c_double),
+                ("scale_tke", ctypes.c_double), ("scale_height", ctypes.c_double)]
+
+    @classmethod
+    def make(cls, scale_height, **kw):
+        """The reference's defaults (Source/Forcing.H: gravity 9.81, theta0 300, Coriolis
+        off, rotation period 86400 s; convection van Leer, eps 1e-5; JvpScales 10, 10, 0.1)."""
+        p = cls(gravity=9.81, theta0=300.0, coriolis=0, coriolis_3d=1, geostrophic=0, latitude=0.0,
+                rotation_period=86400.0, ug=0.0, vg=0.0, limiter=LIMITER_VAN_LEER, smooth_eps_velocity=1e-5,
+                smooth_eps_theta=1e-5, log_mean=0, scale_velocity=10.0, scale_theta=10.0, scale_tke=0.1,
+                scale_height=scale_height)
+        for k, v in kw.items():
+            if k == "pressure_gradient":
+                for d in range(3):
+                    p.pressure_gradient[d] = v[d]
+            else:
+                setattr(p, k, v)
+        return p
+
+
+class SimplecOptions(ctypes.Structure):
+    """gb_simplec_opts: simplec.*, steady.zline_sweeps, turb.tke_floor and the
+    correction's Poisson solver."""
+    _fields_ = [("pressure_reltol", ctypes.c_double), ("alpha_p", ctypes.c_double),
+                ("rotation_relax", ctypes.c_double), ("w_vnn_cap", ctypes.c_double),
+                ("w_vnn_cap_slope_margin", ctypes.c_double), ("tke_floor", ctypes.c_double),
+                ("zline_sweeps", ctypes.c_int32), ("precision", ctypes.c_int32), ("poisson", PoissonOptions)]
+
+    @classmethod
+    def make(cls, **kw):
+        """The reference's defaults (Source/Simplec.H:80-90, Source/Driver.H:92)."""
+        o = cls(pressure_reltol=1e-3, alpha_p=1.0, rotation_relax=0.3, w_vnn_cap=0.0, w_vnn_cap_slope_margin=4.0,
+                tke_floor=0.0, zline_sweeps=2, precision=0, poisson=PoissonOptions.defaults())
+        for k, v in kw.items():
+            setattr(o, k, v)
+        return o
+
+
+class State(ctypes.Structure):
+    _fields_ = [("u", ctypes.c_void_p), ("v", ctypes.c_void_p), ("w", ctypes.c_void_p), ("p", ctypes.c_void_p),
+                ("theta", ctypes.c_void_p), ("tke", ctypes.c_void_p), ("z_nd", ctypes.c_void_p)]
+
+
+class MeshFields(ctypes.Structure):
+    _fields_ = [("detJ", ctypes.c_void_p), ("ax", ctypes.c_void_p), ("ay", ctypes.c_void_p), ("az", ctypes.c_void_p)]
+
+
+class Diffusivities(ctypes.Structure):
+    _fields_ = [("nu", ctypes.c_void_p), ("gamma_theta", ctypes.c_void_p), ("gamma_tke", ctypes.c_void_p)]
+
+
+class IterInfo(ctypes.Structure):
+    _fields_ = [("residual_norms", ctypes.c_double * 6), ("max_speed", ctypes.c_double),
+                ("mean_tke", ctypes.c_double), ("max_du", ctypes.c_double), ("max_dv", ctypes.c_double),
+                ("max_dw", ctypes.c_double), ("last_sweep_du", ctypes.c_double), ("last_sweep_dv", ctypes.c_double),
+                ("last_sweep_dw", ctypes.c_double), ("divergence_before", ctypes.c_double),
+                ("divergence_after", ctypes.c_double), ("max_dp", ctypes.c_double),
+                ("poisson_removed_mean", ctypes.c_double), ("poisson_iterations", ctypes.c_int32),
+                ("max_dtheta", ctypes.c_double), ("max_dtke", ctypes.c_double), ("tke_clipped", ctypes.c_int64)]
+
+    def as_dict(self):
+        d = {f: getattr(self, f) for f, _ in self._fields_ if f != "residual_norms"}
+        d["residual_norms"] = list(self.residual_norms)
+        return d
+
+
+def np_ptr(a):
+    assert a.dtype == np.float64 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data

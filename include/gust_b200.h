@@ -202,6 +202,89 @@ gb_status gb_poisson_fluxes(gb_poisson* p, const double* phi, const double* bx, 
 gb_status gb_face_divergence(gb_ctx* ctx, const gb_grid* g, const double* ax, const double* ay, const double* az,
                              const double* detJ, const double* fx, const double* fy, const double* fz, double* div);
 
+/* ---- SIMPLEC stage ------------------------------------------------------ */
+
+/* Domain face types (gust::FaceType, Source/BoundaryConditions.H:91), the
+ * subset with no wall model: periodic, inflow (profile), outflow, slip_wall,
+ * no_slip_wall. */
+enum { GB_FACE_PERIODIC = 0, GB_FACE_INFLOW = 1, GB_FACE_OUTFLOW = 2, GB_FACE_SLIP_WALL = 3, GB_FACE_NO_SLIP_WALL = 4 };
+/* convection.limiter (Source/Limiter_K.H:21). */
+enum { GB_LIMITER_VAN_LEER = 0, GB_LIMITER_VAN_ALBADA = 1, GB_LIMITER_UPWIND = 2 };
+
+#define GB_MAX_PROFILE 32
+
+/* The boundary conditions (gust::BoundaryInputs, Source/BoundaryConditions.H:
+ * 99-143) with the log-law inflow (gust::InflowProfileOptions, Source/InflowProfile.H). */
+typedef struct gb_bc {
+    int32_t face[6];                 /* bc.xlo, bc.ylo, bc.zlo, bc.xhi, bc.yhi, bc.zhi */
+    double wall_velocity[6][3];      /* bc.<face>_wall_velocity of a no_slip_wall */
+    double zhi_theta_grad;           /* bc.zhi_theta_grad (K/m) */
+    double inflow_ustar;             /* bc.inflow_ustar (m/s) */
+    double inflow_z0;                /* bc.inflow_z0 (m) */
+    double inflow_direction;         /* bc.inflow_direction: degrees the wind blows towards, CCW from +x */
+    double kappa, Cmu0;              /* the closure's constants of the inflow k */
+    double inflow_inv_lmax;          /* 1 / turb.max_geom_lscale, 0 = unbounded length */
+    int32_t theta_ref_n;             /* theta_ref(z): the hydrostatic reference and the inflow's theta */
+    double theta_ref_z[GB_MAX_PROFILE];
+    double theta_ref_theta[GB_MAX_PROFILE];
+} gb_bc;
+
+/* The residual's physics inputs (gust::ResidualInputs without a closure and a
+ * wall model, Source/Residual.H:61-128; gust::ForcingOptions, Source/Forcing.H). */
+typedef struct gb_physics {
+    double gravity, theta0;                       /* forcing.gravity, forcing.theta0 */
+    int32_t coriolis, coriolis_3d, geostrophic;   /* forcing.coriolis, forcing.coriolis_3d, forcing.geostrophic */
+    double latitude, rotation_period, ug, vg;     /* forcing.latitude, rotation_period, ug, vg */
+    double pressure_gradient[3];                  /* forcing.pressure_gradient (m/s^2) */
+    int32_t limiter;                              /* convection.limiter */
+    double smooth_eps_velocity, smooth_eps_theta; /* convection.smooth_eps_* (van Albada) */
+    int32_t log_mean;                             /* diffusivity face mean: 0 arithmetic, 1 logarithmic */
+    double scale_velocity, scale_theta, scale_tke;/* residual scales U, theta_s, k_s (JvpScales) */
+    double scale_height;                          /* H (gust::residual_scale_height) */
+} gb_physics;
+
+/* simplec.* and steady.zline_sweeps (gust::SimplecOptions, Source/Simplec.H:80-90). */
+typedef struct gb_simplec_opts {
+    double pressure_reltol;          /* simplec.pressure_reltol */
+    double alpha_p;                  /* simplec.alpha_p */
+    double rotation_relax;           /* simplec.rotation_relax */
+    double w_vnn_cap;                /* simplec.w_vnn_cap (0 off) */
+    double w_vnn_cap_slope_margin;   /* simplec.w_vnn_cap_slope_margin */
+    double tke_floor;                /* turb.tke_floor */
+    int32_t zline_sweeps;            /* steady.zline_sweeps */
+    int32_t precision;               /* 0 plain FP64; 1 FP32 inner solves (sweeps, multigrid) in FP64 defect correction */
+    gb_poisson_opts poisson;         /* the correction's Poisson solver (reltol taken from pressure_reltol) */
+} gb_simplec_opts;
+
+/* The solution fields (gust::State, Source/State.H:18-36): device arrays of
+ * the grid with two ghost layers; z_nd the node heights. */
+typedef struct gb_state {
+    double *u, *v, *w, *p, *theta, *tke;
+    const double* z_nd;
+} gb_state;
+
+/* The mesh metrics (gust::Mesh) and the given diffusivities (nu, gamma_theta,
+ * gamma_tke: cell arrays with one ghost layer filled). */
+typedef struct gb_mesh_fields {
+    const double *detJ, *ax, *ay, *az;
+} gb_mesh_fields;
+typedef struct gb_diffusivities {
+    const double *nu, *gamma_theta, *gamma_tke;
+} gb_diffusivities;
+
+/* What one SIMPLEC iteration reports (SimplecStage's norms and the results of
+ * its parts: MomentumPredictorResult, PressureCorrectionResult, ScalarSweepResult). */
+typedef struct gb_iter_info {
+    double residual_norms[6];        /* scaled RMS of R_u, R_v, R_w, R_p, R_theta, R_k (stage_norms) */
+    double max_speed, mean_tke;      /* monitors */
+    double max_du, max_dv, max_dw;
+    double last_sweep_du, last_sweep_dv, last_sweep_dw;
+    double divergence_before, divergence_after, max_dp, poisson_removed_mean;
+    int32_t poisson_iterations;
+    double max_dtheta, max_dtke;
+    int64_t tke_clipped;
+} gb_iter_info;
+
 #ifdef __cplusplus
 }
 #endif

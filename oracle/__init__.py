@@ -181,3 +181,131 @@ class Multigrid:
 
     def __del__(self):
         self.close()
+
+
+# ------------------------------------------------------------------ SIMPLEC
+def _declare_simplec(L):
+    from ablsteadyrans_b200.abi import BC, Diffusivities, IterInfo, MeshFields, Physics, SimplecOptions, State
+    from ablsteadyrans_b200.grid import GbGrid
+    G = ctypes.POINTER(GbGrid)
+    P = ctypes.c_void_p
+    i32, f64 = ctypes.c_int32, ctypes.c_double
+    PP = ctypes.POINTER(ctypes.c_void_p)
+    L.og_fill_ghosts.argtypes = [G, ctypes.POINTER(BC), P, P, P, P, P, P, P]
+    L.og_residual.argtypes = [G, ctypes.POINTER(BC), ctypes.POINTER(Physics), ctypes.POINTER(State),
+                              ctypes.POINTER(MeshFields), ctypes.POINTER(Diffusivities), PP]
+    L.og_implicit_rows.argtypes = [G, ctypes.POINTER(BC), ctypes.POINTER(Physics), i32, P, P, P, P, P,
+                                   ctypes.POINTER(Diffusivities), P]
+    L.og_simplec_iterate.argtypes = [G, ctypes.POINTER(BC), ctypes.POINTER(Physics), ctypes.POINTER(SimplecOptions),
+                                     ctypes.POINTER(State), ctypes.POINTER(MeshFields), ctypes.POINTER(Diffusivities),
+                                     P, PP, ctypes.POINTER(IterInfo)]
+    L.og_simplec_iterate.restype = i32
+    L.og_local_dtau.argtypes = [G, P, P, P, P, P, P, f64, P]
+    L.og_transport_fluxes.argtypes = [G, P, P, P, P, P, P, P, P, P]
+    L.og_velocity_divergence.argtypes = [G, P, P, P, P, P, P, P, P, P]
+    L.og_pressure_gradient.argtypes = [G, P, P, P, P, P, P, P, P]
+    L.og_convection.argtypes = [G, i32, P, P, P, P, P, i32, f64, i32, P]
+    L.og_scalar_diffusive_fluxes.argtypes = [G, P, P, P, i32, P, P, P]
+    L.og_momentum_diffusive_fluxes.argtypes = [G, i32, P, P, P, P, P, i32, P, P, P]
+    L.og_flux_divergence.argtypes = [G, i32, P, P, P, P, P]
+    L.og_implicit_coefficients.argtypes = [G, i32, P, P, P, P, P, P, i32, P]
+    L.og_omega_from_w.argtypes = [G, P, P, P, P, P, i32]
+    L.og_w_from_omega.argtypes = [G, P, P, P, P, P]
+    L.og_face_dtau.argtypes = [G, P, P, P, P]
+
+
+class Case:
+    """The host arrays of one SIMPLEC instance in the grid layout: state, mesh,
+    diffusivities, and the ctypes views the oracle and the GPU take."""
+
+    FIELDS = ("u", "v", "w", "p", "theta", "tke")
+
+    def __init__(self, grid, z, J, ax, ay, az, nu, gamma_theta, gamma_tke):
+        self.grid = grid
+        self.z, self.J, self.ax, self.ay, self.az = z, J, ax, ay, az
+        self.nu, self.gt, self.gk = nu, gamma_theta, gamma_tke
+        self.q = {f: grid.np_zeros() for f in self.FIELDS}
+
+    def state(self):
+        from ablsteadyrans_b200.abi import State
+        return State(*[self.q[f].ctypes.data for f in self.FIELDS], self.z.ctypes.data)
+
+    def mesh(self):
+        from ablsteadyrans_b200.abi import MeshFields
+        return MeshFields(self.J.ctypes.data, self.ax.ctypes.data, self.ay.ctypes.data, self.az.ctypes.data)
+
+    def diffusivities(self):
+        from ablsteadyrans_b200.abi import Diffusivities
+        return Diffusivities(self.nu.ctypes.data, self.gt.ctypes.data, self.gk.ctypes.data)
+
+    def copy(self):
+        c = Case(self.grid, self.z, self.J, self.ax, self.ay, self.az, self.nu, self.gt, self.gk)
+        c.q = {f: a.copy() for f, a in self.q.items()}
+        return c
+
+
+def _L():
+    L = lib()
+    if not getattr(L, "_og_simplec", False):
+        _declare_simplec(L)
+        L._og_simplec = True
+    return L
+
+
+def fill_ghosts(case, bc):
+    q = case.q
+    _L().og_fill_ghosts(ctypes.byref(case.grid.c), ctypes.byref(bc), *[_p(q[f]) for f in Case.FIELDS], _p(case.z))
+
+
+def residual(case, bc, phys):
+    """Residual.cpp:159-256 at the case's state (ghosts filled by the caller)."""
+    R = [case.grid.np_zeros() for _ in range(6)]
+    arr = (ctypes.c_void_p * 6)(*[r.ctypes.data for r in R])
+    st, m, d = case.state(), case.mesh(), case.diffusivities()
+    _L().og_residual(ctypes.byref(case.grid.c), ctypes.byref(bc), ctypes.byref(phys), ctypes.byref(st), ctypes.byref(m),
+                     ctypes.byref(d), arr)
+    return R
+
+
+def local_dtau(case, cfl, use_nu=True):
+    dt = case.grid.np_zeros()
+    q = case.q
+    _L().og_local_dtau(ctypes.byref(case.grid.c), _p(q["u"]), _p(q["v"]), _p(q["w"]), _p(case.z), _p(case.J),
+                       _p(case.nu) if use_nu else None, float(cfl), _p(dt))
+    return dt
+
+
+def simplec_iterate(case, bc, phys, opts, dtau):
+    """One SimplecStage::iterate (Simplec.cpp:452-506); returns (status, IterInfo, R)."""
+    from ablsteadyrans_b200.abi import IterInfo
+    R = [case.grid.np_zeros() for _ in range(6)]
+    arr = (ctypes.c_void_p * 6)(*[r.ctypes.data for r in R])
+    info = IterInfo()
+    st, m, d = case.state(), case.mesh(), case.diffusivities()
+    rc = _L().og_simplec_iterate(ctypes.byref(case.grid.c), ctypes.byref(bc), ctypes.byref(phys), ctypes.byref(opts),
+                                 ctypes.byref(st), ctypes.byref(m), ctypes.byref(d), _p(dtau), arr, ctypes.byref(info))
+    return int(rc), info, R
+
+
+def transport_fluxes(grid, u, v, w, z, ax, ay):
+    F = [grid.np_zeros() for _ in range(3)]
+    _L().og_transport_fluxes(ctypes.byref(grid.c), _p(u), _p(v), _p(w), _p(z), _p(ax), _p(ay), *[_p(f) for f in F])
+    return F
+
+
+def convection(grid, loc, q, F, J, limiter=0, eps=1e-5, bounded=False):
+    out = grid.np_zeros()
+    _L().og_convection(ctypes.byref(grid.c), loc, _p(q), *[_p(f) for f in F], _p(J), limiter, eps, int(bounded), _p(out))
+    return out
+
+
+def implicit_coefficients(grid, C, F, gamma, z, J, logz=False):
+    A = grid.np_zeros(7)
+    _L().og_implicit_coefficients(ctypes.byref(grid.c), C, *[_p(f) for f in F], _p(gamma), _p(z), _p(J), int(logz), _p(A))
+    return A
+
+
+def velocity_divergence(grid, u, v, w, z, ax, ay, az, J):
+    d = grid.np_zeros()
+    _L().og_velocity_divergence(ctypes.byref(grid.c), _p(u), _p(v), _p(w), _p(z), _p(ax), _p(ay), _p(az), _p(J), _p(d))
+    return d

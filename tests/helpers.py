@@ -155,3 +155,18 @@ def smooth_terrain_case(nx, ny, nz, periodic_x, periodic_y, hill=80.0, dx=40.0, 
     z = oracle.btf_heights(g, zl, ground)
     J, ax, ay, az, zcc = oracle.metrics(g, z)
     return g, z, J, ax, ay, az, zcc
+
+
+# ------------------------------------------------------------------ SIMPLEC
+def flat_case(nx, ny, nz, Lx, Ly, H, periodic_x, periodic_y, visc):
+    """A flat mesh with uniform layers (test_Simplec.cpp:45-58 flat_case) and
+    uniform diffusivities (the Laminar fixture, :129-160)."""
+    import oracle
+    g = Grid(nx, ny, nz, Lx / nx, Ly / ny, H / nz, periodic_x, periodic_y)
+    zl = np.arange(nz + 1) * (H / nz)
+    ground = np.zeros((ny + 3, nx + 3))
+    z = oracle.btf_heights(g, zl, ground)
+    J, ax, ay, az, zcc = oracle.metrics(g, z)
+    nu = g.np_zeros() + visc
+    case = oracle.Case(g, z, J, ax, ay, az, nu, nu.copy(), nu.copy())
+    return case

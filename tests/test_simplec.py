@@ -1,0 +1,104 @@
+"""The SIMPLEC outer iteration (Source/Simplec.cpp:452-506) with given
+diffusivities: the oracle is pinned to the reference's known answers
+(test_Simplec.cpp: PoiseuilleToMachinePrecision :344-403, the uniform state's
+fixed point :482, one correction removes the divergence :173)."""
+import numpy as np
+import pytest
+
+import oracle
+from ablsteadyrans_b200.abi import BC, FACE_NO_SLIP_WALL, FACE_PERIODIC, FACE_SLIP_WALL, Physics, SimplecOptions
+from helpers import flat_case, seam_sync
+
+
+def laminar(case, ground, top, H):
+    g = case.grid
+    faces = (FACE_PERIODIC if g.periodic_x else FACE_SLIP_WALL, FACE_PERIODIC if g.periodic_y else FACE_SLIP_WALL,
+             ground, FACE_PERIODIC if g.periodic_x else FACE_SLIP_WALL,
+             FACE_PERIODIC if g.periodic_y else FACE_SLIP_WALL, top)
+    bc = BC.make(faces, theta_ref=((-1000.0, 5000.0), (300.0, 300.0)))
+    return bc
+
+
+def test_oracle_poiseuille_to_machine_precision():
+    """Laminar Poiseuille flow between no-slip walls driven by a constant force:
+    the discrete steady solution is u_k = F/(2 nu) (z_k (H - z_k) + dz^2/4),
+    reached to machine precision; w, v, p' stay 0; theta and k untouched; a
+    converged state is a fixed point of one more iteration."""
+    H, F, nu, nz = 500.0, 1e-4, 10.0, 16
+    case = flat_case(2, 2, nz, 1000.0, 1000.0, H, True, True, nu)
+    bc = laminar(case, FACE_NO_SLIP_WALL, FACE_NO_SLIP_WALL, H)
+    phys = Physics.make(H, gravity=0.0, pressure_gradient=(F, 0.0, 0.0))
+    opts = SimplecOptions.make(zline_sweeps=2)
+    opts.poisson.reltol = 0.1
+    case.q["theta"][...] = 300.0
+    case.q["tke"][...] = 0.5
+    oracle.fill_ghosts(case, bc)
+    umax = F * H * H / (8 * nu)
+    its = 0
+    for its in range(400):
+        dtau = oracle.local_dtau(case, 10.0)
+        st, info, _ = oracle.simplec_iterate(case, bc, phys, opts, dtau)
+        assert st == 0
+        if its > 5 and info.max_du < 1e-15 * umax:
+            break
+    assert its < 399
+    g = case.grid
+    G = g.ng
+    dz = H / nz
+    zc = (np.arange(nz) + 0.5) * dz
+    exact = F / (2 * nu) * (zc * (H - zc) + dz * dz / 4)
+    u = case.q["u"][G:G + nz, G:G + g.ny, G:G + g.nx + 1]
+    assert np.abs(u - exact[:, None, None]).max() < 1e-13 * umax
+    v = g.valid
+    assert np.abs(case.q["w"][v(4)]).max() == 0
+    assert np.abs(case.q["v"][v(2)]).max() == 0
+    assert np.abs(case.q["p"][v(0)]).max() < 1e-14 * umax * umax
+    assert case.q["theta"][v(0)].min() == 300.0 and case.q["theta"][v(0)].max() == 300.0
+    assert case.q["tke"][v(0)].min() == 0.5
+    q0 = case.copy()
+    dtau = oracle.local_dtau(case, 10.0)
+    st, info, _ = oracle.simplec_iterate(case, bc, phys, opts, dtau)
+    assert np.abs(case.q["u"][v(1)] - q0.q["u"][v(1)]).max() < 1e-14 * umax
+    assert np.abs(case.q["w"][v(4)] - q0.q["w"][v(4)]).max() == 0
+    assert max(info.residual_norms) < 1e-12
+
+
+def test_oracle_uniform_state_is_a_fixed_point():
+    """A uniform wind over flat ground with slip walls has R = 0: an iteration
+    changes nothing (test_Simplec.cpp:482)."""
+    case = flat_case(8, 4, 6, 1000.0, 800.0, 500.0, True, True, 1.0)
+    bc = laminar(case, FACE_SLIP_WALL, FACE_SLIP_WALL, 500.0)
+    phys = Physics.make(500.0, gravity=9.81)
+    opts = SimplecOptions.make()
+    case.q["u"][...] = 6.0
+    case.q["v"][...] = -2.0
+    case.q["theta"][...] = 300.0
+    case.q["tke"][...] = 0.1
+    oracle.fill_ghosts(case, bc)
+    q0 = case.copy()
+    dtau = oracle.local_dtau(case, 5.0)
+    st, info, R = oracle.simplec_iterate(case, bc, phys, opts, dtau)
+    assert st == 0
+    assert max(info.residual_norms) < 1e-14
+    for f in ("u", "v", "w", "p", "theta", "tke"):
+        assert np.abs(case.q[f] - q0.q[f])[case.grid.valid(0)].max() < 1e-13
+
+
+def test_oracle_one_correction_reduces_the_divergence():
+    """One pressure correction of a predicted random velocity leaves a
+    divergence below the Poisson tolerance times the predicted one."""
+    case = flat_case(8, 4, 6, 1000.0, 800.0, 500.0, True, True, 1.0)
+    bc = laminar(case, FACE_SLIP_WALL, FACE_SLIP_WALL, 500.0)
+    phys = Physics.make(500.0, gravity=0.0)
+    opts = SimplecOptions.make(pressure_reltol=1e-10)
+    rng = np.random.default_rng(21)
+    g = case.grid
+    for f, loc, lo, hi in (("u", 1, 5, 10), ("v", 2, -2, 2), ("w", 4, -0.5, 0.5)):
+        case.q[f][g.valid(loc)] = rng.uniform(lo, hi, case.q[f][g.valid(loc)].shape)
+        seam_sync(g, loc, case.q[f])
+    case.q["theta"][...] = 300.0
+    oracle.fill_ghosts(case, bc)
+    dtau = oracle.local_dtau(case, 5.0)
+    st, info, _ = oracle.simplec_iterate(case, bc, phys, opts, dtau)
+    assert st == 0
+    assert info.divergence_after < 1e-8 * info.divergence_before
