@@ -1,0 +1,203 @@
+// C ABI of the SIMPLEC stage: argument and inputs checks with the reference's
+// messages (Source/Simplec.cpp:25-48 check_simplec_options,
+// Source/BoundaryConditions.cpp check_boundary_inputs), then gb_simplec.cu.
+#include "gb_poisson_api.cuh"
+#include "gb_simplec.cuh"
+
+#include <cmath>
+#include <limits>
+#include <new>
+
+// the handle's layout lives in gb_simplec.cu; only the fields the checks need are read here
+namespace gb {
+gb_status simplec_create_checked(gb_ctx* ctx, const gb_grid* g, const gb_bc* bc, const gb_physics* ph,
+                                 const gb_simplec_opts* opt, const double* z_nd, const gb_mesh_fields* mesh,
+                                 const gb_diffusivities* df, gb_simplec** out);
+void simplec_delete(gb_simplec* S);
+}  // namespace gb
+
+namespace {
+
+gb_status check_simplec_options(const gb_simplec_opts& o)
+{
+    const double eps10 = 10 * std::numeric_limits<double>::epsilon();
+    if (std::isnan(o.pressure_reltol) || !(o.pressure_reltol >= eps10 && o.pressure_reltol < 1)) {
+        gb::set_error("gust: invalid inputs:\n  simplec.pressure_reltol = %g: must be >= 10 machine epsilon and < 1 "
+                      "(the Poisson solver's own bound)", o.pressure_reltol);
+        return GB_BAD_ARG;
+    }
+    if (std::isnan(o.alpha_p) || !(o.alpha_p > 0 && o.alpha_p <= 1)) {
+        gb::set_error("gust: invalid inputs:\n  simplec.alpha_p = %g: must be > 0 and <= 1", o.alpha_p);
+        return GB_BAD_ARG;
+    }
+    if (std::isnan(o.rotation_relax) || !(o.rotation_relax > 0 && o.rotation_relax <= 1)) {
+        gb::set_error("gust: invalid inputs:\n  simplec.rotation_relax = %g: must be > 0 and <= 1", o.rotation_relax);
+        return GB_BAD_ARG;
+    }
+    if (std::isnan(o.w_vnn_cap) || !(o.w_vnn_cap == 0 || (o.w_vnn_cap >= 16 && std::isfinite(o.w_vnn_cap)))) {
+        gb::set_error("gust: invalid inputs:\n  simplec.w_vnn_cap = %g: must be 0 (off), or finite and >= 16", o.w_vnn_cap);
+        return GB_BAD_ARG;
+    }
+    if (std::isnan(o.w_vnn_cap_slope_margin)
+        || !(o.w_vnn_cap_slope_margin == 0 || (o.w_vnn_cap_slope_margin >= 1 && std::isfinite(o.w_vnn_cap_slope_margin)))) {
+        gb::set_error("gust: invalid inputs:\n  simplec.w_vnn_cap_slope_margin = %g: must be 0 (off), or finite and >= 1",
+                      o.w_vnn_cap_slope_margin);
+        return GB_BAD_ARG;
+    }
+    if (o.zline_sweeps < 1 || o.zline_sweeps > 100) {
+        gb::set_error("gust: SimplecStage: sweeps must be >= 1 (steady.zline_sweeps; 2..100 for zjacobi)");
+        return GB_BAD_ARG;
+    }
+    if (std::isnan(o.tke_floor) || !(o.tke_floor >= 0)) {
+        gb::set_error("gust: SimplecStage: tke_floor must be >= 0 (turb.tke_floor)");
+        return GB_BAD_ARG;
+    }
+    if (o.precision != 0 && o.precision != 1) {
+        gb::set_error("gust: SimplecStage: precision must be 0 (plain FP64) or 1 (FP32 inner solves)");
+        return GB_BAD_ARG;
+    }
+    return GB_OK;
+}
+
+gb_status check_bc(const gb_grid& g, const gb_bc& bc)
+{
+    const char* keys[6] = {"bc.xlo", "bc.ylo", "bc.zlo", "bc.xhi", "bc.yhi", "bc.zhi"};
+    const int per[3] = {g.periodic_x, g.periodic_y, 0};
+    for (int f = 0; f < 6; ++f) {
+        const int d = f % 3;
+        const int t = bc.face[f];
+        if (t < GB_FACE_PERIODIC || t > GB_FACE_NO_SLIP_WALL) {
+            gb::set_error("gust: invalid inputs:\n  %s: unknown face type %d", keys[f], t);
+            return GB_BAD_ARG;
+        }
+        if ((per[d] != 0) != (t == GB_FACE_PERIODIC)) {
+            gb::set_error("gust: invalid inputs:\n  %s: periodic exactly where the geometry is periodic", keys[f]);
+            return GB_BAD_ARG;
+        }
+        if (d == 2 && (t == GB_FACE_INFLOW || t == GB_FACE_OUTFLOW)) {
+            gb::set_error("gust: invalid inputs:\n  %s: inflow and outflow are lateral faces only", keys[f]);
+            return GB_BAD_ARG;
+        }
+    }
+    if (bc.theta_ref_n < 1 || bc.theta_ref_n > GB_MAX_PROFILE) {
+        gb::set_error("gust: invalid inputs:\n  theta_ref: 1 to %d levels", GB_MAX_PROFILE);
+        return GB_BAD_ARG;
+    }
+    for (int n = 1; n < bc.theta_ref_n; ++n) {
+        if (!(bc.theta_ref_z[n] > bc.theta_ref_z[n - 1])) {
+            gb::set_error("gust: invalid inputs:\n  theta_ref: heights must increase");
+            return GB_BAD_ARG;
+        }
+    }
+    bool inflow = false;
+    for (int f = 0; f < 6; ++f) { inflow = inflow || bc.face[f] == GB_FACE_INFLOW; }
+    if (inflow && !(bc.inflow_ustar > 0 && bc.inflow_z0 > 0 && bc.kappa > 0 && bc.Cmu0 > 0)) {
+        gb::set_error("gust: invalid inputs:\n  bc.inflow_ustar and bc.inflow_z0 must be > 0 (log law)");
+        return GB_BAD_ARG;
+    }
+    return GB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+gb_status gb_simplec_create(gb_ctx* ctx, const gb_grid* g, const gb_bc* bc, const gb_physics* ph,
+                            const gb_simplec_opts* opt, const double* z_nd, const gb_mesh_fields* mesh,
+                            const gb_diffusivities* df, gb_simplec** out)
+{
+    gb::clear_error();
+    if (ctx == nullptr || bc == nullptr || ph == nullptr || opt == nullptr || z_nd == nullptr || mesh == nullptr
+        || df == nullptr || out == nullptr) {
+        gb::set_error("gust: SimplecStage: null argument");
+        return GB_BAD_ARG;
+    }
+    gb_status st = gb::check_grid("SimplecStage", g);
+    if (st == GB_OK) { st = check_simplec_options(*opt); }
+    if (st == GB_OK) { st = check_bc(*g, *bc); }
+    if (st != GB_OK) { return st; }
+    if (!mesh->detJ || !mesh->ax || !mesh->ay || !mesh->az || !df->nu || !df->gamma_theta || !df->gamma_tke) {
+        gb::set_error("gust: SimplecStage: without a closure the residual inputs need the diffusivities");
+        return GB_BAD_ARG;
+    }
+    if (!(ph->scale_velocity > 0 && ph->scale_theta > 0 && ph->scale_tke > 0 && ph->scale_height > 0)) {
+        gb::set_error("gust: SimplecStage: the residual scales (jvp_scales) must be finite and > 0");
+        return GB_BAD_ARG;
+    }
+    if (std::isnan(ph->gravity) || !(ph->gravity >= 0) || !(ph->theta0 > 0)) {
+        gb::set_error("gust: invalid inputs:\n  forcing.gravity must be >= 0 and forcing.theta0 > 0");
+        return GB_BAD_ARG;
+    }
+    if (ph->coriolis && !(ph->rotation_period > 0 && ph->latitude >= -90 && ph->latitude <= 90)) {
+        gb::set_error("gust: invalid inputs:\n  forcing.latitude must be in [-90, 90] and forcing.rotation_period > 0");
+        return GB_BAD_ARG;
+    }
+    if (ph->limiter < GB_LIMITER_VAN_LEER || ph->limiter > GB_LIMITER_UPWIND) {
+        gb::set_error("gust: invalid inputs:\n  convection.limiter must be van_leer, van_albada or upwind");
+        return GB_BAD_ARG;
+    }
+    return gb::simplec_create_checked(ctx, g, bc, ph, opt, z_nd, mesh, df, out);
+}
+
+gb_status gb_simplec_destroy(gb_simplec* s)
+{
+    gb::clear_error();
+    gb::simplec_delete(s);
+    return gb::check_cuda("SimplecStage::~SimplecStage");
+}
+
+gb_status gb_simplec_fill_ghosts(gb_simplec* s, const gb_state* q)
+{
+    gb::clear_error();
+    if (s == nullptr || q == nullptr) {
+        gb::set_error("gust: fill_ghosts: null argument");
+        return GB_BAD_ARG;
+    }
+    gb::simplec_fill_ghosts(s, *q);
+    return gb::check_cuda("fill_ghosts");
+}
+
+gb_status gb_simplec_residual(gb_simplec* s, const gb_state* q, double* const* R)
+{
+    gb::clear_error();
+    if (s == nullptr || q == nullptr || R == nullptr) {
+        gb::set_error("gust: residual: null argument");
+        return GB_BAD_ARG;
+    }
+    double* r[6];
+    for (int n = 0; n < 6; ++n) {
+        if (R[n] == nullptr) {
+            gb::set_error("gust: residual: R needs six device arrays (u, v, w, p, theta, tke)");
+            return GB_BAD_ARG;
+        }
+        r[n] = R[n];
+    }
+    gb::simplec_residual(s, *q, r);
+    return gb::check_cuda("residual");
+}
+
+gb_status gb_simplec_iterate(gb_simplec* s, const gb_state* q, const double* dtau, gb_iter_info* info)
+{
+    gb::clear_error();
+    if (s == nullptr || q == nullptr || dtau == nullptr || info == nullptr) {
+        gb::set_error("gust: SimplecStage::iterate: null argument");
+        return GB_BAD_ARG;
+    }
+    return gb::simplec_iterate(s, *q, dtau, info);
+}
+
+gb_status gb_local_dtau(gb_simplec* s, const gb_state* q, double cfl, double* dtau)
+{
+    gb::clear_error();
+    if (s == nullptr || q == nullptr || dtau == nullptr) {
+        gb::set_error("gust: local_dtau: null argument");
+        return GB_BAD_ARG;
+    }
+    if (std::isnan(cfl) || !std::isfinite(cfl) || !(cfl > 0)) {
+        gb::set_error("gust: local_dtau: cfl must be finite and > 0 (got %g)", cfl);
+        return GB_BAD_ARG;
+    }
+    return gb::simplec_local_dtau(s, *q, cfl, dtau);
+}
+
+}  // extern "C"

@@ -1,0 +1,1641 @@
+// The SIMPLEC outer iteration on the GPU (gust::SimplecStage::iterate,
+// Source/Simplec.cpp:452-506) without a closure and a wall model: boundary
+// ghost fills, the FP64 residual (convection, full-stress terrain diffusion,
+// pressure gradient, forcing, continuity), the implicit rows, the momentum
+// predictor with z-line sweeps, the pressure correction through the Poisson
+// layer, the theta and k sweeps and the stage norms. Every reduction is
+// deterministic (block partials summed in a fixed order, maxima by bit
+// pattern), so a run repeats to the bit.
+#include "gb_line.cuh"
+#include "gb_poisson_api.cuh"
+#include "gb_simplec.cuh"
+#include "gb_stencil.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+namespace gb {
+
+using namespace st;
+
+namespace {
+
+enum { R_EVEN = 0, R_ODD, R_VALUE, R_PROFILE, R_GRADIENT };
+enum { F_U = 0, F_V, F_W, F_P, F_THETA, F_TKE };
+
+constexpr int kRedBlocks = 512;
+
+// ------------------------------------------------------------- heights ---
+
+__device__ __forceinline__ double node_z(const double* __restrict__ z, const gb_grid& g, int i, int j, int k)
+{
+    const int lo = -1, hix = g.nx + 1, hiy = g.ny + 1, hiz = g.nz + 1;
+    i = i < lo ? lo : (i > hix ? hix : i);
+    j = j < lo ? lo : (j > hiy ? hiy : j);
+    if (k < lo) { return z[at(g, i, j, lo)] + (lo - k) * (z[at(g, i, j, lo)] - z[at(g, i, j, lo + 1)]); }
+    if (k > hiz) { return z[at(g, i, j, hiz)] + (k - hiz) * (z[at(g, i, j, hiz)] - z[at(g, i, j, hiz - 1)]); }
+    return z[at(g, i, j, k)];
+}
+
+//! Height of point (i, j, k) of type t above its column's ground (Heights_K.H:40-56).
+__device__ __forceinline__ double height_above_ground(const double* z, const gb_grid& g, int t, int i, int j, int k)
+{
+    const int nx = nodal(t, 0) ? 1 : 2, ny = nodal(t, 1) ? 1 : 2, nz = nodal(t, 2) ? 1 : 2;
+    double zp = 0, zg = 0;
+    for (int a = 0; a < nx; ++a) {
+        for (int b = 0; b < ny; ++b) {
+            zg += node_z(z, g, i + a, j + b, 0);
+            for (int c = 0; c < nz; ++c) { zp += node_z(z, g, i + a, j + b, k + c); }
+        }
+    }
+    return zp / (nx * ny * nz) - zg / (nx * ny);
+}
+
+//! Node-mean height of point (i, j, k) of type t (Heights_K.H:60-71).
+__device__ __forceinline__ double point_z(const double* z, const gb_grid& g, int t, int i, int j, int k)
+{
+    const int nx = nodal(t, 0) ? 1 : 2, ny = nodal(t, 1) ? 1 : 2, nz = nodal(t, 2) ? 1 : 2;
+    double zp = 0;
+    for (int a = 0; a < nx; ++a) {
+        for (int b = 0; b < ny; ++b) {
+            for (int c = 0; c < nz; ++c) { zp += node_z(z, g, i + a, j + b, k + c); }
+        }
+    }
+    return zp / (nx * ny * nz);
+}
+
+//! The log-law inflow profile's value of field f at height h (InflowProfile.H eval).
+struct Profile {
+    double ustar, z0, kappa, Cmu0, inv_lmax, cosd, sind;
+    int rn;
+    double rz[GB_MAX_PROFILE], rt[GB_MAX_PROFILE];
+    __device__ double value(int f, double h) const
+    {
+        h = fmax(h, 0.0);
+        const double c = 1.0 / (1.0 + kappa * (h + z0) * inv_lmax);
+        const double S = ustar / kappa * log((h + z0) / z0);
+        const double ul = ustar * c;
+        switch (f) {
+        case F_U: return S * cosd;
+        case F_V: return S * sind;
+        case F_THETA: {
+            if (rn == 1 || h <= rz[0]) { return rt[0]; }
+            if (h >= rz[rn - 1]) { return rt[rn - 1]; }
+            int m = 1;
+            while (m < rn - 1 && !(h < rz[m])) { ++m; }
+            const double w = (h - rz[m - 1]) / (rz[m] - rz[m - 1]);
+            return rt[m - 1] + w * (rt[m] - rt[m - 1]);
+        }
+        case F_TKE: return ul * ul / (Cmu0 * Cmu0);
+        default: return 0;
+        }
+    }
+};
+
+int rule_for(int f, int t, int d, bool lo)
+{
+    const bool normal_vel = (f == F_U && d == 0) || (f == F_V && d == 1) || (f == F_W && d == 2);
+    const bool vel = (f == F_U || f == F_V || f == F_W);
+    switch (t) {
+    case GB_FACE_INFLOW: return (f == F_P) ? R_EVEN : R_PROFILE;
+    case GB_FACE_OUTFLOW: return (f == F_P) ? R_ODD : R_EVEN;
+    case GB_FACE_SLIP_WALL:
+        if (normal_vel) { return R_VALUE; }
+        return (f == F_THETA && d == 2 && !lo) ? R_GRADIENT : R_EVEN;
+    case GB_FACE_NO_SLIP_WALL: return vel ? R_VALUE : R_EVEN;
+    default: return R_EVEN;
+    }
+}
+
+bool dirichlet_normal(const gb_bc& bc, int face)
+{
+    const int t = bc.face[face];
+    return t == GB_FACE_INFLOW || t == GB_FACE_SLIP_WALL || t == GB_FACE_NO_SLIP_WALL;
+}
+
+inline int ext(const gb_grid& g, int t, int d) { return ((d == 0) ? g.nx : (d == 1) ? g.ny : g.nz) + nodal(t, d); }
+inline bool is_per(const gb_grid& g, int d) { return d == 0 ? g.periodic_x : d == 1 ? g.periodic_y : false; }
+const int kLoc[6] = {XF, YF, ZF, CC, CC, CC};
+
+// ------------------------------------------------------ deterministic sums ---
+
+__global__ void k_sumsq_partial(gb_grid g, Box b, const double* __restrict__ f, double* __restrict__ partial, int mode)
+{
+    // mode 0: sum of squares, 1: sum
+    __shared__ double red[8];
+    double s = 0;
+    const int64_t n_tot = b.count();
+    const int nx = b.hi[0] - b.lo[0] + 1, ny = b.hi[1] - b.lo[1] + 1;
+    for (int64_t n = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; n < n_tot;
+         n += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int i = b.lo[0] + static_cast<int>(n % nx);
+        const int j = b.lo[1] + static_cast<int>((n / nx) % ny);
+        const int k = b.lo[2] + static_cast<int>(n / (static_cast<int64_t>(nx) * ny));
+        const double v = f[at(g, i, j, k)];
+        s += (mode == 0) ? v * v : v;
+    }
+    s = warp_sum(s);
+    if ((threadIdx.x & 31) == 0) { red[threadIdx.x >> 5] = s; }
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double t = (threadIdx.x < 8) ? red[threadIdx.x] : 0.0;
+        t = warp_sum(t);
+        if (threadIdx.x == 0) { partial[blockIdx.x] = t; }
+    }
+}
+
+__global__ void k_sum_partials(const double* __restrict__ partial, int n, double* __restrict__ out)
+{
+    __shared__ double red[8];
+    double s = 0;
+    for (int t = threadIdx.x; t < n; t += blockDim.x) { s += partial[t]; }
+    s = warp_sum(s);
+    if ((threadIdx.x & 31) == 0) { red[threadIdx.x >> 5] = s; }
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double t = (threadIdx.x < 8) ? red[threadIdx.x] : 0.0;
+        t = warp_sum(t);
+        if (threadIdx.x == 0) { *out = t; }
+    }
+}
+
+__global__ void k_maxabs(gb_grid g, Box b, const double* __restrict__ f, const double* __restrict__ mul,
+                         unsigned long long* __restrict__ slot)
+{
+    const int64_t n = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    double v = 0;
+    if (n < b.count()) {
+        const int nx = b.hi[0] - b.lo[0] + 1, ny = b.hi[1] - b.lo[1] + 1;
+        const int i = b.lo[0] + static_cast<int>(n % nx);
+        const int j = b.lo[1] + static_cast<int>((n / nx) % ny);
+        const int k = b.lo[2] + static_cast<int>(n / (static_cast<int64_t>(nx) * ny));
+        const int64_t o = at(g, i, j, k);
+        v = fabs(mul ? f[o] * mul[o] : f[o]);
+    }
+    v = warp_max(v);
+    if ((threadIdx.x & 31) == 0) { atomic_max_nonneg(slot, v); }
+}
+
+}  // namespace
+
+// ================================================================ host ===
+
+struct SimplecWork {
+    double* R[6];
+    double* F[3];
+    double* G[9];
+    double* tmp;
+    double* A;
+    double* At;
+    double* ap[3];
+    double* dd[3];
+    double* mask;
+    double* rhs;
+    double* delta;
+    double* dtf[3];
+    double* beta[3];
+    double* keep[3];
+    double* phi;
+    double* om;
+    double* theta_ref;
+    double* conv0;
+    double* conv1;
+    double* og;
+    double* level_sum;
+    double* partial;
+    double* sums;
+    float* A32;
+    float* ap32;
+    float* rhs32;
+    float* delta32;
+};
+
+}  // namespace gb
+
+struct gb_simplec {
+    gb_ctx* ctx{nullptr};
+    gb_grid g{};
+    gb_bc bc{};
+    gb_physics ph{};
+    gb_simplec_opts opt{};
+    gb_mesh_fields mesh{};
+    gb_diffusivities df{};
+    const double* z{nullptr};
+    gb::SimplecWork w{};
+    gb::Profile prof{};
+    gb_poisson* poisson{nullptr};
+    double jmin{0};
+    std::vector<void*> owned;
+    unsigned long long* h_words{nullptr};
+    ~gb_simplec();
+};
+
+gb_simplec::~gb_simplec()
+{
+    if (poisson) { gb_poisson_destroy(poisson); }
+    for (void* p : owned) { cudaFree(p); }
+}
+
+namespace gb {
+
+namespace {
+
+double* dbuf(gb_simplec* S, int64_t n)
+{
+    void* p = nullptr;
+    if (cudaMalloc(&p, sizeof(double) * std::max<int64_t>(n, 1)) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    cudaMemset(p, 0, sizeof(double) * std::max<int64_t>(n, 1));
+    S->owned.push_back(p);
+    return static_cast<double*>(p);
+}
+
+float* fbuf(gb_simplec* S, int64_t n)
+{
+    void* p = nullptr;
+    if (cudaMalloc(&p, sizeof(float) * std::max<int64_t>(n, 1)) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    cudaMemset(p, 0, sizeof(float) * std::max<int64_t>(n, 1));
+    S->owned.push_back(p);
+    return static_cast<float*>(p);
+}
+
+// --------------------------------------------------------- reductions ---
+
+//! Sum (mode 1) or sum of squares (mode 0) of f over box b into S->w.sums[slot].
+void dsum(gb_simplec* S, const Box& b, const double* f, int mode, int slot)
+{
+    gb_ctx* ctx = S->ctx;
+    Span span(ctx, GB_KERNEL_VECTOR);
+    k_sumsq_partial<<<kRedBlocks, 256, 0, ctx->stream>>>(S->g, b, f, S->w.partial + slot * kRedBlocks, mode);
+    k_sum_partials<<<1, 256, 0, ctx->stream>>>(S->w.partial + slot * kRedBlocks, kRedBlocks, S->w.sums + slot);
+    ctx->launches += 2;
+}
+
+//! max |f (* mul)| over box b into result word `word` of the context (bits).
+void dmax(gb_simplec* S, const Box& b, const double* f, const double* mul, int word)
+{
+    gb_ctx* ctx = S->ctx;
+    const int64_t n = b.count();
+    Span span(ctx, GB_KERNEL_VECTOR);
+    k_maxabs<<<static_cast<unsigned>((n + 255) / 256), 256, 0, ctx->stream>>>(S->g, b, f, mul, dword(ctx, word));
+    ++ctx->launches;
+}
+
+// ---------------------------------------------------------- ghost fills ---
+
+struct FieldPtrs {
+    double* p[6];
+    int t[6];
+    int n;
+};
+struct FieldFill {
+    double* a;
+    int t, f, rule;
+    double V;
+};
+struct FillPack {
+    FieldFill F[6];
+};
+
+//! FillBoundary of the lateral ghosts (two layers) of every field for the
+//! periodic directions: x over the valid y and z, then y over the x ghosts.
+void fill_periodic_all(gb_simplec* S, double* const* f, const int* t, int nf)
+{
+    const gb_grid g = S->g;
+    const int ng = g.ng;
+    FieldPtrs P{};
+    for (int n = 0; n < nf; ++n) {
+        P.p[n] = f[n];
+        P.t[n] = t[n];
+    }
+    P.n = nf;
+    if (g.periodic_x) {
+        Box b{{0, 0, 0}, {2 * ng - 1, g.ny, g.nz}};
+        for_box(S->ctx, b, [=] __device__(int l2, int j, int k) {
+            const int l = (l2 % ng) + 1;
+            const bool hi = l2 >= ng;
+            for (int n = 0; n < P.n; ++n) {
+                const int t = P.t[n];
+                const int nvx = g.nx + (t & 1), nvy = g.ny + ((t >> 1) & 1), nvz = g.nz + ((t >> 2) & 1);
+                if (j >= nvy || k >= nvz) { continue; }
+                double* a = P.p[n];
+                if (!hi) { a[at(g, -l, j, k)] = a[at(g, g.nx - l, j, k)]; }
+                else { a[at(g, nvx - 1 + l, j, k)] = a[at(g, nvx - 1 + l - g.nx, j, k)]; }
+            }
+        }, GB_KERNEL_BC);
+    }
+    if (g.periodic_y) {
+        const int ilo = g.periodic_x ? -ng : 0;
+        Box b{{ilo, 0, 0}, {g.nx + ng, 2 * ng - 1, g.nz}};
+        const bool px = g.periodic_x;
+        for_box(S->ctx, b, [=] __device__(int i, int l2, int k) {
+            const int l = (l2 % ng) + 1;
+            const bool hi = l2 >= ng;
+            for (int n = 0; n < P.n; ++n) {
+                const int t = P.t[n];
+                const int nvx = g.nx + (t & 1), nvy = g.ny + ((t >> 1) & 1), nvz = g.nz + ((t >> 2) & 1);
+                const int ihi = px ? nvx - 1 + ng : nvx - 1;
+                if (i > ihi || k >= nvz) { continue; }
+                double* a = P.p[n];
+                if (!hi) { a[at(g, i, -l, k)] = a[at(g, i, g.ny - l, k)]; }
+                else { a[at(g, i, nvy - 1 + l, k)] = a[at(g, i, nvy - 1 + l - g.ny, k)]; }
+            }
+        }, GB_KERNEL_BC);
+    }
+}
+
+//! The face fills of every field along d on one side (fill_face / fill_gradient_z,
+//! BoundaryConditions.cpp:418-517), fields in the reference's order.
+void fill_side(gb_simplec* S, const gb_state& q, int d, bool lo)
+{
+    const gb_grid g = S->g;
+    const int ng = g.ng;
+    const int face = d + (lo ? 0 : 3);
+    const int ft = S->bc.face[face];
+    FieldFill FF[6];
+    double* arr[6] = {q.u, q.v, q.w, q.p, q.theta, q.tke};
+    for (int f = 0; f < 6; ++f) {
+        FF[f].a = arr[f];
+        FF[f].t = kLoc[f];
+        FF[f].f = f;
+        FF[f].rule = rule_for(f, ft, d, lo);
+        FF[f].V = (ft == GB_FACE_NO_SLIP_WALL && f <= F_W) ? S->bc.wall_velocity[face][f] : 0.0;
+    }
+    FillPack P;
+    std::memcpy(P.F, FF, sizeof(FF));
+    const Profile prof = S->prof;
+    const double* z = S->z;
+    const double G = S->bc.zhi_theta_grad;
+    const int per[3] = {g.periodic_x, g.periodic_y, 0};
+    // union box over the slab: layers 0..ng along d, the grown extents elsewhere
+    Box b{};
+    for (int e = 0; e < 3; ++e) {
+        if (e == d) { continue; }
+        const bool grow = (e < d) || per[e];
+        b.lo[e] = grow ? -ng : 0;
+        b.hi[e] = ((e == 0) ? g.nx : (e == 1) ? g.ny : g.nz) + (grow ? ng : 0);
+    }
+    b.lo[d] = 0;
+    b.hi[d] = ng;
+    const int pe0 = per[0], pe1 = per[1];
+    for_box(S->ctx, b, [=] __device__(int i, int j, int k) {
+        int c[3] = {i, j, k};
+        const int layer = c[d];
+        for (int n = 0; n < 6; ++n) {
+            const FieldFill& F = P.F[n];
+            const int t = F.t;
+            // this field's slab extent in the other directions
+            bool inside = true;
+            for (int e = 0; e < 3 && inside; ++e) {
+                if (e == d) { continue; }
+                const bool grow = (e < d) || (e == 0 ? pe0 : (e == 1 ? pe1 : 0));
+                const int nv = ((e == 0) ? g.nx : (e == 1) ? g.ny : g.nz) + nodal(t, e);
+                const int lo_e = grow ? -ng : 0, hi_e = nv - 1 + (grow ? ng : 0);
+                if (c[e] < lo_e || c[e] > hi_e) { inside = false; }
+            }
+            if (!inside) { continue; }
+            const int nd = (d == 0) ? g.nx : (d == 1) ? g.ny : g.nz;
+            const bool nod = nodal(t, d);
+            double* a = F.a;
+            if (F.rule == R_GRADIENT) {
+                // the top (d == 2, not lo): one thread per column does both layers
+                if (layer != 1) { continue; }
+                const int edge = lo ? 0 : nd - 1 + nod;
+                const int c1 = lo ? edge + 1 : edge - 1, g1 = lo ? edge - 1 : edge + 1, g2 = lo ? edge - 2 : edge + 2;
+                const double zc1 = point_z(z, g, t, i, j, c1), zg1 = point_z(z, g, t, i, j, g1),
+                             zg2 = point_z(z, g, t, i, j, g2);
+                const double v1 = a[at(g, i, j, c1)] + (zg1 - zc1) * G;
+                a[at(g, i, j, g1)] = v1;
+                a[at(g, i, j, g2)] = v1 + (zg2 - zg1) * G;
+                continue;
+            }
+            const int edge = lo ? 0 : (nod ? nd : nd - 1);
+            if (layer == 0) {
+                if (!(nod && (F.rule == R_VALUE || F.rule == R_PROFILE))) { continue; }
+                int p[3] = {i, j, k};
+                p[d] = edge;
+                a[at(g, p[0], p[1], p[2])] = (F.rule == R_PROFILE)
+                    ? prof.value(F.f, height_above_ground(z, g, t, p[0], p[1], p[2])) : F.V;
+                continue;
+            }
+            const int gidx = lo ? edge - layer : edge + layer;
+            const int mirror = nod ? 2 * edge : (lo ? 2 * edge - 1 : 2 * edge + 1);
+            int p[3] = {i, j, k}, s[3] = {i, j, k};
+            p[d] = gidx;
+            s[d] = mirror - gidx;
+            double* dst = &a[at(g, p[0], p[1], p[2])];
+            if (F.rule == R_PROFILE) {
+                *dst = prof.value(F.f, height_above_ground(z, g, t, p[0], p[1], p[2]));
+            } else if (F.rule == R_VALUE) {
+                *dst = 2 * F.V - a[at(g, s[0], s[1], s[2])];
+            } else {
+                const double v = a[at(g, s[0], s[1], s[2])];
+                *dst = (F.rule == R_ODD) ? -v : v;
+            }
+        }
+    }, GB_KERNEL_BC);
+}
+
+//! fill_no_flux_w (BoundaryConditions.cpp:754-799).
+void fill_no_flux_w(gb_simplec* S, const gb_state& q)
+{
+    const gb_grid g = S->g;
+    const bool lo_on = dirichlet_normal(S->bc, 2), hi_on = dirichlet_normal(S->bc, 5);
+    if (!lo_on && !hi_on) { return; }
+    double* w = q.w;
+    const double* u = q.u;
+    const double* v = q.v;
+    const double* z = S->z;
+    const int ng = g.ng;
+    Box b{{-1, -1, 0}, {g.nx, g.ny, 1}};
+    for_box(S->ctx, b, [=] __device__(int i, int j, int side) {
+        const bool lo = (side == 0);
+        if ((lo && !lo_on) || (!lo && !hi_on)) { return; }
+        const int face = lo ? 0 : g.nz;
+        const int sgn = lo ? -1 : 1;
+        const double V = deriv<NODE, ZF, 0>(z, g, i, j, face) * (1.0 / g.dx) * interp<XF, ZF>(u, g, i, j, face)
+                       + deriv<NODE, ZF, 1>(z, g, i, j, face) * (1.0 / g.dy) * interp<YF, ZF>(v, g, i, j, face);
+        w[at(g, i, j, face)] = V;
+        for (int m = 1; m <= ng; ++m) { w[at(g, i, j, face + sgn * m)] = 2 * V - w[at(g, i, j, face - sgn * m)]; }
+    }, GB_KERNEL_BC);
+}
+
+}  // namespace
+
+void simplec_fill_ghosts(gb_simplec* S, const gb_state& q)
+{
+    double* f[6] = {q.u, q.v, q.w, q.p, q.theta, q.tke};
+    fill_periodic_all(S, f, kLoc, 6);
+    for (int d = 0; d < 3; ++d) {
+        if (is_per(S->g, d)) { continue; }
+        fill_side(S, q, d, true);
+        fill_side(S, q, d, false);
+        if (d == 2) {
+            // the no-flux w faces after u, v, w (p, theta, k do not read w)
+            fill_no_flux_w(S, q);
+        }
+    }
+    fill_periodic_all(S, f, kLoc, 6);
+}
+
+// ------------------------------------------------------------ stencils ---
+
+namespace {
+
+//! transport_fluxes (MassFlux.cpp:101-127): a_x u, a_y v, Omega, valid + one ghost.
+void transport_fluxes(gb_simplec* S, const gb_state& q, double* F0, double* F1, double* F2)
+{
+    const gb_grid g = S->g;
+    const double* u = q.u;
+    const double* v = q.v;
+    const double* w = q.w;
+    const double* ax = S->mesh.ax;
+    const double* ay = S->mesh.ay;
+    const double* z = S->z;
+    for_box(S->ctx, Box{{-1, -1, -1}, {g.nx + 1, g.ny + 1, g.nz + 1}}, [=] __device__(int i, int j, int k) {
+        if (k <= g.nz) {
+            if (j <= g.ny) { F0[at(g, i, j, k)] = ax[at(g, i, j, k)] * u[at(g, i, j, k)]; }
+            if (i <= g.nx) { F1[at(g, i, j, k)] = ay[at(g, i, j, k)] * v[at(g, i, j, k)]; }
+        }
+        if (i <= g.nx && j <= g.ny) {
+            F2[at(g, i, j, k)] = w[at(g, i, j, k)]
+                               - deriv<NODE, ZF, 0>(z, g, i, j, k) * (1.0 / g.dx) * interp<XF, ZF>(u, g, i, j, k)
+                               - deriv<NODE, ZF, 1>(z, g, i, j, k) * (1.0 / g.dy) * interp<YF, ZF>(v, g, i, j, k);
+        }
+    }, GB_KERNEL_MASSFLUX);
+}
+
+//! omega_from_w on the valid z-faces.
+void omega_from_w(gb_simplec* S, const double* u, const double* v, const double* w, double* om)
+{
+    const gb_grid g = S->g;
+    const double* z = S->z;
+    for_box(S->ctx, valid_box(g, ZF), [=] __device__(int i, int j, int k) {
+        om[at(g, i, j, k)] = w[at(g, i, j, k)]
+                           - deriv<NODE, ZF, 0>(z, g, i, j, k) * (1.0 / g.dx) * interp<XF, ZF>(u, g, i, j, k)
+                           - deriv<NODE, ZF, 1>(z, g, i, j, k) * (1.0 / g.dy) * interp<YF, ZF>(v, g, i, j, k);
+    }, GB_KERNEL_MASSFLUX);
+}
+
+//! velocity_divergence (MassFlux.cpp:129-136): Omega on the fly, then the face divergence.
+void velocity_divergence(gb_simplec* S, const double* u, const double* v, const double* w, double* div)
+{
+    const gb_grid g = S->g;
+    const double* z = S->z;
+    const double* ax = S->mesh.ax;
+    const double* ay = S->mesh.ay;
+    const double* az = S->mesh.az;
+    const double* J = S->mesh.detJ;
+    for_box(S->ctx, valid_box(g, CC), [=] __device__(int i, int j, int k) {
+        auto om = [&](int kk) {
+            return w[at(g, i, j, kk)] - deriv<NODE, ZF, 0>(z, g, i, j, kk) * (1.0 / g.dx) * interp<XF, ZF>(u, g, i, j, kk)
+                 - deriv<NODE, ZF, 1>(z, g, i, j, kk) * (1.0 / g.dy) * interp<YF, ZF>(v, g, i, j, kk);
+        };
+        const int64_t o = at(g, i, j, k), ox = at(g, i + 1, j, k), oy = at(g, i, j + 1, k), oz = at(g, i, j, k + 1);
+        div[o] = ((ax[ox] * u[ox] - ax[o] * u[o]) * (1.0 / g.dx) + (ay[oy] * v[oy] - ay[o] * v[o]) * (1.0 / g.dy)
+                  + (az[oz] * om(k + 1) - az[o] * om(k)) * (1.0 / g.dzeta))
+               / J[o];
+    }, GB_KERNEL_MASSFLUX);
+}
+
+template <int D>
+__device__ __forceinline__ double slope_dp(const double* z, const double* p, const gb_grid& g, int i, int j, int k)
+{
+    const double s = (D == 0) ? deriv<NODE, ZF, 0>(z, g, i, j, k) * (1.0 / g.dx) : deriv<NODE, ZF, 1>(z, g, i, j, k) * (1.0 / g.dy);
+    const double dp = (k == 0) ? 3.0 * p[at(g, i, j, k + 1)] - 2.0 * p[at(g, i, j, k)] - p[at(g, i, j, k + 2)]
+                               : p[at(g, i, j, k)] - p[at(g, i, j, k - 1)];
+    return s * dp * (1.0 / g.dzeta);
+}
+
+//! R_c += (G p)_c (MassFlux.cpp:138-179) fused into the residual.
+void add_pressure_gradient(gb_simplec* S, const double* p, double* Ru, double* Rv, double* Rw)
+{
+    const gb_grid g = S->g;
+    const double* z = S->z;
+    const double* J = S->mesh.detJ;
+    const double* ax = S->mesh.ax;
+    const double* ay = S->mesh.ay;
+    for_box(S->ctx, Box{{0, 0, 0}, {g.nx, g.ny, g.nz}}, [=] __device__(int i, int j, int k) {
+        if (j < g.ny && k < g.nz) {
+            const double cross = 0.25 * ((slope_dp<0>(z, p, g, i - 1, j, k) + slope_dp<0>(z, p, g, i, j, k))
+                                         + (slope_dp<0>(z, p, g, i - 1, j, k + 1) + slope_dp<0>(z, p, g, i, j, k + 1)));
+            Ru[at(g, i, j, k)] += (ax[at(g, i, j, k)] * (p[at(g, i, j, k)] - p[at(g, i - 1, j, k)]) * (1.0 / g.dx) - cross)
+                                / interp<CC, XF>(J, g, i, j, k);
+        }
+        if (i < g.nx && k < g.nz) {
+            const double cross = 0.25 * ((slope_dp<1>(z, p, g, i, j - 1, k) + slope_dp<1>(z, p, g, i, j, k))
+                                         + (slope_dp<1>(z, p, g, i, j - 1, k + 1) + slope_dp<1>(z, p, g, i, j, k + 1)));
+            Rv[at(g, i, j, k)] += (ay[at(g, i, j, k)] * (p[at(g, i, j, k)] - p[at(g, i, j - 1, k)]) * (1.0 / g.dy) - cross)
+                                / interp<CC, YF>(J, g, i, j, k);
+        }
+        if (i < g.nx && j < g.ny) {
+            Rw[at(g, i, j, k)] += (p[at(g, i, j, k)] - p[at(g, i, j, k - 1)]) * (1.0 / g.dzeta) / interp<CC, ZF>(J, g, i, j, k);
+        }
+    }, GB_KERNEL_RESIDUAL);
+}
+
+// ----------------------------------------------------------- convection ---
+
+__device__ __forceinline__ double limited_slope(int lim, double a, double b, double eps2)
+{
+    if (lim == GB_LIMITER_VAN_LEER) {
+        const double ab = a * b;
+        return (ab > 0) ? 2.0 * ab / (a + b) : 0.0;
+    }
+    if (lim == GB_LIMITER_VAN_ALBADA) { return ((b * b + eps2) * a + (a * a + eps2) * b) / (a * a + b * b + 2.0 * eps2); }
+    return 0.0;
+}
+
+__device__ __forceinline__ double muscl_face(int lim, double tr, double qm, double q0, double q1, double qp, double eps2)
+{
+    if (lim == GB_LIMITER_UPWIND) { return (tr >= 0) ? q0 : q1; }
+    return (tr >= 0) ? q0 + 0.5 * limited_slope(lim, q0 - qm, q1 - q0, eps2)
+                     : q1 - 0.5 * limited_slope(lim, q1 - q0, qp - q1, eps2);
+}
+
+//! The box of the control-volume fluxes of a field at T along D (CVFluxes.cpp:52-66).
+template <int T>
+Box flux_box(const gb_grid& g, int D)
+{
+    Box b = valid_box(g, T);
+    const int n = (D == 0) ? g.nx : (D == 1) ? g.ny : g.nz;
+    if (nodal(T, D)) {
+        b.lo[D] = -1;
+        b.hi[D] = n;
+    } else {
+        b.lo[D] = 0;
+        b.hi[D] = n;
+    }
+    return b;
+}
+
+//! Convection.cpp:17-43 flux_kernel<T, D, L>.
+template <int T, int D>
+void conv_fluxes(gb_simplec* S, const double* q, const double* F, int lim, double eps2, double* G)
+{
+    const gb_grid g = S->g;
+    constexpr int Sx = T ^ (1 << D);
+    constexpr int TF = 1 << D;
+    constexpr int l = lo_off(T, Sx, D);
+    constexpr int ex = (D == 0), ey = (D == 1), ez = (D == 2);
+    for_box(S->ctx, flux_box<T>(g, D), [=] __device__(int i, int j, int k) {
+        const double tr = interp<TF, Sx>(F, g, i, j, k);
+        const int i0 = i + l * ex, j0 = j + l * ey, k0 = k + l * ez;
+        G[at(g, i, j, k)] = tr * muscl_face(lim, tr, q[at(g, i0 - ex, j0 - ey, k0 - ez)], q[at(g, i0, j0, k0)],
+                                            q[at(g, i0 + ex, j0 + ey, k0 + ez)],
+                                            q[at(g, i0 + 2 * ex, j0 + 2 * ey, k0 + 2 * ez)], eps2);
+    }, GB_KERNEL_RESIDUAL);
+}
+
+//! out (op)= the control-volume divergence of G (CVFluxes.cpp:16-39); sign +1: =, -1: -=.
+template <int T>
+void flux_divergence(gb_simplec* S, const double* gx, const double* gy, const double* gz, double* out, int mode)
+{
+    const gb_grid g = S->g;
+    const double* J = S->mesh.detJ;
+    constexpr int lx = flux_lo(T, 0), ly = flux_lo(T, 1), lz = flux_lo(T, 2);
+    for_box(S->ctx, valid_box(g, T), [=] __device__(int i, int j, int k) {
+        const double v = ((gx[at(g, i + lx + 1, j, k)] - gx[at(g, i + lx, j, k)]) * (1.0 / g.dx)
+                          + (gy[at(g, i, j + ly + 1, k)] - gy[at(g, i, j + ly, k)]) * (1.0 / g.dy)
+                          + (gz[at(g, i, j, k + lz + 1)] - gz[at(g, i, j, k + lz)]) * (1.0 / g.dzeta))
+                       / interp<CC, T>(J, g, i, j, k);
+        const int64_t o = at(g, i, j, k);
+        if (mode == 0) { out[o] = v; } else { out[o] -= v; }
+    }, GB_KERNEL_RESIDUAL);
+}
+
+//! The bounded form's - q (transport divergence) (Convection.cpp:65-90).
+template <int T>
+void subtract_transport_divergence(gb_simplec* S, const double* q, const double* F0, const double* F1, const double* F2,
+                                   double* out)
+{
+    const gb_grid g = S->g;
+    const double* J = S->mesh.detJ;
+    constexpr int SX = T ^ XF, SY = T ^ YF, SZ = T ^ ZF;
+    constexpr int lx = flux_lo(T, 0), ly = flux_lo(T, 1), lz = flux_lo(T, 2);
+    for_box(S->ctx, valid_box(g, T), [=] __device__(int i, int j, int k) {
+        const double div = (interp<XF, SX>(F0, g, i + lx + 1, j, k) - interp<XF, SX>(F0, g, i + lx, j, k)) * (1.0 / g.dx)
+                         + (interp<YF, SY>(F1, g, i, j + ly + 1, k) - interp<YF, SY>(F1, g, i, j + ly, k)) * (1.0 / g.dy)
+                         + (interp<ZF, SZ>(F2, g, i, j, k + lz + 1) - interp<ZF, SZ>(F2, g, i, j, k + lz)) * (1.0 / g.dzeta);
+        out[at(g, i, j, k)] -= q[at(g, i, j, k)] * div / interp<CC, T>(J, g, i, j, k);
+    }, GB_KERNEL_RESIDUAL);
+}
+
+template <int T>
+void convection(gb_simplec* S, const double* q, double* const* F, int lim, double eps, bool bounded, double* out)
+{
+    const double eps2 = eps * eps;
+    double** G = S->w.G;
+    conv_fluxes<T, 0>(S, q, F[0], lim, eps2, G[0]);
+    conv_fluxes<T, 1>(S, q, F[1], lim, eps2, G[1]);
+    conv_fluxes<T, 2>(S, q, F[2], lim, eps2, G[2]);
+    flux_divergence<T>(S, G[0], G[1], G[2], out, 0);
+    if (bounded) { subtract_transport_divergence<T>(S, q, F[0], F[1], F[2], out); }
+}
+
+// ------------------------------------------------------------ diffusion ---
+
+__device__ __forceinline__ double log_mean(double a, double b)
+{
+    const double tiny = 2.2250738585072014e-308;
+    const double sum = a + b;
+    const double x = (a - b) / (sum + tiny);
+    const double s = (fabs(x) < 0.01) ? 1.0 : 0.0;
+    const double x2 = x * x;
+    const double series = 0.5 * sum * (1.0 - x2 * (1.0 / 3 + x2 * (4.0 / 45 + x2 * (44.0 / 945))));
+    const double direct = (a - b) / (log(a + tiny) - log(b + tiny) + s);
+    return (1.0 - s) * direct + s * series;
+}
+
+template <int Sx>
+__device__ __forceinline__ double face_gamma(const double* gm, const gb_grid& g, int i, int j, int k, int logz)
+{
+    if (!logz || !nodal(Sx, 2)) { return interp<CC, Sx>(gm, g, i, j, k); }
+    constexpr int lx = lo_off(CC, Sx, 0), ly = lo_off(CC, Sx, 1);
+    constexpr int nx = npts(CC, Sx, 0), ny = npts(CC, Sx, 1);
+    double sum = 0;
+    for (int b = 0; b < ny; ++b) {
+        for (int a = 0; a < nx; ++a) { sum += log_mean(gm[at(g, i + lx + a, j + ly + b, k - 1)], gm[at(g, i + lx + a, j + ly + b, k)]); }
+    }
+    return sum * (1.0 / (nx * ny));
+}
+
+template <int D>
+__device__ __forceinline__ double area_dot(const Metric<double>& m, const double v[3])
+{
+    if (D == 0) { return m.zz * v[0]; }
+    if (D == 1) { return m.zz * v[1]; }
+    return v[2] - m.zx * v[0] - m.zy * v[1];
+}
+
+template <int D>
+void scalar_diffusive_flux(gb_simplec* S, const double* q, const double* gamma, double* G)
+{
+    const gb_grid g = S->g;
+    const double* z = S->z;
+    const int logz = S->ph.log_mean;
+    constexpr int Sx = 1 << D;
+    for_box(S->ctx, flux_box<CC>(g, D), [=] __device__(int i, int j, int k) {
+        const Metric<double> m = metric_at<Sx>(z, g, i, j, k);
+        double gr[3];
+        grad_at<CC, Sx>(q, g, i, j, k, m, gr);
+        G[at(g, i, j, k)] = face_gamma<Sx>(gamma, g, i, j, k, logz) * area_dot<D>(m, gr);
+    }, GB_KERNEL_RESIDUAL);
+}
+
+template <int C, int D>
+void momentum_diffusive_flux(gb_simplec* S, const gb_state& q, const double* nu, double* G)
+{
+    const gb_grid g = S->g;
+    const double* z = S->z;
+    const double* u = q.u;
+    const double* v = q.v;
+    const double* w = q.w;
+    const int logz = S->ph.log_mean;
+    constexpr int T = 1 << C;
+    constexpr int Sx = T ^ (1 << D);
+    for_box(S->ctx, flux_box<T>(g, D), [=] __device__(int i, int j, int k) {
+        const Metric<double> m = metric_at<Sx>(z, g, i, j, k);
+        double gu[3], gv[3], gw[3];
+        grad_at<XF, Sx>(u, g, i, j, k, m, gu);
+        grad_at<YF, Sx>(v, g, i, j, k, m, gv);
+        grad_at<ZF, Sx>(w, g, i, j, k, m, gw);
+        const double* gc = (C == 0) ? gu : (C == 1) ? gv : gw;
+        const double tau[3] = {gc[0] + gu[C], gc[1] + gv[C], gc[2] + gw[C]};
+        G[at(g, i, j, k)] = face_gamma<Sx>(nu, g, i, j, k, logz) * area_dot<D>(m, tau);
+    }, GB_KERNEL_RESIDUAL);
+}
+
+template <int C>
+void momentum_diffusion_subtract(gb_simplec* S, const gb_state& q, double* R)
+{
+    double** G = S->w.G;
+    momentum_diffusive_flux<C, 0>(S, q, S->df.nu, G[0]);
+    momentum_diffusive_flux<C, 1>(S, q, S->df.nu, G[1]);
+    momentum_diffusive_flux<C, 2>(S, q, S->df.nu, G[2]);
+    flux_divergence<1 << C>(S, G[0], G[1], G[2], R, 1);
+}
+
+void scalar_diffusion_subtract(gb_simplec* S, const double* q, const double* gamma, double* R)
+{
+    double** G = S->w.G;
+    scalar_diffusive_flux<0>(S, q, gamma, G[0]);
+    scalar_diffusive_flux<1>(S, q, gamma, G[1]);
+    scalar_diffusive_flux<2>(S, q, gamma, G[2]);
+    flux_divergence<CC>(S, G[0], G[1], G[2], R, 1);
+}
+
+// ------------------------------------------------------------- forcing ---
+
+void forcing(gb_simplec* S, const gb_state& q, double** R)
+{
+    const gb_grid g = S->g;
+    const gb_physics ph = S->ph;
+    if (ph.gravity > 0) {
+        const double gt = ph.gravity / ph.theta0;
+        const double* th = q.theta;
+        const double* tr = S->w.theta_ref;
+        double* Rw = R[2];
+        for_box(S->ctx, valid_box(g, ZF), [=] __device__(int i, int j, int k) {
+            Rw[at(g, i, j, k)] -= gt * 0.5 * ((th[at(g, i, j, k - 1)] - tr[at(g, i, j, k - 1)]) + (th[at(g, i, j, k)] - tr[at(g, i, j, k)]));
+        }, GB_KERNEL_RESIDUAL);
+    }
+    if (ph.coriolis) {
+        const double pi = 3.14159265358979323846;
+        const double phi = ph.latitude * pi / 180;
+        const double fc = 4 * pi / ph.rotation_period;
+        const double fs = fc * std::sin(phi);
+        const double fcos = ph.coriolis_3d ? fc * std::cos(phi) : 0.0;
+        const double ug = ph.geostrophic ? ph.ug : 0.0, vg = ph.geostrophic ? ph.vg : 0.0;
+        const double* u = q.u;
+        const double* v = q.v;
+        const double* w = q.w;
+        double* Ru = R[0];
+        double* Rv = R[1];
+        double* Rw = R[2];
+        const bool three_d = ph.coriolis_3d;
+        for_box(S->ctx, Box{{0, 0, 0}, {g.nx, g.ny, g.nz}}, [=] __device__(int i, int j, int k) {
+            if (j < g.ny && k < g.nz) {
+                Ru[at(g, i, j, k)] -= fs * (interp<YF, XF>(v, g, i, j, k) - vg) - fcos * interp<ZF, XF>(w, g, i, j, k);
+            }
+            if (i < g.nx && k < g.nz) { Rv[at(g, i, j, k)] += fs * (interp<XF, YF>(u, g, i, j, k) - ug); }
+            if (three_d && i < g.nx && j < g.ny) { Rw[at(g, i, j, k)] -= fcos * interp<XF, ZF>(u, g, i, j, k); }
+        }, GB_KERNEL_RESIDUAL);
+    }
+    for (int c = 0; c < 3; ++c) {
+        if (ph.pressure_gradient[c] == 0) { continue; }
+        const double f = -ph.pressure_gradient[c];
+        double* Rc = R[c];
+        for_box(S->ctx, valid_box(g, kLoc[c]), [=] __device__(int i, int j, int k) { Rc[at(g, i, j, k)] += f; },
+                GB_KERNEL_RESIDUAL);
+    }
+}
+
+void fill_theta_ref(gb_simplec* S)
+{
+    const gb_grid g = S->g;
+    const Profile prof = S->prof;
+    const double* z = S->z;
+    double* tr = S->w.theta_ref;
+    for_box(S->ctx, Box{{-1, -1, -1}, {g.nx, g.ny, g.nz}}, [=] __device__(int i, int j, int k) {
+        const double zc = interp<NODE, CC>(z, g, i, j, k);
+        const int n = prof.rn;
+        double v = prof.rt[0];
+        if (zc >= prof.rz[n - 1]) {
+            v = prof.rt[n - 1];
+        } else {
+            for (int m = 1; m < n; ++m) {
+                if (zc < prof.rz[m]) {
+                    if (zc > prof.rz[m - 1]) {
+                        const double wgt = (zc - prof.rz[m - 1]) / (prof.rz[m] - prof.rz[m - 1]);
+                        v = prof.rt[m - 1] + wgt * (prof.rt[m] - prof.rt[m - 1]);
+                    } else {
+                        v = prof.rt[m - 1];
+                    }
+                    break;
+                }
+            }
+        }
+        tr[at(g, i, j, k)] = v;
+    }, GB_KERNEL_RESIDUAL);
+}
+
+//! apply_rows (BoundaryConditions.cpp:801-852).
+void apply_rows(gb_simplec* S, const gb_state& q, double** R)
+{
+    const gb_grid g = S->g;
+    const Profile prof = S->prof;
+    const double* z = S->z;
+    const double* qv[3] = {q.u, q.v, q.w};
+    for (int d = 0; d < 3; ++d) {
+        if (is_per(g, d)) { continue; }
+        for (int lo = 1; lo >= 0; --lo) {
+            const int fc = d + (lo ? 0 : 3);
+            if (!dirichlet_normal(S->bc, fc)) { continue; }
+            const bool is_profile = S->bc.face[fc] == GB_FACE_INFLOW;
+            const int t = 1 << d;
+            Box b = valid_box(g, t);
+            const int face = lo ? 0 : ((d == 0) ? g.nx : (d == 1) ? g.ny : g.nz);
+            b.lo[d] = b.hi[d] = face;
+            double* Rd = R[d];
+            const double* qd = qv[d];
+            const double* u = q.u;
+            const double* v = q.v;
+            const int dd = d;
+            for_box(S->ctx, b, [=] __device__(int i, int j, int k) {
+                double V;
+                if (dd < 2) {
+                    V = is_profile ? prof.value(dd, height_above_ground(z, g, 1 << dd, i, j, k)) : 0.0;
+                } else {
+                    V = deriv<NODE, ZF, 0>(z, g, i, j, k) * (1.0 / g.dx) * interp<XF, ZF>(u, g, i, j, k)
+                      + deriv<NODE, ZF, 1>(z, g, i, j, k) * (1.0 / g.dy) * interp<YF, ZF>(v, g, i, j, k);
+                }
+                Rd[at(g, i, j, k)] = qd[at(g, i, j, k)] - V;
+            }, GB_KERNEL_BC);
+        }
+    }
+}
+
+}  // namespace
+
+// ------------------------------------------------------------ residual ---
+
+void simplec_residual(gb_simplec* S, const gb_state& q, double** R)
+{
+    gb_ctx* ctx = S->ctx;
+    const gb_grid g = S->g;
+    const int64_t vol = volume(g);
+    for (int n = 0; n < 6; ++n) { cudaMemsetAsync(R[n], 0, sizeof(double) * vol, ctx->stream); }
+    double** F = S->w.F;
+    transport_fluxes(S, q, F[0], F[1], F[2]);
+    const gb_physics& ph = S->ph;
+    convection<XF>(S, q.u, F, ph.limiter, ph.smooth_eps_velocity, false, R[0]);
+    convection<YF>(S, q.v, F, ph.limiter, ph.smooth_eps_velocity, false, R[1]);
+    convection<ZF>(S, q.w, F, ph.limiter, ph.smooth_eps_velocity, false, R[2]);
+    momentum_diffusion_subtract<0>(S, q, R[0]);
+    momentum_diffusion_subtract<1>(S, q, R[1]);
+    momentum_diffusion_subtract<2>(S, q, R[2]);
+    add_pressure_gradient(S, q.p, R[0], R[1], R[2]);
+    forcing(S, q, R);
+    velocity_divergence(S, q.u, q.v, q.w, R[3]);
+    convection<CC>(S, q.theta, F, ph.limiter, ph.smooth_eps_theta, false, R[4]);
+    scalar_diffusion_subtract(S, q.theta, S->df.gamma_theta, R[4]);
+    convection<CC>(S, q.tke, F, GB_LIMITER_UPWIND, 1e-5, true, R[5]);
+    scalar_diffusion_subtract(S, q.tke, S->df.gamma_tke, R[5]);
+    apply_rows(S, q, R);
+    seam_sync<double>(ctx, g, XF, R[0]);
+    seam_sync<double>(ctx, g, YF, R[1]);
+    seam_sync<double>(ctx, g, ZF, R[2]);
+}
+
+// -------------------------------------------------------- implicit rows ---
+
+namespace {
+
+template <int T, int C, int D>
+__device__ __forceinline__ double face_weight(int side, int i, int j, int k, const double* f, const double* gm,
+                                              const double* z, const gb_grid& g, int logz)
+{
+    constexpr int Sx = T ^ (1 << D);
+    const double dxinv[3] = {1.0 / g.dx, 1.0 / g.dy, 1.0 / g.dzeta};
+    const Metric<double> m = metric_at<Sx>(z, g, i, j, k);
+    const double gs = face_gamma<Sx>(gm, g, i, j, k, logz);
+    const double tr = interp<(1 << D), Sx>(f, g, i, j, k);
+    double dif;
+    if (D < 2) {
+        const double own = (C == D) ? 2.0 : 1.0;
+        dif = gs * m.zz * own * dxinv[D];
+    } else {
+        double nc2 = 0;
+        if (C == 0) { nc2 = m.zx * m.zx; }
+        if (C == 1) { nc2 = m.zy * m.zy; }
+        if (C == 2) { nc2 = 1; }
+        dif = gs * (1 + m.zx * m.zx + m.zy * m.zy + nc2) / m.zz * dxinv[2];
+    }
+    const double inflow = (side == 0) ? fmax(tr, 0.0) : fmax(-tr, 0.0);
+    return (dif + inflow) * dxinv[D];
+}
+
+//! ImplicitOperator.cpp:39-74 coefficients<C> (C = -1: a cell scalar).
+template <int C>
+void implicit_coefficients(gb_simplec* S, double* const* F, const double* gm, double* A)
+{
+    const gb_grid g = S->g;
+    const double* z = S->z;
+    const double* J = S->mesh.detJ;
+    const int logz = S->ph.log_mean;
+    constexpr int T = (C < 0) ? CC : (1 << C);
+    constexpr int lx = flux_lo(T, 0), ly = flux_lo(T, 1), lz = flux_lo(T, 2);
+    const int64_t cs = volume(g);
+    const double* F0 = F[0];
+    const double* F1 = F[1];
+    const double* F2 = F[2];
+    for_box(S->ctx, valid_box(g, T), [=] __device__(int i, int j, int k) {
+        const double Jinv = 1.0 / interp<CC, T>(J, g, i, j, k);
+        const double xm = face_weight<T, C, 0>(0, i + lx, j, k, F0, gm, z, g, logz) * Jinv;
+        const double xp = face_weight<T, C, 0>(1, i + lx + 1, j, k, F0, gm, z, g, logz) * Jinv;
+        const double ym = face_weight<T, C, 1>(0, i, j + ly, k, F1, gm, z, g, logz) * Jinv;
+        const double yp = face_weight<T, C, 1>(1, i, j + ly + 1, k, F1, gm, z, g, logz) * Jinv;
+        const double zm = face_weight<T, C, 2>(0, i, j, k + lz, F2, gm, z, g, logz) * Jinv;
+        const double zp = face_weight<T, C, 2>(1, i, j, k + lz + 1, F2, gm, z, g, logz) * Jinv;
+        const int64_t o = at(g, i, j, k);
+        A[GB_COEF_XM * cs + o] = xm;
+        A[GB_COEF_XP * cs + o] = xp;
+        A[GB_COEF_YM * cs + o] = ym;
+        A[GB_COEF_YP * cs + o] = yp;
+        A[GB_COEF_ZM * cs + o] = zm;
+        A[GB_COEF_ZP * cs + o] = zp;
+        A[GB_COEF_P * cs + o] = ((xm + xp) + (ym + yp)) + (zm + zp);
+    }, GB_KERNEL_COEFS);
+}
+
+//! apply_to_implicit (BoundaryConditions.cpp:885-941) without damping.
+void apply_to_implicit(gb_simplec* S, int f, int t, double* A)
+{
+    const gb_grid g = S->g;
+    const int64_t cs = volume(g);
+    for (int d = 0; d < 3; ++d) {
+        if (is_per(g, d)) { continue; }
+        for (int lo = 1; lo >= 0; --lo) {
+            const int fc = d + (lo ? 0 : 3);
+            const int rule = rule_for(f, S->bc.face[fc], d, lo);
+            const bool nod = nodal(t, d);
+            const bool dirichlet_pt = nod && (rule == R_VALUE || rule == R_PROFILE);
+            const int nd = (d == 0) ? g.nx : (d == 1) ? g.ny : g.nz;
+            const int edge = lo ? 0 : (nod ? nd : nd - 1);
+            const int cm = (d == 0) ? GB_COEF_XM : (d == 1) ? GB_COEF_YM : GB_COEF_ZM;
+            const int cp = (d == 0) ? GB_COEF_XP : (d == 1) ? GB_COEF_YP : GB_COEF_ZP;
+            const int ghost_coef = lo ? cm : cp, other_coef = lo ? cp : cm;
+            double fold = 0;
+            bool to_other = false;
+            if (nod) { to_other = true; }
+            else if (rule == R_EVEN) { fold = -1; }
+            else if (rule == R_ODD || rule == R_VALUE) { fold = 1; }
+            else if (rule == R_GRADIENT) { to_other = true; }
+            Box b = valid_box(g, t);
+            b.lo[d] = b.hi[d] = edge;
+            for_box(S->ctx, b, [=] __device__(int i, int j, int k) {
+                const int64_t o = at(g, i, j, k);
+                if (dirichlet_pt) {
+                    for (int n = 0; n < GB_N_COEFS; ++n) { A[n * cs + o] = 0; }
+                    A[GB_COEF_P * cs + o] = 1;
+                } else {
+                    const double ag = A[ghost_coef * cs + o];
+                    A[ghost_coef * cs + o] = 0;
+                    if (to_other) { A[other_coef * cs + o] += ag; } else { A[GB_COEF_P * cs + o] += fold * ag; }
+                }
+            }, GB_KERNEL_COEFS);
+        }
+    }
+}
+
+void dirichlet_rows(gb_simplec* S, int f, int t, double* mask)
+{
+    const gb_grid g = S->g;
+    cudaMemsetAsync(mask, 0, sizeof(double) * volume(g), S->ctx->stream);
+    for (int d = 0; d < 3; ++d) {
+        if (is_per(g, d)) { continue; }
+        for (int lo = 1; lo >= 0; --lo) {
+            const int fc = d + (lo ? 0 : 3);
+            const int rule = rule_for(f, S->bc.face[fc], d, lo);
+            if (!(nodal(t, d) && (rule == R_VALUE || rule == R_PROFILE))) { continue; }
+            const int edge = lo ? 0 : ((d == 0) ? g.nx : (d == 1) ? g.ny : g.nz);
+            Box b = valid_box(g, t);
+            b.lo[d] = b.hi[d] = edge;
+            for_box(S->ctx, b, [=] __device__(int i, int j, int k) { mask[at(g, i, j, k)] = 1.0; }, GB_KERNEL_COEFS);
+        }
+    }
+}
+
+}  // namespace
+
+void simplec_implicit_rows(gb_simplec* S, int eq, double* const* F, double* A)
+{
+    switch (eq) {
+    case F_U: implicit_coefficients<0>(S, F, S->df.nu, A); break;
+    case F_V: implicit_coefficients<1>(S, F, S->df.nu, A); break;
+    case F_W: implicit_coefficients<2>(S, F, S->df.nu, A); break;
+    case F_THETA: implicit_coefficients<-1>(S, F, S->df.gamma_theta, A); break;
+    default: implicit_coefficients<-1>(S, F, S->df.gamma_tke, A); break;
+    }
+    const int t = (eq <= F_W) ? (1 << eq) : CC;
+    apply_to_implicit(S, eq, t, A);
+}
+
+// ------------------------------------------------------------ face dtau ---
+
+namespace {
+
+void face_dtau(gb_simplec* S, const double* dc, double** f)
+{
+    const gb_grid g = S->g;
+    double* fx = f[0];
+    double* fy = f[1];
+    double* fz = f[2];
+    const bool px = g.periodic_x, py = g.periodic_y;
+    for_box(S->ctx, Box{{0, 0, 0}, {g.nx, g.ny, g.nz}}, [=] __device__(int i, int j, int k) {
+        auto D = [&](int a, int b, int c) {
+            if (px) { a = (a < 0) ? a + g.nx : (a >= g.nx ? a - g.nx : a); }
+            if (py) { b = (b < 0) ? b + g.ny : (b >= g.ny ? b - g.ny : b); }
+            return dc[at(g, a, b, c)];
+        };
+        if (j < g.ny && k < g.nz) {
+            const bool lo = (!px && i == 0), hi = (!px && i == g.nx);
+            fx[at(g, i, j, k)] = lo ? D(i, j, k) : hi ? D(i - 1, j, k) : 0.5 * (D(i - 1, j, k) + D(i, j, k));
+        }
+        if (i < g.nx && k < g.nz) {
+            const bool lo = (!py && j == 0), hi = (!py && j == g.ny);
+            fy[at(g, i, j, k)] = lo ? D(i, j, k) : hi ? D(i, j - 1, k) : 0.5 * (D(i, j - 1, k) + D(i, j, k));
+        }
+        if (i < g.nx && j < g.ny) {
+            const bool lo = (k == 0), hi = (k == g.nz);
+            fz[at(g, i, j, k)] = lo ? D(i, j, k) : hi ? D(i, j, k - 1) : 0.5 * (D(i, j, k - 1) + D(i, j, k));
+        }
+    }, GB_KERNEL_COEFS);
+}
+
+template <typename TD>
+__global__ void k_convert(TD* __restrict__ dst, const double* __restrict__ src, int64_t n)
+{
+    const int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (t < n) { dst[t] = static_cast<TD>(src[t]); }
+}
+
+//! The z-line sweeps of one system, FP64 or (precision 1) FP32 inner solve:
+//! delta (FP64) receives the correction.
+gb_status line_solve(gb_simplec* S, int loc, const double* A, const double* ap, const double* rhs, double* delta,
+                     int word)
+{
+    gb_ctx* ctx = S->ctx;
+    const int64_t vol = volume(S->g);
+    cudaMemsetAsync(delta, 0, sizeof(double) * vol, ctx->stream);
+    if (S->opt.precision == 0) {
+        return zline_sweeps<double>(ctx, S->g, loc, A, ap, rhs, S->opt.zline_sweeps, delta, dword(ctx, word),
+                                    LineScratch::automatic);
+    }
+    const unsigned nb = static_cast<unsigned>((vol + 255) / 256);
+    k_convert<float><<<nb * GB_N_COEFS, 256, 0, ctx->stream>>>(S->w.A32, A, vol * GB_N_COEFS);
+    k_convert<float><<<nb, 256, 0, ctx->stream>>>(S->w.ap32, ap, vol);
+    k_convert<float><<<nb, 256, 0, ctx->stream>>>(S->w.rhs32, rhs, vol);
+    ctx->launches += 3;
+    cudaMemsetAsync(S->w.delta32, 0, sizeof(float) * vol, ctx->stream);
+    gb_status st = zline_sweeps<float>(ctx, S->g, loc, S->w.A32, S->w.ap32, S->w.rhs32, S->opt.zline_sweeps,
+                                       S->w.delta32, dword(ctx, word), LineScratch::automatic);
+    const float* d32 = S->w.delta32;
+    const gb_grid g = S->g;
+    for_box(ctx, valid_box(g, loc), [=] __device__(int i, int j, int k) {
+        delta[at(g, i, j, k)] = static_cast<double>(d32[at(g, i, j, k)]);
+    });
+    return st;
+}
+
+}  // namespace
+
+// ------------------------------------------------------- predictor etc. ---
+
+namespace {
+
+enum Word : int {
+    W_MAX_DU = 0, W_MAX_DV, W_MAX_DW, W_LAST_U, W_LAST_V, W_LAST_W, W_DIV_BEFORE, W_DIV_AFTER, W_MAX_PHI,
+    W_MAX_FU, W_MAX_FV, W_MAX_FW, W_SPEED_U, W_SPEED_V, W_SPEED_W, W_MAX_DTH, W_MAX_DK, W_LAST_TH, W_LAST_K,
+    W_CLIPPED, W_MON_U, W_MON_V, W_MON_W, W_COUNT
+};
+enum Sum : int { SUM_R0 = 0, SUM_TKE = 6, SUM_LEVEL = 8, SUM_COUNT = 8 };
+
+gb_status momentum_predictor(gb_simplec* S, const gb_state& q, double** R)
+{
+    gb_ctx* ctx = S->ctx;
+    const gb_grid g = S->g;
+    const int64_t cs = volume(g);
+    SimplecWork& w = S->w;
+    double* comps[3] = {q.u, q.v, q.w};
+    const double fs = S->ph.coriolis ? 4 * 3.14159265358979323846 * std::sin(S->ph.latitude * 3.14159265358979323846 / 180)
+                                         / S->ph.rotation_period
+                                     : 0.0;
+    for (int c = 0; c < 3; ++c) {
+        const int t = 1 << c;
+        simplec_implicit_rows(S, c, w.F, w.A);
+        dirichlet_rows(S, c, t, w.mask);
+        double* ap = w.ap[c];
+        double* dd = w.dd[c];
+        const double* A = w.A;
+        const double* mask = w.mask;
+        const double* dt = w.dtf[c];
+        const double* Rc = R[c];
+        double* rhs = w.rhs;
+        const double inv_cap = S->opt.w_vnn_cap > 0 ? 1.0 / S->opt.w_vnn_cap : 0.0;
+        const double s_margin = S->opt.w_vnn_cap_slope_margin;
+        const bool cap = (c == 2 && S->opt.w_vnn_cap > 0);
+        const double* z = S->z;
+        for_box(ctx, valid_box(g, t), [=] __device__(int i, int j, int k) {
+            const int64_t o = at(g, i, j, k);
+            const double keep = 1.0 - mask[o];
+            double p = keep / dt[o] + A[GB_COEF_P * cs + o];
+            const double nb = A[GB_COEF_XM * cs + o] + A[GB_COEF_XP * cs + o] + A[GB_COEF_YM * cs + o]
+                            + A[GB_COEF_YP * cs + o] + A[GB_COEF_ZM * cs + o] + A[GB_COEF_ZP * cs + o];
+            double d = keep * (p - nb);
+            if (cap) {
+                double term = inv_cap * (A[GB_COEF_ZM * cs + o] + A[GB_COEF_ZP * cs + o]);
+                if (s_margin > 0) {
+                    const double hx = 0.5 * (z[at(g, i + 1, j + 1, k)] + z[at(g, i + 1, j, k)] - z[at(g, i, j + 1, k)] - z[at(g, i, j, k)]) * (1.0 / g.dx);
+                    const double hy = 0.5 * (z[at(g, i + 1, j + 1, k)] + z[at(g, i, j + 1, k)] - z[at(g, i + 1, j, k)] - z[at(g, i, j, k)]) * (1.0 / g.dy);
+                    const double slope2 = hx * hx + hy * hy;
+                    if (slope2 > 0) {
+                        const double root = sqrt(1.0 + slope2) + 1.0;
+                        const double rc = slope2 / (root * root);
+                        const double lim = fmax(0.0, 1.0 / (s_margin * rc) - 1.0) / dt[o];
+                        term = fmin(term, lim);
+                    }
+                }
+                p += keep * term;
+                d += keep * term;
+            }
+            ap[o] = p;
+            dd[o] = d;
+            rhs[o] = -Rc[o];
+        }, GB_KERNEL_COEFS);
+        if (c < 2 && S->ph.coriolis && fs != 0) {
+            // the other component's residual: its horizontal mean per level
+            // (deterministic column-ordered sums), then the coupling
+            const double* other = (c == 0) ? R[1] : R[0];
+            const int to = (c == 0) ? YF : XF;
+            const int d_o = 1 - c;
+            const bool per_o = is_per(g, d_o);
+            const int n_o = (d_o == 0) ? g.nx : g.ny, n_c = (c == 0) ? g.nx : g.ny;
+            const double npts_level = static_cast<double>(n_o + (per_o ? 0 : 1)) * static_cast<double>(n_c);
+            for (int k = 0; k < g.nz; ++k) {
+                Box b = valid_box(g, to);
+                b.lo[2] = b.hi[2] = k;
+                if (per_o) { b.hi[d_o] -= 1; }
+                dsum(S, b, other, 1, SUM_LEVEL + k);
+            }
+            double* mean = w.level_sum;
+            const double* sums = w.sums + SUM_LEVEL;
+            const int nz = g.nz;
+            for_box(ctx, Box{{0, 0, 0}, {nz - 1, 0, 0}}, [=] __device__(int k, int, int) { mean[k] = sums[k] / npts_level; });
+            // the periodic images of the other residual (one ghost) for the four-face mean
+            cudaMemcpyAsync(w.og, other, sizeof(double) * cs, cudaMemcpyDeviceToDevice, ctx->stream);
+            double* og = w.og;
+            const bool px = g.periodic_x, py = g.periodic_y;
+            const double relax = S->opt.rotation_relax;
+            const bool per_c = is_per(g, c);
+            const int hi_edge = (c == 0) ? g.nx : g.ny;
+            const int cc = c;
+            for_box(ctx, valid_box(g, t), [=] __device__(int i, int j, int k) {
+                const int64_t o = at(g, i, j, k);
+                const double keep = 1.0 - mask[o];
+                if (keep == 0) { return; }
+                const int n = (cc == 0) ? i : j;
+                if (!per_c && (n == 0 || n == hi_edge)) { return; }
+                const double nb = A[GB_COEF_XM * cs + o] + A[GB_COEF_XP * cs + o] + A[GB_COEF_YM * cs + o]
+                                + A[GB_COEF_YP * cs + o] + A[GB_COEF_ZM * cs + o] + A[GB_COEF_ZP * cs + o];
+                const double net = fmax(A[GB_COEF_P * cs + o] - nb, 0.0);
+                const double tau_c = 1.0 / fmax(fabs(fs) / relax, net);
+                const double tau_own = 1.0 / (1.0 / dt[o] + net);
+                const double stiff = fs * fs * fmax(tau_c, tau_own);
+                ap[o] += stiff;
+                dd[o] += stiff;
+                // four-face mean with periodic images (og's ghosts resolved by index)
+                auto RO = [&](int a, int b2, int kk) {
+                    const int nvx = g.nx + (to & 1), nvy = g.ny + ((to >> 1) & 1);
+                    if (a < 0 || a >= nvx) {
+                        if (!px) { return og[at(g, a, b2, kk)]; }
+                        a = (a < 0) ? a + g.nx : a - g.nx;
+                    }
+                    if (b2 < 0 || b2 >= nvy) {
+                        if (!py) { return og[at(g, a, b2, kk)]; }
+                        b2 = (b2 < 0) ? b2 + g.ny : b2 - g.ny;
+                    }
+                    return og[at(g, a, b2, kk)];
+                };
+                double avg;
+                if (cc == 0) {  // interp<YF, XF>: v at (i-1..i, j..j+1)
+                    avg = ((RO(i - 1, j, k) + RO(i, j, k)) + (RO(i - 1, j + 1, k) + RO(i, j + 1, k))) * 0.25;
+                } else {        // interp<XF, YF>: u at (i..i+1, j-1..j)
+                    avg = ((RO(i, j - 1, k) + RO(i + 1, j - 1, k)) + (RO(i, j, k) + RO(i + 1, j, k))) * 0.25;
+                }
+                const double m = mean[k];
+                rhs[o] += ((cc == 0) ? -fs : fs) * (tau_c * m + tau_own * (avg - m));
+            }, GB_KERNEL_COEFS);
+        }
+        if (c == 2 && S->ph.gravity > 0) {
+            const double gt = S->ph.gravity / S->ph.theta0;
+            simplec_implicit_rows(S, F_THETA, w.F, w.At);
+            const double* At = w.At;
+            const double* th = q.theta;
+            const double* Rt = R[4];
+            for_box(ctx, valid_box(g, ZF), [=] __device__(int i, int j, int k) {
+                const int64_t o = at(g, i, j, k);
+                const double keep = 1.0 - mask[o];
+                if (keep == 0) { return; }
+                auto zc = [&](int kk) {
+                    return 0.125 * (z[at(g, i, j, kk)] + z[at(g, i + 1, j, kk)] + z[at(g, i, j + 1, kk)] + z[at(g, i + 1, j + 1, kk)]
+                                    + z[at(g, i, j, kk + 1)] + z[at(g, i + 1, j, kk + 1)] + z[at(g, i, j + 1, kk + 1)]
+                                    + z[at(g, i + 1, j + 1, kk + 1)]);
+                };
+                const double gamma = (th[at(g, i, j, k)] - th[at(g, i, j, k - 1)]) / (zc(k) - zc(k - 1));
+                const double ap_theta = 0.5 * (At[GB_COEF_P * cs + at(g, i, j, k - 1)] + At[GB_COEF_P * cs + o]);
+                const double tau = 1.0 / (1.0 / dt[o] + ap_theta);
+                const double stiff = gt * fmax(gamma, 0.0) * tau;
+                ap[o] += stiff;
+                dd[o] += stiff;
+                rhs[o] -= gt * tau * 0.5 * (Rt[at(g, i, j, k - 1)] + Rt[o]);
+            }, GB_KERNEL_COEFS);
+        }
+        gb_status st = line_solve(S, t, w.A, ap, w.rhs, w.delta, W_LAST_U + c);
+        if (st != GB_OK) { return st; }
+        dmax(S, valid_box(g, t), w.delta, nullptr, W_MAX_DU + c);
+        double* qc = comps[c];
+        const double* delta = w.delta;
+        for_box(ctx, valid_box(g, t), [=] __device__(int i, int j, int k) {
+            const int64_t o = at(g, i, j, k);
+            qc[o] += delta[o];
+        });
+    }
+    return check_cuda("momentum_predictor");
+}
+
+gb_status pressure_correction(gb_simplec* S, const gb_state& q, gb_iter_info* info)
+{
+    gb_ctx* ctx = S->ctx;
+    const gb_grid g = S->g;
+    SimplecWork& w = S->w;
+    for (int c = 0; c < 3; ++c) {
+        const double* dd = w.dd[c];
+        double* beta = w.beta[c];
+        double* keep = w.keep[c];
+        for_box(ctx, valid_box(g, kLoc[c]), [=] __device__(int i, int j, int k) {
+            const int64_t o = at(g, i, j, k);
+            const bool on = dd[o] > 0;
+            beta[o] = on ? 1.0 / dd[o] : 1.0;
+            keep[o] = on ? 1.0 : 0.0;
+        }, GB_KERNEL_COEFS);
+    }
+    velocity_divergence(S, q.u, q.v, q.w, w.rhs);
+    dmax(S, valid_box(g, CC), w.rhs, nullptr, W_DIV_BEFORE);
+    dmax(S, valid_box(g, XF), q.u, nullptr, W_SPEED_U);
+    dmax(S, valid_box(g, YF), q.v, nullptr, W_SPEED_V);
+    dmax(S, valid_box(g, ZF), q.w, nullptr, W_SPEED_W);
+    gb_status st = poisson_set_coeffs(S->poisson, S->mesh.ax, S->mesh.ay, S->mesh.az, w.beta[0], w.beta[1], w.beta[2]);
+    if (st != GB_OK) { return st; }
+    gb_poisson_result pr{};
+    st = poisson_solve(S->poisson, w.rhs, w.phi, &pr);
+    if (st != GB_OK) { return st; }
+    info->poisson_iterations = pr.iterations;
+    info->poisson_removed_mean = pr.removed_mean;
+    if (pr.singular) {
+        unsigned long long sp[3];
+        if ((st = read_words(ctx, W_SPEED_U, 3, sp)) != GB_OK) { return st; }
+        const double speed = std::max(std::max(bits_to_double(sp[0]), bits_to_double(sp[1])), bits_to_double(sp[2]));
+        const double inv_h = 1.0 / g.dx + 1.0 / g.dy + 1.0 / (S->jmin * g.dzeta);
+        if (std::fabs(pr.removed_mean) > 1.0e-8 * speed * inv_h) {
+            set_error("gust: pressure_correction: the predicted velocity has a net source the boundaries cannot carry: "
+                      "J-weighted mean divergence %g 1/s against the scale %g 1/s (a boundary condition or the "
+                      "predictor is inconsistent)", pr.removed_mean, speed * inv_h);
+            return GB_BAD_ARG;
+        }
+    }
+    double* F[3] = {w.G[0], w.G[1], w.G[2]};
+    if ((st = poisson_fluxes(S->poisson, w.phi, w.beta[0], w.beta[1], w.beta[2], F[0], F[1], F[2])) != GB_OK) { return st; }
+    const double alpha = S->opt.alpha_p;
+    double* p = q.p;
+    const double* phi = w.phi;
+    for_box(ctx, valid_box(g, CC), [=] __device__(int i, int j, int k) {
+        const int64_t o = at(g, i, j, k);
+        p[o] += alpha * phi[o];
+    });
+    dmax(S, valid_box(g, CC), w.phi, nullptr, W_MAX_PHI);
+    for (int c = 0; c < 3; ++c) { dmax(S, valid_box(g, kLoc[c]), F[c], w.keep[c], W_MAX_FU + c); }
+    omega_from_w(S, q.u, q.v, q.w, w.om);
+    double* tgt[3] = {q.u, q.v, w.om};
+    for (int c = 0; c < 3; ++c) {
+        double* tc = tgt[c];
+        const double* fc = F[c];
+        const double* kc = w.keep[c];
+        for_box(ctx, valid_box(g, kLoc[c]), [=] __device__(int i, int j, int k) {
+            const int64_t o = at(g, i, j, k);
+            tc[o] += fc[o] * kc[o];
+        });
+    }
+    seam_sync<double>(ctx, g, XF, q.u);
+    seam_sync<double>(ctx, g, YF, q.v);
+    seam_sync<double>(ctx, g, ZF, w.om);
+    {
+        double* f2[2] = {q.u, q.v};
+        const int t2[2] = {XF, YF};
+        fill_periodic_all(S, f2, t2, 2);
+    }
+    // w = Omega + z_x u_f + z_y v_f
+    {
+        double* ww = q.w;
+        const double* u = q.u;
+        const double* v = q.v;
+        const double* om = w.om;
+        const double* z = S->z;
+        for_box(ctx, valid_box(g, ZF), [=] __device__(int i, int j, int k) {
+            ww[at(g, i, j, k)] = om[at(g, i, j, k)] + deriv<NODE, ZF, 0>(z, g, i, j, k) * (1.0 / g.dx) * interp<XF, ZF>(u, g, i, j, k)
+                               + deriv<NODE, ZF, 1>(z, g, i, j, k) * (1.0 / g.dy) * interp<YF, ZF>(v, g, i, j, k);
+        }, GB_KERNEL_MASSFLUX);
+    }
+    seam_sync<double>(ctx, g, ZF, q.w);
+    {
+        double* f1[1] = {q.w};
+        const int t1[1] = {ZF};
+        fill_periodic_all(S, f1, t1, 1);
+    }
+    velocity_divergence(S, q.u, q.v, q.w, w.rhs);
+    dmax(S, valid_box(g, CC), w.rhs, nullptr, W_DIV_AFTER);
+    return check_cuda("pressure_correction");
+}
+
+gb_status scalar_sweep(gb_simplec* S, int eq, double* field, const double* Req, const double* dtau, double floor,
+                       bool clip, int w_max, int w_last)
+{
+    gb_ctx* ctx = S->ctx;
+    const gb_grid g = S->g;
+    SimplecWork& w = S->w;
+    const int64_t cs = volume(g);
+    simplec_implicit_rows(S, eq, w.F, w.A);
+    double* rhs = w.rhs;
+    double* ap = w.ap[0];
+    const double* A = w.A;
+    for_box(ctx, valid_box(g, CC), [=] __device__(int i, int j, int k) {
+        const int64_t o = at(g, i, j, k);
+        rhs[o] = -Req[o];
+        ap[o] = 1.0 / dtau[o] + A[GB_COEF_P * cs + o];
+    }, GB_KERNEL_COEFS);
+    gb_status st = line_solve(S, CC, w.A, ap, w.rhs, w.delta, w_last);
+    if (st != GB_OK) { return st; }
+    dmax(S, valid_box(g, CC), w.delta, nullptr, w_max);
+    const double* delta = w.delta;
+    unsigned long long* count = dword(ctx, W_CLIPPED);
+    const bool do_clip = clip && eq == F_TKE;
+    for_box(ctx, valid_box(g, CC), [=] __device__(int i, int j, int k) {
+        const int64_t o = at(g, i, j, k);
+        double v = field[o] + delta[o];
+        if (do_clip && v < floor) {
+            v = floor;
+            atomicAdd(count, 1ull);
+        }
+        field[o] = v;
+    });
+    return check_cuda("scalar_sweep");
+}
+
+}  // namespace
+
+// ------------------------------------------------------------- iterate ---
+
+gb_status simplec_iterate(gb_simplec* S, const gb_state& q, const double* dtau, gb_iter_info* info)
+{
+    gb_ctx* ctx = S->ctx;
+    const gb_grid g = S->g;
+    SimplecWork& w = S->w;
+    *info = gb_iter_info{};
+    cudaMemsetAsync(dword(ctx, 0), 0, sizeof(unsigned long long) * W_COUNT, ctx->stream);
+    simplec_fill_ghosts(S, q);
+    simplec_residual(S, q, w.R);
+    for (int n = 0; n < 6; ++n) { dsum(S, valid_box(g, kLoc[n]), w.R[n], 0, SUM_R0 + n); }
+    dsum(S, valid_box(g, CC), q.tke, 1, SUM_TKE);
+    dmax(S, valid_box(g, XF), q.u, nullptr, W_MON_U);
+    dmax(S, valid_box(g, YF), q.v, nullptr, W_MON_V);
+    dmax(S, valid_box(g, ZF), q.w, nullptr, W_MON_W);
+    transport_fluxes(S, q, w.F[0], w.F[1], w.F[2]);
+    face_dtau(S, dtau, w.dtf);
+    gb_status st = momentum_predictor(S, q, w.R);
+    if (st != GB_OK) { return st; }
+    simplec_fill_ghosts(S, q);
+    if ((st = pressure_correction(S, q, info)) != GB_OK) { return st; }
+    convection<CC>(S, q.theta, w.F, S->ph.limiter, S->ph.smooth_eps_theta, false, w.conv0);
+    simplec_fill_ghosts(S, q);
+    transport_fluxes(S, q, w.F[0], w.F[1], w.F[2]);
+    convection<CC>(S, q.theta, w.F, S->ph.limiter, S->ph.smooth_eps_theta, false, w.conv1);
+    {
+        double* Rt = w.R[4];
+        const double* c0 = w.conv0;
+        const double* c1 = w.conv1;
+        for_box(ctx, valid_box(g, CC), [=] __device__(int i, int j, int k) {
+            const int64_t o = at(g, i, j, k);
+            Rt[o] += c1[o] - c0[o];
+        });
+    }
+    if ((st = scalar_sweep(S, F_THETA, q.theta, w.R[4], dtau, 0, false, W_MAX_DTH, W_LAST_TH)) != GB_OK) { return st; }
+    if ((st = scalar_sweep(S, F_TKE, q.tke, w.R[5], dtau, S->opt.tke_floor, true, W_MAX_DK, W_LAST_K)) != GB_OK) {
+        return st;
+    }
+    // read every result of the iteration at once
+    unsigned long long words[W_COUNT];
+    if ((st = read_words(ctx, 0, W_COUNT, words)) != GB_OK) { return st; }
+    double sums[8];
+    cudaMemcpyAsync(S->h_words, w.sums, sizeof(double) * 8, cudaMemcpyDeviceToHost, ctx->stream);
+    if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) { return check_cuda("simplec_iterate"); }
+    std::memcpy(sums, S->h_words, sizeof(double) * 8);
+    auto wd = [&](int n) { return bits_to_double(words[n]); };
+    const gb_physics& ph = S->ph;
+    const double U = ph.scale_velocity, H = ph.scale_height;
+    const double scale[6] = {U * U / H, U * U / H, U * U / H, U / H, U * ph.scale_theta / H, U * ph.scale_tke / H};
+    for (int n = 0; n < 6; ++n) {
+        const Box b = valid_box(g, kLoc[n]);
+        info->residual_norms[n] = std::sqrt(sums[n]) / std::sqrt(static_cast<double>(b.count())) / scale[n];
+    }
+    info->mean_tke = sums[SUM_TKE] / (static_cast<double>(g.nx) * g.ny * g.nz);
+    info->max_speed = std::max(std::max(wd(W_MON_U), wd(W_MON_V)), wd(W_MON_W));
+    info->max_du = wd(W_MAX_DU);
+    info->max_dv = wd(W_MAX_DV);
+    info->max_dw = wd(W_MAX_DW);
+    info->last_sweep_du = wd(W_LAST_U);
+    info->last_sweep_dv = wd(W_LAST_V);
+    info->last_sweep_dw = wd(W_LAST_W);
+    info->divergence_before = wd(W_DIV_BEFORE);
+    info->divergence_after = wd(W_DIV_AFTER);
+    info->max_dp = S->opt.alpha_p * wd(W_MAX_PHI);
+    info->max_dtheta = wd(W_MAX_DTH);
+    info->max_dtke = wd(W_MAX_DK);
+    info->tke_clipped = static_cast<int64_t>(words[W_CLIPPED]);
+    for (int n = 0; n < 6; ++n) {
+        if (!std::isfinite(info->residual_norms[n])) {
+            set_error("gust: SimplecStage::iterate: non-finite residual (equation %d)", n);
+            return GB_NONFINITE;
+        }
+    }
+    return check_cuda("SimplecStage::iterate");
+}
+
+// ------------------------------------------------------ pseudo-time step ---
+
+gb_status simplec_local_dtau(gb_simplec* S, const gb_state& q, double cfl, double* dtau)
+{
+    const gb_grid g = S->g;
+    omega_from_w(S, q.u, q.v, q.w, S->w.om);
+    const double* u = q.u;
+    const double* v = q.v;
+    const double* om = S->w.om;
+    const double* J = S->mesh.detJ;
+    const double* nu = S->df.nu;
+    const double dxinv = 1.0 / g.dx, dyinv = 1.0 / g.dy, dzinv = 1.0 / g.dzeta;
+    const double diff_h = 2 * (dxinv * dxinv + dyinv * dyinv);
+    for_box(S->ctx, valid_box(g, CC), [=] __device__(int i, int j, int k) {
+        const double uc = interp<XF, CC>(u, g, i, j, k), vc = interp<YF, CC>(v, g, i, j, k), oc = interp<ZF, CC>(om, g, i, j, k);
+        double rate = fabs(uc) * dxinv + fabs(vc) * dyinv + fabs(oc) * dzinv / J[at(g, i, j, k)];
+        if (nu) { rate += nu[at(g, i, j, k)] * diff_h; }
+        dtau[at(g, i, j, k)] = cfl / fmax(rate, 1.0e-12);
+    }, GB_KERNEL_COEFS);
+    return check_cuda("local_dtau");
+}
+
+// ----------------------------------------------------------- creation ---
+
+gb_status simplec_build(gb_simplec* S)
+{
+    gb_ctx* ctx = S->ctx;
+    const gb_grid& g = S->g;
+    const int64_t vol = volume(g);
+    SimplecWork& w = S->w;
+    for (int n = 0; n < 6; ++n) { w.R[n] = dbuf(S, vol); }
+    for (int n = 0; n < 3; ++n) {
+        w.F[n] = dbuf(S, vol);
+        w.ap[n] = dbuf(S, vol);
+        w.dd[n] = dbuf(S, vol);
+        w.dtf[n] = dbuf(S, vol);
+        w.beta[n] = dbuf(S, vol);
+        w.keep[n] = dbuf(S, vol);
+    }
+    for (int n = 0; n < 3; ++n) { w.G[n] = dbuf(S, vol); }
+    w.tmp = dbuf(S, vol);
+    w.A = dbuf(S, vol * GB_N_COEFS);
+    w.At = dbuf(S, vol * GB_N_COEFS);
+    w.mask = dbuf(S, vol);
+    w.rhs = dbuf(S, vol);
+    w.delta = dbuf(S, vol);
+    w.phi = dbuf(S, vol);
+    w.om = dbuf(S, vol);
+    w.theta_ref = dbuf(S, vol);
+    w.conv0 = dbuf(S, vol);
+    w.conv1 = dbuf(S, vol);
+    w.og = dbuf(S, vol);
+    w.level_sum = dbuf(S, g.nz + 1);
+    w.partial = dbuf(S, static_cast<int64_t>(kRedBlocks) * (SUM_LEVEL + g.nz + 1));
+    w.sums = dbuf(S, SUM_LEVEL + g.nz + 1);
+    if (S->opt.precision == 1) {
+        w.A32 = fbuf(S, vol * GB_N_COEFS);
+        w.ap32 = fbuf(S, vol);
+        w.rhs32 = fbuf(S, vol);
+        w.delta32 = fbuf(S, vol);
+    }
+    for (void* p : S->owned) {
+        if (p == nullptr) {
+            set_error("gust: SimplecStage: cannot allocate the workspace");
+            return GB_OOM;
+        }
+    }
+    if (cudaMallocHost(&S->h_words, sizeof(double) * 64) != cudaSuccess) {
+        cudaGetLastError();
+        return GB_OOM;
+    }
+    // the profile view and theta_ref
+    Profile& p = S->prof;
+    p.ustar = S->bc.inflow_ustar;
+    p.z0 = S->bc.inflow_z0;
+    p.kappa = S->bc.kappa;
+    p.Cmu0 = S->bc.Cmu0;
+    p.inv_lmax = S->bc.inflow_inv_lmax;
+    const double pi = 3.14159265358979323846;
+    p.cosd = std::cos(S->bc.inflow_direction * pi / 180.0);
+    p.sind = std::sin(S->bc.inflow_direction * pi / 180.0);
+    p.rn = S->bc.theta_ref_n;
+    for (int n = 0; n < p.rn; ++n) {
+        p.rz[n] = S->bc.theta_ref_z[n];
+        p.rt[n] = S->bc.theta_ref_theta[n];
+    }
+    if (S->ph.gravity > 0) { fill_theta_ref(S); }
+    // the Poisson solver of the correction (poisson_bc_from_faces, BoundaryConditions.cpp:362-380)
+    int32_t pbc[6];
+    for (int f = 0; f < 6; ++f) {
+        const int d = f % 3;
+        pbc[f] = is_per(g, d) ? GB_POISSON_PERIODIC
+                              : (S->bc.face[f] == GB_FACE_OUTFLOW ? GB_POISSON_DIRICHLET : GB_POISSON_NEUMANN);
+    }
+    gb_poisson_opts po = S->opt.poisson;
+    po.reltol = S->opt.pressure_reltol;
+    po.precision = S->opt.precision;
+    gb_status st = gb_poisson_create(ctx, &g, pbc, S->z, S->mesh.detJ, &po, &S->poisson);
+    if (st != GB_OK) { return st; }
+    // min J for the net-source scale (the mesh is fixed): one host pass at creation
+    {
+        std::vector<double> h(vol);
+        cudaMemcpyAsync(h.data(), S->mesh.detJ, sizeof(double) * vol, cudaMemcpyDeviceToHost, ctx->stream);
+        cudaStreamSynchronize(ctx->stream);
+        double m = 1e300;
+        for (int k = 0; k < g.nz; ++k) {
+            for (int j = 0; j < g.ny; ++j) {
+                for (int i = 0; i < g.nx; ++i) { m = std::min(m, h[at(g, i, j, k)]); }
+            }
+        }
+        S->jmin = m;
+    }
+    return check_cuda("SimplecStage");
+}
+
+}  // namespace gb
+
+namespace gb {
+
+gb_status simplec_create_checked(gb_ctx* ctx, const gb_grid* g, const gb_bc* bc, const gb_physics* ph,
+                                 const gb_simplec_opts* opt, const double* z_nd, const gb_mesh_fields* mesh,
+                                 const gb_diffusivities* df, gb_simplec** out)
+{
+    *out = nullptr;
+    auto* S = new (std::nothrow) gb_simplec;
+    if (S == nullptr) { return GB_OOM; }
+    S->ctx = ctx;
+    S->g = *g;
+    S->bc = *bc;
+    S->ph = *ph;
+    S->opt = *opt;
+    S->z = z_nd;
+    S->mesh = *mesh;
+    S->df = *df;
+    const gb_status st = simplec_build(S);
+    if (st != GB_OK) {
+        simplec_delete(S);
+        return st;
+    }
+    *out = S;
+    return GB_OK;
+}
+
+void simplec_delete(gb_simplec* S)
+{
+    if (S == nullptr) { return; }
+    cudaStreamSynchronize(S->ctx->stream);
+    if (S->h_words) { cudaFreeHost(S->h_words); }
+    delete S;
+}
+
+}  // namespace gb

@@ -1,0 +1,18 @@
+// The SIMPLEC stage's internal entry points (the C ABI wraps them).
+#pragma once
+
+#include "gb_common.cuh"
+
+struct gb_simplec;
+
+namespace gb {
+
+gb_status simplec_build(gb_simplec* S);
+void simplec_delete(gb_simplec* S);
+void simplec_fill_ghosts(gb_simplec* S, const gb_state& q);
+void simplec_residual(gb_simplec* S, const gb_state& q, double** R);
+void simplec_implicit_rows(gb_simplec* S, int eq, double* const* F, double* A);
+gb_status simplec_iterate(gb_simplec* S, const gb_state& q, const double* dtau, gb_iter_info* info);
+gb_status simplec_local_dtau(gb_simplec* S, const gb_state& q, double cfl, double* dtau);
+
+}  // namespace gb

@@ -1,0 +1,117 @@
+"""gust::SimplecStage on the GPU (Source/Simplec.H:185-263): one instance's
+SIMPLEC outer iteration through the C ABI. The fields are torch tensors in
+the grid layout (ablsteadyrans_b200.grid.Grid)."""
+import ctypes
+
+from . import abi
+from .grid import GbGrid
+
+
+def _declare(L):
+    P = ctypes.c_void_p
+    G = ctypes.POINTER(GbGrid)
+    L.gb_simplec_create.argtypes = [P, G, ctypes.POINTER(abi.BC), ctypes.POINTER(abi.Physics),
+                                    ctypes.POINTER(abi.SimplecOptions), P, ctypes.POINTER(abi.MeshFields),
+                                    ctypes.POINTER(abi.Diffusivities), ctypes.POINTER(P)]
+    L.gb_simplec_destroy.argtypes = [P]
+    L.gb_simplec_fill_ghosts.argtypes = [P, ctypes.POINTER(abi.State)]
+    L.gb_simplec_residual.argtypes = [P, ctypes.POINTER(abi.State), ctypes.POINTER(ctypes.c_void_p)]
+    L.gb_simplec_iterate.argtypes = [P, ctypes.POINTER(abi.State), P, ctypes.POINTER(abi.IterInfo)]
+    L.gb_local_dtau.argtypes = [P, ctypes.POINTER(abi.State), ctypes.c_double, P]
+
+
+FIELDS = ("u", "v", "w", "p", "theta", "tke")
+
+
+class DeviceCase:
+    """Device copies of one instance: state (u, v, w, p, theta, k), node
+    heights, metrics, diffusivities."""
+
+    def __init__(self, grid, z, J, ax, ay, az, nu, gamma_theta, gamma_tke, q=None):
+        import torch
+
+        def dev(a):
+            return torch.from_numpy(a).cuda() if not isinstance(a, torch.Tensor) else a.cuda()
+
+        self.grid = grid
+        self.z, self.J, self.ax, self.ay, self.az = map(dev, (z, J, ax, ay, az))
+        self.nu, self.gt, self.gk = map(dev, (nu, gamma_theta, gamma_tke))
+        self.q = {f: (dev(q[f]) if q is not None else torch.zeros(grid.shape, dtype=torch.float64, device="cuda"))
+                  for f in FIELDS}
+
+    @classmethod
+    def from_oracle(cls, case):
+        return cls(case.grid, case.z, case.J, case.ax, case.ay, case.az, case.nu, case.gt, case.gk, case.q)
+
+    def state(self):
+        return abi.State(*[self.q[f].data_ptr() for f in FIELDS], self.z.data_ptr())
+
+    def mesh(self):
+        return abi.MeshFields(self.J.data_ptr(), self.ax.data_ptr(), self.ay.data_ptr(), self.az.data_ptr())
+
+    def diffusivities(self):
+        return abi.Diffusivities(self.nu.data_ptr(), self.gt.data_ptr(), self.gk.data_ptr())
+
+    def host(self, f):
+        return self.q[f].cpu().numpy()
+
+
+class SimplecStage:
+    """One instance's SIMPLEC stage (gb_simplec)."""
+
+    def __init__(self, ctx, case, bc, physics, options):
+        from . import _lib_full, check
+        self._L = _lib_full()
+        if not getattr(self._L, "_gb_simplec", False):
+            _declare(self._L)
+            self._L._gb_simplec = True
+        self.ctx = ctx
+        self.case = case
+        self.bc, self.physics, self.options = bc, physics, options
+        self._m = case.mesh()
+        self._d = case.diffusivities()
+        self._h = ctypes.c_void_p()
+        check(self._L.gb_simplec_create(ctx.handle, ctypes.byref(case.grid.c), ctypes.byref(bc), ctypes.byref(physics),
+                                        ctypes.byref(options), ctypes.c_void_p(case.z.data_ptr()),
+                                        ctypes.byref(self._m), ctypes.byref(self._d), ctypes.byref(self._h)))
+
+    def fill_ghosts(self):
+        from . import check
+        st = self.case.state()
+        check(self._L.gb_simplec_fill_ghosts(self._h, ctypes.byref(st)))
+
+    def residual(self):
+        import torch
+        from . import check
+        R = [torch.zeros(self.case.grid.shape, dtype=torch.float64, device="cuda") for _ in range(6)]
+        arr = (ctypes.c_void_p * 6)(*[r.data_ptr() for r in R])
+        st = self.case.state()
+        check(self._L.gb_simplec_residual(self._h, ctypes.byref(st), arr))
+        return R
+
+    def local_dtau(self, cfl, out=None):
+        import torch
+        from . import check
+        dt = out if out is not None else torch.zeros(self.case.grid.shape, dtype=torch.float64, device="cuda")
+        st = self.case.state()
+        check(self._L.gb_local_dtau(self._h, ctypes.byref(st), float(cfl), ctypes.c_void_p(dt.data_ptr())))
+        return dt
+
+    def iterate(self, dtau):
+        from . import check
+        info = abi.IterInfo()
+        st = self.case.state()
+        check(self._L.gb_simplec_iterate(self._h, ctypes.byref(st), ctypes.c_void_p(dtau.data_ptr()), ctypes.byref(info)))
+        return info
+
+    def close(self):
+        from . import check
+        if self._h:
+            check(self._L.gb_simplec_destroy(self._h))
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -285,6 +285,33 @@ typedef struct gb_iter_info {
     int64_t tke_clipped;
 } gb_iter_info;
 
+typedef struct gb_simplec gb_simplec;
+
+/* gust::SimplecStage (Source/Simplec.H:185-263) for one instance: the
+ * boundary conditions, physics and options, the mesh (z_nd, metrics: device
+ * arrays kept by reference) and the diffusivities. Builds the workspace and
+ * the correction's Poisson solver. Checks the simplec.* ranges and the face
+ * types with the reference's messages. */
+gb_status gb_simplec_create(gb_ctx* ctx, const gb_grid* g, const gb_bc* bc, const gb_physics* ph,
+                            const gb_simplec_opts* opt, const double* z_nd, const gb_mesh_fields* mesh,
+                            const gb_diffusivities* df, gb_simplec** out);
+gb_status gb_simplec_destroy(gb_simplec* s);
+
+/* BoundaryConditions::fill_ghosts (Source/BoundaryConditions.H:174-175): two
+ * ghost layers of u, v, w, p, theta, k and the Dirichlet face points. */
+gb_status gb_simplec_fill_ghosts(gb_simplec* s, const gb_state* q);
+
+/* gust::residual (Source/Residual.H:133-134) at q (ghosts filled by the
+ * caller): R[0..5] = R_u, R_v, R_w, R_p, R_theta, R_k (device arrays). */
+gb_status gb_simplec_residual(gb_simplec* s, const gb_state* q, double* const* R);
+
+/* SimplecStage::iterate (Source/Simplec.cpp:452-506): one SIMPLEC outer
+ * iteration of q with the local pseudo-time step dtau (cells). */
+gb_status gb_simplec_iterate(gb_simplec* s, const gb_state* q, const double* dtau, gb_iter_info* info);
+
+/* gust::local_dtau (Source/PseudoTime.H:32-33) with the stage's diffusivity nu. */
+gb_status gb_local_dtau(gb_simplec* s, const gb_state* q, double cfl, double* dtau);
+
 #ifdef __cplusplus
 }
 #endif

@@ -170,3 +170,31 @@ def flat_case(nx, ny, nz, Lx, Ly, H, periodic_x, periodic_y, visc):
     nu = g.np_zeros() + visc
     case = oracle.Case(g, z, J, ax, ay, az, nu, nu.copy(), nu.copy())
     return case
+
+
+def terrain_simplec_case(nx, ny, nz, periodic_x, periodic_y, hill=60.0, dx=40.0, seed=0, visc=(5.0, 20.0)):
+    """An oracle.Case over a BTF Gaussian hill with diffusivities that vary in
+    height and a smooth seeded state (a shear profile plus small random
+    perturbations; seam copies made one unknown)."""
+    import oracle
+    g, z, J, ax, ay, az, zcc = smooth_terrain_case(nx, ny, nz, periodic_x, periodic_y, hill=hill, dx=dx, seed=seed)
+    zc = zcc.copy()
+    nu = visc[0] + (visc[1] - visc[0]) * np.clip(zc / 1500.0, 0, 1)
+    case = oracle.Case(g, z, J, ax, ay, az, nu, 1.3 * nu, 2.0 * nu)
+    rng = np.random.default_rng(seed + 17)
+    hfac = np.log1p(np.maximum(zc, 0.0) / 0.1)
+    for f, loc, amp, base in (("u", 1, 0.3, 8.0), ("v", 2, 0.3, -1.5), ("w", 4, 0.05, 0.0), ("p", 0, 2.0, 0.0),
+                              ("theta", 0, 0.5, 300.0), ("tke", 0, 0.05, 0.3)):
+        v = g.valid(loc)
+        shape = case.q[f][v].shape
+        prof = hfac[g.valid(0)].mean(axis=(1, 2))
+        nk = shape[0]
+        col = np.interp(np.arange(nk), np.arange(len(prof)), prof)[:, None, None] / max(prof.max(), 1e-9)
+        val = base * (col if f in ("u", "v") else 1.0) + amp * rng.standard_normal(shape)
+        if f == "theta":
+            val = base + 0.003 * np.arange(nk)[:, None, None] * 40 + amp * rng.standard_normal(shape)
+        if f == "tke":
+            val = np.abs(val) + 0.01
+        case.q[f][v] = val
+        seam_sync(g, loc, case.q[f])
+    return case
