@@ -261,40 +261,95 @@ __global__ void k_coarse_areas(gb_grid gc, double* __restrict__ AXc, double* __r
     }
 }
 
-//! One colour of the zebra z-line relaxation: on every column with (i + j) & 1
-//! == color, r = b - A x over the column, T the principal tridiagonal, and
-//! x += T^{-1} r (Thomas; c', e' in shared memory [k][thread]).
+//! The principal tridiagonal (D, C, U) of every cell of a level, computed
+//! once per set of coefficients (the smoother's line operator T).
 template <typename T>
-__global__ void __launch_bounds__(64) k_smooth_color(gb_grid g, PBC b, int color, T* __restrict__ x,
-                                                     const T* __restrict__ wrap, const T* __restrict__ bv,
-                                                     const T* __restrict__ AX, const T* __restrict__ AY,
-                                                     const T* __restrict__ AZ, const T* __restrict__ J,
-                                                     const T* __restrict__ z)
+__global__ void k_line_tridiag(gb_grid g, PBC b, const T* __restrict__ AX, const T* __restrict__ AY,
+                               const T* __restrict__ AZ, const T* __restrict__ J, const T* __restrict__ z,
+                               T* __restrict__ TD, T* __restrict__ TC, T* __restrict__ TU)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = blockIdx.z;
+    if (i >= g.nx || j >= g.ny) { return; }
+    T D, C, U;
+    line_tridiag<T>(g, b, AX, AY, AZ, J, z, i, j, k, D, C, U);
+    const int64_t o = at(g, i, j, k);
+    TD[o] = D;
+    TC[o] = C;
+    TU[o] = U;
+}
+
+//! Zebra relaxation, first half of a colour: r = b - A x on every cell of the
+//! columns with (i + j) & 1 == color (one thread per cell; every read happens
+//! before the colour's updates, so the periodic wrap reads see the old values).
+template <typename T>
+__global__ void k_color_residual(gb_grid g, PBC b, int color, const T* __restrict__ x, const T* __restrict__ bv,
+                                 const T* __restrict__ AX, const T* __restrict__ AY, const T* __restrict__ AZ,
+                                 const T* __restrict__ J, const T* __restrict__ z, T* __restrict__ r)
+{
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int i = 2 * (blockIdx.x * blockDim.x + threadIdx.x) + ((j + color) & 1);
+    const int k = blockIdx.z;
+    if (i >= g.nx || j >= g.ny) { return; }
+    const int64_t o = at(g, i, j, k);
+    r[o] = bv[o] - adotx<T>(g, b, i, j, k, x, x, AX, AY, AZ, J, z);
+}
+
+//! Zebra relaxation, second half: on every column of the colour x += T^{-1} r
+//! by the Thomas recurrences, the column's r, D, C, U staged R levels ahead
+//! into shared memory with asynchronous copies (c', e' in shared memory).
+template <typename T, int R>
+__global__ void __launch_bounds__(64) k_color_solve(gb_grid g, int color, const T* __restrict__ r,
+                                                    const T* __restrict__ TD, const T* __restrict__ TC,
+                                                    const T* __restrict__ TU, T* __restrict__ x)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int tid = threadIdx.x;
     const int nthr = blockDim.x;
     const int j = blockIdx.y;
     const int i = 2 * (blockIdx.x * blockDim.x + threadIdx.x) + ((j + color) & 1);
-    if (i >= g.nx) { return; }
-    T* cs = reinterpret_cast<T*>(smem_raw);
+    const bool active = i < g.nx;
+    T* ring = reinterpret_cast<T*>(smem_raw);
+    T* cs = ring + R * 4 * nthr;
     T* es = cs + static_cast<int64_t>(g.nz) * nthr;
+    const int64_t o0 = active ? at(g, i, j, 0) : 0;
+    auto issue = [&](int k) {
+        if (active && k < g.nz) {
+            const int64_t o = o0 + static_cast<int64_t>(k) * g.sz;
+            T* s = ring + (k % R) * 4 * nthr + tid;
+            cp_async_elem(s, r + o);
+            cp_async_elem(s + nthr, TD + o);
+            cp_async_elem(s + 2 * nthr, TC + o);
+            cp_async_elem(s + 3 * nthr, TU + o);
+        }
+        cp_async_commit();
+    };
+#pragma unroll
+    for (int k = 0; k < R - 1; ++k) { issue(k); }
     T cp = T(0), ep = T(0);
     for (int k = 0; k < g.nz; ++k) {
-        const T r = bv[at(g, i, j, k)] - adotx<T>(g, b, i, j, k, x, wrap, AX, AY, AZ, J, z);
-        T D, C, U;
-        line_tridiag<T>(g, b, AX, AY, AZ, J, z, i, j, k, D, C, U);
-        const T m = (k == 0) ? C : C - D * cp;
-        cp = U / m;
-        ep = ((k == 0) ? r : r - D * ep) / m;
-        cs[k * nthr + tid] = cp;
-        es[k * nthr + tid] = ep;
+        issue(k + R - 1);
+        cp_async_wait<R - 1>();
+        if (active) {
+            const T* s = ring + (k % R) * 4 * nthr + tid;
+            const T rk = s[0], D = s[nthr], C = s[2 * nthr], U = s[3 * nthr];
+            const T m = (k == 0) ? C : C - D * cp;
+            cp = U / m;
+            ep = ((k == 0) ? rk : rk - D * ep) / m;
+            cs[k * nthr + tid] = cp;
+            es[k * nthr + tid] = ep;
+        }
     }
+    cp_async_wait<0>();
+    if (!active) { return; }
     T xk = ep;
-    x[at(g, i, j, g.nz - 1)] += xk;
+    int64_t o = o0 + static_cast<int64_t>(g.nz - 1) * g.sz;
+    x[o] += xk;
     for (int k = g.nz - 2; k >= 0; --k) {
+        o -= g.sz;
         xk = es[k * nthr + tid] - cs[k * nthr + tid] * xk;
-        x[at(g, i, j, k)] += xk;
+        x[o] += xk;
     }
 }
 
@@ -497,19 +552,35 @@ void mg_smooth(gb_poisson* P, PoissonLevels<T>& L, int l)
     gb_ctx* ctx = P->ctx;
     const gb_grid& g = L.g[l];
     const PBC& b = L.b[l];
-    const bool odd_wrap = (g.periodic_x && (g.nx & 1)) || (g.periodic_y && (g.ny & 1));
-    const int nthr = 64;
-    const size_t smem = static_cast<size_t>(2) * g.nz * nthr * sizeof(T);
+    constexpr int R = 4;
+    const int nthr = 32;
+    const size_t smem = static_cast<size_t>(R * 4 + 2 * g.nz) * nthr * sizeof(T);
+    static bool attr_done[2] = {false, false};
+    const int ti = sizeof(T) == 8 ? 1 : 0;
+    if (!attr_done[ti]) {
+        cudaFuncSetAttribute(k_color_solve<T, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        attr_done[ti] = true;
+    }
+    const int half = (g.nx + 1) / 2;
     for (int color = 0; color < 2; ++color) {
-        const T* wrap = L.x[l];
-        if (odd_wrap) {
-            cudaMemcpyAsync(L.snap[l], L.x[l], sizeof(T) * volume(g), cudaMemcpyDeviceToDevice, ctx->stream);
-            wrap = L.snap[l];
-        }
-        const dim3 grid(((g.nx + 1) / 2 + nthr - 1) / nthr, g.ny);
         Span span(ctx, GB_KERNEL_MG_SMOOTH);
-        k_smooth_color<T><<<grid, nthr, smem, ctx->stream>>>(g, b, color, L.x[l], wrap, L.bv[l], L.AX[l], L.AY[l],
-                                                            L.AZ[l], L.J[l], L.z[l]);
+        const dim3 rgrid((half + 31) / 32, (g.ny + 3) / 4, g.nz);
+        k_color_residual<T><<<rgrid, dim3(32, 4), 0, ctx->stream>>>(g, b, color, L.x[l], L.bv[l], L.AX[l], L.AY[l],
+                                                                   L.AZ[l], L.J[l], L.z[l], L.r[l]);
+        const dim3 sgrid((half + nthr - 1) / nthr, g.ny);
+        k_color_solve<T, R><<<sgrid, nthr, smem, ctx->stream>>>(g, color, L.r[l], L.TD[l], L.TC[l], L.TU[l], L.x[l]);
+        ctx->launches += 2;
+    }
+}
+
+template <typename T>
+void build_line_tridiag(gb_poisson* P, PoissonLevels<T>& L)
+{
+    gb_ctx* ctx = P->ctx;
+    for (int l = 0; l < P->nlev; ++l) {
+        const gb_grid& g = L.g[l];
+        k_line_tridiag<T><<<cols_grid(g, g.nz), kColsBlock, 0, ctx->stream>>>(g, L.b[l], L.AX[l], L.AY[l], L.AZ[l],
+                                                                              L.J[l], L.z[l], L.TD[l], L.TC[l], L.TU[l]);
         ++ctx->launches;
     }
 }
@@ -641,6 +712,13 @@ gb_status poisson_build(gb_poisson* P)
         D.bv[l] = dalloc<double>(D.owned, vol);
         D.r[l] = dalloc<double>(D.owned, vol);
         D.snap[l] = dalloc<double>(D.owned, vol);
+        D.TD[l] = dalloc<double>(D.owned, vol);
+        D.TC[l] = dalloc<double>(D.owned, vol);
+        D.TU[l] = dalloc<double>(D.owned, vol);
+        if (!D.TD[l] || !D.TC[l] || !D.TU[l]) {
+            set_error("gust: PoissonSolver: cannot allocate the multigrid levels");
+            return GB_OOM;
+        }
         if (!D.AX[l] || !D.AY[l] || !D.AZ[l] || !D.x[l] || !D.bv[l] || !D.r[l] || !D.snap[l] || (l > 0 && (!D.z[l] || !D.J[l]))) {
             set_error("gust: PoissonSolver: cannot allocate the multigrid levels");
             return GB_OOM;
@@ -673,6 +751,13 @@ gb_status poisson_build(gb_poisson* P)
             F.bv[l] = dalloc<float>(F.owned, vol);
             F.r[l] = dalloc<float>(F.owned, vol);
             F.snap[l] = dalloc<float>(F.owned, vol);
+            F.TD[l] = dalloc<float>(F.owned, vol);
+            F.TC[l] = dalloc<float>(F.owned, vol);
+            F.TU[l] = dalloc<float>(F.owned, vol);
+            if (!F.TD[l] || !F.TC[l] || !F.TU[l]) {
+                set_error("gust: PoissonSolver: cannot allocate the FP32 multigrid levels");
+                return GB_OOM;
+            }
             if (!F.z[l] || !F.J[l] || !F.AX[l] || !F.AY[l] || !F.AZ[l] || !F.x[l] || !F.bv[l] || !F.r[l] || !F.snap[l]) {
                 set_error("gust: PoissonSolver: cannot allocate the FP32 multigrid levels");
                 return GB_OOM;
@@ -737,6 +822,7 @@ gb_status poisson_set_coeffs(gb_poisson* P, const double* ax, const double* ay, 
             ctx->launches += 3;
         }
     }
+    if (P->opt.precision == 1) { build_line_tridiag(P, P->fl); } else { build_line_tridiag(P, P->dl); }
     P->coeffs_set = true;
     return check_cuda("PoissonSolver::set_coeffs");
 }

@@ -23,6 +23,9 @@ struct PoissonLevels {
     T* bv[kMaxLevels] = {};
     T* r[kMaxLevels] = {};
     T* snap[kMaxLevels] = {};
+    T* TD[kMaxLevels] = {};   // the smoother's line tridiagonal, per level
+    T* TC[kMaxLevels] = {};
+    T* TU[kMaxLevels] = {};
     std::vector<void*> owned;
     void release();
 };

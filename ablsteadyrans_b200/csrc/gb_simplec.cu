@@ -160,6 +160,29 @@ __global__ void k_sum_partials(const double* __restrict__ partial, int n, double
     }
 }
 
+//! The mean of f over one k-plane of box b per block (block k: level k),
+//! summed in a fixed order (Predictor.cpp:286-306: the horizontal mean of the
+//! other component's residual per level, every face once).
+__global__ void k_level_mean(gb_grid g, Box b, const double* __restrict__ f, double npts_level, double* __restrict__ mean)
+{
+    __shared__ double red[8];
+    const int k = blockIdx.x;
+    const int nx = b.hi[0] - b.lo[0] + 1, ny = b.hi[1] - b.lo[1] + 1;
+    double s = 0;
+    for (int n = threadIdx.x; n < nx * ny; n += blockDim.x) {
+        const int i = b.lo[0] + n % nx, j = b.lo[1] + n / nx;
+        s += f[at(g, i, j, k)];
+    }
+    s = warp_sum(s);
+    if ((threadIdx.x & 31) == 0) { red[threadIdx.x >> 5] = s; }
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double t = (threadIdx.x < 8) ? red[threadIdx.x] : 0.0;
+        t = warp_sum(t);
+        if (threadIdx.x == 0) { mean[k] = t / npts_level; }
+    }
+}
+
 __global__ void k_maxabs(gb_grid g, Box b, const double* __restrict__ f, const double* __restrict__ mul,
                          unsigned long long* __restrict__ slot)
 {
@@ -1189,16 +1212,15 @@ gb_status momentum_predictor(gb_simplec* S, const gb_state& q, double** R)
             const bool per_o = is_per(g, d_o);
             const int n_o = (d_o == 0) ? g.nx : g.ny, n_c = (c == 0) ? g.nx : g.ny;
             const double npts_level = static_cast<double>(n_o + (per_o ? 0 : 1)) * static_cast<double>(n_c);
-            for (int k = 0; k < g.nz; ++k) {
+            {
+                // one block per level, a fixed summation order: deterministic
                 Box b = valid_box(g, to);
-                b.lo[2] = b.hi[2] = k;
                 if (per_o) { b.hi[d_o] -= 1; }
-                dsum(S, b, other, 1, SUM_LEVEL + k);
+                Span span(ctx, GB_KERNEL_VECTOR);
+                k_level_mean<<<g.nz, 256, 0, ctx->stream>>>(g, b, other, npts_level, w.level_sum);
+                ++ctx->launches;
             }
             double* mean = w.level_sum;
-            const double* sums = w.sums + SUM_LEVEL;
-            const int nz = g.nz;
-            for_box(ctx, Box{{0, 0, 0}, {nz - 1, 0, 0}}, [=] __device__(int k, int, int) { mean[k] = sums[k] / npts_level; });
             // the periodic images of the other residual (one ghost) for the four-face mean
             cudaMemcpyAsync(w.og, other, sizeof(double) * cs, cudaMemcpyDeviceToDevice, ctx->stream);
             double* og = w.og;

@@ -102,3 +102,32 @@ def test_oracle_one_correction_reduces_the_divergence():
     st, info, _ = oracle.simplec_iterate(case, bc, phys, opts, dtau)
     assert st == 0
     assert info.divergence_after < 1e-8 * info.divergence_before
+
+
+def test_workload_mesh_matches_oracle_bit_for_bit():
+    """The product's host mesh construction (BTF from the ground, ghost rows)
+    equals the oracle's restatement bit for bit; the stretched levels have
+    the solved ratios the configurations need."""
+    from ablsteadyrans_b200 import workloads
+    for nz, ratio in ((48, 1.0927), (64, 1.0622), (96, 1.0350)):
+        zl, r = workloads.geometric_zlevels(nz)
+        assert abs(r - ratio) < 5e-5 and zl[1] == 2.0 and abs(zl[-1] - 1500.0) < 1e-9
+    inst = workloads.config1(nx=24, ny=20, nz=16)
+    g = inst.grid
+    ground = workloads.node_ground(g, lambda x, y: 150.0 * np.exp(-(((x - 300) ** 2 + (y - 250) ** 2) / 300.0 ** 2)))
+    zl, _ = workloads.geometric_zlevels(16)
+    a = workloads.btf_heights(g, zl, ground)
+    b = oracle.btf_heights(g, zl, ground)
+    G = g.ng
+    sl = (slice(G - 1, G + g.nz + 2), slice(G - 1, G + g.ny + 2), slice(G - 1, G + g.nx + 2))
+    assert np.array_equal(a[sl], b[sl])
+
+
+def test_driver_ser_law():
+    """ser_cfl (Source/PseudoTime.cpp:53-61): the cap, the growth limit and cfl0 r^-p."""
+    from ablsteadyrans_b200.driver import ser_cfl
+    assert ser_cfl(1.0, 1.0, 1.0, 10.0, 1.0, 2.0) == 1.0
+    assert ser_cfl(1.0, 0.1, 1.0, 10.0, 1.0, 2.0) == 2.0
+    assert ser_cfl(8.0, 0.01, 1.0, 10.0, 1.0, 2.0) == 10.0
+    assert ser_cfl(4.0, 0.2, 1.0, 10.0, 1.0, 2.0) == pytest.approx(5.0)
+    assert ser_cfl(4.0, 0.2, 1.0, 10.0, 0.0, 2.0) == 1.0
