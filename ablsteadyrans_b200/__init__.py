@@ -71,6 +71,7 @@ def _declare(L):
     L.gb_ctx_profile_read.argtypes = [P, i32, ctypes.POINTER(f64), ctypes.POINTER(i64)]
     L.gb_zline_jacobi.argtypes = [P, G, i32, P, P, P, i32, P, ctypes.POINTER(f64)]
     L.gb_zline_jacobi_f32.argtypes = [P, G, i32, P, P, P, i32, P, ctypes.POINTER(ctypes.c_float)]
+    L.gb_zline_jacobi_noalloc.argtypes = [G, i32, P, P, P, i32, P, ctypes.POINTER(f64), P]
 
 
 def check(status):
@@ -141,6 +142,22 @@ def zline_jacobi(ctx, grid, loc, A, ap, rhs, sweeps, delta):
         out = ctypes.c_float()
         check(L.gb_zline_jacobi_f32(ctx.handle, ctypes.byref(grid.c), loc, _ptr(A), _ptr(ap), _ptr(rhs), sweeps,
                                     _ptr(delta), ctypes.byref(out)))
+    return float(out.value)
+
+
+def zline_jacobi_noalloc(grid, loc, A, ap, rhs, sweeps, delta, stream=None):
+    """The FP64 z-line Jacobi solve without a context and without any device
+    allocation (gb_zline_jacobi_noalloc): its scratch is a fixed array in the
+    library (grids up to 2^21 padded points); calls that may overlap on one
+    device race on it. stream: a torch.cuda.Stream (default: the current
+    one). Returns max |change of the last sweep|."""
+    import torch
+    L = lib()
+    if stream is None:
+        stream = torch.cuda.current_stream()
+    out = ctypes.c_double()
+    check(L.gb_zline_jacobi_noalloc(ctypes.byref(grid.c), loc, _ptr(A), _ptr(ap), _ptr(rhs), sweeps, _ptr(delta),
+                                    ctypes.byref(out), ctypes.c_void_p(stream.cuda_stream)))
     return float(out.value)
 
 

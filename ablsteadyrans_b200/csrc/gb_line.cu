@@ -14,6 +14,7 @@
 #include "gb_line.cuh"
 
 #include <algorithm>
+#include <mutex>
 
 namespace gb {
 
@@ -396,3 +397,145 @@ gb_status gb_zline_jacobi_f32(gb_ctx* ctx, const gb_grid* g, int32_t loc, const 
 }
 
 }  // extern "C"
+
+// ---- The allocation-free z-line solve ------------------------------------
+//
+// gb_zline_jacobi_noalloc runs the same FP64 sweeps as gb_zline_jacobi (the
+// pipelined kernel with one-warp blocks, which is what a context with default
+// tuning runs) for a caller that may not allocate device memory at all: no
+// gb_ctx (creating one allocates), no cudaMalloc or cudaFree behind its back.
+// Its only scratch, the ping-pong iterate and the change word, live in the
+// fixed array below, which the CUDA runtime reserves on each device when it
+// loads this library's device code.
+namespace {
+
+//! Largest padded grid volume (points) the allocation-free solve accepts:
+//! 2^21 points, 16 MiB of FP64 iterate (a 128 x 128 x 64 cell grid with two
+//! ghost layers is 1.22 M points).
+constexpr int64_t kNoAllocMaxPoints = int64_t(1) << 21;
+//! The change word sits one 256-byte block past the iterate.
+constexpr int64_t kNoAllocWords = kNoAllocMaxPoints + 32;
+
+//! Shared by every call on a device. The iterate part needs no initial value:
+//! each sweep writes every point the next sweep reads. The change word must be
+//! zero when the last sweep starts; each call zeroes it on its own stream.
+static __device__ __align__(256) double g_line_noalloc_scratch[kNoAllocWords];
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+double* g_noalloc_addr[kNoAllocMaxDevices] = {};
+
+//! Per-device set-up, once, with that device current: the array's device
+//! address and the shared-memory limit of the two sweep kernels.
+gb_status noalloc_setup(int dev, double** out)
+{
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (g_noalloc_addr[dev] == nullptr) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_line_noalloc_scratch);
+        if (e == cudaSuccess) {
+            e = cudaFuncSetAttribute(gb::zline_pipe_kernel<double, true, 4>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        }
+        if (e == cudaSuccess) {
+            e = cudaFuncSetAttribute(gb::zline_pipe_kernel<double, false, 4>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        }
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            gb::set_error("gust: zline_jacobi_noalloc: set-up on device %d failed: %s (%s)", dev,
+                          cudaGetErrorName(e), cudaGetErrorString(e));
+            return GB_CUDA;
+        }
+        g_noalloc_addr[dev] = static_cast<double*>(p);
+    }
+    *out = g_noalloc_addr[dev];
+    return GB_OK;
+}
+
+}  // namespace
+
+extern "C" gb_status gb_zline_jacobi_noalloc(const gb_grid* g, int32_t loc, const double* A, const double* ap,
+                                             const double* rhs, int32_t sweeps, double* delta, double* change,
+                                             void* stream)
+{
+    gb::clear_error();
+    const char* op = "zline_jacobi_noalloc";
+    gb_status st = gb::check_grid(op, g);
+    if (st != GB_OK) { return st; }
+    if ((st = gb::check_loc(op, loc)) != GB_OK) { return st; }
+    if (sweeps < 1) {
+        gb::set_error("gust: zline_jacobi_noalloc: sweeps must be >= 1 (got %d)", sweeps);
+        return GB_BAD_ARG;
+    }
+    if (A == nullptr || ap == nullptr || rhs == nullptr || delta == nullptr) {
+        gb::set_error("gust: zline_jacobi_noalloc: A, ap, rhs and delta must be device arrays of the grid");
+        return GB_BAD_ARG;
+    }
+    const int64_t vol = gb::volume(*g);
+    if (vol > kNoAllocMaxPoints) {
+        gb::set_error("gust: zline_jacobi_noalloc: the grid has %lld padded points, more than the fixed scratch "
+                      "of %lld points (16 MiB); use gb_zline_jacobi with a context",
+                      static_cast<long long>(vol), static_cast<long long>(kNoAllocMaxPoints));
+        return GB_BAD_ARG;
+    }
+    constexpr int R = 4, NTHR = 32;
+    const int ni = gb::ext_x(*g, loc), nj = gb::ext_y(*g, loc), nk = gb::ext_z(*g, loc);
+    const size_t smem_first = static_cast<size_t>(R * 4 + 2 * nk) * NTHR * sizeof(double);
+    const size_t smem = static_cast<size_t>(R * 12 + 2 * nk) * NTHR * sizeof(double);
+    if (smem > 200 * 1024) {
+        gb::set_error("gust: zline_jacobi_noalloc: %d z-levels need %zu bytes of shared memory per block, more than "
+                      "200 KiB", nk, smem);
+        return GB_BAD_ARG;
+    }
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNoAllocMaxDevices) {
+        cudaGetLastError();
+        gb::set_error("gust: zline_jacobi_noalloc: no usable current CUDA device");
+        return GB_CUDA;
+    }
+    double* base = nullptr;
+    if ((st = noalloc_setup(dev, &base)) != GB_OK) { return st; }
+    double* next = base;
+    unsigned long long* word = reinterpret_cast<unsigned long long*>(base + kNoAllocMaxPoints);
+    const cudaStream_t s = static_cast<cudaStream_t>(stream);
+    cudaMemsetAsync(delta, 0, sizeof(double) * vol, s);
+    cudaMemsetAsync(word, 0, sizeof(unsigned long long), s);
+    double* buf[2] = {delta, next};
+    for (int k = 0; k < sweeps; ++k) {
+        gb::LineArgs<double> a;
+        a.g = *g;
+        a.ni = ni;
+        a.nj = nj;
+        a.nk = nk;
+        a.A = A;
+        a.cs = vol;
+        a.ap = ap;
+        a.rhs = rhs;
+        a.dold = buf[(sweeps - k) & 1];
+        a.dnew = buf[(sweeps - 1 - k) & 1];
+        a.cbuf = nullptr;
+        a.ebuf = nullptr;
+        a.first = (k == 0) ? 1 : 0;
+        a.change = (k == sweeps - 1) ? word : nullptr;
+        const dim3 grid((ni + NTHR - 1) / NTHR, nj);
+        if (a.first) {
+            gb::zline_pipe_kernel<double, true, R><<<grid, NTHR, smem_first, s>>>(a);
+        } else {
+            gb::zline_pipe_kernel<double, false, R><<<grid, NTHR, smem, s>>>(a);
+        }
+    }
+    const bool sx = (loc & 1) && g->periodic_x, sy = ((loc >> 1) & 1) && g->periodic_y;
+    if (sx || sy) {
+        const int n = std::max(nj, ni) * nk;
+        gb::seam_sync_kernel<double><<<(n + 255) / 256, 256, 0, s>>>(*g, loc, delta);
+    }
+    if ((st = gb::check_cuda(op)) != GB_OK) { return st; }
+    if (change != nullptr) {
+        unsigned long long w = 0;
+        cudaMemcpyAsync(&w, word, sizeof(w), cudaMemcpyDeviceToHost, s);
+        if (cudaStreamSynchronize(s) != cudaSuccess) { return gb::check_cuda(op); }
+        *change = gb::bits_to_double(w);
+    }
+    return GB_OK;
+}

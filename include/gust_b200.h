@@ -121,6 +121,32 @@ gb_status gb_zline_jacobi(gb_ctx* ctx, const gb_grid* g, int32_t loc, const doub
 /* The same in FP32 (the inner solver of the mixed-precision defect correction). */
 gb_status gb_zline_jacobi_f32(gb_ctx* ctx, const gb_grid* g, int32_t loc, const float* A, const float* ap,
                               const float* rhs, int32_t sweeps, float* delta, float* change);
+/* The FP64 z-line Jacobi solve of gb_zline_jacobi for a caller that must not
+ * allocate device memory. This entry point has no counterpart in the
+ * reference; it exists for hosts that cannot let a library allocate: one that
+ * has handed its device memory to its own arena up front (as an AMReX
+ * application does), or that cannot take the device-wide synchronisation a
+ * cudaMalloc/cudaFree pair brings in the middle of its step. It takes no
+ * context and allocates nothing: its scratch (the ping-pong iterate and the
+ * change word) is one fixed array in this library's device memory, reserved
+ * by the CUDA runtime when the library's device code is loaded on a device.
+ * - Limit: gb_grid_volume(g) <= 2^21 padded points (16 MiB of scratch) and
+ *   at most 376 z-levels; larger grids are refused with GB_BAD_ARG and a
+ *   message (use gb_zline_jacobi).
+ * - Set-up: the first call on each device (that device current) looks up the
+ *   array's address and sets the kernels' shared-memory limit; later calls on
+ *   that device reuse it. Make that first call before any stream capture.
+ * - Sharing: every call on a device uses the same array. Calls issued one
+ *   after another on one stream are safe; calls that may overlap (other
+ *   streams, other threads) race on it. The iterate needs no initial value
+ *   (each sweep writes every point the next one reads); the change word must
+ *   start at zero, and each call zeroes it on its stream before the sweeps.
+ * - stream: the caller's cudaStream_t (NULL: the default stream). With change
+ *   non-NULL the call waits for the stream to read max |change|; with change
+ *   NULL it returns as soon as the work is queued.
+ * Results equal those of gb_zline_jacobi on a context with default tuning. */
+gb_status gb_zline_jacobi_noalloc(const gb_grid* g, int32_t loc, const double* A, const double* ap,
+                                  const double* rhs, int32_t sweeps, double* delta, double* change, void* stream);
 
 /* ---- mesh --------------------------------------------------------------- */
 
