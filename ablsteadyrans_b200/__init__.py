@@ -30,7 +30,7 @@ _lib = None
 GB_OK = 0
 KERNEL_LINE_SWEEP, KERNEL_POISSON_APPLY, KERNEL_MG_SMOOTH, KERNEL_MG_TRANSFER, KERNEL_RESIDUAL, \
     KERNEL_MASSFLUX, KERNEL_COEFS, KERNEL_VECTOR, KERNEL_BC = range(9)
-TUNE_LINE_VARIANT, TUNE_LINE_BLOCK, TUNE_MG_SMOOTH_BLOCK = range(3)
+TUNE_LINE_VARIANT, TUNE_LINE_BLOCK, TUNE_MG_COARSE_KERNEL = range(3)
 STATUS_NAMES = {0: "OK", 1: "BAD_ARG", 2: "NONFINITE", 3: "NOT_CONVERGED", 4: "TIMEOUT", 5: "OOM", 6: "CUDA"}
 
 
@@ -69,6 +69,7 @@ def _declare(L):
     L.gb_ctx_tune.argtypes = [P, i32, i32]
     L.gb_ctx_profile.argtypes = [P, i32]
     L.gb_ctx_profile_read.argtypes = [P, i32, ctypes.POINTER(f64), ctypes.POINTER(i64)]
+    L.gb_ctx_profile_mask.argtypes = [P, ctypes.c_uint32]
     L.gb_zline_jacobi.argtypes = [P, G, i32, P, P, P, i32, P, ctypes.POINTER(f64)]
     L.gb_zline_jacobi_f32.argtypes = [P, G, i32, P, P, P, i32, P, ctypes.POINTER(ctypes.c_float)]
     L.gb_zline_jacobi_noalloc.argtypes = [G, i32, P, P, P, i32, P, ctypes.POINTER(f64), P]
@@ -108,6 +109,13 @@ class Context:
 
     def profile(self, enable):
         check(lib().gb_ctx_profile(self._h, int(bool(enable))))
+
+    def profile_mask(self, families):
+        """Time only these kernel families while profiling (default: all)."""
+        mask = 0
+        for f in families:
+            mask |= 1 << int(f)
+        check(lib().gb_ctx_profile_mask(self._h, mask))
 
     def profile_read(self, family):
         """(total milliseconds, launches) of one kernel family since profile(True)."""

@@ -50,6 +50,15 @@ __device__ __forceinline__ double warp_max(double v)
     for (int o = 16; o > 0; o >>= 1) { v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o)); }
     return v;
 }
+//! Warp max that keeps a NaN (fmax drops it): a diverged field reports NaN.
+__device__ __forceinline__ double warp_max_nan(double v)
+{
+    for (int o = 16; o > 0; o >>= 1) {
+        const double w = __shfl_xor_sync(0xffffffffu, v, o);
+        v = (w > v || w != w) ? w : v;
+    }
+    return v;
+}
 __device__ __forceinline__ float warp_max(float v)
 {
     for (int o = 16; o > 0; o >>= 1) { v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o)); }
@@ -122,6 +131,8 @@ struct gb_ctx {
     bool profiling{false};
     struct Span { int family; cudaEvent_t start, stop; };
     std::vector<Span> spans;
+    std::vector<int> open_spans;        // per open Span: its index in spans, or -1 (family not timed)
+    uint32_t profile_mask{0xffffffffu};  // families timed while profiling (bit = GB_KERNEL_*)
     std::vector<cudaEvent_t> event_pool;
     //! Tuning knobs (GB_TUNE_*), 0 = default.
     int tune[GB_N_TUNE] = {};

@@ -81,15 +81,22 @@ cudaEvent_t take_event(gb_ctx* ctx)
 void span_begin(gb_ctx* ctx, int family)
 {
     if (!ctx->profiling) { return; }
+    if (((ctx->profile_mask >> family) & 1u) == 0) {
+        ctx->open_spans.push_back(-1);
+        return;
+    }
     gb_ctx::Span s{family, take_event(ctx), take_event(ctx)};
     cudaEventRecord(s.start, ctx->stream);
+    ctx->open_spans.push_back(static_cast<int>(ctx->spans.size()));
     ctx->spans.push_back(s);
 }
 
 void span_end(gb_ctx* ctx)
 {
-    if (!ctx->profiling || ctx->spans.empty()) { return; }
-    cudaEventRecord(ctx->spans.back().stop, ctx->stream);
+    if (!ctx->profiling || ctx->open_spans.empty()) { return; }
+    const int n = ctx->open_spans.back();
+    ctx->open_spans.pop_back();
+    if (n >= 0) { cudaEventRecord(ctx->spans[n].stop, ctx->stream); }
 }
 
 gb_status check_grid(const char* op, const gb_grid* g)
@@ -216,8 +223,20 @@ gb_status gb_ctx_profile(gb_ctx* ctx, int32_t enable)
         ctx->event_pool.push_back(s.stop);
     }
     ctx->spans.clear();
+    ctx->open_spans.clear();
     ctx->profiling = enable != 0;
     return gb::check_cuda("gb_ctx_profile");
+}
+
+gb_status gb_ctx_profile_mask(gb_ctx* ctx, uint32_t mask)
+{
+    gb::clear_error();
+    if (ctx == nullptr) {
+        gb::set_error("gust: gb_ctx_profile_mask: ctx is null");
+        return GB_BAD_ARG;
+    }
+    ctx->profile_mask = mask;
+    return GB_OK;
 }
 
 gb_status gb_ctx_profile_read(gb_ctx* ctx, int32_t family, double* total_ms, int64_t* spans)

@@ -213,6 +213,125 @@ __global__ void __launch_bounds__(128) zline_pipe_kernel(LineArgs<T> a)
     }
 }
 
+//! The pipelined sweep with the column factorisation kept between sweeps.
+//! The system (a_P, a_ZM, a_ZP) is the same in every sweep of a solve, so the
+//! first sweep stores the reciprocal pivots 1/m_k and the eliminated uppers
+//! c'_k = -a_ZP,k / m_k (m_0 = a_P,0, m_k = a_P,k + a_ZM,k c'_{k-1}) in
+//! scratch, and every later sweep runs the forward recurrence
+//! e_k = (r_k + a_ZM,k e_{k-1}) / m_k as a multiply by the stored 1/m_k:
+//! no division on the k chain. Inputs are staged R levels ahead with cp.async
+//! as in zline_pipe_kernel.
+template <typename T, bool FIRST, int R>
+__global__ void __launch_bounds__(128) zline_fact_kernel(LineArgs<T> a, T* __restrict__ im_out,
+                                                         const T* __restrict__ im_in, T* __restrict__ cp_out,
+                                                         const T* __restrict__ cp_in)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    constexpr int NV = FIRST ? 4 : 12;
+    const int nthr = blockDim.x * blockDim.y;
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const bool active = (i < a.ni) && (j < a.nj);
+    const gb_grid& g = a.g;
+    T* ring = reinterpret_cast<T*>(smem_raw);
+    T* cs = ring + R * NV * nthr;
+    T* es = cs + static_cast<int64_t>(a.nk) * nthr;
+    int64_t o0 = 0, oxm = -1, oxp = -1, oym = -1, oyp = -1;
+    if (active) {
+        const int im = lateral_image(i - 1, a.ni, g.nx, g.periodic_x != 0);
+        const int ip = lateral_image(i + 1, a.ni, g.nx, g.periodic_x != 0);
+        const int jm = lateral_image(j - 1, a.nj, g.ny, g.periodic_y != 0);
+        const int jp = lateral_image(j + 1, a.nj, g.ny, g.periodic_y != 0);
+        o0 = at(g, i, j, 0);
+        oxm = (im >= 0) ? at(g, im, j, 0) : -1;
+        oxp = (ip >= 0) ? at(g, ip, j, 0) : -1;
+        oym = (jm >= 0) ? at(g, i, jm, 0) : -1;
+        oyp = (jp >= 0) ? at(g, i, jp, 0) : -1;
+    }
+    const T* __restrict__ azm = a.A + GB_COEF_ZM * a.cs + o0;
+    const T* __restrict__ azp = a.A + GB_COEF_ZP * a.cs + o0;
+    const T* __restrict__ axm = a.A + GB_COEF_XM * a.cs + o0;
+    const T* __restrict__ axp = a.A + GB_COEF_XP * a.cs + o0;
+    const T* __restrict__ aym = a.A + GB_COEF_YM * a.cs + o0;
+    const T* __restrict__ ayp = a.A + GB_COEF_YP * a.cs + o0;
+    // slots: 0 rhs, 1 a_P (first) or 1/m, 2 a_ZM, 3 a_ZP (first) or c', 4-7 lateral
+    // coefficients, 8-11 the lagged neighbours
+    auto issue = [&](int k) {
+        if (active && k < a.nk) {
+            const int64_t ko = static_cast<int64_t>(k) * g.sz;
+            T* s = ring + (k % R) * NV * nthr + tid;
+            cp_async_elem(s, a.rhs + o0 + ko);
+            cp_async_elem(s + nthr, FIRST ? a.ap + o0 + ko : im_in + o0 + ko);
+            cp_async_elem(s + 2 * nthr, azm + ko);
+            cp_async_elem(s + 3 * nthr, FIRST ? azp + ko : cp_in + o0 + ko);
+            if (!FIRST) {
+                cp_async_elem(s + 4 * nthr, axm + ko);
+                cp_async_elem(s + 5 * nthr, axp + ko);
+                cp_async_elem(s + 6 * nthr, aym + ko);
+                cp_async_elem(s + 7 * nthr, ayp + ko);
+                if (oxm >= 0) { cp_async_elem(s + 8 * nthr, a.dold + oxm + ko); } else { s[8 * nthr] = T(0); }
+                if (oxp >= 0) { cp_async_elem(s + 9 * nthr, a.dold + oxp + ko); } else { s[9 * nthr] = T(0); }
+                if (oym >= 0) { cp_async_elem(s + 10 * nthr, a.dold + oym + ko); } else { s[10 * nthr] = T(0); }
+                if (oyp >= 0) { cp_async_elem(s + 11 * nthr, a.dold + oyp + ko); } else { s[11 * nthr] = T(0); }
+            }
+        }
+        cp_async_commit();
+    };
+#pragma unroll
+    for (int k = 0; k < R - 1; ++k) { issue(k); }
+    T cprev = T(0), eprev = T(0);
+    for (int k = 0; k < a.nk; ++k) {
+        issue(k + R - 1);
+        cp_async_wait<R - 1>();
+        if (active) {
+            const T* s = ring + (k % R) * NV * nthr + tid;
+            T rk = s[0];
+            const T lower = -s[2 * nthr];
+            T inv, c;
+            if (FIRST) {
+                const T m = (k == 0) ? s[nthr] : s[nthr] - lower * cprev;
+                inv = T(1) / m;
+                c = -s[3 * nthr] * inv;
+                const int64_t o = o0 + static_cast<int64_t>(k) * g.sz;
+                im_out[o] = inv;
+                cp_out[o] = c;
+            } else {
+                inv = s[nthr];
+                c = s[3 * nthr];
+                rk = rk + s[4 * nthr] * s[8 * nthr] + s[5 * nthr] * s[9 * nthr] + s[6 * nthr] * s[10 * nthr]
+                   + s[7 * nthr] * s[11 * nthr];
+            }
+            cprev = c;
+            eprev = ((k == 0) ? rk : rk - lower * eprev) * inv;
+            cs[k * nthr + tid] = c;
+            es[k * nthr + tid] = eprev;
+        }
+    }
+    cp_async_wait<0>();
+    T chg = T(0);
+    if (active) {
+        T x = eprev;
+        int64_t ko = static_cast<int64_t>(a.nk - 1) * g.sz;
+        a.dnew[o0 + ko] = x;
+        if (a.change) { chg = fabs(x - (FIRST ? T(0) : a.dold[o0 + ko])); }
+#pragma unroll 4
+        for (int k = a.nk - 2; k >= 0; --k) {
+            ko -= g.sz;
+            x = es[k * nthr + tid] - cs[k * nthr + tid] * x;
+            a.dnew[o0 + ko] = x;
+            if (a.change) {
+                const T d = fabs(x - (FIRST ? T(0) : a.dold[o0 + ko]));
+                chg = (d > chg || d != d) ? d : chg;
+            }
+        }
+    }
+    if (a.change != nullptr) {
+        chg = warp_max(chg);
+        if ((threadIdx.x & 31) == 0) { atomic_max_nonneg(a.change, chg); }
+    }
+}
+
 //! The two copies of a periodic seam face take the low copy's value.
 template <typename T>
 __global__ void seam_sync_kernel(gb_grid g, int loc, T* __restrict__ f)
@@ -264,9 +383,20 @@ gb_status zline_sweeps(gb_ctx* ctx, const gb_grid& g, int loc, const T* A, const
     const size_t smem = line_smem_bytes<T>(nk);
     if (scratch_kind == LineScratch::automatic) {
         const int v = ctx->tune[GB_TUNE_LINE_VARIANT];
-        scratch_kind = (v == 2) ? LineScratch::shared : (v == 3) ? LineScratch::global : LineScratch::pipelined;
+        scratch_kind = (v == 1)   ? LineScratch::pipelined
+                       : (v == 2) ? LineScratch::shared
+                       : (v == 3) ? LineScratch::global
+                                  : LineScratch::factored;
     }
-    const bool pipelined = (scratch_kind == LineScratch::pipelined);
+    const bool factored = (scratch_kind == LineScratch::factored);
+    const bool pipelined = factored || (scratch_kind == LineScratch::pipelined);
+    T* inv = nullptr;
+    T* cpr = nullptr;
+    if (factored) {
+        inv = static_cast<T*>(scratch(ctx, kSlotLineInv, sizeof(T) * vol));
+        cpr = static_cast<T*>(scratch(ctx, kSlotLineCp, sizeof(T) * vol));
+        if (inv == nullptr || cpr == nullptr) { return GB_OOM; }
+    }
     bool use_smem = (scratch_kind == LineScratch::shared);
     T* cbuf = nullptr;
     T* ebuf = nullptr;
@@ -282,6 +412,8 @@ gb_status zline_sweeps(gb_ctx* ctx, const gb_grid& g, int loc, const T* A, const
         if (!attr_done[ti]) {
             cudaFuncSetAttribute(zline_pipe_kernel<T, true, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
             cudaFuncSetAttribute(zline_pipe_kernel<T, false, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+            cudaFuncSetAttribute(zline_fact_kernel<T, true, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+            cudaFuncSetAttribute(zline_fact_kernel<T, false, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
             attr_done[ti] = true;
         }
     } else if (!use_smem) {
@@ -315,7 +447,16 @@ gb_status zline_sweeps(gb_ctx* ctx, const gb_grid& g, int loc, const T* A, const
         a.first = (s == 0) ? 1 : 0;
         a.change = (s == sweeps - 1) ? change_word : nullptr;
         Span span(ctx, GB_KERNEL_LINE_SWEEP);
-        if (pipelined) {
+        if (factored) {
+            const dim3 block(pipe_thr, 1);
+            const dim3 grid((ni + pipe_thr - 1) / pipe_thr, nj);
+            if (a.first) {
+                zline_fact_kernel<T, true, R><<<grid, block, pipe_smem_first, ctx->stream>>>(a, inv, nullptr, cpr,
+                                                                                           nullptr);
+            } else {
+                zline_fact_kernel<T, false, R><<<grid, block, pipe_smem, ctx->stream>>>(a, nullptr, inv, nullptr, cpr);
+            }
+        } else if (pipelined) {
             const dim3 block(pipe_thr, 1);
             const dim3 grid((ni + pipe_thr - 1) / pipe_thr, nj);
             if (a.first) {

@@ -11,10 +11,12 @@ enum ScratchSlot : int {
     kSlotLineNext = 0,
     kSlotLineC,
     kSlotLineE,
+    kSlotLineInv,  // 1/m of the factored sweeps
+    kSlotLineCp,   // c' of the factored sweeps
     kSlotFirstFree
 };
 
-enum class LineScratch { automatic, pipelined, shared, global };
+enum class LineScratch { automatic, pipelined, shared, global, factored };
 
 //! `sweeps` z-line Jacobi sweeps into delta (which must hold 0 on entry,
 //! ghosts included). change_word (device, may be null) receives the bit

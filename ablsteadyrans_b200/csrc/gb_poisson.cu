@@ -78,106 +78,122 @@ __device__ __forceinline__ bool cell_of(const gb_grid& g, int64_t n, int& i, int
 //! y = A x, or with rhs given y = rhs - A x (the residual).
 template <typename T>
 __global__ void k_apply(gb_grid g, PBC b, const T* __restrict__ x, const T* __restrict__ AX, const T* __restrict__ AY,
-                        const T* __restrict__ AZ, const T* __restrict__ J, const T* __restrict__ z,
+                        const T* __restrict__ AZ, const T* __restrict__ J, MeshRatios<T> m,
                         const T* __restrict__ rhs, T* __restrict__ y)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     const int k = blockIdx.z;
     if (i >= g.nx || j >= g.ny) { return; }
-    const T v = adotx<T>(g, b, i, j, k, x, x, AX, AY, AZ, J, z);
+    const T v = adotx_cell<T>(g, b, i, j, k, x, AX, AY, AZ, J, m);
     const int64_t o = at(g, i, j, k);
     y[o] = rhs ? rhs[o] - v : v;
 }
 
+//! The mesh ratios of one level (MeshRatios) in FP64 from the node heights,
+//! stored as T, on every valid point of each array's location.
+template <typename T>
+__global__ void k_mesh_ratios(gb_grid g, const double* __restrict__ zp, T* __restrict__ rx, T* __restrict__ ry,
+                              T* __restrict__ hz, T* __restrict__ sx, T* __restrict__ sy)
+{
+    const int64_t n = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    const int ni = g.nx + 1, nj = g.ny + 1, nk = g.nz + 1;
+    if (n >= static_cast<int64_t>(ni) * nj * nk) { return; }
+    const int i = static_cast<int>(n % ni);
+    const int j = static_cast<int>((n / ni) % nj);
+    const int k = static_cast<int>(n / (static_cast<int64_t>(ni) * nj));
+    const double dxinv = 1.0 / g.dx, dyinv = 1.0 / g.dy, q = 0.25, h = 0.5;
+    const int64_t o = at(g, i, j, k);
+#define Z(a, bb, c) zp[at(g, a, bb, c)]
+    if (j < g.ny) {  // x-z edge at x-node i, z-node k
+        const double h_xi = q * (Z(i + 1, j, k) - Z(i - 1, j, k) + Z(i + 1, j + 1, k) - Z(i - 1, j + 1, k)) * dxinv;
+        const double h_zeta = q * (Z(i, j, k + 1) - Z(i, j, k - 1) + Z(i, j + 1, k + 1) - Z(i, j + 1, k - 1));
+        rx[o] = static_cast<T>(h_xi / h_zeta);
+    }
+    if (i < g.nx) {  // y-z edge at y-node j, z-node k
+        const double h_eta = q * (Z(i, j + 1, k) - Z(i, j - 1, k) + Z(i + 1, j + 1, k) - Z(i + 1, j - 1, k)) * dyinv;
+        const double h_zeta = q * (Z(i, j, k + 1) - Z(i, j, k - 1) + Z(i + 1, j, k + 1) - Z(i + 1, j, k - 1));
+        ry[o] = static_cast<T>(h_eta / h_zeta);
+    }
+    if (i < g.nx && j < g.ny) {  // z-face k
+        hz[o] = static_cast<T>(8.0 / ((Z(i, j, k + 1) + Z(i + 1, j, k + 1) + Z(i, j + 1, k + 1) + Z(i + 1, j + 1, k + 1))
+                                      - (Z(i, j, k - 1) + Z(i + 1, j, k - 1) + Z(i, j + 1, k - 1) + Z(i + 1, j + 1, k - 1))));
+        sx[o] = static_cast<T>(h * (Z(i + 1, j + 1, k) + Z(i + 1, j, k) - Z(i, j + 1, k) - Z(i, j, k)) * dxinv);
+        sy[o] = static_cast<T>(h * (Z(i + 1, j + 1, k) + Z(i, j + 1, k) - Z(i + 1, j, k) - Z(i, j, k)) * dyinv);
+    }
+#undef Z
+}
+
 // ---------------------------------------------------------------- fluxes ---
 
+//! The face fluxes -grad phi of the terrain operator at x-face (i, j, k),
+//! y-face and z-face (ERF_TerrainPoisson_3D_K.H:22-275), with the mesh
+//! ratios precomputed (MeshRatios) in place of their inline divisions.
 template <typename T>
-__device__ __forceinline__ T flux_x(const gb_grid& g, const PBC& b, int i, int j, int k, const T* x, const T* zp)
+__device__ __forceinline__ T flux_x_r(const gb_grid& g, const PBC& b, int i, int j, int k, const T* x,
+                                      const MeshRatios<T>& m)
 {
-    const T dxinv = static_cast<T>(1.0 / g.dx), h = T(0.5), q = T(0.25);
+    const T dxinv = static_cast<T>(1.0 / g.dx), h = T(0.5);
+    const int64_t o = at(g, i, j, k);
 #define X(a, bb, c) ldc<T>(x, x, g, b, a, bb, c)
-#define Z(a, bb, c) zp[at(g, a, bb, c)]
     T px_lo = (X(i, j, k) - X(i - 1, j, k)) * dxinv;
     T pz_lo_md_hi = h * (X(i, j, k + 1) + X(i - 1, j, k + 1) - X(i, j, k) - X(i - 1, j, k));
-    T h_xi = q * (Z(i + 1, j, k + 1) - Z(i - 1, j, k + 1) + Z(i + 1, j + 1, k + 1) - Z(i - 1, j + 1, k + 1)) * dxinv;
-    T h_zeta = q * (Z(i, j, k + 2) - Z(i, j, k) + Z(i, j + 1, k + 2) - Z(i, j + 1, k));
-    pz_lo_md_hi *= h_xi / h_zeta;
+    pz_lo_md_hi *= m.rx[o + g.sz];
     T pz_lo_md_lo = h * (X(i, j, k) + X(i - 1, j, k) - X(i, j, k - 1) - X(i - 1, j, k - 1));
-    h_xi = q * (Z(i + 1, j, k) - Z(i - 1, j, k) + Z(i + 1, j + 1, k) - Z(i - 1, j + 1, k)) * dxinv;
-    h_zeta = q * (Z(i, j, k + 1) - Z(i, j, k - 1) + Z(i, j + 1, k + 1) - Z(i, j + 1, k - 1));
-    pz_lo_md_lo *= h_xi / h_zeta;
+    pz_lo_md_lo *= m.rx[o];
     px_lo -= h * (pz_lo_md_hi + pz_lo_md_lo);
     return -px_lo;
 #undef X
-#undef Z
 }
 
 template <typename T>
-__device__ __forceinline__ T flux_y(const gb_grid& g, const PBC& b, int i, int j, int k, const T* x, const T* zp)
+__device__ __forceinline__ T flux_y_r(const gb_grid& g, const PBC& b, int i, int j, int k, const T* x,
+                                      const MeshRatios<T>& m)
 {
-    const T dyinv = static_cast<T>(1.0 / g.dy), h = T(0.5), q = T(0.25);
+    const T dyinv = static_cast<T>(1.0 / g.dy), h = T(0.5);
+    const int64_t o = at(g, i, j, k);
 #define X(a, bb, c) ldc<T>(x, x, g, b, a, bb, c)
-#define Z(a, bb, c) zp[at(g, a, bb, c)]
     T py_lo = (X(i, j, k) - X(i, j - 1, k)) * dyinv;
     T pz_md_lo_hi = h * (X(i, j, k + 1) + X(i, j - 1, k + 1) - X(i, j, k) - X(i, j - 1, k));
-    T h_eta = q * (Z(i, j + 1, k + 1) - Z(i, j - 1, k + 1) + Z(i + 1, j + 1, k + 1) - Z(i + 1, j - 1, k + 1)) * dyinv;
-    T h_zeta = q * (Z(i, j, k + 2) - Z(i, j, k) + Z(i + 1, j, k + 2) - Z(i + 1, j, k));
-    pz_md_lo_hi *= h_eta / h_zeta;
+    pz_md_lo_hi *= m.ry[o + g.sz];
     T pz_md_lo_lo = h * (X(i, j, k) + X(i, j - 1, k) - X(i, j, k - 1) - X(i, j - 1, k - 1));
-    h_eta = q * (Z(i, j + 1, k) - Z(i, j - 1, k) + Z(i + 1, j + 1, k) - Z(i + 1, j - 1, k)) * dyinv;
-    h_zeta = q * (Z(i, j, k + 1) - Z(i, j, k - 1) + Z(i + 1, j, k + 1) - Z(i + 1, j, k - 1));
-    pz_md_lo_lo *= h_eta / h_zeta;
+    pz_md_lo_lo *= m.ry[o];
     py_lo -= h * (pz_md_lo_hi + pz_md_lo_lo);
     return -py_lo;
 #undef X
-#undef Z
 }
 
 template <typename T>
-__device__ __forceinline__ T flux_z(const gb_grid& g, const PBC& b, int i, int j, int k, const T* x, const T* zp)
+__device__ __forceinline__ T flux_z_r(const gb_grid& g, const PBC& b, int i, int j, int k, const T* x,
+                                      const MeshRatios<T>& m)
 {
-    const T dxinv = static_cast<T>(1.0 / g.dx), dyinv = static_cast<T>(1.0 / g.dy), h = T(0.5), q = T(0.25);
+    const T dxinv = static_cast<T>(1.0 / g.dx), dyinv = static_cast<T>(1.0 / g.dy), h = T(0.5);
+    const int64_t o = at(g, i, j, k);
 #define X(a, bb, c) ldc<T>(x, x, g, b, a, bb, c)
-#define Z(a, bb, c) zp[at(g, a, bb, c)]
-    T h_xi, h_eta, h_zeta;
     T pz_lo = X(i, j, k) - X(i, j, k - 1);
-    const T hzi = T(8) / ((Z(i, j, k + 1) + Z(i + 1, j, k + 1) + Z(i, j + 1, k + 1) + Z(i + 1, j + 1, k + 1))
-                          - (Z(i, j, k - 1) + Z(i + 1, j, k - 1) + Z(i, j + 1, k - 1) + Z(i + 1, j + 1, k - 1)));
-    pz_lo *= hzi;
+    pz_lo *= m.hz[o];
     const T px_hi_md_lo = h * (X(i + 1, j, k) - X(i, j, k) + X(i + 1, j, k - 1) - X(i, j, k - 1)) * dxinv;
     const T px_lo_md_lo = h * (X(i, j, k) - X(i - 1, j, k) + X(i, j, k - 1) - X(i - 1, j, k - 1)) * dxinv;
     const T py_md_hi_lo = h * (X(i, j + 1, k) - X(i, j, k) + X(i, j + 1, k - 1) - X(i, j, k - 1)) * dyinv;
     const T py_md_lo_lo = h * (X(i, j, k) - X(i, j - 1, k) + X(i, j, k - 1) - X(i, j - 1, k - 1)) * dyinv;
     T pz_hi_md_lo = h * (X(i + 1, j, k) + X(i, j, k) - X(i + 1, j, k - 1) - X(i, j, k - 1));
-    h_xi = q * (Z(i + 2, j, k) - Z(i, j, k) + Z(i + 2, j + 1, k) - Z(i, j + 1, k)) * dxinv;
-    h_zeta = q * (Z(i + 1, j, k + 1) - Z(i + 1, j, k - 1) + Z(i + 1, j + 1, k + 1) - Z(i + 1, j + 1, k - 1));
-    pz_hi_md_lo *= h_xi / h_zeta;
+    pz_hi_md_lo *= m.rx[o + 1];
     T pz_lo_md_lo = h * (X(i, j, k) + X(i - 1, j, k) - X(i, j, k - 1) - X(i - 1, j, k - 1));
-    h_xi = q * (Z(i + 1, j, k) - Z(i - 1, j, k) + Z(i + 1, j + 1, k) - Z(i - 1, j + 1, k)) * dxinv;
-    h_zeta = q * (Z(i, j, k + 1) - Z(i, j, k - 1) + Z(i, j + 1, k + 1) - Z(i, j + 1, k - 1));
-    pz_lo_md_lo *= h_xi / h_zeta;
+    pz_lo_md_lo *= m.rx[o];
     T pz_md_hi_lo = h * (X(i, j + 1, k) + X(i, j, k) - X(i, j + 1, k - 1) - X(i, j, k - 1));
-    h_eta = q * (Z(i, j + 2, k) - Z(i, j, k) + Z(i + 1, j + 2, k) - Z(i + 1, j, k)) * dyinv;
-    h_zeta = q * (Z(i, j + 1, k + 1) - Z(i, j + 1, k - 1) + Z(i + 1, j + 1, k + 1) - Z(i + 1, j + 1, k - 1));
-    pz_md_hi_lo *= h_eta / h_zeta;
+    pz_md_hi_lo *= m.ry[o + g.sy];
     T pz_md_lo_lo = h * (X(i, j, k) + X(i, j - 1, k) - X(i, j, k - 1) - X(i, j - 1, k - 1));
-    h_eta = q * (Z(i, j + 1, k) - Z(i, j - 1, k) + Z(i + 1, j + 1, k) - Z(i + 1, j - 1, k)) * dyinv;
-    h_zeta = q * (Z(i, j, k + 1) - Z(i, j, k - 1) + Z(i + 1, j, k + 1) - Z(i + 1, j, k - 1));
-    pz_md_lo_lo *= h_eta / h_zeta;
-    const T h_xi_on_zlo = h * (Z(i + 1, j + 1, k) + Z(i + 1, j, k) - Z(i, j + 1, k) - Z(i, j, k)) * dxinv;
-    const T h_eta_on_zlo = h * (Z(i + 1, j + 1, k) + Z(i, j + 1, k) - Z(i + 1, j, k) - Z(i, j, k)) * dyinv;
-    pz_lo -= h * h_xi_on_zlo * ((px_hi_md_lo + px_lo_md_lo) - (pz_hi_md_lo + pz_lo_md_lo));
-    pz_lo -= h * h_eta_on_zlo * ((py_md_hi_lo + py_md_lo_lo) - (pz_md_hi_lo + pz_md_lo_lo));
+    pz_md_lo_lo *= m.ry[o];
+    pz_lo -= h * m.sx[o] * ((px_hi_md_lo + px_lo_md_lo) - (pz_hi_md_lo + pz_lo_md_lo));
+    pz_lo -= h * m.sy[o] * ((py_md_hi_lo + py_md_lo_lo) - (pz_md_hi_lo + pz_md_lo_lo));
     if (k == 0) { pz_lo = T(0); }
     return -pz_lo;
 #undef X
-#undef Z
 }
 
 //! The face fluxes -grad phi with the zero-flux faces masked, times beta
 //! (null: 1). One thread per node column (i, j) slot and level k.
-__global__ void k_fluxes(gb_grid g, PBC b, const double* __restrict__ phi, const double* __restrict__ z,
+__global__ void k_fluxes(gb_grid g, PBC b, const double* __restrict__ phi, MeshRatios<double> m,
                          const double* __restrict__ bx, const double* __restrict__ by, const double* __restrict__ bz,
                          double* __restrict__ fx, double* __restrict__ fy, double* __restrict__ fz)
 {
@@ -186,19 +202,19 @@ __global__ void k_fluxes(gb_grid g, PBC b, const double* __restrict__ phi, const
     const int k = blockIdx.z;
     if (i > g.nx || j > g.ny) { return; }
     if (j < g.ny && k < g.nz) {
-        double f = flux_x<double>(g, b, i, j, k, phi, z);
+        double f = flux_x_r<double>(g, b, i, j, k, phi, m);
         if (((b.zf & TP_XLO) && i == 0) || ((b.zf & TP_XHI) && i == g.nx)) { f = 0; }
         const int64_t o = at(g, i, j, k);
         fx[o] = bx ? f * bx[o] : f;
     }
     if (i < g.nx && k < g.nz) {
-        double f = flux_y<double>(g, b, i, j, k, phi, z);
+        double f = flux_y_r<double>(g, b, i, j, k, phi, m);
         if (((b.zf & TP_YLO) && j == 0) || ((b.zf & TP_YHI) && j == g.ny)) { f = 0; }
         const int64_t o = at(g, i, j, k);
         fy[o] = by ? f * by[o] : f;
     }
     if (i < g.nx && j < g.ny) {
-        double f = flux_z<double>(g, b, i, j, k, phi, z);
+        double f = flux_z_r<double>(g, b, i, j, k, phi, m);
         if ((b.zf & TP_ZHI) && k == g.nz) { f = 0; }
         const int64_t o = at(g, i, j, k);
         fz[o] = bz ? f * bz[o] : f;
@@ -286,19 +302,60 @@ __global__ void k_line_tridiag(gb_grid g, PBC b, const T* __restrict__ AX, const
 template <typename T>
 __global__ void k_color_residual(gb_grid g, PBC b, int color, const T* __restrict__ x, const T* __restrict__ bv,
                                  const T* __restrict__ AX, const T* __restrict__ AY, const T* __restrict__ AZ,
-                                 const T* __restrict__ J, const T* __restrict__ z, T* __restrict__ r)
+                                 const T* __restrict__ J, MeshRatios<T> m, T* __restrict__ r)
 {
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     const int i = 2 * (blockIdx.x * blockDim.x + threadIdx.x) + ((j + color) & 1);
     const int k = blockIdx.z;
     if (i >= g.nx || j >= g.ny) { return; }
     const int64_t o = at(g, i, j, k);
-    r[o] = bv[o] - adotx<T>(g, b, i, j, k, x, x, AX, AY, AZ, J, z);
+    r[o] = bv[o] - adotx_cell<T>(g, b, i, j, k, x, AX, AY, AZ, J, m);
+}
+
+//! The LU factors of every column's line tridiagonal T, once per coefficient
+//! set (T does not change between relaxations): in place of C and U the
+//! reciprocal pivots 1/m_k and the eliminated uppers c'_k = U_k / m_k, with
+//! m_0 = C_0, m_k = C_k - D_k c'_{k-1} (D, the lower diagonal, is kept). One
+//! thread per column; the loads of 8 levels are batched ahead of the chain.
+template <typename T>
+__global__ void k_line_factor(gb_grid g, T* __restrict__ TD, T* __restrict__ TC, T* __restrict__ TU)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i >= g.nx || j >= g.ny) { return; }
+    const int64_t o0 = at(g, i, j, 0);
+    T cp = T(0);
+    for (int k0 = 0; k0 < g.nz; k0 += 8) {
+        T D[8], C[8], U[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            if (k0 + q < g.nz) {
+                const int64_t o = o0 + static_cast<int64_t>(k0 + q) * g.sz;
+                D[q] = TD[o];
+                C[q] = TC[o];
+                U[q] = TU[o];
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const int k = k0 + q;
+            if (k < g.nz) {
+                const T m = (k == 0) ? C[q] : C[q] - D[q] * cp;
+                const T im = T(1) / m;
+                cp = U[q] * im;
+                const int64_t o = o0 + static_cast<int64_t>(k) * g.sz;
+                TC[o] = im;
+                TU[o] = cp;
+            }
+        }
+    }
 }
 
 //! Zebra relaxation, second half: on every column of the colour x += T^{-1} r
-//! by the Thomas recurrences, the column's r, D, C, U staged R levels ahead
-//! into shared memory with asynchronous copies (c', e' in shared memory).
+//! with the factors of k_line_factor (e_k = (r_k - D_k e_{k-1}) / m_k, then
+//! x_k = e_k - c'_k x_{k+1}), the column's r, D, 1/m, c' staged R levels ahead
+//! into shared memory with asynchronous copies (c', e' kept in shared memory).
+//! Used when a whole column does not fit the staged kernel below.
 template <typename T, int R>
 __global__ void __launch_bounds__(64) k_color_solve(gb_grid g, int color, const T* __restrict__ r,
                                                     const T* __restrict__ TD, const T* __restrict__ TC,
@@ -327,17 +384,15 @@ __global__ void __launch_bounds__(64) k_color_solve(gb_grid g, int color, const 
     };
 #pragma unroll
     for (int k = 0; k < R - 1; ++k) { issue(k); }
-    T cp = T(0), ep = T(0);
+    T ep = T(0);
     for (int k = 0; k < g.nz; ++k) {
         issue(k + R - 1);
         cp_async_wait<R - 1>();
         if (active) {
             const T* s = ring + (k % R) * 4 * nthr + tid;
-            const T rk = s[0], D = s[nthr], C = s[2 * nthr], U = s[3 * nthr];
-            const T m = (k == 0) ? C : C - D * cp;
-            cp = U / m;
-            ep = ((k == 0) ? rk : rk - D * ep) / m;
-            cs[k * nthr + tid] = cp;
+            const T rk = s[0], D = s[nthr], im = s[2 * nthr];
+            ep = ((k == 0) ? rk : rk - D * ep) * im;
+            cs[k * nthr + tid] = s[3 * nthr];
             es[k * nthr + tid] = ep;
         }
     }
@@ -353,6 +408,85 @@ __global__ void __launch_bounds__(64) k_color_solve(gb_grid g, int color, const 
     }
 }
 
+//! The same relaxation with the whole column staged at once: every level's r,
+//! D, 1/m, c' and x goes into shared memory ([array][k][thread]) in one burst
+//! of asynchronous copies, so the column's memory latency is paid once and the
+//! two recurrences then run from shared memory without a division; e
+//! overwrites r in place and x is written back once per level.
+template <typename T>
+__global__ void __launch_bounds__(32) k_color_solve_staged(gb_grid g, int color, const T* __restrict__ r,
+                                                           const T* __restrict__ TD, const T* __restrict__ TC,
+                                                           const T* __restrict__ TU, T* __restrict__ x)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int tid = threadIdx.x;
+    const int nthr = blockDim.x;
+    const int j = blockIdx.y;
+    const int i = 2 * (blockIdx.x * blockDim.x + threadIdx.x) + ((j + color) & 1);
+    if (i >= g.nx) { return; }  // no block barrier below: each thread owns its column
+    const int nz = g.nz;
+    const int64_t plane = static_cast<int64_t>(nz) * nthr;
+    T* sr = reinterpret_cast<T*>(smem_raw) + tid;
+    T* sd = sr + plane;
+    T* sm = sd + plane;
+    T* sc = sm + plane;
+    T* sx = sc + plane;
+    const int64_t o0 = at(g, i, j, 0);
+    for (int k = 0; k < nz; ++k) {
+        const int64_t o = o0 + static_cast<int64_t>(k) * g.sz;
+        const int s = k * nthr;
+        cp_async_elem(sr + s, r + o);
+        cp_async_elem(sd + s, TD + o);
+        cp_async_elem(sm + s, TC + o);
+        cp_async_elem(sc + s, TU + o);
+        cp_async_elem(sx + s, x + o);
+    }
+    cp_async_commit();
+    cp_async_wait<0>();
+    T ep = sr[0] * sm[0];
+    sr[0] = ep;
+    for (int k = 1; k < nz; ++k) {
+        const int s = k * nthr;
+        ep = (sr[s] - sd[s] * ep) * sm[s];
+        sr[s] = ep;
+    }
+    T xk = ep;
+    int64_t o = o0 + static_cast<int64_t>(nz - 1) * g.sz;
+    x[o] = sx[(nz - 1) * nthr] + xk;
+    for (int k = nz - 2; k >= 0; --k) {
+        const int s = k * nthr;
+        o -= g.sz;
+        xk = sr[s] - sc[s] * xk;
+        x[o] = sx[s] + xk;
+    }
+}
+
+//! Coarse right-hand side at coarse cell (I, J2, k): the J-weighted sum of
+//! the four fine residuals over 4 J_c (a coarse cell's flux balance is the sum
+//! of its fine cells').
+template <typename T>
+__device__ __forceinline__ void restrict_cell(const gb_grid& gf, const T* Jf, const T* rf, const gb_grid& gc,
+                                              const T* Jc, T* bc, int I, int J2, int k)
+{
+    const int i = 2 * I, j = 2 * J2;
+    const T s = (Jf[at(gf, i, j, k)] * rf[at(gf, i, j, k)] + Jf[at(gf, i + 1, j, k)] * rf[at(gf, i + 1, j, k)])
+              + (Jf[at(gf, i, j + 1, k)] * rf[at(gf, i, j + 1, k)] + Jf[at(gf, i + 1, j + 1, k)] * rf[at(gf, i + 1, j + 1, k)]);
+    bc[at(gc, I, J2, k)] = s / (T(4) * Jc[at(gc, I, J2, k)]);
+}
+
+//! Fine correction at fine cell (i, j, k): bilinear in x-y from the coarse
+//! cell centres (weights 9, 3, 3, 1 over 16), coarse ghosts from the BC.
+template <typename T>
+__device__ __forceinline__ void prolong_cell(const gb_grid& gc, const PBC& bcb, const T* xc, const gb_grid& gf,
+                                             T* xf, int i, int j, int k)
+{
+    const int I = i >> 1, J2 = j >> 1;
+    const int si = (i & 1) ? 1 : -1, sj = (j & 1) ? 1 : -1;
+    const T v = (T(9) * ldc<T>(xc, xc, gc, bcb, I, J2, k) + T(3) * ldc<T>(xc, xc, gc, bcb, I + si, J2, k))
+              + (T(3) * ldc<T>(xc, xc, gc, bcb, I, J2 + sj, k) + T(1) * ldc<T>(xc, xc, gc, bcb, I + si, J2 + sj, k));
+    xf[at(gf, i, j, k)] += v * T(0.0625);
+}
+
 template <typename T>
 __global__ void k_restrict(gb_grid gf, const T* __restrict__ Jf, const T* __restrict__ rf, gb_grid gc,
                            const T* __restrict__ Jc, T* __restrict__ bc)
@@ -361,10 +495,7 @@ __global__ void k_restrict(gb_grid gf, const T* __restrict__ Jf, const T* __rest
     const int J2 = blockIdx.y * blockDim.y + threadIdx.y;
     const int k = blockIdx.z;
     if (I >= gc.nx || J2 >= gc.ny) { return; }
-    const int i = 2 * I, j = 2 * J2;
-    const T s = (Jf[at(gf, i, j, k)] * rf[at(gf, i, j, k)] + Jf[at(gf, i + 1, j, k)] * rf[at(gf, i + 1, j, k)])
-              + (Jf[at(gf, i, j + 1, k)] * rf[at(gf, i, j + 1, k)] + Jf[at(gf, i + 1, j + 1, k)] * rf[at(gf, i + 1, j + 1, k)]);
-    bc[at(gc, I, J2, k)] = s / (T(4) * Jc[at(gc, I, J2, k)]);
+    restrict_cell<T>(gf, Jf, rf, gc, Jc, bc, I, J2, k);
 }
 
 template <typename T>
@@ -374,11 +505,81 @@ __global__ void k_prolong_add(gb_grid gc, PBC bcb, const T* __restrict__ xc, gb_
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     const int k = blockIdx.z;
     if (i >= gf.nx || j >= gf.ny) { return; }
-    const int I = i >> 1, J2 = j >> 1;
-    const int si = (i & 1) ? 1 : -1, sj = (j & 1) ? 1 : -1;
-    const T v = (T(9) * ldc<T>(xc, xc, gc, bcb, I, J2, k) + T(3) * ldc<T>(xc, xc, gc, bcb, I + si, J2, k))
-              + (T(3) * ldc<T>(xc, xc, gc, bcb, I, J2 + sj, k) + T(1) * ldc<T>(xc, xc, gc, bcb, I + si, J2 + sj, k));
-    xf[at(gf, i, j, k)] += v * T(0.0625);
+    prolong_cell<T>(gc, bcb, xc, gf, xf, i, j, k);
+}
+
+//! All relaxations of the coarsest level in ONE block. On a level of a few
+//! columns every launch is latency, and the coarsest level takes nu_coarse
+//! relaxations: here the columns' line factors stay in shared memory for the
+//! whole kernel, each colour's residual goes to shared memory, and block
+//! barriers separate the phases. Operations and order are those of the
+//! per-level kernels (colour residual, then the factored Thomas solve).
+//! Shared memory: [k][column] arrays D, 1/m, c', r and x (5 * ncols * nz).
+template <typename T>
+__global__ void __launch_bounds__(256) k_coarse_relax(gb_grid g, PBC b, int nrelax, T* x, const T* __restrict__ bv,
+                                                      const T* __restrict__ AX, const T* __restrict__ AY,
+                                                      const T* __restrict__ AZ, const T* __restrict__ J,
+                                                      MeshRatios<T> m, const T* __restrict__ TD,
+                                                      const T* __restrict__ TC, const T* __restrict__ TU)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int ncols = g.nx * g.ny, nz = g.nz;
+    const int plane = ncols * nz;
+    T* sd = reinterpret_cast<T*>(smem_raw);
+    T* sm = sd + plane;
+    T* sc = sm + plane;
+    T* sr = sc + plane;
+    T* sx = sr + plane;
+    for (int n = threadIdx.x; n < plane; n += blockDim.x) {
+        const int col = n % ncols, k = n / ncols;
+        const int64_t o = at(g, col % g.nx, col / g.nx, k);
+        cp_async_elem(sd + n, TD + o);
+        cp_async_elem(sm + n, TC + o);
+        cp_async_elem(sc + n, TU + o);
+    }
+    cp_async_commit();
+    cp_async_wait<0>();
+    __syncthreads();
+    const int half = (g.nx + 1) / 2;
+    for (int s = 0; s < nrelax; ++s) {
+        for (int color = 0; color < 2; ++color) {
+            const int ccols = half * g.ny;  // columns of the colour (some past nx when nx is odd)
+            for (int n = threadIdx.x; n < ccols * nz; n += blockDim.x) {
+                const int cc = n % ccols, k = n / ccols;
+                const int j = cc / half;
+                const int i = 2 * (cc % half) + ((j + color) & 1);
+                if (i >= g.nx) { continue; }
+                const int64_t o = at(g, i, j, k);
+                const int q = k * ncols + j * g.nx + i;
+                sx[q] = x[o];
+                sr[q] = bv[o] - adotx_cell<T>(g, b, i, j, k, x, AX, AY, AZ, J, m);
+            }
+            __syncthreads();
+            for (int cc = threadIdx.x; cc < ccols; cc += blockDim.x) {
+                const int j = cc / half;
+                const int i = 2 * (cc % half) + ((j + color) & 1);
+                if (i >= g.nx) { continue; }
+                const int col = j * g.nx + i;
+                T ep = sr[col] * sm[col];
+                sr[col] = ep;
+                for (int k = 1; k < nz; ++k) {
+                    const int q = k * ncols + col;
+                    ep = (sr[q] - sd[q] * ep) * sm[q];
+                    sr[q] = ep;
+                }
+                T xk = ep;
+                int64_t o = at(g, i, j, nz - 1);
+                x[o] = sx[(nz - 1) * ncols + col] + xk;
+                for (int k = nz - 2; k >= 0; --k) {
+                    const int q = k * ncols + col;
+                    o -= g.sz;
+                    xk = sr[q] - sc[q] * xk;
+                    x[o] = sx[q] + xk;
+                }
+            }
+            __syncthreads();
+        }
+    }
 }
 
 // --------------------------------------------------------- vector ops ---
@@ -546,6 +747,9 @@ namespace gb {
 
 namespace {
 
+//! Largest dynamic shared memory a relaxation kernel asks for.
+constexpr size_t kSmoothSmemMax = 200 * 1024;
+
 template <typename T>
 void mg_smooth(gb_poisson* P, PoissonLevels<T>& L, int l)
 {
@@ -554,11 +758,14 @@ void mg_smooth(gb_poisson* P, PoissonLevels<T>& L, int l)
     const PBC& b = L.b[l];
     constexpr int R = 4;
     const int nthr = 32;
-    const size_t smem = static_cast<size_t>(R * 4 + 2 * g.nz) * nthr * sizeof(T);
+    const size_t smem_ring = static_cast<size_t>(R * 4 + 2 * g.nz) * nthr * sizeof(T);
+    const size_t smem_staged = static_cast<size_t>(5) * g.nz * nthr * sizeof(T);
+    const bool staged = smem_staged <= kSmoothSmemMax;
     static bool attr_done[2] = {false, false};
     const int ti = sizeof(T) == 8 ? 1 : 0;
     if (!attr_done[ti]) {
-        cudaFuncSetAttribute(k_color_solve<T, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        cudaFuncSetAttribute(k_color_solve<T, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmoothSmemMax);
+        cudaFuncSetAttribute(k_color_solve_staged<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmoothSmemMax);
         attr_done[ti] = true;
     }
     const int half = (g.nx + 1) / 2;
@@ -566,9 +773,15 @@ void mg_smooth(gb_poisson* P, PoissonLevels<T>& L, int l)
         Span span(ctx, GB_KERNEL_MG_SMOOTH);
         const dim3 rgrid((half + 31) / 32, (g.ny + 3) / 4, g.nz);
         k_color_residual<T><<<rgrid, dim3(32, 4), 0, ctx->stream>>>(g, b, color, L.x[l], L.bv[l], L.AX[l], L.AY[l],
-                                                                   L.AZ[l], L.J[l], L.z[l], L.r[l]);
+                                                                   L.AZ[l], L.J[l], L.ratios(l), L.r[l]);
         const dim3 sgrid((half + nthr - 1) / nthr, g.ny);
-        k_color_solve<T, R><<<sgrid, nthr, smem, ctx->stream>>>(g, color, L.r[l], L.TD[l], L.TC[l], L.TU[l], L.x[l]);
+        if (staged) {
+            k_color_solve_staged<T><<<sgrid, nthr, smem_staged, ctx->stream>>>(g, color, L.r[l], L.TD[l], L.TC[l],
+                                                                              L.TU[l], L.x[l]);
+        } else {
+            k_color_solve<T, R><<<sgrid, nthr, smem_ring, ctx->stream>>>(g, color, L.r[l], L.TD[l], L.TC[l], L.TU[l],
+                                                                         L.x[l]);
+        }
         ctx->launches += 2;
     }
 }
@@ -581,7 +794,8 @@ void build_line_tridiag(gb_poisson* P, PoissonLevels<T>& L)
         const gb_grid& g = L.g[l];
         k_line_tridiag<T><<<cols_grid(g, g.nz), kColsBlock, 0, ctx->stream>>>(g, L.b[l], L.AX[l], L.AY[l], L.AZ[l],
                                                                               L.J[l], L.z[l], L.TD[l], L.TC[l], L.TU[l]);
-        ++ctx->launches;
+        k_line_factor<T><<<cols_grid(g, 1), kColsBlock, 0, ctx->stream>>>(g, L.TD[l], L.TC[l], L.TU[l]);
+        ctx->launches += 2;
     }
 }
 
@@ -592,7 +806,7 @@ void mg_residual(gb_poisson* P, PoissonLevels<T>& L, int l)
     const gb_grid& g = L.g[l];
     Span span(ctx, GB_KERNEL_POISSON_APPLY);
     k_apply<T><<<cols_grid(g, g.nz), kColsBlock, 0, ctx->stream>>>(g, L.b[l], L.x[l], L.AX[l], L.AY[l], L.AZ[l],
-                                                                   L.J[l], L.z[l], L.bv[l], L.r[l]);
+                                                                   L.J[l], L.ratios(l), L.bv[l], L.r[l]);
     ++ctx->launches;
 }
 
@@ -601,6 +815,24 @@ void vcycle(gb_poisson* P, PoissonLevels<T>& L, int l)
 {
     gb_ctx* ctx = P->ctx;
     if (l == P->nlev - 1) {
+        const gb_grid& g = L.g[l];
+        const size_t smem = static_cast<size_t>(5) * g.nx * g.ny * g.nz * sizeof(T);
+        const bool one_block = ctx->tune[GB_TUNE_MG_COARSE_KERNEL] != 1 && g.nx * g.ny <= 64 && smem <= kSmoothSmemMax
+                               && !(g.periodic_x && (g.nx & 1)) && !(g.periodic_y && (g.ny & 1));
+        if (one_block && P->opt.nu_coarse > 0) {
+            static bool attr_done[2] = {false, false};
+            const int ti = sizeof(T) == 8 ? 1 : 0;
+            if (!attr_done[ti]) {
+                cudaFuncSetAttribute(k_coarse_relax<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmoothSmemMax);
+                attr_done[ti] = true;
+            }
+            Span span(ctx, GB_KERNEL_MG_SMOOTH);
+            k_coarse_relax<T><<<1, 256, smem, ctx->stream>>>(g, L.b[l], P->opt.nu_coarse, L.x[l], L.bv[l], L.AX[l],
+                                                             L.AY[l], L.AZ[l], L.J[l], L.ratios(l), L.TD[l], L.TC[l],
+                                                             L.TU[l]);
+            ++ctx->launches;
+            return;
+        }
         for (int s = 0; s < P->opt.nu_coarse; ++s) { mg_smooth(P, L, l); }
         return;
     }
@@ -654,7 +886,7 @@ void apply_fine(gb_poisson* P, const double* x, const double* rhs, double* y)
     const gb_grid& g = P->g;
     Span span(ctx, GB_KERNEL_POISSON_APPLY);
     k_apply<double><<<cols_grid(g, g.nz), kColsBlock, 0, ctx->stream>>>(g, P->dl.b[0], x, P->dl.AX[0], P->dl.AY[0],
-                                                                        P->dl.AZ[0], P->dl.J[0], P->dl.z[0], rhs, y);
+                                                                        P->dl.AZ[0], P->dl.J[0], P->dl.ratios(0), rhs, y);
     ++ctx->launches;
 }
 
@@ -715,7 +947,12 @@ gb_status poisson_build(gb_poisson* P)
         D.TD[l] = dalloc<double>(D.owned, vol);
         D.TC[l] = dalloc<double>(D.owned, vol);
         D.TU[l] = dalloc<double>(D.owned, vol);
-        if (!D.TD[l] || !D.TC[l] || !D.TU[l]) {
+        D.RX[l] = dalloc<double>(D.owned, vol);
+        D.RY[l] = dalloc<double>(D.owned, vol);
+        D.HZ[l] = dalloc<double>(D.owned, vol);
+        D.SX[l] = dalloc<double>(D.owned, vol);
+        D.SY[l] = dalloc<double>(D.owned, vol);
+        if (!D.TD[l] || !D.TC[l] || !D.TU[l] || !D.RX[l] || !D.RY[l] || !D.HZ[l] || !D.SX[l] || !D.SY[l]) {
             set_error("gust: PoissonSolver: cannot allocate the multigrid levels");
             return GB_OOM;
         }
@@ -734,6 +971,10 @@ gb_status poisson_build(gb_poisson* P)
             k_metrics<<<nblocks(nm), kBlock, 0, ctx->stream>>>(g, D.z[l], D.J[l], ax, ay, zcc);
             ctx->launches += 2;
         }
+        const int64_t nr = static_cast<int64_t>(g.nx + 1) * (g.ny + 1) * (g.nz + 1);
+        k_mesh_ratios<double><<<nblocks(nr), kBlock, 0, ctx->stream>>>(g, D.z[l], D.RX[l], D.RY[l], D.HZ[l], D.SX[l],
+                                                                       D.SY[l]);
+        ++ctx->launches;
     }
     if (P->opt.precision == 1) {
         auto& F = P->fl;
@@ -754,10 +995,19 @@ gb_status poisson_build(gb_poisson* P)
             F.TD[l] = dalloc<float>(F.owned, vol);
             F.TC[l] = dalloc<float>(F.owned, vol);
             F.TU[l] = dalloc<float>(F.owned, vol);
-            if (!F.TD[l] || !F.TC[l] || !F.TU[l]) {
+            F.RX[l] = dalloc<float>(F.owned, vol);
+            F.RY[l] = dalloc<float>(F.owned, vol);
+            F.HZ[l] = dalloc<float>(F.owned, vol);
+            F.SX[l] = dalloc<float>(F.owned, vol);
+            F.SY[l] = dalloc<float>(F.owned, vol);
+            if (!F.TD[l] || !F.TC[l] || !F.TU[l] || !F.RX[l] || !F.RY[l] || !F.HZ[l] || !F.SX[l] || !F.SY[l]) {
                 set_error("gust: PoissonSolver: cannot allocate the FP32 multigrid levels");
                 return GB_OOM;
             }
+            const int64_t nr = static_cast<int64_t>(g.nx + 1) * (g.ny + 1) * (g.nz + 1);
+            k_mesh_ratios<float><<<nblocks(nr), kBlock, 0, ctx->stream>>>(g, D.z[l], F.RX[l], F.RY[l], F.HZ[l],
+                                                                          F.SX[l], F.SY[l]);
+            ++ctx->launches;
             if (!F.z[l] || !F.J[l] || !F.AX[l] || !F.AY[l] || !F.AZ[l] || !F.x[l] || !F.bv[l] || !F.r[l] || !F.snap[l]) {
                 set_error("gust: PoissonSolver: cannot allocate the FP32 multigrid levels");
                 return GB_OOM;
@@ -857,7 +1107,7 @@ gb_status poisson_fluxes(gb_poisson* P, const double* phi, const double* bx, con
     gb_ctx* ctx = P->ctx;
     const gb_grid& g = P->g;
     Span span(ctx, GB_KERNEL_POISSON_APPLY);
-    k_fluxes<<<cols_grid(g, g.nz + 1, 1), kColsBlock, 0, ctx->stream>>>(g, P->dl.b[0], phi, P->dl.z[0], bx, by, bz, fx,
+    k_fluxes<<<cols_grid(g, g.nz + 1, 1), kColsBlock, 0, ctx->stream>>>(g, P->dl.b[0], phi, P->dl.ratios(0), bx, by, bz, fx,
                                                                         fy, fz);
     ++ctx->launches;
     return check_cuda("PoissonSolver::fluxes");

@@ -50,7 +50,7 @@ inline PBC make_pbc(const gb_grid& g, const int* bc, bool ground_even)
 //! x(i, j, k) of a cell field with its one ghost layer resolved for the BC.
 //! `wrap` (may equal x) serves the reads that cross a periodic seam.
 template <typename T>
-__device__ __forceinline__ T ldc(const T* __restrict__ x, const T* __restrict__ wrap, const gb_grid& g, const PBC& b,
+__device__ __forceinline__ T ldc(const T* x, const T* wrap, const gb_grid& g, const PBC& b,
                                  int i, int j, int k)
 {
     int s = 1;
@@ -70,99 +70,123 @@ __device__ __forceinline__ T ldc(const T* __restrict__ x, const T* __restrict__ 
     return (s < 0) ? -v : v;
 }
 
-//! The terrain operator at cell (i, j, k): ERF_TerrainPoisson_3D_K.H:316-530
-//! (terrpoisson_adotx) with the premultiplied areas a beta and the zero-flux mask.
+//! The mesh-only factors of the operator, precomputed once per level from the
+//! node heights (they do not depend on the coefficients or the iterate):
+//!   rx(I, j, K) = h_xi / h_zeta on the x-z edge at x-node I, z-node K,
+//!   ry(i, J, K) = h_eta / h_zeta on the y-z edge at y-node J, z-node K,
+//!   hz(i, j, K) = 1 / (h_zeta / 8) on z-face K,
+//!   sx(i, j, K), sy(i, j, K) = the x and y slopes of z-face K,
+//! each the exact expression terrpoisson_adotx evaluates inline
+//! (ERF_TerrainPoisson_3D_K.H:316-530), so the products are unchanged.
 template <typename T>
-__device__ __forceinline__ T adotx(const gb_grid& g, const PBC& b, int i, int j, int k, const T* __restrict__ x,
-                                   const T* __restrict__ wrap, const T* __restrict__ axa, const T* __restrict__ aya,
-                                   const T* __restrict__ aza, const T* __restrict__ Jc, const T* __restrict__ zp)
+struct MeshRatios {
+    const T* __restrict__ rx;
+    const T* __restrict__ ry;
+    const T* __restrict__ hz;
+    const T* __restrict__ sx;
+    const T* __restrict__ sy;
+};
+
+//! One value of the iterate at offset (di, dj, dk) from cell (i, j, k) at
+//! flat index o: a direct load inside, the BC-resolved ghost otherwise.
+template <typename T, bool INTERIOR>
+__device__ __forceinline__ T xoff(const T* x, const gb_grid& g, const PBC& b, int64_t o, int i, int j,
+                                  int k, int di, int dj, int dk)
+{
+    if (INTERIOR) { return x[o + di + dj * g.sy + dk * g.sz]; }
+    return ldc<T>(x, x, g, b, i + di, j + dj, k + dk);
+}
+
+//! The terrain operator at cell (i, j, k): terrpoisson_adotx
+//! (ERF_TerrainPoisson_3D_K.H:316-530) with the premultiplied areas a beta and
+//! the zero-flux mask, the mesh ratios precomputed (MeshRatios): the same
+//! operations in the same order on the same values, without its ~19 divisions
+//! per cell. INTERIOR:
+//! every neighbour read lies in the valid cells (no ghost resolution). x is
+//! not declared restrict: one kernel may update it between applications.
+template <typename T, bool INTERIOR>
+__device__ __forceinline__ T adotx_r(const gb_grid& g, const PBC& b, int i, int j, int k, const T* x,
+                                     const T* __restrict__ axa, const T* __restrict__ aya, const T* __restrict__ aza,
+                                     const T* __restrict__ Jc, const MeshRatios<T>& m)
 {
     const T dxinv = static_cast<T>(1.0 / g.dx), dyinv = static_cast<T>(1.0 / g.dy), dzinv = static_cast<T>(1.0 / g.dzeta);
-    const T h = T(0.5), q = T(0.25);
-#define X(a, bb, c) ldc<T>(x, wrap, g, b, a, bb, c)
-#define Z(a, bb, c) zp[at(g, a, bb, c)]
-    T h_xi, h_eta, h_zeta;
-    T px_hi = (X(i + 1, j, k) - X(i, j, k)) * dxinv;
-    T pz_hi_md_hi = h * (X(i + 1, j, k + 1) + X(i, j, k + 1) - X(i + 1, j, k) - X(i, j, k));
-    h_xi = q * (Z(i + 2, j, k + 1) - Z(i, j, k + 1) + Z(i + 2, j + 1, k + 1) - Z(i, j + 1, k + 1)) * dxinv;
-    h_zeta = q * (Z(i + 1, j, k + 2) - Z(i + 1, j, k) + Z(i + 1, j + 1, k + 2) - Z(i + 1, j + 1, k));
-    pz_hi_md_hi *= h_xi / h_zeta;
-    T pz_hi_md_lo = h * (X(i + 1, j, k) + X(i, j, k) - X(i + 1, j, k - 1) - X(i, j, k - 1));
-    h_xi = q * (Z(i + 2, j, k) - Z(i, j, k) + Z(i + 2, j + 1, k) - Z(i, j + 1, k)) * dxinv;
-    h_zeta = q * (Z(i + 1, j, k + 1) - Z(i + 1, j, k - 1) + Z(i + 1, j + 1, k + 1) - Z(i + 1, j + 1, k - 1));
-    pz_hi_md_lo *= h_xi / h_zeta;
+    const T h = T(0.5);
+    const int64_t o = at(g, i, j, k);
+#define X(di, dj, dk) xoff<T, INTERIOR>(x, g, b, o, i, j, k, di, dj, dk)
+    const T x000 = X(0, 0, 0), xp00 = X(1, 0, 0), xm00 = X(-1, 0, 0), x0p0 = X(0, 1, 0), x0m0 = X(0, -1, 0);
+    const T x00p = X(0, 0, 1), x00m = X(0, 0, -1);
+    const T xp0p = X(1, 0, 1), xp0m = X(1, 0, -1), xm0p = X(-1, 0, 1), xm0m = X(-1, 0, -1);
+    const T x0pp = X(0, 1, 1), x0pm = X(0, 1, -1), x0mp = X(0, -1, 1), x0mm = X(0, -1, -1);
+#undef X
+    const int64_t sy = g.sy, sz = g.sz;
+    T px_hi = (xp00 - x000) * dxinv;
+    T pz_hi_md_hi = h * (xp0p + x00p - xp00 - x000);
+    pz_hi_md_hi *= m.rx[o + 1 + sz];
+    T pz_hi_md_lo = h * (xp00 + x000 - xp0m - x00m);
+    pz_hi_md_lo *= m.rx[o + 1];
     px_hi -= h * (pz_hi_md_hi + pz_hi_md_lo);
 
-    T px_lo = (X(i, j, k) - X(i - 1, j, k)) * dxinv;
-    T pz_lo_md_hi = h * (X(i, j, k + 1) + X(i - 1, j, k + 1) - X(i, j, k) - X(i - 1, j, k));
-    h_xi = q * (Z(i + 1, j, k + 1) - Z(i - 1, j, k + 1) + Z(i + 1, j + 1, k + 1) - Z(i - 1, j + 1, k + 1)) * dxinv;
-    h_zeta = q * (Z(i, j, k + 2) - Z(i, j, k) + Z(i, j + 1, k + 2) - Z(i, j + 1, k));
-    pz_lo_md_hi *= h_xi / h_zeta;
-    T pz_lo_md_lo = h * (X(i, j, k) + X(i - 1, j, k) - X(i, j, k - 1) - X(i - 1, j, k - 1));
-    h_xi = q * (Z(i + 1, j, k) - Z(i - 1, j, k) + Z(i + 1, j + 1, k) - Z(i - 1, j + 1, k)) * dxinv;
-    h_zeta = q * (Z(i, j, k + 1) - Z(i, j, k - 1) + Z(i, j + 1, k + 1) - Z(i, j + 1, k - 1));
-    pz_lo_md_lo *= h_xi / h_zeta;
+    T px_lo = (x000 - xm00) * dxinv;
+    T pz_lo_md_hi = h * (x00p + xm0p - x000 - xm00);
+    pz_lo_md_hi *= m.rx[o + sz];
+    T pz_lo_md_lo = h * (x000 + xm00 - x00m - xm0m);
+    pz_lo_md_lo *= m.rx[o];
     px_lo -= h * (pz_lo_md_hi + pz_lo_md_lo);
 
-    T py_hi = (X(i, j + 1, k) - X(i, j, k)) * dyinv;
-    T pz_md_hi_hi = h * (X(i, j + 1, k + 1) + X(i, j, k + 1) - X(i, j + 1, k) - X(i, j, k));
-    h_eta = q * (Z(i, j + 2, k + 1) - Z(i, j, k + 1) + Z(i + 1, j + 2, k + 1) - Z(i + 1, j, k + 1)) * dyinv;
-    h_zeta = q * (Z(i, j + 1, k + 2) - Z(i, j + 1, k) + Z(i + 1, j + 1, k + 2) - Z(i + 1, j + 1, k));
-    pz_md_hi_hi *= h_eta / h_zeta;
-    T pz_md_hi_lo = h * (X(i, j + 1, k) + X(i, j, k) - X(i, j + 1, k - 1) - X(i, j, k - 1));
-    h_eta = q * (Z(i, j + 2, k) - Z(i, j, k) + Z(i + 1, j + 2, k) - Z(i + 1, j, k)) * dyinv;
-    h_zeta = q * (Z(i, j + 1, k + 1) - Z(i, j + 1, k - 1) + Z(i + 1, j + 1, k + 1) - Z(i + 1, j + 1, k - 1));
-    pz_md_hi_lo *= h_eta / h_zeta;
+    T py_hi = (x0p0 - x000) * dyinv;
+    T pz_md_hi_hi = h * (x0pp + x00p - x0p0 - x000);
+    pz_md_hi_hi *= m.ry[o + sy + sz];
+    T pz_md_hi_lo = h * (x0p0 + x000 - x0pm - x00m);
+    pz_md_hi_lo *= m.ry[o + sy];
     py_hi -= h * (pz_md_hi_hi + pz_md_hi_lo);
 
-    T py_lo = (X(i, j, k) - X(i, j - 1, k)) * dyinv;
-    T pz_md_lo_hi = h * (X(i, j, k + 1) + X(i, j - 1, k + 1) - X(i, j, k) - X(i, j - 1, k));
-    h_eta = q * (Z(i, j + 1, k + 1) - Z(i, j - 1, k + 1) + Z(i + 1, j + 1, k + 1) - Z(i + 1, j - 1, k + 1)) * dyinv;
-    h_zeta = q * (Z(i, j, k + 2) - Z(i, j, k) + Z(i + 1, j, k + 2) - Z(i + 1, j, k));
-    pz_md_lo_hi *= h_eta / h_zeta;
-    T pz_md_lo_lo = h * (X(i, j, k) + X(i, j - 1, k) - X(i, j, k - 1) - X(i, j - 1, k - 1));
-    h_eta = q * (Z(i, j + 1, k) - Z(i, j - 1, k) + Z(i + 1, j + 1, k) - Z(i + 1, j - 1, k)) * dyinv;
-    h_zeta = q * (Z(i, j, k + 1) - Z(i, j, k - 1) + Z(i + 1, j, k + 1) - Z(i + 1, j, k - 1));
-    pz_md_lo_lo *= h_eta / h_zeta;
+    T py_lo = (x000 - x0m0) * dyinv;
+    T pz_md_lo_hi = h * (x00p + x0mp - x000 - x0m0);
+    pz_md_lo_hi *= m.ry[o + sz];
+    T pz_md_lo_lo = h * (x000 + x0m0 - x00m - x0mm);
+    pz_md_lo_lo *= m.ry[o];
     py_lo -= h * (pz_md_lo_hi + pz_md_lo_lo);
 
-    T pz_hi = X(i, j, k + 1) - X(i, j, k);
-    const T hzi_hi = T(8) / ((Z(i, j, k + 2) + Z(i + 1, j, k + 2) + Z(i, j + 1, k + 2) + Z(i + 1, j + 1, k + 2))
-                             - (Z(i, j, k) + Z(i + 1, j, k) + Z(i, j + 1, k) + Z(i + 1, j + 1, k)));
-    pz_hi *= hzi_hi;
-    const T px_hi_md_hi = h * (X(i + 1, j, k + 1) - X(i, j, k + 1) + X(i + 1, j, k) - X(i, j, k)) * dxinv;
-    const T px_lo_md_hi = h * (X(i, j, k + 1) - X(i - 1, j, k + 1) + X(i, j, k) - X(i - 1, j, k)) * dxinv;
-    const T py_md_hi_hi = h * (X(i, j + 1, k + 1) - X(i, j, k + 1) + X(i, j + 1, k) - X(i, j, k)) * dyinv;
-    const T py_md_lo_hi = h * (X(i, j, k + 1) - X(i, j - 1, k + 1) + X(i, j, k) - X(i, j - 1, k)) * dyinv;
-    const T h_xi_on_zhi = h * (Z(i + 1, j + 1, k + 1) + Z(i + 1, j, k + 1) - Z(i, j + 1, k + 1) - Z(i, j, k + 1)) * dxinv;
-    const T h_eta_on_zhi = h * (Z(i + 1, j + 1, k + 1) + Z(i, j + 1, k + 1) - Z(i + 1, j, k + 1) - Z(i, j, k + 1)) * dyinv;
-    pz_hi -= h * h_xi_on_zhi * ((px_hi_md_hi + px_lo_md_hi) - (pz_hi_md_hi + pz_lo_md_hi));
-    pz_hi -= h * h_eta_on_zhi * ((py_md_hi_hi + py_md_lo_hi) - (pz_md_hi_hi + pz_md_lo_hi));
+    T pz_hi = x00p - x000;
+    pz_hi *= m.hz[o + sz];
+    const T px_hi_md_hi = h * (xp0p - x00p + xp00 - x000) * dxinv;
+    const T px_lo_md_hi = h * (x00p - xm0p + x000 - xm00) * dxinv;
+    const T py_md_hi_hi = h * (x0pp - x00p + x0p0 - x000) * dyinv;
+    const T py_md_lo_hi = h * (x00p - x0mp + x000 - x0m0) * dyinv;
+    pz_hi -= h * m.sx[o + sz] * ((px_hi_md_hi + px_lo_md_hi) - (pz_hi_md_hi + pz_lo_md_hi));
+    pz_hi -= h * m.sy[o + sz] * ((py_md_hi_hi + py_md_lo_hi) - (pz_md_hi_hi + pz_md_lo_hi));
 
-    T pz_lo = X(i, j, k) - X(i, j, k - 1);
-    const T hzi_lo = T(8) / ((Z(i, j, k + 1) + Z(i + 1, j, k + 1) + Z(i, j + 1, k + 1) + Z(i + 1, j + 1, k + 1))
-                             - (Z(i, j, k - 1) + Z(i + 1, j, k - 1) + Z(i, j + 1, k - 1) + Z(i + 1, j + 1, k - 1)));
-    pz_lo *= hzi_lo;
-    const T px_hi_md_lo = h * (X(i + 1, j, k) - X(i, j, k) + X(i + 1, j, k - 1) - X(i, j, k - 1)) * dxinv;
-    const T px_lo_md_lo = h * (X(i, j, k) - X(i - 1, j, k) + X(i, j, k - 1) - X(i - 1, j, k - 1)) * dxinv;
-    const T py_md_hi_lo = h * (X(i, j + 1, k) - X(i, j, k) + X(i, j + 1, k - 1) - X(i, j, k - 1)) * dyinv;
-    const T py_md_lo_lo = h * (X(i, j, k) - X(i, j - 1, k) + X(i, j, k - 1) - X(i, j - 1, k - 1)) * dyinv;
-    const T h_xi_on_zlo = h * (Z(i + 1, j + 1, k) + Z(i + 1, j, k) - Z(i, j + 1, k) - Z(i, j, k)) * dxinv;
-    const T h_eta_on_zlo = h * (Z(i + 1, j + 1, k) + Z(i, j + 1, k) - Z(i + 1, j, k) - Z(i, j, k)) * dyinv;
-    pz_lo -= h * h_xi_on_zlo * ((px_hi_md_lo + px_lo_md_lo) - (pz_hi_md_lo + pz_lo_md_lo));
-    pz_lo -= h * h_eta_on_zlo * ((py_md_hi_lo + py_md_lo_lo) - (pz_md_hi_lo + pz_md_lo_lo));
-#undef X
-#undef Z
-    if (k == 0) { pz_lo = T(0); }
-    if ((b.zf & TP_XLO) && i == 0) { px_lo = T(0); }
-    if ((b.zf & TP_XHI) && i == g.nx - 1) { px_hi = T(0); }
-    if ((b.zf & TP_YLO) && j == 0) { py_lo = T(0); }
-    if ((b.zf & TP_YHI) && j == g.ny - 1) { py_hi = T(0); }
-    if ((b.zf & TP_ZHI) && k == g.nz - 1) { pz_hi = T(0); }
-    const T y = (axa[at(g, i + 1, j, k)] * px_hi - axa[at(g, i, j, k)] * px_lo) * dxinv
-              + (aya[at(g, i, j + 1, k)] * py_hi - aya[at(g, i, j, k)] * py_lo) * dyinv
-              + (aza[at(g, i, j, k + 1)] * pz_hi - aza[at(g, i, j, k)] * pz_lo) * dzinv;
-    return y / Jc[at(g, i, j, k)];
+    T pz_lo = x000 - x00m;
+    pz_lo *= m.hz[o];
+    const T px_hi_md_lo = h * (xp00 - x000 + xp0m - x00m) * dxinv;
+    const T px_lo_md_lo = h * (x000 - xm00 + x00m - xm0m) * dxinv;
+    const T py_md_hi_lo = h * (x0p0 - x000 + x0pm - x00m) * dyinv;
+    const T py_md_lo_lo = h * (x000 - x0m0 + x00m - x0mm) * dyinv;
+    pz_lo -= h * m.sx[o] * ((px_hi_md_lo + px_lo_md_lo) - (pz_hi_md_lo + pz_lo_md_lo));
+    pz_lo -= h * m.sy[o] * ((py_md_hi_lo + py_md_lo_lo) - (pz_md_hi_lo + pz_md_lo_lo));
+    if (!INTERIOR) {
+        if (k == 0) { pz_lo = T(0); }
+        if ((b.zf & TP_XLO) && i == 0) { px_lo = T(0); }
+        if ((b.zf & TP_XHI) && i == g.nx - 1) { px_hi = T(0); }
+        if ((b.zf & TP_YLO) && j == 0) { py_lo = T(0); }
+        if ((b.zf & TP_YHI) && j == g.ny - 1) { py_hi = T(0); }
+        if ((b.zf & TP_ZHI) && k == g.nz - 1) { pz_hi = T(0); }
+    }
+    const T y = (axa[o + 1] * px_hi - axa[o] * px_lo) * dxinv
+              + (aya[o + sy] * py_hi - aya[o] * py_lo) * dyinv
+              + (aza[o + sz] * pz_hi - aza[o] * pz_lo) * dzinv;
+    return y / Jc[o];
+}
+
+//! adotx_r at any valid cell: the direct form where all 18 neighbours are valid cells.
+template <typename T>
+__device__ __forceinline__ T adotx_cell(const gb_grid& g, const PBC& b, int i, int j, int k, const T* x,
+                                        const T* __restrict__ axa, const T* __restrict__ aya,
+                                        const T* __restrict__ aza, const T* __restrict__ Jc, const MeshRatios<T>& m)
+{
+    const bool inside = i > 0 && i < g.nx - 1 && j > 0 && j < g.ny - 1 && k > 0 && k < g.nz - 1;
+    return inside ? adotx_r<T, true>(g, b, i, j, k, x, axa, aya, aza, Jc, m)
+                  : adotx_r<T, false>(g, b, i, j, k, x, axa, aya, aza, Jc, m);
 }
 
 //! The principal tridiagonal of the operator on column (i, j) at level k

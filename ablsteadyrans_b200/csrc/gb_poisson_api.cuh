@@ -26,6 +26,12 @@ struct PoissonLevels {
     T* TD[kMaxLevels] = {};   // the smoother's line tridiagonal, per level
     T* TC[kMaxLevels] = {};
     T* TU[kMaxLevels] = {};
+    T* RX[kMaxLevels] = {};  // the mesh ratios of the operator (MeshRatios), per level
+    T* RY[kMaxLevels] = {};
+    T* HZ[kMaxLevels] = {};
+    T* SX[kMaxLevels] = {};
+    T* SY[kMaxLevels] = {};
+    MeshRatios<T> ratios(int l) const { return MeshRatios<T>{RX[l], RY[l], HZ[l], SX[l], SY[l]}; }
     std::vector<void*> owned;
     void release();
 };

@@ -114,7 +114,6 @@ bool dirichlet_normal(const gb_bc& bc, int face)
     return t == GB_FACE_INFLOW || t == GB_FACE_SLIP_WALL || t == GB_FACE_NO_SLIP_WALL;
 }
 
-inline int ext(const gb_grid& g, int t, int d) { return ((d == 0) ? g.nx : (d == 1) ? g.ny : g.nz) + nodal(t, d); }
 inline bool is_per(const gb_grid& g, int d) { return d == 0 ? g.periodic_x : d == 1 ? g.periodic_y : false; }
 const int kLoc[6] = {XF, YF, ZF, CC, CC, CC};
 
@@ -183,21 +182,31 @@ __global__ void k_level_mean(gb_grid g, Box b, const double* __restrict__ f, dou
     }
 }
 
-__global__ void k_maxabs(gb_grid g, Box b, const double* __restrict__ f, const double* __restrict__ mul,
-                         unsigned long long* __restrict__ slot)
+__global__ void __launch_bounds__(256) k_maxabs(gb_grid g, Box b, const double* __restrict__ f,
+                                                const double* __restrict__ mul, unsigned long long* __restrict__ slot)
 {
-    const int64_t n = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    // rows (j, k) of the box over the blocks, i over the threads; a block max,
+    // then one atomic per block (one per warp on a single word serialises)
+    __shared__ double red[8];
+    const int nx = b.hi[0] - b.lo[0] + 1, ny = b.hi[1] - b.lo[1] + 1, nz = b.hi[2] - b.lo[2] + 1;
+    const int rows = ny * nz;
     double v = 0;
-    if (n < b.count()) {
-        const int nx = b.hi[0] - b.lo[0] + 1, ny = b.hi[1] - b.lo[1] + 1;
-        const int i = b.lo[0] + static_cast<int>(n % nx);
-        const int j = b.lo[1] + static_cast<int>((n / nx) % ny);
-        const int k = b.lo[2] + static_cast<int>(n / (static_cast<int64_t>(nx) * ny));
-        const int64_t o = at(g, i, j, k);
-        v = fabs(mul ? f[o] * mul[o] : f[o]);
+    for (int r = blockIdx.x; r < rows; r += gridDim.x) {
+        const int j = b.lo[1] + r % ny, k = b.lo[2] + r / ny;
+        const int64_t o0 = at(g, b.lo[0], j, k);
+        for (int i = threadIdx.x; i < nx; i += blockDim.x) {
+            const double a = fabs(mul ? f[o0 + i] * mul[o0 + i] : f[o0 + i]);
+            v = (a > v || a != a) ? a : v;
+        }
     }
-    v = warp_max(v);
-    if ((threadIdx.x & 31) == 0) { atomic_max_nonneg(slot, v); }
+    v = warp_max_nan(v);
+    if ((threadIdx.x & 31) == 0) { red[threadIdx.x >> 5] = v; }
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double t = (threadIdx.x < (blockDim.x >> 5)) ? red[threadIdx.x] : 0.0;
+        t = warp_max_nan(t);
+        if (threadIdx.x == 0) { atomic_max_nonneg(slot, t); }
+    }
 }
 
 }  // namespace
@@ -304,9 +313,11 @@ void dsum(gb_simplec* S, const Box& b, const double* f, int mode, int slot)
 void dmax(gb_simplec* S, const Box& b, const double* f, const double* mul, int word)
 {
     gb_ctx* ctx = S->ctx;
-    const int64_t n = b.count();
+    const int rows = (b.hi[1] - b.lo[1] + 1) * (b.hi[2] - b.lo[2] + 1);
     Span span(ctx, GB_KERNEL_VECTOR);
-    k_maxabs<<<static_cast<unsigned>((n + 255) / 256), 256, 0, ctx->stream>>>(S->g, b, f, mul, dword(ctx, word));
+    const int nthr = (b.hi[0] - b.lo[0] + 1) > 128 ? 256 : 128;
+    k_maxabs<<<std::max(1, std::min(rows, 4 * ctx->num_sms)), nthr, 0, ctx->stream>>>(S->g, b, f, mul,
+                                                                                     dword(ctx, word));
     ++ctx->launches;
 }
 

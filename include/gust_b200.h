@@ -93,11 +93,16 @@ enum {
  * gb_ctx_profile_read sums the recorded spans of one family. */
 gb_status gb_ctx_profile(gb_ctx* ctx, int32_t enable);
 gb_status gb_ctx_profile_read(gb_ctx* ctx, int32_t family, double* total_ms, int64_t* spans);
+/* Which families profiling times: bit f set = family f (default: all). Timing
+ * only the family of interest keeps the events' own cost out of a timed step. */
+gb_status gb_ctx_profile_mask(gb_ctx* ctx, uint32_t mask);
 /* Tuning knobs of a context (the in-project autotuner sets them per shape). */
 enum {
-    GB_TUNE_LINE_VARIANT = 0,   /* z-line sweep kernel: 0 auto, 1 pipelined (cp.async ring), 2 shared, 3 global scratch */
+    GB_TUNE_LINE_VARIANT = 0,   /* z-line sweep kernel: 0 auto (= 4), 1 pipelined (cp.async ring), 2 shared,
+                                   3 global scratch, 4 pipelined with the column factors kept between sweeps */
     GB_TUNE_LINE_BLOCK,         /* threads per block of the pipelined sweep (32, 64 or 128; 0 = default) */
-    GB_TUNE_MG_SMOOTH_BLOCK,    /* threads per block of the multigrid smoother (32 or 64; 0 = default) */
+    GB_TUNE_MG_COARSE_KERNEL,   /* the coarsest level's relaxations: 0 auto (one single-block launch when the
+                                   level has at most 64 columns), 1 the per-relaxation launches */
     GB_N_TUNE
 };
 gb_status gb_ctx_tune(gb_ctx* ctx, int32_t key, int32_t value);

@@ -624,13 +624,16 @@ static void mg_smooth(og_mg* mg, og_level* L)
                 for (int k = 0; k < nz; ++k) {
                     r[k] = L->b[IX(g, i, j, k)] - adotx_cell(g, i, j, k, L->x, L->AX, L->AY, L->AZ, L->J, L->z, zf);
                 }
+                /* Factored Thomas: reciprocal pivots 1/m_k and eliminated uppers
+                 * c'_k = U_k (1/m_k), then e_k = (r_k - D_k e_{k-1}) (1/m_k). */
                 double cp = 0, ep = 0;
                 for (int k = 0; k < nz; ++k) {
                     double D, C, U;
                     og_line_tridiag(g, mg->bc, zf, L->AX, L->AY, L->AZ, L->J, L->z, i, j, k, &D, &C, &U);
                     const double m = (k == 0) ? C : C - D * cp;
-                    cp = U / m;
-                    ep = ((k == 0) ? r[k] : r[k] - D * ep) / m;
+                    const double im = 1.0 / m;
+                    cp = U * im;
+                    ep = ((k == 0) ? r[k] : r[k] - D * ep) * im;
                     c[k] = cp;
                     e[k] = ep;
                 }

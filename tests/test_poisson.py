@@ -137,10 +137,14 @@ def test_gpu_apply_and_fluxes_match_oracle(ctx, per):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("kernel", [0, 1])
 @pytest.mark.parametrize("per", [(True, True), (False, False), (True, False)])
-def test_gpu_vcycle_matches_oracle_fp64(ctx, per):
-    """One V-cycle of the FP64 multigrid agrees with the oracle's to 1e-12."""
+def test_gpu_vcycle_matches_oracle_fp64(ctx, per, kernel):
+    """One V-cycle of the FP64 multigrid agrees with the oracle's to 1e-12,
+    with the coarsest level's relaxations in one single-block launch (kernel
+    0, the default) and launched one by one (kernel 1)."""
     import ablsteadyrans_b200 as gb
+    ctx.tune(gb.TUNE_MG_COARSE_KERNEL, kernel)
     g, z, J, ax, ay, az, _ = smooth_terrain_case(32, 24, 16, *per, hill=150.0)
     bc = (PERIODIC if per[0] else NEUMANN, PERIODIC if per[1] else NEUMANN, NEUMANN,
           PERIODIC if per[0] else DIRICHLET, PERIODIC if per[1] else NEUMANN, DIRICHLET)
@@ -154,8 +158,37 @@ def test_gpu_vcycle_matches_oracle_fp64(ctx, per):
     ps = gb.PoissonSolver(ctx, g, dz, dJ, bc, opts)
     ps.set_coeffs(dax, day, daz)
     e = to_host(ps.vcycle(to_dev(r)))
+    ctx.tune(gb.TUNE_MG_COARSE_KERNEL, 0)
     assert rel_err(e, e_ref, g.valid(0)) < 1e-12
     ps.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("per", [(True, False), (False, True)])
+def test_gpu_coarse_kernel_equals_per_relaxation_launches(ctx, precision, per):
+    """The single-block coarsest-level kernel performs the per-relaxation
+    launches' arithmetic: a V-cycle on a 64 x 48 x 24 hill (coarsest level
+    4 x 3 ... down to the last even split) agrees with the launch-by-launch
+    V-cycle to rounding, in FP64 and FP32."""
+    import ablsteadyrans_b200 as gb
+    g, z, J, ax, ay, az, _ = smooth_terrain_case(64, 48, 24, *per, hill=150.0)
+    bc = (PERIODIC if per[0] else NEUMANN, PERIODIC if per[1] else NEUMANN, NEUMANN,
+          PERIODIC if per[0] else DIRICHLET, PERIODIC if per[1] else DIRICHLET, DIRICHLET)
+    rng = np.random.default_rng(4)
+    r = g.np_zeros()
+    r[g.valid(0)] = rng.standard_normal(r[g.valid(0)].shape)
+    out = []
+    for kernel in (0, 1):
+        ctx.tune(gb.TUNE_MG_COARSE_KERNEL, kernel)
+        dz, dJ, dax, day, daz = _gpu_case(g, z, J, ax, ay, az)
+        opts = gb.PoissonOptions.default(precision=precision, nu1=1, nu2=1, nu_coarse=8, max_levels=12, min_coarse=2)
+        ps = gb.PoissonSolver(ctx, g, dz, dJ, bc, opts)
+        ps.set_coeffs(dax, day, daz)
+        out.append(to_host(ps.vcycle(to_dev(r))))
+        ps.close()
+    ctx.tune(gb.TUNE_MG_COARSE_KERNEL, 0)
+    assert rel_err(out[0], out[1], g.valid(0)) < (1e-13 if precision == 0 else 1e-5)
 
 
 @pytest.mark.gpu
