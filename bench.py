@@ -20,6 +20,7 @@ the oracle (the FP64 C restatement; the reference itself needs AMReX, which
 is not available), on every host thread, on the same workload and metric.
 """
 import argparse
+import ctypes
 import json
 import os
 import statistics
@@ -102,10 +103,30 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------ the workload ---
-# algorithmic bytes of one z-line sweep launch per point (FP64: 8 B words):
-# A off-diagonals 6, a_P 1, rhs 1, delta_old 1 read, delta_new 1 written (the
-# first sweep of a solve reads no delta_old: 9 words)
-LINE_WORDS_FIRST, LINE_WORDS = 9, 10
+# algorithmic words of one z-line sweep launch per point: a later sweep reads
+# the 4 lateral coefficients, a_ZM, the two kept factors (1/m, c', in place of
+# a_P and a_ZP), rhs and the lagged iterate and writes the new iterate (10);
+# the first sweep of a solve (zero initial iterate, no lateral terms) reads
+# a_P, a_ZM, a_ZP and rhs and writes the iterate (5)
+LINE_WORDS_FIRST, LINE_WORDS = 5, 10
+LINE_PROFILE = os.path.join(ROOT, "profiles", "zline_fact_kernel_config1_fp64.txt")
+
+
+def line_traffic_per_point():
+    """DRAM bytes per point of the first and the later sweeps from the
+    committed ncu capture (None when absent)."""
+    vals = {}
+    try:
+        with open(LINE_PROFILE) as f:
+            for line in f:
+                if line.startswith("traffic_bytes_per_point_"):
+                    key, val = line.split(":")
+                    vals[key.strip()[len("traffic_bytes_per_point_"):]] = float(val)
+    except OSError:
+        return None
+    if "first" in vals and "later" in vals:
+        return vals["first"], vals["later"]
+    return None
 
 
 class SimplecWorkload:
@@ -123,15 +144,17 @@ class SimplecWorkload:
     def cells(self):
         return self.inst.cells
 
-    def line_bytes_per_step(self):
-        """Algorithmic bytes of the z-line sweep launches of one iteration
-        (u, v, w, theta, k systems, `sweeps` sweeps each)."""
+    def line_bytes_per_step(self, per_point=None):
+        """Bytes of the z-line sweep launches of one iteration (u, v, w,
+        theta, k systems, `sweeps` sweeps each): algorithmic, or with
+        per_point = (first, later) bytes per point."""
         g = self.inst.grid
         word = 8 if self.precision == 0 else 4
+        first, later = per_point if per_point else (LINE_WORDS_FIRST * word, LINE_WORDS * word)
         total = 0
         for loc in (1, 2, 4, 0, 0):
             ni, nj, nk = g.extents(loc)
-            total += ni * nj * nk * word * (LINE_WORDS_FIRST + LINE_WORDS * (self.sweeps - 1))
+            total += ni * nj * nk * (first + later * (self.sweeps - 1))
         return total
 
     def setup(self, ctx):
@@ -153,19 +176,33 @@ class SimplecWorkload:
     def step(self):
         return self.driver.step()
 
-    # end to end: the state in host memory each step
-    def e2e_setup(self):
+    # end to end: one solve through the public API from host memory. The
+    # instance's initial state comes from pinned host buffers, the iterations
+    # run with the state resident (as a steady solve keeps it), every step
+    # reads its residual norms back (gb_iter_info), and the final state
+    # returns to pinned host buffers.
+    def e2e_setup(self, steps):
         import torch
-        self.host = {f: t.cpu().pin_memory() for f, t in self.case.q.items()}
-        self.h2d = sum(t.numel() * 8 for t in self.host.values())
-        self.d2h = self.h2d
 
-    def e2e_step(self):
+        from ablsteadyrans_b200 import abi
+        self.host_in = {f: t.cpu().pin_memory() for f, t in self.q0.items()}
+        self.host_out = {f: torch.empty_like(t).pin_memory() for f, t in self.host_in.items()}
+        state_bytes = sum(t.numel() * t.element_size() for t in self.host_in.values())
+        info_bytes = ctypes.sizeof(abi.IterInfo)
+        self.h2d = int(round(state_bytes / steps))
+        self.d2h = int(round(state_bytes / steps)) + info_bytes
+
+    def e2e_solve(self, steps):
+        from ablsteadyrans_b200.driver import Driver
         for f, t in self.case.q.items():
-            t.copy_(self.host[f], non_blocking=True)
-        status = self.driver.step()
+            t.copy_(self.host_in[f], non_blocking=True)
+        self.stage.fill_ghosts()
+        driver = Driver(self.stage)
+        status = "running"
+        for _ in range(steps):
+            status = driver.step()
         for f, t in self.case.q.items():
-            self.host[f].copy_(t, non_blocking=True)
+            self.host_out[f].copy_(t, non_blocking=True)
         return status
 
     # CPU: the oracle on the same instance
@@ -273,18 +310,16 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         total_ms = float(t.item())
 
-    # end to end through the public API with the state in host memory
-    wl.e2e_setup()
-    for _ in range(2):
-        wl.e2e_step()
+    # end to end through the public API: one solve of K steps from host memory
+    wl.e2e_setup(args.steps)
+    wl.e2e_solve(2)
     torch.cuda.synchronize()
     if dist is not None:
         dist.barrier()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record()
-    for s in range(args.steps):
-        wl.e2e_step()
+    wl.e2e_solve(args.steps)
     e1.record()
     torch.cuda.synchronize()
     e2e_ms = e0.elapsed_time(e1)
@@ -299,6 +334,8 @@ def main():
     peak, peak_kind = hbm_peak()
     line_bytes = wl.line_bytes_per_step() * args.steps
     achieved = (line_bytes / (sweep_ms / 1e3)) / 1e9 if sweep_ms > 0 else None
+    tpp = line_traffic_per_point() if args.precision == 0 else None
+    traffic = (wl.line_bytes_per_step(tpp) * args.steps / max(sweep_n, 1)) if tpp else None
 
     line = {
         "metric": "cell-updates/s",
@@ -320,8 +357,9 @@ def main():
                 "d2h_bytes_per_step": wl.d2h},
         "gpu_launches": launches,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": (achieved / peak) if achieved else None, "traffic": None,
-                     "kernel": "zline_pipe_kernel (z-line Thomas sweep)", "peak_kind": peak_kind,
+                     "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                     "kernel": "zline_fact_kernel (z-line Thomas sweeps of u, v, w, theta, k)",
+                     "peak_kind": peak_kind,
                      "bytes_per_launch": line_bytes / max(sweep_n, 1), "launch_ms": sweep_ms / max(sweep_n, 1)},
         "breakdown": families,
         "clocks": clocks,
