@@ -73,6 +73,7 @@ def _declare(L):
     L.gb_zline_jacobi.argtypes = [P, G, i32, P, P, P, i32, P, ctypes.POINTER(f64)]
     L.gb_zline_jacobi_f32.argtypes = [P, G, i32, P, P, P, i32, P, ctypes.POINTER(ctypes.c_float)]
     L.gb_zline_jacobi_noalloc.argtypes = [G, i32, P, P, P, i32, P, ctypes.POINTER(f64), P]
+    L.gb_zline_lusgs.argtypes = [P, G, i32, P, P, P, i32, i32, P, ctypes.POINTER(f64)]
 
 
 def check(status):
@@ -150,6 +151,16 @@ def zline_jacobi(ctx, grid, loc, A, ap, rhs, sweeps, delta):
         out = ctypes.c_float()
         check(L.gb_zline_jacobi_f32(ctx.handle, ctypes.byref(grid.c), loc, _ptr(A), _ptr(ap), _ptr(rhs), sweeps,
                                     _ptr(delta), ctypes.byref(out)))
+    return float(out.value)
+
+
+def zline_lusgs(ctx, grid, loc, A, ap, rhs, sweeps, delta, alternate=0):
+    """gust::zline_lusgs with line_ghosts = lagged (Source/LineSweeps.H:
+    159-161): symmetric line LU-SGS passes into delta (FP64); returns max
+    |change| over the last backward pass."""
+    out = ctypes.c_double()
+    check(lib().gb_zline_lusgs(ctx.handle, ctypes.byref(grid.c), loc, _ptr(A), _ptr(ap), _ptr(rhs), int(sweeps),
+                               int(alternate), _ptr(delta), ctypes.byref(out)))
     return float(out.value)
 
 

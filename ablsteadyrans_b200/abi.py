@@ -87,21 +87,46 @@ class Physics(ctypes.Structure):
 
 
 class SimplecOptions(ctypes.Structure):
-    """gb_simplec_opts: simplec.*, steady.zline_sweeps, turb.tke_floor and the
-    correction's Poisson solver."""
+    """gb_simplec_opts: simplec.*, steady.zline_sweeps, steady.sweep (0 zjacobi,
+    1 lusgs), steady.line_alternate, turb.tke_floor and the correction's
+    Poisson solver."""
     _fields_ = [("pressure_reltol", ctypes.c_double), ("alpha_p", ctypes.c_double),
                 ("rotation_relax", ctypes.c_double), ("w_vnn_cap", ctypes.c_double),
                 ("w_vnn_cap_slope_margin", ctypes.c_double), ("tke_floor", ctypes.c_double),
-                ("zline_sweeps", ctypes.c_int32), ("precision", ctypes.c_int32), ("poisson", PoissonOptions)]
+                ("zline_sweeps", ctypes.c_int32), ("precision", ctypes.c_int32), ("poisson", PoissonOptions),
+                ("line_sweep", ctypes.c_int32), ("line_alternate", ctypes.c_int32)]
 
     @classmethod
     def make(cls, **kw):
         """The reference's defaults (Source/Simplec.H:80-90, Source/Driver.H:92)."""
         o = cls(pressure_reltol=1e-3, alpha_p=1.0, rotation_relax=0.3, w_vnn_cap=0.0, w_vnn_cap_slope_margin=4.0,
-                tke_floor=0.0, zline_sweeps=2, precision=0, poisson=PoissonOptions.defaults())
+                tke_floor=0.0, zline_sweeps=2, precision=0, poisson=PoissonOptions.defaults(), line_sweep=0,
+                line_alternate=0)
         for k, v in kw.items():
             setattr(o, k, v)
         return o
+
+
+class InitOptions(ctypes.Structure):
+    """gb_init_opts: init.* of the mass-consistent initializer and the
+    projection's solver.poisson_*."""
+    _fields_ = [("z_agl_min", ctypes.c_double), ("alpha_h", ctypes.c_double), ("alpha_v", ctypes.c_double),
+                ("k_decay_height", ctypes.c_double), ("projection", ctypes.c_int32), ("obrien", ctypes.c_int32),
+                ("poisson", PoissonOptions)]
+
+    @classmethod
+    def make(cls, **kw):
+        """The reference's defaults (Source/Initializer.H:63-111, Source/Poisson.H:41-75)."""
+        o = cls(z_agl_min=0.0, alpha_h=1.0, alpha_v=1.0, k_decay_height=0.0, projection=1, obrien=0,
+                poisson=PoissonOptions.defaults())
+        for k, v in kw.items():
+            setattr(o, k, v)
+        return o
+
+
+class InitResult(ctypes.Structure):
+    _fields_ = [("divergence_before", ctypes.c_double), ("divergence_after", ctypes.c_double),
+                ("poisson_iterations", ctypes.c_int32), ("poisson_final_residual", ctypes.c_double)]
 
 
 class State(ctypes.Structure):

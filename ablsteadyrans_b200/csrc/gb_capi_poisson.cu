@@ -15,7 +15,9 @@ gb_status need(bool ok, const char* fmt, const char* what)
     return GB_BAD_ARG;
 }
 
-gb_status check_opts(const gb_poisson_opts& o)
+}  // namespace
+
+gb_status gb::check_poisson_options(const gb_poisson_opts& o)
 {
     const double eps = std::numeric_limits<double>::epsilon();
     if (!std::isfinite(o.reltol) || !(o.reltol >= 10 * eps) || !(o.reltol < 1)) {
@@ -46,6 +48,10 @@ gb_status check_opts(const gb_poisson_opts& o)
     }
     return GB_OK;
 }
+
+namespace {
+
+gb_status check_opts(const gb_poisson_opts& o) { return gb::check_poisson_options(o); }
 
 }  // namespace
 

@@ -48,6 +48,23 @@ gb_status check_simplec_options(const gb_simplec_opts& o)
         gb::set_error("gust: SimplecStage: sweeps must be >= 1 (steady.zline_sweeps; 2..100 for zjacobi)");
         return GB_BAD_ARG;
     }
+    if (o.line_sweep != 0 && o.line_sweep != 1) {
+        gb::set_error("gust: invalid inputs:\n  steady.sweep = %d: must be zjacobi (0) or lusgs (1)", o.line_sweep);
+        return GB_BAD_ARG;
+    }
+    if (o.line_alternate != 0 && o.line_alternate != 1) {
+        gb::set_error("gust: invalid inputs:\n  steady.line_alternate = %d: must be 0 or 1", o.line_alternate);
+        return GB_BAD_ARG;
+    }
+    if (o.line_alternate == 1 && o.line_sweep != 1) {
+        gb::set_error("gust: invalid inputs:\n  steady.line_alternate has no effect unless steady.sweep = lusgs");
+        return GB_BAD_ARG;
+    }
+    if (o.line_alternate == 1 && o.zline_sweeps < 2) {
+        gb::set_error("gust: invalid inputs:\n  steady.line_alternate = 1 needs steady.zline_sweeps >= 2 (only the odd "
+                      "sweeps are reversed)");
+        return GB_BAD_ARG;
+    }
     if (std::isnan(o.tke_floor) || !(o.tke_floor >= 0)) {
         gb::set_error("gust: SimplecStage: tke_floor must be >= 0 (turb.tke_floor)");
         return GB_BAD_ARG;
@@ -198,6 +215,66 @@ gb_status gb_local_dtau(gb_simplec* s, const gb_state* q, double cfl, double* dt
         return GB_BAD_ARG;
     }
     return gb::simplec_local_dtau(s, *q, cfl, dtau);
+}
+
+gb_status gb_init_options_default(gb_init_opts* o)
+{
+    gb::clear_error();
+    if (o == nullptr) {
+        gb::set_error("gust: gb_init_options_default: null argument");
+        return GB_BAD_ARG;
+    }
+    *o = gb_init_opts{};
+    o->z_agl_min = 0.0;
+    o->alpha_h = 1.0;
+    o->alpha_v = 1.0;
+    o->k_decay_height = 0.0;
+    o->projection = 1;
+    o->obrien = 0;
+    return gb_poisson_options_default(&o->poisson);
+}
+
+gb_status gb_simplec_initialize(gb_simplec* s, const gb_state* q, const gb_init_opts* o, gb_init_result* r)
+{
+    gb::clear_error();
+    if (s == nullptr || q == nullptr || o == nullptr || r == nullptr) {
+        gb::set_error("gust: initialize_state: null argument");
+        return GB_BAD_ARG;
+    }
+    // check_init_options (Source/Initializer.cpp:110-140)
+    auto bad = [](double x, bool ok) { return std::isnan(x) || !std::isfinite(x) || !ok; };
+    if (bad(o->z_agl_min, o->z_agl_min >= 0)) {
+        gb::set_error("gust: invalid inputs:\n  init.z_agl_min = %g: must be finite and >= 0 (m)", o->z_agl_min);
+        return GB_BAD_ARG;
+    }
+    if (bad(o->alpha_h, o->alpha_h > 0)) {
+        gb::set_error("gust: invalid inputs:\n  init.alpha_h = %g: must be finite and > 0", o->alpha_h);
+        return GB_BAD_ARG;
+    }
+    if (bad(o->alpha_v, o->alpha_v > 0)) {
+        gb::set_error("gust: invalid inputs:\n  init.alpha_v = %g: must be finite and > 0", o->alpha_v);
+        return GB_BAD_ARG;
+    }
+    if (bad(o->k_decay_height, o->k_decay_height >= 0)) {
+        gb::set_error("gust: invalid inputs:\n  init.k_decay_height = %g: must be finite and >= 0 (m)", o->k_decay_height);
+        return GB_BAD_ARG;
+    }
+    if (o->projection != 0 && o->projection != 1) {
+        gb::set_error("gust: init.projection must be 0 or 1");
+        return GB_BAD_ARG;
+    }
+    if (o->obrien != 0) {
+        gb::set_error("gust: init.obrien = %d: the O'Brien column correction is not built here (0 only)", o->obrien);
+        return GB_BAD_ARG;
+    }
+    if (o->alpha_v != o->alpha_h) {
+        gb::set_error("gust: init.alpha_v = %g with init.alpha_h = %g: the split z-face coefficient "
+                      "(FaceCoeffs::z_cross) is not built here; give alpha_v = alpha_h", o->alpha_v, o->alpha_h);
+        return GB_BAD_ARG;
+    }
+    gb_status st = gb::check_poisson_options(o->poisson);
+    if (st != GB_OK) { return st; }
+    return gb::simplec_initialize(s, *q, *o, r);
 }
 
 }  // extern "C"

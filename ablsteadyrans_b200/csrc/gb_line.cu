@@ -14,6 +14,7 @@
 #include "gb_line.cuh"
 
 #include <algorithm>
+#include <atomic>
 #include <mutex>
 
 namespace gb {
@@ -407,25 +408,25 @@ gb_status zline_sweeps(gb_ctx* ctx, const gb_grid& g, int loc, const T* A, const
     const size_t pipe_smem_first = static_cast<size_t>(R * 4 + 2 * nk) * pipe_thr * sizeof(T);
     const size_t pipe_smem = static_cast<size_t>(R * 12 + 2 * nk) * pipe_thr * sizeof(T);
     if (pipelined) {
-        static bool attr_done[2] = {false, false};
+        static std::atomic<bool> attr_done[2];  // set once per process (one device per process)
         const int ti = sizeof(T) == 8 ? 1 : 0;
-        if (!attr_done[ti]) {
+        if (!attr_done[ti].load()) {
             cudaFuncSetAttribute(zline_pipe_kernel<T, true, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
             cudaFuncSetAttribute(zline_pipe_kernel<T, false, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
             cudaFuncSetAttribute(zline_fact_kernel<T, true, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
             cudaFuncSetAttribute(zline_fact_kernel<T, false, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-            attr_done[ti] = true;
+            attr_done[ti].store(true);
         }
     } else if (!use_smem) {
         cbuf = static_cast<T*>(scratch(ctx, kSlotLineC, sizeof(T) * vol));
         ebuf = static_cast<T*>(scratch(ctx, kSlotLineE, sizeof(T) * vol));
         if (cbuf == nullptr || ebuf == nullptr) { return GB_OOM; }
     } else {
-        static bool attr_set[2] = {false, false};
+        static std::atomic<bool> attr_set[2];
         const int ti = sizeof(T) == 8 ? 1 : 0;
-        if (!attr_set[ti]) {
+        if (!attr_set[ti].load()) {
             cudaFuncSetAttribute(zline_sweep_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-            attr_set[ti] = true;
+            attr_set[ti].store(true);
         }
     }
     T* buf[2] = {delta, tmp};

@@ -25,6 +25,11 @@ template <typename T>
 gb_status zline_sweeps(gb_ctx* ctx, const gb_grid& g, int loc, const T* A, const T* ap, const T* rhs, int sweeps,
                        T* delta, unsigned long long* change_word, LineScratch scratch_kind);
 
+//! The line LU-SGS passes (gb_zline_lusgs) into delta (0 on entry, ghosts
+//! included); change_word as for zline_sweeps. FP64.
+gb_status zline_lusgs(gb_ctx* ctx, const gb_grid& g, int loc, const double* A, const double* ap, const double* rhs,
+                      int sweeps, int alternate, double* delta, unsigned long long* change_word);
+
 //! OverrideSync of a field at loc: the high copy of a periodic seam takes the
 //! low copy's value.
 template <typename T>

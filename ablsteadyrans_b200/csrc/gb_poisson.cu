@@ -13,6 +13,7 @@
 #include "gb_poisson_api.cuh"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <vector>
 
@@ -761,12 +762,12 @@ void mg_smooth(gb_poisson* P, PoissonLevels<T>& L, int l)
     const size_t smem_ring = static_cast<size_t>(R * 4 + 2 * g.nz) * nthr * sizeof(T);
     const size_t smem_staged = static_cast<size_t>(5) * g.nz * nthr * sizeof(T);
     const bool staged = smem_staged <= kSmoothSmemMax;
-    static bool attr_done[2] = {false, false};
+    static std::atomic<bool> attr_done[2];  // set once per process (one device per process)
     const int ti = sizeof(T) == 8 ? 1 : 0;
-    if (!attr_done[ti]) {
+    if (!attr_done[ti].load()) {
         cudaFuncSetAttribute(k_color_solve<T, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmoothSmemMax);
         cudaFuncSetAttribute(k_color_solve_staged<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmoothSmemMax);
-        attr_done[ti] = true;
+        attr_done[ti].store(true);
     }
     const int half = (g.nx + 1) / 2;
     for (int color = 0; color < 2; ++color) {
@@ -820,11 +821,11 @@ void vcycle(gb_poisson* P, PoissonLevels<T>& L, int l)
         const bool one_block = ctx->tune[GB_TUNE_MG_COARSE_KERNEL] != 1 && g.nx * g.ny <= 64 && smem <= kSmoothSmemMax
                                && !(g.periodic_x && (g.nx & 1)) && !(g.periodic_y && (g.ny & 1));
         if (one_block && P->opt.nu_coarse > 0) {
-            static bool attr_done[2] = {false, false};
+            static std::atomic<bool> attr_done[2];  // set once per process (one device per process)
             const int ti = sizeof(T) == 8 ? 1 : 0;
-            if (!attr_done[ti]) {
+            if (!attr_done[ti].load()) {
                 cudaFuncSetAttribute(k_coarse_relax<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmoothSmemMax);
-                attr_done[ti] = true;
+                attr_done[ti].store(true);
             }
             Span span(ctx, GB_KERNEL_MG_SMOOTH);
             k_coarse_relax<T><<<1, 256, smem, ctx->stream>>>(g, L.b[l], P->opt.nu_coarse, L.x[l], L.bv[l], L.AX[l],

@@ -67,6 +67,8 @@ struct gb_poisson {
 
 namespace gb {
 
+//! The range checks of solver.poisson_* (messages name the keys).
+gb_status check_poisson_options(const gb_poisson_opts& o);
 gb_status poisson_build(gb_poisson* P);
 gb_status poisson_set_coeffs(gb_poisson* P, const double* ax, const double* ay, const double* az, const double* bx,
                              const double* by, const double* bz);

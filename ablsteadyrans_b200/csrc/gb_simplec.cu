@@ -185,22 +185,24 @@ __global__ void k_level_mean(gb_grid g, Box b, const double* __restrict__ f, dou
 __global__ void __launch_bounds__(256) k_maxabs(gb_grid g, Box b, const double* __restrict__ f,
                                                 const double* __restrict__ mul, unsigned long long* __restrict__ slot)
 {
-    // rows (j, k) of the box over the blocks, i over the threads; a block max,
-    // then one atomic per block (one per warp on a single word serialises)
+    // one warp per row (j, k) of the box, the lanes over i (a row's loads all
+    // in flight at once); a block max, then one atomic per block (one per
+    // warp on a single word serialises)
     __shared__ double red[8];
     const int nx = b.hi[0] - b.lo[0] + 1, ny = b.hi[1] - b.lo[1] + 1, nz = b.hi[2] - b.lo[2] + 1;
-    const int rows = ny * nz;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int r = blockIdx.x * (blockDim.x >> 5) + warp;
     double v = 0;
-    for (int r = blockIdx.x; r < rows; r += gridDim.x) {
-        const int j = b.lo[1] + r % ny, k = b.lo[2] + r / ny;
-        const int64_t o0 = at(g, b.lo[0], j, k);
-        for (int i = threadIdx.x; i < nx; i += blockDim.x) {
+    if (r < ny * nz) {
+        const int64_t o0 = at(g, b.lo[0], b.lo[1] + r % ny, b.lo[2] + r / ny);
+#pragma unroll 4
+        for (int i = lane; i < nx; i += 32) {
             const double a = fabs(mul ? f[o0 + i] * mul[o0 + i] : f[o0 + i]);
             v = (a > v || a != a) ? a : v;
         }
     }
     v = warp_max_nan(v);
-    if ((threadIdx.x & 31) == 0) { red[threadIdx.x >> 5] = v; }
+    if (lane == 0) { red[warp] = v; }
     __syncthreads();
     if (threadIdx.x < 32) {
         double t = (threadIdx.x < (blockDim.x >> 5)) ? red[threadIdx.x] : 0.0;
@@ -257,6 +259,7 @@ struct gb_simplec {
     gb::SimplecWork w{};
     gb::Profile prof{};
     gb_poisson* poisson{nullptr};
+    gb_poisson* init_poisson{nullptr};  // the initializer's projection (its own BC), made on use
     double jmin{0};
     std::vector<void*> owned;
     unsigned long long* h_words{nullptr};
@@ -266,6 +269,7 @@ struct gb_simplec {
 gb_simplec::~gb_simplec()
 {
     if (poisson) { gb_poisson_destroy(poisson); }
+    if (init_poisson) { gb_poisson_destroy(init_poisson); }
     for (void* p : owned) { cudaFree(p); }
 }
 
@@ -315,9 +319,7 @@ void dmax(gb_simplec* S, const Box& b, const double* f, const double* mul, int w
     gb_ctx* ctx = S->ctx;
     const int rows = (b.hi[1] - b.lo[1] + 1) * (b.hi[2] - b.lo[2] + 1);
     Span span(ctx, GB_KERNEL_VECTOR);
-    const int nthr = (b.hi[0] - b.lo[0] + 1) > 128 ? 256 : 128;
-    k_maxabs<<<std::max(1, std::min(rows, 4 * ctx->num_sms)), nthr, 0, ctx->stream>>>(S->g, b, f, mul,
-                                                                                     dword(ctx, word));
+    k_maxabs<<<std::max(1, (rows + 7) / 8), 256, 0, ctx->stream>>>(S->g, b, f, mul, dword(ctx, word));
     ++ctx->launches;
 }
 
@@ -1129,6 +1131,10 @@ gb_status line_solve(gb_simplec* S, int loc, const double* A, const double* ap, 
     gb_ctx* ctx = S->ctx;
     const int64_t vol = volume(S->g);
     cudaMemsetAsync(delta, 0, sizeof(double) * vol, ctx->stream);
+    if (S->opt.line_sweep == 1) {  // steady.sweep = lusgs (FP64 in either precision)
+        return zline_lusgs(ctx, S->g, loc, A, ap, rhs, S->opt.zline_sweeps, S->opt.line_alternate, delta,
+                           dword(ctx, word));
+    }
     if (S->opt.precision == 0) {
         return zline_sweeps<double>(ctx, S->g, loc, A, ap, rhs, S->opt.zline_sweeps, delta, dword(ctx, word),
                                     LineScratch::automatic);
@@ -1540,6 +1546,146 @@ gb_status simplec_local_dtau(gb_simplec* S, const gb_state& q, double cfl, doubl
         dtau[at(g, i, j, k)] = cfl / fmax(rate, 1.0e-12);
     }, GB_KERNEL_COEFS);
     return check_cuda("local_dtau");
+}
+
+// ------------------------------------------------------ initializer ---
+
+namespace {
+
+//! A profile component at every point of a field of type T (the valid box
+//! grown by the state's two ghost layers) at the point's height above its
+//! column's ground floored at h_min; k decays as exp(-(h - zi)/zi) above zi
+//! (Source/Initializer.cpp:14-40 fill_from_profile).
+void fill_from_profile(gb_simplec* S, int t, int f, double h_min, double zi, double* a)
+{
+    const gb_grid g = S->g;
+    const Profile prof = S->prof;
+    const double* z = S->z;
+    const double zinv = 1.0 / std::max(zi, 2.2250738585072014e-308);
+    Box b = valid_box(g, t);
+    for (int d = 0; d < 3; ++d) {
+        b.lo[d] -= 2;
+        b.hi[d] += 2;
+    }
+    for_box(S->ctx, b, [=] __device__(int i, int j, int k) {
+        const double h = fmax(height_above_ground(z, g, t, i, j, k), h_min);
+        double val = prof.value(f, h);
+        if (f == F_TKE && zi > 0) { val *= exp(-(fmax(h - zi, 0.0) * zinv)); }
+        a[at(g, i, j, k)] = val;
+    });
+}
+
+//! w = Omega + z_x u_f + z_y v_f on the valid z-faces (MassFlux.cpp w_from_omega).
+void w_from_omega(gb_simplec* S, const double* u, const double* v, const double* om, double* w)
+{
+    const gb_grid g = S->g;
+    const double* z = S->z;
+    for_box(S->ctx, valid_box(g, ZF), [=] __device__(int i, int j, int k) {
+        w[at(g, i, j, k)] = om[at(g, i, j, k)] + deriv<NODE, ZF, 0>(z, g, i, j, k) * (1.0 / g.dx) * interp<XF, ZF>(u, g, i, j, k)
+                          + deriv<NODE, ZF, 1>(z, g, i, j, k) * (1.0 / g.dy) * interp<YF, ZF>(v, g, i, j, k);
+    }, GB_KERNEL_MASSFLUX);
+}
+
+}  // namespace
+
+gb_status simplec_initialize(gb_simplec* S, const gb_state& q, const gb_init_opts& o, gb_init_result* r)
+{
+    gb_ctx* ctx = S->ctx;
+    const gb_grid g = S->g;
+    const int64_t vol = volume(g);
+    SimplecWork& w = S->w;
+    *r = gb_init_result{};
+    // 1. u, v at every point; w = 0 but the ground faces, which carry no flux
+    fill_from_profile(S, XF, F_U, o.z_agl_min, 0.0, q.u);
+    fill_from_profile(S, YF, F_V, o.z_agl_min, 0.0, q.v);
+    cudaMemsetAsync(q.w, 0, sizeof(double) * vol, ctx->stream);
+    omega_from_w(S, q.u, q.v, q.w, w.om);
+    {
+        double* om = w.om;
+        Box ground = valid_box(g, ZF);
+        ground.hi[2] = 0;
+        for_box(ctx, ground, [=] __device__(int i, int j, int k) { om[at(g, i, j, k)] = 0.0; });
+    }
+    w_from_omega(S, q.u, q.v, w.om, q.w);
+    // 2. k from the profile, theta the sounding (one ghost layer), p' = 0
+    fill_from_profile(S, CC, F_TKE, o.z_agl_min, o.k_decay_height, q.tke);
+    fill_theta_ref(S);
+    cudaMemsetAsync(q.theta, 0, sizeof(double) * vol, ctx->stream);
+    {
+        const double* tr = w.theta_ref;
+        double* th = q.theta;
+        for_box(ctx, Box{{-1, -1, -1}, {g.nx, g.ny, g.nz}}, [=] __device__(int i, int j, int k) {
+            th[at(g, i, j, k)] = tr[at(g, i, j, k)];
+        });
+    }
+    cudaMemsetAsync(q.p, 0, sizeof(double) * vol, ctx->stream);
+    // 3. the mass-consistent correction
+    velocity_divergence(S, q.u, q.v, q.w, w.rhs);
+    dsum(S, valid_box(g, CC), w.rhs, 0, 0);
+    if (o.projection) {
+        if (S->init_poisson != nullptr) {
+            gb_poisson_destroy(S->init_poisson);
+            S->init_poisson = nullptr;
+        }
+        // initializer_poisson_bc (Initializer.cpp:181-195): lambda = 0 on the
+        // inflow and outflow faces, zero flux through the others
+        int32_t pbc[6];
+        for (int f = 0; f < 6; ++f) {
+            const int d = f % 3;
+            const int t = S->bc.face[f];
+            pbc[f] = is_per(g, d) ? GB_POISSON_PERIODIC
+                                  : ((t == GB_FACE_INFLOW || t == GB_FACE_OUTFLOW) ? GB_POISSON_DIRICHLET
+                                                                                     : GB_POISSON_NEUMANN);
+        }
+        gb_poisson_opts po = o.poisson;
+        gb_status st = gb_poisson_create(ctx, &g, pbc, S->z, S->mesh.detJ, &po, &S->init_poisson);
+        if (st != GB_OK) { return st; }
+        const bool unit = (o.alpha_h == 1 && o.alpha_v == 1);
+        const double* beta[3] = {nullptr, nullptr, nullptr};
+        if (!unit) {
+            // Sigma = alpha^2 I on every face (alpha_h = alpha_v)
+            const double a2 = o.alpha_h * o.alpha_h;
+            for (int c = 0; c < 3; ++c) {
+                double* b = w.beta[c];
+                for_box(ctx, Box{{-g.ng, -g.ng, -g.ng}, {g.nx + g.ng, g.ny + g.ng, g.nz + g.ng}},
+                        [=] __device__(int i, int j, int k) { b[at(g, i, j, k)] = a2; });
+                beta[c] = w.beta[c];
+            }
+        }
+        st = poisson_set_coeffs(S->init_poisson, S->mesh.ax, S->mesh.ay, S->mesh.az, beta[0], beta[1], beta[2]);
+        if (st != GB_OK) { return st; }
+        gb_poisson_result pr{};
+        if ((st = poisson_solve(S->init_poisson, w.rhs, w.phi, &pr)) != GB_OK) { return st; }
+        r->poisson_iterations = pr.iterations;
+        r->poisson_final_residual = pr.final_residual;
+        double* F[3] = {w.G[0], w.G[1], w.G[2]};
+        if ((st = poisson_fluxes(S->init_poisson, w.phi, beta[0], beta[1], beta[2], F[0], F[1], F[2])) != GB_OK) {
+            return st;
+        }
+        omega_from_w(S, q.u, q.v, q.w, w.om);
+        double* tgt[3] = {q.u, q.v, w.om};
+        for (int c = 0; c < 3; ++c) {
+            double* tc = tgt[c];
+            const double* fc = F[c];
+            for_box(ctx, valid_box(g, kLoc[c]), [=] __device__(int i, int j, int k) {
+                tc[at(g, i, j, k)] += fc[at(g, i, j, k)];
+            });
+        }
+        {
+            double* f2[2] = {q.u, q.v};
+            const int t2[2] = {XF, YF};
+            fill_periodic_all(S, f2, t2, 2);
+        }
+        w_from_omega(S, q.u, q.v, w.om, q.w);
+        velocity_divergence(S, q.u, q.v, q.w, w.rhs);
+    }
+    dsum(S, valid_box(g, CC), w.rhs, 0, 1);
+    double sums[2];
+    cudaMemcpyAsync(sums, w.sums, sizeof(double) * 2, cudaMemcpyDeviceToHost, ctx->stream);
+    if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) { return check_cuda("initialize_state"); }
+    r->divergence_before = std::sqrt(sums[0]);
+    r->divergence_after = std::sqrt(sums[1]);
+    return check_cuda("initialize_state");
 }
 
 // ----------------------------------------------------------- creation ---

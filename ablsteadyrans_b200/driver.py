@@ -57,12 +57,21 @@ class SteadyCriterion:
         return True
 
 
+def default_cfl_max(line_sweep):
+    """Source/Driver.cpp:133-136 (default_cfl_max): 8 with steady.sweep =
+    lusgs, 10 with zjacobi."""
+    return 8.0 if line_sweep == 1 else 10.0
+
+
 class Driver:
     """Drives one SimplecStage to the steady criterion (steady.* defaults:
-    cfl0 1, cfl_max 10, ser_exponent 1, ser_max_growth 2)."""
+    cfl0 1, cfl_max the sweep's default, ser_exponent 1, ser_max_growth 2)."""
 
-    def __init__(self, stage, cfl0=1.0, cfl_max=10.0, ser_exponent=1.0, growth=2.0, criterion=None):
+    def __init__(self, stage, cfl0=1.0, cfl_max=None, ser_exponent=1.0, growth=2.0, criterion=None):
         self.stage = stage
+        if cfl_max is None:
+            opts = getattr(stage, "options", None)
+            cfl_max = default_cfl_max(getattr(opts, "line_sweep", 0))
         self.cfl0, self.cfl_max, self.p, self.growth = cfl0, cfl_max, ser_exponent, growth
         self.cfl = cfl0
         self.criterion = criterion or SteadyCriterion()

@@ -18,6 +18,9 @@ def _declare(L):
     L.gb_simplec_residual.argtypes = [P, ctypes.POINTER(abi.State), ctypes.POINTER(ctypes.c_void_p)]
     L.gb_simplec_iterate.argtypes = [P, ctypes.POINTER(abi.State), P, ctypes.POINTER(abi.IterInfo)]
     L.gb_local_dtau.argtypes = [P, ctypes.POINTER(abi.State), ctypes.c_double, P]
+    L.gb_init_options_default.argtypes = [ctypes.POINTER(abi.InitOptions)]
+    L.gb_simplec_initialize.argtypes = [P, ctypes.POINTER(abi.State), ctypes.POINTER(abi.InitOptions),
+                                        ctypes.POINTER(abi.InitResult)]
 
 
 FIELDS = ("u", "v", "w", "p", "theta", "tke")
@@ -103,6 +106,16 @@ class SimplecStage:
         st = self.case.state()
         check(self._L.gb_simplec_iterate(self._h, ctypes.byref(st), ctypes.c_void_p(dtau.data_ptr()), ctypes.byref(info)))
         return info
+
+    def initialize(self, options=None):
+        """gust::initialize_state with init.first_guess = profile: the
+        mass-consistent initial state (gb_simplec_initialize) in place."""
+        from . import check
+        o = options if options is not None else abi.InitOptions.make()
+        res = abi.InitResult()
+        st = self.case.state()
+        check(self._L.gb_simplec_initialize(self._h, ctypes.byref(st), ctypes.byref(o), ctypes.byref(res)))
+        return res
 
     def close(self):
         from . import check

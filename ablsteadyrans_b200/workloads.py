@@ -208,7 +208,8 @@ def config1(nx=128, ny=128, nz=64, precision=0, zline_sweeps=4):
 def tile(n, nz, seed, rms=None, ustar=None, z0=None, met=None, dx=30.0, precision=1, zline_sweeps=4):
     """One instance of the batched/served configurations: n x n x nz over
     seeded fractal terrain (|k|^-3, rms uniform 20-150 m unless given), a
-    random wind direction, u* and z0 (seed-derived)."""
+    random wind direction, u* and z0 (seed-derived); inflow on the upwind x
+    and y faces of the wind's quadrant, outflow on the others."""
     rng = np.random.default_rng(1000 + seed)
     rms = rms if rms is not None else rng.uniform(20, 150)
     ustar = ustar if ustar is not None else rng.uniform(0.2, 0.6)
@@ -216,11 +217,11 @@ def tile(n, nz, seed, rms=None, ustar=None, z0=None, met=None, dx=30.0, precisio
     met = met if met is not None else rng.uniform(0, 360)
     direction = (270.0 - met) % 360.0
     zl, _ = geometric_zlevels(nz)
-    g = Grid(n, n, nz, dx, dx, 1500.0 / nz, False, True)
+    g = Grid(n, n, nz, dx, dx, 1500.0 / nz, False, False)
     terrain = fractal_field(n + 1, seed, rms)
     ground = node_ground(g, lambda x, y: float(terrain[int(round(y / dx)) % (n + 1), int(round(x / dx)) % (n + 1)]))
-    bc = abi.BC.make(_faces_for(direction), theta_ref=((0.0, 1500.0), (300.0, 300.0)), ustar=ustar, z0=z0,
-                     direction=direction, kappa=KAPPA, Cmu0=CMU0, l_max=LMAX)
+    bc = abi.BC.make(_faces_for(direction, periodic_y=False), theta_ref=((0.0, 1500.0), (300.0, 300.0)),
+                     ustar=ustar, z0=z0, direction=direction, kappa=KAPPA, Cmu0=CMU0, l_max=LMAX)
     ph = abi.Physics.make(1500.0, gravity=9.81)
     opts = abi.SimplecOptions.make(zline_sweeps=zline_sweeps, precision=precision)
     return Instance(f"tile-{seed}-{n}x{n}x{nz}", g, zl, ground, bc, ph, opts, ustar, z0, direction)

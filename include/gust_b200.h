@@ -126,6 +126,19 @@ gb_status gb_zline_jacobi(gb_ctx* ctx, const gb_grid* g, int32_t loc, const doub
 /* The same in FP32 (the inner solver of the mixed-precision defect correction). */
 gb_status gb_zline_jacobi_f32(gb_ctx* ctx, const gb_grid* g, int32_t loc, const float* A, const float* ap,
                               const float* rhs, int32_t sweeps, float* delta, float* change);
+/* The line LU-SGS solve, replacing gust::zline_lusgs with steady.line_ghosts =
+ * lagged (Source/LineSweeps.H:159-161, Source/LineSweeps.cpp:183-210, 415-428):
+ * `sweeps` symmetric passes of in-place column solves of the system of
+ * gb_zline_jacobi, each column with its x/y neighbours as they stand at that
+ * moment of the pass (forward (+i, +j), backward (-i, -j); with alternate = 1
+ * (steady.line_alternate) the odd sweeps take (+i, -j) then (-i, +j)); before
+ * every pass the periodic ghosts take the images of the pass's starting values
+ * (FillBoundary). delta is set to 0 first; *change receives max |change| over
+ * the last backward pass; the seam copies are synced at the end (the low copy
+ * wins). The GPU walks the wavefront planes (the reference's diagonal order,
+ * which equals its sequential order value for value). FP64. */
+gb_status gb_zline_lusgs(gb_ctx* ctx, const gb_grid* g, int32_t loc, const double* A, const double* ap,
+                         const double* rhs, int32_t sweeps, int32_t alternate, double* delta, double* change);
 /* The FP64 z-line Jacobi solve of gb_zline_jacobi for a caller that must not
  * allocate device memory. This entry point has no counterpart in the
  * reference; it exists for hosts that cannot let a library allocate: one that
@@ -285,6 +298,8 @@ typedef struct gb_simplec_opts {
     int32_t zline_sweeps;            /* steady.zline_sweeps */
     int32_t precision;               /* 0 plain FP64; 1 FP32 inner solves (sweeps, multigrid) in FP64 defect correction */
     gb_poisson_opts poisson;         /* the correction's Poisson solver (reltol taken from pressure_reltol) */
+    int32_t line_sweep;              /* steady.sweep: 0 zjacobi (z-line Jacobi), 1 lusgs (line LU-SGS, FP64) */
+    int32_t line_alternate;          /* steady.line_alternate (lusgs): 1 = odd sweeps j-reversed */
 } gb_simplec_opts;
 
 /* The solution fields (gust::State, Source/State.H:18-36): device arrays of
@@ -316,6 +331,24 @@ typedef struct gb_iter_info {
     int64_t tke_clipped;
 } gb_iter_info;
 
+/* init.* of the mass-consistent initializer (gust::InitOptions,
+ * Source/Initializer.H:63-111) with init.first_guess = profile. */
+typedef struct gb_init_opts {
+    double z_agl_min;                /* init.z_agl_min (m, >= 0): floor of the profile's height */
+    double alpha_h, alpha_v;         /* init.alpha_h, init.alpha_v (> 0); alpha_v != alpha_h is not built */
+    double k_decay_height;           /* init.k_decay_height (m, >= 0; 0: no decay) */
+    int32_t projection;              /* init.projection (0 or 1) */
+    int32_t obrien;                  /* init.obrien (must be 0: the O'Brien column correction is not built) */
+    gb_poisson_opts poisson;         /* solver.poisson_* of the projection */
+} gb_init_opts;
+
+/* What the initializer reports (gust::InitResult). */
+typedef struct gb_init_result {
+    double divergence_before, divergence_after;   /* L2 norms of the velocity divergence (1/s) */
+    int32_t poisson_iterations;
+    double poisson_final_residual;
+} gb_init_result;
+
 typedef struct gb_simplec gb_simplec;
 
 /* gust::SimplecStage (Source/Simplec.H:185-263) for one instance: the
@@ -339,6 +372,20 @@ gb_status gb_simplec_residual(gb_simplec* s, const gb_state* q, double* const* R
 /* SimplecStage::iterate (Source/Simplec.cpp:452-506): one SIMPLEC outer
  * iteration of q with the local pseudo-time step dtau (cells). */
 gb_status gb_simplec_iterate(gb_simplec* s, const gb_state* q, const double* dtau, gb_iter_info* info);
+
+/* The defaults of init.* (Source/Initializer.H: z_agl_min 0, alpha_h = alpha_v
+ * = 1, k_decay_height 0, projection 1, obrien 0) and solver.poisson_*. */
+gb_status gb_init_options_default(gb_init_opts* o);
+/* gust::initialize_state with init.first_guess = profile (Source/Initializer.cpp:
+ * 281-332 first_guess_state, 344-430 the projection), on the stage's mesh and
+ * boundary conditions: u, v from the inflow profile at every point's height
+ * above the ground (ghosts included), w = 0 but the ground faces' kinematic w,
+ * theta = theta_ref(z), k from the profile (decaying above k_decay_height),
+ * p = 0; then, with projection = 1, the mass-consistent correction: the
+ * divergence removed by the terrain Poisson solve with lambda = 0 on the
+ * inflow and outflow faces and zero flux through the others (u, v, Omega +=
+ * the fluxes, w from Omega). */
+gb_status gb_simplec_initialize(gb_simplec* s, const gb_state* q, const gb_init_opts* o, gb_init_result* r);
 
 /* gust::local_dtau (Source/PseudoTime.H:32-33) with the stage's diffusivity nu. */
 gb_status gb_local_dtau(gb_simplec* s, const gb_state* q, double cfl, double* dtau);

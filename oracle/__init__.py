@@ -48,6 +48,8 @@ def _declare(L):
     L.og_override_sync.argtypes = [G, i32, P]
     L.og_zline_jacobi.argtypes = [G, i32, P, P, P, i32, P]
     L.og_zline_jacobi.restype = f64
+    L.og_zline_lusgs.argtypes = [G, i32, P, P, P, i32, i32, i32, P]
+    L.og_zline_lusgs.restype = f64
     # mesh and Poisson layer
     I = ctypes.POINTER(ctypes.c_int)
     L.og_btf_heights.argtypes = [G, P, P, P]
@@ -94,6 +96,14 @@ def fill_periodic(grid, loc, f, layers=1):
 def zline_jacobi(grid, loc, A, ap, rhs, sweeps, delta):
     """Source/Predictor.cpp:87-127 restated; returns the last sweep's change."""
     return float(lib().og_zline_jacobi(ctypes.byref(grid.c), loc, _p(A), _p(ap), _p(rhs), int(sweeps), _p(delta)))
+
+
+def zline_lusgs(grid, loc, A, ap, rhs, sweeps, delta, order=0, alternate=0):
+    """Source/LineSweeps.cpp:183-210, 415-428 restated (line_ghosts =
+    lagged): order 0 sequential, 1 diagonal wavefronts; returns the last
+    backward pass's change."""
+    return float(lib().og_zline_lusgs(ctypes.byref(grid.c), loc, _p(A), _p(ap), _p(rhs), int(sweeps), int(order),
+                                      int(alternate), _p(delta)))
 
 
 # ------------------------------------------------------------ mesh / Poisson
@@ -200,6 +210,10 @@ def _declare_simplec(L):
                                      ctypes.POINTER(State), ctypes.POINTER(MeshFields), ctypes.POINTER(Diffusivities),
                                      P, PP, ctypes.POINTER(IterInfo)]
     L.og_simplec_iterate.restype = i32
+    from ablsteadyrans_b200.abi import InitOptions
+    L.og_initialize.argtypes = [G, ctypes.POINTER(BC), ctypes.POINTER(InitOptions), ctypes.POINTER(State),
+                                ctypes.POINTER(MeshFields), P]
+    L.og_initialize.restype = i32
     L.og_local_dtau.argtypes = [G, P, P, P, P, P, P, f64, P]
     L.og_transport_fluxes.argtypes = [G, P, P, P, P, P, P, P, P, P]
     L.og_velocity_divergence.argtypes = [G, P, P, P, P, P, P, P, P, P]
@@ -287,6 +301,17 @@ def simplec_iterate(case, bc, phys, opts, dtau):
     return int(rc), info, R
 
 
+def initialize(case, bc, init_opts):
+    """gust::initialize_state with init.first_guess = profile
+    (Source/Initializer.cpp:281-430) on the case's state; returns (status,
+    [divergence before, after, Poisson iterations, final residual])."""
+    info = np.zeros(4)
+    st, m = case.state(), case.mesh()
+    rc = _L().og_initialize(ctypes.byref(case.grid.c), ctypes.byref(bc), ctypes.byref(init_opts), ctypes.byref(st),
+                            ctypes.byref(m), _p(info))
+    return int(rc), info
+
+
 def transport_fluxes(grid, u, v, w, z, ax, ay):
     F = [grid.np_zeros() for _ in range(3)]
     _L().og_transport_fluxes(ctypes.byref(grid.c), _p(u), _p(v), _p(w), _p(z), _p(ax), _p(ay), *[_p(f) for f in F])
@@ -309,3 +334,10 @@ def velocity_divergence(grid, u, v, w, z, ax, ay, az, J):
     d = grid.np_zeros()
     _L().og_velocity_divergence(ctypes.byref(grid.c), _p(u), _p(v), _p(w), _p(z), _p(ax), _p(ay), _p(az), _p(J), _p(d))
     return d
+
+
+def omega_from_w(grid, u, v, w, z):
+    """MassFlux.cpp omega_from_w on the valid z-faces."""
+    om = grid.np_zeros()
+    _L().og_omega_from_w(ctypes.byref(grid.c), _p(u), _p(v), _p(w), _p(z), _p(om), 0)
+    return om

@@ -158,3 +158,84 @@ double og_zline_jacobi(const og_grid* g, int loc, const double* A, const double*
     free(next);
     return change;
 }
+
+/* ------------------------------------------------------------------ */
+/* line LU-SGS                                                         */
+/* ------------------------------------------------------------------ */
+
+/* One pass of the line LU-SGS sweep over the columns of the valid box, in
+ * place (Source/LineSweeps.cpp:38-171): forward = (+i, +j) or, j-reversed,
+ * (+i, -j); backward the opposite pair. order 0 walks the columns
+ * sequentially (j outer, i inner), order 1 the wavefront planes
+ * (i - ilo) + (j - jlo) = s (or (i - ilo) + (jhi - j) = s reversed), one
+ * column after another inside a plane: the two orders give the same values. */
+static void lusgs_pass(const og_grid* g, int ni, int nj, int nk, const double* A, int64_t cs, const double* ap,
+                       const double* rhs, double* d, double* c, double* e, int forward, int jrev, int order)
+{
+    if (order == 0) {
+        if (forward) {
+            for (int jj = 0; jj < nj; ++jj) {
+                const int j = jrev ? nj - 1 - jj : jj;
+                for (int i = 0; i < ni; ++i) { solve_column(g, A, cs, ap, rhs, d, c, e, d, i, j, 0, nk - 1); }
+            }
+        } else {
+            for (int jj = nj - 1; jj >= 0; --jj) {
+                const int j = jrev ? nj - 1 - jj : jj;
+                for (int i = ni - 1; i >= 0; --i) { solve_column(g, A, cs, ap, rhs, d, c, e, d, i, j, 0, nk - 1); }
+            }
+        }
+        return;
+    }
+    const int last = ni + nj - 2;
+    for (int q = 0; q <= last; ++q) {
+        const int s = forward ? q : last - q;
+        const int amin = (s - (nj - 1) > 0) ? s - (nj - 1) : 0;
+        const int amax = (s < ni - 1) ? s : ni - 1;
+        for (int ia = amin; ia <= amax; ++ia) {
+            const int jb = s - ia;
+            const int j = jrev ? nj - 1 - jb : jb;
+            solve_column(g, A, cs, ap, rhs, d, c, e, d, ia, j, 0, nk - 1);
+        }
+    }
+}
+
+/* Source/LineSweeps.cpp:183-210 (lusgs_lagged) with check_line_system's
+ * delta.setVal(0) and zline_lusgs's dispatch (:415-428): `sweeps` symmetric
+ * passes; before every pass FillBoundary copies the periodic images of the
+ * pass's starting values into the ghosts; with alternate the odd sweeps take
+ * the j-reversed pair; the change is max |delta| change over the last
+ * backward pass (valid points); OverrideSync at the end. */
+double og_zline_lusgs(const og_grid* g, int loc, const double* A, const double* ap, const double* rhs, int sweeps,
+                      int order, int alternate, double* delta)
+{
+    const int64_t vol = VOL(g);
+    double* c = (double*)calloc((size_t)vol, sizeof(double));
+    double* e = (double*)calloc((size_t)vol, sizeof(double));
+    double* before = (double*)calloc((size_t)vol, sizeof(double));
+    const int ni = g->nx + nodal(loc, 0), nj = g->ny + nodal(loc, 1), nk = g->nz + nodal(loc, 2);
+    memset(delta, 0, sizeof(double) * (size_t)vol);
+    double change = 0;
+    for (int s = 0; s < sweeps; ++s) {
+        for (int forward = 1; forward >= 0; --forward) {
+            if (s == sweeps - 1 && !forward) { memcpy(before, delta, sizeof(double) * (size_t)vol); }
+            fill_periodic(g, loc, delta, 1);
+            lusgs_pass(g, ni, nj, nk, A, vol, ap, rhs, delta, c, e, forward, alternate && (s % 2 == 1), order);
+        }
+        if (s == sweeps - 1) {
+            change = 0;
+            for (int k = 0; k < nk; ++k) {
+                for (int j = 0; j < nj; ++j) {
+                    for (int i = 0; i < ni; ++i) {
+                        const double dd = fabs(before[IX(g, i, j, k)] - delta[IX(g, i, j, k)]);
+                        if (dd > change || dd != dd) { change = dd; }
+                    }
+                }
+            }
+        }
+    }
+    override_sync(g, loc, delta);
+    free(c);
+    free(e);
+    free(before);
+    return change;
+}

@@ -49,6 +49,8 @@ void og_implicit_coefficients(const og_grid* g, int C, const double* F0, const d
 void og_face_dtau(const og_grid* g, double* dc, double* fx, double* fy, double* fz);
 double og_zline_jacobi(const og_grid* g, int loc, const double* A, const double* ap, const double* rhs, int sweeps,
                        double* delta);
+double og_zline_lusgs(const og_grid* g, int loc, const double* A, const double* ap, const double* rhs, int sweeps,
+                      int order, int alternate, double* delta);
 void og_poisson_fluxes(const og_grid* g, const int* bc, const double* z, double* phi, const double* bx,
                        const double* by, const double* bz, double* fx, double* fy, double* fz);
 typedef struct og_mg og_mg;
@@ -604,6 +606,16 @@ void og_implicit_rows(const og_grid* g, const gb_bc* bc, const gb_physics* ph, i
 
 /* Predictor.cpp:129-405 momentum_predictor (zjacobi sweeps). ap/d: the
  * predictor fields a_P, d per component (face arrays). */
+/* The line solver of the sweeps (steady.sweep, Source/Predictor.H:257-259
+ * line_sweeps): z-line Jacobi, or line LU-SGS (lagged ghosts, sequential
+ * order) with steady.line_alternate. */
+static double line_solve(const og_grid* g, const gb_simplec_opts* so, int loc, const double* A, const double* ap,
+                         const double* rhs, double* delta)
+{
+    if (so->line_sweep == 1) { return og_zline_lusgs(g, loc, A, ap, rhs, so->zline_sweeps, 0, so->line_alternate, delta); }
+    return og_zline_jacobi(g, loc, A, ap, rhs, so->zline_sweeps, delta);
+}
+
 void og_momentum_predictor(const og_grid* g, const gb_bc* bc, const gb_physics* ph, const gb_simplec_opts* so,
                            gb_state* q, double** R, const double* F0, const double* F1, const double* F2,
                            double** dtau_f, const gb_mesh_fields* m, const gb_diffusivities* df, double** ap,
@@ -746,7 +758,7 @@ void og_momentum_predictor(const og_grid* g, const gb_bc* bc, const gb_physics* 
             }
             free(At);
         }
-        info[3 + c] = og_zline_jacobi(g, t, A, ap[c], rhs, so->zline_sweeps, delta);
+        info[3 + c] = line_solve(g, so, t, A, ap[c], rhs, delta);
         double mx = 0;
         for (int k = 0; k < nk; ++k) {
             for (int j = 0; j < nj; ++j) {
@@ -931,7 +943,7 @@ double og_scalar_sweep(const og_grid* g, const gb_bc* bc, const gb_physics* ph, 
             }
         }
     }
-    *last = og_zline_jacobi(g, CC, A, ap, rhs, so->zline_sweeps, delta);
+    *last = line_solve(g, so, CC, A, ap, rhs, delta);
     double mx = 0;
     int64_t n = 0;
     for (int k = 0; k < g->nz; ++k) {
@@ -1057,4 +1069,136 @@ int og_simplec_iterate(const og_grid* g, const gb_bc* bc, const gb_physics* ph, 
     free(conv0);
     free(conv1);
     return st;
+}
+
+/* ------------------------------------------------------------------ */
+/* mass-consistent initializer                                         */
+/* ------------------------------------------------------------------ */
+
+/* A profile component at every point of a field of type t (the valid box
+ * grown by the state's two ghost layers) at the point's height above its
+ * column's ground floored at h_min; k decays as exp(-(h - zi)/zi) above zi
+ * (Source/Initializer.cpp:14-40 fill_from_profile). */
+static void fill_from_profile(const og_grid* g, const gb_bc* bc, int t, int f, double h_min, double zi, const double* z,
+                              double* a)
+{
+    const double zinv = 1.0 / fmax(zi, 2.2250738585072014e-308);
+    for (int k = -2; k <= ext(g, t, 2) + 1; ++k) {
+        for (int j = -2; j <= ext(g, t, 1) + 1; ++j) {
+            for (int i = -2; i <= ext(g, t, 0) + 1; ++i) {
+                const double h = fmax(height_above_ground(g, z, t, i, j, k), h_min);
+                double val = profile_value(bc, f, h);
+                if (f == F_TKE && zi > 0) { val *= exp(-(fmax(h - zi, 0.0) * zinv)); }
+                a[IX(g, i, j, k)] = val;
+            }
+        }
+    }
+}
+
+static double norm2_valid(const og_grid* g, const double* f)
+{
+    double s = 0;
+    for (int k = 0; k < g->nz; ++k) {
+        for (int j = 0; j < g->ny; ++j) {
+            for (int i = 0; i < g->nx; ++i) { s += f[IX(g, i, j, k)] * f[IX(g, i, j, k)]; }
+        }
+    }
+    return sqrt(s);
+}
+
+/* initializer_poisson_bc (Source/Initializer.cpp:181-195): periodic where
+ * the geometry is; lambda = 0 (Dirichlet) on the inflow and outflow faces;
+ * zero flux elsewhere. */
+static void init_poisson_bc(const og_grid* g, const gb_bc* bc, int* pbc)
+{
+    for (int f = 0; f < 6; ++f) {
+        const int d = f % 3;
+        if (is_per(g, d)) { pbc[f] = 0; }
+        else { pbc[f] = (bc->face[f] == GB_FACE_INFLOW || bc->face[f] == GB_FACE_OUTFLOW) ? 2 : 1; }
+    }
+}
+
+/* gust::initialize_state with init.first_guess = profile and no O'Brien
+ * correction (Source/Initializer.cpp:281-332 first_guess_state, 344-430):
+ * the first guess, then with projection the mass-consistent correction
+ * with Sigma = alpha^2 I (alpha_h = alpha_v). info: [divergence before,
+ * divergence after, Poisson iterations, final Poisson residual]. Returns 0,
+ * or -2 on a Poisson failure. */
+int og_initialize(const og_grid* g, const gb_bc* bc, const gb_init_opts* io, gb_state* q, const gb_mesh_fields* m,
+                  double* info)
+{
+    const int64_t vol = VOL(g);
+    const double* z = q->z_nd;
+    /* 1. u, v at every point; w = 0 but the ground faces, which carry no flux */
+    fill_from_profile(g, bc, XF, F_U, io->z_agl_min, 0.0, z, q->u);
+    fill_from_profile(g, bc, YF, F_V, io->z_agl_min, 0.0, z, q->v);
+    memset(q->w, 0, sizeof(double) * (size_t)vol);
+    double* om = zalloc(g);
+    og_omega_from_w(g, q->u, q->v, q->w, z, om, 0);
+    for (int j = 0; j < g->ny; ++j) {
+        for (int i = 0; i < g->nx; ++i) { om[IX(g, i, j, 0)] = 0; }
+    }
+    og_w_from_omega(g, q->u, q->v, om, z, q->w);
+    /* 2. k from the profile, theta the sounding (one ghost layer), p' = 0 */
+    fill_from_profile(g, bc, CC, F_TKE, io->z_agl_min, io->k_decay_height, z, q->tke);
+    memset(q->theta, 0, sizeof(double) * (size_t)vol);
+    fill_theta_ref(g, bc, z, q->theta);
+    memset(q->p, 0, sizeof(double) * (size_t)vol);
+    info[0] = info[1] = info[2] = info[3] = 0;
+    int status = 0;
+    double* rhs = zalloc(g);
+    og_velocity_divergence(g, q->u, q->v, q->w, z, m->ax, m->ay, m->az, m->detJ, rhs);
+    info[0] = info[1] = norm2_valid(g, rhs);
+    if (io->projection) {
+        int pbc[6];
+        init_poisson_bc(g, bc, pbc);
+        const double a2 = io->alpha_h * io->alpha_h;
+        const int unit = (io->alpha_h == 1 && io->alpha_v == 1);
+        double* beta = zalloc(g);
+        for (int64_t n = 0; n < vol; ++n) { beta[n] = a2; }
+        double* AX = zalloc(g);
+        double* AY = zalloc(g);
+        double* AZ = zalloc(g);
+        for (int64_t n = 0; n < vol; ++n) {
+            AX[n] = unit ? m->ax[n] : m->ax[n] * a2;
+            AY[n] = unit ? m->ay[n] : m->ay[n] * a2;
+            AZ[n] = unit ? m->az[n] : m->az[n] * a2;
+        }
+        const gb_poisson_opts* po = &io->poisson;
+        og_mg* mg = og_mg_create(g, pbc, z, m->detJ, AX, AY, AZ, po->max_levels, po->min_coarse, po->nu1, po->nu2,
+                                 po->nu_coarse);
+        double* lam = zalloc(g);
+        double res[3];
+        const int it = og_poisson_solve(mg, rhs, lam, po->reltol, po->abstol, po->max_iter, po->restart, 1, res);
+        og_mg_destroy(mg);
+        if (it < 0) { status = -2; }
+        info[2] = it;
+        info[3] = res[1];
+        double* F[3] = {zalloc(g), zalloc(g), zalloc(g)};
+        og_poisson_fluxes(g, pbc, z, lam, unit ? NULL : beta, unit ? NULL : beta, unit ? NULL : beta, F[0], F[1], F[2]);
+        og_omega_from_w(g, q->u, q->v, q->w, z, om, 0);
+        double* tgt[3] = {q->u, q->v, om};
+        const int tt[3] = {XF, YF, ZF};
+        for (int c = 0; c < 3; ++c) {
+            for (int k = 0; k < ext(g, tt[c], 2); ++k) {
+                for (int j = 0; j < ext(g, tt[c], 1); ++j) {
+                    for (int i = 0; i < ext(g, tt[c], 0); ++i) { tgt[c][IX(g, i, j, k)] += F[c][IX(g, i, j, k)]; }
+                }
+            }
+        }
+        fill_periodic2(g, XF, q->u);
+        fill_periodic2(g, YF, q->v);
+        og_w_from_omega(g, q->u, q->v, om, z, q->w);
+        og_velocity_divergence(g, q->u, q->v, q->w, z, m->ax, m->ay, m->az, m->detJ, rhs);
+        info[1] = norm2_valid(g, rhs);
+        for (int c = 0; c < 3; ++c) { free(F[c]); }
+        free(beta);
+        free(AX);
+        free(AY);
+        free(AZ);
+        free(lam);
+    }
+    free(rhs);
+    free(om);
+    return status;
 }

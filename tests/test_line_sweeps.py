@@ -119,3 +119,76 @@ def test_gpu_zline_jacobi_refusals(ctx):
         gb.zline_jacobi(ctx, g, 0, z, z[0], z[0], 0, z[1])
     with pytest.raises(gb.GustError, match="loc must be"):
         gb.zline_jacobi(ctx, g, 3, z, z[0], z[0], 1, z[1])
+
+
+# ------------------------------------------------------------------ LU-SGS
+# gust::zline_lusgs (Source/LineSweeps.cpp:38-428) with line_ghosts = lagged.
+
+@pytest.mark.parametrize("loc", LOCS)
+@pytest.mark.parametrize("alternate", [0, 1])
+@pytest.mark.parametrize("case", CASES)
+def test_oracle_lusgs_diagonal_equals_sequential(loc, alternate, case):
+    """The wavefront order performs the sequential order's operations on the
+    same values: bit-identical results (the reference's
+    LineSweeps.DiagonalOrderingEqualsTheSequentialSweep, test_LineSweeps.cpp:483)."""
+    nx, ny, nz, px, py = case
+    g = Grid(nx, ny, nz, 30.0, 30.0, 10.0, px, py)
+    A, ap, rhs = random_system(g, loc, seed=21 + loc, extra=0.3)
+    d0, d1 = g.np_zeros(), g.np_zeros()
+    c0 = oracle.zline_lusgs(g, loc, A, ap, rhs, 3, d0, order=0, alternate=alternate)
+    c1 = oracle.zline_lusgs(g, loc, A, ap, rhs, 3, d1, order=1, alternate=alternate)
+    assert np.array_equal(d0, d1) and c0 == c1
+
+
+@pytest.mark.parametrize("loc", LOCS)
+@pytest.mark.parametrize("case", CASES)
+def test_oracle_lusgs_converges_to_dense_solve(loc, case):
+    """Symmetric line Gauss-Seidel converges to the same system's dense solve,
+    in fewer sweeps than the z-line Jacobi iteration."""
+    nx, ny, nz, px, py = case
+    g = Grid(nx, ny, nz, 30.0, 30.0, 10.0, px, py)
+    A, ap, rhs = random_system(g, loc, seed=7 + loc, extra=0.3)
+    exact = dense_line_system_solve(g, loc, A, ap, rhs)
+    scale = np.abs(exact).max()
+    v = g.valid(loc)
+    d = g.np_zeros()
+    change = oracle.zline_lusgs(g, loc, A, ap, rhs, 200, d)
+    assert np.abs(d - exact)[v].max() / scale < 1e-12
+    assert change / scale < 1e-12
+    dl, dj = g.np_zeros(), g.np_zeros()
+    oracle.zline_lusgs(g, loc, A, ap, rhs, 4, dl)
+    oracle.zline_jacobi(g, loc, A, ap, rhs, 8, dj)
+    assert np.abs(dl - exact)[v].max() <= np.abs(dj - exact)[v].max() * (1 + 1e-12)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("loc", LOCS)
+@pytest.mark.parametrize("case", CASES + [(37, 29, 17, True, False), (24, 40, 33, False, True)])
+@pytest.mark.parametrize("alternate", [0, 1])
+def test_gpu_zline_lusgs_matches_oracle(ctx, loc, case, alternate):
+    import torch
+    import ablsteadyrans_b200 as gb
+    nx, ny, nz, px, py = case
+    g = Grid(nx, ny, nz, 30.0, 30.0, 10.0, px, py)
+    A, ap, rhs = random_system(g, loc, seed=31 + 3 * loc + alternate, extra=0.2, xscale=3.0)
+    d_ref = g.np_zeros()
+    ch_ref = oracle.zline_lusgs(g, loc, A, ap, rhs, 3, d_ref, alternate=alternate)
+    dd = torch.full(g.shape, 7.0, dtype=torch.float64, device="cuda")  # overwritten: delta starts at 0
+    ch = gb.zline_lusgs(ctx, g, loc, to_dev(A), to_dev(ap), to_dev(rhs), 3, dd, alternate=alternate)
+    d = to_host(dd)
+    assert rel_err(d, d_ref, g.valid(loc)) < 1e-12
+    assert abs(ch - ch_ref) <= 1e-11 * max(abs(ch_ref), 1e-300)
+    G = g.ng
+    assert np.all(d[:G] == 0)
+
+
+@pytest.mark.gpu
+def test_gpu_zline_lusgs_refusals(ctx):
+    import torch
+    import ablsteadyrans_b200 as gb
+    g = Grid(4, 4, 4, 1.0, 1.0, 1.0)
+    z = torch.zeros((7,) + g.shape, dtype=torch.float64, device="cuda")
+    with pytest.raises(gb.GustError, match="sweeps must be >= 1"):
+        gb.zline_lusgs(ctx, g, 0, z, z[0], z[0], 0, z[1])
+    with pytest.raises(gb.GustError, match="steady.line_alternate = 2"):
+        gb.zline_lusgs(ctx, g, 0, z, z[0], z[0], 1, z[1], alternate=2)

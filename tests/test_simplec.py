@@ -131,3 +131,58 @@ def test_driver_ser_law():
     assert ser_cfl(8.0, 0.01, 1.0, 10.0, 1.0, 2.0) == 10.0
     assert ser_cfl(4.0, 0.2, 1.0, 10.0, 1.0, 2.0) == pytest.approx(5.0)
     assert ser_cfl(4.0, 0.2, 1.0, 10.0, 0.0, 2.0) == 1.0
+
+
+# ----------------------------------------------------- mass-consistent init
+# gust::initialize_state with init.first_guess = profile (Source/Initializer.cpp).
+
+INIT_FACES = {
+    "periodic": (True, True, (0, 0, 4, 0, 0, 3)),
+    "inflow_x": (False, True, (1, 0, 4, 2, 0, 3)),
+}
+
+
+def _init_case(name, seed=3):
+    from ablsteadyrans_b200.abi import BC
+    from helpers import terrain_simplec_case
+    px, py, faces = INIT_FACES[name]
+    case = terrain_simplec_case(20, 14, 10, px, py, seed=seed)
+    bc = BC.make(faces, theta_ref=((0.0, 500.0, 1500.0), (300.0, 301.5, 305.0)), ustar=0.4, z0=0.1)
+    return case, bc
+
+
+@pytest.mark.parametrize("name", list(INIT_FACES))
+def test_oracle_initializer_is_mass_consistent(name):
+    """The projection removes the first guess's divergence (Mass_Consistent_*:
+    divergence after at most solver.poisson_reltol times before, Tests/
+    Initialization/Mass_Consistent_Askervein/README.md); theta is the
+    sounding, p' = 0, k > 0, and the ground faces carry no flux."""
+    from ablsteadyrans_b200.abi import InitOptions
+    case, bc = _init_case(name)
+    io = InitOptions.make()
+    io.poisson.reltol = 1e-11
+    rc, info = oracle.initialize(case, bc, io)
+    assert rc == 0
+    before, after, iters = info[0], info[1], info[2]
+    assert before > 1e-3 and after <= 1e-10 * before
+    assert 1 <= iters <= 30
+    g = case.grid
+    v = g.valid(0)
+    assert np.all(case.q["p"] == 0)
+    assert np.all(case.q["tke"][v] > 0)
+    assert np.all((case.q["theta"][v] >= 300.0) & (case.q["theta"][v] <= 305.0))
+    # no flux through the ground: Omega = 0 on the ground faces
+    om = oracle.omega_from_w(g, case.q["u"], case.q["v"], case.q["w"], case.z)
+    G = g.ng
+    assert np.abs(om[G, G:G + g.ny, G:G + g.nx]).max() <= 1e-12 * np.abs(case.q["u"]).max()
+
+
+def test_oracle_initializer_projection_off_keeps_the_first_guess():
+    from ablsteadyrans_b200.abi import InitOptions
+    case, bc = _init_case("inflow_x")
+    rc, info = oracle.initialize(case, bc, InitOptions.make(projection=0))
+    assert rc == 0 and info[0] == info[1] and info[2] == 0
+    # w is 0 above the ground faces
+    g = case.grid
+    G = g.ng
+    assert np.all(case.q["w"][G + 1:G + g.nz + 1, G:G + g.ny, G:G + g.nx] == 0)

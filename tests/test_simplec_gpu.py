@@ -77,14 +77,18 @@ def test_gpu_residual_matches_oracle(ctx, name, opts):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("sweep", [(0, 0), (1, 1)], ids=["zjacobi", "lusgs-alternate"])
 @pytest.mark.parametrize("name", list(CONFIGS))
-def test_gpu_iterations_match_oracle(ctx, name):
+def test_gpu_iterations_match_oracle(ctx, name, sweep):
     """Three SIMPLEC iterations (gravity, Coriolis, VNN cap on) agree with the
-    oracle's to 1e-9 relative per field (the Poisson solves to 1e-11)."""
+    oracle's to 1e-9 relative per field (the Poisson solves to 1e-11), with
+    z-line Jacobi sweeps and with line LU-SGS sweeps (steady.sweep = lusgs,
+    steady.line_alternate = 1)."""
     from ablsteadyrans_b200.simplec import DeviceCase, SimplecStage
     case, bc = make(name, seed=5)
     ph = physics(case, coriolis=1, latitude=40.0, geostrophic=1, ug=7.0, vg=-1.0)
-    opts = SimplecOptions.make(pressure_reltol=1e-11, zline_sweeps=3, w_vnn_cap=16.0, tke_floor=1e-3)
+    opts = SimplecOptions.make(pressure_reltol=1e-11, zline_sweeps=3, w_vnn_cap=16.0, tke_floor=1e-3,
+                               line_sweep=sweep[0], line_alternate=sweep[1])
     oracle.fill_ghosts(case, bc)
     dc = DeviceCase.from_oracle(case)
     st = SimplecStage(ctx, dc, bc, ph, opts)
@@ -162,3 +166,68 @@ def test_gpu_mixed_precision_tracks_fp64(ctx):
         v = case.grid.valid(loc)
         a, b = runs[1][f][v], runs[0][f][v]
         assert np.abs(a - b).max() <= 1e-4 * np.abs(b).max(), f
+
+
+@pytest.mark.gpu
+def test_gpu_line_sweep_option_refusals(ctx):
+    """steady.sweep / steady.line_alternate checks with the reference's
+    messages (Source/Driver.cpp:99-118)."""
+    import ablsteadyrans_b200 as gb
+    from ablsteadyrans_b200.simplec import DeviceCase, SimplecStage
+    case, bc = make(list(CONFIGS)[0], seed=5)
+    ph = physics(case)
+    oracle.fill_ghosts(case, bc)
+    dc = DeviceCase.from_oracle(case)
+    for kw, msg in (({"line_sweep": 2}, "steady.sweep = 2"),
+                    ({"line_alternate": 1}, "has no effect unless steady.sweep = lusgs"),
+                    ({"line_sweep": 1, "line_alternate": 1, "zline_sweeps": 1}, "needs steady.zline_sweeps >= 2")):
+        with pytest.raises(gb.GustError, match=msg):
+            SimplecStage(ctx, dc, bc, ph, SimplecOptions.make(**kw))
+
+
+# ----------------------------------------------------- mass-consistent init
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("alpha", [1.0, 0.5])
+@pytest.mark.parametrize("name", list(CONFIGS))
+def test_gpu_initializer_matches_oracle(ctx, name, alpha):
+    """gust::initialize_state (init.first_guess = profile, projection on) on
+    the B200 against the oracle: every field to 1e-9 relative (the
+    projections to 1e-11), the divergence removed, the same iteration count;
+    alpha_h = alpha_v = alpha (Sigma = alpha^2 I)."""
+    from ablsteadyrans_b200.abi import InitOptions
+    from ablsteadyrans_b200.simplec import DeviceCase, SimplecStage
+    case, bc = make(name, seed=5)
+    ph = physics(case)
+    dc = DeviceCase.from_oracle(case)
+    st = SimplecStage(ctx, dc, bc, ph, SimplecOptions.make())
+    io = InitOptions.make(alpha_h=alpha, alpha_v=alpha, k_decay_height=600.0, z_agl_min=1.0)
+    io.poisson.reltol = 1e-11
+    rc, info = oracle.initialize(case, bc, io)
+    assert rc == 0
+    res = st.initialize(io)
+    assert res.divergence_before == pytest.approx(info[0], rel=1e-11)
+    assert res.divergence_after <= 1e-10 * res.divergence_before
+    assert res.poisson_iterations == int(info[2])
+    for f, loc in zip(FIELDS, LOCS):
+        ref = case.q[f]
+        got = dc.host(f)
+        scale = max(np.abs(ref).max(), 1e-300)
+        # every point the initializer writes, ghosts included
+        assert np.abs(got - ref).max() <= 1e-9 * scale, (f, np.abs(got - ref).max() / scale)
+    st.close()
+
+
+@pytest.mark.gpu
+def test_gpu_initializer_refusals(ctx):
+    import ablsteadyrans_b200 as gb
+    from ablsteadyrans_b200.abi import InitOptions
+    from ablsteadyrans_b200.simplec import DeviceCase, SimplecStage
+    case, bc = make(list(CONFIGS)[0], seed=5)
+    dc = DeviceCase.from_oracle(case)
+    st = SimplecStage(ctx, dc, bc, physics(case), SimplecOptions.make())
+    for kw, msg in (({"alpha_v": 0.5}, "split z-face coefficient"), ({"obrien": 1}, "init.obrien = 1"),
+                    ({"z_agl_min": -1.0}, "init.z_agl_min"), ({"alpha_h": 0.0, "alpha_v": 0.0}, "init.alpha_h")):
+        with pytest.raises(gb.GustError, match=msg):
+            st.initialize(InitOptions.make(**kw))
+    st.close()
