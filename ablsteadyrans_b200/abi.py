@@ -160,3 +160,22 @@ class IterInfo(ctypes.Structure):
 def np_ptr(a):
     assert a.dtype == np.float64 and a.flags["C_CONTIGUOUS"]
     return a.ctypes.data
+
+
+class DriverOptions(ctypes.Structure):
+    """gb_driver_opts: steady.* of the pseudo-time driver and the criterion."""
+    _fields_ = [("cfl0", ctypes.c_double), ("cfl_max", ctypes.c_double), ("ser_exponent", ctypes.c_double),
+                ("ser_max_growth", ctypes.c_double), ("residual_tol", ctypes.c_double),
+                ("residual_drop_orders", ctypes.c_double), ("residual_ref_iterations", ctypes.c_int32)]
+
+    @classmethod
+    def make(cls, line_sweep=0, **kw):
+        """The reference's defaults (cfl_max 8 with steady.sweep = lusgs, else 10)."""
+        o = cls(cfl0=1.0, cfl_max=8.0 if line_sweep == 1 else 10.0, ser_exponent=1.0, ser_max_growth=2.0,
+                residual_tol=5e-5, residual_drop_orders=4.0, residual_ref_iterations=5)
+        for k, v in kw.items():
+            setattr(o, k, v)
+        return o
+
+
+DRIVER_VERDICTS = {0: "running", 1: "steady", 2: "diverged", 3: "failed"}

@@ -2,11 +2,12 @@
 uneven terrain tiles and wind directions).
 
 Each member is one instance with its own CUDA stream, gb_ctx (scratch,
-result words), resident state and host driver. Members share nothing on the
-device. Host threads step the members, so one member's host-synchronising
-parts (the Krylov dot products of its Poisson solve, the result words of
-its iteration) overlap the kernels of the others, and the GPU runs the
-small kernels of many members at once. A member's arithmetic does not
+result words), resident state and driver. Members share nothing on the
+device. Native threads (gb_driver_run: the C++ steady driver, one thread
+per member) step the members, so one member's host-synchronising parts
+(the Krylov dot products of its Poisson solve, the result words of its
+iteration) overlap the kernels of the others, and the GPU runs the small
+kernels of many members at once. A member's arithmetic does not
 depend on what else runs: its result is the same alone and in the mix, bit
 for bit (deterministic reductions, no shared scratch).
 
@@ -67,6 +68,15 @@ class Member:
         self.stream.synchronize()
         self.status = "running"
         self.iterations = 0
+        self._native = None
+
+    @property
+    def native(self):
+        """This member's C++ driver (gb_driver), made on first use."""
+        if self._native is None:
+            from .simplec import NativeDriver
+            self._native = NativeDriver(self.stage)
+        return self._native
 
     @property
     def cells(self):
@@ -87,6 +97,8 @@ class Member:
         return out
 
     def close(self):
+        if self._native is not None:
+            self._native.close()
         self.stage.close()
         self.ctx.close()
 
@@ -132,12 +144,38 @@ class Batch:
         return device_ms, wall
 
     def run(self, iterations, concurrent=True, threads=None):
-        """iterations outer iterations of every member; returns (device ms,
-        wall ms)."""
+        """iterations outer iterations of every member (Python drivers on
+        Python threads); returns (device ms, wall ms)."""
         def work(m):
             for _ in range(iterations):
                 m.step()
         return self._run(work, concurrent, threads)
+
+    def run_native(self, iterations, threads=0):
+        """iterations outer iterations of every member with the C++ drivers on
+        native threads (gb_driver_run, one call); returns (device ms, wall ms)."""
+        import torch
+
+        from .simplec import run_drivers
+        drivers = [m.native for m in self.members]
+        torch.cuda.synchronize()
+        starts = []
+        for m in self.members:
+            e = torch.cuda.Event(enable_timing=True)
+            e.record(m.stream)
+            starts.append(e)
+        t0 = time.perf_counter()
+        out = run_drivers(drivers, iterations, threads)
+        ends = []
+        for m, (verdict, n) in zip(self.members, out):
+            m.status = verdict
+            m.iterations += n
+            e = torch.cuda.Event(enable_timing=True)
+            e.record(m.stream)
+            ends.append(e)
+        torch.cuda.synchronize()
+        wall = (time.perf_counter() - t0) * 1e3
+        return max(starts[0].elapsed_time(e) for e in ends), wall
 
     def close(self):
         for m in self.members:
@@ -159,9 +197,9 @@ def main(argv=None):
     free0, _ = torch.cuda.mem_get_info()
     batch = Batch(insts)
     free1, _ = torch.cuda.mem_get_info()
-    batch.run(args.warmup, concurrent=True, threads=args.threads or None)
-    seq_ms, seq_wall = batch.run(args.iterations, concurrent=False)
-    bat_ms, bat_wall = batch.run(args.iterations, concurrent=True, threads=args.threads or None)
+    batch.run_native(args.warmup, threads=args.threads)
+    seq_ms, seq_wall = batch.run_native(args.iterations, threads=1)
+    bat_ms, bat_wall = batch.run_native(args.iterations, threads=args.threads)
     cells = batch.cells * args.iterations
     line = {
         "metric": "cell-updates/s", "unit": "cell-updates/s",

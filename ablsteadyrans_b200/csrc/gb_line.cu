@@ -407,6 +407,11 @@ gb_status zline_sweeps(gb_ctx* ctx, const gb_grid& g, int loc, const T* A, const
                            ? ctx->tune[GB_TUNE_LINE_BLOCK] : 32;
     const size_t pipe_smem_first = static_cast<size_t>(R * 4 + 2 * nk) * pipe_thr * sizeof(T);
     const size_t pipe_smem = static_cast<size_t>(R * 12 + 2 * nk) * pipe_thr * sizeof(T);
+    // the factored sweep with twice the levels in flight (GB_TUNE_LINE_DEPTH = 2)
+    constexpr int R2 = 2 * R;
+    const bool deep = factored && ctx->tune[GB_TUNE_LINE_DEPTH] == 2;
+    const size_t deep_smem_first = static_cast<size_t>(R2 * 4 + 2 * nk) * pipe_thr * sizeof(T);
+    const size_t deep_smem = static_cast<size_t>(R2 * 12 + 2 * nk) * pipe_thr * sizeof(T);
     if (pipelined) {
         static std::atomic<bool> attr_done[2];  // set once per process (one device per process)
         const int ti = sizeof(T) == 8 ? 1 : 0;
@@ -415,6 +420,8 @@ gb_status zline_sweeps(gb_ctx* ctx, const gb_grid& g, int loc, const T* A, const
             cudaFuncSetAttribute(zline_pipe_kernel<T, false, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
             cudaFuncSetAttribute(zline_fact_kernel<T, true, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
             cudaFuncSetAttribute(zline_fact_kernel<T, false, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+            cudaFuncSetAttribute(zline_fact_kernel<T, true, R2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+            cudaFuncSetAttribute(zline_fact_kernel<T, false, R2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
             attr_done[ti].store(true);
         }
     } else if (!use_smem) {
@@ -448,7 +455,16 @@ gb_status zline_sweeps(gb_ctx* ctx, const gb_grid& g, int loc, const T* A, const
         a.first = (s == 0) ? 1 : 0;
         a.change = (s == sweeps - 1) ? change_word : nullptr;
         Span span(ctx, GB_KERNEL_LINE_SWEEP);
-        if (factored) {
+        if (deep) {
+            const dim3 block(pipe_thr, 1);
+            const dim3 grid((ni + pipe_thr - 1) / pipe_thr, nj);
+            if (a.first) {
+                zline_fact_kernel<T, true, R2><<<grid, block, deep_smem_first, ctx->stream>>>(a, inv, nullptr, cpr,
+                                                                                            nullptr);
+            } else {
+                zline_fact_kernel<T, false, R2><<<grid, block, deep_smem, ctx->stream>>>(a, nullptr, inv, nullptr, cpr);
+            }
+        } else if (factored) {
             const dim3 block(pipe_thr, 1);
             const dim3 grid((ni + pipe_thr - 1) / pipe_thr, nj);
             if (a.first) {

@@ -1678,6 +1678,9 @@ gb_status simplec_initialize(gb_simplec* S, const gb_state& q, const gb_init_opt
         }
         w_from_omega(S, q.u, q.v, w.om, q.w);
         velocity_divergence(S, q.u, q.v, q.w, w.rhs);
+        // the projection runs once per solve: its solver's memory goes back
+        gb_poisson_destroy(S->init_poisson);
+        S->init_poisson = nullptr;
     }
     dsum(S, valid_box(g, CC), w.rhs, 0, 1);
     double sums[2];
@@ -1687,6 +1690,9 @@ gb_status simplec_initialize(gb_simplec* S, const gb_state& q, const gb_init_opt
     r->divergence_after = std::sqrt(sums[1]);
     return check_cuda("initialize_state");
 }
+
+const gb_grid& simplec_grid(const gb_simplec* S) { return S->g; }
+gb_ctx* simplec_ctx(const gb_simplec* S) { return S->ctx; }
 
 // ----------------------------------------------------------- creation ---
 

@@ -12,6 +12,8 @@ The monitor window test of the reference's criterion is not applied here.
 """
 import math
 
+NONFINITE = 2  # gb_status GB_NONFINITE
+
 
 def ser_cfl(cfl, r, cfl0, cfl_max, p, growth):
     """Source/PseudoTime.cpp:53-61: min(cfl_max, growth cfl, cfl0 r^-p)."""
@@ -79,9 +81,19 @@ class Driver:
         self.dtau = None
 
     def step(self):
-        """One iteration; returns 'steady', 'diverged' or 'running'."""
+        """One iteration; returns 'steady', 'diverged' or 'running'. An
+        iteration that produced non-finite values (GB_NONFINITE) ends the
+        solve as diverged, as the criterion's non-finite residual does."""
+        from . import GustError
         self.dtau = self.stage.local_dtau(self.cfl, out=self.dtau)
-        info = self.stage.iterate(self.dtau)
+        try:
+            info = self.stage.iterate(self.dtau)
+        except GustError as e:
+            if e.status != NONFINITE:
+                raise
+            self.criterion.nonfinite = True
+            self.history.append((self.cfl, float("nan"), [float("nan")] * 6))
+            return "diverged"
         res = list(info.residual_norms)
         self.criterion.add(res)
         if self.criterion.nonfinite:

@@ -67,9 +67,9 @@ class Server:
     """Admission by device footprint under `budget` bytes, one driving
     thread per admitted request, retire and backfill."""
 
-    def __init__(self, budget, bytes_per_point, max_iterations=2000, poll=0.002):
+    def __init__(self, budget, footprint, max_iterations=2000, poll=0.002):
         self.budget = budget
-        self.bytes_per_point = bytes_per_point
+        self.model = footprint      # (a, b): bytes = a + b * padded points
         self.max_iterations = max_iterations
         self.poll = poll
         self.lock = threading.Lock()
@@ -79,7 +79,8 @@ class Server:
         self.peak_active = 0
 
     def footprint(self, req):
-        return int(self.bytes_per_point * req.inst.grid.volume)
+        a, b = self.model
+        return int(1.1 * (a + b * req.inst.grid.volume))
 
     def _serve_one(self, req, t0):
         from .batch import Member
@@ -92,15 +93,20 @@ class Server:
                 req.result = {"divergence_before": res.divergence_before, "divergence_after": res.divergence_after,
                               "poisson_iterations": res.poisson_iterations}
             else:
-                status = "running"
-                while status == "running" and m.iterations < self.max_iterations:
-                    status = m.step()
+                # the application's order: the mass-consistent initial state, then the
+                # stage, driven to the criterion by the C++ driver (one native call)
+                from .simplec import run_drivers
+                m.stage.initialize()
+                (status, n), = run_drivers([m.native], self.max_iterations, 1)
                 m.stream.synchronize()
                 req.status = status
-                req.iterations = m.iterations
+                req.iterations = n
             m.close()
         except Exception as e:  # the request fails; the server carries on
             req.status = f"error: {e}"
+        import torch
+        with self.lock:
+            torch.cuda.empty_cache()   # the member's stream-bound blocks go back to the device
         req.done = time.perf_counter() - t0
         with self.lock:
             self.in_use -= req.bytes
@@ -140,24 +146,39 @@ class Server:
         return time.perf_counter() - t0
 
 
-def calibrate_bytes_per_point(n=64, nz=48):
-    """Device bytes of one resident request per grid point (padded volume),
-    measured on one tile."""
+def measure_peak_bytes(n, nz):
+    """Peak device bytes of one request on an n x n x nz tile: the resident
+    member plus the initializer's Poisson solver, which lives only while the
+    initial state is projected."""
     import torch
 
+    import ablsteadyrans_b200 as gb
     from . import workloads
     from .batch import Member
     inst = workloads.tile(n, nz, 0)
     torch.cuda.synchronize()
     free0, _ = torch.cuda.mem_get_info()
     m = Member(inst)
-    m.stage.initialize()   # the initializer's solver too
+    opts = gb.PoissonOptions.default(precision=inst.options.precision)
+    ps = gb.PoissonSolver(m.ctx, inst.grid, m.case.z, m.case.J, [1, 1, 1, 2, 2, 1], opts)
     torch.cuda.synchronize()
     free1, _ = torch.cuda.mem_get_info()
+    ps.close()
     m.close()
     del m
     torch.cuda.empty_cache()
-    return max(free0 - free1, 1) / inst.grid.volume
+    return max(free0 - free1, 1), inst.grid.volume
+
+
+def calibrate_footprint():
+    """(a, b) of the footprint model bytes = a + b * volume (padded points),
+    fitted on a small and a large tile (fixed per-request costs dominate
+    small tiles)."""
+    b1, v1 = measure_peak_bytes(64, 48)
+    b2, v2 = measure_peak_bytes(128, 64)
+    b = max((b2 - b1) / (v2 - v1), 1.0)
+    a = max(b1 - b * v1, 0.0)
+    return a, b
 
 
 def main(argv=None):
@@ -170,9 +191,9 @@ def main(argv=None):
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--precision", type=int, default=1, choices=[0, 1])
     args = ap.parse_args(argv)
-    bpp = calibrate_bytes_per_point()
+    model = calibrate_footprint()
     reqs = requests_config4(args.requests, args.rate, args.seed, precision=args.precision)
-    srv = Server(args.budget_gb * 1e9, bpp * 1.1, max_iterations=args.max_iterations)
+    srv = Server(args.budget_gb * 1e9, model, max_iterations=args.max_iterations)
     wall = srv.run(reqs)
     lat = np.array([r.latency for r in reqs if r.latency is not None])
     by_kind = {k: np.array([r.latency for r in reqs if r.kind == k and r.latency is not None]) for k in ("init", "rans")}
@@ -183,9 +204,11 @@ def main(argv=None):
         "p50_init_s": float(np.percentile(by_kind["init"], 50)) if len(by_kind["init"]) else None,
         "p50_rans_s": float(np.percentile(by_kind["rans"], 50)) if len(by_kind["rans"]) else None,
         "steady": sum(1 for r in reqs if r.status == "steady"),
+        "diverged": sum(1 for r in reqs if r.status == "diverged"),
         "capped": sum(1 for r in reqs if r.kind == "rans" and r.status == "running"),
         "errors": [r.status for r in reqs if r.status and r.status.startswith("error")][:3],
-        "peak_concurrent": srv.peak_active, "peak_bytes": srv.peak, "bytes_per_point": bpp,
+        "peak_concurrent": srv.peak_active, "peak_bytes": srv.peak,
+        "footprint_model": {"fixed_bytes": model[0], "bytes_per_point": model[1]},
         "max_iterations": args.max_iterations,
     }
     print(json.dumps(line))

@@ -19,6 +19,12 @@ def _declare(L):
     L.gb_simplec_iterate.argtypes = [P, ctypes.POINTER(abi.State), P, ctypes.POINTER(abi.IterInfo)]
     L.gb_local_dtau.argtypes = [P, ctypes.POINTER(abi.State), ctypes.c_double, P]
     L.gb_init_options_default.argtypes = [ctypes.POINTER(abi.InitOptions)]
+    L.gb_driver_create.argtypes = [P, ctypes.POINTER(abi.State), ctypes.POINTER(abi.DriverOptions), ctypes.POINTER(P)]
+    L.gb_driver_destroy.argtypes = [P]
+    L.gb_driver_step.argtypes = [P, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(abi.IterInfo),
+                                 ctypes.POINTER(ctypes.c_double)]
+    L.gb_driver_run.argtypes = [ctypes.POINTER(P), ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32)]
     L.gb_simplec_initialize.argtypes = [P, ctypes.POINTER(abi.State), ctypes.POINTER(abi.InitOptions),
                                         ctypes.POINTER(abi.InitResult)]
 
@@ -128,3 +134,65 @@ class SimplecStage:
             self.close()
         except Exception:
             pass
+
+
+class NativeDriver:
+    """gust::Driver in C++ (gb_driver): the local dtau, one iteration, the
+    steady criterion and the SER law per step, with no Python in the loop."""
+
+    def __init__(self, stage, options=None):
+        from . import check
+        self.stage = stage
+        self._L = stage._L
+        self.options = options or abi.DriverOptions.make(getattr(stage.options, "line_sweep", 0))
+        self._state = stage.case.state()
+        self._h = ctypes.c_void_p()
+        check(self._L.gb_driver_create(stage._h, ctypes.byref(self._state), ctypes.byref(self.options),
+                                       ctypes.byref(self._h)))
+        self.iterations = 0
+
+    @property
+    def handle(self):
+        return self._h
+
+    def step(self):
+        """One step; returns ('running' | 'steady' | 'diverged', IterInfo, cfl used)."""
+        from . import check
+        v = ctypes.c_int32()
+        info = abi.IterInfo()
+        cfl = ctypes.c_double()
+        check(self._L.gb_driver_step(self._h, ctypes.byref(v), ctypes.byref(info), ctypes.byref(cfl)))
+        self.iterations += 1
+        return abi.DRIVER_VERDICTS[v.value], info, cfl.value
+
+    def close(self):
+        from . import check
+        if self._h:
+            check(self._L.gb_driver_destroy(self._h))
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def run_drivers(drivers, max_iterations, threads=0):
+    """gb_driver_run: every driver steps until it is steady, diverged or has
+    taken max_iterations steps, on native threads (0: one per driver).
+    Returns [(verdict, iterations)]."""
+    from . import check
+    if not drivers:
+        return []
+    L = drivers[0]._L
+    n = len(drivers)
+    hs = (ctypes.c_void_p * n)(*[d.handle.value for d in drivers])
+    v = (ctypes.c_int32 * n)()
+    it = (ctypes.c_int32 * n)()
+    check(L.gb_driver_run(hs, n, int(max_iterations), int(threads), v, it))
+    out = []
+    for d, a, b in zip(drivers, v, it):
+        d.iterations += b
+        out.append((abi.DRIVER_VERDICTS[a], b))
+    return out

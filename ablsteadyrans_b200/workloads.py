@@ -82,9 +82,12 @@ def node_ground(grid, height_fn):
     return out
 
 
-def fractal_field(n, seed, rms, slope=3.0):
+def fractal_field(n, seed, rms, slope=3.0, dx=None, max_slope=None):
     """A Gaussian random field on an n x n grid with isotropic power spectrum
-    |k|^-slope, standardised, scaled to `rms`, minimum shifted to 0."""
+    |k|^-slope, standardised, scaled to `rms`, minimum shifted to 0. With
+    dx and max_slope the field is scaled down where its steepest node-to-node
+    slope would exceed max_slope (beyond a slope of about 2 the terrain-
+    following Poisson operator loses definiteness and the solves stagnate)."""
     rng = np.random.default_rng(seed)
     kx = np.fft.fftfreq(n)[:, None]
     ky = np.fft.fftfreq(n)[None, :]
@@ -95,6 +98,10 @@ def fractal_field(n, seed, rms, slope=3.0):
     noise = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
     f = np.real(np.fft.ifft2(noise * amp))
     f = (f - f.mean()) / f.std() * rms
+    if dx is not None and max_slope is not None:
+        steepest = max(np.abs(np.diff(f, axis=0)).max(), np.abs(np.diff(f, axis=1)).max()) / dx
+        if steepest > max_slope:
+            f = f * (max_slope / steepest)
     return f - f.min()
 
 
@@ -205,11 +212,17 @@ def config1(nx=128, ny=128, nz=64, precision=0, zline_sweeps=4):
     return Instance("config1-hill-128x128x64", g, zl, ground, bc, ph, opts, ustar, z0, direction)
 
 
+#: The steepest node-to-node terrain slope of a generated tile (the fractal
+#: field is scaled down to it where steeper).
+MAX_TILE_SLOPE = 1.0
+
+
 def tile(n, nz, seed, rms=None, ustar=None, z0=None, met=None, dx=30.0, precision=1, zline_sweeps=4):
     """One instance of the batched/served configurations: n x n x nz over
     seeded fractal terrain (|k|^-3, rms uniform 20-150 m unless given), a
     random wind direction, u* and z0 (seed-derived); inflow on the upwind x
-    and y faces of the wind's quadrant, outflow on the others."""
+    and y faces of the wind's quadrant, outflow on the others. The terrain
+    is scaled down where its slope would exceed MAX_TILE_SLOPE."""
     rng = np.random.default_rng(1000 + seed)
     rms = rms if rms is not None else rng.uniform(20, 150)
     ustar = ustar if ustar is not None else rng.uniform(0.2, 0.6)
@@ -218,7 +231,7 @@ def tile(n, nz, seed, rms=None, ustar=None, z0=None, met=None, dx=30.0, precisio
     direction = (270.0 - met) % 360.0
     zl, _ = geometric_zlevels(nz)
     g = Grid(n, n, nz, dx, dx, 1500.0 / nz, False, False)
-    terrain = fractal_field(n + 1, seed, rms)
+    terrain = fractal_field(n + 1, seed, rms, dx=dx, max_slope=MAX_TILE_SLOPE)
     ground = node_ground(g, lambda x, y: float(terrain[int(round(y / dx)) % (n + 1), int(round(x / dx)) % (n + 1)]))
     bc = abi.BC.make(_faces_for(direction, periodic_y=False), theta_ref=((0.0, 1500.0), (300.0, 300.0)),
                      ustar=ustar, z0=z0, direction=direction, kappa=KAPPA, Cmu0=CMU0, l_max=LMAX)

@@ -103,6 +103,8 @@ enum {
     GB_TUNE_LINE_BLOCK,         /* threads per block of the pipelined sweep (32, 64 or 128; 0 = default) */
     GB_TUNE_MG_COARSE_KERNEL,   /* the coarsest level's relaxations: 0 auto (one single-block launch when the
                                    level has at most 64 columns), 1 the per-relaxation launches */
+    GB_TUNE_LINE_DEPTH,         /* levels the factored z-line sweep keeps in flight: 0 default (4 FP64, 8 FP32),
+                                   2 twice that */
     GB_N_TUNE
 };
 gb_status gb_ctx_tune(gb_ctx* ctx, int32_t key, int32_t value);
@@ -389,6 +391,45 @@ gb_status gb_simplec_initialize(gb_simplec* s, const gb_state* q, const gb_init_
 
 /* gust::local_dtau (Source/PseudoTime.H:32-33) with the stage's diffusivity nu. */
 gb_status gb_local_dtau(gb_simplec* s, const gb_state* q, double cfl, double* dtau);
+
+/* ---- the steady driver -------------------------------------------------- */
+
+/* steady.* of the pseudo-time driver and the steady criterion (gust::
+ * SteadyOptions, Source/Driver.H:52-110; gust::SteadyParams,
+ * Source/SteadyCriterion.H:13-33; the monitor window is not applied). */
+typedef struct gb_driver_opts {
+    double cfl0, cfl_max;            /* steady.cfl0, steady.cfl_max */
+    double ser_exponent;             /* steady.ser_exponent */
+    double ser_max_growth;           /* steady.ser_max_growth */
+    double residual_tol;             /* steady.residual_tol */
+    double residual_drop_orders;     /* steady.residual_drop_orders */
+    int32_t residual_ref_iterations; /* steady.residual_ref_iterations */
+} gb_driver_opts;
+
+enum { GB_DRIVER_RUNNING = 0, GB_DRIVER_STEADY = 1, GB_DRIVER_DIVERGED = 2, GB_DRIVER_FAILED = 3 };
+
+typedef struct gb_driver gb_driver;
+
+/* The defaults (cfl0 1, cfl_max 8 with steady.sweep = lusgs else 10 (Source/
+ * Driver.cpp:133-136), ser_exponent 1, ser_max_growth 2, residual_tol 5e-5,
+ * residual_drop_orders 4, residual_ref_iterations 5). */
+gb_status gb_driver_options_default(gb_driver_opts* o, int32_t line_sweep);
+/* gust::Driver for one stage and state (allocates the local dtau). */
+gb_status gb_driver_create(gb_simplec* s, const gb_state* q, const gb_driver_opts* o, gb_driver** out);
+gb_status gb_driver_destroy(gb_driver* d);
+/* Driver::step (Source/Driver.cpp:403-468): the local dtau at the current CFL,
+ * one SIMPLEC iteration, the criterion, the next CFL from the SER law.
+ * *verdict: GB_DRIVER_RUNNING, _STEADY or _DIVERGED (a non-finite iteration
+ * or residual); info and cfl (the CFL used) may be NULL. */
+gb_status gb_driver_step(gb_driver* d, int32_t* verdict, gb_iter_info* info, double* cfl);
+/* Many drivers at once: each steps until its verdict is not RUNNING or it
+ * has taken max_iterations steps, on `threads` host threads (<= 0: one per
+ * driver), so that one driver's host synchronisations overlap the others'
+ * kernels. verdicts[n] (GB_DRIVER_FAILED when a step returned an error) and
+ * iterations[n] receive each driver's outcome. Drivers must not share a
+ * context. */
+gb_status gb_driver_run(gb_driver* const* drivers, int32_t n, int32_t max_iterations, int32_t threads,
+                        int32_t* verdicts, int32_t* iterations);
 
 #ifdef __cplusplus
 }
