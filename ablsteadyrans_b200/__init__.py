@@ -211,6 +211,7 @@ def _declare_poisson(L):
                                     ctypes.POINTER(P)]
     L.gb_poisson_destroy.argtypes = [P]
     L.gb_poisson_set_coeffs.argtypes = [P, P, P, P, P, P, P]
+    L.gb_poisson_set_z_cross.argtypes = [P, P, P, P]
     L.gb_poisson_apply.argtypes = [P, P, P]
     L.gb_poisson_vcycle.argtypes = [P, P, P]
     L.gb_poisson_solve.argtypes = [P, P, P, ctypes.POINTER(PoissonResult)]
@@ -268,6 +269,11 @@ class PoissonSolver:
     def set_coeffs(self, ax, ay, az, bx=None, by=None, bz=None):
         self._coeffs = (ax, ay, az, bx, by, bz)
         check(_lib_full().gb_poisson_set_coeffs(self._h, _ptr(ax), _ptr(ay), _ptr(az), _ptr(bx), _ptr(by), _ptr(bz)))
+
+    def set_z_cross(self, az, bz, z_cross):
+        """FaceCoeffs::z_cross: the split z-face coefficient (None removes it)."""
+        self._cross = (az, bz, z_cross)
+        check(_lib_full().gb_poisson_set_z_cross(self._h, _ptr(az), _ptr(bz), _ptr(z_cross)))
 
     def apply(self, phi, out=None):
         y = out if out is not None else _zeros(self.grid)

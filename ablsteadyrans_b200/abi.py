@@ -126,7 +126,8 @@ class InitOptions(ctypes.Structure):
 
 class InitResult(ctypes.Structure):
     _fields_ = [("divergence_before", ctypes.c_double), ("divergence_after", ctypes.c_double),
-                ("poisson_iterations", ctypes.c_int32), ("poisson_final_residual", ctypes.c_double)]
+                ("poisson_iterations", ctypes.c_int32), ("poisson_final_residual", ctypes.c_double),
+                ("obrien_top_residual", ctypes.c_double)]
 
 
 class State(ctypes.Structure):

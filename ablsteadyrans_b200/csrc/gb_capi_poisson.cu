@@ -158,7 +158,6 @@ gb_status gb_poisson_destroy(gb_poisson* p)
     gb::clear_error();
     if (p == nullptr) { return GB_OK; }
     cudaStreamSynchronize(p->ctx->stream);
-    if (p->h_dots) { cudaFreeHost(p->h_dots); }
     delete p;
     return gb::check_cuda("PoissonSolver::~PoissonSolver");
 }
@@ -171,6 +170,15 @@ gb_status gb_poisson_set_coeffs(gb_poisson* p, const double* ax, const double* a
                         "PoissonSolver::set_coeffs");
     if (st != GB_OK) { return st; }
     return gb::poisson_set_coeffs(p, ax, ay, az, bx, by, bz);
+}
+
+gb_status gb_poisson_set_z_cross(gb_poisson* p, const double* az, const double* bz, const double* z_cross)
+{
+    gb::clear_error();
+    gb_status st = need(p != nullptr && (z_cross == nullptr || az != nullptr),
+                        "gust: %s: the solver and the z areas are needed", "PoissonSolver::set_z_cross");
+    if (st != GB_OK) { return st; }
+    return gb::poisson_set_z_cross(p, az, bz, z_cross);
 }
 
 gb_status gb_poisson_apply(gb_poisson* p, const double* phi, double* Aphi)

@@ -263,13 +263,8 @@ gb_status gb_simplec_initialize(gb_simplec* s, const gb_state* q, const gb_init_
         gb::set_error("gust: init.projection must be 0 or 1");
         return GB_BAD_ARG;
     }
-    if (o->obrien != 0) {
-        gb::set_error("gust: init.obrien = %d: the O'Brien column correction is not built here (0 only)", o->obrien);
-        return GB_BAD_ARG;
-    }
-    if (o->alpha_v != o->alpha_h) {
-        gb::set_error("gust: init.alpha_v = %g with init.alpha_h = %g: the split z-face coefficient "
-                      "(FaceCoeffs::z_cross) is not built here; give alpha_v = alpha_h", o->alpha_v, o->alpha_h);
+    if (o->obrien != 0 && o->obrien != 1) {
+        gb::set_error("gust: init.obrien must be 0 or 1");
         return GB_BAD_ARG;
     }
     gb_status st = gb::check_poisson_options(o->poisson);

@@ -223,9 +223,9 @@ __global__ void __launch_bounds__(128) zline_pipe_kernel(LineArgs<T> a)
 //! no division on the k chain. Inputs are staged R levels ahead with cp.async
 //! as in zline_pipe_kernel.
 template <typename T, bool FIRST, int R>
-__global__ void __launch_bounds__(128) zline_fact_kernel(LineArgs<T> a, T* __restrict__ im_out,
-                                                         const T* __restrict__ im_in, T* __restrict__ cp_out,
-                                                         const T* __restrict__ cp_in)
+__device__ __forceinline__ void zline_fact_body(const LineArgs<T>& a, T* __restrict__ im_out,
+                                                const T* __restrict__ im_in, T* __restrict__ cp_out,
+                                                const T* __restrict__ cp_in)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr int NV = FIRST ? 4 : 12;
@@ -330,6 +330,48 @@ __global__ void __launch_bounds__(128) zline_fact_kernel(LineArgs<T> a, T* __res
     if (a.change != nullptr) {
         chg = warp_max(chg);
         if ((threadIdx.x & 31) == 0) { atomic_max_nonneg(a.change, chg); }
+    }
+}
+
+template <typename T, bool FIRST, int R>
+__global__ void __launch_bounds__(128) zline_fact_kernel(LineArgs<T> a, T* __restrict__ im_out,
+                                                         const T* __restrict__ im_in, T* __restrict__ cp_out,
+                                                         const T* __restrict__ cp_in)
+{
+    zline_fact_body<T, FIRST, R>(a, im_out, im_in, cp_out, cp_in);
+}
+
+//! Several independent systems (up to kMaxLineSystems, each at its own
+//! location) swept by one launch: blockIdx.z picks the system, the grid
+//! covers the largest one and a block past a system's extents idles. More
+//! columns in flight per launch than one system gives.
+constexpr int kMaxLineSystems = 3;
+
+template <typename T>
+struct MultiLineArgs {
+    LineArgs<T> a[kMaxLineSystems];
+    T* inv[kMaxLineSystems];
+    T* cp[kMaxLineSystems];
+};
+
+template <typename T, bool FIRST, int R, int S>
+__device__ __forceinline__ void zline_fact_system(const MultiLineArgs<T>& m)
+{
+    if (FIRST) {
+        zline_fact_body<T, true, R>(m.a[S], m.inv[S], nullptr, m.cp[S], nullptr);
+    } else {
+        zline_fact_body<T, false, R>(m.a[S], nullptr, m.inv[S], nullptr, m.cp[S]);
+    }
+}
+
+template <typename T, bool FIRST, int R>
+__global__ void __launch_bounds__(128) zline_fact_multi_kernel(MultiLineArgs<T> m)
+{
+    // constant indices into the parameter block (no dynamic parameter indexing)
+    switch (blockIdx.z) {
+    case 0: zline_fact_system<T, FIRST, R, 0>(m); break;
+    case 1: zline_fact_system<T, FIRST, R, 1>(m); break;
+    default: zline_fact_system<T, FIRST, R, 2>(m); break;
     }
 }
 
@@ -496,6 +538,90 @@ gb_status zline_sweeps(gb_ctx* ctx, const gb_grid& g, int loc, const T* A, const
     return check_cuda("zline_jacobi");
 }
 
+template <typename T>
+gb_status zline_sweeps_multi(gb_ctx* ctx, const gb_grid& g, int n, const int* locs, const T* const* A,
+                             const T* const* ap, const T* const* rhs, int sweeps, T* const* delta,
+                             unsigned long long* const* change_words)
+{
+    if (n < 1 || n > kMaxLineSystems) {
+        set_error("gust: zline_sweeps_multi: 1 to %d systems (got %d)", kMaxLineSystems, n);
+        return GB_BAD_ARG;
+    }
+    const int64_t vol = volume(g);
+    constexpr int R = (sizeof(T) == 8) ? 4 : 8;
+    constexpr int kThr = 32;
+    int ni[kMaxLineSystems], nj[kMaxLineSystems], nk[kMaxLineSystems];
+    T* tmp[kMaxLineSystems];
+    T* inv[kMaxLineSystems];
+    T* cpr[kMaxLineSystems];
+    int max_ni = 0, max_nj = 0, max_nk = 0;
+    for (int s = 0; s < n; ++s) {
+        ni[s] = ext_x(g, locs[s]);
+        nj[s] = ext_y(g, locs[s]);
+        nk[s] = ext_z(g, locs[s]);
+        max_ni = std::max(max_ni, ni[s]);
+        max_nj = std::max(max_nj, nj[s]);
+        max_nk = std::max(max_nk, nk[s]);
+        tmp[s] = static_cast<T*>(scratch(ctx, kSlotMultiBase + 3 * s, sizeof(T) * vol));
+        inv[s] = static_cast<T*>(scratch(ctx, kSlotMultiBase + 3 * s + 1, sizeof(T) * vol));
+        cpr[s] = static_cast<T*>(scratch(ctx, kSlotMultiBase + 3 * s + 2, sizeof(T) * vol));
+        if (!tmp[s] || !inv[s] || !cpr[s]) { return GB_OOM; }
+        if (change_words != nullptr && change_words[s] != nullptr) {
+            cudaMemsetAsync(change_words[s], 0, sizeof(unsigned long long), ctx->stream);
+        }
+    }
+    static std::atomic<bool> attr_done[2];  // set once per process (one device per process)
+    const int ti = sizeof(T) == 8 ? 1 : 0;
+    if (!attr_done[ti].load()) {
+        cudaFuncSetAttribute(zline_fact_multi_kernel<T, true, R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             200 * 1024);
+        cudaFuncSetAttribute(zline_fact_multi_kernel<T, false, R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             200 * 1024);
+        attr_done[ti].store(true);
+    }
+    const size_t smem_first = static_cast<size_t>(R * 4 + 2 * max_nk) * kThr * sizeof(T);
+    const size_t smem = static_cast<size_t>(R * 12 + 2 * max_nk) * kThr * sizeof(T);
+    const dim3 grid((max_ni + kThr - 1) / kThr, max_nj, n);
+    for (int k = 0; k < sweeps; ++k) {
+        MultiLineArgs<T> m{};
+        for (int s = 0; s < n; ++s) {
+            T* buf[2] = {delta[s], tmp[s]};
+            LineArgs<T>& a = m.a[s];
+            a.g = g;
+            a.ni = ni[s];
+            a.nj = nj[s];
+            a.nk = nk[s];
+            a.A = A[s];
+            a.cs = vol;
+            a.ap = ap[s];
+            a.rhs = rhs[s];
+            a.dold = buf[(sweeps - k) & 1];
+            a.dnew = buf[(sweeps - 1 - k) & 1];
+            a.cbuf = nullptr;
+            a.ebuf = nullptr;
+            a.first = (k == 0) ? 1 : 0;
+            a.change = (k == sweeps - 1 && change_words != nullptr) ? change_words[s] : nullptr;
+            m.inv[s] = inv[s];
+            m.cp[s] = cpr[s];
+        }
+        Span span(ctx, GB_KERNEL_LINE_SWEEP);
+        if (k == 0) {
+            zline_fact_multi_kernel<T, true, R><<<grid, kThr, smem_first, ctx->stream>>>(m);
+        } else {
+            zline_fact_multi_kernel<T, false, R><<<grid, kThr, smem, ctx->stream>>>(m);
+        }
+        ++ctx->launches;
+    }
+    for (int s = 0; s < n; ++s) { seam_sync<T>(ctx, g, locs[s], delta[s]); }
+    return check_cuda("zline_sweeps_multi");
+}
+
+template gb_status zline_sweeps_multi<double>(gb_ctx*, const gb_grid&, int, const int*, const double* const*,
+                                              const double* const*, const double* const*, int, double* const*,
+                                              unsigned long long* const*);
+template gb_status zline_sweeps_multi<float>(gb_ctx*, const gb_grid&, int, const int*, const float* const*,
+                                             const float* const*, const float* const*, int, float* const*,
+                                             unsigned long long* const*);
 template gb_status zline_sweeps<double>(gb_ctx*, const gb_grid&, int, const double*, const double*, const double*, int,
                                         double*, unsigned long long*, LineScratch);
 template gb_status zline_sweeps<float>(gb_ctx*, const gb_grid&, int, const float*, const float*, const float*, int,

@@ -13,7 +13,8 @@ enum ScratchSlot : int {
     kSlotLineE,
     kSlotLineInv,  // 1/m of the factored sweeps
     kSlotLineCp,   // c' of the factored sweeps
-    kSlotFirstFree
+    kSlotFirstFree,
+    kSlotMultiBase = 24  // 3 slots (next, 1/m, c') per system of zline_sweeps_multi
 };
 
 enum class LineScratch { automatic, pipelined, shared, global, factored };
@@ -24,6 +25,14 @@ enum class LineScratch { automatic, pipelined, shared, global, factored };
 template <typename T>
 gb_status zline_sweeps(gb_ctx* ctx, const gb_grid& g, int loc, const T* A, const T* ap, const T* rhs, int sweeps,
                        T* delta, unsigned long long* change_word, LineScratch scratch_kind);
+
+//! zline_sweeps for n <= 3 independent systems (each at its own location,
+//! each into its own delta, 0 on entry) in one launch per sweep (the
+//! factored kernel; more columns in flight than one system gives).
+template <typename T>
+gb_status zline_sweeps_multi(gb_ctx* ctx, const gb_grid& g, int n, const int* locs, const T* const* A,
+                             const T* const* ap, const T* const* rhs, int sweeps, T* const* delta,
+                             unsigned long long* const* change_words);
 
 //! The line LU-SGS passes (gb_zline_lusgs) into delta (0 on entry, ghosts
 //! included); change_word as for zline_sweeps. FP64.

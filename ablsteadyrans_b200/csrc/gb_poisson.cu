@@ -222,6 +222,63 @@ __global__ void k_fluxes(gb_grid g, PBC b, const double* __restrict__ phi, MeshR
     }
 }
 
+//! z_face_cross (Source/PoissonCross_K.H:16-58): the terrain cross part
+//! h_x dphi/dx + h_y dphi/dy of the gradient at the low z-face of cell (i, j, k),
+//! the edge ratios and face slopes taken from MeshRatios.
+__device__ __forceinline__ double z_face_cross_r(const gb_grid& g, const PBC& b, int i, int j, int k,
+                                                 const double* x, const MeshRatios<double>& m)
+{
+    const double dxinv = 1.0 / g.dx, dyinv = 1.0 / g.dy, h = 0.5;
+    const int64_t o = at(g, i, j, k);
+#define X(a, bb, c) ldc<double>(x, x, g, b, a, bb, c)
+    const double px_hi_md_lo = h * (X(i + 1, j, k) - X(i, j, k) + X(i + 1, j, k - 1) - X(i, j, k - 1)) * dxinv;
+    const double px_lo_md_lo = h * (X(i, j, k) - X(i - 1, j, k) + X(i, j, k - 1) - X(i - 1, j, k - 1)) * dxinv;
+    const double py_md_hi_lo = h * (X(i, j + 1, k) - X(i, j, k) + X(i, j + 1, k - 1) - X(i, j, k - 1)) * dyinv;
+    const double py_md_lo_lo = h * (X(i, j, k) - X(i, j - 1, k) + X(i, j, k - 1) - X(i, j - 1, k - 1)) * dyinv;
+    const double pz_hi_md_lo = h * (X(i + 1, j, k) + X(i, j, k) - X(i + 1, j, k - 1) - X(i, j, k - 1)) * m.rx[o + 1];
+    const double pz_lo_md_lo = h * (X(i, j, k) + X(i - 1, j, k) - X(i, j, k - 1) - X(i - 1, j, k - 1)) * m.rx[o];
+    const double pz_md_hi_lo = h * (X(i, j + 1, k) + X(i, j, k) - X(i, j + 1, k - 1) - X(i, j, k - 1)) * m.ry[o + g.sy];
+    const double pz_md_lo_lo = h * (X(i, j, k) + X(i, j - 1, k) - X(i, j, k - 1) - X(i, j - 1, k - 1)) * m.ry[o];
+#undef X
+    return h * m.sx[o] * ((px_hi_md_lo + px_lo_md_lo) - (pz_hi_md_lo + pz_lo_md_lo))
+         + h * m.sy[o] * ((py_md_hi_lo + py_md_lo_lo) - (pz_md_hi_lo + pz_md_lo_lo));
+}
+
+//! The z-faces the split correction touches: not the ground, not a Neumann
+//! top (Source/Poisson.cpp:233-235, 246-249).
+__device__ __forceinline__ bool cross_face(const gb_grid& g, const PBC& b, int kf)
+{
+    return kf != 0 && !((b.zf & TP_ZHI) && kf == g.nz);
+}
+
+//! PoissonSolver::Op::add_cross (Source/Poisson.cpp:229-253): y += sign (1/J)
+//! d_zeta (a_z d cross), a_z d given per z-face. One thread per cell.
+__global__ void k_add_cross(gb_grid g, PBC b, const double* __restrict__ x, const double* __restrict__ ad,
+                            const double* __restrict__ J, MeshRatios<double> m, double sign, double* __restrict__ y)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = blockIdx.z;
+    if (i >= g.nx || j >= g.ny) { return; }
+    const int64_t o = at(g, i, j, k);
+    const double hi = cross_face(g, b, k + 1) ? ad[o + g.sz] * z_face_cross_r(g, b, i, j, k + 1, x, m) : 0.0;
+    const double lo = cross_face(g, b, k) ? ad[o] * z_face_cross_r(g, b, i, j, k, x, m) : 0.0;
+    y[o] += sign * ((hi - lo) * (1.0 / g.dzeta) / J[o]);
+}
+
+//! PoissonSolver::Op::add_cross_flux (Source/Poisson.cpp:255-273):
+//! F_z -= d cross on the same faces. One thread per z-face.
+__global__ void k_cross_flux(gb_grid g, PBC b, const double* __restrict__ x, const double* __restrict__ d,
+                             MeshRatios<double> m, double* __restrict__ fz)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = blockIdx.z;
+    if (i >= g.nx || j >= g.ny || !cross_face(g, b, k)) { return; }
+    const int64_t o = at(g, i, j, k);
+    fz[o] -= d[o] * z_face_cross_r(g, b, i, j, k, x, m);
+}
+
 __global__ void k_face_divergence(gb_grid g, const double* __restrict__ ax, const double* __restrict__ ay,
                                   const double* __restrict__ az, const double* __restrict__ J,
                                   const double* __restrict__ fx, const double* __restrict__ fy,
@@ -702,14 +759,16 @@ dim3 cols_grid(const gb_grid& g, int nk, int extra = 0)
 const dim3 kColsBlock(32, 4, 1);
 
 template <typename T>
-T* dalloc(std::vector<void*>& owned, int64_t n)
+T* dalloc(cudaStream_t stream, std::vector<void*>& owned, int64_t n)
 {
     void* p = nullptr;
     if (cudaMalloc(&p, sizeof(T) * std::max<int64_t>(n, 1)) != cudaSuccess) {
         cudaGetLastError();
         return nullptr;
     }
-    cudaMemset(p, 0, sizeof(T) * std::max<int64_t>(n, 1));
+    // zeroed on the solver's stream: ordered before every later kernel of the
+    // solver (a plain cudaMemset is not ordered against non-blocking streams)
+    cudaMemsetAsync(p, 0, sizeof(T) * std::max<int64_t>(n, 1), stream);
     owned.push_back(p);
     return static_cast<T*>(p);
 }
@@ -742,6 +801,7 @@ gb_poisson::~gb_poisson()
     for (void* p : owned) { cudaFree(p); }
     dl.release();
     fl.release();
+    if (h_dots) { cudaFreeHost(h_dots); }
 }
 
 namespace gb {
@@ -889,6 +949,13 @@ void apply_fine(gb_poisson* P, const double* x, const double* rhs, double* y)
     k_apply<double><<<cols_grid(g, g.nz), kColsBlock, 0, ctx->stream>>>(g, P->dl.b[0], x, P->dl.AX[0], P->dl.AY[0],
                                                                         P->dl.AZ[0], P->dl.J[0], P->dl.ratios(0), rhs, y);
     ++ctx->launches;
+    if (P->cross_ad != nullptr) {
+        // PoissonSolver::Op::apply (Source/Poisson.cpp:148-156): the split
+        // correction on top (subtracted when y is the residual rhs - A x)
+        k_add_cross<<<cols_grid(g, g.nz), kColsBlock, 0, ctx->stream>>>(g, P->dl.b[0], x, P->cross_ad, P->dl.J[0],
+                                                                          P->dl.ratios(0), rhs ? -1.0 : 1.0, y);
+        ++ctx->launches;
+    }
 }
 
 //! Dots <w, V_q> for q < nq (or <a, b> with V = b, nq = 1) into P->h_dots (host), deterministic.
@@ -935,24 +1002,24 @@ gb_status poisson_build(gb_poisson* P)
             D.z[l] = const_cast<double*>(P->z_fine);
             D.J[l] = const_cast<double*>(P->J_fine);
         } else {
-            D.z[l] = dalloc<double>(D.owned, vol);
-            D.J[l] = dalloc<double>(D.owned, vol);
+            D.z[l] = dalloc<double>(ctx->stream, D.owned, vol);
+            D.J[l] = dalloc<double>(ctx->stream, D.owned, vol);
         }
-        D.AX[l] = dalloc<double>(D.owned, vol);
-        D.AY[l] = dalloc<double>(D.owned, vol);
-        D.AZ[l] = dalloc<double>(D.owned, vol);
-        D.x[l] = dalloc<double>(D.owned, vol);
-        D.bv[l] = dalloc<double>(D.owned, vol);
-        D.r[l] = dalloc<double>(D.owned, vol);
-        D.snap[l] = dalloc<double>(D.owned, vol);
-        D.TD[l] = dalloc<double>(D.owned, vol);
-        D.TC[l] = dalloc<double>(D.owned, vol);
-        D.TU[l] = dalloc<double>(D.owned, vol);
-        D.RX[l] = dalloc<double>(D.owned, vol);
-        D.RY[l] = dalloc<double>(D.owned, vol);
-        D.HZ[l] = dalloc<double>(D.owned, vol);
-        D.SX[l] = dalloc<double>(D.owned, vol);
-        D.SY[l] = dalloc<double>(D.owned, vol);
+        D.AX[l] = dalloc<double>(ctx->stream, D.owned, vol);
+        D.AY[l] = dalloc<double>(ctx->stream, D.owned, vol);
+        D.AZ[l] = dalloc<double>(ctx->stream, D.owned, vol);
+        D.x[l] = dalloc<double>(ctx->stream, D.owned, vol);
+        D.bv[l] = dalloc<double>(ctx->stream, D.owned, vol);
+        D.r[l] = dalloc<double>(ctx->stream, D.owned, vol);
+        D.snap[l] = dalloc<double>(ctx->stream, D.owned, vol);
+        D.TD[l] = dalloc<double>(ctx->stream, D.owned, vol);
+        D.TC[l] = dalloc<double>(ctx->stream, D.owned, vol);
+        D.TU[l] = dalloc<double>(ctx->stream, D.owned, vol);
+        D.RX[l] = dalloc<double>(ctx->stream, D.owned, vol);
+        D.RY[l] = dalloc<double>(ctx->stream, D.owned, vol);
+        D.HZ[l] = dalloc<double>(ctx->stream, D.owned, vol);
+        D.SX[l] = dalloc<double>(ctx->stream, D.owned, vol);
+        D.SY[l] = dalloc<double>(ctx->stream, D.owned, vol);
         if (!D.TD[l] || !D.TC[l] || !D.TU[l] || !D.RX[l] || !D.RY[l] || !D.HZ[l] || !D.SX[l] || !D.SY[l]) {
             set_error("gust: PoissonSolver: cannot allocate the multigrid levels");
             return GB_OOM;
@@ -965,9 +1032,9 @@ gb_status poisson_build(gb_poisson* P)
             const gb_grid& gf = grids[l - 1];
             const int64_t nz3 = static_cast<int64_t>(g.nx + 3) * (g.ny + 3) * (g.nz + 3);
             k_coarse_z<<<nblocks(nz3), kBlock, 0, ctx->stream>>>(g, D.z[l], gf, D.z[l - 1]);
-            double* ax = dalloc<double>(D.owned, vol);
-            double* ay = dalloc<double>(D.owned, vol);
-            double* zcc = dalloc<double>(D.owned, vol);
+            double* ax = dalloc<double>(ctx->stream, D.owned, vol);
+            double* ay = dalloc<double>(ctx->stream, D.owned, vol);
+            double* zcc = dalloc<double>(ctx->stream, D.owned, vol);
             const int64_t nm = static_cast<int64_t>(g.nx + 3) * (g.ny + 3) * (g.nz + 2);
             k_metrics<<<nblocks(nm), kBlock, 0, ctx->stream>>>(g, D.z[l], D.J[l], ax, ay, zcc);
             ctx->launches += 2;
@@ -984,23 +1051,23 @@ gb_status poisson_build(gb_poisson* P)
             F.g[l] = g;
             F.b[l] = D.b[l];
             const int64_t vol = volume(g);
-            F.z[l] = dalloc<float>(F.owned, vol);
-            F.J[l] = dalloc<float>(F.owned, vol);
-            F.AX[l] = dalloc<float>(F.owned, vol);
-            F.AY[l] = dalloc<float>(F.owned, vol);
-            F.AZ[l] = dalloc<float>(F.owned, vol);
-            F.x[l] = dalloc<float>(F.owned, vol);
-            F.bv[l] = dalloc<float>(F.owned, vol);
-            F.r[l] = dalloc<float>(F.owned, vol);
-            F.snap[l] = dalloc<float>(F.owned, vol);
-            F.TD[l] = dalloc<float>(F.owned, vol);
-            F.TC[l] = dalloc<float>(F.owned, vol);
-            F.TU[l] = dalloc<float>(F.owned, vol);
-            F.RX[l] = dalloc<float>(F.owned, vol);
-            F.RY[l] = dalloc<float>(F.owned, vol);
-            F.HZ[l] = dalloc<float>(F.owned, vol);
-            F.SX[l] = dalloc<float>(F.owned, vol);
-            F.SY[l] = dalloc<float>(F.owned, vol);
+            F.z[l] = dalloc<float>(ctx->stream, F.owned, vol);
+            F.J[l] = dalloc<float>(ctx->stream, F.owned, vol);
+            F.AX[l] = dalloc<float>(ctx->stream, F.owned, vol);
+            F.AY[l] = dalloc<float>(ctx->stream, F.owned, vol);
+            F.AZ[l] = dalloc<float>(ctx->stream, F.owned, vol);
+            F.x[l] = dalloc<float>(ctx->stream, F.owned, vol);
+            F.bv[l] = dalloc<float>(ctx->stream, F.owned, vol);
+            F.r[l] = dalloc<float>(ctx->stream, F.owned, vol);
+            F.snap[l] = dalloc<float>(ctx->stream, F.owned, vol);
+            F.TD[l] = dalloc<float>(ctx->stream, F.owned, vol);
+            F.TC[l] = dalloc<float>(ctx->stream, F.owned, vol);
+            F.TU[l] = dalloc<float>(ctx->stream, F.owned, vol);
+            F.RX[l] = dalloc<float>(ctx->stream, F.owned, vol);
+            F.RY[l] = dalloc<float>(ctx->stream, F.owned, vol);
+            F.HZ[l] = dalloc<float>(ctx->stream, F.owned, vol);
+            F.SX[l] = dalloc<float>(ctx->stream, F.owned, vol);
+            F.SY[l] = dalloc<float>(ctx->stream, F.owned, vol);
             if (!F.TD[l] || !F.TC[l] || !F.TU[l] || !F.RX[l] || !F.RY[l] || !F.HZ[l] || !F.SX[l] || !F.SY[l]) {
                 set_error("gust: PoissonSolver: cannot allocate the FP32 multigrid levels");
                 return GB_OOM;
@@ -1022,14 +1089,14 @@ gb_status poisson_build(gb_poisson* P)
     const int64_t vol = volume(P->g);
     const int m = P->opt.restart;
     P->vstride = vol;
-    P->V = dalloc<double>(P->owned, vol * (m + 1));
-    P->Zv = dalloc<double>(P->owned, vol * m);
-    P->w = dalloc<double>(P->owned, vol);
-    P->t = dalloc<double>(P->owned, vol);
+    P->V = dalloc<double>(ctx->stream, P->owned, vol * (m + 1));
+    P->Zv = dalloc<double>(ctx->stream, P->owned, vol * m);
+    P->w = dalloc<double>(ctx->stream, P->owned, vol);
+    P->t = dalloc<double>(ctx->stream, P->owned, vol);
     P->dot_blocks = std::min(4 * ctx->num_sms, nblocks(static_cast<int64_t>(P->g.nx) * P->g.ny * P->g.nz));
-    P->d_partial = dalloc<double>(P->owned, static_cast<int64_t>(P->dot_blocks) * (m + 2));
-    P->d_dots = dalloc<double>(P->owned, m + 2);
-    P->d_coef = dalloc<double>(P->owned, m + 2);
+    P->d_partial = dalloc<double>(ctx->stream, P->owned, static_cast<int64_t>(P->dot_blocks) * (m + 2));
+    P->d_dots = dalloc<double>(ctx->stream, P->owned, m + 2);
+    P->d_coef = dalloc<double>(ctx->stream, P->owned, m + 2);
     if (!P->V || !P->Zv || !P->w || !P->t || !P->d_partial || !P->d_dots || !P->d_coef) {
         set_error("gust: PoissonSolver: cannot allocate the Krylov workspace");
         return GB_OOM;
@@ -1090,6 +1157,44 @@ void multiply_inplace(gb_ctx* ctx, double* a, const double* b, int64_t n)
     ++ctx->launches;
 }
 
+__global__ void k_cross_coeffs(int64_t n, const double* __restrict__ az, const double* __restrict__ bz,
+                               const double* __restrict__ zc, double* __restrict__ d, double* __restrict__ ad)
+{
+    const int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (t >= n) { return; }
+    const double v = (bz ? bz[t] : 1.0) - zc[t];
+    d[t] = v;
+    ad[t] = az[t] * v;
+}
+
+gb_status poisson_set_z_cross(gb_poisson* P, const double* az, const double* bz, const double* z_cross)
+{
+    gb_ctx* ctx = P->ctx;
+    if (z_cross == nullptr) {
+        P->cross_d = P->cross_ad = nullptr;  // the arrays stay owned until the solver goes
+        return GB_OK;
+    }
+    if (P->bc[2] == GB_POISSON_DIRICHLET) {
+        set_error("gust: FaceCoeffs::z_cross with a Dirichlet ground is not supported");
+        return GB_BAD_ARG;
+    }
+    const int64_t vol = volume(P->g);
+    if (P->cross_store[0] == nullptr) {
+        P->cross_store[0] = dalloc<double>(ctx->stream, P->owned, vol);
+        P->cross_store[1] = dalloc<double>(ctx->stream, P->owned, vol);
+        if (!P->cross_store[0] || !P->cross_store[1]) {
+            set_error("gust: PoissonSolver::set_z_cross: cannot allocate the split coefficients");
+            return GB_OOM;
+        }
+    }
+    P->cross_d = P->cross_store[0];
+    P->cross_ad = P->cross_store[1];
+    // FaceCoeffs::z_cross (Source/Poisson.cpp:461-479): d = (beta_z or 1) - z_cross
+    k_cross_coeffs<<<nblocks(vol), kBlock, 0, ctx->stream>>>(vol, az, bz, z_cross, P->cross_d, P->cross_ad);
+    ++ctx->launches;
+    return check_cuda("PoissonSolver::set_z_cross");
+}
+
 gb_status poisson_apply(gb_poisson* P, const double* phi, double* y)
 {
     apply_fine(P, phi, nullptr, y);
@@ -1111,6 +1216,11 @@ gb_status poisson_fluxes(gb_poisson* P, const double* phi, const double* bx, con
     k_fluxes<<<cols_grid(g, g.nz + 1, 1), kColsBlock, 0, ctx->stream>>>(g, P->dl.b[0], phi, P->dl.ratios(0), bx, by, bz, fx,
                                                                         fy, fz);
     ++ctx->launches;
+    if (P->cross_d != nullptr) {
+        k_cross_flux<<<cols_grid(g, g.nz + 1), kColsBlock, 0, ctx->stream>>>(g, P->dl.b[0], phi, P->cross_d,
+                                                                              P->dl.ratios(0), fz);
+        ++ctx->launches;
+    }
     return check_cuda("PoissonSolver::fluxes");
 }
 

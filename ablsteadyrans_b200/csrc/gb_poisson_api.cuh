@@ -49,6 +49,12 @@ struct gb_poisson {
     gb::PoissonLevels<double> dl;  // FP64 hierarchy (geometry and coefficients of every level)
     gb::PoissonLevels<float> fl;   // FP32 copies (precision == 1)
     bool coeffs_set{false};
+    // FaceCoeffs::z_cross: d = beta_z - z_cross and a_z d per z-face (owned;
+    // null: no split). The Krylov operator and the fluxes carry it, the
+    // V-cycle (the preconditioner) does not.
+    double* cross_d{nullptr};
+    double* cross_ad{nullptr};
+    double* cross_store[2]{nullptr, nullptr};
     // Krylov workspace
     int64_t vstride{0};
     double* V{nullptr};
@@ -72,6 +78,7 @@ gb_status check_poisson_options(const gb_poisson_opts& o);
 gb_status poisson_build(gb_poisson* P);
 gb_status poisson_set_coeffs(gb_poisson* P, const double* ax, const double* ay, const double* az, const double* bx,
                              const double* by, const double* bz);
+gb_status poisson_set_z_cross(gb_poisson* P, const double* az, const double* bz, const double* z_cross);
 gb_status poisson_apply(gb_poisson* P, const double* phi, double* y);
 gb_status poisson_vcycle(gb_poisson* P, const double* r, double* e);
 gb_status poisson_fluxes(gb_poisson* P, const double* phi, const double* bx, const double* by, const double* bz,

@@ -243,6 +243,14 @@ struct SimplecWork {
     float* ap32;
     float* rhs32;
     float* delta32;
+    // per system of the batched line solves (index 0 = A, rhs, delta, and the FP32 arrays above)
+    double* Am[3];
+    double* rhsm[3];
+    double* deltam[3];
+    float* A32m[3];
+    float* ap32m[3];
+    float* rhs32m[3];
+    float* delta32m[3];
 };
 
 }  // namespace gb
@@ -284,7 +292,9 @@ double* dbuf(gb_simplec* S, int64_t n)
         cudaGetLastError();
         return nullptr;
     }
-    cudaMemset(p, 0, sizeof(double) * std::max<int64_t>(n, 1));
+    // zeroed on the stage's stream: ordered before the stage's kernels (a plain
+    // cudaMemset is not ordered against non-blocking streams)
+    cudaMemsetAsync(p, 0, sizeof(double) * std::max<int64_t>(n, 1), S->ctx->stream);
     S->owned.push_back(p);
     return static_cast<double*>(p);
 }
@@ -296,7 +306,7 @@ float* fbuf(gb_simplec* S, int64_t n)
         cudaGetLastError();
         return nullptr;
     }
-    cudaMemset(p, 0, sizeof(float) * std::max<int64_t>(n, 1));
+    cudaMemsetAsync(p, 0, sizeof(float) * std::max<int64_t>(n, 1), S->ctx->stream);
     S->owned.push_back(p);
     return static_cast<float*>(p);
 }
@@ -1155,6 +1165,62 @@ gb_status line_solve(gb_simplec* S, int loc, const double* A, const double* ap, 
     return st;
 }
 
+//! n <= 3 independent systems (each at its own location) solved by the z-line
+//! sweeps in one launch per sweep (zline_sweeps_multi), FP64 or (precision 1)
+//! FP32; line LU-SGS solves them one after another. delta[s] (FP64) receives
+//! each correction, words[s] the change of its last sweep.
+gb_status line_solve_multi(gb_simplec* S, int n, const int* locs, double* const* A, double* const* ap,
+                           double* const* rhs, double* const* delta, const int* words)
+{
+    gb_ctx* ctx = S->ctx;
+    const gb_grid g = S->g;
+    const int64_t vol = volume(g);
+    if (S->opt.line_sweep == 1) {
+        for (int s = 0; s < n; ++s) {
+            gb_status st = line_solve(S, locs[s], A[s], ap[s], rhs[s], delta[s], words[s]);
+            if (st != GB_OK) { return st; }
+        }
+        return GB_OK;
+    }
+    unsigned long long* cw[3];
+    for (int s = 0; s < n; ++s) {
+        cudaMemsetAsync(delta[s], 0, sizeof(double) * vol, ctx->stream);
+        cw[s] = dword(ctx, words[s]);
+    }
+    if (S->opt.precision == 0) {
+        const double* Ac[3] = {A[0], n > 1 ? A[1] : nullptr, n > 2 ? A[2] : nullptr};
+        const double* apc[3] = {ap[0], n > 1 ? ap[1] : nullptr, n > 2 ? ap[2] : nullptr};
+        const double* rc[3] = {rhs[0], n > 1 ? rhs[1] : nullptr, n > 2 ? rhs[2] : nullptr};
+        return zline_sweeps_multi<double>(ctx, g, n, locs, Ac, apc, rc, S->opt.zline_sweeps, delta, cw);
+    }
+    SimplecWork& w = S->w;
+    const unsigned nb = static_cast<unsigned>((vol + 255) / 256);
+    const float* A32[3] = {};
+    const float* ap32[3] = {};
+    const float* r32[3] = {};
+    float* d32[3] = {};
+    for (int s = 0; s < n; ++s) {
+        k_convert<float><<<nb * GB_N_COEFS, 256, 0, ctx->stream>>>(w.A32m[s], A[s], vol * GB_N_COEFS);
+        k_convert<float><<<nb, 256, 0, ctx->stream>>>(w.ap32m[s], ap[s], vol);
+        k_convert<float><<<nb, 256, 0, ctx->stream>>>(w.rhs32m[s], rhs[s], vol);
+        ctx->launches += 3;
+        cudaMemsetAsync(w.delta32m[s], 0, sizeof(float) * vol, ctx->stream);
+        A32[s] = w.A32m[s];
+        ap32[s] = w.ap32m[s];
+        r32[s] = w.rhs32m[s];
+        d32[s] = w.delta32m[s];
+    }
+    gb_status st = zline_sweeps_multi<float>(ctx, g, n, locs, A32, ap32, r32, S->opt.zline_sweeps, d32, cw);
+    for (int s = 0; s < n; ++s) {
+        const float* dsrc = d32[s];
+        double* dst = delta[s];
+        for_box(ctx, valid_box(g, locs[s]), [=] __device__(int i, int j, int k) {
+            dst[at(g, i, j, k)] = static_cast<double>(dsrc[at(g, i, j, k)]);
+        });
+    }
+    return st;
+}
+
 }  // namespace
 
 // ------------------------------------------------------- predictor etc. ---
@@ -1180,15 +1246,15 @@ gb_status momentum_predictor(gb_simplec* S, const gb_state& q, double** R)
                                      : 0.0;
     for (int c = 0; c < 3; ++c) {
         const int t = 1 << c;
-        simplec_implicit_rows(S, c, w.F, w.A);
+        simplec_implicit_rows(S, c, w.F, w.Am[c]);
         dirichlet_rows(S, c, t, w.mask);
         double* ap = w.ap[c];
         double* dd = w.dd[c];
-        const double* A = w.A;
+        const double* A = w.Am[c];
         const double* mask = w.mask;
         const double* dt = w.dtf[c];
         const double* Rc = R[c];
-        double* rhs = w.rhs;
+        double* rhs = w.rhsm[c];
         const double inv_cap = S->opt.w_vnn_cap > 0 ? 1.0 / S->opt.w_vnn_cap : 0.0;
         const double s_margin = S->opt.w_vnn_cap_slope_margin;
         const bool cap = (c == 2 && S->opt.w_vnn_cap > 0);
@@ -1307,11 +1373,17 @@ gb_status momentum_predictor(gb_simplec* S, const gb_state& q, double** R)
                 rhs[o] -= gt * tau * 0.5 * (Rt[at(g, i, j, k - 1)] + Rt[o]);
             }, GB_KERNEL_COEFS);
         }
-        gb_status st = line_solve(S, t, w.A, ap, w.rhs, w.delta, W_LAST_U + c);
-        if (st != GB_OK) { return st; }
-        dmax(S, valid_box(g, t), w.delta, nullptr, W_MAX_DU + c);
+    }
+    // the three systems are independent: one batched solve
+    const int locs[3] = {XF, YF, ZF};
+    const int words[3] = {W_LAST_U, W_LAST_V, W_LAST_W};
+    gb_status st = line_solve_multi(S, 3, locs, w.Am, w.ap, w.rhsm, w.deltam, words);
+    if (st != GB_OK) { return st; }
+    for (int c = 0; c < 3; ++c) {
+        const int t = 1 << c;
+        dmax(S, valid_box(g, t), w.deltam[c], nullptr, W_MAX_DU + c);
         double* qc = comps[c];
-        const double* delta = w.delta;
+        const double* delta = w.deltam[c];
         for_box(ctx, valid_box(g, t), [=] __device__(int i, int j, int k) {
             const int64_t o = at(g, i, j, k);
             qc[o] += delta[o];
@@ -1413,37 +1485,53 @@ gb_status pressure_correction(gb_simplec* S, const gb_state& q, gb_iter_info* in
     return check_cuda("pressure_correction");
 }
 
-gb_status scalar_sweep(gb_simplec* S, int eq, double* field, const double* Req, const double* dtau, double floor,
-                       bool clip, int w_max, int w_last)
+//! Simplec.cpp:222-281 scalar_sweep for theta and for k: each system's rows
+//! (the A1 rows, a_P = 1/dtau + A_P, rhs = -R), the two solved by one batched
+//! line solve (the systems are independent), the increments added, k clipped
+//! at the floor with the clipped points counted.
+gb_status scalar_sweeps(gb_simplec* S, const gb_state& q, const double* dtau)
 {
     gb_ctx* ctx = S->ctx;
     const gb_grid g = S->g;
     SimplecWork& w = S->w;
     const int64_t cs = volume(g);
-    simplec_implicit_rows(S, eq, w.F, w.A);
-    double* rhs = w.rhs;
-    double* ap = w.ap[0];
-    const double* A = w.A;
-    for_box(ctx, valid_box(g, CC), [=] __device__(int i, int j, int k) {
-        const int64_t o = at(g, i, j, k);
-        rhs[o] = -Req[o];
-        ap[o] = 1.0 / dtau[o] + A[GB_COEF_P * cs + o];
-    }, GB_KERNEL_COEFS);
-    gb_status st = line_solve(S, CC, w.A, ap, w.rhs, w.delta, w_last);
+    const int eqs[2] = {F_THETA, F_TKE};
+    double* fields[2] = {q.theta, q.tke};
+    const double* Rq[2] = {w.R[4], w.R[5]};
+    for (int e = 0; e < 2; ++e) {
+        simplec_implicit_rows(S, eqs[e], w.F, w.Am[e]);
+        double* rhs = w.rhsm[e];
+        double* ap = w.ap[e];
+        const double* A = w.Am[e];
+        const double* Req = Rq[e];
+        for_box(ctx, valid_box(g, CC), [=] __device__(int i, int j, int k) {
+            const int64_t o = at(g, i, j, k);
+            rhs[o] = -Req[o];
+            ap[o] = 1.0 / dtau[o] + A[GB_COEF_P * cs + o];
+        }, GB_KERNEL_COEFS);
+    }
+    const int locs[2] = {CC, CC};
+    const int words[2] = {W_LAST_TH, W_LAST_K};
+    gb_status st = line_solve_multi(S, 2, locs, w.Am, w.ap, w.rhsm, w.deltam, words);
     if (st != GB_OK) { return st; }
-    dmax(S, valid_box(g, CC), w.delta, nullptr, w_max);
-    const double* delta = w.delta;
+    const int wmax[2] = {W_MAX_DTH, W_MAX_DK};
     unsigned long long* count = dword(ctx, W_CLIPPED);
-    const bool do_clip = clip && eq == F_TKE;
-    for_box(ctx, valid_box(g, CC), [=] __device__(int i, int j, int k) {
-        const int64_t o = at(g, i, j, k);
-        double v = field[o] + delta[o];
-        if (do_clip && v < floor) {
-            v = floor;
-            atomicAdd(count, 1ull);
-        }
-        field[o] = v;
-    });
+    for (int e = 0; e < 2; ++e) {
+        dmax(S, valid_box(g, CC), w.deltam[e], nullptr, wmax[e]);
+        const double* delta = w.deltam[e];
+        double* field = fields[e];
+        const bool do_clip = (eqs[e] == F_TKE);
+        const double floor = S->opt.tke_floor;
+        for_box(ctx, valid_box(g, CC), [=] __device__(int i, int j, int k) {
+            const int64_t o = at(g, i, j, k);
+            double v = field[o] + delta[o];
+            if (do_clip && v < floor) {
+                v = floor;
+                atomicAdd(count, 1ull);
+            }
+            field[o] = v;
+        });
+    }
     return check_cuda("scalar_sweep");
 }
 
@@ -1484,10 +1572,7 @@ gb_status simplec_iterate(gb_simplec* S, const gb_state& q, const double* dtau, 
             Rt[o] += c1[o] - c0[o];
         });
     }
-    if ((st = scalar_sweep(S, F_THETA, q.theta, w.R[4], dtau, 0, false, W_MAX_DTH, W_LAST_TH)) != GB_OK) { return st; }
-    if ((st = scalar_sweep(S, F_TKE, q.tke, w.R[5], dtau, S->opt.tke_floor, true, W_MAX_DK, W_LAST_K)) != GB_OK) {
-        return st;
-    }
+    if ((st = scalar_sweeps(S, q, dtau)) != GB_OK) { return st; }
     // read every result of the iteration at once
     unsigned long long words[W_COUNT];
     if ((st = read_words(ctx, 0, W_COUNT, words)) != GB_OK) { return st; }
@@ -1619,6 +1704,46 @@ gb_status simplec_initialize(gb_simplec* S, const gb_state& q, const gb_init_opt
         });
     }
     cudaMemsetAsync(q.p, 0, sizeof(double) * vol, ctx->stream);
+    cudaMemsetAsync(w.sums + 2, 0, sizeof(double), ctx->stream);
+    if (o.obrien) {
+        // O'Brien (Initializer.cpp:326-333; obrien_omega :197-274): Omega from
+        // the column continuity of (a_x u, a_y v), a_z Omega_{k+1/2} =
+        // a_z Omega_{k-1/2} - J Dh dzeta from 0 at the ground, the top value
+        // E removed with ((z_f - z_ground) / depth)^2; one thread per column.
+        cudaMemsetAsync(w.G[2], 0, sizeof(double) * vol, ctx->stream);
+        gb_status st = face_divergence(ctx, g, S->mesh.ax, S->mesh.ay, S->mesh.az, S->mesh.detJ, q.u, q.v, w.G[2],
+                                       w.rhs);
+        if (st != GB_OK) { return st; }
+        const double* az = S->mesh.az;
+        const double* J = S->mesh.detJ;
+        const double* dh = w.rhs;
+        const double* zn = S->z;
+        double* om = w.om;
+        auto* worst = reinterpret_cast<unsigned long long*>(w.sums + 2);
+        const double dzeta = g.dzeta;
+        for_box(ctx, Box{{0, 0, 0}, {g.nx - 1, g.ny - 1, 0}}, [=] __device__(int i, int j, int) {
+            om[at(g, i, j, 0)] = 0.0;
+            for (int k = 0; k < g.nz; ++k) {
+                om[at(g, i, j, k + 1)] = (az[at(g, i, j, k)] * om[at(g, i, j, k)]
+                                          - J[at(g, i, j, k)] * dh[at(g, i, j, k)] * dzeta)
+                                         / az[at(g, i, j, k + 1)];
+            }
+            const double E = om[at(g, i, j, g.nz)];
+            // non-negative doubles order as their bit patterns (a NaN above all)
+            atomicMax(worst, static_cast<unsigned long long>(__double_as_longlong(fabs(E))));
+            auto zf = [&](int k) {
+                return 0.25 * (zn[at(g, i, j, k)] + zn[at(g, i + 1, j, k)] + zn[at(g, i, j + 1, k)]
+                               + zn[at(g, i + 1, j + 1, k)]);
+            };
+            const double zg = zf(0), depth = zf(g.nz) - zg;
+            for (int k = 1; k <= g.nz; ++k) {
+                const double frac = (zf(k) - zg) / depth;
+                om[at(g, i, j, k)] -= frac * frac * E;
+            }
+            om[at(g, i, j, g.nz)] = 0.0;
+        });
+        w_from_omega(S, q.u, q.v, w.om, q.w);
+    }
     // 3. the mass-consistent correction
     velocity_divergence(S, q.u, q.v, q.w, w.rhs);
     dsum(S, valid_box(g, CC), w.rhs, 0, 0);
@@ -1643,17 +1768,25 @@ gb_status simplec_initialize(gb_simplec* S, const gb_state& q, const gb_init_opt
         const bool unit = (o.alpha_h == 1 && o.alpha_v == 1);
         const double* beta[3] = {nullptr, nullptr, nullptr};
         if (!unit) {
-            // Sigma = alpha^2 I on every face (alpha_h = alpha_v)
-            const double a2 = o.alpha_h * o.alpha_h;
+            // Sigma = diag(alpha_h^2, alpha_h^2, alpha_v^2): x, y and the cross
+            // part of the z-faces carry alpha_h^2, the z part alpha_v^2
+            // (Initializer.cpp:380-403)
+            const double ah2 = o.alpha_h * o.alpha_h, av2 = o.alpha_v * o.alpha_v;
             for (int c = 0; c < 3; ++c) {
                 double* b = w.beta[c];
+                const double v = (c == 2) ? av2 : ah2;
                 for_box(ctx, Box{{-g.ng, -g.ng, -g.ng}, {g.nx + g.ng, g.ny + g.ng, g.nz + g.ng}},
-                        [=] __device__(int i, int j, int k) { b[at(g, i, j, k)] = a2; });
+                        [=] __device__(int i, int j, int k) { b[at(g, i, j, k)] = v; });
                 beta[c] = w.beta[c];
             }
         }
         st = poisson_set_coeffs(S->init_poisson, S->mesh.ax, S->mesh.ay, S->mesh.az, beta[0], beta[1], beta[2]);
         if (st != GB_OK) { return st; }
+        if (o.alpha_v != o.alpha_h) {
+            // the split only where alpha_v != alpha_h: z_cross = alpha_h^2
+            st = poisson_set_z_cross(S->init_poisson, S->mesh.az, beta[2], beta[0]);
+            if (st != GB_OK) { return st; }
+        }
         gb_poisson_result pr{};
         if ((st = poisson_solve(S->init_poisson, w.rhs, w.phi, &pr)) != GB_OK) { return st; }
         r->poisson_iterations = pr.iterations;
@@ -1683,11 +1816,12 @@ gb_status simplec_initialize(gb_simplec* S, const gb_state& q, const gb_init_opt
         S->init_poisson = nullptr;
     }
     dsum(S, valid_box(g, CC), w.rhs, 0, 1);
-    double sums[2];
-    cudaMemcpyAsync(sums, w.sums, sizeof(double) * 2, cudaMemcpyDeviceToHost, ctx->stream);
+    double sums[3];
+    cudaMemcpyAsync(sums, w.sums, sizeof(double) * 3, cudaMemcpyDeviceToHost, ctx->stream);
     if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) { return check_cuda("initialize_state"); }
     r->divergence_before = std::sqrt(sums[0]);
     r->divergence_after = std::sqrt(sums[1]);
+    r->obrien_top_residual = sums[2];
     return check_cuda("initialize_state");
 }
 
@@ -1732,6 +1866,24 @@ gb_status simplec_build(gb_simplec* S)
         w.ap32 = fbuf(S, vol);
         w.rhs32 = fbuf(S, vol);
         w.delta32 = fbuf(S, vol);
+    }
+    w.Am[0] = w.A;
+    w.rhsm[0] = w.rhs;
+    w.deltam[0] = w.delta;
+    w.A32m[0] = w.A32;
+    w.ap32m[0] = w.ap32;
+    w.rhs32m[0] = w.rhs32;
+    w.delta32m[0] = w.delta32;
+    for (int s = 1; s < 3; ++s) {
+        w.Am[s] = dbuf(S, vol * GB_N_COEFS);
+        w.rhsm[s] = dbuf(S, vol);
+        w.deltam[s] = dbuf(S, vol);
+        if (S->opt.precision == 1) {
+            w.A32m[s] = fbuf(S, vol * GB_N_COEFS);
+            w.ap32m[s] = fbuf(S, vol);
+            w.rhs32m[s] = fbuf(S, vol);
+            w.delta32m[s] = fbuf(S, vol);
+        }
     }
     for (void* p : S->owned) {
         if (p == nullptr) {

@@ -238,3 +238,25 @@ def tile(n, nz, seed, rms=None, ustar=None, z0=None, met=None, dx=30.0, precisio
     ph = abi.Physics.make(1500.0, gravity=9.81)
     opts = abi.SimplecOptions.make(zline_sweeps=zline_sweeps, precision=precision)
     return Instance(f"tile-{seed}-{n}x{n}x{nz}", g, zl, ground, bc, ph, opts, ustar, z0, direction)
+
+
+def config2(precision=1, zline_sweeps=4, n=256, nz=96, seed=2, max_slope=2.0):
+    """Mixed precision against plain FP64 on a 256 x 256 x 96 grid, dx = dy =
+    30 m, over seeded fractal terrain (|k|^-3, 120 m rms, minimum 0, scaled
+    down where steeper than max_slope); log-law inflow u* = 0.4 m/s from
+    225 deg (inflow on the x and y faces upwind). The configuration's
+    per-column lognormal z0 has no counterpart here (the ground is a no-slip
+    wall; z0 enters through the inflow log law): its median, 0.05 m, is used."""
+    dx = 30.0
+    met = 225.0
+    direction = (270.0 - met) % 360.0
+    zl, _ = geometric_zlevels(nz)
+    g = Grid(n, n, nz, dx, dx, 1500.0 / nz, False, False)
+    terrain = fractal_field(n + 1, seed, 120.0, dx=dx, max_slope=max_slope)
+    ground = node_ground(g, lambda x, y: float(terrain[int(round(y / dx)) % (n + 1), int(round(x / dx)) % (n + 1)]))
+    ustar, z0 = 0.4, 0.05
+    bc = abi.BC.make(_faces_for(direction, periodic_y=False), theta_ref=((0.0, 1500.0), (300.0, 300.0)),
+                     ustar=ustar, z0=z0, direction=direction, kappa=KAPPA, Cmu0=CMU0, l_max=LMAX)
+    ph = abi.Physics.make(1500.0, gravity=9.81)
+    opts = abi.SimplecOptions.make(zline_sweeps=zline_sweeps, precision=precision)
+    return Instance(f"config2-fractal-{n}x{n}x{nz}", g, zl, ground, bc, ph, opts, ustar, z0, direction)

@@ -358,7 +358,7 @@ def main():
         "gpu_launches": launches,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None, "traffic": traffic,
-                     "kernel": "zline_fact_kernel (z-line Thomas sweeps of u, v, w, theta, k)",
+                     "kernel": "zline_fact_multi_kernel (z-line Thomas sweeps: u, v, w in one launch, theta and k in one)",
                      "peak_kind": peak_kind,
                      "bytes_per_launch": line_bytes / max(sweep_n, 1), "launch_ms": sweep_ms / max(sweep_n, 1)},
         "breakdown": families,

@@ -222,6 +222,17 @@ gb_status gb_poisson_destroy(gb_poisson* p);
 gb_status gb_poisson_set_coeffs(gb_poisson* p, const double* ax, const double* ay, const double* az, const double* bx,
                                 const double* by, const double* bz);
 
+/* FaceCoeffs::z_cross (Source/Poisson.H:83-102, Source/Poisson.cpp:461-479):
+ * the split z-face coefficient. The z-face gradient becomes
+ * beta_z dphi/dz - z_cross (h_x dphi/dx + h_y dphi/dy): the operator adds
+ * (1/J) d_zeta (a_z (beta_z - z_cross) cross) (PoissonSolver::Op::add_cross,
+ * Source/Poisson.cpp:229-253) and the fluxes subtract (beta_z - z_cross) cross
+ * (add_cross_flux, :255-273), on every z-face but the ground and a Neumann
+ * top. The multigrid preconditioner keeps the unsplit operator. az: the raw
+ * z areas; bz: the beta_z given to set_coeffs (null = 1); z_cross null
+ * removes the split. A Dirichlet ground is refused, as the reference does. */
+gb_status gb_poisson_set_z_cross(gb_poisson* p, const double* az, const double* bz, const double* z_cross);
+
 /* A phi (PoissonSolver::apply / TerrainPoisson::apply with the zero-flux faces,
  * extern_erf/ERF_TerrainPoisson.cpp:74-101). Ghosts of phi are not read from
  * memory: they are resolved by index for the boundary types. */
@@ -337,10 +348,11 @@ typedef struct gb_iter_info {
  * Source/Initializer.H:63-111) with init.first_guess = profile. */
 typedef struct gb_init_opts {
     double z_agl_min;                /* init.z_agl_min (m, >= 0): floor of the profile's height */
-    double alpha_h, alpha_v;         /* init.alpha_h, init.alpha_v (> 0); alpha_v != alpha_h is not built */
+    double alpha_h, alpha_v;         /* init.alpha_h, init.alpha_v (> 0); alpha_v != alpha_h: the split z-face
+                                        coefficient (gb_poisson_set_z_cross) */
     double k_decay_height;           /* init.k_decay_height (m, >= 0; 0: no decay) */
     int32_t projection;              /* init.projection (0 or 1) */
-    int32_t obrien;                  /* init.obrien (must be 0: the O'Brien column correction is not built) */
+    int32_t obrien;                  /* init.obrien (0 or 1): the O'Brien column correction of w0 */
     gb_poisson_opts poisson;         /* solver.poisson_* of the projection */
 } gb_init_opts;
 
@@ -349,6 +361,7 @@ typedef struct gb_init_result {
     double divergence_before, divergence_after;   /* L2 norms of the velocity divergence (1/s) */
     int32_t poisson_iterations;
     double poisson_final_residual;
+    double obrien_top_residual;   /* max |Omega_top| the O'Brien pass removed (m/s; 0 without it) */
 } gb_init_result;
 
 typedef struct gb_simplec gb_simplec;
@@ -383,10 +396,13 @@ gb_status gb_init_options_default(gb_init_opts* o);
  * boundary conditions: u, v from the inflow profile at every point's height
  * above the ground (ghosts included), w = 0 but the ground faces' kinematic w,
  * theta = theta_ref(z), k from the profile (decaying above k_decay_height),
- * p = 0; then, with projection = 1, the mass-consistent correction: the
- * divergence removed by the terrain Poisson solve with lambda = 0 on the
- * inflow and outflow faces and zero flux through the others (u, v, Omega +=
- * the fluxes, w from Omega). */
+ * p = 0; with obrien = 1, w0 from O'Brien's column correction (obrien_omega,
+ * Source/Initializer.cpp:197-274); then, with projection = 1, the
+ * mass-consistent correction: the divergence removed by the terrain Poisson
+ * solve with lambda = 0 on the inflow and outflow faces and zero flux through
+ * the others, Sigma = diag(alpha_h^2, alpha_h^2, alpha_v^2) with the split
+ * z-face coefficient when alpha_v != alpha_h (u, v, Omega += the fluxes, w
+ * from Omega). */
 gb_status gb_simplec_initialize(gb_simplec* s, const gb_state* q, const gb_init_opts* o, gb_init_result* r);
 
 /* gust::local_dtau (Source/PseudoTime.H:32-33) with the stage's diffusivity nu. */

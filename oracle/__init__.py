@@ -68,6 +68,10 @@ def _declare(L):
     L.og_mg_levels.argtypes = [P]
     L.og_mg_levels.restype = i32
     L.og_mg_vcycle.argtypes = [P, P, P]
+    L.og_mg_set_cross.argtypes = [P, P, P, P]
+    L.og_mg_apply.argtypes = [P, P, P]
+    L.og_poisson_add_cross.argtypes = [G, I, P, P, P, P, P, P]
+    L.og_poisson_cross_flux.argtypes = [G, I, P, P, P, P]
     L.og_poisson_solve.argtypes = [P, P, P, f64, f64, i32, i32, i32, ctypes.POINTER(f64)]
     L.og_poisson_solve.restype = i32
     L.og_line_tridiag.argtypes = [G, I, i32, P, P, P, P, P, i32, i32, i32, ctypes.POINTER(f64),
@@ -148,6 +152,28 @@ def poisson_fluxes(grid, bc, z, phi, bx=None, by=None, bz=None):
     return f
 
 
+def poisson_apply_split(grid, bc, ax, ay, az, J, z, phi, bx, by, bz, z_cross):
+    """PoissonSolver::apply with FaceCoeffs {bx, by, bz, z_cross}
+    (Source/Poisson.cpp:524-529): the operator on the premultiplied areas plus,
+    when z_cross is given, the split correction (add_cross)."""
+    AX, AY, AZ = ax * bx, ay * by, az * bz
+    y = poisson_apply(grid, bc, AX, AY, AZ, J, z, phi)
+    if z_cross is not None:
+        d = np.ascontiguousarray(bz - z_cross)
+        lib().og_poisson_add_cross(ctypes.byref(grid.c), _bc(bc), _p(az), _p(d), _p(J), _p(z), _p(phi), _p(y))
+    return y
+
+
+def poisson_fluxes_split(grid, bc, z, phi, bx, by, bz, z_cross):
+    """The solve's fluxes with FaceCoeffs {bx, by, bz, z_cross}
+    (Source/Poisson.cpp:603-615)."""
+    f = poisson_fluxes(grid, bc, z, phi, bx, by, bz)
+    if z_cross is not None:
+        d = np.ascontiguousarray(bz - z_cross)
+        lib().og_poisson_cross_flux(ctypes.byref(grid.c), _bc(bc), _p(d), _p(z), _p(phi), _p(f[2]))
+    return f
+
+
 def face_divergence(grid, ax, ay, az, J, fx, fy, fz):
     d = grid.np_zeros()
     lib().og_face_divergence(ctypes.byref(grid.c), _p(ax), _p(ay), _p(az), _p(J), _p(fx), _p(fy), _p(fz), _p(d))
@@ -170,6 +196,16 @@ class Multigrid:
     @property
     def levels(self):
         return int(lib().og_mg_levels(self._h))
+
+    def set_cross(self, az, bz, z_cross):
+        """FaceCoeffs::z_cross for the solve's operator (not the V-cycle)."""
+        lib().og_mg_set_cross(self._h, _p(np.ascontiguousarray(az)), _p(bz), _p(z_cross))
+
+    def apply(self, phi):
+        """The solve's operator (the split correction included when set)."""
+        y = self.grid.np_zeros()
+        lib().og_mg_apply(self._h, _p(phi), _p(y))
+        return y
 
     def vcycle(self, r):
         e = self.grid.np_zeros()
@@ -214,6 +250,8 @@ def _declare_simplec(L):
     L.og_initialize.argtypes = [G, ctypes.POINTER(BC), ctypes.POINTER(InitOptions), ctypes.POINTER(State),
                                 ctypes.POINTER(MeshFields), P]
     L.og_initialize.restype = i32
+    L.og_obrien_omega.argtypes = [G, P, P, P, P, P, P, P, P]
+    L.og_obrien_omega.restype = f64
     L.og_local_dtau.argtypes = [G, P, P, P, P, P, P, f64, P]
     L.og_transport_fluxes.argtypes = [G, P, P, P, P, P, P, P, P, P]
     L.og_velocity_divergence.argtypes = [G, P, P, P, P, P, P, P, P, P]
@@ -304,12 +342,23 @@ def simplec_iterate(case, bc, phys, opts, dtau):
 def initialize(case, bc, init_opts):
     """gust::initialize_state with init.first_guess = profile
     (Source/Initializer.cpp:281-430) on the case's state; returns (status,
-    [divergence before, after, Poisson iterations, final residual])."""
-    info = np.zeros(4)
+    [divergence before, after, Poisson iterations, final residual, O'Brien's
+    top residual])."""
+    info = np.zeros(5)
     st, m = case.state(), case.mesh()
     rc = _L().og_initialize(ctypes.byref(case.grid.c), ctypes.byref(bc), ctypes.byref(init_opts), ctypes.byref(st),
                             ctypes.byref(m), _p(info))
     return int(rc), info
+
+
+def obrien_omega(case):
+    """obrien_omega (Source/Initializer.cpp:197-274) on the case's u, v:
+    returns (Omega on the z-faces, max |E|)."""
+    g = case.grid
+    om = g.np_zeros()
+    E = _L().og_obrien_omega(ctypes.byref(g.c), _p(case.q["u"]), _p(case.q["v"]), _p(case.z), _p(case.ax),
+                             _p(case.ay), _p(case.az), _p(case.J), _p(om))
+    return om, float(E)
 
 
 def transport_fluxes(grid, u, v, w, z, ax, ay):

@@ -319,8 +319,86 @@ static double flux_z(const og_grid* g, int i, int j, int k, const double* x, con
     return -pz_lo;
 }
 
+/* z_face_cross (Source/PoissonCross_K.H:16-58): the terrain cross part
+ * h_x dphi/dx + h_y dphi/dy of the z-face gradient at the low z-face of cell
+ * (i, j, k), in the reference's operation order. phi's ghosts filled. */
+static double z_face_cross(const og_grid* g, int i, int j, int k, const double* x, const double* zp)
+{
+    const double dxinv = 1.0 / g->dx, dyinv = 1.0 / g->dy;
+    const double px_hi_md_lo = 0.5 * (X(i + 1, j, k) - X(i, j, k) + X(i + 1, j, k - 1) - X(i, j, k - 1)) * dxinv;
+    const double px_lo_md_lo = 0.5 * (X(i, j, k) - X(i - 1, j, k) + X(i, j, k - 1) - X(i - 1, j, k - 1)) * dxinv;
+    const double py_md_hi_lo = 0.5 * (X(i, j + 1, k) - X(i, j, k) + X(i, j + 1, k - 1) - X(i, j, k - 1)) * dyinv;
+    const double py_md_lo_lo = 0.5 * (X(i, j, k) - X(i, j - 1, k) + X(i, j, k - 1) - X(i, j - 1, k - 1)) * dyinv;
+    double pz_hi_md_lo = 0.5 * (X(i + 1, j, k) + X(i, j, k) - X(i + 1, j, k - 1) - X(i, j, k - 1));
+    double h_xi = 0.25 * (Z(i + 2, j, k) - Z(i, j, k) + Z(i + 2, j + 1, k) - Z(i, j + 1, k)) * dxinv;
+    double h_zeta = 0.25 * (Z(i + 1, j, k + 1) - Z(i + 1, j, k - 1) + Z(i + 1, j + 1, k + 1) - Z(i + 1, j + 1, k - 1));
+    pz_hi_md_lo *= h_xi / h_zeta;
+    double pz_lo_md_lo = 0.5 * (X(i, j, k) + X(i - 1, j, k) - X(i, j, k - 1) - X(i - 1, j, k - 1));
+    h_xi = 0.25 * (Z(i + 1, j, k) - Z(i - 1, j, k) + Z(i + 1, j + 1, k) - Z(i - 1, j + 1, k)) * dxinv;
+    h_zeta = 0.25 * (Z(i, j, k + 1) - Z(i, j, k - 1) + Z(i, j + 1, k + 1) - Z(i, j + 1, k - 1));
+    pz_lo_md_lo *= h_xi / h_zeta;
+    double pz_md_hi_lo = 0.5 * (X(i, j + 1, k) + X(i, j, k) - X(i, j + 1, k - 1) - X(i, j, k - 1));
+    double h_eta = 0.25 * (Z(i, j + 2, k) - Z(i, j, k) + Z(i + 1, j + 2, k) - Z(i + 1, j, k)) * dyinv;
+    h_zeta = 0.25 * (Z(i, j + 1, k + 1) - Z(i, j + 1, k - 1) + Z(i + 1, j + 1, k + 1) - Z(i + 1, j + 1, k - 1));
+    pz_md_hi_lo *= h_eta / h_zeta;
+    double pz_md_lo_lo = 0.5 * (X(i, j, k) + X(i, j - 1, k) - X(i, j, k - 1) - X(i, j - 1, k - 1));
+    h_eta = 0.25 * (Z(i, j + 1, k) - Z(i, j - 1, k) + Z(i + 1, j + 1, k) - Z(i + 1, j - 1, k)) * dyinv;
+    h_zeta = 0.25 * (Z(i, j, k + 1) - Z(i, j, k - 1) + Z(i + 1, j, k + 1) - Z(i + 1, j, k - 1));
+    pz_md_lo_lo *= h_eta / h_zeta;
+    const double h_xi_on_zlo = 0.5 * (Z(i + 1, j + 1, k) + Z(i + 1, j, k) - Z(i, j + 1, k) - Z(i, j, k)) * dxinv;
+    const double h_eta_on_zlo = 0.5 * (Z(i + 1, j + 1, k) + Z(i, j + 1, k) - Z(i + 1, j, k) - Z(i, j, k)) * dyinv;
+    return 0.5 * h_xi_on_zlo * ((px_hi_md_lo + px_lo_md_lo) - (pz_hi_md_lo + pz_lo_md_lo))
+         + 0.5 * h_eta_on_zlo * ((py_md_hi_lo + py_md_lo_lo) - (pz_md_hi_lo + pz_md_lo_lo));
+}
+
 #undef X
 #undef Z
+
+/* The z-faces whose flux the split correction touches: not the ground, not a
+ * Neumann top (Source/Poisson.cpp:233-235, 246-249). */
+static int cross_face(const og_grid* g, const int* bc, int kf)
+{
+    return kf != 0 && !(kf == g->nz && bc[FACE_ZHI] == PF_NEUMANN);
+}
+
+/* PoissonSolver::Op::add_cross (Source/Poisson.cpp:229-253):
+ * y += (1/J) d_zeta (a_z d cross) with d = beta_z - z_cross per z-face.
+ * phi's ghosts filled for the boundary types. */
+void og_poisson_add_cross(const og_grid* g, const int* bc, const double* az, const double* d, const double* J,
+                          const double* z, const double* phi, double* y)
+{
+    const double dzinv = 1.0 / g->dzeta;
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = 0; k < g->nz; ++k) {
+        for (int j = 0; j < g->ny; ++j) {
+            for (int i = 0; i < g->nx; ++i) {
+                double hi = 0, lo = 0;
+                if (cross_face(g, bc, k + 1)) {
+                    hi = az[IX(g, i, j, k + 1)] * d[IX(g, i, j, k + 1)] * z_face_cross(g, i, j, k + 1, phi, z);
+                }
+                if (cross_face(g, bc, k)) {
+                    lo = az[IX(g, i, j, k)] * d[IX(g, i, j, k)] * z_face_cross(g, i, j, k, phi, z);
+                }
+                y[IX(g, i, j, k)] += (hi - lo) * dzinv / J[IX(g, i, j, k)];
+            }
+        }
+    }
+}
+
+/* PoissonSolver::Op::add_cross_flux (Source/Poisson.cpp:255-273):
+ * F_z -= d cross on the same faces. phi's ghosts filled. */
+void og_poisson_cross_flux(const og_grid* g, const int* bc, const double* d, const double* z, const double* phi,
+                           double* fz)
+{
+    for (int k = 0; k <= g->nz; ++k) {
+        if (!cross_face(g, bc, k)) { continue; }
+        for (int j = 0; j < g->ny; ++j) {
+            for (int i = 0; i < g->nx; ++i) {
+                fz[IX(g, i, j, k)] -= d[IX(g, i, j, k)] * z_face_cross(g, i, j, k, phi, z);
+            }
+        }
+    }
+}
 
 /* TerrainPoisson::apply (ERF_TerrainPoisson.cpp:74-101): ghosts for the BC
  * (ground even), then the operator with the premultiplied areas a beta. */
@@ -405,6 +483,9 @@ typedef struct og_mg {
     og_level lev[OG_MAX_LEVELS];
     int bc[6];
     int nu1, nu2, nu_coarse;
+    /* the split z-face correction of the Krylov operator (null: none): the raw
+     * z areas and d = beta_z - z_cross per z-face; the V-cycle never sees it */
+    double *cross_az, *cross_d;
 } og_mg;
 
 /* The coarse grid of a level: x and y halved, z kept. */
@@ -532,8 +613,37 @@ void og_mg_destroy(og_mg* mg)
         free(L->b);
         free(L->r);
     }
+    free(mg->cross_az);
+    free(mg->cross_d);
     free(mg);
 }
+
+/* FaceCoeffs::z_cross (Source/Poisson.cpp:461-479): d = (beta_z or 1) -
+ * z_cross on the z-faces, used by the solver's operator and fluxes; z_cross
+ * null removes it. */
+void og_mg_set_cross(og_mg* mg, const double* az, const double* bz, const double* z_cross)
+{
+    free(mg->cross_az);
+    free(mg->cross_d);
+    mg->cross_az = mg->cross_d = NULL;
+    if (!z_cross) { return; }
+    const int64_t vol = VOL(&mg->lev[0].g);
+    mg->cross_az = (double*)malloc(sizeof(double) * (size_t)vol);
+    mg->cross_d = (double*)malloc(sizeof(double) * (size_t)vol);
+    memcpy(mg->cross_az, az, sizeof(double) * (size_t)vol);
+    for (int64_t n = 0; n < vol; ++n) { mg->cross_d[n] = (bz ? bz[n] : 1.0) - z_cross[n]; }
+}
+
+/* PoissonSolver::Op::apply (Source/Poisson.cpp:148-156): the terrain operator
+ * plus the split correction when set. */
+static void mg_apply(og_mg* mg, double* phi, double* y)
+{
+    og_level* L = &mg->lev[0];
+    og_poisson_apply(&L->g, mg->bc, L->AX, L->AY, L->AZ, L->J, L->z, phi, y);
+    if (mg->cross_d) { og_poisson_add_cross(&L->g, mg->bc, mg->cross_az, mg->cross_d, L->J, L->z, phi, y); }
+}
+
+void og_mg_apply(og_mg* mg, double* phi, double* y) { mg_apply(mg, phi, y); }
 
 int og_mg_levels(const og_mg* mg) { return mg->nlev; }
 void og_mg_level_dims(const og_mg* mg, int l, int* nx, int* ny, int* nz)
@@ -815,7 +925,7 @@ int og_poisson_solve(og_mg* mg, double* rhs, double* phi, double reltol, double 
     int it = 0, converged = (bnorm <= tol);
     while (!converged && it < max_iter) {
         /* r = rhs - A phi */
-        og_poisson_apply(g, mg->bc, L->AX, L->AY, L->AZ, L->J, L->z, phi, t);
+        mg_apply(mg, phi, t);
         memset(w, 0, sizeof(double) * vol);
         for (int k = 0; k < g->nz; ++k) {
             for (int j = 0; j < g->ny; ++j) {
@@ -832,7 +942,7 @@ int og_poisson_solve(og_mg* mg, double* rhs, double* phi, double reltol, double 
             double* vj = V + (size_t)jj * vol;
             double* zj = Zs + (size_t)jj * vol;
             if (precond) { og_mg_vcycle(mg, vj, zj); } else { memcpy(zj, vj, sizeof(double) * vol); }
-            og_poisson_apply(g, mg->bc, L->AX, L->AY, L->AZ, L->J, L->z, zj, w);
+            mg_apply(mg, zj, w);
             /* modified Gram-Schmidt */
             for (int q = 0; q <= jj; ++q) {
                 const double* vq = V + (size_t)q * vol;
@@ -888,7 +998,7 @@ int og_poisson_solve(og_mg* mg, double* rhs, double* phi, double reltol, double 
         memset(H, 0, sizeof(double) * (m + 1) * m);
     }
     if (singular) { add_const_valid(g, phi, -og_weighted_mean(g, phi, L->J)); }
-    og_poisson_apply(g, mg->bc, L->AX, L->AY, L->AZ, L->J, L->z, phi, t);
+    mg_apply(mg, phi, t);
     double rn = 0;
     for (int k = 0; k < g->nz; ++k) {
         for (int j = 0; j < g->ny; ++j) {

@@ -57,8 +57,13 @@ typedef struct og_mg og_mg;
 og_mg* og_mg_create(const og_grid* g, const int* bc, const double* z, const double* J, const double* AX,
                     const double* AY, const double* AZ, int max_levels, int min_coarse, int nu1, int nu2, int nu_coarse);
 void og_mg_destroy(og_mg* mg);
+void og_mg_set_cross(og_mg* mg, const double* az, const double* bz, const double* z_cross);
+void og_poisson_cross_flux(const og_grid* g, const int* bc, const double* d, const double* z, const double* phi,
+                           double* fz);
 int og_poisson_solve(og_mg* mg, double* rhs, double* phi, double reltol, double abstol, int max_iter, int restart,
                      int precond, double* res);
+void og_face_divergence(const og_grid* g, const double* ax, const double* ay, const double* az, const double* J,
+                        const double* fx, const double* fy, const double* fz, double* div);
 
 static double* zalloc(const og_grid* g) { return (double*)calloc(VOL(g), sizeof(double)); }
 static int ext(const og_grid* g, int t, int d) { return ((d == 0) ? g->nx : (d == 1) ? g->ny : g->nz) + nodal(t, d); }
@@ -1124,6 +1129,48 @@ static void init_poisson_bc(const og_grid* g, const gb_bc* bc, int* pbc)
  * with Sigma = alpha^2 I (alpha_h = alpha_v). info: [divergence before,
  * divergence after, Poisson iterations, final Poisson residual]. Returns 0,
  * or -2 on a Poisson failure. */
+/* obrien_omega (Source/Initializer.cpp:197-274): Omega on the z-faces from the
+ * column continuity of (a_x u, a_y v) from Omega = 0 at the ground,
+ * a_z Omega_{k+1/2} = a_z Omega_{k-1/2} - J_k Dh_k dzeta with Dh the horizontal
+ * part of face_divergence, then the column's top value E removed with the
+ * weight ((z_f - z_ground) / depth)^2 of the face's node-mean height, the top
+ * face set to 0 exactly. Returns max |E| over the columns. */
+double og_obrien_omega(const og_grid* g, const double* u, const double* v, const double* z, const double* ax,
+                       const double* ay, const double* az, const double* J, double* om)
+{
+    double* zero = zalloc(g);
+    double* dh = zalloc(g);
+    og_face_divergence(g, ax, ay, az, J, u, v, zero, dh);
+    const double dzeta = g->dzeta;
+    double worst = 0;
+    for (int j = 0; j < g->ny; ++j) {
+        for (int i = 0; i < g->nx; ++i) {
+            om[IX(g, i, j, 0)] = 0;
+            for (int k = 0; k < g->nz; ++k) {
+                om[IX(g, i, j, k + 1)] = (az[IX(g, i, j, k)] * om[IX(g, i, j, k)]
+                                          - J[IX(g, i, j, k)] * dh[IX(g, i, j, k)] * dzeta)
+                                         / az[IX(g, i, j, k + 1)];
+            }
+            const double E = om[IX(g, i, j, g->nz)];
+            worst = fmax(worst, fabs(E));
+            const double zg = 0.25 * (z[IX(g, i, j, 0)] + z[IX(g, i + 1, j, 0)] + z[IX(g, i, j + 1, 0)]
+                                      + z[IX(g, i + 1, j + 1, 0)]);
+            const double depth = 0.25 * (z[IX(g, i, j, g->nz)] + z[IX(g, i + 1, j, g->nz)] + z[IX(g, i, j + 1, g->nz)]
+                                         + z[IX(g, i + 1, j + 1, g->nz)]) - zg;
+            for (int k = 1; k <= g->nz; ++k) {
+                const double zf = 0.25 * (z[IX(g, i, j, k)] + z[IX(g, i + 1, j, k)] + z[IX(g, i, j + 1, k)]
+                                          + z[IX(g, i + 1, j + 1, k)]);
+                const double frac = (zf - zg) / depth;
+                om[IX(g, i, j, k)] -= frac * frac * E;
+            }
+            om[IX(g, i, j, g->nz)] = 0;
+        }
+    }
+    free(zero);
+    free(dh);
+    return worst;
+}
+
 int og_initialize(const og_grid* g, const gb_bc* bc, const gb_init_opts* io, gb_state* q, const gb_mesh_fields* m,
                   double* info)
 {
@@ -1144,7 +1191,15 @@ int og_initialize(const og_grid* g, const gb_bc* bc, const gb_init_opts* io, gb_
     memset(q->theta, 0, sizeof(double) * (size_t)vol);
     fill_theta_ref(g, bc, z, q->theta);
     memset(q->p, 0, sizeof(double) * (size_t)vol);
-    info[0] = info[1] = info[2] = info[3] = 0;
+    info[0] = info[1] = info[2] = info[3] = info[4] = 0;
+    /* 3. O'Brien: w0 from the column continuity, the top residual removed
+     * (Source/Initializer.cpp:326-333) */
+    if (io->obrien) {
+        double* om0 = zalloc(g);
+        info[4] = og_obrien_omega(g, q->u, q->v, z, m->ax, m->ay, m->az, m->detJ, om0);
+        og_w_from_omega(g, q->u, q->v, om0, z, q->w);
+        free(om0);
+    }
     int status = 0;
     double* rhs = zalloc(g);
     og_velocity_divergence(g, q->u, q->v, q->w, z, m->ax, m->ay, m->az, m->detJ, rhs);
@@ -1152,21 +1207,30 @@ int og_initialize(const og_grid* g, const gb_bc* bc, const gb_init_opts* io, gb_
     if (io->projection) {
         int pbc[6];
         init_poisson_bc(g, bc, pbc);
-        const double a2 = io->alpha_h * io->alpha_h;
+        /* Sigma = diag(alpha_h^2, alpha_h^2, alpha_v^2): x, y and the cross part
+         * of the z-faces carry alpha_h^2, the z part alpha_v^2; the split only
+         * when alpha_v != alpha_h (Source/Initializer.cpp:380-403) */
+        const double ah2 = io->alpha_h * io->alpha_h, av2 = io->alpha_v * io->alpha_v;
         const int unit = (io->alpha_h == 1 && io->alpha_v == 1);
-        double* beta = zalloc(g);
-        for (int64_t n = 0; n < vol; ++n) { beta[n] = a2; }
+        const int split = (io->alpha_v != io->alpha_h);
+        double* bh = zalloc(g);
+        double* bv = zalloc(g);
+        for (int64_t n = 0; n < vol; ++n) {
+            bh[n] = ah2;
+            bv[n] = av2;
+        }
         double* AX = zalloc(g);
         double* AY = zalloc(g);
         double* AZ = zalloc(g);
         for (int64_t n = 0; n < vol; ++n) {
-            AX[n] = unit ? m->ax[n] : m->ax[n] * a2;
-            AY[n] = unit ? m->ay[n] : m->ay[n] * a2;
-            AZ[n] = unit ? m->az[n] : m->az[n] * a2;
+            AX[n] = unit ? m->ax[n] : m->ax[n] * ah2;
+            AY[n] = unit ? m->ay[n] : m->ay[n] * ah2;
+            AZ[n] = unit ? m->az[n] : m->az[n] * av2;
         }
         const gb_poisson_opts* po = &io->poisson;
         og_mg* mg = og_mg_create(g, pbc, z, m->detJ, AX, AY, AZ, po->max_levels, po->min_coarse, po->nu1, po->nu2,
                                  po->nu_coarse);
+        if (split) { og_mg_set_cross(mg, m->az, bv, bh); }
         double* lam = zalloc(g);
         double res[3];
         const int it = og_poisson_solve(mg, rhs, lam, po->reltol, po->abstol, po->max_iter, po->restart, 1, res);
@@ -1175,7 +1239,13 @@ int og_initialize(const og_grid* g, const gb_bc* bc, const gb_init_opts* io, gb_
         info[2] = it;
         info[3] = res[1];
         double* F[3] = {zalloc(g), zalloc(g), zalloc(g)};
-        og_poisson_fluxes(g, pbc, z, lam, unit ? NULL : beta, unit ? NULL : beta, unit ? NULL : beta, F[0], F[1], F[2]);
+        og_poisson_fluxes(g, pbc, z, lam, unit ? NULL : bh, unit ? NULL : bh, unit ? NULL : bv, F[0], F[1], F[2]);
+        if (split) {
+            double* d = zalloc(g);
+            for (int64_t n = 0; n < vol; ++n) { d[n] = bv[n] - bh[n]; }
+            og_poisson_cross_flux(g, pbc, d, z, lam, F[2]);
+            free(d);
+        }
         og_omega_from_w(g, q->u, q->v, q->w, z, om, 0);
         double* tgt[3] = {q->u, q->v, om};
         const int tt[3] = {XF, YF, ZF};
@@ -1192,7 +1262,8 @@ int og_initialize(const og_grid* g, const gb_bc* bc, const gb_init_opts* io, gb_
         og_velocity_divergence(g, q->u, q->v, q->w, z, m->ax, m->ay, m->az, m->detJ, rhs);
         info[1] = norm2_valid(g, rhs);
         for (int c = 0; c < 3; ++c) { free(F[c]); }
-        free(beta);
+        free(bh);
+        free(bv);
         free(AX);
         free(AY);
         free(AZ);

@@ -136,6 +136,51 @@ def askervein_case():
                 info=__import__("json").loads(str(d["info"])))
 
 
+def init_askervein_case():
+    """The reference's Mass_Consistent_Askervein regression (Tests/Initialization/
+    Mass_Consistent_Askervein/inputs_init_askervein) on the Poisson_Askervein
+    mesh: log-law first guess along x (u* 0.6 m/s, z0 0.03 m, kappa 0.41,
+    Cmu0 0.5562, l_max 30 m), inflow at xlo, outflow at xhi, slip walls in y
+    and at the top; the ground (surface_layer there) is a wall; theta 300 K;
+    alpha_h 1, alpha_v 0.5, reltol 1e-10. Returns (case, bc, init options, gold)
+    with gold's cell fields [k, j, i] and its info."""
+    import json
+    import os
+    import oracle
+    from ablsteadyrans_b200.abi import BC, InitOptions
+    d = np.load(os.path.join(GOLDEN, "poisson_askervein.npz"))
+    gd = np.load(os.path.join(GOLDEN, "init_askervein.npz"))
+    nx, ny, nz = 30, 30, 18
+    plo, phi_hi = d["prob_lo"], d["prob_hi"]
+    g = Grid(nx, ny, nz, (phi_hi[0] - plo[0]) / nx, (phi_hi[1] - plo[1]) / ny, (phi_hi[2] - plo[2]) / nz)
+    z = oracle.btf_heights(g, d["zlevels"], d["ground"])
+    J, ax, ay, az, _ = oracle.metrics(g, z)
+    nu = np.ones_like(J)
+    case = oracle.Case(g, z, J, ax, ay, az, nu, nu, nu)
+    bc = BC.make((1, 3, 4, 2, 3, 3), theta_ref=((0.0,), (300.0,)), ustar=0.6, z0=0.03, kappa=0.41, Cmu0=0.5562,
+                 l_max=30.0)
+    io = InitOptions.make(alpha_h=1.0, alpha_v=0.5)
+    io.poisson.reltol = 1e-10
+    gold = {f: gd[f] for f in ("u", "v", "w", "p", "theta", "tke")}
+    gold["info"] = json.loads(str(gd["info"]))
+    return case, bc, io, gold
+
+
+def gold_cell_fields(g, q):
+    """The reference plotfile's cell values (Source/StateIO.cpp:59-74): u, v, w
+    the means of the cell's two faces, the cell fields as they are; [k, j, i]."""
+    G, nx, ny, nz = g.ng, g.nx, g.ny, g.nz
+    c = (slice(G, G + nz), slice(G, G + ny), slice(G, G + nx))
+    out = {
+        "u": 0.5 * (q["u"][c] + q["u"][G:G + nz, G:G + ny, G + 1:G + nx + 1]),
+        "v": 0.5 * (q["v"][c] + q["v"][G:G + nz, G + 1:G + ny + 1, G:G + nx]),
+        "w": 0.5 * (q["w"][c] + q["w"][G + 1:G + nz + 1, G:G + ny, G:G + nx]),
+    }
+    for f in ("p", "theta", "tke"):
+        out[f] = q[f][c]
+    return out
+
+
 def smooth_terrain_case(nx, ny, nz, periodic_x, periodic_y, hill=80.0, dx=40.0, seed=0):
     """A BTF mesh over a smooth Gaussian hill (periodic images or clamped
     ghost columns as the reference builds them), stretched layers to 1500 m."""

@@ -243,3 +243,52 @@ def test_gpu_poisson_refusals(ctx):
     with pytest.raises(gb.GustError, match="solver.poisson_reltol"):
         gb.PoissonSolver(ctx, g, dz, dJ, (PERIODIC, NEUMANN, NEUMANN, PERIODIC, NEUMANN, DIRICHLET),
                          gb.PoissonOptions.default(reltol=2.0))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("top", [NEUMANN, DIRICHLET])
+def test_gpu_split_operator_fluxes_and_solve_match_oracle(ctx, top):
+    """FaceCoeffs::z_cross (beta_h = 1 on x, y and the cross part, beta_z =
+    0.25): the GPU operator and fluxes equal the oracle's to 1e-12 relative
+    (the top face's cross term counted when the top is not Neumann), and the
+    split solve's potential agrees to 1e-9."""
+    import ablsteadyrans_b200 as gb
+    g, z, J, ax, ay, az, _ = smooth_terrain_case(24, 20, 12, False, False, hill=200.0)
+    bc = (DIRICHLET, NEUMANN, NEUMANN, DIRICHLET, NEUMANN, top)
+    bh = np.ones_like(ax)
+    bv = np.full_like(ax, 0.25)
+    rng = np.random.default_rng(12)
+    phi = g.np_zeros()
+    phi[g.valid(0)] = rng.standard_normal(phi[g.valid(0)].shape)
+    y_ref = oracle.poisson_apply_split(g, bc, ax, ay, az, J, z, phi.copy(), bh, bh, bv, bh)
+    F_ref = oracle.poisson_fluxes_split(g, bc, z, phi.copy(), bh, bh, bv, bh)
+    dz, dJ, dax, day, daz = _gpu_case(g, z, J, ax, ay, az)
+    dbh, dbv = to_dev(bh), to_dev(bv)
+    ps = gb.PoissonSolver(ctx, g, dz, dJ, bc, gb.PoissonOptions.default(reltol=1e-12))
+    ps.set_coeffs(dax, day, daz, dbh, dbh, dbv)
+    ps.set_z_cross(daz, dbv, dbh)
+    y = to_host(ps.apply(to_dev(phi)))
+    v = g.valid(0)
+    assert np.abs(y[v] - y_ref[v]).max() <= 1e-12 * np.abs(y_ref[v]).max()
+    F = [to_host(f) for f in ps.fluxes(to_dev(phi), dbh, dbh, dbv)]
+    for d in range(3):
+        vf = g.valid(1 << d)
+        assert np.abs(F[d][vf] - F_ref[d][vf]).max() <= 1e-12 * np.abs(F_ref[d][vf]).max(), d
+    # the split solve against the oracle's
+    b = g.np_zeros()
+    b[v] = rng.standard_normal(b[v].shape)
+    mg = oracle.Multigrid(g, bc, z, J, ax * bh, ay * bh, az * bv)
+    mg.set_cross(az, bv, bh)
+    phi_ref, it_ref, *_ = mg.solve(b.copy(), reltol=1e-12, max_iter=200)
+    assert it_ref > 0
+    out = to_dev(g.np_zeros())
+    res = ps.solve(to_dev(b), out)
+    assert res.final_residual <= 1e-12 * res.initial_residual * 1.01
+    got = to_host(out)
+    assert np.abs(got[v] - phi_ref[v]).max() <= 1e-9 * np.abs(phi_ref[v]).max()
+    # removing the split gives back the plain operator
+    ps.set_z_cross(None, None, None)
+    y0 = to_host(ps.apply(to_dev(phi)))
+    y0_ref = oracle.poisson_apply(g, bc, ax * bh, ay * bh, az * bv, J, z, phi.copy())
+    assert np.abs(y0[v] - y0_ref[v]).max() <= 1e-12 * np.abs(y0_ref[v]).max()
+    ps.close()

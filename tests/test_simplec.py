@@ -177,6 +177,112 @@ def test_oracle_initializer_is_mass_consistent(name):
     assert np.abs(om[G, G:G + g.ny, G:G + g.nx]).max() <= 1e-12 * np.abs(case.q["u"]).max()
 
 
+def test_oracle_initializer_askervein_matches_reference_gold():
+    """The reference's Mass_Consistent_Askervein regression: the split
+    projection (alpha_h = 1, alpha_v = 0.5; FaceCoeffs::z_cross) on ERF's
+    Askervein mesh gives the gold u, v, w, k, theta (cell values, faces
+    averaged) at 1e-8 relative, with the gold's divergence before the
+    projection and p' = 0."""
+    from helpers import gold_cell_fields, init_askervein_case
+    case, bc, io, gold = init_askervein_case()
+    rc, info = oracle.initialize(case, bc, io)
+    assert rc == 0
+    assert info[0] == pytest.approx(gold["info"]["div_before"], rel=1e-9)
+    assert info[1] <= io.poisson.reltol * info[0]
+    got = gold_cell_fields(case.grid, case.q)
+    for f in ("u", "v", "w", "tke", "theta"):
+        err = np.abs(got[f] - gold[f]).max() / np.abs(gold[f]).max()
+        assert err < 1e-8, (f, err)
+    assert np.all(got["p"] == 0) and np.all(gold["p"] == 0)
+
+
+def test_oracle_split_operator_matches_split_flux_divergence():
+    """With z_cross the operator stays minus the divergence of its own fluxes
+    (test_Poisson.cpp:321's property, on the split coefficient): A phi =
+    -face_divergence(F(phi)) with F_z = -(beta_z dphi/dz - z_cross cross)."""
+    from helpers import init_askervein_case
+    case, bc, io, gold = init_askervein_case()
+    g = case.grid
+    pbc = (2, 1, 1, 2, 1, 1)
+    rng = np.random.default_rng(11)
+    phi = g.np_zeros()
+    phi[g.valid(0)] = rng.standard_normal(phi[g.valid(0)].shape)
+    bh = np.full_like(case.ax, 1.0)
+    bv = np.full_like(case.ax, 0.25)
+    y = oracle.poisson_apply_split(g, pbc, case.ax, case.ay, case.az, case.J, case.z, phi, bh, bh, bv, bh)
+    F = oracle.poisson_fluxes_split(g, pbc, case.z, phi, bh, bh, bv, bh)
+    div = oracle.face_divergence(g, case.ax, case.ay, case.az, case.J, *F)
+    v = g.valid(0)
+    assert np.abs(y[v] + div[v]).max() <= 1e-10 * np.abs(y[v]).max()
+    # the split changes the operator (the cross part carries beta_h, not beta_z)
+    y0 = oracle.poisson_apply_split(g, pbc, case.ax, case.ay, case.az, case.J, case.z, phi, bh, bh, bv, None)
+    assert np.abs(y0[v] - y[v]).max() > 1e-6 * np.abs(y[v]).max()
+
+
+def _obrien_case(seed=3):
+    from ablsteadyrans_b200.abi import BC
+    from helpers import terrain_simplec_case
+    case = terrain_simplec_case(16, 12, 10, False, True, hill=150.0, seed=seed)
+    bc = BC.make((1, 0, 4, 2, 0, 3), theta_ref=((0.0, 500.0, 1500.0), (300.0, 301.5, 305.0)), ustar=0.4, z0=0.1,
+                 direction=30.0)
+    return case, bc
+
+
+def test_oracle_obrien_column_correction():
+    """O'Brien (Initializer.OBrienColumnCorrection, test_Initializer.cpp:662-737):
+    Omega vanishes at the ground and the top exactly, each cell keeps the
+    weight difference times its column's residual E, the column sum of J D is
+    the residual flux, the worst |E| is the one reported; through the
+    initializer the field differs and the projection still converges."""
+    from ablsteadyrans_b200.abi import InitOptions
+    case, bc = _obrien_case()
+    rc, _ = oracle.initialize(case, bc, InitOptions.make(projection=0))
+    assert rc == 0
+    g = case.grid
+    om, E = oracle.obrien_omega(case)
+    assert E > 1e-3
+    G = g.ng
+    zero = g.np_zeros()
+    u, v = case.q["u"], case.q["v"]
+    d = oracle.face_divergence(g, case.ax, case.ay, case.az, case.J, u, v, om)
+    d0 = oracle.face_divergence(g, case.ax, case.ay, case.az, case.J, u, v, zero)
+    nz, dzeta = g.nz, g.dzeta
+    z = case.z
+    worst = 0.0
+    for j in range(g.ny):
+        for i in range(g.nx):
+            I, Jc = i + G, j + G
+            assert om[G, Jc, I] == 0 and om[G + nz, Jc, I] == 0
+            Jk = case.J[G:G + nz, Jc, I]
+            Ecol = -(Jk * d0[G:G + nz, Jc, I] * dzeta).sum() / case.az[G + nz, Jc, I]
+            worst = max(worst, abs(Ecol))
+            zf = 0.25 * (z[G:G + nz + 1, Jc, I] + z[G:G + nz + 1, Jc, I + 1] + z[G:G + nz + 1, Jc + 1, I]
+                         + z[G:G + nz + 1, Jc + 1, I + 1])
+            depth = zf[-1] - zf[0]
+            assert zf[1] - zf[0] < 0.9 * depth / nz   # stretched: the index weight would differ
+            f = (zf - zf[0]) / depth
+            azc = case.az[G:G + nz + 1, Jc, I]
+            want = -(f[1:] ** 2 * azc[1:] - f[:-1] ** 2 * azc[:-1]) * Ecol / (Jk * dzeta)
+            got = d[G:G + nz, Jc, I]
+            assert np.all(np.abs(got - want) <= 1e-11 * (np.abs(d0[G:G + nz, Jc, I]) + np.abs(want)))
+            total = (Jk * got).sum()
+            assert total == pytest.approx(-Ecol * azc[-1] / dzeta, rel=1e-11)
+    assert worst == pytest.approx(E, rel=1e-12)
+    # through the initializer
+    co, _ = _obrien_case()
+    cp, _ = _obrien_case()
+    io = InitOptions.make(obrien=1)
+    io.poisson.reltol = 1e-11
+    ro, info_o = oracle.initialize(co, bc, io)
+    io.obrien = 0
+    rp, info_p = oracle.initialize(cp, bc, io)
+    assert ro == 0 and rp == 0
+    assert info_o[4] == pytest.approx(E, rel=1e-12) and info_p[4] == 0
+    assert info_o[0] != info_p[0]
+    assert info_o[1] < 10 * 1e-11 * info_o[0]
+    assert np.abs(co.q["w"] - cp.q["w"]).max() > 1e-3
+
+
 def test_oracle_initializer_projection_off_keeps_the_first_guess():
     from ablsteadyrans_b200.abi import InitOptions
     case, bc = _init_case("inflow_x")

@@ -188,20 +188,21 @@ def test_gpu_line_sweep_option_refusals(ctx):
 # ----------------------------------------------------- mass-consistent init
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("alpha", [1.0, 0.5])
+@pytest.mark.parametrize("alpha", [(1.0, 1.0), (0.5, 0.5), (1.0, 0.5)])
 @pytest.mark.parametrize("name", list(CONFIGS))
 def test_gpu_initializer_matches_oracle(ctx, name, alpha):
     """gust::initialize_state (init.first_guess = profile, projection on) on
     the B200 against the oracle: every field to 1e-9 relative (the
     projections to 1e-11), the divergence removed, the same iteration count;
-    alpha_h = alpha_v = alpha (Sigma = alpha^2 I)."""
+    Sigma = diag(alpha_h^2, alpha_h^2, alpha_v^2), the split z-face
+    coefficient where alpha_v != alpha_h."""
     from ablsteadyrans_b200.abi import InitOptions
     from ablsteadyrans_b200.simplec import DeviceCase, SimplecStage
     case, bc = make(name, seed=5)
     ph = physics(case)
     dc = DeviceCase.from_oracle(case)
     st = SimplecStage(ctx, dc, bc, ph, SimplecOptions.make())
-    io = InitOptions.make(alpha_h=alpha, alpha_v=alpha, k_decay_height=600.0, z_agl_min=1.0)
+    io = InitOptions.make(alpha_h=alpha[0], alpha_v=alpha[1], k_decay_height=600.0, z_agl_min=1.0)
     io.poisson.reltol = 1e-11
     rc, info = oracle.initialize(case, bc, io)
     assert rc == 0
@@ -226,8 +227,56 @@ def test_gpu_initializer_refusals(ctx):
     case, bc = make(list(CONFIGS)[0], seed=5)
     dc = DeviceCase.from_oracle(case)
     st = SimplecStage(ctx, dc, bc, physics(case), SimplecOptions.make())
-    for kw, msg in (({"alpha_v": 0.5}, "split z-face coefficient"), ({"obrien": 1}, "init.obrien = 1"),
+    for kw, msg in (({"obrien": 2}, "init.obrien must be 0 or 1"),
                     ({"z_agl_min": -1.0}, "init.z_agl_min"), ({"alpha_h": 0.0, "alpha_v": 0.0}, "init.alpha_h")):
         with pytest.raises(gb.GustError, match=msg):
             st.initialize(InitOptions.make(**kw))
+    st.close()
+
+
+@pytest.mark.gpu
+def test_gpu_initializer_askervein_matches_reference_gold(ctx):
+    """The reference's Mass_Consistent_Askervein regression on the B200: the
+    split projection (alpha_h = 1, alpha_v = 0.5) gives the gold u, v, w, k
+    and theta (cell values, faces averaged) at 1e-8 relative."""
+    from ablsteadyrans_b200.simplec import DeviceCase, SimplecStage
+    from helpers import gold_cell_fields, init_askervein_case
+    case, bc, io, gold = init_askervein_case()
+    dc = DeviceCase.from_oracle(case)
+    st = SimplecStage(ctx, dc, bc, physics(case), SimplecOptions.make())
+    res = st.initialize(io)
+    assert res.divergence_before == pytest.approx(gold["info"]["div_before"], rel=1e-9)
+    assert res.divergence_after <= io.poisson.reltol * res.divergence_before
+    got = gold_cell_fields(case.grid, {f: dc.host(f) for f in FIELDS})
+    for f in ("u", "v", "w", "tke", "theta"):
+        err = np.abs(got[f] - gold[f]).max() / np.abs(gold[f]).max()
+        assert err < 1e-8, (f, err)
+    st.close()
+
+
+@pytest.mark.gpu
+def test_gpu_initializer_obrien_matches_oracle(ctx):
+    """init.obrien = 1 on the B200 against the oracle: the column pass's top
+    residual to 1e-12, every field to 1e-9 after the projection."""
+    from ablsteadyrans_b200.abi import BC, InitOptions
+    from ablsteadyrans_b200.simplec import DeviceCase, SimplecStage
+    from helpers import terrain_simplec_case
+    case = terrain_simplec_case(16, 12, 10, False, True, hill=150.0, seed=3)
+    bc = BC.make((1, 0, 4, 2, 0, 3), theta_ref=((0.0, 500.0, 1500.0), (300.0, 301.5, 305.0)), ustar=0.4, z0=0.1,
+                 direction=30.0)
+    dc = DeviceCase.from_oracle(case)
+    st = SimplecStage(ctx, dc, bc, physics(case), SimplecOptions.make())
+    io = InitOptions.make(obrien=1, alpha_v=0.5)
+    io.poisson.reltol = 1e-11
+    rc, info = oracle.initialize(case, bc, io)
+    assert rc == 0 and info[4] > 1e-3
+    res = st.initialize(io)
+    assert res.obrien_top_residual == pytest.approx(info[4], rel=1e-12)
+    assert res.divergence_before == pytest.approx(info[0], rel=1e-11)
+    assert res.poisson_iterations == int(info[2])
+    for f in FIELDS:
+        ref = case.q[f]
+        got = dc.host(f)
+        scale = max(np.abs(ref).max(), 1e-300)
+        assert np.abs(got - ref).max() <= 1e-9 * scale, (f, np.abs(got - ref).max() / scale)
     st.close()
