@@ -6,7 +6,10 @@ import numpy as np
 
 from .grid import GbGrid  # noqa: F401
 
-FACE_PERIODIC, FACE_INFLOW, FACE_OUTFLOW, FACE_SLIP_WALL, FACE_NO_SLIP_WALL = range(5)
+FACE_PERIODIC, FACE_INFLOW, FACE_OUTFLOW, FACE_SLIP_WALL, FACE_NO_SLIP_WALL, FACE_SURFACE_LAYER = range(6)
+SURFACE_NEUTRAL, SURFACE_HEAT_FLUX = range(2)
+WALL_K_DIRICHLET, WALL_K_SOURCE = range(2)
+DENOMINATOR_LOG_LAW, DENOMINATOR_ONE = range(2)
 LIMITER_VAN_LEER, LIMITER_VAN_ALBADA, LIMITER_UPWIND = range(3)
 MAX_PROFILE = 32
 
@@ -35,12 +38,23 @@ class BC(ctypes.Structure):
                 ("zhi_theta_grad", ctypes.c_double), ("inflow_ustar", ctypes.c_double),
                 ("inflow_z0", ctypes.c_double), ("inflow_direction", ctypes.c_double), ("kappa", ctypes.c_double),
                 ("Cmu0", ctypes.c_double), ("inflow_inv_lmax", ctypes.c_double), ("theta_ref_n", ctypes.c_int32),
-                ("theta_ref_z", ctypes.c_double * MAX_PROFILE), ("theta_ref_theta", ctypes.c_double * MAX_PROFILE)]
+                ("theta_ref_z", ctypes.c_double * MAX_PROFILE), ("theta_ref_theta", ctypes.c_double * MAX_PROFILE),
+                ("surface_z0", ctypes.c_double), ("surface_zref", ctypes.c_double),
+                ("surface_stability", ctypes.c_int32), ("surface_heat_flux", ctypes.c_double),
+                ("surface_wall_k", ctypes.c_int32), ("surface_denominator_floor", ctypes.c_int32)]
 
     @classmethod
     def make(cls, faces, theta_ref=((0.0,), (300.0,)), ustar=0.4, z0=0.1, direction=0.0, kappa=0.41, Cmu0=0.5562,
-             l_max=30.0, zhi_theta_grad=0.0, wall_velocity=None):
+             l_max=30.0, zhi_theta_grad=0.0, wall_velocity=None, surface=None):
+        """surface: bc.surface_* of a surface_layer ground as a dict (z0, zref,
+        stability, heat_flux, wall_k, denominator_floor); the reference's
+        defaults (Source/SurfaceLayer.H: z0 0.1 m, first cell centre, neutral,
+        Dirichlet wall k, log-law floor) otherwise."""
         b = cls()
+        b.surface_z0, b.surface_zref, b.surface_stability = 0.1, 0.0, SURFACE_NEUTRAL
+        b.surface_heat_flux, b.surface_wall_k, b.surface_denominator_floor = 0.0, WALL_K_DIRICHLET, DENOMINATOR_LOG_LAW
+        for k, v in (surface or {}).items():
+            setattr(b, "surface_" + k, v)
         for n, f in enumerate(faces):
             b.face[n] = int(f)
         if wall_velocity:
@@ -67,16 +81,26 @@ class Physics(ctypes.Structure):
                 ("pressure_gradient", ctypes.c_double * 3), ("limiter", ctypes.c_int32),
                 ("smooth_eps_velocity", ctypes.c_double), ("smooth_eps_theta", ctypes.c_double),
                 ("log_mean", ctypes.c_int32), ("scale_velocity", ctypes.c_double), ("scale_theta", ctypes.c_double),
-                ("scale_tke", ctypes.c_double), ("scale_height", ctypes.c_double)]
+                ("scale_tke", ctypes.c_double), ("scale_height", ctypes.c_double), ("closure", ctypes.c_int32),
+                ("turb_Cmu0", ctypes.c_double), ("turb_Cb", ctypes.c_double), ("turb_Rt_crit", ctypes.c_double),
+                ("turb_Rt_min", ctypes.c_double), ("turb_max_geom_lscale", ctypes.c_double),
+                ("turb_tke_floor", ctypes.c_double), ("turb_sigma_k", ctypes.c_double),
+                ("turb_nu_molecular", ctypes.c_double), ("turb_alpha_molecular", ctypes.c_double),
+                ("turb_kappa", ctypes.c_double)]
 
     @classmethod
     def make(cls, scale_height, **kw):
         """The reference's defaults (Source/Forcing.H: gravity 9.81, theta0 300, Coriolis
-        off, rotation period 86400 s; convection van Leer, eps 1e-5; JvpScales 10, 10, 0.1)."""
+        off, rotation period 86400 s; convection van Leer, eps 1e-5; JvpScales 10, 10, 0.1;
+        Source/Closure.H: turb.Cmu0 0.5562, Cb 0.35, Rt_crit -1, Rt_min -3,
+        max_geom_lscale 30 m, tke_floor 0, sigma_k 1, molecular 0, kappa 0.41;
+        closure off: the diffusivities are given)."""
         p = cls(gravity=9.81, theta0=300.0, coriolis=0, coriolis_3d=1, geostrophic=0, latitude=0.0,
                 rotation_period=86400.0, ug=0.0, vg=0.0, limiter=LIMITER_VAN_LEER, smooth_eps_velocity=1e-5,
                 smooth_eps_theta=1e-5, log_mean=0, scale_velocity=10.0, scale_theta=10.0, scale_tke=0.1,
-                scale_height=scale_height)
+                scale_height=scale_height, closure=0, turb_Cmu0=0.5562, turb_Cb=0.35, turb_Rt_crit=-1.0,
+                turb_Rt_min=-3.0, turb_max_geom_lscale=30.0, turb_tke_floor=0.0, turb_sigma_k=1.0,
+                turb_nu_molecular=0.0, turb_alpha_molecular=0.0, turb_kappa=0.41)
         for k, v in kw.items():
             if k == "pressure_gradient":
                 for d in range(3):
@@ -136,7 +160,8 @@ class State(ctypes.Structure):
 
 
 class MeshFields(ctypes.Structure):
-    _fields_ = [("detJ", ctypes.c_void_p), ("ax", ctypes.c_void_p), ("ay", ctypes.c_void_p), ("az", ctypes.c_void_p)]
+    _fields_ = [("detJ", ctypes.c_void_p), ("ax", ctypes.c_void_p), ("ay", ctypes.c_void_p), ("az", ctypes.c_void_p),
+                ("z0", ctypes.c_void_p)]
 
 
 class Diffusivities(ctypes.Structure):

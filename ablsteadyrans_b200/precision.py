@@ -38,7 +38,7 @@ def main(argv=None):
     ap.add_argument("--max-iterations", type=int, default=4000)
     ap.add_argument("--n", type=int, default=256)
     ap.add_argument("--nz", type=int, default=96)
-    ap.add_argument("--max-slope", type=float, default=2.0)
+    ap.add_argument("--max-slope", type=float, default=1.0)
     args = ap.parse_args(argv)
     out = {"workload": f"config 2: fractal terrain {args.n}x{args.n}x{args.nz}, dx 30 m, 120 m rms (slopes capped "
                        f"at {args.max_slope}), u* 0.4 m/s, 225 deg"}

@@ -240,7 +240,7 @@ def tile(n, nz, seed, rms=None, ustar=None, z0=None, met=None, dx=30.0, precisio
     return Instance(f"tile-{seed}-{n}x{n}x{nz}", g, zl, ground, bc, ph, opts, ustar, z0, direction)
 
 
-def config2(precision=1, zline_sweeps=4, n=256, nz=96, seed=2, max_slope=2.0):
+def config2(precision=1, zline_sweeps=4, n=256, nz=96, seed=2, max_slope=1.0):
     """Mixed precision against plain FP64 on a 256 x 256 x 96 grid, dx = dy =
     30 m, over seeded fractal terrain (|k|^-3, 120 m rms, minimum 0, scaled
     down where steeper than max_slope); log-law inflow u* = 0.4 m/s from

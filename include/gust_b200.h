@@ -261,10 +261,21 @@ gb_status gb_face_divergence(gb_ctx* ctx, const gb_grid* g, const double* ax, co
 
 /* ---- SIMPLEC stage ------------------------------------------------------ */
 
-/* Domain face types (gust::FaceType, Source/BoundaryConditions.H:91), the
- * subset with no wall model: periodic, inflow (profile), outflow, slip_wall,
- * no_slip_wall. */
-enum { GB_FACE_PERIODIC = 0, GB_FACE_INFLOW = 1, GB_FACE_OUTFLOW = 2, GB_FACE_SLIP_WALL = 3, GB_FACE_NO_SLIP_WALL = 4 };
+/* Domain face types (gust::FaceType, Source/BoundaryConditions.H:91):
+ * periodic, inflow (profile), outflow, slip_wall, no_slip_wall and, on the
+ * ground only, surface_layer (the wall model of Source/SurfaceLayer.H). */
+enum {
+    GB_FACE_PERIODIC = 0,
+    GB_FACE_INFLOW = 1,
+    GB_FACE_OUTFLOW = 2,
+    GB_FACE_SLIP_WALL = 3,
+    GB_FACE_NO_SLIP_WALL = 4,
+    GB_FACE_SURFACE_LAYER = 5
+};
+/* bc.surface_stability, bc.surface_wall_k, bc.surface_denominator_floor. */
+enum { GB_SURFACE_NEUTRAL = 0, GB_SURFACE_HEAT_FLUX = 1 };
+enum { GB_WALL_K_DIRICHLET = 0, GB_WALL_K_SOURCE = 1 };
+enum { GB_DENOMINATOR_LOG_LAW = 0, GB_DENOMINATOR_ONE = 1 };
 /* convection.limiter (Source/Limiter_K.H:21). */
 enum { GB_LIMITER_VAN_LEER = 0, GB_LIMITER_VAN_ALBADA = 1, GB_LIMITER_UPWIND = 2 };
 
@@ -284,10 +295,19 @@ typedef struct gb_bc {
     int32_t theta_ref_n;             /* theta_ref(z): the hydrostatic reference and the inflow's theta */
     double theta_ref_z[GB_MAX_PROFILE];
     double theta_ref_theta[GB_MAX_PROFILE];
+    /* bc.surface_* of a surface_layer ground (gust::SurfaceLayerOptions,
+     * Source/SurfaceLayer.H:120-170, Businger-Dyer functions); kappa and Cmu0
+     * above are the wall law's too. */
+    double surface_z0;               /* bc.surface_z0 (m, > 0), every column's without a map (gb_mesh_fields.z0) */
+    double surface_zref;             /* bc.surface_zref (m, vertical; <= 0: each column's first cell centre) */
+    int32_t surface_stability;       /* GB_SURFACE_NEUTRAL or GB_SURFACE_HEAT_FLUX */
+    double surface_heat_flux;        /* bc.surface_heat_flux (K m/s, upward > 0; heat_flux only) */
+    int32_t surface_wall_k;          /* GB_WALL_K_DIRICHLET or GB_WALL_K_SOURCE */
+    int32_t surface_denominator_floor;  /* GB_DENOMINATOR_LOG_LAW or GB_DENOMINATOR_ONE */
 } gb_bc;
 
-/* The residual's physics inputs (gust::ResidualInputs without a closure and a
- * wall model, Source/Residual.H:61-128; gust::ForcingOptions, Source/Forcing.H). */
+/* The residual's physics inputs (gust::ResidualInputs, Source/Residual.H:61-128;
+ * gust::ForcingOptions, Source/Forcing.H; the closure's turb.* options). */
 typedef struct gb_physics {
     double gravity, theta0;                       /* forcing.gravity, forcing.theta0 */
     int32_t coriolis, coriolis_3d, geostrophic;   /* forcing.coriolis, forcing.coriolis_3d, forcing.geostrophic */
@@ -298,6 +318,17 @@ typedef struct gb_physics {
     int32_t log_mean;                             /* diffusivity face mean: 0 arithmetic, 1 logarithmic */
     double scale_velocity, scale_theta, scale_tke;/* residual scales U, theta_s, k_s (JvpScales) */
     double scale_height;                          /* H (gust::residual_scale_height) */
+    /* The k-L closure (gust::Closure, turb.*: Source/Closure.H:87-110).
+     * closure = 0: the diffusivities are given (gb_diffusivities); 1: nu,
+     * gamma_theta, gamma_tke and the k sources from the closure at the state,
+     * with the wall distance the height above the ground. */
+    int32_t closure;
+    double turb_Cmu0, turb_Cb, turb_Rt_crit, turb_Rt_min; /* turb.Cmu0, Cb, Rt_crit, Rt_min */
+    double turb_max_geom_lscale;                  /* turb.max_geom_lscale (m) */
+    double turb_tke_floor;                        /* turb.tke_floor (0: machine epsilon) */
+    double turb_sigma_k;                          /* turb.sigma_k */
+    double turb_nu_molecular, turb_alpha_molecular; /* turb.nu_molecular, turb.alpha_molecular (m^2/s) */
+    double turb_kappa;                            /* turb.kappa */
 } gb_physics;
 
 /* simplec.* and steady.zline_sweeps (gust::SimplecOptions, Source/Simplec.H:80-90). */
@@ -326,6 +357,12 @@ typedef struct gb_state {
  * gamma_tke: cell arrays with one ghost layer filled). */
 typedef struct gb_mesh_fields {
     const double *detJ, *ax, *ay, *az;
+    /* The ground's roughness per column (bc.surface_z0_file, Source/
+     * SurfaceRoughness.H): a plane of (ny + 1 + 2 ng) rows of sy doubles,
+     * column (i, j) at (j + ng) sy + i + ng, set on the columns -1..nx,
+     * -1..ny (the ghost columns the periodic image or the nearest domain
+     * column); null: bc.surface_z0 everywhere. */
+    const double* z0;
 } gb_mesh_fields;
 typedef struct gb_diffusivities {
     const double *nu, *gamma_theta, *gamma_tke;

@@ -250,6 +250,17 @@ def _declare_simplec(L):
     L.og_initialize.argtypes = [G, ctypes.POINTER(BC), ctypes.POINTER(InitOptions), ctypes.POINTER(State),
                                 ctypes.POINTER(MeshFields), P]
     L.og_initialize.restype = i32
+    L.og_fill_ghosts2.argtypes = [G, ctypes.POINTER(BC), ctypes.POINTER(Physics), P, P, P, P, P, P, P, P, PP]
+    L.og_residual2.argtypes = [G, ctypes.POINTER(BC), ctypes.POINTER(Physics), ctypes.POINTER(State),
+                               ctypes.POINTER(MeshFields), ctypes.POINTER(Diffusivities), PP, PP, PP]
+    L.og_simplec_iterate2.argtypes = [G, ctypes.POINTER(BC), ctypes.POINTER(Physics), ctypes.POINTER(SimplecOptions),
+                                      ctypes.POINTER(State), ctypes.POINTER(MeshFields), ctypes.POINTER(Diffusivities),
+                                      P, PP, ctypes.POINTER(IterInfo), PP, PP]
+    L.og_simplec_iterate2.restype = i32
+    L.og_closure_evaluate.argtypes = [G, ctypes.POINTER(BC), ctypes.POINTER(Physics), P, P, P, P, P, P, P, PP]
+    L.og_surface_state.argtypes = [G, ctypes.POINTER(BC), ctypes.POINTER(Physics), P, P, P, P, P, PP]
+    L.og_surface_state.restype = i32
+    L.og_height_above_ground.argtypes = [G, P, P]
     L.og_obrien_omega.argtypes = [G, P, P, P, P, P, P, P, P]
     L.og_obrien_omega.restype = f64
     L.og_local_dtau.argtypes = [G, P, P, P, P, P, P, f64, P]
@@ -272,11 +283,14 @@ class Case:
 
     FIELDS = ("u", "v", "w", "p", "theta", "tke")
 
-    def __init__(self, grid, z, J, ax, ay, az, nu, gamma_theta, gamma_tke):
+    def __init__(self, grid, z, J, ax, ay, az, nu, gamma_theta, gamma_tke, z0map=None):
         self.grid = grid
         self.z, self.J, self.ax, self.ay, self.az = z, J, ax, ay, az
         self.nu, self.gt, self.gk = nu, gamma_theta, gamma_tke
+        self.z0map = z0map                 # per-column roughness plane (CLOSURE_FIELDS / SURFACE_FIELDS below)
         self.q = {f: grid.np_zeros() for f in self.FIELDS}
+        self.cf = None                     # the closure's fields of the last iteration (with turbulence)
+        self.closure_nu = None             # nu the next local dtau reads (0 before the first iteration)
 
     def state(self):
         from ablsteadyrans_b200.abi import State
@@ -284,16 +298,22 @@ class Case:
 
     def mesh(self):
         from ablsteadyrans_b200.abi import MeshFields
-        return MeshFields(self.J.ctypes.data, self.ax.ctypes.data, self.ay.ctypes.data, self.az.ctypes.data)
+        return MeshFields(self.J.ctypes.data, self.ax.ctypes.data, self.ay.ctypes.data, self.az.ctypes.data,
+                          None if self.z0map is None else self.z0map.ctypes.data)
 
     def diffusivities(self):
         from ablsteadyrans_b200.abi import Diffusivities
         return Diffusivities(self.nu.ctypes.data, self.gt.ctypes.data, self.gk.ctypes.data)
 
     def copy(self):
-        c = Case(self.grid, self.z, self.J, self.ax, self.ay, self.az, self.nu, self.gt, self.gk)
+        c = Case(self.grid, self.z, self.J, self.ax, self.ay, self.az, self.nu, self.gt, self.gk, self.z0map)
         c.q = {f: a.copy() for f, a in self.q.items()}
         return c
+
+    def plane(self):
+        """A zeroed per-column plane of the grid (the layout of z0map and the surface state)."""
+        g = self.grid
+        return np.zeros(int(g.c.sy) * (g.ny + 1 + 2 * g.ng))
 
 
 def _L():
@@ -304,26 +324,72 @@ def _L():
     return L
 
 
-def fill_ghosts(case, bc):
+# The closure's fields (volumes) and the surface state's columns (planes), in the oracle's order.
+CLOSURE_FIELDS = ("nu", "gamma_theta", "gamma_tke", "nut", "length", "Rt", "Ps", "Pb", "eps", "dSdk")
+SURFACE_FIELDS = ("ustar", "speed", "zref", "d0", "inv_L", "tau_x", "tau_y", "tau_z", "drag", "kwall", "area")
+
+
+def _arrays(arrs):
+    return (ctypes.c_void_p * len(arrs))(*[a.ctypes.data for a in arrs])
+
+
+def fill_ghosts(case, bc, phys=None):
+    """BoundaryConditions::fill_ghosts; with a surface_layer ground returns the
+    surface state (dict of planes) the ground fill used."""
     q = case.q
-    _L().og_fill_ghosts(ctypes.byref(case.grid.c), ctypes.byref(bc), *[_p(q[f]) for f in Case.FIELDS], _p(case.z))
+    ss = [case.plane() for _ in SURFACE_FIELDS]
+    _L().og_fill_ghosts2(ctypes.byref(case.grid.c), ctypes.byref(bc), None if phys is None else ctypes.byref(phys),
+                         _p(case.z0map), *[_p(q[f]) for f in Case.FIELDS], _p(case.z), _arrays(ss))
+    return dict(zip(SURFACE_FIELDS, ss))
 
 
-def residual(case, bc, phys):
-    """Residual.cpp:159-256 at the case's state (ghosts filled by the caller)."""
+def residual(case, bc, phys, fields=False):
+    """Residual.cpp:159-256 at the case's state (ghosts filled by the caller);
+    with fields=True also (closure fields, surface state) as dicts."""
     R = [case.grid.np_zeros() for _ in range(6)]
-    arr = (ctypes.c_void_p * 6)(*[r.ctypes.data for r in R])
+    cf = [case.grid.np_zeros() for _ in CLOSURE_FIELDS]
+    ss = [case.plane() for _ in SURFACE_FIELDS]
     st, m, d = case.state(), case.mesh(), case.diffusivities()
-    _L().og_residual(ctypes.byref(case.grid.c), ctypes.byref(bc), ctypes.byref(phys), ctypes.byref(st), ctypes.byref(m),
-                     ctypes.byref(d), arr)
+    _L().og_residual2(ctypes.byref(case.grid.c), ctypes.byref(bc), ctypes.byref(phys), ctypes.byref(st), ctypes.byref(m),
+                      ctypes.byref(d), _arrays(R), _arrays(cf), _arrays(ss))
+    if fields:
+        return R, dict(zip(CLOSURE_FIELDS, cf)), dict(zip(SURFACE_FIELDS, ss))
     return R
 
 
-def local_dtau(case, cfl, use_nu=True):
+def closure_fields(case, bc, phys):
+    """Closure::evaluate at the case's state (ghosts filled): dict of volumes."""
+    q = case.q
+    cf = [case.grid.np_zeros() for _ in CLOSURE_FIELDS]
+    _L().og_closure_evaluate(ctypes.byref(case.grid.c), ctypes.byref(bc), ctypes.byref(phys), _p(q["u"]), _p(q["v"]),
+                             _p(q["w"]), _p(q["theta"]), _p(q["tke"]), _p(case.z), _p(case.z0map), _arrays(cf))
+    return dict(zip(CLOSURE_FIELDS, cf))
+
+
+def surface_state(case, bc, phys):
+    """compute_surface_state's columns (ghosts filled): (dict of planes, bad columns)."""
+    q = case.q
+    ss = [case.plane() for _ in SURFACE_FIELDS]
+    bad = _L().og_surface_state(ctypes.byref(case.grid.c), ctypes.byref(bc), ctypes.byref(phys), _p(q["u"]), _p(q["v"]),
+                                _p(q["w"]), _p(case.z), _p(case.z0map), _arrays(ss))
+    return dict(zip(SURFACE_FIELDS, ss)), int(bad)
+
+
+def height_above_ground(case):
+    d = case.grid.np_zeros()
+    _L().og_height_above_ground(ctypes.byref(case.grid.c), _p(case.z), _p(d))
+    return d
+
+
+def local_dtau(case, cfl, use_nu=True, nu=None):
+    """local_dtau with nu (default: the case's diffusivity, or with the closure
+    the last iteration's nu, 0 before the first)."""
     dt = case.grid.np_zeros()
     q = case.q
+    if nu is None and use_nu:
+        nu = case.closure_nu if case.closure_nu is not None else case.nu
     _L().og_local_dtau(ctypes.byref(case.grid.c), _p(q["u"]), _p(q["v"]), _p(q["w"]), _p(case.z), _p(case.J),
-                       _p(case.nu) if use_nu else None, float(cfl), _p(dt))
+                       _p(nu) if use_nu else None, float(cfl), _p(dt))
     return dt
 
 
@@ -334,8 +400,13 @@ def simplec_iterate(case, bc, phys, opts, dtau):
     arr = (ctypes.c_void_p * 6)(*[r.ctypes.data for r in R])
     info = IterInfo()
     st, m, d = case.state(), case.mesh(), case.diffusivities()
-    rc = _L().og_simplec_iterate(ctypes.byref(case.grid.c), ctypes.byref(bc), ctypes.byref(phys), ctypes.byref(opts),
-                                 ctypes.byref(st), ctypes.byref(m), ctypes.byref(d), _p(dtau), arr, ctypes.byref(info))
+    if phys.closure and case.cf is None:
+        case.cf = [case.grid.np_zeros() for _ in CLOSURE_FIELDS]
+    rc = _L().og_simplec_iterate2(ctypes.byref(case.grid.c), ctypes.byref(bc), ctypes.byref(phys), ctypes.byref(opts),
+                                  ctypes.byref(st), ctypes.byref(m), ctypes.byref(d), _p(dtau), arr,
+                                  ctypes.byref(info), None if case.cf is None else _arrays(case.cf), None)
+    if phys.closure:
+        case.closure_nu = case.cf[0]
     return int(rc), info, R
 
 

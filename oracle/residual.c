@@ -86,6 +86,18 @@ static void grad_at(const og_grid* g, const double* q, int tq, int ts, int i, in
     out[2] = qz;
 }
 
+/* The stencil helpers for the closure and the wall model (turbulence.c). */
+double og_deriv(const og_grid* g, const double* q, int tq, int ts, int m, int i, int j, int k)
+{
+    return deriv(g, q, tq, ts, m, i, j, k);
+}
+
+/* grad_at<TQ, TS> with metric_at<TS> at (i, j, k). */
+void og_grad_at(const og_grid* g, const double* q, int tq, int ts, const double* z, int i, int j, int k, double out[3])
+{
+    grad_at(g, q, tq, ts, i, j, k, metric_at(g, z, ts, i, j, k), out);
+}
+
 /* ------------------------------------------------------------------ */
 /* mass flux                                                           */
 /* ------------------------------------------------------------------ */

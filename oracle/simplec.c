@@ -65,7 +65,32 @@ int og_poisson_solve(og_mg* mg, double* rhs, double* phi, double reltol, double 
 void og_face_divergence(const og_grid* g, const double* ax, const double* ay, const double* az, const double* J,
                         const double* fx, const double* fy, const double* fz, double* div);
 
+/* turbulence.c: the closure and the wall model */
+void og_closure_evaluate(const og_grid* g, const gb_bc* bc, const gb_physics* ph, const double* u, const double* v,
+                         const double* w, const double* th, const double* tk, const double* z, const double* z0map,
+                         double** out);
+int og_surface_state(const og_grid* g, const gb_bc* bc, const gb_physics* ph, const double* u, const double* v,
+                     const double* w, const double* z, const double* z0map, double** ss);
+void og_ground_gradients(const og_grid* g, const gb_bc* bc, const double* const* ss, const double* z0map, double** gg);
+double og_ground_gradient_at(const og_grid* g, const double* gg, int t, int i, int j);
+void og_set_ground_fluxes(const og_grid* g, const gb_bc* bc, const double* const* ss, double* Gu, double* Gv,
+                          double* Gt, double* Gk);
+void og_apply_wall_k(const og_grid* g, const gb_bc* bc, const double* const* ss, const double* tke, double* Rk);
+void og_apply_wall_to_implicit(const og_grid* g, const double* const* ss, int loc, const double* J, double* A);
+void og_apply_wall_k_to_implicit(const og_grid* g, const gb_bc* bc, const double* const* ss, double* A);
+
+enum { N_CF = 10, N_SS = 11 };
+enum { CF_NU = 0, CF_GTH, CF_GK, CF_NUT, CF_L, CF_RT, CF_PS, CF_PB, CF_EPS, CF_DSDK };
+
+/* The closure's fields (N_CF volumes) and the surface state (N_SS planes) an
+ * iteration evaluates once and its parts read (null: none). */
+typedef struct og_turb {
+    double* const* cf;
+    double* const* ss;
+} og_turb;
+
 static double* zalloc(const og_grid* g) { return (double*)calloc(VOL(g), sizeof(double)); }
+static double* palloc(const og_grid* g) { return (double*)calloc((size_t)(g->sy * (g->ny + 1 + 2 * g->ng)), sizeof(double)); }
 static int ext(const og_grid* g, int t, int d) { return ((d == 0) ? g->nx : (d == 1) ? g->ny : g->nz) + nodal(t, d); }
 static int is_per(const og_grid* g, int d) { return d == 0 ? g->periodic_x : d == 1 ? g->periodic_y : 0; }
 
@@ -157,6 +182,9 @@ static int rule_for(int f, int t, int d, int lo)
         if (normal_vel) { return R_VALUE; }
         return (f == F_THETA && d == 2 && !lo) ? R_GRADIENT : R_EVEN;
     case GB_FACE_NO_SLIP_WALL: return vel ? R_VALUE : R_EVEN;
+    case GB_FACE_SURFACE_LAYER:
+        if (normal_vel) { return R_VALUE; }
+        return (vel || f == F_THETA) ? R_GRADIENT : R_EVEN;
     default: return R_EVEN;
     }
 }
@@ -248,8 +276,9 @@ static void fill_face(const og_grid* g, int t, double* a, const double* z, int d
     }
 }
 
-/* fill_gradient_z<T> (BoundaryConditions.cpp:474-517) with a constant gradient. */
-static void fill_gradient_z(const og_grid* g, int t, double* a, const double* z, int lo, double G)
+/* fill_gradient_z<T> (BoundaryConditions.cpp:474-517): a constant gradient
+ * G, or per column from gg (the wall law's, og_ground_gradient_at). */
+static void fill_gradient_z(const og_grid* g, int t, double* a, const double* z, int lo, double Gc, const double* gg)
 {
     const int edge = lo ? 0 : g->nz - 1 + nodal(t, 2);
     const int c1 = lo ? edge + 1 : edge - 1;
@@ -258,6 +287,7 @@ static void fill_gradient_z(const og_grid* g, int t, double* a, const double* z,
     for (int e = 0; e < 2; ++e) { slab_range(g, t, 2, e, &rlo[e], &rhi[e]); }
     for (int j = rlo[1]; j <= rhi[1]; ++j) {
         for (int i = rlo[0]; i <= rhi[0]; ++i) {
+            const double G = gg ? og_ground_gradient_at(g, gg, t, i, j) : Gc;
             const double zc1 = point_z(g, z, t, i, j, c1), zg1 = point_z(g, z, t, i, j, g1), zg2 = point_z(g, z, t, i, j, g2);
             a[IX(g, i, j, g1)] = a[IX(g, i, j, c1)] + (zg1 - zc1) * G;
             a[IX(g, i, j, g2)] = a[IX(g, i, j, g1)] + (zg2 - zg1) * G;
@@ -265,7 +295,8 @@ static void fill_gradient_z(const og_grid* g, int t, double* a, const double* z,
     }
 }
 
-static void fill_field(const og_grid* g, int t, double* q, int f, int d, const gb_bc* bc, const double* z)
+static void fill_field(const og_grid* g, int t, double* q, int f, int d, const gb_bc* bc, const double* z,
+                       double* const* gg)
 {
     for (int lo = 1; lo >= 0; --lo) {
         const int face = d + (lo ? 0 : 3);
@@ -274,7 +305,11 @@ static void fill_field(const og_grid* g, int t, double* q, int f, int d, const g
         double value = 0;
         if (ft == GB_FACE_NO_SLIP_WALL && f <= F_W) { value = bc->wall_velocity[face][f]; }
         if (rule == R_GRADIENT) {
-            fill_gradient_z(g, t, q, z, lo, bc->zhi_theta_grad);
+            if (ft == GB_FACE_SURFACE_LAYER) {
+                fill_gradient_z(g, t, q, z, lo, 0.0, gg[f == F_U ? 0 : f == F_V ? 1 : 2]);
+            } else {
+                fill_gradient_z(g, t, q, z, lo, bc->zhi_theta_grad, NULL);
+            }
         } else {
             fill_face(g, t, q, z, d, lo, f, rule, value, bc);
         }
@@ -284,7 +319,7 @@ static void fill_field(const og_grid* g, int t, double* q, int f, int d, const g
 static int dirichlet_normal(const gb_bc* bc, int face)
 {
     const int t = bc->face[face];
-    return t == GB_FACE_INFLOW || t == GB_FACE_SLIP_WALL || t == GB_FACE_NO_SLIP_WALL;
+    return t == GB_FACE_INFLOW || t == GB_FACE_SLIP_WALL || t == GB_FACE_NO_SLIP_WALL || t == GB_FACE_SURFACE_LAYER;
 }
 
 /* fill_no_flux_w (BoundaryConditions.cpp:754-799): the ground and top faces
@@ -306,27 +341,60 @@ static void fill_no_flux_w(const og_grid* g, const gb_bc* bc, double* u, double*
     fill_periodic2(g, ZF, w);
 }
 
-/* BoundaryConditions::fill_ghosts (BoundaryConditions.cpp:597-663) without a
- * wall model: periodic images, then x, y and z faces for every field in
- * order (u, v, w, the no-flux w faces, p, theta, k), then the periodic images
- * of the rows the face fills rewrote (sync_ghost_copies). */
-void og_fill_ghosts(const og_grid* g, const gb_bc* bc, double* u, double* v, double* w, double* p, double* th,
-                    double* tk, const double* z)
+/* BoundaryConditions::fill_ghosts (BoundaryConditions.cpp:597-663):
+ * periodic images, then x, y and z faces for every field in order (u, v, w,
+ * the no-flux w faces, p, theta, k), then the periodic images of the rows the
+ * face fills rewrote (sync_ghost_copies). A surface_layer ground: the surface
+ * state from the laterally filled state (into ss_out, N_SS planes, when
+ * given) and the wall law's gradient for the ground fills of u, v, theta. */
+static const gb_physics* default_buoyancy(void)
+{
+    static gb_physics ph;
+    ph.gravity = 9.81;
+    ph.theta0 = 300.0;
+    return &ph;
+}
+
+void og_fill_ghosts2(const og_grid* g, const gb_bc* bc, const gb_physics* ph, const double* z0map, double* u, double* v,
+                     double* w, double* p, double* th, double* tk, const double* z, double** ss_out)
 {
     double* f[6] = {u, v, w, p, th, tk};
     const int t[6] = {XF, YF, ZF, CC, CC, CC};
-    for (int n = 0; n < 6; ++n) { fill_periodic2(g, t[n], f[n]); }
-    for (int d = 0; d < 3; ++d) {
-        if (is_per(g, d)) { continue; }
-        fill_field(g, XF, u, F_U, d, bc, z);
-        fill_field(g, YF, v, F_V, d, bc, z);
-        fill_field(g, ZF, w, F_W, d, bc, z);
-        if (d == 2) { fill_no_flux_w(g, bc, u, v, w, z); }
-        fill_field(g, CC, p, F_P, d, bc, z);
-        fill_field(g, CC, th, F_THETA, d, bc, z);
-        fill_field(g, CC, tk, F_TKE, d, bc, z);
+    const int wall = bc->face[2] == GB_FACE_SURFACE_LAYER;
+    double* ssl[N_SS] = {0};
+    double* gg[3] = {0};
+    double* const* ss = ss_out;
+    if (wall) {
+        if (!ss_out) {
+            for (int n = 0; n < N_SS; ++n) { ssl[n] = palloc(g); }
+            ss = ssl;
+        }
+        for (int n = 0; n < 3; ++n) { gg[n] = palloc(g); }
     }
     for (int n = 0; n < 6; ++n) { fill_periodic2(g, t[n], f[n]); }
+    for (int d = 0; d < 3; ++d) {
+        if (d == 2 && wall) {
+            og_surface_state(g, bc, ph ? ph : default_buoyancy(), u, v, w, z, z0map, (double**)ss);
+            og_ground_gradients(g, bc, (const double* const*)ss, z0map, gg);
+        }
+        if (is_per(g, d)) { continue; }
+        fill_field(g, XF, u, F_U, d, bc, z, gg);
+        fill_field(g, YF, v, F_V, d, bc, z, gg);
+        fill_field(g, ZF, w, F_W, d, bc, z, gg);
+        if (d == 2) { fill_no_flux_w(g, bc, u, v, w, z); }
+        fill_field(g, CC, p, F_P, d, bc, z, gg);
+        fill_field(g, CC, th, F_THETA, d, bc, z, gg);
+        fill_field(g, CC, tk, F_TKE, d, bc, z, gg);
+    }
+    for (int n = 0; n < 6; ++n) { fill_periodic2(g, t[n], f[n]); }
+    for (int n = 0; n < N_SS; ++n) { free(ssl[n]); }
+    for (int n = 0; n < 3; ++n) { free(gg[n]); }
+}
+
+void og_fill_ghosts(const og_grid* g, const gb_bc* bc, double* u, double* v, double* w, double* p, double* th,
+                    double* tk, const double* z)
+{
+    og_fill_ghosts2(g, bc, NULL, NULL, u, v, w, p, th, tk, z, NULL);
 }
 
 /* apply_rows (BoundaryConditions.cpp:801-852): R = q - V on the Dirichlet
@@ -483,12 +551,22 @@ typedef struct og_fields {
     const double* z;
 } og_fields;
 
-/* Residual.cpp:159-256 residual() with the given diffusivities, no closure and
- * no wall model. R[6]: u, v, w, p, theta, k. */
-void og_residual(const og_grid* g, const gb_bc* bc, const gb_physics* ph, const gb_state* q, const gb_mesh_fields* m,
-                 const gb_diffusivities* df, double** R)
+/* Residual.cpp:159-256 residual(): the diffusivities given (ph->closure = 0)
+ * or the closure's at q (its fields into t->cf), the wall model's ground
+ * fluxes and wall-k rows with a surface_layer ground (the surface state into
+ * t->ss). R[6]: u, v, w, p, theta, k. */
+static void residual_t(const og_grid* g, const gb_bc* bc, const gb_physics* ph, const gb_state* q,
+                       const gb_mesh_fields* m, const gb_diffusivities* df, double** R, const og_turb* t)
 {
     const int64_t vol = VOL(g);
+    const int wall = bc->face[2] == GB_FACE_SURFACE_LAYER;
+    const double *nu = df ? df->nu : NULL, *gamma_theta = df ? df->gamma_theta : NULL, *gamma_tke = df ? df->gamma_tke : NULL;
+    if (ph->closure) {
+        og_closure_evaluate(g, bc, ph, q->u, q->v, q->w, q->theta, q->tke, q->z_nd, m->z0, (double**)t->cf);
+        nu = t->cf[CF_NU];
+        gamma_theta = t->cf[CF_GTH];
+        gamma_tke = t->cf[CF_GK];
+    }
     double* F[3];
     for (int d = 0; d < 3; ++d) { F[d] = zalloc(g); }
     og_transport_fluxes(g, q->u, q->v, q->w, q->z_nd, m->ax, m->ay, F[0], F[1], F[2]);
@@ -498,15 +576,19 @@ void og_residual(const og_grid* g, const gb_bc* bc, const gb_physics* ph, const 
     for (int c = 0; c < 3; ++c) {
         og_convection(g, 1 << c, vel[c], F[0], F[1], F[2], m->detJ, ph->limiter, ph->smooth_eps_velocity, 0, R[c]);
         for (int d = 0; d < 3; ++d) { Gm[c][d] = zalloc(g); }
-        og_momentum_diffusive_fluxes(g, c, q->u, q->v, q->w, df->nu, q->z_nd, ph->log_mean, Gm[c][0], Gm[c][1], Gm[c][2]);
+        og_momentum_diffusive_fluxes(g, c, q->u, q->v, q->w, nu, q->z_nd, ph->log_mean, Gm[c][0], Gm[c][1], Gm[c][2]);
     }
     double *Gt[3], *Gk[3];
     for (int d = 0; d < 3; ++d) {
         Gt[d] = zalloc(g);
         Gk[d] = zalloc(g);
     }
-    og_scalar_diffusive_fluxes(g, q->theta, df->gamma_theta, q->z_nd, ph->log_mean, Gt[0], Gt[1], Gt[2]);
-    og_scalar_diffusive_fluxes(g, q->tke, df->gamma_tke, q->z_nd, ph->log_mean, Gk[0], Gk[1], Gk[2]);
+    og_scalar_diffusive_fluxes(g, q->theta, gamma_theta, q->z_nd, ph->log_mean, Gt[0], Gt[1], Gt[2]);
+    og_scalar_diffusive_fluxes(g, q->tke, gamma_tke, q->z_nd, ph->log_mean, Gk[0], Gk[1], Gk[2]);
+    if (wall) {
+        og_surface_state(g, bc, ph, q->u, q->v, q->w, q->z_nd, m->z0, (double**)t->ss);
+        og_set_ground_fluxes(g, bc, (const double* const*)t->ss, Gm[0][2], Gm[1][2], Gt[2], Gk[2]);
+    }
     for (int c = 0; c < 3; ++c) {
         og_flux_divergence(g, 1 << c, Gm[c][0], Gm[c][1], Gm[c][2], m->detJ, tmp);
         for (int64_t n = 0; n < vol; ++n) { R[c][n] -= tmp[n]; }
@@ -579,6 +661,25 @@ void og_residual(const og_grid* g, const gb_bc* bc, const gb_physics* ph, const 
     og_convection(g, CC, q->tke, F[0], F[1], F[2], m->detJ, 2 /* upwind */, 1e-5, 1, R[5]);
     og_flux_divergence(g, CC, Gk[0], Gk[1], Gk[2], m->detJ, tmp);
     for (int64_t n = 0; n < vol; ++n) { R[5][n] -= tmp[n]; }
+    if (ph->closure) {
+        /* R_k -= S_k = P_s + P_b - eps on the valid cells */
+        for (int k = 0; k < g->nz; ++k) {
+            for (int j = 0; j < g->ny; ++j) {
+                for (int i = 0; i < g->nx; ++i) { R[5][IX(g, i, j, k)] -= t->cf[CF_PS][IX(g, i, j, k)]; }
+            }
+        }
+        for (int k = 0; k < g->nz; ++k) {
+            for (int j = 0; j < g->ny; ++j) {
+                for (int i = 0; i < g->nx; ++i) { R[5][IX(g, i, j, k)] -= t->cf[CF_PB][IX(g, i, j, k)]; }
+            }
+        }
+        for (int k = 0; k < g->nz; ++k) {
+            for (int j = 0; j < g->ny; ++j) {
+                for (int i = 0; i < g->nx; ++i) { R[5][IX(g, i, j, k)] += t->cf[CF_EPS][IX(g, i, j, k)]; }
+            }
+        }
+    }
+    if (wall) { og_apply_wall_k(g, bc, (const double* const*)t->ss, q->tke, R[5]); }
     apply_rows(g, bc, q->u, q->v, q->w, q->z_nd, R[0], R[1], R[2]);
     og_override_sync(g, XF, R[0]);
     og_override_sync(g, YF, R[1]);
@@ -593,16 +694,70 @@ void og_residual(const og_grid* g, const gb_bc* bc, const gb_physics* ph, const 
     free(tmp);
 }
 
-/* Residual.cpp:272-304 implicit_rows without a closure and a wall model. */
+/* The residual with the closure's fields (N_CF volumes) and the surface
+ * state (N_SS planes) into cf_out, ss_out when given. */
+void og_residual2(const og_grid* g, const gb_bc* bc, const gb_physics* ph, const gb_state* q, const gb_mesh_fields* m,
+                  const gb_diffusivities* df, double** R, double** cf_out, double** ss_out)
+{
+    double* cfl[N_CF] = {0};
+    double* ssl[N_SS] = {0};
+    og_turb t = {cf_out, ss_out};
+    if (ph->closure && !cf_out) {
+        for (int n = 0; n < N_CF; ++n) { cfl[n] = zalloc(g); }
+        t.cf = cfl;
+    }
+    if (bc->face[2] == GB_FACE_SURFACE_LAYER && !ss_out) {
+        for (int n = 0; n < N_SS; ++n) { ssl[n] = palloc(g); }
+        t.ss = ssl;
+    }
+    residual_t(g, bc, ph, q, m, df, R, &t);
+    for (int n = 0; n < N_CF; ++n) { free(cfl[n]); }
+    for (int n = 0; n < N_SS; ++n) { free(ssl[n]); }
+}
+
+void og_residual(const og_grid* g, const gb_bc* bc, const gb_physics* ph, const gb_state* q, const gb_mesh_fields* m,
+                 const gb_diffusivities* df, double** R)
+{
+    og_residual2(g, bc, ph, q, m, df, R, NULL, NULL);
+}
+
+/* Residual.cpp:272-304 implicit_rows: the closure's diffusivity and the
+ * Patankar diagonal of k (tc->cf), the first cells' wall rows (tc->ss) for
+ * every equation but w, then the boundary folds. */
+static void implicit_rows_t(const og_grid* g, const gb_bc* bc, const gb_physics* ph, int eq, const double* F0,
+                            const double* F1, const double* F2, const double* z, const double* J,
+                            const gb_diffusivities* df, const og_turb* tc, double* A)
+{
+    const int closure = ph->closure && tc && tc->cf;
+    const double* gm;
+    if (closure) {
+        gm = (eq <= F_W) ? tc->cf[CF_NU] : (eq == F_THETA) ? tc->cf[CF_GTH] : tc->cf[CF_GK];
+    } else {
+        gm = (eq <= F_W) ? df->nu : (eq == F_THETA) ? df->gamma_theta : df->gamma_tke;
+    }
+    const int C = (eq <= F_W) ? eq : -1;
+    const int t = (eq <= F_W) ? (1 << eq) : CC;
+    og_implicit_coefficients(g, C, F0, F1, F2, gm, z, J, ph->log_mean, A);
+    if (closure && eq == F_TKE) {
+        const int64_t cs = VOL(g);
+        for (int k = 0; k < g->nz; ++k) {
+            for (int j = 0; j < g->ny; ++j) {
+                for (int i = 0; i < g->nx; ++i) { A[COEF_P * cs + IX(g, i, j, k)] += tc->cf[CF_DSDK][IX(g, i, j, k)]; }
+            }
+        }
+    }
+    if (bc->face[2] == GB_FACE_SURFACE_LAYER && eq != F_W && tc && tc->ss) {
+        og_apply_wall_to_implicit(g, (const double* const*)tc->ss, t, J, A);
+        if (eq == F_TKE) { og_apply_wall_k_to_implicit(g, bc, (const double* const*)tc->ss, A); }
+    }
+    apply_to_implicit(g, bc, eq, t, A);
+}
+
 void og_implicit_rows(const og_grid* g, const gb_bc* bc, const gb_physics* ph, int eq, const double* F0,
                       const double* F1, const double* F2, const double* z, const double* J, const gb_diffusivities* df,
                       double* A)
 {
-    const double* gm = (eq <= F_W) ? df->nu : (eq == F_THETA) ? df->gamma_theta : df->gamma_tke;
-    const int C = (eq <= F_W) ? eq : -1;
-    const int t = (eq <= F_W) ? (1 << eq) : CC;
-    og_implicit_coefficients(g, C, F0, F1, F2, gm, z, J, ph->log_mean, A);
-    apply_to_implicit(g, bc, eq, t, A);
+    implicit_rows_t(g, bc, ph, eq, F0, F1, F2, z, J, df, NULL, A);
 }
 
 /* ------------------------------------------------------------------ */
@@ -623,8 +778,8 @@ static double line_solve(const og_grid* g, const gb_simplec_opts* so, int loc, c
 
 void og_momentum_predictor(const og_grid* g, const gb_bc* bc, const gb_physics* ph, const gb_simplec_opts* so,
                            gb_state* q, double** R, const double* F0, const double* F1, const double* F2,
-                           double** dtau_f, const gb_mesh_fields* m, const gb_diffusivities* df, double** ap,
-                           double** dd, double* info)
+                           double** dtau_f, const gb_mesh_fields* m, const gb_diffusivities* df, const og_turb* tc,
+                           double** ap, double** dd, double* info)
 {
     const int64_t vol = VOL(g), cs = vol;
     double* comps[3] = {q->u, q->v, q->w};
@@ -636,7 +791,7 @@ void og_momentum_predictor(const og_grid* g, const gb_bc* bc, const gb_physics* 
     const double fs = coriolis_parameter(ph);
     for (int c = 0; c < 3; ++c) {
         const int t = 1 << c;
-        og_implicit_rows(g, bc, ph, c, F0, F1, F2, q->z_nd, m->detJ, df, A);
+        implicit_rows_t(g, bc, ph, c, F0, F1, F2, q->z_nd, m->detJ, df, tc, A);
         dirichlet_rows(g, bc, c, t, mask);
         const int ni = ext(g, t, 0), nj = ext(g, t, 1), nk = ext(g, t, 2);
         for (int k = 0; k < nk; ++k) {
@@ -740,7 +895,7 @@ void og_momentum_predictor(const og_grid* g, const gb_bc* bc, const gb_physics* 
         if (c == 2 && ph->gravity > 0) {
             const double gt = ph->gravity / ph->theta0;
             double* At = (double*)calloc(N_COEFS * vol, sizeof(double));
-            og_implicit_rows(g, bc, ph, F_THETA, F0, F1, F2, q->z_nd, m->detJ, df, At);
+            implicit_rows_t(g, bc, ph, F_THETA, F0, F1, F2, q->z_nd, m->detJ, df, tc, At);
             const double* z = q->z_nd;
             for (int k = 0; k < nk; ++k) {
                 for (int j = 0; j < nj; ++j) {
@@ -930,12 +1085,12 @@ int og_pressure_correction(const og_grid* g, const gb_bc* bc, const gb_simplec_o
 /* Simplec.cpp:222-281 scalar_sweep. Returns max |dq|; *clipped the k floor count. */
 double og_scalar_sweep(const og_grid* g, const gb_bc* bc, const gb_physics* ph, const gb_simplec_opts* so, int eq,
                        double* field, const double* Req, const double* F0, const double* F1, const double* F2,
-                       const double* z, const double* J, const gb_diffusivities* df, const double* dtau, double floor,
-                       int clip, double* last, int64_t* clipped)
+                       const double* z, const double* J, const gb_diffusivities* df, const og_turb* tc,
+                       const double* dtau, double floor, int clip, double* last, int64_t* clipped)
 {
     const int64_t vol = VOL(g), cs = vol;
     double* A = (double*)calloc(N_COEFS * vol, sizeof(double));
-    og_implicit_rows(g, bc, ph, eq, F0, F1, F2, z, J, df, A);
+    implicit_rows_t(g, bc, ph, eq, F0, F1, F2, z, J, df, tc, A);
     double* rhs = zalloc(g);
     double* ap = zalloc(g);
     double* delta = zalloc(g);
@@ -1006,14 +1161,30 @@ void og_stage_norms(const og_grid* g, const gb_physics* ph, double** R, const gb
 /* SimplecStage::iterate (Simplec.cpp:452-506) without a closure, a wall model
  * and the hybrid blend. R[6] receives the residual at the start. Returns 0 or
  * the pressure correction's status. */
-int og_simplec_iterate(const og_grid* g, const gb_bc* bc, const gb_physics* ph, const gb_simplec_opts* so, gb_state* q,
-                       const gb_mesh_fields* m, const gb_diffusivities* df, const double* dtau, double** R,
-                       gb_iter_info* out)
+/* SimplecStage::iterate (Simplec.cpp:452-506). With the closure its fields
+ * at q (N_CF volumes, nu first: the next step's local dtau reads it) go to
+ * cf_out, the surface state of step 1 to ss_out (N_SS planes), when given. */
+int og_simplec_iterate2(const og_grid* g, const gb_bc* bc, const gb_physics* ph, const gb_simplec_opts* so, gb_state* q,
+                        const gb_mesh_fields* m, const gb_diffusivities* df, const double* dtau, double** R,
+                        gb_iter_info* out, double** cf_out, double** ss_out)
 {
     const int64_t vol = VOL(g);
     memset(out, 0, sizeof(*out));
-    og_fill_ghosts(g, bc, q->u, q->v, q->w, q->p, q->theta, q->tke, q->z_nd);
-    og_residual(g, bc, ph, q, m, df, R);
+    double* cfl[N_CF] = {0};
+    double* ssl[N_SS] = {0};
+    og_turb tcv = {cf_out, ss_out};
+    if (ph->closure && !cf_out) {
+        for (int n = 0; n < N_CF; ++n) { cfl[n] = zalloc(g); }
+        tcv.cf = cfl;
+    }
+    if (bc->face[2] == GB_FACE_SURFACE_LAYER && !ss_out) {
+        for (int n = 0; n < N_SS; ++n) { ssl[n] = palloc(g); }
+        tcv.ss = ssl;
+    }
+    const og_turb* tc = &tcv;
+    /* 1. ghosts and the wall state at q; 2. the residual (the closure at q) */
+    og_fill_ghosts2(g, bc, ph, m->z0, q->u, q->v, q->w, q->p, q->theta, q->tke, q->z_nd, (double**)tc->ss);
+    residual_t(g, bc, ph, q, m, df, R, tc);
     double mon[2];
     og_stage_norms(g, ph, R, q, out->residual_norms, mon);
     out->max_speed = mon[0];
@@ -1027,14 +1198,14 @@ int og_simplec_iterate(const og_grid* g, const gb_bc* bc, const gb_physics* ph, 
     double* ap[3] = {zalloc(g), zalloc(g), zalloc(g)};
     double* dd[3] = {zalloc(g), zalloc(g), zalloc(g)};
     double pinfo[8];
-    og_momentum_predictor(g, bc, ph, so, q, R, F[0], F[1], F[2], dtf, m, df, ap, dd, pinfo);
+    og_momentum_predictor(g, bc, ph, so, q, R, F[0], F[1], F[2], dtf, m, df, tc, ap, dd, pinfo);
     out->max_du = pinfo[0];
     out->max_dv = pinfo[1];
     out->max_dw = pinfo[2];
     out->last_sweep_du = pinfo[3];
     out->last_sweep_dv = pinfo[4];
     out->last_sweep_dw = pinfo[5];
-    og_fill_ghosts(g, bc, q->u, q->v, q->w, q->p, q->theta, q->tke, q->z_nd);
+    og_fill_ghosts2(g, bc, ph, m->z0, q->u, q->v, q->w, q->p, q->theta, q->tke, q->z_nd, NULL);
     double cinfo[8];
     const int st = og_pressure_correction(g, bc, so, q, dd, m, cinfo);
     out->divergence_before = cinfo[0];
@@ -1046,7 +1217,7 @@ int og_simplec_iterate(const og_grid* g, const gb_bc* bc, const gb_physics* ph, 
     double* conv0 = zalloc(g);
     double* conv1 = zalloc(g);
     og_convection(g, CC, q->theta, F[0], F[1], F[2], m->detJ, ph->limiter, ph->smooth_eps_theta, 0, conv0);
-    og_fill_ghosts(g, bc, q->u, q->v, q->w, q->p, q->theta, q->tke, q->z_nd);
+    og_fill_ghosts2(g, bc, ph, m->z0, q->u, q->v, q->w, q->p, q->theta, q->tke, q->z_nd, NULL);
     og_transport_fluxes(g, q->u, q->v, q->w, q->z_nd, m->ax, m->ay, F[0], F[1], F[2]);
     og_convection(g, CC, q->theta, F[0], F[1], F[2], m->detJ, ph->limiter, ph->smooth_eps_theta, 0, conv1);
     for (int k = 0; k < g->nz; ++k) {
@@ -1060,9 +1231,9 @@ int og_simplec_iterate(const og_grid* g, const gb_bc* bc, const gb_physics* ph, 
     double last;
     int64_t clipped = 0;
     out->max_dtheta = og_scalar_sweep(g, bc, ph, so, F_THETA, q->theta, R[4], F[0], F[1], F[2], q->z_nd, m->detJ, df,
-                                      dtau, 0, 0, &last, &clipped);
-    out->max_dtke = og_scalar_sweep(g, bc, ph, so, F_TKE, q->tke, R[5], F[0], F[1], F[2], q->z_nd, m->detJ, df, dtau,
-                                    so->tke_floor, 1, &last, &clipped);
+                                      tc, dtau, 0, 0, &last, &clipped);
+    out->max_dtke = og_scalar_sweep(g, bc, ph, so, F_TKE, q->tke, R[5], F[0], F[1], F[2], q->z_nd, m->detJ, df, tc,
+                                    dtau, so->tke_floor, 1, &last, &clipped);
     out->tke_clipped = clipped;
     for (int c = 0; c < 3; ++c) {
         free(F[c]);
@@ -1073,7 +1244,16 @@ int og_simplec_iterate(const og_grid* g, const gb_bc* bc, const gb_physics* ph, 
     free(dcc);
     free(conv0);
     free(conv1);
+    for (int n = 0; n < N_CF; ++n) { free(cfl[n]); }
+    for (int n = 0; n < N_SS; ++n) { free(ssl[n]); }
     return st;
+}
+
+int og_simplec_iterate(const og_grid* g, const gb_bc* bc, const gb_physics* ph, const gb_simplec_opts* so, gb_state* q,
+                       const gb_mesh_fields* m, const gb_diffusivities* df, const double* dtau, double** R,
+                       gb_iter_info* out)
+{
+    return og_simplec_iterate2(g, bc, ph, so, q, m, df, dtau, R, out, NULL, NULL);
 }
 
 /* ------------------------------------------------------------------ */

@@ -166,6 +166,76 @@ def init_askervein_case():
     return case, bc, io, gold
 
 
+def closure_column_case(ustar=0.35, z0=0.1, direction=15.0):
+    """The reference's Closure_Column regression (Tests/Discretization/
+    Closure_Column/inputs_closure_column, Tests/Supporting_Files/Tools/
+    closure_column.cpp): ERF's Neutral_ABL_Flat mesh (8 x 8 x 64 cells over
+    2560 m x 2560 m x 1000 m, flat, periodic sides), a surface_layer ground
+    (z0 0.1 m), a slip top, theta 300 K, the wall law's equilibrium state
+    u = (u*/kappa) ln((h + z0)/z0) along the direction at each point's height
+    above the ground, k = u*^2/Cmu0^2, w = p' = 0; the k-L closure with
+    turb.max_geom_lscale = 1e12 and the logarithmic face mean.
+    Returns (case, bc, physics)."""
+    import math
+    import oracle
+    from ablsteadyrans_b200.abi import BC, FACE_SLIP_WALL, FACE_SURFACE_LAYER, Physics
+    nx, ny, nz = 8, 8, 64
+    g = Grid(nx, ny, nz, 320.0, 320.0, 1000.0 / nz, True, True)
+    z = oracle.btf_heights(g, np.arange(nz + 1) * (1000.0 / nz), np.zeros((ny + 3, nx + 3)))
+    J, ax, ay, az, _ = oracle.metrics(g, z)
+    case = oracle.Case(g, z, J, ax, ay, az, np.zeros_like(J), np.zeros_like(J), np.zeros_like(J))
+    kappa, cmu0 = 0.41, 0.5562
+    a = math.radians(direction)
+    G = g.ng
+
+    def height(t, i, j, k):
+        nxp, nyp, nzp = (1 if t & 1 else 2), (1 if t & 2 else 2), (1 if t & 4 else 2)
+        zp = zg = 0.0
+        for aa in range(nxp):
+            for b in range(nyp):
+                zg += z[G, G + j + b, G + i + aa]
+                for c in range(nzp):
+                    zp += z[G + k + c, G + j + b, G + i + aa]
+        return zp / (nxp * nyp * nzp) - zg / (nxp * nyp)
+
+    def speed(h):
+        return ustar / kappa * math.log((max(h, 0.0) + z0) / z0)
+
+    q = case.q
+    for k in range(nz):
+        for j in range(ny):
+            for i in range(nx + 1):
+                q["u"][G + k, G + j, G + i] = speed(height(1, i, j, k)) * math.cos(a)
+        for j in range(ny + 1):
+            for i in range(nx):
+                q["v"][G + k, G + j, G + i] = speed(height(2, i, j, k)) * math.sin(a)
+    q["theta"][G:G + nz, G:G + ny, G:G + nx] = 300.0
+    q["tke"][...] = ustar * ustar / (cmu0 * cmu0)
+    bc = BC.make((0, 0, FACE_SURFACE_LAYER, 0, 0, FACE_SLIP_WALL), theta_ref=((0.0,), (300.0,)), ustar=ustar, z0=z0,
+                 surface={"z0": z0})
+    ph = Physics.make(1000.0, closure=1, turb_max_geom_lscale=1e12, log_mean=1)
+    return case, bc, ph
+
+
+def closure_column_outputs(g, q, R, cf, ss):
+    """closure_column.cpp's plotfile fields [k, j, i]: cell means of the face
+    values, the cell fields, and u* on the ground cells."""
+    G, nx, ny, nz = g.ng, g.nx, g.ny, g.nz
+    c = (slice(G, G + nz), slice(G, G + ny), slice(G, G + nx))
+    out = {
+        "u": 0.5 * (q["u"][c] + q["u"][G:G + nz, G:G + ny, G + 1:G + nx + 1]),
+        "tke": q["tke"][c], "nut": cf["nut"][c], "length": cf["length"][c],
+        "R_u": 0.5 * (R[0][c] + R[0][G:G + nz, G:G + ny, G + 1:G + nx + 1]),
+        "R_v": 0.5 * (R[1][c] + R[1][G:G + nz, G + 1:G + ny + 1, G:G + nx]),
+        "R_w": 0.5 * (R[2][c] + R[2][G + 1:G + nz + 1, G:G + ny, G:G + nx]),
+        "R_theta": R[4][c], "R_tke": R[5][c], "Ps": cf["Ps"][c], "eps": cf["eps"][c],
+    }
+    ust = np.zeros((nz, ny, nx))
+    ust[0] = np.asarray(ss["ustar"]).reshape(-1, int(g.c.sy))[G:G + ny, G:G + nx]
+    out["ustar"] = ust
+    return out
+
+
 def gold_cell_fields(g, q):
     """The reference plotfile's cell values (Source/StateIO.cpp:59-74): u, v, w
     the means of the cell's two faces, the cell fields as they are; [k, j, i]."""

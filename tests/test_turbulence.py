@@ -1,0 +1,198 @@
+"""The k-L closure and the surface layer (the wall model): the oracle's
+restatement (oracle/turbulence.c) pinned to the reference's Closure_Column
+gold (Tests/Discretization/Closure_Column: "The plotfile matches
+Gold/closure_column_plt00000 at relative 1e-10") and to that test's closed
+forms (check_closure.py), the stratified branches of the closure against the
+AL01 relations, and the heat-flux MOST solve; GPU tests compare the CUDA
+closure, wall model, residual and SIMPLEC iterations with the oracle."""
+import math
+
+import numpy as np
+import pytest
+
+import oracle
+from helpers import GOLDEN, closure_column_case, closure_column_outputs
+
+KAPPA, CMU0 = 0.41, 0.5562
+
+
+def _gold():
+    d = np.load(f"{GOLDEN}/closure_column.npz")
+    return {k: d[k] for k in d.files}
+
+
+def test_oracle_closure_column_matches_reference_gold():
+    case, bc, ph = closure_column_case()
+    oracle.fill_ghosts(case, bc, ph)
+    R, cf, ss = oracle.residual(case, bc, ph, fields=True)
+    got = closure_column_outputs(case.grid, case.q, R, cf, ss)
+    gold = _gold()
+    for f, ref in gold.items():
+        scale = np.abs(ref).max()
+        err = np.abs(got[f] - ref).max()
+        if scale == 0:
+            assert err <= 1e-13, f
+        else:
+            assert err <= 1e-10 * scale, (f, err / scale)
+
+
+def test_oracle_closure_column_closed_forms():
+    """check_closure.py: nu_t = kappa u* (z + z0) and L = kappa (z + z0) (1e-9),
+    u* recovered (1e-10), eps = u*^3/(kappa (z + z0)) (1e-9), R_u, R_v zero
+    below the top cell (1e-10 of u*^2/dz) and u*^2/dz (cos, sin) there (1e-8), R_w =
+    R_theta = 0, the first cell's R_k 0 (the wall-k row at k = k_w)."""
+    us, z0, deg = 0.35, 0.1, 15.0
+    case, bc, ph = closure_column_case(us, z0, deg)
+    oracle.fill_ghosts(case, bc, ph)
+    R, cf, ss = oracle.residual(case, bc, ph, fields=True)
+    g = case.grid
+    out = closure_column_outputs(g, case.q, R, cf, ss)
+    dz = g.dzeta
+    zc = (np.arange(g.nz) + 0.5) * dz
+    nut_ref = KAPPA * us * (zc + z0)
+    assert np.abs(out["nut"] - nut_ref[:, None, None]).max() <= 1e-9 * nut_ref.max()
+    L_ref = KAPPA * (zc + z0)
+    assert np.abs(out["length"] - L_ref[:, None, None]).max() <= 1e-9 * L_ref.max()
+    assert np.abs(out["ustar"][0] - us).max() <= 1e-10 * us
+    eps_ref = us ** 3 / (KAPPA * (zc + z0))
+    assert np.abs(out["eps"] - eps_ref[:, None, None]).max() <= 1e-9 * eps_ref.max()
+    s = us * us / dz
+    a = math.radians(deg)
+    assert np.abs(out["R_u"][:-1]).max() <= 1e-10 * s and np.abs(out["R_v"][:-1]).max() <= 1e-10 * s
+    assert np.abs(out["R_u"][-1] - s * math.cos(a)).max() <= 1e-8 * s
+    assert np.abs(out["R_v"][-1] - s * math.sin(a)).max() <= 1e-8 * s
+    assert np.abs(out["R_w"]).max() <= 1e-12 and np.abs(out["R_theta"]).max() <= 1e-12
+    assert np.abs(out["R_tke"][0]).max() <= 1e-15
+
+
+def _al01(k, N2, l_g, Cb=0.35, Rt_crit=-1.0, Rt_min=-3.0):
+    """AL01 (Axell and Liungman 2001) relations as ERF_RANSClosure.H states them."""
+    c3 = CMU0 ** 3
+
+    def smooth(rt):
+        if rt >= Rt_crit:
+            return rt
+        x, aa = rt - Rt_crit, Rt_min - Rt_crit
+        return Rt_crit + aa * x / (x + aa)
+
+    if abs(N2) <= np.finfo(float).eps:
+        L = l_g
+    elif N2 > 0:
+        L = math.sqrt(1.0 / (1.0 / (l_g * l_g) + N2 / (Cb * Cb) / k))
+    else:
+        L = l_g * math.sqrt(1.0 - c3 * c3 / (Cb * Cb) * smooth(l_g * l_g * N2 / (k * c3 * c3)))
+    rt = smooth(L * L * N2 / (k * c3 * c3))
+    cmu = (CMU0 + 0.108 * rt) / (1 + 0.308 * rt + 0.00837 * rt * rt)
+    cmup = CMU0 / (1 + 0.277 * rt)
+    nut = cmu * math.sqrt(k) * L
+    return L, rt, nut, cmup / cmu * nut, c3 * k ** 1.5 / L
+
+
+@pytest.mark.parametrize("dtdz", [0.02, -0.02, -2.0])
+def test_oracle_closure_stratified_branches(dtdz):
+    """A stable, an unstable and a strongly unstable (Rt smoothed) column:
+    the length, Rt, nu_t, gamma_theta and eps of every cell against the AL01
+    relations, with N^2 = (g/theta_0) dtheta/dz and the capped l_g."""
+    case, bc, ph = closure_column_case()
+    g = case.grid
+    G = g.ng
+    zc = (np.arange(-G, g.nz + 1 + G) + 0.5) * g.dzeta
+    case.q["theta"][...] = (300.0 + dtdz * zc)[:, None, None]
+    ph.turb_max_geom_lscale = 30.0
+    case.q["tke"][...] = 0.05
+    oracle.fill_ghosts(case, bc, ph)
+    cf = oracle.closure_fields(case, bc, ph)
+    N2 = 9.81 / 300.0 * dtdz
+    kk = 0.05
+    smoothed = 0
+    for k in range(1, g.nz - 1):   # the ground gradient and the top differ from dtheta/dz
+        d = (k + 0.5) * g.dzeta
+        lraw = KAPPA * (d + 0.1)
+        l_g = 30.0 * lraw / (30.0 + lraw)
+        L, rt, nut, nutp, eps = _al01(kk, N2, l_g)
+        smoothed += rt < -1.0
+        o = (G + k, G + 3, G + 4)
+        assert cf["length"][o] == pytest.approx(L, rel=1e-12)
+        assert cf["Rt"][o] == pytest.approx(rt, rel=1e-11, abs=1e-14)
+        assert cf["nut"][o] == pytest.approx(nut, rel=1e-11)
+        assert cf["gamma_theta"][o] == pytest.approx(nutp, rel=1e-11)
+        assert cf["eps"][o] == pytest.approx(eps, rel=1e-12)
+    if dtdz == -2.0:
+        assert smoothed > 0
+
+
+@pytest.mark.parametrize("q", [0.1, -0.02])
+def test_oracle_surface_layer_heat_flux(q):
+    """bc.surface_stability = heat_flux: u* solves the MOST relation
+    u* = kappa U / max(ln((d + z0)/z0) - psi_m(d/L), m), 1/L = -kappa g q /
+    (u*^3 theta_0), to round-off; an upward flux raises u* above the neutral
+    value and k_w to (u*^3 + kappa g q d0/theta_0)^(2/3)/Cmu0^2, a downward one
+    lowers u*."""
+    from ablsteadyrans_b200.abi import SURFACE_HEAT_FLUX
+    case, bc, ph = closure_column_case()
+    oracle.fill_ghosts(case, bc, ph)
+    neutral, bad0 = oracle.surface_state(case, bc, ph)
+    bc.surface_stability, bc.surface_heat_flux = SURFACE_HEAT_FLUX, q
+    ss, bad = oracle.surface_state(case, bc, ph)
+    assert bad0 == 0 and bad == 0
+    g = case.grid
+    p = (g.ng + 2) * int(g.c.sy) + g.ng + 3
+    us, U, d0, invL = ss["ustar"][p], ss["speed"][p], ss["d0"][p], ss["inv_L"][p]
+    z0 = 0.1
+    zeta = max(min(d0 * invL, 100.0), -100.0)
+    if zeta > 0:
+        psi = -5.0 * zeta
+    else:
+        x = (1 - 16 * zeta) ** 0.25
+        psi = 2 * math.log(0.5 * (1 + x)) + math.log(0.5 * (1 + x * x)) - 2 * math.atan(x) + math.pi / 2
+    lz = math.log((d0 + z0) / z0)
+    assert us == pytest.approx(KAPPA * U / max(lz - psi, min(lz, 1.0)), rel=1e-12)
+    assert invL == pytest.approx(-KAPPA * 9.81 * q / (300.0 * us ** 3), rel=1e-12)
+    if q > 0:
+        assert us > neutral["ustar"][p]
+        kw = (us ** 3 + KAPPA * 9.81 / 300.0 * q * d0) ** (2.0 / 3.0) / CMU0 ** 2
+        assert ss["kwall"][p] == pytest.approx(kw, rel=1e-12)
+    else:
+        assert us < neutral["ustar"][p]
+        assert ss["kwall"][p] == pytest.approx(us * us / CMU0 ** 2, rel=1e-12)
+
+
+def test_oracle_stage_with_closure_and_wall_model():
+    """SIMPLEC iterations with the closure and the surface layer over a hill:
+    every field stays finite, u* stays positive, and the momentum residual
+    falls over 30 iterations from the log-law start."""
+    from ablsteadyrans_b200.abi import FACE_SURFACE_LAYER, SimplecOptions
+    case, bc, ph = _hill_case()
+    so = SimplecOptions.make()
+    norms = []
+    for _ in range(30):
+        dt = oracle.local_dtau(case, 2.0)
+        rc, info, R = oracle.simplec_iterate(case, bc, ph, so, dt)
+        assert rc == 0
+        norms.append(info.residual_norms[0])
+    assert bc.face[2] == FACE_SURFACE_LAYER
+    for f in case.FIELDS:
+        assert np.all(np.isfinite(case.q[f])), f
+    assert norms[-1] < 0.5 * norms[0], norms
+    ss, bad = oracle.surface_state(case, bc, ph)
+    assert bad == 0
+
+
+def _hill_case(seed=1):
+    """A 16 x 12 x 16 Gaussian hill (periodic in y) with inflow and outflow in
+    x, the surface layer on the ground (per-column z0 around 0.1 m), the
+    closure, and the log-law state with k from the inflow profile."""
+    from ablsteadyrans_b200.abi import BC, FACE_INFLOW, FACE_OUTFLOW, FACE_SLIP_WALL, FACE_SURFACE_LAYER, Physics
+    from helpers import terrain_simplec_case
+    case = terrain_simplec_case(16, 12, 16, False, True, hill=60.0, seed=seed)
+    rng = np.random.default_rng(seed)
+    z0 = case.plane()
+    z0[:] = 0.1 * np.exp(0.3 * rng.standard_normal(z0.shape))
+    case.z0map = z0
+    bc = BC.make((FACE_INFLOW, 0, FACE_SURFACE_LAYER, FACE_OUTFLOW, 0, FACE_SLIP_WALL),
+                 theta_ref=((0.0, 1500.0), (300.0, 300.0)), ustar=0.4, z0=0.1, surface={"z0": 0.1})
+    ph = Physics.make(1500.0, closure=1, log_mean=1)
+    case.q["tke"][...] = np.abs(case.q["tke"]) + 0.2
+    case.q["theta"][...] = 300.0
+    case.q["w"][...] = 0.0
+    return case, bc, ph
