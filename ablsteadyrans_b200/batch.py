@@ -60,7 +60,7 @@ class Member:
             self.ctx = gb.Context(self.stream)
             z = torch.from_numpy(inst.z).cuda()
             J, ax, ay, az, _ = gb.mesh_metrics(self.ctx, g, z)
-            self.case = DeviceCase(g, z, J, ax, ay, az, inst.nu, inst.gamma_theta, inst.gamma_tke, inst.q)
+            self.case = DeviceCase(g, z, J, ax, ay, az, inst.nu, inst.gamma_theta, inst.gamma_tke, inst.q, inst.z0map)
             self.stage = SimplecStage(self.ctx, self.case, inst.bc, inst.physics, inst.options)
             self.stage.fill_ghosts()
             self.driver = Driver(self.stage)

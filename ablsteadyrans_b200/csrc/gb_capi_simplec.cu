@@ -83,8 +83,13 @@ gb_status check_bc(const gb_grid& g, const gb_bc& bc)
     for (int f = 0; f < 6; ++f) {
         const int d = f % 3;
         const int t = bc.face[f];
-        if (t < GB_FACE_PERIODIC || t > GB_FACE_NO_SLIP_WALL) {
+        if (t < GB_FACE_PERIODIC || t > GB_FACE_SURFACE_LAYER) {
             gb::set_error("gust: invalid inputs:\n  %s: unknown face type %d", keys[f], t);
+            return GB_BAD_ARG;
+        }
+        if (t == GB_FACE_SURFACE_LAYER && f != 2) {
+            gb::set_error("gust: invalid inputs:\n  %s = surface_layer: the surface layer is the ground's only "
+                          "(bc.zlo)", keys[f]);
             return GB_BAD_ARG;
         }
         if ((per[d] != 0) != (t == GB_FACE_PERIODIC)) {
@@ -106,11 +111,88 @@ gb_status check_bc(const gb_grid& g, const gb_bc& bc)
             return GB_BAD_ARG;
         }
     }
+    if (bc.face[2] == GB_FACE_SURFACE_LAYER) {
+        // check_surface_layer_options (SurfaceLayer.cpp:236-280), the keys bc.surface_*
+        auto bad = [](double x) { return std::isnan(x) || !std::isfinite(x); };
+        if (bad(bc.surface_z0) || !(bc.surface_z0 > 0)) {
+            gb::set_error("gust: invalid inputs:\n  bc.surface_z0 = %g: must be finite and > 0", bc.surface_z0);
+            return GB_BAD_ARG;
+        }
+        if (bad(bc.kappa) || !(bc.kappa > 0) || bad(bc.Cmu0) || !(bc.Cmu0 > 0)) {
+            gb::set_error("gust: invalid inputs:\n  the surface layer's kappa and Cmu0 must be finite and > 0");
+            return GB_BAD_ARG;
+        }
+        if (bad(bc.surface_zref)) {
+            gb::set_error("gust: invalid inputs:\n  bc.surface_zref = %g: must be finite (<= 0: first cell centre)",
+                          bc.surface_zref);
+            return GB_BAD_ARG;
+        }
+        if (bc.surface_stability != GB_SURFACE_NEUTRAL && bc.surface_stability != GB_SURFACE_HEAT_FLUX) {
+            gb::set_error("gust: invalid inputs:\n  bc.surface_stability must be neutral or heat_flux");
+            return GB_BAD_ARG;
+        }
+        if (bad(bc.surface_heat_flux)) {
+            gb::set_error("gust: invalid inputs:\n  bc.surface_heat_flux = %g: must be finite", bc.surface_heat_flux);
+            return GB_BAD_ARG;
+        }
+        if (bc.surface_stability == GB_SURFACE_NEUTRAL && bc.surface_heat_flux != 0) {
+            gb::set_error("gust: invalid inputs:\n  bc.surface_heat_flux is set but the stability is neutral; it would be "
+                          "ignored");
+            return GB_BAD_ARG;
+        }
+        if (bc.surface_wall_k != GB_WALL_K_DIRICHLET && bc.surface_wall_k != GB_WALL_K_SOURCE) {
+            gb::set_error("gust: invalid inputs:\n  bc.surface_wall_k must be dirichlet or source");
+            return GB_BAD_ARG;
+        }
+        if (bc.surface_denominator_floor != GB_DENOMINATOR_LOG_LAW && bc.surface_denominator_floor != GB_DENOMINATOR_ONE) {
+            gb::set_error("gust: invalid inputs:\n  bc.surface_denominator_floor must be log_law or one");
+            return GB_BAD_ARG;
+        }
+    }
     bool inflow = false;
     for (int f = 0; f < 6; ++f) { inflow = inflow || bc.face[f] == GB_FACE_INFLOW; }
     if (inflow && !(bc.inflow_ustar > 0 && bc.inflow_z0 > 0 && bc.kappa > 0 && bc.Cmu0 > 0)) {
         gb::set_error("gust: invalid inputs:\n  bc.inflow_ustar and bc.inflow_z0 must be > 0 (log law)");
         return GB_BAD_ARG;
+    }
+    return GB_OK;
+}
+
+//! check_closure_options (Closure.cpp:171-210): one message naming the key.
+gb_status check_closure(const gb_physics& ph)
+{
+    if (ph.closure != 0 && ph.closure != 1) {
+        gb::set_error("gust: invalid inputs:\n  the closure switch must be 0 (given diffusivities) or 1 (k-L)");
+        return GB_BAD_ARG;
+    }
+    if (!ph.closure) { return GB_OK; }
+    auto bad = [](double x) { return std::isnan(x) || !std::isfinite(x); };
+    struct Rule {
+        const char* key;
+        double x;
+        bool ok;
+        const char* range;
+    };
+    const double eps = std::numeric_limits<double>::epsilon();
+    const Rule rules[] = {
+        {"Cmu0", ph.turb_Cmu0, ph.turb_Cmu0 > 0, "finite and > 0"},
+        {"Cb", ph.turb_Cb, ph.turb_Cb > 0, "finite and > 0"},
+        {"Rt_crit", ph.turb_Rt_crit, ph.turb_Rt_crit <= 0, "finite and <= 0"},
+        {"Rt_min", ph.turb_Rt_min, ph.turb_Rt_min < ph.turb_Rt_crit && ph.turb_Rt_min > -3.598,
+         "finite, < turb.Rt_crit and > -3.598 (c_mu has its pole at -3.5987)"},
+        {"max_geom_lscale", ph.turb_max_geom_lscale, ph.turb_max_geom_lscale > 0, "finite and > 0 (m)"},
+        {"tke_floor", ph.turb_tke_floor, ph.turb_tke_floor == 0 || ph.turb_tke_floor >= eps,
+         "0 (machine epsilon) or >= machine epsilon (m^2/s^2)"},
+        {"sigma_k", ph.turb_sigma_k, ph.turb_sigma_k > 0, "finite and > 0"},
+        {"nu_molecular", ph.turb_nu_molecular, ph.turb_nu_molecular >= 0, "finite and >= 0 (m^2/s)"},
+        {"alpha_molecular", ph.turb_alpha_molecular, ph.turb_alpha_molecular >= 0, "finite and >= 0 (m^2/s)"},
+        {"kappa", ph.turb_kappa, ph.turb_kappa > 0, "finite and > 0"},
+    };
+    for (const Rule& r : rules) {
+        if (bad(r.x) || !r.ok) {
+            gb::set_error("gust: invalid closure options:\n  turb.%s = %g: must be %s", r.key, r.x, r.range);
+            return GB_BAD_ARG;
+        }
     }
     return GB_OK;
 }
@@ -132,8 +214,13 @@ gb_status gb_simplec_create(gb_ctx* ctx, const gb_grid* g, const gb_bc* bc, cons
     gb_status st = gb::check_grid("SimplecStage", g);
     if (st == GB_OK) { st = check_simplec_options(*opt); }
     if (st == GB_OK) { st = check_bc(*g, *bc); }
+    if (st == GB_OK) { st = check_closure(*ph); }
     if (st != GB_OK) { return st; }
-    if (!mesh->detJ || !mesh->ax || !mesh->ay || !mesh->az || !df->nu || !df->gamma_theta || !df->gamma_tke) {
+    if (!mesh->detJ || !mesh->ax || !mesh->ay || !mesh->az) {
+        gb::set_error("gust: SimplecStage: the mesh's detJ, ax, ay and az are needed");
+        return GB_BAD_ARG;
+    }
+    if (!ph->closure && (!df->nu || !df->gamma_theta || !df->gamma_tke)) {
         gb::set_error("gust: SimplecStage: without a closure the residual inputs need the diffusivities");
         return GB_BAD_ARG;
     }
@@ -154,6 +241,16 @@ gb_status gb_simplec_create(gb_ctx* ctx, const gb_grid* g, const gb_bc* bc, cons
         return GB_BAD_ARG;
     }
     return gb::simplec_create_checked(ctx, g, bc, ph, opt, z_nd, mesh, df, out);
+}
+
+gb_status gb_simplec_turbulence(gb_simplec* s, double* const* closure, double* const* surface)
+{
+    gb::clear_error();
+    if (s == nullptr) {
+        gb::set_error("gust: SimplecStage: null argument");
+        return GB_BAD_ARG;
+    }
+    return gb::simplec_turbulence(s, closure, surface);
 }
 
 gb_status gb_simplec_destroy(gb_simplec* s)

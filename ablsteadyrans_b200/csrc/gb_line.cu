@@ -222,7 +222,11 @@ __global__ void __launch_bounds__(128) zline_pipe_kernel(LineArgs<T> a)
 //! e_k = (r_k + a_ZM,k e_{k-1}) / m_k as a multiply by the stored 1/m_k:
 //! no division on the k chain. Inputs are staged R levels ahead with cp.async
 //! as in zline_pipe_kernel.
-template <typename T, bool FIRST, int R>
+//! BG: the forward sweep's c' and e' stay in global memory for the back
+//! substitution (c' in its stored array, e' in the output array, which the
+//! back substitution overwrites level by level), so shared memory holds the
+//! ring alone and more warps fit on an SM; otherwise both go to shared memory.
+template <typename T, bool FIRST, int R, bool BG = false>
 __device__ __forceinline__ void zline_fact_body(const LineArgs<T>& a, T* __restrict__ im_out,
                                                 const T* __restrict__ im_in, T* __restrict__ cp_out,
                                                 const T* __restrict__ cp_in)
@@ -305,13 +309,34 @@ __device__ __forceinline__ void zline_fact_body(const LineArgs<T>& a, T* __restr
             }
             cprev = c;
             eprev = ((k == 0) ? rk : rk - lower * eprev) * inv;
-            cs[k * nthr + tid] = c;
-            es[k * nthr + tid] = eprev;
+            if (BG) {
+                a.dnew[o0 + static_cast<int64_t>(k) * g.sz] = eprev;
+            } else {
+                cs[k * nthr + tid] = c;
+                es[k * nthr + tid] = eprev;
+            }
         }
     }
     cp_async_wait<0>();
     T chg = T(0);
-    if (active) {
+    if (BG && active) {
+        // x_k = e'_k - c'_k x_{k+1} in place over e' (this thread's own writes)
+        const T* cpk = FIRST ? cp_out : cp_in;
+        T x = eprev;
+        int64_t ko = static_cast<int64_t>(a.nk - 1) * g.sz;
+        if (a.change) { chg = fabs(x - (FIRST ? T(0) : a.dold[o0 + ko])); }
+#pragma unroll 8
+        for (int k = a.nk - 2; k >= 0; --k) {
+            ko -= g.sz;
+            x = a.dnew[o0 + ko] - cpk[o0 + ko] * x;
+            a.dnew[o0 + ko] = x;
+            if (a.change) {
+                const T d = fabs(x - (FIRST ? T(0) : a.dold[o0 + ko]));
+                chg = (d > chg || d != d) ? d : chg;
+            }
+        }
+    }
+    if (!BG && active) {
         T x = eprev;
         int64_t ko = static_cast<int64_t>(a.nk - 1) * g.sz;
         a.dnew[o0 + ko] = x;
@@ -354,24 +379,24 @@ struct MultiLineArgs {
     T* cp[kMaxLineSystems];
 };
 
-template <typename T, bool FIRST, int R, int S>
+template <typename T, bool FIRST, int R, int S, bool BG>
 __device__ __forceinline__ void zline_fact_system(const MultiLineArgs<T>& m)
 {
     if (FIRST) {
-        zline_fact_body<T, true, R>(m.a[S], m.inv[S], nullptr, m.cp[S], nullptr);
+        zline_fact_body<T, true, R, BG>(m.a[S], m.inv[S], nullptr, m.cp[S], nullptr);
     } else {
-        zline_fact_body<T, false, R>(m.a[S], nullptr, m.inv[S], nullptr, m.cp[S]);
+        zline_fact_body<T, false, R, BG>(m.a[S], nullptr, m.inv[S], nullptr, m.cp[S]);
     }
 }
 
-template <typename T, bool FIRST, int R>
+template <typename T, bool FIRST, int R, bool BG>
 __global__ void __launch_bounds__(128) zline_fact_multi_kernel(MultiLineArgs<T> m)
 {
     // constant indices into the parameter block (no dynamic parameter indexing)
     switch (blockIdx.z) {
-    case 0: zline_fact_system<T, FIRST, R, 0>(m); break;
-    case 1: zline_fact_system<T, FIRST, R, 1>(m); break;
-    default: zline_fact_system<T, FIRST, R, 2>(m); break;
+    case 0: zline_fact_system<T, FIRST, R, 0, BG>(m); break;
+    case 1: zline_fact_system<T, FIRST, R, 1, BG>(m); break;
+    default: zline_fact_system<T, FIRST, R, 2, BG>(m); break;
     }
 }
 
@@ -573,14 +598,17 @@ gb_status zline_sweeps_multi(gb_ctx* ctx, const gb_grid& g, int n, const int* lo
     static std::atomic<bool> attr_done[2];  // set once per process (one device per process)
     const int ti = sizeof(T) == 8 ? 1 : 0;
     if (!attr_done[ti].load()) {
-        cudaFuncSetAttribute(zline_fact_multi_kernel<T, true, R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaFuncSetAttribute(zline_fact_multi_kernel<T, true, R, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              200 * 1024);
-        cudaFuncSetAttribute(zline_fact_multi_kernel<T, false, R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaFuncSetAttribute(zline_fact_multi_kernel<T, false, R, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              200 * 1024);
         attr_done[ti].store(true);
     }
-    const size_t smem_first = static_cast<size_t>(R * 4 + 2 * max_nk) * kThr * sizeof(T);
-    const size_t smem = static_cast<size_t>(R * 12 + 2 * max_nk) * kThr * sizeof(T);
+    // c' and e' of the back substitution in shared memory (1) or in the global arrays (2)
+    const bool bg = ctx->tune[GB_TUNE_LINE_BACK] == 2;
+    const size_t back = bg ? 0 : static_cast<size_t>(2 * max_nk);
+    const size_t smem_first = static_cast<size_t>(R * 4 + back) * kThr * sizeof(T);
+    const size_t smem = static_cast<size_t>(R * 12 + back) * kThr * sizeof(T);
     const dim3 grid((max_ni + kThr - 1) / kThr, max_nj, n);
     for (int k = 0; k < sweeps; ++k) {
         MultiLineArgs<T> m{};
@@ -606,9 +634,15 @@ gb_status zline_sweeps_multi(gb_ctx* ctx, const gb_grid& g, int n, const int* lo
         }
         Span span(ctx, GB_KERNEL_LINE_SWEEP);
         if (k == 0) {
-            zline_fact_multi_kernel<T, true, R><<<grid, kThr, smem_first, ctx->stream>>>(m);
+            if (bg) {
+                zline_fact_multi_kernel<T, true, R, true><<<grid, kThr, smem_first, ctx->stream>>>(m);
+            } else {
+                zline_fact_multi_kernel<T, true, R, false><<<grid, kThr, smem_first, ctx->stream>>>(m);
+            }
+        } else if (bg) {
+            zline_fact_multi_kernel<T, false, R, true><<<grid, kThr, smem, ctx->stream>>>(m);
         } else {
-            zline_fact_multi_kernel<T, false, R><<<grid, kThr, smem, ctx->stream>>>(m);
+            zline_fact_multi_kernel<T, false, R, false><<<grid, kThr, smem, ctx->stream>>>(m);
         }
         ++ctx->launches;
     }

@@ -1,7 +1,9 @@
 // The SIMPLEC outer iteration on the GPU (gust::SimplecStage::iterate,
-// Source/Simplec.cpp:452-506) without a closure and a wall model: boundary
-// ghost fills, the FP64 residual (convection, full-stress terrain diffusion,
-// pressure gradient, forcing, continuity), the implicit rows, the momentum
+// Source/Simplec.cpp:452-506): boundary ghost fills (the wall law's ground
+// gradient on a surface_layer ground), the FP64 residual (convection,
+// full-stress terrain diffusion with the given diffusivities or the k-L
+// closure's, the wall model's ground fluxes, pressure gradient, forcing,
+// continuity, the k sources and wall-k rows), the implicit rows, the momentum
 // predictor with z-line sweeps, the pressure correction through the Poisson
 // layer, the theta and k sweeps and the stage norms. Every reduction is
 // deterministic (block partials summed in a fixed order, maxima by bit
@@ -10,6 +12,7 @@
 #include "gb_poisson_api.cuh"
 #include "gb_simplec.cuh"
 #include "gb_stencil.cuh"
+#include "gb_turbulence.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -25,6 +28,8 @@ enum { R_EVEN = 0, R_ODD, R_VALUE, R_PROFILE, R_GRADIENT };
 enum { F_U = 0, F_V, F_W, F_P, F_THETA, F_TKE };
 
 constexpr int kRedBlocks = 512;
+//! The result word that counts the ground columns without a positive, finite u*.
+constexpr int W_SURFACE_BAD = 40;
 
 // ------------------------------------------------------------- heights ---
 
@@ -104,6 +109,9 @@ int rule_for(int f, int t, int d, bool lo)
         if (normal_vel) { return R_VALUE; }
         return (f == F_THETA && d == 2 && !lo) ? R_GRADIENT : R_EVEN;
     case GB_FACE_NO_SLIP_WALL: return vel ? R_VALUE : R_EVEN;
+    case GB_FACE_SURFACE_LAYER:
+        if (normal_vel) { return R_VALUE; }
+        return (vel || f == F_THETA) ? R_GRADIENT : R_EVEN;
     default: return R_EVEN;
     }
 }
@@ -111,7 +119,7 @@ int rule_for(int f, int t, int d, bool lo)
 bool dirichlet_normal(const gb_bc& bc, int face)
 {
     const int t = bc.face[face];
-    return t == GB_FACE_INFLOW || t == GB_FACE_SLIP_WALL || t == GB_FACE_NO_SLIP_WALL;
+    return t == GB_FACE_INFLOW || t == GB_FACE_SLIP_WALL || t == GB_FACE_NO_SLIP_WALL || t == GB_FACE_SURFACE_LAYER;
 }
 
 inline bool is_per(const gb_grid& g, int d) { return d == 0 ? g.periodic_x : d == 1 ? g.periodic_y : false; }
@@ -263,6 +271,16 @@ struct gb_simplec {
     gb_simplec_opts opt{};
     gb_mesh_fields mesh{};
     gb_diffusivities df{};
+    // the diffusivities the stencils read: df, or the closure's fields
+    // (0 before the first residual: the first local dtau's, Simplec.cpp:328)
+    gb_diffusivities dfe{};
+    bool wall{false};                    // bc.zlo = surface_layer
+    double* cf[gb::kClosureFields]{};    // the closure's fields at the last residual
+    double* dist{nullptr};               // the cells' height above the ground (closure)
+    double* ss[gb::kSsPlanes]{};         // the surface state of the iteration's first fill
+    double* ssr[gb::kSsPlanes]{};        // the residual's own surface state
+    double* sst[gb::kSsPlanes]{};        // the later fills' surface state
+    double* gg[3]{};                     // the wall law's ground gradient (u, v, theta)
     const double* z{nullptr};
     gb::SimplecWork w{};
     gb::Profile prof{};
@@ -344,6 +362,7 @@ struct FieldFill {
     double* a;
     int t, f, rule;
     double V;
+    const double* gg;   // the wall law's gradient per column (null: the constant G)
 };
 struct FillPack {
     FieldFill F[6];
@@ -412,6 +431,8 @@ void fill_side(gb_simplec* S, const gb_state& q, int d, bool lo)
         FF[f].f = f;
         FF[f].rule = rule_for(f, ft, d, lo);
         FF[f].V = (ft == GB_FACE_NO_SLIP_WALL && f <= F_W) ? S->bc.wall_velocity[face][f] : 0.0;
+        FF[f].gg = nullptr;
+        if (ft == GB_FACE_SURFACE_LAYER && FF[f].rule == R_GRADIENT) { FF[f].gg = S->gg[f == F_U ? 0 : f == F_V ? 1 : 2]; }
     }
     FillPack P;
     std::memcpy(P.F, FF, sizeof(FF));
@@ -450,15 +471,16 @@ void fill_side(gb_simplec* S, const gb_state& q, int d, bool lo)
             const bool nod = nodal(t, d);
             double* a = F.a;
             if (F.rule == R_GRADIENT) {
-                // the top (d == 2, not lo): one thread per column does both layers
+                // the top or a surface_layer ground (d == 2): one thread per column does both layers
                 if (layer != 1) { continue; }
                 const int edge = lo ? 0 : nd - 1 + nod;
                 const int c1 = lo ? edge + 1 : edge - 1, g1 = lo ? edge - 1 : edge + 1, g2 = lo ? edge - 2 : edge + 2;
                 const double zc1 = point_z(z, g, t, i, j, c1), zg1 = point_z(z, g, t, i, j, g1),
                              zg2 = point_z(z, g, t, i, j, g2);
-                const double v1 = a[at(g, i, j, c1)] + (zg1 - zc1) * G;
+                const double Gp = F.gg ? ground_gradient_at(g, F.gg, t, i, j) : G;
+                const double v1 = a[at(g, i, j, c1)] + (zg1 - zc1) * Gp;
                 a[at(g, i, j, g1)] = v1;
-                a[at(g, i, j, g2)] = v1 + (zg2 - zg1) * G;
+                a[at(g, i, j, g2)] = v1 + (zg2 - zg1) * Gp;
                 continue;
             }
             const int edge = lo ? 0 : (nod ? nd : nd - 1);
@@ -514,11 +536,18 @@ void fill_no_flux_w(gb_simplec* S, const gb_state& q)
 
 }  // namespace
 
-void simplec_fill_ghosts(gb_simplec* S, const gb_state& q)
+//! BoundaryConditions::fill_ghosts (BoundaryConditions.cpp:597-663); a
+//! surface_layer ground: the surface state from the laterally filled state
+//! into ss and the wall law's gradient for the ground fills.
+void fill_ghosts_into(gb_simplec* S, const gb_state& q, double* const* ss)
 {
     double* f[6] = {q.u, q.v, q.w, q.p, q.theta, q.tke};
     fill_periodic_all(S, f, kLoc, 6);
     for (int d = 0; d < 3; ++d) {
+        if (d == 2 && S->wall) {
+            turb_surface_state(S->ctx, S->g, S->bc, S->ph, q, S->z, S->mesh.z0, ss, dword(S->ctx, W_SURFACE_BAD));
+            turb_ground_gradients(S->ctx, S->g, S->bc, ss, S->mesh.z0, S->gg);
+        }
         if (is_per(S->g, d)) { continue; }
         fill_side(S, q, d, true);
         fill_side(S, q, d, false);
@@ -529,6 +558,8 @@ void simplec_fill_ghosts(gb_simplec* S, const gb_state& q)
     }
     fill_periodic_all(S, f, kLoc, 6);
 }
+
+void simplec_fill_ghosts(gb_simplec* S, const gb_state& q) { fill_ghosts_into(S, q, S->ss); }
 
 // ------------------------------------------------------------ stencils ---
 
@@ -798,22 +829,29 @@ void momentum_diffusive_flux(gb_simplec* S, const gb_state& q, const double* nu,
     }, GB_KERNEL_RESIDUAL);
 }
 
+//! The diffusion of velocity component C subtracted from R; a surface_layer
+//! ground sets the u and v control volumes' ground fluxes to the wall
+//! stress first (set_ground_fluxes; w's ground row is a boundary row).
 template <int C>
 void momentum_diffusion_subtract(gb_simplec* S, const gb_state& q, double* R)
 {
     double** G = S->w.G;
-    momentum_diffusive_flux<C, 0>(S, q, S->df.nu, G[0]);
-    momentum_diffusive_flux<C, 1>(S, q, S->df.nu, G[1]);
-    momentum_diffusive_flux<C, 2>(S, q, S->df.nu, G[2]);
+    momentum_diffusive_flux<C, 0>(S, q, S->dfe.nu, G[0]);
+    momentum_diffusive_flux<C, 1>(S, q, S->dfe.nu, G[1]);
+    momentum_diffusive_flux<C, 2>(S, q, S->dfe.nu, G[2]);
+    if (S->wall && C < 2) { turb_ground_flux(S->ctx, S->g, S->bc, S->ssr, C, G[2]); }
     flux_divergence<1 << C>(S, G[0], G[1], G[2], R, 1);
 }
 
-void scalar_diffusion_subtract(gb_simplec* S, const double* q, const double* gamma, double* R)
+//! The diffusion of a cell scalar subtracted from R; field 2 theta, 3 k (the
+//! wall model's ground flux on a surface_layer ground).
+void scalar_diffusion_subtract(gb_simplec* S, const double* q, const double* gamma, double* R, int field)
 {
     double** G = S->w.G;
     scalar_diffusive_flux<0>(S, q, gamma, G[0]);
     scalar_diffusive_flux<1>(S, q, gamma, G[1]);
     scalar_diffusive_flux<2>(S, q, gamma, G[2]);
+    if (S->wall) { turb_ground_flux(S->ctx, S->g, S->bc, S->ssr, field, G[2]); }
     flux_divergence<CC>(S, G[0], G[1], G[2], R, 1);
 }
 
@@ -938,6 +976,9 @@ void simplec_residual(gb_simplec* S, const gb_state& q, double** R)
     const gb_grid g = S->g;
     const int64_t vol = volume(g);
     for (int n = 0; n < 6; ++n) { cudaMemsetAsync(R[n], 0, sizeof(double) * vol, ctx->stream); }
+    // the closure's fields and the wall state at q (Residual.cpp:166-176, 205-208)
+    if (S->ph.closure) { turb_closure(ctx, g, S->bc, S->ph, q, S->z, S->dist, S->mesh.z0, S->cf); }
+    if (S->wall) { turb_surface_state(ctx, g, S->bc, S->ph, q, S->z, S->mesh.z0, S->ssr, dword(ctx, W_SURFACE_BAD)); }
     double** F = S->w.F;
     transport_fluxes(S, q, F[0], F[1], F[2]);
     const gb_physics& ph = S->ph;
@@ -951,9 +992,11 @@ void simplec_residual(gb_simplec* S, const gb_state& q, double** R)
     forcing(S, q, R);
     velocity_divergence(S, q.u, q.v, q.w, R[3]);
     convection<CC>(S, q.theta, F, ph.limiter, ph.smooth_eps_theta, false, R[4]);
-    scalar_diffusion_subtract(S, q.theta, S->df.gamma_theta, R[4]);
+    scalar_diffusion_subtract(S, q.theta, S->dfe.gamma_theta, R[4], 2);
     convection<CC>(S, q.tke, F, GB_LIMITER_UPWIND, 1e-5, true, R[5]);
-    scalar_diffusion_subtract(S, q.tke, S->df.gamma_tke, R[5]);
+    scalar_diffusion_subtract(S, q.tke, S->dfe.gamma_tke, R[5], 3);
+    if (S->ph.closure) { turb_k_sources(ctx, g, S->cf, R[5]); }
+    if (S->wall) { turb_apply_wall_k(ctx, g, S->bc, S->ssr, q.tke, R[5]); }
     apply_rows(S, q, R);
     seam_sync<double>(ctx, g, XF, R[0]);
     seam_sync<double>(ctx, g, YF, R[1]);
@@ -1081,16 +1124,25 @@ void dirichlet_rows(gb_simplec* S, int f, int t, double* mask)
 
 }  // namespace
 
+//! implicit_rows (Residual.cpp:272-304): the coefficients with the
+//! effective diffusivity, the Patankar diagonal of k with the closure, the
+//! first cells' wall rows (the surface state of the iteration's first fill)
+//! for every equation but w, then the boundary folds.
 void simplec_implicit_rows(gb_simplec* S, int eq, double* const* F, double* A)
 {
     switch (eq) {
-    case F_U: implicit_coefficients<0>(S, F, S->df.nu, A); break;
-    case F_V: implicit_coefficients<1>(S, F, S->df.nu, A); break;
-    case F_W: implicit_coefficients<2>(S, F, S->df.nu, A); break;
-    case F_THETA: implicit_coefficients<-1>(S, F, S->df.gamma_theta, A); break;
-    default: implicit_coefficients<-1>(S, F, S->df.gamma_tke, A); break;
+    case F_U: implicit_coefficients<0>(S, F, S->dfe.nu, A); break;
+    case F_V: implicit_coefficients<1>(S, F, S->dfe.nu, A); break;
+    case F_W: implicit_coefficients<2>(S, F, S->dfe.nu, A); break;
+    case F_THETA: implicit_coefficients<-1>(S, F, S->dfe.gamma_theta, A); break;
+    default: implicit_coefficients<-1>(S, F, S->dfe.gamma_tke, A); break;
     }
     const int t = (eq <= F_W) ? (1 << eq) : CC;
+    if (S->ph.closure && eq == F_TKE) { turb_patankar(S->ctx, S->g, S->cf[kClosureDSdk], A); }
+    if (S->wall && eq != F_W) {
+        turb_wall_rows(S->ctx, S->g, S->ss, t, S->mesh.detJ, A);
+        if (eq == F_TKE) { turb_wall_k_rows(S->ctx, S->g, S->bc, S->ss, A); }
+    }
     apply_to_implicit(S, eq, t, A);
 }
 
@@ -1546,7 +1598,9 @@ gb_status simplec_iterate(gb_simplec* S, const gb_state& q, const double* dtau, 
     SimplecWork& w = S->w;
     *info = gb_iter_info{};
     cudaMemsetAsync(dword(ctx, 0), 0, sizeof(unsigned long long) * W_COUNT, ctx->stream);
-    simplec_fill_ghosts(S, q);
+    cudaMemsetAsync(dword(ctx, W_SURFACE_BAD), 0, sizeof(unsigned long long), ctx->stream);
+    // 1. ghosts and the wall state at q; 2. the residual (the closure at q)
+    fill_ghosts_into(S, q, S->ss);
     simplec_residual(S, q, w.R);
     for (int n = 0; n < 6; ++n) { dsum(S, valid_box(g, kLoc[n]), w.R[n], 0, SUM_R0 + n); }
     dsum(S, valid_box(g, CC), q.tke, 1, SUM_TKE);
@@ -1557,10 +1611,10 @@ gb_status simplec_iterate(gb_simplec* S, const gb_state& q, const double* dtau, 
     face_dtau(S, dtau, w.dtf);
     gb_status st = momentum_predictor(S, q, w.R);
     if (st != GB_OK) { return st; }
-    simplec_fill_ghosts(S, q);
+    fill_ghosts_into(S, q, S->sst);
     if ((st = pressure_correction(S, q, info)) != GB_OK) { return st; }
     convection<CC>(S, q.theta, w.F, S->ph.limiter, S->ph.smooth_eps_theta, false, w.conv0);
-    simplec_fill_ghosts(S, q);
+    fill_ghosts_into(S, q, S->sst);
     transport_fluxes(S, q, w.F[0], w.F[1], w.F[2]);
     convection<CC>(S, q.theta, w.F, S->ph.limiter, S->ph.smooth_eps_theta, false, w.conv1);
     {
@@ -1602,6 +1656,15 @@ gb_status simplec_iterate(gb_simplec* S, const gb_state& q, const double* dtau, 
     info->max_dtheta = wd(W_MAX_DTH);
     info->max_dtke = wd(W_MAX_DK);
     info->tke_clipped = static_cast<int64_t>(words[W_CLIPPED]);
+    if (S->wall) {
+        unsigned long long bad = 0;
+        if ((st = read_words(ctx, W_SURFACE_BAD, 1, &bad)) != GB_OK) { return st; }
+        if (bad > 0) {
+            set_error("gust: compute_surface_state: no positive, finite friction velocity at %llu column fills "
+                      "(surface layer heat_flux = %g)", bad, S->bc.surface_heat_flux);
+            return GB_NONFINITE;
+        }
+    }
     for (int n = 0; n < 6; ++n) {
         if (!std::isfinite(info->residual_norms[n])) {
             set_error("gust: SimplecStage::iterate: non-finite residual (equation %d)", n);
@@ -1621,7 +1684,7 @@ gb_status simplec_local_dtau(gb_simplec* S, const gb_state& q, double cfl, doubl
     const double* v = q.v;
     const double* om = S->w.om;
     const double* J = S->mesh.detJ;
-    const double* nu = S->df.nu;
+    const double* nu = S->dfe.nu;
     const double dxinv = 1.0 / g.dx, dyinv = 1.0 / g.dy, dzinv = 1.0 / g.dzeta;
     const double diff_h = 2 * (dxinv * dxinv + dyinv * dyinv);
     for_box(S->ctx, valid_box(g, CC), [=] __device__(int i, int j, int k) {
@@ -1825,6 +1888,35 @@ gb_status simplec_initialize(gb_simplec* S, const gb_state& q, const gb_init_opt
     return check_cuda("initialize_state");
 }
 
+gb_status simplec_turbulence(gb_simplec* S, double* const* closure, double* const* surface)
+{
+    gb_ctx* ctx = S->ctx;
+    if (closure != nullptr) {
+        if (!S->ph.closure) {
+            set_error("gust: SimplecStage::closure_fields: the stage has no closure");
+            return GB_BAD_ARG;
+        }
+        for (int n = 0; n < kClosureFields; ++n) {
+            if (closure[n]) {
+                cudaMemcpyAsync(closure[n], S->cf[n], sizeof(double) * volume(S->g), cudaMemcpyDeviceToDevice, ctx->stream);
+            }
+        }
+    }
+    if (surface != nullptr) {
+        if (!S->wall) {
+            set_error("gust: SimplecStage: the stage's ground is not a surface layer");
+            return GB_BAD_ARG;
+        }
+        for (int n = 0; n < kSsPlanes; ++n) {
+            if (surface[n]) {
+                cudaMemcpyAsync(surface[n], S->ss[n], sizeof(double) * plane_size(S->g), cudaMemcpyDeviceToDevice,
+                                ctx->stream);
+            }
+        }
+    }
+    return check_cuda("SimplecStage::closure_fields");
+}
+
 const gb_grid& simplec_grid(const gb_simplec* S) { return S->g; }
 gb_ctx* simplec_ctx(const gb_simplec* S) { return S->ctx; }
 
@@ -1885,6 +1977,30 @@ gb_status simplec_build(gb_simplec* S)
             w.delta32m[s] = fbuf(S, vol);
         }
     }
+    // the closure's fields and the surface state (gust::ClosureFields,
+    // gust::SurfaceState), when the closure is on or the ground is a surface layer
+    S->wall = S->bc.face[2] == GB_FACE_SURFACE_LAYER;
+    S->dfe = S->df;
+    bool turb_ok = true;
+    if (S->ph.closure) {
+        for (int n = 0; n < kClosureFields; ++n) { turb_ok = (S->cf[n] = dbuf(S, vol)) && turb_ok; }
+        turb_ok = (S->dist = dbuf(S, vol)) && turb_ok;
+        S->dfe = gb_diffusivities{S->cf[kClosureNu], S->cf[kClosureGammaTheta], S->cf[kClosureGammaTke]};
+    }
+    if (S->wall) {
+        const int64_t np = plane_size(g);
+        for (int n = 0; n < kSsPlanes; ++n) {
+            turb_ok = (S->ss[n] = dbuf(S, np)) && turb_ok;
+            turb_ok = (S->ssr[n] = dbuf(S, np)) && turb_ok;
+            turb_ok = (S->sst[n] = dbuf(S, np)) && turb_ok;
+        }
+        for (int n = 0; n < 3; ++n) { turb_ok = (S->gg[n] = dbuf(S, np)) && turb_ok; }
+    }
+    if (!turb_ok) {
+        set_error("gust: SimplecStage: cannot allocate the closure's fields and the surface state");
+        return GB_OOM;
+    }
+    if (S->ph.closure) { turb_height_above_ground(ctx, g, S->z, S->dist); }
     for (void* p : S->owned) {
         if (p == nullptr) {
             set_error("gust: SimplecStage: cannot allocate the workspace");

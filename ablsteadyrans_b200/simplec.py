@@ -27,6 +27,12 @@ def _declare(L):
                                 ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32)]
     L.gb_simplec_initialize.argtypes = [P, ctypes.POINTER(abi.State), ctypes.POINTER(abi.InitOptions),
                                         ctypes.POINTER(abi.InitResult)]
+    L.gb_simplec_turbulence.argtypes = [P, ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_void_p)]
+
+
+# The closure's fields and the surface state's planes, in the ABI's order.
+CLOSURE_FIELDS = ("nu", "gamma_theta", "gamma_tke", "nut", "length", "Rt", "Ps", "Pb", "eps", "dSdk")
+SURFACE_FIELDS = ("ustar", "speed", "zref", "d0", "inv_L", "tau_x", "tau_y", "tau_z", "drag", "kwall", "area")
 
 
 FIELDS = ("u", "v", "w", "p", "theta", "tke")
@@ -36,7 +42,7 @@ class DeviceCase:
     """Device copies of one instance: state (u, v, w, p, theta, k), node
     heights, metrics, diffusivities."""
 
-    def __init__(self, grid, z, J, ax, ay, az, nu, gamma_theta, gamma_tke, q=None):
+    def __init__(self, grid, z, J, ax, ay, az, nu, gamma_theta, gamma_tke, q=None, z0map=None):
         import torch
 
         def dev(a):
@@ -45,18 +51,21 @@ class DeviceCase:
         self.grid = grid
         self.z, self.J, self.ax, self.ay, self.az = map(dev, (z, J, ax, ay, az))
         self.nu, self.gt, self.gk = map(dev, (nu, gamma_theta, gamma_tke))
+        self.z0map = None if z0map is None else dev(z0map)
         self.q = {f: (dev(q[f]) if q is not None else torch.zeros(grid.shape, dtype=torch.float64, device="cuda"))
                   for f in FIELDS}
 
     @classmethod
     def from_oracle(cls, case):
-        return cls(case.grid, case.z, case.J, case.ax, case.ay, case.az, case.nu, case.gt, case.gk, case.q)
+        return cls(case.grid, case.z, case.J, case.ax, case.ay, case.az, case.nu, case.gt, case.gk, case.q,
+                   getattr(case, "z0map", None))
 
     def state(self):
         return abi.State(*[self.q[f].data_ptr() for f in FIELDS], self.z.data_ptr())
 
     def mesh(self):
-        return abi.MeshFields(self.J.data_ptr(), self.ax.data_ptr(), self.ay.data_ptr(), self.az.data_ptr())
+        return abi.MeshFields(self.J.data_ptr(), self.ax.data_ptr(), self.ay.data_ptr(), self.az.data_ptr(),
+                              None if self.z0map is None else self.z0map.data_ptr())
 
     def diffusivities(self):
         return abi.Diffusivities(self.nu.data_ptr(), self.gt.data_ptr(), self.gk.data_ptr())
@@ -97,6 +106,23 @@ class SimplecStage:
         st = self.case.state()
         check(self._L.gb_simplec_residual(self._h, ctypes.byref(st), arr))
         return R
+
+    def turbulence(self, closure=True, surface=True):
+        """(closure fields, surface state) as dicts of host arrays: the
+        closure's at the last residual, the wall state of the last fill."""
+        import torch
+        from . import check
+        g = self.case.grid
+        cf = [torch.zeros(g.shape, dtype=torch.float64, device="cuda") for _ in CLOSURE_FIELDS] if closure else None
+        np_ = int(g.c.sy) * (g.ny + 1 + 2 * g.ng)
+        ss = [torch.zeros(np_, dtype=torch.float64, device="cuda") for _ in SURFACE_FIELDS] if surface else None
+        ca = (ctypes.c_void_p * len(cf))(*[t.data_ptr() for t in cf]) if cf else None
+        sa = (ctypes.c_void_p * len(ss))(*[t.data_ptr() for t in ss]) if ss else None
+        check(self._L.gb_simplec_turbulence(self._h, ca, sa))
+        torch.cuda.synchronize()
+        out_c = dict(zip(CLOSURE_FIELDS, [t.cpu().numpy() for t in cf])) if cf else None
+        out_s = dict(zip(SURFACE_FIELDS, [t.cpu().numpy() for t in ss])) if ss else None
+        return out_c, out_s
 
     def local_dtau(self, cfl, out=None):
         import torch

@@ -1,7 +1,7 @@
 """Synthetic inputs of the benchmark configurations (one seeded generator for
 the GPU path and the CPU baseline): vertical levels, terrain (Gaussian hill,
-fractal field), BTF node heights, the log-law inflow state and frozen eddy
-diffusivities, boundary and physics settings.
+fractal field), BTF node heights, the per-column roughness, the log-law
+inflow state, boundary and physics settings.
 
 Resolved ambiguities of the configurations:
   * "a 2 m first cell at ratio 1.1 up to a 1500 m lid" is over-determined:
@@ -11,10 +11,13 @@ Resolved ambiguities of the configurations:
     one the wind blows towards, CCW from +x: 270 - met.
   * Coriolis f: forcing.latitude = 90 with rotation_period = 4 pi / f; the
     geostrophic wind is the log-law wind at the lid.
-  * The wall model and the k-L closure are outside this build's first slice:
-    the ground is a no-slip wall and the diffusivities are frozen at the
-    inflow's equilibrium mixing-length profile, nu = nu_mol + kappa u* (h +
-    z0) / (1 + kappa (h + z0) / l_max), gamma_theta = nu / 0.85, gamma_k = nu.
+  * Physics (turbulence=True, the default): the k-L closure (turb.*
+    defaults, max_geom_lscale 30 m) and a neutral surface_layer ground
+    (MOST, Dirichlet wall k) with the configuration's z0. With
+    turbulence=False the ground is a no-slip wall and the diffusivities are
+    frozen at the inflow's equilibrium mixing-length profile, nu = nu_mol +
+    kappa u* (h + z0) / (1 + kappa (h + z0) / l_max), gamma_theta = nu / 0.85,
+    gamma_k = nu (the given-diffusivity form of the residual).
 """
 import math
 
@@ -113,8 +116,9 @@ class Instance:
     """One solve: grid, host arrays (node heights, diffusivities, initial
     state) and the C ABI settings."""
 
-    def __init__(self, name, grid, zlevels, ground, bc, physics, options, ustar, z0, direction):
+    def __init__(self, name, grid, zlevels, ground, bc, physics, options, ustar, z0, direction, z0map=None):
         self.name = name
+        self.z0map = z0map   # per-column roughness plane (gb_mesh_fields.z0), or None
         self.grid = grid
         self.zlevels = zlevels
         self.z = btf_heights(grid, zlevels, ground)
@@ -179,7 +183,7 @@ class Instance:
         return self.grid.cells
 
 
-def _faces_for(direction, periodic_y=True):
+def _faces_for(direction, periodic_y=True, ground=abi.FACE_NO_SLIP_WALL):
     """Inflow on the upwind x face (and y face when not periodic), outflow downwind."""
     c = math.cos(math.radians(direction))
     xlo, xhi = (abi.FACE_INFLOW, abi.FACE_OUTFLOW) if c >= 0 else (abi.FACE_OUTFLOW, abi.FACE_INFLOW)
@@ -188,14 +192,40 @@ def _faces_for(direction, periodic_y=True):
     else:
         s = math.sin(math.radians(direction))
         ylo, yhi = (abi.FACE_INFLOW, abi.FACE_OUTFLOW) if s >= 0 else (abi.FACE_OUTFLOW, abi.FACE_INFLOW)
-    return (xlo, ylo, abi.FACE_NO_SLIP_WALL, xhi, yhi, abi.FACE_SLIP_WALL)
+    return (xlo, ylo, ground, xhi, yhi, abi.FACE_SLIP_WALL)
 
 
-def config1(nx=128, ny=128, nz=64, precision=0, zline_sweeps=4):
+def _turbulence(turbulence, z0):
+    """(ground face type, surface options, physics keywords) of the physics
+    switch: the k-L closure and a neutral surface layer, or none."""
+    if not turbulence:
+        return abi.FACE_NO_SLIP_WALL, None, {}
+    return (abi.FACE_SURFACE_LAYER, {"z0": z0},
+            dict(closure=1, turb_Cmu0=CMU0, turb_kappa=KAPPA, turb_max_geom_lscale=LMAX))
+
+
+def lognormal_z0(grid, seed, median, sigma):
+    """A per-column roughness plane (gb_mesh_fields.z0's layout): z0 lognormal
+    with the median and the log-standard deviation given, on the domain
+    columns; the ghost columns the periodic image or the nearest column."""
+    rng = np.random.default_rng(seed)
+    cols = median * np.exp(sigma * rng.standard_normal((grid.ny, grid.nx)))
+    G = grid.ng
+    plane = np.zeros((grid.ny + 1 + 2 * G, grid.nx + 1 + 2 * G))
+    for j in range(-G, grid.ny + 1 + G):
+        for i in range(-G, grid.nx + 1 + G):
+            ii = (i % grid.nx) if grid.periodic_x else min(max(i, 0), grid.nx - 1)
+            jj = (j % grid.ny) if grid.periodic_y else min(max(j, 0), grid.ny - 1)
+            plane[j + G, i + G] = cols[jj, ii]
+    return plane.reshape(-1)
+
+
+def config1(nx=128, ny=128, nz=64, precision=0, zline_sweeps=4, turbulence=True):
     """Plain FP64 on the GPU over a single Gaussian hill h = 150 exp(-(r/300)^2)
     centred in a 128 x 128 x 64 grid, dx = dy = 25 m, the stretched layers to a
     1500 m lid; log-law inflow u* = 0.45 m/s, z0 = 0.03 m from 270 deg;
-    Coriolis f = 1e-4 1/s with the geostrophic wind at the lid; neutral."""
+    Coriolis f = 1e-4 1/s with the geostrophic wind at the lid; neutral; the
+    k-L closure and the surface layer (turbulence)."""
     dx = 25.0
     zl, _ = geometric_zlevels(nz)
     g = Grid(nx, ny, nz, dx, dx, 1500.0 / nz, False, True)
@@ -204,10 +234,11 @@ def config1(nx=128, ny=128, nz=64, precision=0, zline_sweeps=4):
     ustar, z0, direction = 0.45, 0.03, 270.0 - 270.0
     f = 1e-4
     ug = float(log_law(np.array([1500.0]), ustar, z0)[0])
-    bc = abi.BC.make(_faces_for(direction), theta_ref=((0.0, 1500.0), (300.0, 300.0)), ustar=ustar, z0=z0,
-                     direction=direction, kappa=KAPPA, Cmu0=CMU0, l_max=LMAX)
+    ground_face, surface, turb = _turbulence(turbulence, z0)
+    bc = abi.BC.make(_faces_for(direction, ground=ground_face), theta_ref=((0.0, 1500.0), (300.0, 300.0)), ustar=ustar,
+                     z0=z0, direction=direction, kappa=KAPPA, Cmu0=CMU0, l_max=LMAX, surface=surface)
     ph = abi.Physics.make(1500.0, gravity=9.81, coriolis=1, latitude=90.0, rotation_period=4 * math.pi / f,
-                          geostrophic=1, ug=ug, vg=0.0)
+                          geostrophic=1, ug=ug, vg=0.0, **turb)
     opts = abi.SimplecOptions.make(zline_sweeps=zline_sweeps, precision=precision)
     return Instance("config1-hill-128x128x64", g, zl, ground, bc, ph, opts, ustar, z0, direction)
 
@@ -217,7 +248,7 @@ def config1(nx=128, ny=128, nz=64, precision=0, zline_sweeps=4):
 MAX_TILE_SLOPE = 1.0
 
 
-def tile(n, nz, seed, rms=None, ustar=None, z0=None, met=None, dx=30.0, precision=1, zline_sweeps=4):
+def tile(n, nz, seed, rms=None, ustar=None, z0=None, met=None, dx=30.0, precision=1, zline_sweeps=4, turbulence=True):
     """One instance of the batched/served configurations: n x n x nz over
     seeded fractal terrain (|k|^-3, rms uniform 20-150 m unless given), a
     random wind direction, u* and z0 (seed-derived); inflow on the upwind x
@@ -233,20 +264,21 @@ def tile(n, nz, seed, rms=None, ustar=None, z0=None, met=None, dx=30.0, precisio
     g = Grid(n, n, nz, dx, dx, 1500.0 / nz, False, False)
     terrain = fractal_field(n + 1, seed, rms, dx=dx, max_slope=MAX_TILE_SLOPE)
     ground = node_ground(g, lambda x, y: float(terrain[int(round(y / dx)) % (n + 1), int(round(x / dx)) % (n + 1)]))
-    bc = abi.BC.make(_faces_for(direction, periodic_y=False), theta_ref=((0.0, 1500.0), (300.0, 300.0)),
-                     ustar=ustar, z0=z0, direction=direction, kappa=KAPPA, Cmu0=CMU0, l_max=LMAX)
-    ph = abi.Physics.make(1500.0, gravity=9.81)
+    ground_face, surface, turb = _turbulence(turbulence, z0)
+    bc = abi.BC.make(_faces_for(direction, periodic_y=False, ground=ground_face), theta_ref=((0.0, 1500.0), (300.0, 300.0)),
+                     ustar=ustar, z0=z0, direction=direction, kappa=KAPPA, Cmu0=CMU0, l_max=LMAX, surface=surface)
+    ph = abi.Physics.make(1500.0, gravity=9.81, **turb)
     opts = abi.SimplecOptions.make(zline_sweeps=zline_sweeps, precision=precision)
     return Instance(f"tile-{seed}-{n}x{n}x{nz}", g, zl, ground, bc, ph, opts, ustar, z0, direction)
 
 
-def config2(precision=1, zline_sweeps=4, n=256, nz=96, seed=2, max_slope=1.0):
+def config2(precision=1, zline_sweeps=4, n=256, nz=96, seed=2, max_slope=1.0, turbulence=True):
     """Mixed precision against plain FP64 on a 256 x 256 x 96 grid, dx = dy =
     30 m, over seeded fractal terrain (|k|^-3, 120 m rms, minimum 0, scaled
     down where steeper than max_slope); log-law inflow u* = 0.4 m/s from
-    225 deg (inflow on the x and y faces upwind). The configuration's
-    per-column lognormal z0 has no counterpart here (the ground is a no-slip
-    wall; z0 enters through the inflow log law): its median, 0.05 m, is used."""
+    225 deg (inflow on the x and y faces upwind); the ground's z0 per column
+    lognormal with median 0.05 m and sigma 0.7 (the surface layer's map; the
+    inflow log law takes the median); the k-L closure (turbulence)."""
     dx = 30.0
     met = 225.0
     direction = (270.0 - met) % 360.0
@@ -255,8 +287,10 @@ def config2(precision=1, zline_sweeps=4, n=256, nz=96, seed=2, max_slope=1.0):
     terrain = fractal_field(n + 1, seed, 120.0, dx=dx, max_slope=max_slope)
     ground = node_ground(g, lambda x, y: float(terrain[int(round(y / dx)) % (n + 1), int(round(x / dx)) % (n + 1)]))
     ustar, z0 = 0.4, 0.05
-    bc = abi.BC.make(_faces_for(direction, periodic_y=False), theta_ref=((0.0, 1500.0), (300.0, 300.0)),
-                     ustar=ustar, z0=z0, direction=direction, kappa=KAPPA, Cmu0=CMU0, l_max=LMAX)
-    ph = abi.Physics.make(1500.0, gravity=9.81)
+    ground_face, surface, turb = _turbulence(turbulence, z0)
+    bc = abi.BC.make(_faces_for(direction, periodic_y=False, ground=ground_face), theta_ref=((0.0, 1500.0), (300.0, 300.0)),
+                     ustar=ustar, z0=z0, direction=direction, kappa=KAPPA, Cmu0=CMU0, l_max=LMAX, surface=surface)
+    ph = abi.Physics.make(1500.0, gravity=9.81, **turb)
     opts = abi.SimplecOptions.make(zline_sweeps=zline_sweeps, precision=precision)
-    return Instance(f"config2-fractal-{n}x{n}x{nz}", g, zl, ground, bc, ph, opts, ustar, z0, direction)
+    z0map = lognormal_z0(g, 5000 + seed, z0, 0.7) if turbulence else None
+    return Instance(f"config2-fractal-{n}x{n}x{nz}", g, zl, ground, bc, ph, opts, ustar, z0, direction, z0map)

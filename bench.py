@@ -138,7 +138,8 @@ class SimplecWorkload:
         g = self.inst.grid
         self.name = (f"SIMPLEC outer iteration, config 1: Gaussian hill 150 m, {g.nx}x{g.ny}x{g.nz} cells, dx 25 m, "
                      f"{'plain FP64' if precision == 0 else 'FP32 inner solves in FP64 defect correction'}, "
-                     f"zline_sweeps {sweeps}, pressure_reltol 1e-3")
+                     f"zline_sweeps {sweeps}, pressure_reltol 1e-3"
+                     f"{', k-L closure and surface layer' if self.inst.physics.closure else ''}")
 
     @property
     def cells(self):
@@ -167,7 +168,7 @@ class SimplecWorkload:
         g = inst.grid
         z = torch.from_numpy(inst.z).cuda()
         J, ax, ay, az, _ = gb.mesh_metrics(ctx, g, z)
-        self.case = DeviceCase(g, z, J, ax, ay, az, inst.nu, inst.gamma_theta, inst.gamma_tke, inst.q)
+        self.case = DeviceCase(g, z, J, ax, ay, az, inst.nu, inst.gamma_theta, inst.gamma_tke, inst.q, inst.z0map)
         self.stage = SimplecStage(ctx, self.case, inst.bc, inst.physics, inst.options)
         self.stage.fill_ghosts()
         self.driver = Driver(self.stage)
@@ -211,15 +212,15 @@ class SimplecWorkload:
         inst = self.inst
         g = inst.grid
         J, ax, ay, az, _ = oracle.metrics(g, inst.z)
-        self.ocase = oracle.Case(g, inst.z, J, ax, ay, az, inst.nu, inst.gamma_theta, inst.gamma_tke)
+        self.ocase = oracle.Case(g, inst.z, J, ax, ay, az, inst.nu, inst.gamma_theta, inst.gamma_tke, inst.z0map)
         self.ocase.q = {f: a.copy() for f, a in inst.q.items()}
-        oracle.fill_ghosts(self.ocase, inst.bc)
+        oracle.fill_ghosts(self.ocase, inst.bc, inst.physics)
         self.ocfl = 1.0
 
     def cpu_step(self):
         import oracle
         inst = self.inst
-        dt = oracle.local_dtau(self.ocase, self.ocfl)
+        dt = oracle.local_dtau(self.ocase, self.ocfl, phys=inst.physics)
         rc, info, _ = oracle.simplec_iterate(self.ocase, inst.bc, inst.physics, inst.options, dt)
         return rc
 
@@ -233,6 +234,8 @@ def main():
     ap.add_argument("--precision", type=int, default=0, choices=[0, 1])
     ap.add_argument("--sweeps", type=int, default=4)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
+    ap.add_argument("--tune", action="append", default=[], metavar="KEY=VALUE",
+                    help="a context tuning knob (GB_TUNE_*, by number or name without the prefix), repeatable")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -255,6 +258,9 @@ def main():
     import ablsteadyrans_b200 as gb
     wl = SimplecWorkload(precision=args.precision, sweeps=args.sweeps)
     ctx = gb.Context()
+    for kv in args.tune:
+        key, val = kv.split("=")
+        ctx.tune(int(key) if key.isdigit() else getattr(gb, "TUNE_" + key.upper()), int(val))
     wl.setup(ctx)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")  # > L2 (126 MB)
 
@@ -349,10 +355,13 @@ def main():
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "f64" if args.precision == 0 else "f64 outer, f32 inner",
-        "data": "synthetic (config 1 generated in-project: Gaussian hill, log-law inflow; frozen mixing-length "
-                "diffusivities, no-slip ground)",
+        "data": ("synthetic (config 1 generated in-project: Gaussian hill, log-law inflow; k-L closure, neutral "
+                 "MOST surface layer)" if wl.inst.physics.closure else
+                 "synthetic (config 1 generated in-project: Gaussian hill, log-law inflow; frozen mixing-length "
+                 "diffusivities, no-slip ground)"),
         "config": {"workload": wl.name, "cells": wl.cells, "l2": "flushed between timed steps (256 MB write)",
-                   "parallelism": f"independent instances x{world}", "driver_status_last": statuses[-1]},
+                   "parallelism": f"independent instances x{world}", "driver_status_last": statuses[-1],
+                   **({"tune": args.tune} if args.tune else {})},
         "e2e": {"value": e2e_value, "unit": "cell-updates/s", "h2d_bytes_per_step": wl.h2d,
                 "d2h_bytes_per_step": wl.d2h},
         "gpu_launches": launches,

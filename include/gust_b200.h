@@ -105,6 +105,9 @@ enum {
                                    level has at most 64 columns), 1 the per-relaxation launches */
     GB_TUNE_LINE_DEPTH,         /* levels the factored z-line sweep keeps in flight: 0 default (4 FP64, 8 FP32),
                                    2 twice that */
+    GB_TUNE_LINE_BACK,          /* where the batched factored sweep keeps c' and e' for the back substitution:
+                                   0 auto (= 1), 1 shared memory, 2 the global arrays (c' stored, e' in the
+                                   output array): less shared memory per warp, more warps per SM */
     GB_N_TUNE
 };
 gb_status gb_ctx_tune(gb_ctx* ctx, int32_t key, int32_t value);
@@ -424,6 +427,16 @@ gb_status gb_simplec_residual(gb_simplec* s, const gb_state* q, double* const* R
 /* SimplecStage::iterate (Source/Simplec.cpp:452-506): one SIMPLEC outer
  * iteration of q with the local pseudo-time step dtau (cells). */
 gb_status gb_simplec_iterate(gb_simplec* s, const gb_state* q, const double* dtau, gb_iter_info* info);
+
+/* SimplecStage::closure_fields (Source/Simplec.H:216) and the wall model's
+ * state: the closure's fields at the last residual (nu, gamma_theta,
+ * gamma_tke, nu_t, L, Rt, P_s, P_b, eps, dS_k/dk: device volumes of the
+ * grid) and the surface state of the last ghost fill (u*, U, z_ref, d0,
+ * 1/L, the stress tau x, y, z, drag, k_w, |A|: device planes of one value
+ * per column, gb_mesh_fields.z0's layout), copied into the given arrays;
+ * null arrays (or entries) are skipped. GB_BAD_ARG when the stage has no
+ * closure (closure) or no surface_layer ground (surface). */
+gb_status gb_simplec_turbulence(gb_simplec* s, double* const* closure, double* const* surface);
 
 /* The defaults of init.* (Source/Initializer.H: z_agl_min 0, alpha_h = alpha_v
  * = 1, k_decay_height 0, projection 1, obrien 0) and solver.poisson_*. */

@@ -381,13 +381,17 @@ def height_above_ground(case):
     return d
 
 
-def local_dtau(case, cfl, use_nu=True, nu=None):
-    """local_dtau with nu (default: the case's diffusivity, or with the closure
-    the last iteration's nu, 0 before the first)."""
+def local_dtau(case, cfl, use_nu=True, nu=None, phys=None):
+    """local_dtau with nu: the given one, else with the closure (phys.closure)
+    the last iteration's nu (0 before the first, Simplec.cpp:328), else the
+    case's diffusivity."""
     dt = case.grid.np_zeros()
     q = case.q
     if nu is None and use_nu:
-        nu = case.closure_nu if case.closure_nu is not None else case.nu
+        if phys is not None and phys.closure:
+            nu = case.closure_nu if case.closure_nu is not None else case.grid.np_zeros()
+        else:
+            nu = case.nu
     _L().og_local_dtau(ctypes.byref(case.grid.c), _p(q["u"]), _p(q["v"]), _p(q["w"]), _p(case.z), _p(case.J),
                        _p(nu) if use_nu else None, float(cfl), _p(dt))
     return dt

@@ -192,3 +192,30 @@ def test_gpu_zline_lusgs_refusals(ctx):
         gb.zline_lusgs(ctx, g, 0, z, z[0], z[0], 0, z[1])
     with pytest.raises(gb.GustError, match="steady.line_alternate = 2"):
         gb.zline_lusgs(ctx, g, 0, z, z[0], z[0], 1, z[1], alternate=2)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", [0, 1])
+def test_gpu_batched_sweep_back_substitution_placement_is_bitwise_neutral(ctx, precision):
+    """The batched factored sweeps keep c' and e' for the back substitution in
+    shared memory (TUNE_LINE_BACK = 1) or in the global arrays (2): the same
+    arithmetic in the same order, so three SIMPLEC iterations (u, v, w and
+    theta, k swept in batched launches) give identical fields."""
+    import ablsteadyrans_b200 as gb
+    from ablsteadyrans_b200 import workloads
+    from ablsteadyrans_b200.simplec import DeviceCase, SimplecStage
+    out = []
+    for back in (1, 2):
+        inst = workloads.tile(40, 24, 3, precision=precision)
+        ctx.tune(gb.TUNE_LINE_BACK, back)
+        J, ax, ay, az, _ = oracle.metrics(inst.grid, inst.z)
+        dc = DeviceCase(inst.grid, inst.z, J, ax, ay, az, inst.nu, inst.gamma_theta, inst.gamma_tke, inst.q, inst.z0map)
+        st = SimplecStage(ctx, dc, inst.bc, inst.physics, inst.options)
+        st.fill_ghosts()
+        for _ in range(3):
+            st.iterate(st.local_dtau(2.0))
+        out.append({f: dc.host(f) for f in ("u", "v", "w", "p", "theta", "tke")})
+        st.close()
+    ctx.tune(gb.TUNE_LINE_BACK, 0)
+    for f in out[0]:
+        assert np.array_equal(out[0][f], out[1][f]), f

@@ -166,7 +166,7 @@ def test_oracle_stage_with_closure_and_wall_model():
     so = SimplecOptions.make()
     norms = []
     for _ in range(30):
-        dt = oracle.local_dtau(case, 2.0)
+        dt = oracle.local_dtau(case, 2.0, phys=ph)
         rc, info, R = oracle.simplec_iterate(case, bc, ph, so, dt)
         assert rc == 0
         norms.append(info.residual_norms[0])
@@ -196,3 +196,122 @@ def _hill_case(seed=1):
     case.q["theta"][...] = 300.0
     case.q["w"][...] = 0.0
     return case, bc, ph
+
+
+# ---------------------------------------------------------------- GPU ---
+
+FIELDS = ("u", "v", "w", "p", "theta", "tke")
+LOCS = (1, 2, 4, 0, 0, 0)
+
+
+def _stage(ctx, case, bc, ph, **opts):
+    from ablsteadyrans_b200.abi import SimplecOptions
+    from ablsteadyrans_b200.simplec import DeviceCase, SimplecStage
+    dc = DeviceCase.from_oracle(case)
+    return dc, SimplecStage(ctx, dc, bc, ph, SimplecOptions.make(**opts))
+
+
+def _cells(g, a):
+    G = g.ng
+    return a[G:G + g.nz, G:G + g.ny, G:G + g.nx]
+
+
+def _columns(g, a):
+    G = g.ng
+    return np.asarray(a).reshape(-1, int(g.c.sy))[G - 1:G + g.ny + 1, G - 1:G + g.nx + 1]
+
+
+@pytest.mark.gpu
+def test_gpu_closure_column_matches_reference_gold(ctx):
+    """The reference's Closure_Column regression on the B200: the closure,
+    the surface layer and the full residual give the gold plotfile's fields
+    at the reference's 1e-10 relative."""
+    case, bc, ph = closure_column_case()
+    dc, st = _stage(ctx, case, bc, ph)
+    st.fill_ghosts()
+    R = [r.cpu().numpy() for r in st.residual()]
+    cf, ss = st.turbulence()
+    q = {f: dc.host(f) for f in FIELDS}
+    got = closure_column_outputs(case.grid, q, R, cf, ss)
+    for f, ref in _gold().items():
+        scale = np.abs(ref).max()
+        err = np.abs(got[f] - ref).max()
+        assert err <= (1e-13 if scale == 0 else 1e-10 * scale), (f, err / max(scale, 1e-300))
+    st.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("heat", [0.0, 0.05])
+def test_gpu_wall_model_and_closure_match_oracle(ctx, heat):
+    """Over a hill with a per-column z0: the ghost fill (the wall law's
+    ground gradient), the surface state, the closure's fields and all six
+    residuals of the GPU equal the oracle's (1e-11 relative per field; the
+    MOST Newton and pow/log of the two libraries differ in the last bits)."""
+    from ablsteadyrans_b200.abi import SURFACE_HEAT_FLUX
+    case, bc, ph = _hill_case()
+    if heat:
+        bc.surface_stability, bc.surface_heat_flux = SURFACE_HEAT_FLUX, heat
+    dc, st = _stage(ctx, case, bc, ph)
+    ss_ref = oracle.fill_ghosts(case, bc, ph)
+    R_ref, cf_ref, _ = oracle.residual(case, bc, ph, fields=True)
+    st.fill_ghosts()
+    R = [r.cpu().numpy() for r in st.residual()]
+    cf, ss = st.turbulence()
+    g = case.grid
+    for f in FIELDS:
+        ref, got = case.q[f], dc.host(f)
+        assert np.abs(got - ref).max() <= 1e-11 * np.abs(ref).max(), f
+    for f in ("ustar", "speed", "d0", "inv_L", "tau_x", "tau_y", "drag", "kwall", "area"):
+        ref, got = _columns(g, ss_ref[f]), _columns(g, ss[f])
+        assert np.abs(got - ref).max() <= 1e-11 * max(np.abs(ref).max(), 1e-300), f
+    for f in ("nu", "gamma_theta", "gamma_tke", "nut", "length", "Ps", "Pb", "eps", "dSdk"):
+        ref, got = _cells(g, cf_ref[f]), _cells(g, cf[f])
+        assert np.abs(got - ref).max() <= 1e-11 * max(np.abs(ref).max(), 1e-300), f
+    for n, loc in enumerate(LOCS):
+        v = g.valid(loc)
+        ref, got = R_ref[n][v], R[n][v]
+        assert np.abs(got - ref).max() <= 1e-10 * max(np.abs(ref).max(), 1e-300), n
+    st.close()
+
+
+@pytest.mark.gpu
+def test_gpu_iterations_with_closure_and_wall_model_match_oracle(ctx):
+    """Five SIMPLEC iterations with the closure and the surface layer (the
+    local dtau from the last iteration's nu, 0 at first) agree with the
+    oracle's to 1e-9 relative per field."""
+    from ablsteadyrans_b200.abi import SimplecOptions
+    case, bc, ph = _hill_case()
+    opts = dict(pressure_reltol=1e-11, zline_sweeps=3)
+    dc, st = _stage(ctx, case, bc, ph, **opts)
+    so = SimplecOptions.make(**opts)
+    for it in range(5):
+        dt_ref = oracle.local_dtau(case, 2.0, phys=ph)
+        dt = st.local_dtau(2.0)
+        v0 = case.grid.valid(0)
+        assert np.abs(dt.cpu().numpy()[v0] - dt_ref[v0]).max() <= 1e-10 * dt_ref[v0].max(), it
+        rc, info_ref, _ = oracle.simplec_iterate(case, bc, ph, so, dt_ref)
+        assert rc == 0
+        info = st.iterate(dt)
+        for n in range(6):
+            assert info.residual_norms[n] == pytest.approx(info_ref.residual_norms[n], rel=1e-9, abs=1e-14), (it, n)
+        for f, loc in zip(FIELDS, LOCS):
+            v = case.grid.valid(loc)
+            ref, got = case.q[f][v], dc.host(f)[v]
+            assert np.abs(got - ref).max() <= 1e-9 * max(np.abs(ref).max(), 1e-300), (it, f)
+    st.close()
+
+
+@pytest.mark.gpu
+def test_gpu_turbulence_refusals(ctx):
+    import ablsteadyrans_b200 as gb
+    from ablsteadyrans_b200.abi import FACE_SURFACE_LAYER
+    case, bc, ph = _hill_case()
+    for mutate, msg in ((lambda b, p: setattr(b, "surface_z0", 0.0), "bc.surface_z0"),
+                        (lambda b, p: b.face.__setitem__(5, FACE_SURFACE_LAYER), "the ground's only"),
+                        (lambda b, p: setattr(b, "surface_heat_flux", 0.1), "stability is neutral"),
+                        (lambda b, p: setattr(p, "turb_Rt_min", -4.0), "turb.Rt_min"),
+                        (lambda b, p: setattr(p, "turb_Cb", 0.0), "turb.Cb")):
+        case, bc, ph = _hill_case()
+        mutate(bc, ph)
+        with pytest.raises(gb.GustError, match=msg):
+            _stage(ctx, case, bc, ph)
