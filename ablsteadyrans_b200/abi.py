@@ -41,16 +41,24 @@ class BC(ctypes.Structure):
                 ("theta_ref_z", ctypes.c_double * MAX_PROFILE), ("theta_ref_theta", ctypes.c_double * MAX_PROFILE),
                 ("surface_z0", ctypes.c_double), ("surface_zref", ctypes.c_double),
                 ("surface_stability", ctypes.c_int32), ("surface_heat_flux", ctypes.c_double),
-                ("surface_wall_k", ctypes.c_int32), ("surface_denominator_floor", ctypes.c_int32)]
+                ("surface_wall_k", ctypes.c_int32), ("surface_denominator_floor", ctypes.c_int32),
+                ("rayleigh_zdamp", ctypes.c_double), ("rayleigh_dampcoef", ctypes.c_double),
+                ("rayleigh_fields", ctypes.c_int32), ("rayleigh_above_ground", ctypes.c_int32),
+                ("sponge_width", ctypes.c_double), ("sponge_strength", ctypes.c_double)]
 
     @classmethod
     def make(cls, faces, theta_ref=((0.0,), (300.0,)), ustar=0.4, z0=0.1, direction=0.0, kappa=0.41, Cmu0=0.5562,
-             l_max=30.0, zhi_theta_grad=0.0, wall_velocity=None, surface=None):
+             l_max=30.0, zhi_theta_grad=0.0, wall_velocity=None, surface=None, damping=None):
         """surface: bc.surface_* of a surface_layer ground as a dict (z0, zref,
         stability, heat_flux, wall_k, denominator_floor); the reference's
         defaults (Source/SurfaceLayer.H: z0 0.1 m, first cell centre, neutral,
-        Dirichlet wall k, log-law floor) otherwise."""
+        Dirichlet wall k, log-law floor) otherwise. damping: bc.rayleigh_* and
+        bc.sponge_* as a dict (zdamp, dampcoef, fields, above_ground, width,
+        strength); off otherwise."""
         b = cls()
+        b.rayleigh_fields = 31
+        for k, v in (damping or {}).items():
+            setattr(b, ("sponge_" if k in ("width", "strength") else "rayleigh_") + k, v)
         b.surface_z0, b.surface_zref, b.surface_stability = 0.1, 0.0, SURFACE_NEUTRAL
         b.surface_heat_flux, b.surface_wall_k, b.surface_denominator_floor = 0.0, WALL_K_DIRICHLET, DENOMINATOR_LOG_LAW
         for k, v in (surface or {}).items():

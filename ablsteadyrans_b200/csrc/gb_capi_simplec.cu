@@ -149,9 +149,55 @@ gb_status check_bc(const gb_grid& g, const gb_bc& bc)
             return GB_BAD_ARG;
         }
     }
+    {
+        // the damping checks (BoundaryConditions.cpp:330-357)
+        auto bad = [](double x) { return std::isnan(x) || !std::isfinite(x); };
+        bool lateral = false;
+        for (int f : {0, 1, 3, 4}) { lateral = lateral || bc.face[f] == GB_FACE_INFLOW || bc.face[f] == GB_FACE_OUTFLOW; }
+        if (bad(bc.rayleigh_zdamp) || !(bc.rayleigh_zdamp >= 0)) {
+            gb::set_error("gust: invalid inputs:\n  bc.rayleigh_zdamp = %g: must be in [0, the top level) (0: off)",
+                          bc.rayleigh_zdamp);
+            return GB_BAD_ARG;
+        }
+        if (bad(bc.rayleigh_dampcoef) || !(bc.rayleigh_dampcoef >= 0)) {
+            gb::set_error("gust: invalid inputs:\n  bc.rayleigh_dampcoef = %g: must be finite and >= 0 (1/s)",
+                          bc.rayleigh_dampcoef);
+            return GB_BAD_ARG;
+        }
+        if (bc.rayleigh_zdamp > 0 && !(bc.rayleigh_dampcoef > 0)) {
+            gb::set_error("gust: invalid inputs:\n  bc.rayleigh_zdamp > 0 needs bc.rayleigh_dampcoef > 0");
+            return GB_BAD_ARG;
+        }
+        if (bc.rayleigh_fields < 0 || bc.rayleigh_fields > 31 || bc.rayleigh_above_ground < 0
+            || bc.rayleigh_above_ground > 1) {
+            gb::set_error("gust: invalid inputs:\n  bc.rayleigh_fields must be among u, v, w, theta, tke and "
+                          "bc.rayleigh_height absolute or above_ground");
+            return GB_BAD_ARG;
+        }
+        if (bad(bc.sponge_width) || !(bc.sponge_width >= 0)) {
+            gb::set_error("gust: invalid inputs:\n  bc.sponge_width = %g: must be finite and >= 0 (0: off)",
+                          bc.sponge_width);
+            return GB_BAD_ARG;
+        }
+        if (bc.sponge_width > 0 && !lateral) {
+            gb::set_error("gust: invalid inputs:\n  bc.sponge_width > 0 needs an inflow or outflow face to damp towards");
+            return GB_BAD_ARG;
+        }
+        if (bad(bc.sponge_strength) || !(bc.sponge_strength >= 0)) {
+            gb::set_error("gust: invalid inputs:\n  bc.sponge_strength = %g: must be finite and >= 0 (1/s)",
+                          bc.sponge_strength);
+            return GB_BAD_ARG;
+        }
+        if (bc.sponge_width > 0 && !(bc.sponge_strength > 0)) {
+            gb::set_error("gust: invalid inputs:\n  bc.sponge_width > 0 needs bc.sponge_strength > 0");
+            return GB_BAD_ARG;
+        }
+    }
     bool inflow = false;
     for (int f = 0; f < 6; ++f) { inflow = inflow || bc.face[f] == GB_FACE_INFLOW; }
-    if (inflow && !(bc.inflow_ustar > 0 && bc.inflow_z0 > 0 && bc.kappa > 0 && bc.Cmu0 > 0)) {
+    // the profile serves the inflow faces and the damping's reference (needs_profile, BoundaryConditions.cpp:287)
+    const bool damping = bc.rayleigh_zdamp > 0 || bc.sponge_width > 0;
+    if ((inflow || damping) && !(bc.inflow_ustar > 0 && bc.inflow_z0 > 0 && bc.kappa > 0 && bc.Cmu0 > 0)) {
         gb::set_error("gust: invalid inputs:\n  bc.inflow_ustar and bc.inflow_z0 must be > 0 (log law)");
         return GB_BAD_ARG;
     }

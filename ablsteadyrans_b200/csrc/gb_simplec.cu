@@ -930,6 +930,118 @@ void fill_theta_ref(gb_simplec* S)
     }, GB_KERNEL_RESIDUAL);
 }
 
+// ------------------------------------------------------------- damping ---
+
+//! The Rayleigh layer and the sponge (DampingCoef, BoundaryConditions.cpp:945-1008).
+struct Damping {
+    double zd, rc, sw, ss, inv_w, lx, ly;
+    int fields, above;
+    int lateral[4];   // xlo, xhi, ylo, yhi hold an inflow or outflow
+    bool on;
+};
+
+Damping damping_of(const gb_simplec* S)
+{
+    const gb_bc& bc = S->bc;
+    Damping d{};
+    d.zd = bc.rayleigh_zdamp;
+    d.rc = bc.rayleigh_dampcoef;
+    d.sw = bc.sponge_width;
+    d.ss = bc.sponge_strength;
+    d.inv_w = d.sw > 0 ? 1 / d.sw : 0.0;
+    d.lx = S->g.nx * S->g.dx;
+    d.ly = S->g.ny * S->g.dy;
+    d.fields = bc.rayleigh_fields;
+    d.above = bc.rayleigh_above_ground;
+    const int faces[4] = {0, 3, 1, 4};
+    for (int n = 0; n < 4; ++n) {
+        const int t = bc.face[faces[n]];
+        d.lateral[n] = (t == GB_FACE_INFLOW || t == GB_FACE_OUTFLOW) ? 1 : 0;
+    }
+    d.on = d.zd > 0 || d.sw > 0;
+    return d;
+}
+
+//! The Rayleigh (cr) and sponge (cs) coefficients of point (i, j, k) of
+//! type t for field n (0 u .. 4 k), its heights above the ground (h) and
+//! absolute (zc); z_top is the top node height.
+__device__ __forceinline__ void damping_at(const Damping& d, const double* z, const gb_grid& g, int n, int t, int i,
+                                           int j, int k, double& cr, double& cs, double& h, double& zc)
+{
+    h = height_above_ground(z, g, t, i, j, k);
+    zc = point_z(z, g, t, i, j, k);
+    const double ztop = z[at(g, 0, 0, g.nz)];
+    const double x = (i + (nodal(t, 0) ? 0 : 0.5)) * g.dx;
+    const double y = (j + (nodal(t, 1) ? 0 : 0.5)) * g.dy;
+    const double zr = d.above ? h : zc;
+    cr = 0;
+    if (((d.fields >> n) & 1) && d.zd > 0 && zr > d.zd) {
+        const double pi = 3.14159265358979323846;
+        const double sn = sin(0.5 * pi * (zr - d.zd) / (ztop - d.zd));
+        cr = d.rc * sn * sn;
+    }
+    cs = 0;
+    if (d.sw > 0) {
+        const double dist[4] = {x - 0.0, d.lx - x, y - 0.0, d.ly - y};
+        for (int m = 0; m < 4; ++m) {
+            if (d.lateral[m] && dist[m] < d.sw) {
+                const double r = 1 - dist[m] * d.inv_w;
+                cs += d.ss * r * r;
+            }
+        }
+    }
+}
+
+//! BoundaryConditions::add_damping (BoundaryConditions.cpp:1022-1071):
+//! R += c (q - q_ref) on the valid points of u, v, w, theta, k.
+void add_damping(gb_simplec* S, const gb_state& q, double** R)
+{
+    const Damping d = damping_of(S);
+    if (!d.on) { return; }
+    const gb_grid g = S->g;
+    const Profile prof = S->prof;
+    const double* z = S->z;
+    const double* qf[5] = {q.u, q.v, q.w, q.theta, q.tke};
+    double* rf[5] = {R[0], R[1], R[2], R[4], R[5]};
+    const int ff[5] = {F_U, F_V, F_W, F_THETA, F_TKE};
+    for (int n = 0; n < 5; ++n) {
+        const int f = ff[n];
+        const int t = (n < 3) ? (1 << n) : CC;
+        const double* a = qf[n];
+        double* r = rf[n];
+        for_box(S->ctx, valid_box(g, t), [=] __device__(int i, int j, int k) {
+            double cr, cs, h, zc;
+            damping_at(d, z, g, n, t, i, j, k, cr, cs, h, zc);
+            const int64_t o = at(g, i, j, k);
+            if (cr > 0) {
+                const double zr = d.above ? h : zc;
+                const double ref = (f == F_W) ? 0.0 : prof.value(f, (f == F_THETA) ? zr : h);
+                r[o] += cr * (a[o] - ref);
+            }
+            if (cs > 0) {
+                const double ref = (f == F_W) ? 0.0 : prof.value(f, h);
+                r[o] += cs * (a[o] - ref);
+            }
+        }, GB_KERNEL_RESIDUAL);
+    }
+}
+
+//! add_damping_to_implicit (BoundaryConditions.cpp:1073-1099): a_P += c.
+void add_damping_to_implicit(gb_simplec* S, int f, int t, double* A)
+{
+    const Damping d = damping_of(S);
+    if (!d.on) { return; }
+    const gb_grid g = S->g;
+    const double* z = S->z;
+    const int64_t cs_ = volume(g);
+    const int n = (f == F_THETA) ? 3 : (f == F_TKE) ? 4 : f;
+    for_box(S->ctx, valid_box(g, t), [=] __device__(int i, int j, int k) {
+        double cr, cs, h, zc;
+        damping_at(d, z, g, n, t, i, j, k, cr, cs, h, zc);
+        A[GB_COEF_P * cs_ + at(g, i, j, k)] += cr + cs;
+    }, GB_KERNEL_COEFS);
+}
+
 //! apply_rows (BoundaryConditions.cpp:801-852).
 void apply_rows(gb_simplec* S, const gb_state& q, double** R)
 {
@@ -997,6 +1109,7 @@ void simplec_residual(gb_simplec* S, const gb_state& q, double** R)
     scalar_diffusion_subtract(S, q.tke, S->dfe.gamma_tke, R[5], 3);
     if (S->ph.closure) { turb_k_sources(ctx, g, S->cf, R[5]); }
     if (S->wall) { turb_apply_wall_k(ctx, g, S->bc, S->ssr, q.tke, R[5]); }
+    add_damping(S, q, R);
     apply_rows(S, q, R);
     seam_sync<double>(ctx, g, XF, R[0]);
     seam_sync<double>(ctx, g, YF, R[1]);
@@ -1064,9 +1177,11 @@ void implicit_coefficients(gb_simplec* S, double* const* F, const double* gm, do
     }, GB_KERNEL_COEFS);
 }
 
-//! apply_to_implicit (BoundaryConditions.cpp:885-941) without damping.
+//! apply_to_implicit (BoundaryConditions.cpp:885-941): the damping first,
+//! then the folds (a Dirichlet face point's row becomes the identity).
 void apply_to_implicit(gb_simplec* S, int f, int t, double* A)
 {
+    add_damping_to_implicit(S, f, t, A);
     const gb_grid g = S->g;
     const int64_t cs = volume(g);
     for (int d = 0; d < 3; ++d) {

@@ -307,6 +307,17 @@ typedef struct gb_bc {
     double surface_heat_flux;        /* bc.surface_heat_flux (K m/s, upward > 0; heat_flux only) */
     int32_t surface_wall_k;          /* GB_WALL_K_DIRICHLET or GB_WALL_K_SOURCE */
     int32_t surface_denominator_floor;  /* GB_DENOMINATOR_LOG_LAW or GB_DENOMINATOR_ONE */
+    /* Damping (BoundaryConditions.H:57-64, off by default): the Rayleigh layer
+     * R += c(z) (q - q_ref) above z_damp, c = coef sin^2(pi/2 (z - z_damp) /
+     * (z_top - z_damp)); the sponge R += c(s) (q - q_ref) within sponge_width
+     * of an inflow or outflow face, c = strength (1 - s/width)^2; q_ref the
+     * inflow profile (w: 0), c on the implicit diagonal. */
+    double rayleigh_zdamp;           /* bc.rayleigh_zdamp (m; 0: off) */
+    double rayleigh_dampcoef;        /* bc.rayleigh_dampcoef (1/s) */
+    int32_t rayleigh_fields;         /* bc.rayleigh_fields: bit 0 u, 1 v, 2 w, 3 theta, 4 k */
+    int32_t rayleigh_above_ground;   /* bc.rayleigh_height: 0 absolute, 1 above_ground */
+    double sponge_width;             /* bc.sponge_width (m; 0: off) */
+    double sponge_strength;          /* bc.sponge_strength (1/s) */
 } gb_bc;
 
 /* The residual's physics inputs (gust::ResidualInputs, Source/Residual.H:61-128;

@@ -375,6 +375,19 @@ def surface_state(case, bc, phys):
     return dict(zip(SURFACE_FIELDS, ss)), int(bad)
 
 
+def implicit_rows(case, bc, phys, eq):
+    """implicit_rows (Residual.cpp:272-304) of equation eq (0 u .. 5 k) with the
+    case's transport fluxes and given diffusivities: A (N_COEFS x grid)."""
+    g = case.grid
+    q = case.q
+    F = transport_fluxes(g, q["u"], q["v"], q["w"], case.z, case.ax, case.ay)
+    A = g.np_zeros(7)
+    d = case.diffusivities()
+    _L().og_implicit_rows(ctypes.byref(g.c), ctypes.byref(bc), ctypes.byref(phys), int(eq), *[_p(f) for f in F],
+                          _p(case.z), _p(case.J), ctypes.byref(d), _p(A))
+    return A
+
+
 def height_above_ground(case):
     d = case.grid.np_zeros()
     _L().og_height_above_ground(ctypes.byref(case.grid.c), _p(case.z), _p(d))

@@ -432,6 +432,107 @@ static void apply_rows(const og_grid* g, const gb_bc* bc, const double* u, const
     }
 }
 
+/* ------------------------------------------------------------------ */
+/* damping (BoundaryConditions.cpp:945-1099)                            */
+/* ------------------------------------------------------------------ */
+
+static int damping_on(const gb_bc* bc) { return bc->rayleigh_zdamp > 0 || bc->sponge_width > 0; }
+
+/* DampingCoef::rayleigh_part with z_top the top node height. */
+static double rayleigh_part(const gb_bc* bc, double ztop, double z)
+{
+    const double pi = 3.14159265358979323846;
+    if (bc->rayleigh_zdamp > 0 && z > bc->rayleigh_zdamp) {
+        const double s = sin(0.5 * pi * (z - bc->rayleigh_zdamp) / (ztop - bc->rayleigh_zdamp));
+        return bc->rayleigh_dampcoef * s * s;
+    }
+    return 0;
+}
+
+/* DampingCoef::sponge_part: the distances to the inflow and outflow faces
+ * (the domain from 0 to nx dx, 0 to ny dy). */
+static double sponge_part(const og_grid* g, const gb_bc* bc, double x, double y)
+{
+    double c = 0;
+    if (bc->sponge_width > 0) {
+        const double inv_w = 1 / bc->sponge_width;
+        const double dist[4] = {x - 0.0, g->nx * g->dx - x, y - 0.0, g->ny * g->dy - y};
+        const int faces[4] = {0, 3, 1, 4};
+        for (int n = 0; n < 4; ++n) {
+            const int t = bc->face[faces[n]];
+            if ((t == GB_FACE_INFLOW || t == GB_FACE_OUTFLOW) && dist[n] < bc->sponge_width) {
+                const double r = 1 - dist[n] * inv_w;
+                c += bc->sponge_strength * r * r;
+            }
+        }
+    }
+    return c;
+}
+
+/* The Rayleigh and sponge coefficients of point (i, j, k) of type t, and
+ * its heights above the ground (h) and absolute (zc). */
+static void damping_at(const og_grid* g, const gb_bc* bc, const double* z, int f, int t, int i, int j, int k,
+                       double* cr, double* cs, double* h, double* zc)
+{
+    *h = height_above_ground(g, z, t, i, j, k);
+    *zc = point_z(g, z, t, i, j, k);
+    const double ztop = z[IX(g, 0, 0, g->nz)];
+    const double x = (i + (nodal(t, 0) ? 0 : 0.5)) * g->dx;
+    const double y = (j + (nodal(t, 1) ? 0 : 0.5)) * g->dy;
+    const double zr = bc->rayleigh_above_ground ? *h : *zc;
+    const int field = (f == F_THETA) ? 3 : (f == F_TKE) ? 4 : f;
+    *cr = ((bc->rayleigh_fields >> field) & 1) ? rayleigh_part(bc, ztop, zr) : 0.0;
+    *cs = sponge_part(g, bc, x, y);
+}
+
+/* BoundaryConditions::add_damping (:1022-1071): R += c (q - q_ref) on the
+ * valid points of u, v, w, theta, k. */
+static void add_damping(const og_grid* g, const gb_bc* bc, const gb_state* q, double** R)
+{
+    if (!damping_on(bc)) { return; }
+    const double* qf[5] = {q->u, q->v, q->w, q->theta, q->tke};
+    double* rf[5] = {R[0], R[1], R[2], R[4], R[5]};
+    const int ff[5] = {F_U, F_V, F_W, F_THETA, F_TKE};
+    for (int n = 0; n < 5; ++n) {
+        const int f = ff[n];
+        const int t = (n < 3) ? (1 << n) : CC;
+        for (int k = 0; k < ext(g, t, 2); ++k) {
+            for (int j = 0; j < ext(g, t, 1); ++j) {
+                for (int i = 0; i < ext(g, t, 0); ++i) {
+                    double cr, cs, h, zc;
+                    damping_at(g, bc, q->z_nd, f, t, i, j, k, &cr, &cs, &h, &zc);
+                    const int64_t o = IX(g, i, j, k);
+                    if (cr > 0) {
+                        const double zr = bc->rayleigh_above_ground ? h : zc;
+                        const double ref = (f == F_W) ? 0.0 : profile_value(bc, f, (f == F_THETA) ? zr : h);
+                        rf[n][o] += cr * (qf[n][o] - ref);
+                    }
+                    if (cs > 0) {
+                        const double ref = (f == F_W) ? 0.0 : profile_value(bc, f, h);
+                        rf[n][o] += cs * (qf[n][o] - ref);
+                    }
+                }
+            }
+        }
+    }
+}
+
+/* add_damping_to_implicit (:1073-1099): a_P += the Rayleigh and sponge parts. */
+static void add_damping_to_implicit(const og_grid* g, const gb_bc* bc, const double* z, int f, int t, double* A)
+{
+    if (!damping_on(bc)) { return; }
+    const int64_t cs = VOL(g);
+    for (int k = 0; k < ext(g, t, 2); ++k) {
+        for (int j = 0; j < ext(g, t, 1); ++j) {
+            for (int i = 0; i < ext(g, t, 0); ++i) {
+                double cr, csp, h, zc;
+                damping_at(g, bc, z, f, t, i, j, k, &cr, &csp, &h, &zc);
+                A[COEF_P * cs + IX(g, i, j, k)] += cr + csp;
+            }
+        }
+    }
+}
+
 /* dirichlet_rows (BoundaryConditions.cpp:854-883). */
 static void dirichlet_rows(const og_grid* g, const gb_bc* bc, int f, int t, double* mask)
 {
@@ -455,9 +556,11 @@ static void dirichlet_rows(const og_grid* g, const gb_bc* bc, int f, int t, doub
     }
 }
 
-/* apply_to_implicit (BoundaryConditions.cpp:885-941) without damping. */
-static void apply_to_implicit(const og_grid* g, const gb_bc* bc, int f, int t, double* A)
+/* apply_to_implicit (BoundaryConditions.cpp:885-941): the damping first,
+ * then the folds (a Dirichlet face point's row becomes the identity). */
+static void apply_to_implicit(const og_grid* g, const gb_bc* bc, const double* z, int f, int t, double* A)
 {
+    add_damping_to_implicit(g, bc, z, f, t, A);
     const int64_t cs = VOL(g);
     for (int d = 0; d < 3; ++d) {
         if (is_per(g, d)) { continue; }
@@ -680,6 +783,7 @@ static void residual_t(const og_grid* g, const gb_bc* bc, const gb_physics* ph, 
         }
     }
     if (wall) { og_apply_wall_k(g, bc, (const double* const*)t->ss, q->tke, R[5]); }
+    add_damping(g, bc, q, R);
     apply_rows(g, bc, q->u, q->v, q->w, q->z_nd, R[0], R[1], R[2]);
     og_override_sync(g, XF, R[0]);
     og_override_sync(g, YF, R[1]);
@@ -750,7 +854,7 @@ static void implicit_rows_t(const og_grid* g, const gb_bc* bc, const gb_physics*
         og_apply_wall_to_implicit(g, (const double* const*)tc->ss, t, J, A);
         if (eq == F_TKE) { og_apply_wall_k_to_implicit(g, bc, (const double* const*)tc->ss, A); }
     }
-    apply_to_implicit(g, bc, eq, t, A);
+    apply_to_implicit(g, bc, z, eq, t, A);
 }
 
 void og_implicit_rows(const og_grid* g, const gb_bc* bc, const gb_physics* ph, int eq, const double* F0,

@@ -315,3 +315,101 @@ def test_gpu_turbulence_refusals(ctx):
         mutate(bc, ph)
         with pytest.raises(gb.GustError, match=msg):
             _stage(ctx, case, bc, ph)
+
+
+# ------------------------------------------------------------ damping ---
+
+def _profile_u(h, ustar=0.35, z0=0.1):
+    return ustar / KAPPA * np.log((np.maximum(h, 0.0) + z0) / z0)
+
+
+def test_oracle_rayleigh_layer_closed_form():
+    """The Rayleigh layer (BoundaryConditions::add_damping): R_u gains
+    c(z) (u - u_profile(h)) with c = coef sin^2(pi/2 (z - z_d)/(z_top - z_d))
+    above z_d, R_w gains c w; the u rows' diagonal gains c; nothing below
+    z_d. A field excluded from bc.rayleigh_fields is left alone."""
+    case, bc, ph = closure_column_case()
+    g = case.grid
+    G = g.ng
+    case.q["w"][G + 1:G + g.nz, G:G + g.ny, G:G + g.nx] = 0.01
+    oracle.fill_ghosts(case, bc, ph)
+    R0 = oracle.residual(case, bc, ph)
+    A0 = oracle.implicit_rows(case, bc, ph, 0)
+    bc.rayleigh_zdamp, bc.rayleigh_dampcoef, bc.rayleigh_fields = 500.0, 0.2, 0b00011   # u and v only
+    R1 = oracle.residual(case, bc, ph)
+    A1 = oracle.implicit_rows(case, bc, ph, 0)
+    zc = (np.arange(g.nz) + 0.5) * g.dzeta
+    c = np.where(zc > 500.0, 0.2 * np.sin(0.5 * np.pi * (zc - 500.0) / (1000.0 - 500.0)) ** 2, 0.0)
+    u = case.q["u"][G:G + g.nz, G:G + g.ny, G:G + g.nx + 1]
+    want = c[:, None, None] * (u - _profile_u(zc)[:, None, None])
+    got = (R1[0] - R0[0])[G:G + g.nz, G:G + g.ny, G:G + g.nx + 1]
+    assert np.abs(got - want).max() <= 1e-13 * np.abs(want).max()
+    dA = (A1[0] - A0[0])[G:G + g.nz, G:G + g.ny, G:G + g.nx + 1]
+    assert np.abs(dA - c[:, None, None]).max() <= 1e-15
+    assert np.array_equal(R1[2], R0[2])   # w not in bc.rayleigh_fields
+    bc.rayleigh_fields = 0b00100           # w alone: towards 0
+    R2 = oracle.residual(case, bc, ph)
+    zf = np.arange(g.nz + 1) * g.dzeta
+    cw = np.where(zf > 500.0, 0.2 * np.sin(0.5 * np.pi * (zf - 500.0) / 500.0) ** 2, 0.0)
+    w = case.q["w"][G:G + g.nz + 1, G:G + g.ny, G:G + g.nx]
+    dRw = (R2[2] - R0[2])[G + 1:G + g.nz, G:G + g.ny, G:G + g.nx]   # the top and ground rows are boundary rows
+    assert np.abs(dRw - (cw[:, None, None] * w)[1:g.nz]).max() <= 1e-15
+
+
+def test_oracle_sponge_closed_form():
+    """The lateral sponge: within sponge_width of an inflow or outflow face,
+    R_k gains strength (1 - s/width)^2 (k - k_profile(h)); beyond it, and
+    along the periodic y faces, nothing."""
+    case, bc, ph = _hill_case()
+    g = case.grid
+    G = g.ng
+    oracle.fill_ghosts(case, bc, ph)
+    R0 = oracle.residual(case, bc, ph)
+    bc.sponge_width, bc.sponge_strength = 100.0, 0.05
+    R1 = oracle.residual(case, bc, ph)
+    dk = (R1[5] - R0[5])[G:G + g.nz, G:G + g.ny, G:G + g.nx]
+    x = (np.arange(g.nx) + 0.5) * g.dx
+    s = np.minimum(x, g.nx * g.dx - x)
+    cs = np.where(s < 100.0, 0.05 * (1 - s / 100.0) ** 2, 0.0)
+    assert np.all(dk[:, :, cs == 0] == 0)
+    inside = np.nonzero(cs > 0)[0]
+    assert inside.size >= 2
+    # k_ref: the inflow profile's k at the cell's height above the ground,
+    # (u* c)^2 / Cmu0^2 with c = 1 / (1 + kappa (h + z0) / l_max)
+    h = oracle.height_above_ground(case)[G:G + g.nz, G:G + g.ny, G:G + g.nx]
+    ul = 0.4 / (1.0 + KAPPA * (h + 0.1) / 30.0)
+    kref = ul * ul / CMU0 ** 2
+    k = case.q["tke"][G:G + g.nz, G:G + g.ny, G:G + g.nx]
+    want = cs[None, None, :] * (k - kref)
+    assert np.abs(dk - want).max() <= 1e-12 * np.abs(want).max()
+
+
+@pytest.mark.gpu
+def test_gpu_damping_matches_oracle(ctx):
+    """The Rayleigh layer and the sponge on the GPU: the residual and five
+    SIMPLEC iterations (with the closure and the surface layer) equal the
+    oracle's."""
+    from ablsteadyrans_b200.abi import SimplecOptions
+    case, bc, ph = _hill_case()
+    bc.rayleigh_zdamp, bc.rayleigh_dampcoef, bc.rayleigh_fields = 400.0, 0.1, 31
+    bc.sponge_width, bc.sponge_strength = 120.0, 0.05
+    opts = dict(pressure_reltol=1e-11, zline_sweeps=3)
+    dc, st = _stage(ctx, case, bc, ph, **opts)
+    oracle.fill_ghosts(case, bc, ph)
+    R_ref = oracle.residual(case, bc, ph)
+    st.fill_ghosts()
+    R = [r.cpu().numpy() for r in st.residual()]
+    for n, loc in enumerate(LOCS):
+        v = case.grid.valid(loc)
+        assert np.abs(R[n][v] - R_ref[n][v]).max() <= 1e-10 * max(np.abs(R_ref[n][v]).max(), 1e-300), n
+    so = SimplecOptions.make(**opts)
+    for it in range(5):
+        dt_ref = oracle.local_dtau(case, 2.0, phys=ph)
+        rc, info_ref, _ = oracle.simplec_iterate(case, bc, ph, so, dt_ref)
+        assert rc == 0
+        st.iterate(st.local_dtau(2.0))
+        for f, loc in zip(FIELDS, LOCS):
+            v = case.grid.valid(loc)
+            ref, got = case.q[f][v], dc.host(f)[v]
+            assert np.abs(got - ref).max() <= 1e-9 * max(np.abs(ref).max(), 1e-300), (it, f)
+    st.close()
