@@ -96,7 +96,16 @@ class Context:
             stream = torch.cuda.current_stream()
         self.stream = stream
         self._h = ctypes.c_void_p()
+        self._owned = []
         check(lib().gb_ctx_create(ctypes.c_void_p(stream.cuda_stream), ctypes.byref(self._h)))
+
+    def own(self, obj):
+        """Record a native object made on this context (a solver, stage or
+        driver): close() destroys the live ones first, newest first, since
+        their destructors synchronise on the context's stream."""
+        import weakref
+        self._owned = [r for r in self._owned if r() is not None]
+        self._owned.append(weakref.ref(obj))
 
     @property
     def handle(self):
@@ -127,6 +136,11 @@ class Context:
 
     def close(self):
         if self._h:
+            for r in reversed(self._owned):
+                obj = r()
+                if obj is not None:
+                    obj.close()
+            self._owned = []
             check(lib().gb_ctx_destroy(self._h))
             self._h = ctypes.c_void_p()
 
@@ -265,6 +279,7 @@ class PoissonSolver:
         bcs = (ctypes.c_int32 * 6)(*[int(b) for b in bc])
         check(_lib_full().gb_poisson_create(ctx.handle, ctypes.byref(grid.c), bcs, _ptr(z_nd), _ptr(detJ),
                                             ctypes.byref(self.options), ctypes.byref(self._h)))
+        ctx.own(self)
 
     def set_coeffs(self, ax, ay, az, bx=None, by=None, bz=None):
         self._coeffs = (ax, ay, az, bx, by, bz)

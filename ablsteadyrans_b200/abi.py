@@ -162,6 +162,11 @@ class InitResult(ctypes.Structure):
                 ("obrien_top_residual", ctypes.c_double)]
 
 
+class ProlongResult(ctypes.Structure):
+    _fields_ = [("divergence_before", ctypes.c_double), ("divergence_after", ctypes.c_double),
+                ("poisson_iterations", ctypes.c_int32), ("tke_clipped", ctypes.c_int64)]
+
+
 class State(ctypes.Structure):
     _fields_ = [("u", ctypes.c_void_p), ("v", ctypes.c_void_p), ("w", ctypes.c_void_p), ("p", ctypes.c_void_p),
                 ("theta", ctypes.c_void_p), ("tke", ctypes.c_void_p), ("z_nd", ctypes.c_void_p)]
@@ -183,12 +188,40 @@ class IterInfo(ctypes.Structure):
                 ("last_sweep_dw", ctypes.c_double), ("divergence_before", ctypes.c_double),
                 ("divergence_after", ctypes.c_double), ("max_dp", ctypes.c_double),
                 ("poisson_removed_mean", ctypes.c_double), ("poisson_iterations", ctypes.c_int32),
-                ("max_dtheta", ctypes.c_double), ("max_dtke", ctypes.c_double), ("tke_clipped", ctypes.c_int64)]
+                ("max_dtheta", ctypes.c_double), ("max_dtke", ctypes.c_double), ("tke_clipped", ctypes.c_int64),
+                ("mean_ustar", ctypes.c_double)]
 
     def as_dict(self):
         d = {f: getattr(self, f) for f, _ in self._fields_ if f != "residual_norms"}
         d["residual_norms"] = list(self.residual_norms)
         return d
+
+
+CRITERION_MAX_RESIDUALS, CRITERION_MAX_MONITORS = 8, 4
+NOT_STEADY, STEADY, DIVERGED = 0, 1, 2
+LOOSE_NONE, LOOSE_RESIDUALS, LOOSE_MONITORS = 0, 1, 2
+
+
+class SteadyHistory(ctypes.Structure):
+    _fields_ = [("count", ctypes.c_int32), ("nonfinite", ctypes.c_int32), ("n_residuals", ctypes.c_int32),
+                ("n_monitors", ctypes.c_int32), ("res_ref", ctypes.c_double * CRITERION_MAX_RESIDUALS),
+                ("res_last", ctypes.c_double * CRITERION_MAX_RESIDUALS),
+                ("monitor_values", ctypes.c_int32 * CRITERION_MAX_MONITORS),
+                ("monitor_last", ctypes.c_double * CRITERION_MAX_MONITORS)]
+
+
+class SequencingOptions(ctypes.Structure):
+    """gb_sequencing_opts: steady.sequencing_* (defaults: off, drop 2 orders,
+    monitor branch off, no hold on the seeded levels, start at cfl0)."""
+    _fields_ = [("enabled", ctypes.c_int32), ("drop_orders", ctypes.c_double), ("monitor_tol", ctypes.c_double),
+                ("hold", ctypes.c_int32), ("cfl_previous", ctypes.c_int32)]
+
+    @classmethod
+    def make(cls, **kw):
+        o = cls(enabled=0, drop_orders=2.0, monitor_tol=0.0, hold=0, cfl_previous=0)
+        for k, v in kw.items():
+            setattr(o, k, v)
+        return o
 
 
 def np_ptr(a):
@@ -200,13 +233,15 @@ class DriverOptions(ctypes.Structure):
     """gb_driver_opts: steady.* of the pseudo-time driver and the criterion."""
     _fields_ = [("cfl0", ctypes.c_double), ("cfl_max", ctypes.c_double), ("ser_exponent", ctypes.c_double),
                 ("ser_max_growth", ctypes.c_double), ("residual_tol", ctypes.c_double),
-                ("residual_drop_orders", ctypes.c_double), ("residual_ref_iterations", ctypes.c_int32)]
+                ("residual_drop_orders", ctypes.c_double), ("residual_ref_iterations", ctypes.c_int32),
+                ("monitor_rel_tol", ctypes.c_double), ("monitor_window", ctypes.c_int32)]
 
     @classmethod
     def make(cls, line_sweep=0, **kw):
         """The reference's defaults (cfl_max 8 with steady.sweep = lusgs, else 10)."""
         o = cls(cfl0=1.0, cfl_max=8.0 if line_sweep == 1 else 10.0, ser_exponent=1.0, ser_max_growth=2.0,
-                residual_tol=5e-5, residual_drop_orders=4.0, residual_ref_iterations=5)
+                residual_tol=5e-5, residual_drop_orders=4.0, residual_ref_iterations=5, monitor_rel_tol=1e-3,
+                monitor_window=50)
         for k, v in kw.items():
             setattr(o, k, v)
         return o

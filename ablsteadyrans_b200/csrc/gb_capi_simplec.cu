@@ -317,6 +317,42 @@ gb_status gb_simplec_fill_ghosts(gb_simplec* s, const gb_state* q)
     return gb::check_cuda("fill_ghosts");
 }
 
+gb_status gb_simplec_prolong(gb_simplec* s, const gb_state* q, const gb_grid* gc, const gb_state* qc, double reltol,
+                             gb_prolong_result* r)
+{
+    gb::clear_error();
+    if (s == nullptr || q == nullptr || gc == nullptr || qc == nullptr || r == nullptr) {
+        gb::set_error("gust: prolong_state: null argument");
+        return GB_BAD_ARG;
+    }
+    gb_status st = gb::check_grid("prolong_state", gc);
+    if (st != GB_OK) { return st; }
+    const gb_grid& g = gb::simplec_grid(s);
+    const int rx = gc->nx > 0 ? g.nx / gc->nx : 0, ry = gc->ny > 0 ? g.ny / gc->ny : 0;
+    if (rx < 2 || rx != ry || rx * gc->nx != g.nx || ry * gc->ny != g.ny || (rx & (rx - 1)) != 0 || gc->nz != g.nz
+        || gc->periodic_x != g.periodic_x || gc->periodic_y != g.periodic_y) {
+        gb::set_error("gust: prolong_state: the levels must satisfy 0 <= fine < coarse: the coarse grid coarser by a "
+                      "power of two in x and y, the same layers and periodicity");
+        return GB_BAD_ARG;
+    }
+    if (!std::isfinite(reltol) || !(reltol > 0) || !(reltol < 1)) {
+        gb::set_error("gust: invalid inputs:\n  solver.poisson_reltol must be finite, > 0 and < 1");
+        return GB_BAD_ARG;
+    }
+    return gb::simplec_prolong(s, *q, *gc, *qc, reltol, r);
+}
+
+gb_status gb_simplec_implicit_rows(gb_simplec* s, const gb_state* q, int32_t eq, double* A)
+{
+    gb::clear_error();
+    if (s == nullptr || q == nullptr || A == nullptr || eq < 0 || eq > 5 || eq == 3) {
+        gb::set_error("gust: implicit_rows: the stage, the state, A and an equation among u, v, w, theta, k are needed");
+        return GB_BAD_ARG;
+    }
+    gb::simplec_implicit_rows_at(s, *q, eq, A);
+    return gb::check_cuda("implicit_rows");
+}
+
 gb_status gb_simplec_residual(gb_simplec* s, const gb_state* q, double* const* R)
 {
     gb::clear_error();

@@ -12,7 +12,7 @@ thread_local std::string g_error;
 
 void set_error(const char* fmt, ...)
 {
-    char buf[1024];
+    char buf[4096];
     va_list ap;
     va_start(ap, fmt);
     std::vsnprintf(buf, sizeof(buf), fmt, ap);

@@ -1,23 +1,30 @@
 // The steady driver on the host (gust::Driver::step, Source/Driver.cpp:
-// 403-468; gust::SteadyCriterion, Source/SteadyCriterion.cpp:96-224 without
-// the monitor window; gust::ser_cfl, Source/PseudoTime.cpp:53-61), and a
-// runner that drives many independent stages from native threads.
+// 403-468, with seed_reference, release_reference_hold and start_cfl,
+// :275-313; gust::ser_cfl, Source/PseudoTime.cpp:53-61), and a runner that
+// drives many independent stages from native threads.
 //
 // Per step: the local dtau at the current CFL, one SIMPLEC iteration, the
-// scaled residual norms into the criterion. r_n = max over equations of
-// res / max(res_ref, residual_tol) after the reference hold (res_ref: each
-// residual's largest value over the first residual_ref_iterations); steady
-// when every residual is below residual_tol and has dropped
-// residual_drop_orders orders below its reference; otherwise the next CFL
-// from the SER law.
+// scaled residual norms and the monitors into the steady criterion
+// (gb_criterion). r_n = max over equations of |res| / max(res_ref,
+// residual_tol) after the reference hold (1 during it); the next CFL is
+// cfl0 during the hold, then the SER law.
 #include "gb_simplec.cuh"
 
 #include <algorithm>
 #include <atomic>
 #include <cmath>
 #include <new>
+#include <string>
 #include <thread>
 #include <vector>
+
+namespace gb {
+gb_criterion* criterion_new(const gb_driver_opts& o, int n_res, const char* const* res_names, int n_mon,
+                            const char* const* mon_names, const double* mon_scales);
+void criterion_add(gb_criterion* c, const double* res, const double* mon);
+int criterion_verdict(const gb_criterion* c, bool* residuals_met, bool* monitors_met, std::vector<std::string>* why);
+bool criterion_seed(gb_criterion* c, const double* ref);
+}  // namespace gb
 
 struct gb_driver {
     gb_simplec* stage{nullptr};
@@ -25,13 +32,18 @@ struct gb_driver {
     gb_driver_opts opt{};
     double* dtau{nullptr};
     double cfl{1};
+    double r_last{0};
     int iterations{0};
+    int hold{-1};              // -1: residual_ref_iterations (Driver::hold_iterations)
+    int n_mon{2};
     bool nonfinite{false};
-    double res_ref[6]{};
+    gb_criterion* crit{nullptr};
     ~gb_driver()
     {
         if (dtau) { cudaFree(dtau); }
+        gb_criterion_destroy(crit);
     }
+    int hold_iterations() const { return hold < 0 ? opt.residual_ref_iterations : hold; }
 };
 
 namespace {
@@ -63,37 +75,38 @@ gb_status driver_step(gb_driver* d, int32_t* verdict, gb_iter_info* info_out, do
     if (st != GB_OK) { return st; }
     if (info_out) { *info_out = info; }
     const double* res = info.residual_norms;
-    for (int n = 0; n < 6; ++n) {
-        if (!std::isfinite(res[n])) {
-            d->nonfinite = true;
-            *verdict = GB_DRIVER_DIVERGED;
-            return GB_OK;
-        }
-    }
-    if (d->iterations == 1) {
-        for (int n = 0; n < 6; ++n) { d->res_ref[n] = res[n]; }
-    } else if (d->iterations <= o.residual_ref_iterations) {
-        for (int n = 0; n < 6; ++n) { d->res_ref[n] = std::max(d->res_ref[n], res[n]); }
+    const double mon[3] = {info.max_speed, info.mean_tke, info.mean_ustar};
+    gb::criterion_add(d->crit, res, mon);
+    gb_steady_history h{};
+    gb_criterion_history(d->crit, &h);
+    if (h.nonfinite) {
+        d->nonfinite = true;
+        *verdict = GB_DRIVER_DIVERGED;
+        return GB_OK;
     }
     double r = 1.0;
-    bool steady = false;
-    if (d->iterations > o.residual_ref_iterations) {
+    if (h.count > d->hold_iterations()) {
         r = 0;
-        steady = true;
-        const double drop = std::pow(10.0, -o.residual_drop_orders);
-        for (int n = 0; n < 6; ++n) {
-            const double ref = std::max(d->res_ref[n], o.residual_tol);
-            r = std::max(r, std::fabs(res[n]) / ref);
-            if (!(res[n] < o.residual_tol) || !(res[n] <= ref * drop)) { steady = false; }
-        }
+        for (int n = 0; n < 6; ++n) { r = std::max(r, std::fabs(res[n]) / std::max(h.res_ref[n], o.residual_tol)); }
     }
-    if (steady) {
+    d->r_last = r;
+    bool rm = false, mm = false;
+    if (gb::criterion_verdict(d->crit, &rm, &mm, nullptr) == GB_STEADY) {
         *verdict = GB_DRIVER_STEADY;
         return GB_OK;
     }
-    d->cfl = ser_cfl(d->cfl, r, o);
+    d->cfl = (h.count <= d->hold_iterations()) ? o.cfl0 : ser_cfl(d->cfl, r, o);
     *verdict = GB_DRIVER_RUNNING;
     return GB_OK;
+}
+
+bool before_first(const gb_driver* d, const char* what)
+{
+    if (d->iterations != 0) {
+        gb::set_error("gust: Driver::%s: only before the first iteration", what);
+        return false;
+    }
+    return true;
 }
 
 }  // namespace
@@ -114,6 +127,8 @@ gb_status gb_driver_options_default(gb_driver_opts* o, int32_t line_sweep)
     o->residual_tol = 5.0e-5;
     o->residual_drop_orders = 4.0;
     o->residual_ref_iterations = 5;
+    o->monitor_rel_tol = 1.0e-3;
+    o->monitor_window = 50;
     return GB_OK;
 }
 
@@ -139,23 +154,23 @@ gb_status gb_driver_create(gb_simplec* s, const gb_state* q, const gb_driver_opt
         gb::set_error("gust: invalid inputs:\n  steady.ser_max_growth = %g: must be finite and >= 1", o->ser_max_growth);
         return GB_BAD_ARG;
     }
-    if (bad(o->residual_tol, o->residual_tol > 0)) {
-        gb::set_error("gust: steady.residual_tol must be finite and > 0");
-        return GB_BAD_ARG;
-    }
-    if (bad(o->residual_drop_orders, o->residual_drop_orders >= 0 && o->residual_drop_orders <= 300)) {
-        gb::set_error("gust: steady.residual_drop_orders must be >= 0 and <= 300");
-        return GB_BAD_ARG;
-    }
-    if (o->residual_ref_iterations < 1) {
-        gb::set_error("gust: steady.residual_ref_iterations must be >= 1");
-        return GB_BAD_ARG;
-    }
+    // the criterion's residuals and monitors (stage_residual_names,
+    // stage_monitor_specs: Source/Simplec.cpp:363-371)
+    static const char* const kRes[6] = {"u", "v", "w", "p", "theta", "tke"};
+    static const char* const kMon[3] = {"max_speed", "mean_tke", "mean_ustar"};
+    const gb_physics& ph = gb::simplec_physics(s);
+    const double scales[3] = {ph.scale_velocity, ph.scale_tke, 0.1};
+    const int n_mon = gb::simplec_has_wall(s) ? 3 : 2;
+    gb_criterion* crit = gb::criterion_new(*o, 6, kRes, n_mon, kMon, scales);
+    if (crit == nullptr) { return GB_BAD_ARG; }
     gb_driver* d = new (std::nothrow) gb_driver;
     if (d == nullptr) {
+        gb_criterion_destroy(crit);
         gb::set_error("gust: Driver: out of host memory");
         return GB_OOM;
     }
+    d->crit = crit;
+    d->n_mon = n_mon;
     d->stage = s;
     d->q = *q;
     d->opt = *o;
@@ -168,6 +183,81 @@ gb_status gb_driver_create(gb_simplec* s, const gb_state* q, const gb_driver_opt
         return GB_OOM;
     }
     *out = d;
+    return GB_OK;
+}
+
+gb_status gb_driver_criterion(gb_driver* d, gb_criterion** c)
+{
+    gb::clear_error();
+    if (d == nullptr || c == nullptr) {
+        gb::set_error("gust: Driver::criterion: null argument");
+        return GB_BAD_ARG;
+    }
+    *c = d->crit;
+    return GB_OK;
+}
+
+gb_status gb_driver_seed_reference(gb_driver* d, const double* ref)
+{
+    gb::clear_error();
+    if (d == nullptr || ref == nullptr) {
+        gb::set_error("gust: Driver::seed_reference: null argument");
+        return GB_BAD_ARG;
+    }
+    if (!before_first(d, "seed_reference")) { return GB_BAD_ARG; }
+    return gb::criterion_seed(d->crit, ref) ? GB_OK : GB_BAD_ARG;
+}
+
+gb_status gb_driver_release_hold(gb_driver* d)
+{
+    gb::clear_error();
+    if (d == nullptr) {
+        gb::set_error("gust: Driver::release_reference_hold: null argument");
+        return GB_BAD_ARG;
+    }
+    if (!before_first(d, "release_reference_hold")) { return GB_BAD_ARG; }
+    gb_steady_history h{};
+    gb_criterion_history(d->crit, &h);
+    bool seeded = false;
+    for (int n = 0; n < h.n_residuals; ++n) { seeded = seeded || h.res_ref[n] > 0; }
+    if (!seeded) {
+        gb::set_error("gust: Driver::release_reference_hold: the reference is not seeded (seed_reference first)");
+        return GB_BAD_ARG;
+    }
+    d->hold = 0;
+    return GB_OK;
+}
+
+gb_status gb_driver_start_cfl(gb_driver* d, double cfl)
+{
+    gb::clear_error();
+    if (d == nullptr) {
+        gb::set_error("gust: Driver::start_cfl: null argument");
+        return GB_BAD_ARG;
+    }
+    if (!before_first(d, "start_cfl")) { return GB_BAD_ARG; }
+    if (d->hold_iterations() > 0) {
+        gb::set_error("gust: Driver::start_cfl: the reference hold is on");
+        return GB_BAD_ARG;
+    }
+    if (std::isnan(cfl) || !std::isfinite(cfl) || !(cfl > 0) || cfl > d->opt.cfl_max) {
+        gb::set_error("gust: Driver::start_cfl: %.3e is not finite, > 0 and <= steady.cfl_max = %.3e", cfl, d->opt.cfl_max);
+        return GB_BAD_ARG;
+    }
+    d->cfl = std::max(cfl, d->opt.cfl0);
+    return GB_OK;
+}
+
+gb_status gb_driver_status(const gb_driver* d, int32_t* hold_iterations, double* next_cfl, double* relative_residual)
+{
+    gb::clear_error();
+    if (d == nullptr) {
+        gb::set_error("gust: Driver: null argument");
+        return GB_BAD_ARG;
+    }
+    if (hold_iterations) { *hold_iterations = d->hold_iterations(); }
+    if (next_cfl) { *next_cfl = d->cfl; }
+    if (relative_residual) { *relative_residual = d->r_last; }
     return GB_OK;
 }
 

@@ -277,6 +277,9 @@ struct gb_simplec {
     bool wall{false};                    // bc.zlo = surface_layer
     double* cf[gb::kClosureFields]{};    // the closure's fields at the last residual
     double* dist{nullptr};               // the cells' height above the ground (closure)
+    // nu the next local dtau reads: the closure's of the last iteration's
+    // residual (SimplecStage::nu, Simplec.H:214; 0 before the first)
+    double* nu_dtau{nullptr};
     double* ss[gb::kSsPlanes]{};         // the surface state of the iteration's first fill
     double* ssr[gb::kSsPlanes]{};        // the residual's own surface state
     double* sst[gb::kSsPlanes]{};        // the later fills' surface state
@@ -1399,7 +1402,7 @@ enum Word : int {
     W_MAX_FU, W_MAX_FV, W_MAX_FW, W_SPEED_U, W_SPEED_V, W_SPEED_W, W_MAX_DTH, W_MAX_DK, W_LAST_TH, W_LAST_K,
     W_CLIPPED, W_MON_U, W_MON_V, W_MON_W, W_COUNT
 };
-enum Sum : int { SUM_R0 = 0, SUM_TKE = 6, SUM_LEVEL = 8, SUM_COUNT = 8 };
+enum Sum : int { SUM_R0 = 0, SUM_TKE = 6, SUM_USTAR = 7, SUM_LEVEL = 8, SUM_COUNT = 8 };
 
 gb_status momentum_predictor(gb_simplec* S, const gb_state& q, double** R)
 {
@@ -1717,8 +1720,15 @@ gb_status simplec_iterate(gb_simplec* S, const gb_state& q, const double* dtau, 
     // 1. ghosts and the wall state at q; 2. the residual (the closure at q)
     fill_ghosts_into(S, q, S->ss);
     simplec_residual(S, q, w.R);
+    if (S->ph.closure) {
+        cudaMemcpyAsync(S->nu_dtau, S->cf[kClosureNu], sizeof(double) * volume(g), cudaMemcpyDeviceToDevice, ctx->stream);
+    }
     for (int n = 0; n < 6; ++n) { dsum(S, valid_box(g, kLoc[n]), w.R[n], 0, SUM_R0 + n); }
     dsum(S, valid_box(g, CC), q.tke, 1, SUM_TKE);
+    if (S->wall) {
+        // the u* plane of the domain columns (a plane is the k = -ng layer of the indexing)
+        dsum(S, Box{{0, 0, -g.ng}, {g.nx - 1, g.ny - 1, -g.ng}}, S->ss[kSsUstar], 1, SUM_USTAR);
+    }
     dmax(S, valid_box(g, XF), q.u, nullptr, W_MON_U);
     dmax(S, valid_box(g, YF), q.v, nullptr, W_MON_V);
     dmax(S, valid_box(g, ZF), q.w, nullptr, W_MON_W);
@@ -1758,6 +1768,7 @@ gb_status simplec_iterate(gb_simplec* S, const gb_state& q, const double* dtau, 
         info->residual_norms[n] = std::sqrt(sums[n]) / std::sqrt(static_cast<double>(b.count())) / scale[n];
     }
     info->mean_tke = sums[SUM_TKE] / (static_cast<double>(g.nx) * g.ny * g.nz);
+    info->mean_ustar = S->wall ? sums[SUM_USTAR] / (static_cast<double>(g.nx) * g.ny) : 0.0;
     info->max_speed = std::max(std::max(wd(W_MON_U), wd(W_MON_V)), wd(W_MON_W));
     info->max_du = wd(W_MAX_DU);
     info->max_dv = wd(W_MAX_DV);
@@ -1799,7 +1810,7 @@ gb_status simplec_local_dtau(gb_simplec* S, const gb_state& q, double cfl, doubl
     const double* v = q.v;
     const double* om = S->w.om;
     const double* J = S->mesh.detJ;
-    const double* nu = S->dfe.nu;
+    const double* nu = S->ph.closure ? S->nu_dtau : S->df.nu;
     const double dxinv = 1.0 / g.dx, dyinv = 1.0 / g.dy, dzinv = 1.0 / g.dzeta;
     const double diff_h = 2 * (dxinv * dxinv + dyinv * dyinv);
     for_box(S->ctx, valid_box(g, CC), [=] __device__(int i, int j, int k) {
@@ -2003,6 +2014,12 @@ gb_status simplec_initialize(gb_simplec* S, const gb_state& q, const gb_init_opt
     return check_cuda("initialize_state");
 }
 
+void simplec_implicit_rows_at(gb_simplec* S, const gb_state& q, int eq, double* A)
+{
+    transport_fluxes(S, q, S->w.F[0], S->w.F[1], S->w.F[2]);
+    simplec_implicit_rows(S, eq, S->w.F, A);
+}
+
 gb_status simplec_turbulence(gb_simplec* S, double* const* closure, double* const* surface)
 {
     gb_ctx* ctx = S->ctx;
@@ -2032,8 +2049,145 @@ gb_status simplec_turbulence(gb_simplec* S, double* const* closure, double* cons
     return check_cuda("SimplecStage::closure_fields");
 }
 
+namespace {
+
+//! Where a fine point sits among the coarse ones along one direction
+//! (Axis, locate; Transfer.cpp:20-84): ic and the weight t, the domains
+//! starting at 0.
+struct Axis {
+    int r, imin, imax, step;
+    double lin, inv;
+};
+
+Axis make_axis(int N, bool periodic, int r, bool nod)
+{
+    Axis a{r, 0, 0, 1, 1.0, 0.0};
+    if (nod) {
+        a.imax = N - 1;
+        a.inv = 1.0 / static_cast<double>(r);
+    } else {
+        a.inv = 1.0 / static_cast<double>(2 * r);
+        if (periodic) {
+            a.imin = -1;
+            a.imax = N - 1;
+        } else if (N >= 2) {
+            a.imax = N - 2;
+        } else {
+            a.step = 0;
+            a.lin = 0;
+        }
+    }
+    return a;
+}
+
+__device__ __forceinline__ void locate(const Axis& a, bool nod, int i, int& ic, double& t)
+{
+    const int den = nod ? a.r : 2 * a.r;
+    const int m = nod ? i : (2 * i + 1 - a.r);
+    const int mm = nod ? m - 1 : m;
+    int c = (mm >= 0) ? mm / den : -((-mm + den - 1) / den);
+    c = min(max(c, a.imin), a.imax);
+    t = a.lin * static_cast<double>(m - den * c) * a.inv;
+    ic = c;
+}
+
+//! The bilinear interpolation per zeta-level of a coarse field at the fine
+//! valid points of type t (interpolate<T>, Transfer.cpp:86-108). Only the
+//! coarse valid points are read: a cell-centred index one past a periodic
+//! face is its periodic image (the coarse image's ParallelCopy,
+//! Transfer.cpp:316-320), so the coarse ghost cells need not be filled.
+void interpolate(gb_ctx* ctx, const gb_grid& g, const gb_grid& gc, int t, const double* q, double* f, int r)
+{
+    const bool nx = nodal(t, 0), ny = nodal(t, 1);
+    const Axis ax = make_axis(gc.nx, gc.periodic_x != 0, r, nx);
+    const Axis ay = make_axis(gc.ny, gc.periodic_y != 0, r, ny);
+    const bool wx = !nx && gc.periodic_x, wy = !ny && gc.periodic_y;
+    const int NX = gc.nx, NY = gc.ny;
+    const gb_grid gf = g, gcc = gc;
+    for_box(ctx, valid_box(g, t), [=] __device__(int i, int j, int k) {
+        int I, J;
+        double tx, ty;
+        locate(ax, nx, i, I, tx);
+        locate(ay, ny, j, J, ty);
+        int I1 = I + ax.step, J1 = J + ay.step;
+        if (wx) {
+            I = (I + NX) % NX;
+            I1 = (I1 + NX) % NX;
+        }
+        if (wy) {
+            J = (J + NY) % NY;
+            J1 = (J1 + NY) % NY;
+        }
+        const double one = 1;
+        f[at(gf, i, j, k)] = (one - ty) * ((one - tx) * q[at(gcc, I, J, k)] + tx * q[at(gcc, I1, J, k)])
+                           + ty * ((one - tx) * q[at(gcc, I, J1, k)] + tx * q[at(gcc, I1, J1, k)]);
+    }, GB_KERNEL_MG_TRANSFER);
+}
+
+}  // namespace
+
+gb_status simplec_prolong(gb_simplec* S, const gb_state& q, const gb_grid& gc, const gb_state& qc, double reltol,
+                          gb_prolong_result* res)
+{
+    gb_ctx* ctx = S->ctx;
+    const gb_grid g = S->g;
+    SimplecWork& w = S->w;
+    const int r = g.nx / gc.nx;
+    // prolong_fields (Transfer.cpp:290-320)
+    interpolate(ctx, g, gc, CC, qc.theta, q.theta, r);
+    interpolate(ctx, g, gc, CC, qc.tke, q.tke, r);
+    interpolate(ctx, g, gc, CC, qc.p, q.p, r);
+    interpolate(ctx, g, gc, XF, qc.u, q.u, r);
+    interpolate(ctx, g, gc, YF, qc.v, q.v, r);
+    interpolate(ctx, g, gc, ZF, qc.w, q.w, r);
+    // k >= the floor, counted
+    cudaMemsetAsync(dword(ctx, 0), 0, sizeof(unsigned long long) * W_COUNT, ctx->stream);
+    {
+        double* tk = q.tke;
+        const double floor_k = S->opt.tke_floor;
+        unsigned long long* count = dword(ctx, W_CLIPPED);
+        for_box(ctx, valid_box(g, CC), [=] __device__(int i, int j, int k) {
+            double* x = &tk[at(g, i, j, k)];
+            if (*x < floor_k) {
+                *x = floor_k;
+                atomicAdd(count, 1ULL);
+            }
+        });
+    }
+    fill_ghosts_into(S, q, S->sst);
+    // the projection: d = 1 - the Dirichlet mask, alpha_p 1, p' restored
+    for (int c = 0; c < 3; ++c) {
+        dirichlet_rows(S, c, kLoc[c], w.mask);
+        double* dd = w.dd[c];
+        const double* mk = w.mask;
+        for_box(ctx, valid_box(g, kLoc[c]), [=] __device__(int i, int j, int k) {
+            const int64_t o = at(g, i, j, k);
+            dd[o] = mk[o] * -1.0 + 1.0;
+        });
+    }
+    cudaMemcpyAsync(w.tmp, q.p, sizeof(double) * volume(g), cudaMemcpyDeviceToDevice, ctx->stream);
+    const double reltol_keep = S->poisson->opt.reltol, alpha_keep = S->opt.alpha_p;
+    S->poisson->opt.reltol = reltol;
+    S->opt.alpha_p = 1.0;
+    gb_iter_info info{};
+    gb_status st = pressure_correction(S, q, &info);
+    S->poisson->opt.reltol = reltol_keep;
+    S->opt.alpha_p = alpha_keep;
+    if (st != GB_OK) { return st; }
+    cudaMemcpyAsync(q.p, w.tmp, sizeof(double) * volume(g), cudaMemcpyDeviceToDevice, ctx->stream);
+    unsigned long long words[W_COUNT];
+    if ((st = read_words(ctx, 0, W_COUNT, words)) != GB_OK) { return st; }
+    res->divergence_before = bits_to_double(words[W_DIV_BEFORE]);
+    res->divergence_after = bits_to_double(words[W_DIV_AFTER]);
+    res->poisson_iterations = info.poisson_iterations;
+    res->tke_clipped = static_cast<int64_t>(words[W_CLIPPED]);
+    return check_cuda("prolong_state");
+}
+
 const gb_grid& simplec_grid(const gb_simplec* S) { return S->g; }
 gb_ctx* simplec_ctx(const gb_simplec* S) { return S->ctx; }
+const gb_physics& simplec_physics(const gb_simplec* S) { return S->ph; }
+bool simplec_has_wall(const gb_simplec* S) { return S->wall; }
 
 // ----------------------------------------------------------- creation ---
 
@@ -2100,6 +2254,7 @@ gb_status simplec_build(gb_simplec* S)
     if (S->ph.closure) {
         for (int n = 0; n < kClosureFields; ++n) { turb_ok = (S->cf[n] = dbuf(S, vol)) && turb_ok; }
         turb_ok = (S->dist = dbuf(S, vol)) && turb_ok;
+        turb_ok = (S->nu_dtau = dbuf(S, vol)) && turb_ok;
         S->dfe = gb_diffusivities{S->cf[kClosureNu], S->cf[kClosureGammaTheta], S->cf[kClosureGammaTke]};
     }
     if (S->wall) {

@@ -12,11 +12,17 @@ void simplec_delete(gb_simplec* S);
 void simplec_fill_ghosts(gb_simplec* S, const gb_state& q);
 void simplec_residual(gb_simplec* S, const gb_state& q, double** R);
 void simplec_implicit_rows(gb_simplec* S, int eq, double* const* F, double* A);
+void simplec_implicit_rows_at(gb_simplec* S, const gb_state& q, int eq, double* A);
 gb_status simplec_iterate(gb_simplec* S, const gb_state& q, const double* dtau, gb_iter_info* info);
 gb_status simplec_local_dtau(gb_simplec* S, const gb_state& q, double cfl, double* dtau);
 gb_status simplec_initialize(gb_simplec* S, const gb_state& q, const gb_init_opts& o, gb_init_result* r);
 gb_status simplec_turbulence(gb_simplec* S, double* const* closure, double* const* surface);
+gb_status simplec_prolong(gb_simplec* S, const gb_state& q, const gb_grid& gc, const gb_state& qc, double reltol,
+                          gb_prolong_result* r);
 const gb_grid& simplec_grid(const gb_simplec* S);
 gb_ctx* simplec_ctx(const gb_simplec* S);
+const gb_physics& simplec_physics(const gb_simplec* S);
+//! Whether the ground is a surface-layer face (the wall model's state).
+bool simplec_has_wall(const gb_simplec* S);
 
 }  // namespace gb

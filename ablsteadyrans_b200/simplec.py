@@ -28,6 +28,15 @@ def _declare(L):
     L.gb_simplec_initialize.argtypes = [P, ctypes.POINTER(abi.State), ctypes.POINTER(abi.InitOptions),
                                         ctypes.POINTER(abi.InitResult)]
     L.gb_simplec_turbulence.argtypes = [P, ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_void_p)]
+    L.gb_simplec_implicit_rows.argtypes = [P, ctypes.POINTER(abi.State), ctypes.c_int32, P]
+    L.gb_driver_criterion.argtypes = [P, ctypes.POINTER(P)]
+    L.gb_driver_seed_reference.argtypes = [P, ctypes.POINTER(ctypes.c_double)]
+    L.gb_driver_release_hold.argtypes = [P]
+    L.gb_driver_start_cfl.argtypes = [P, ctypes.c_double]
+    L.gb_driver_status.argtypes = [P, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_double),
+                                   ctypes.POINTER(ctypes.c_double)]
+    L.gb_simplec_prolong.argtypes = [P, ctypes.POINTER(abi.State), G, ctypes.POINTER(abi.State), ctypes.c_double,
+                                     ctypes.POINTER(abi.ProlongResult)]
 
 
 # The closure's fields and the surface state's planes, in the ABI's order.
@@ -92,6 +101,7 @@ class SimplecStage:
         check(self._L.gb_simplec_create(ctx.handle, ctypes.byref(case.grid.c), ctypes.byref(bc), ctypes.byref(physics),
                                         ctypes.byref(options), ctypes.c_void_p(case.z.data_ptr()),
                                         ctypes.byref(self._m), ctypes.byref(self._d), ctypes.byref(self._h)))
+        ctx.own(self)
 
     def fill_ghosts(self):
         from . import check
@@ -106,6 +116,15 @@ class SimplecStage:
         st = self.case.state()
         check(self._L.gb_simplec_residual(self._h, ctypes.byref(st), arr))
         return R
+
+    def implicit_rows(self, eq):
+        """implicit_rows of equation eq (0 u .. 5 k) at the state: A (7 x grid)."""
+        import torch
+        from . import check
+        A = torch.zeros((7,) + tuple(self.case.grid.shape), dtype=torch.float64, device="cuda")
+        st = self.case.state()
+        check(self._L.gb_simplec_implicit_rows(self._h, ctypes.byref(st), int(eq), ctypes.c_void_p(A.data_ptr())))
+        return A
 
     def turbulence(self, closure=True, surface=True):
         """(closure fields, surface state) as dicts of host arrays: the
@@ -149,6 +168,17 @@ class SimplecStage:
         check(self._L.gb_simplec_initialize(self._h, ctypes.byref(st), ctypes.byref(o), ctypes.byref(res)))
         return res
 
+    def prolong(self, coarse, reltol):
+        """prolong_state (Transfer.cpp:322-385) into this stage's state from
+        a coarser level's DeviceCase (its valid points): the bilinear fields, k at the floor, the ghost fill and the
+        projection to reltol. Returns the ProlongResult."""
+        from . import check
+        res = abi.ProlongResult()
+        st, sc = self.case.state(), coarse.state()
+        check(self._L.gb_simplec_prolong(self._h, ctypes.byref(st), ctypes.byref(coarse.grid.c), ctypes.byref(sc),
+                                         float(reltol), ctypes.byref(res)))
+        return res
+
     def close(self):
         from . import check
         if self._h:
@@ -175,6 +205,7 @@ class NativeDriver:
         self._h = ctypes.c_void_p()
         check(self._L.gb_driver_create(stage._h, ctypes.byref(self._state), ctypes.byref(self.options),
                                        ctypes.byref(self._h)))
+        stage.ctx.own(self)
         self.iterations = 0
 
     @property
@@ -190,6 +221,37 @@ class NativeDriver:
         check(self._L.gb_driver_step(self._h, ctypes.byref(v), ctypes.byref(info), ctypes.byref(cfl)))
         self.iterations += 1
         return abi.DRIVER_VERDICTS[v.value], info, cfl.value
+
+    @property
+    def criterion(self):
+        """The driver's steady criterion (history, verdict, loose stop)."""
+        from . import check
+        from .driver import SteadyCriterion
+        h = ctypes.c_void_p()
+        check(self._L.gb_driver_criterion(self._h, ctypes.byref(h)))
+        return SteadyCriterion(handle=h, owner=self)
+
+    def seed_reference(self, ref):
+        """Driver::seed_reference: the coarsest level's references (before the first step)."""
+        from . import check
+        check(self._L.gb_driver_seed_reference(self._h, (ctypes.c_double * 6)(*[float(x) for x in ref])))
+
+    def release_hold(self):
+        """Driver::release_reference_hold (steady.sequencing_hold = 0)."""
+        from . import check
+        check(self._L.gb_driver_release_hold(self._h))
+
+    def start_cfl(self, cfl):
+        """Driver::start_cfl (steady.sequencing_cfl_start = previous)."""
+        from . import check
+        check(self._L.gb_driver_start_cfl(self._h, float(cfl)))
+
+    def status(self):
+        """(hold iterations, the next step's CFL, r_n of the last step)."""
+        from . import check
+        hold, cfl, r = ctypes.c_int32(), ctypes.c_double(), ctypes.c_double()
+        check(self._L.gb_driver_status(self._h, ctypes.byref(hold), ctypes.byref(cfl), ctypes.byref(r)))
+        return hold.value, cfl.value, r.value
 
     def close(self):
         from . import check

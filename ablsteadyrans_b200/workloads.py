@@ -119,6 +119,7 @@ class Instance:
     def __init__(self, name, grid, zlevels, ground, bc, physics, options, ustar, z0, direction, z0map=None):
         self.name = name
         self.z0map = z0map   # per-column roughness plane (gb_mesh_fields.z0), or None
+        self.ground = ground  # node ground heights, columns -1..n+1 (ny + 3, nx + 3)
         self.grid = grid
         self.zlevels = zlevels
         self.z = btf_heights(grid, zlevels, ground)

@@ -393,6 +393,8 @@ typedef struct gb_iter_info {
     int32_t poisson_iterations;
     double max_dtheta, max_dtke;
     int64_t tke_clipped;
+    double mean_ustar;               /* monitor with a surface-layer ground: the mean u* of the wall state
+                                        at the start of the iteration (0 without) */
 } gb_iter_info;
 
 /* init.* of the mass-consistent initializer (gust::InitOptions,
@@ -435,6 +437,14 @@ gb_status gb_simplec_fill_ghosts(gb_simplec* s, const gb_state* q);
  * caller): R[0..5] = R_u, R_v, R_w, R_p, R_theta, R_k (device arrays). */
 gb_status gb_simplec_residual(gb_simplec* s, const gb_state* q, double* const* R);
 
+/* implicit_rows (Source/Residual.cpp:272-304) of equation eq (0 u, 1 v, 2 w,
+ * 4 theta, 5 k) at q: the coefficients of the transport fluxes of q and the
+ * stage's diffusivities (the closure's at the last residual), the Patankar
+ * diagonal of k, the first cells' wall rows (the surface state of the last
+ * ghost fill), the damping and the boundary folds, into A (GB_N_COEFS device
+ * arrays of the grid, component-major). */
+gb_status gb_simplec_implicit_rows(gb_simplec* s, const gb_state* q, int32_t eq, double* A);
+
 /* SimplecStage::iterate (Source/Simplec.cpp:452-506): one SIMPLEC outer
  * iteration of q with the local pseudo-time step dtau (cells). */
 gb_status gb_simplec_iterate(gb_simplec* s, const gb_state* q, const double* dtau, gb_iter_info* info);
@@ -466,6 +476,25 @@ gb_status gb_init_options_default(gb_init_opts* o);
  * from Omega). */
 gb_status gb_simplec_initialize(gb_simplec* s, const gb_state* q, const gb_init_opts* o, gb_init_result* r);
 
+/* What a prolongation did (gust::ProlongResult, Source/Transfer.H:112-116). */
+typedef struct gb_prolong_result {
+    double divergence_before, divergence_after;  /* max |div u| before and after the projection (1/s) */
+    int32_t poisson_iterations;
+    int64_t tke_clipped;                         /* fine cells raised to the k floor */
+} gb_prolong_result;
+
+/* prolong_state (Source/Transfer.H:118-128, Transfer.cpp:322-385) into this
+ * stage's state q from a coarser level's state qc on grid gc (coarser by a
+ * power of two in x and y, the same layers; only its valid points are read,
+ * a periodic neighbour through its image): every field bilinear per
+ * zeta-level (the linear extrapolation in the half cell next to a
+ * non-periodic face), k raised to the floor, this stage's ghost fill, then
+ * the projection (the pressure correction with d = 1 off the Dirichlet
+ * rows, the Poisson solve to reltol: the run's solver.poisson_reltol), p'
+ * restored. */
+gb_status gb_simplec_prolong(gb_simplec* s, const gb_state* q, const gb_grid* gc, const gb_state* qc, double reltol,
+                             gb_prolong_result* r);
+
 /* gust::local_dtau (Source/PseudoTime.H:32-33) with the stage's diffusivity nu. */
 gb_status gb_local_dtau(gb_simplec* s, const gb_state* q, double cfl, double* dtau);
 
@@ -473,7 +502,7 @@ gb_status gb_local_dtau(gb_simplec* s, const gb_state* q, double cfl, double* dt
 
 /* steady.* of the pseudo-time driver and the steady criterion (gust::
  * SteadyOptions, Source/Driver.H:52-110; gust::SteadyParams,
- * Source/SteadyCriterion.H:13-33; the monitor window is not applied). */
+ * Source/SteadyCriterion.H:13-33). */
 typedef struct gb_driver_opts {
     double cfl0, cfl_max;            /* steady.cfl0, steady.cfl_max */
     double ser_exponent;             /* steady.ser_exponent */
@@ -481,7 +510,68 @@ typedef struct gb_driver_opts {
     double residual_tol;             /* steady.residual_tol */
     double residual_drop_orders;     /* steady.residual_drop_orders */
     int32_t residual_ref_iterations; /* steady.residual_ref_iterations */
+    double monitor_rel_tol;          /* steady.monitor_rel_tol */
+    int32_t monitor_window;          /* steady.monitor_window (>= 2) */
 } gb_driver_opts;
+
+/* ---- the steady criterion ------------------------------------------------ */
+
+/* gust::SteadyCriterion (Source/SteadyCriterion.H:81-150): residual
+ * references (the largest of the first residual_ref_iterations values, or a
+ * seed they raise), the last residuals and each monitor's last
+ * monitor_window + 1 values; steady when every residual is below
+ * residual_tol and residual_drop_orders orders below its reference (floored
+ * at residual_tol) and every monitor has a full window, changed over it by
+ * at most monitor_rel_tol of max(|last|, scale) and is within that of its
+ * Aitken-extrapolated limit. A NaN or infinity is Diverged for good.
+ * Host only: no GPU is needed. */
+typedef struct gb_criterion gb_criterion;
+enum { GB_CRITERION_MAX_RESIDUALS = 8, GB_CRITERION_MAX_MONITORS = 4 };
+enum { GB_NOT_STEADY = 0, GB_STEADY = 1, GB_DIVERGED = 2 };
+typedef struct gb_steady_history {
+    int32_t count, nonfinite, n_residuals, n_monitors;
+    double res_ref[GB_CRITERION_MAX_RESIDUALS], res_last[GB_CRITERION_MAX_RESIDUALS];
+    int32_t monitor_values[GB_CRITERION_MAX_MONITORS];   /* values in each monitor's window */
+    double monitor_last[GB_CRITERION_MAX_MONITORS];
+} gb_steady_history;
+/* The parameters are o's residual_* and monitor_* (validate, Source/
+ * SteadyCriterion.cpp:26-48: each violation names its key); the names label
+ * the verdict's reasons; each monitor scale finite and > 0. */
+gb_status gb_criterion_create(const gb_driver_opts* o, int32_t n_residuals, const char* const* residual_names,
+                              int32_t n_monitors, const char* const* monitor_names, const double* monitor_scales,
+                              gb_criterion** out);
+gb_status gb_criterion_destroy(gb_criterion* c);
+/* SteadyCriterion::add: one iteration's residuals and monitors. */
+gb_status gb_criterion_add(gb_criterion* c, const double* residuals, const double* monitors);
+/* SteadyCriterion::seed_reference (grid sequencing): before the first add. */
+gb_status gb_criterion_seed_reference(gb_criterion* c, const double* ref);
+/* SteadyCriterion::verdict: *status GB_NOT_STEADY, _STEADY or _DIVERGED;
+ * reasons (may be NULL) receives why it is not steady, one per line. */
+gb_status gb_criterion_verdict(const gb_criterion* c, int32_t* status, int32_t* residuals_met, int32_t* monitors_met,
+                               char* reasons, int32_t reasons_cap);
+gb_status gb_criterion_history(const gb_criterion* c, gb_steady_history* h);
+/* Monitor m's window, oldest first: *n values (at most cap copied). */
+gb_status gb_criterion_monitor_window(const gb_criterion* c, int32_t m, double* values, int32_t cap, int32_t* n);
+
+/* steady.sequencing_* (gust::SequencingOptions, Source/Sequencing.H:87-95). */
+typedef struct gb_sequencing_opts {
+    int32_t enabled;                 /* steady.sequencing */
+    double drop_orders;              /* steady.sequencing_drop_orders (2) */
+    double monitor_tol;              /* steady.sequencing_monitor_tol (0: off) */
+    int32_t hold;                    /* steady.sequencing_hold (0 | 1; 0) */
+    int32_t cfl_previous;            /* steady.sequencing_cfl_start = previous (1) or cfl0 (0) */
+} gb_sequencing_opts;
+/* check_sequencing_options (Source/Sequencing.cpp:120-169) for a mesh of
+ * nx x ny cells over hierarchy_levels levels; strict: the run's criterion. */
+gb_status gb_sequencing_check(const gb_sequencing_opts* o, const gb_driver_opts* strict, int32_t nx, int32_t ny,
+                              int32_t hierarchy_levels);
+enum { GB_LOOSE_NONE = 0, GB_LOOSE_RESIDUALS = 1, GB_LOOSE_MONITORS = 2 };
+/* loose_stop (Source/Sequencing.cpp:172-222) after the last iteration c
+ * recorded: *branch GB_LOOSE_NONE, (a) _RESIDUALS or (b) _MONITORS; reason
+ * (may be NULL) the branch's text. hold_iterations: the level's reference
+ * hold (gb_driver_hold_iterations). */
+gb_status gb_loose_stop(const gb_criterion* c, const gb_sequencing_opts* o, int32_t hold_iterations, int32_t* branch,
+                        char* reason, int32_t reason_cap);
 
 enum { GB_DRIVER_RUNNING = 0, GB_DRIVER_STEADY = 1, GB_DRIVER_DIVERGED = 2, GB_DRIVER_FAILED = 3 };
 
@@ -489,16 +579,32 @@ typedef struct gb_driver gb_driver;
 
 /* The defaults (cfl0 1, cfl_max 8 with steady.sweep = lusgs else 10 (Source/
  * Driver.cpp:133-136), ser_exponent 1, ser_max_growth 2, residual_tol 5e-5,
- * residual_drop_orders 4, residual_ref_iterations 5). */
+ * residual_drop_orders 4, residual_ref_iterations 5, monitor_rel_tol 1e-3,
+ * monitor_window 50). */
 gb_status gb_driver_options_default(gb_driver_opts* o, int32_t line_sweep);
 /* gust::Driver for one stage and state (allocates the local dtau). */
 gb_status gb_driver_create(gb_simplec* s, const gb_state* q, const gb_driver_opts* o, gb_driver** out);
 gb_status gb_driver_destroy(gb_driver* d);
 /* Driver::step (Source/Driver.cpp:403-468): the local dtau at the current CFL,
- * one SIMPLEC iteration, the criterion, the next CFL from the SER law.
- * *verdict: GB_DRIVER_RUNNING, _STEADY or _DIVERGED (a non-finite iteration
- * or residual); info and cfl (the CFL used) may be NULL. */
+ * one SIMPLEC iteration, the residuals and monitors (max_speed, mean_tke and,
+ * with a surface-layer ground, mean_ustar; stage_monitor_specs, Source/
+ * Simplec.cpp:365-371, scales gb_physics.scale_velocity, scale_tke and 0.1)
+ * into the criterion, r_n after the reference hold, the next CFL (cfl0
+ * during the hold, then the SER law). *verdict: GB_DRIVER_RUNNING, _STEADY
+ * or _DIVERGED (a non-finite iteration, residual or monitor); info and cfl
+ * (the CFL used) may be NULL. */
 gb_status gb_driver_step(gb_driver* d, int32_t* verdict, gb_iter_info* info, double* cfl);
+/* The driver's criterion (owned by the driver): history, verdict, loose stop. */
+gb_status gb_driver_criterion(gb_driver* d, gb_criterion** c);
+/* Driver::seed_reference, release_reference_hold and start_cfl (Source/
+ * Driver.cpp:275-313), each only before the first step: the coarsest
+ * level's references; no reference hold (needs a seed); the first CFL
+ * (with the hold released; brought up to cfl0, at most cfl_max). */
+gb_status gb_driver_seed_reference(gb_driver* d, const double* ref);
+gb_status gb_driver_release_hold(gb_driver* d);
+gb_status gb_driver_start_cfl(gb_driver* d, double cfl);
+/* Driver::hold_iterations, the CFL of the next step and r_n of the last. */
+gb_status gb_driver_status(const gb_driver* d, int32_t* hold_iterations, double* next_cfl, double* relative_residual);
 /* Many drivers at once: each steps until its verdict is not RUNNING or it
  * has taken max_iterations steps, on `threads` host threads (<= 0: one per
  * driver), so that one driver's host synchronisations overlap the others'

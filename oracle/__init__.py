@@ -250,6 +250,13 @@ def _declare_simplec(L):
     L.og_initialize.argtypes = [G, ctypes.POINTER(BC), ctypes.POINTER(InitOptions), ctypes.POINTER(State),
                                 ctypes.POINTER(MeshFields), P]
     L.og_initialize.restype = i32
+    L.og_implicit_rows2.argtypes = [G, ctypes.POINTER(BC), ctypes.POINTER(Physics), i32, P, P, P, P, P,
+                                    ctypes.POINTER(Diffusivities), PP, PP, P]
+    L.og_prolong_fields.argtypes = [G, ctypes.POINTER(State), G, ctypes.POINTER(State), i32]
+    L.og_prolong_state.argtypes = [G, ctypes.POINTER(State), G, ctypes.POINTER(State), i32, ctypes.POINTER(BC),
+                                   ctypes.POINTER(Physics), ctypes.POINTER(SimplecOptions), ctypes.POINTER(MeshFields),
+                                   f64, ctypes.POINTER(f64)]
+    L.og_prolong_state.restype = i32
     L.og_fill_ghosts2.argtypes = [G, ctypes.POINTER(BC), ctypes.POINTER(Physics), P, P, P, P, P, P, P, P, PP]
     L.og_residual2.argtypes = [G, ctypes.POINTER(BC), ctypes.POINTER(Physics), ctypes.POINTER(State),
                                ctypes.POINTER(MeshFields), ctypes.POINTER(Diffusivities), PP, PP, PP]
@@ -375,17 +382,39 @@ def surface_state(case, bc, phys):
     return dict(zip(SURFACE_FIELDS, ss)), int(bad)
 
 
-def implicit_rows(case, bc, phys, eq):
+def implicit_rows(case, bc, phys, eq, cf=None, ss=None):
     """implicit_rows (Residual.cpp:272-304) of equation eq (0 u .. 5 k) with the
-    case's transport fluxes and given diffusivities: A (N_COEFS x grid)."""
+    case's transport fluxes: the given diffusivities, or the closure's fields
+    cf and the surface state ss (dicts, as residual(fields=True) gives them):
+    A (N_COEFS x grid)."""
     g = case.grid
     q = case.q
     F = transport_fluxes(g, q["u"], q["v"], q["w"], case.z, case.ax, case.ay)
     A = g.np_zeros(7)
     d = case.diffusivities()
-    _L().og_implicit_rows(ctypes.byref(g.c), ctypes.byref(bc), ctypes.byref(phys), int(eq), *[_p(f) for f in F],
-                          _p(case.z), _p(case.J), ctypes.byref(d), _p(A))
+    ca = None if cf is None else _arrays([cf[n] for n in CLOSURE_FIELDS])
+    sa = None if ss is None else _arrays([ss[n] for n in SURFACE_FIELDS])
+    _L().og_implicit_rows2(ctypes.byref(g.c), ctypes.byref(bc), ctypes.byref(phys), int(eq), *[_p(f) for f in F],
+                           _p(case.z), _p(case.J), ctypes.byref(d), ca, sa, _p(A))
     return A
+
+
+def prolong_fields(coarse, fine, r):
+    """prolong_fields (Transfer.cpp:290-320): the fine case's state from the
+    coarse case's valid points, r the ratio of the cell sizes."""
+    sc, sf = coarse.state(), fine.state()
+    _L().og_prolong_fields(ctypes.byref(coarse.grid.c), ctypes.byref(sc), ctypes.byref(fine.grid.c), ctypes.byref(sf), int(r))
+
+
+def prolong_state(coarse, fine, r, bc, phys, opts, reltol=1e-10):
+    """prolong_state (Transfer.cpp:322-385) into the fine case: returns
+    (status, [divergence before, after, Poisson iterations, k cells raised])."""
+    info = (ctypes.c_double * 4)()
+    sc, sf, m = coarse.state(), fine.state(), fine.mesh()
+    rc = _L().og_prolong_state(ctypes.byref(coarse.grid.c), ctypes.byref(sc), ctypes.byref(fine.grid.c),
+                               ctypes.byref(sf), int(r), ctypes.byref(bc), ctypes.byref(phys), ctypes.byref(opts),
+                               ctypes.byref(m), float(reltol), info)
+    return int(rc), list(info)
 
 
 def height_above_ground(case):

@@ -556,6 +556,8 @@ static void dirichlet_rows(const og_grid* g, const gb_bc* bc, int f, int t, doub
     }
 }
 
+void og_dirichlet_rows(const og_grid* g, const gb_bc* bc, int f, int t, double* mask) { dirichlet_rows(g, bc, f, t, mask); }
+
 /* apply_to_implicit (BoundaryConditions.cpp:885-941): the damping first,
  * then the folds (a Dirichlet face point's row becomes the identity). */
 static void apply_to_implicit(const og_grid* g, const gb_bc* bc, const double* z, int f, int t, double* A)
@@ -862,6 +864,16 @@ void og_implicit_rows(const og_grid* g, const gb_bc* bc, const gb_physics* ph, i
                       double* A)
 {
     implicit_rows_t(g, bc, ph, eq, F0, F1, F2, z, J, df, NULL, A);
+}
+
+/* implicit_rows with the closure's fields (N_CF volumes) and the surface
+ * state (N_SS planes) of an evaluation (either null: none). */
+void og_implicit_rows2(const og_grid* g, const gb_bc* bc, const gb_physics* ph, int eq, const double* F0,
+                       const double* F1, const double* F2, const double* z, const double* J,
+                       const gb_diffusivities* df, double** cf, double** ss, double* A)
+{
+    const og_turb t = {cf, ss};
+    implicit_rows_t(g, bc, ph, eq, F0, F1, F2, z, J, df, &t, A);
 }
 
 /* ------------------------------------------------------------------ */
@@ -1293,6 +1305,14 @@ int og_simplec_iterate2(const og_grid* g, const gb_bc* bc, const gb_physics* ph,
     og_stage_norms(g, ph, R, q, out->residual_norms, mon);
     out->max_speed = mon[0];
     out->mean_tke = mon[1];
+    if (tc->ss) {
+        /* the third monitor (Simplec.cpp:405-408): the mean u* of the domain columns */
+        double su = 0;
+        for (int j = 0; j < g->ny; ++j) {
+            for (int i = 0; i < g->nx; ++i) { su += tc->ss[0][(int64_t)(i + g->ng) + (int64_t)(j + g->ng) * g->sy]; }
+        }
+        out->mean_ustar = su / ((double)g->nx * g->ny);
+    }
     double* F[3] = {zalloc(g), zalloc(g), zalloc(g)};
     og_transport_fluxes(g, q->u, q->v, q->w, q->z_nd, m->ax, m->ay, F[0], F[1], F[2]);
     double* dcc = zalloc(g);

@@ -313,3 +313,15 @@ def terrain_simplec_case(nx, ny, nz, periodic_x, periodic_y, hill=60.0, dx=40.0,
         case.q[f][v] = val
         seam_sync(g, loc, case.q[f])
     return case
+
+
+def case_from_instance(inst):
+    """An oracle.Case of a workloads.Instance: its node heights and metrics,
+    diffusivities, initial state and roughness map."""
+    import oracle
+    g = inst.grid
+    J, ax, ay, az, _ = oracle.metrics(g, inst.z)
+    case = oracle.Case(g, inst.z, J, ax, ay, az, inst.nu, inst.gamma_theta, inst.gamma_tke,
+                       None if inst.z0map is None else np.array(inst.z0map, dtype=np.float64))
+    case.q = {f: a.copy() for f, a in inst.q.items()}
+    return case

@@ -413,3 +413,28 @@ def test_gpu_damping_matches_oracle(ctx):
             ref, got = case.q[f][v], dc.host(f)[v]
             assert np.abs(got - ref).max() <= 1e-9 * max(np.abs(ref).max(), 1e-300), (it, f)
     st.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("damping", [False, True])
+def test_gpu_implicit_rows_match_oracle(ctx, damping):
+    """implicit_rows of u, v, w, theta and k with the closure, the wall rows
+    and (with damping) the Rayleigh layer and the sponge on the diagonal:
+    every coefficient equal to the oracle's (1e-11 relative)."""
+    case, bc, ph = _hill_case()
+    if damping:
+        bc.rayleigh_zdamp, bc.rayleigh_dampcoef, bc.rayleigh_fields = 400.0, 0.1, 31
+        bc.sponge_width, bc.sponge_strength = 120.0, 0.05
+    dc, st = _stage(ctx, case, bc, ph)
+    oracle.fill_ghosts(case, bc, ph)
+    _, cf, ss = oracle.residual(case, bc, ph, fields=True)
+    st.fill_ghosts()
+    st.residual()
+    for eq, loc in ((0, 1), (1, 2), (2, 4), (4, 0), (5, 0)):
+        A_ref = oracle.implicit_rows(case, bc, ph, eq, cf, ss)
+        A = st.implicit_rows(eq).cpu().numpy()
+        v = case.grid.valid(loc)
+        for c in range(7):
+            ref, got = A_ref[c][v], A[c][v]
+            assert np.abs(got - ref).max() <= 1e-11 * max(np.abs(ref).max(), 1e-300), (eq, c, np.abs(got - ref).max())
+    st.close()
