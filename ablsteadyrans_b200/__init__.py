@@ -220,6 +220,9 @@ def _declare_poisson(L):
     G = ctypes.POINTER(GbGrid)
     L.gb_mesh_metrics.argtypes = [P, G, P, P, P, P, P, P]
     L.gb_face_divergence.argtypes = [P, G, P, P, P, P, P, P, P, P]
+    from .abi import MeshFields, State
+    L.gb_restrict_state.argtypes = [P, G, ctypes.POINTER(State), ctypes.POINTER(MeshFields), G, ctypes.POINTER(State),
+                                    ctypes.POINTER(MeshFields), P]
     L.gb_poisson_options_default.argtypes = [ctypes.POINTER(PoissonOptions)]
     L.gb_poisson_create.argtypes = [P, G, ctypes.POINTER(ctypes.c_int32), P, P, ctypes.POINTER(PoissonOptions),
                                     ctypes.POINTER(P)]
@@ -255,6 +258,19 @@ def mesh_metrics(ctx, grid, z_nd):
     out = [_zeros(grid) for _ in range(5)]
     check(_lib_full().gb_mesh_metrics(ctx.handle, ctypes.byref(grid.c), _ptr(z_nd), *[_ptr(t) for t in out]))
     return out
+
+
+def restrict_state(ctx, fine, coarse):
+    """gust::restrict_state (Source/Transfer.H:94-110): the state of a
+    DeviceCase `fine` onto the coarser DeviceCase `coarse` (u, v with their
+    ghost layer filled); returns the coarse Omega (a device tensor)."""
+    L = _lib_full()
+    om = _zeros(coarse.grid)
+    sf, sc = fine.state(), coarse.state()
+    mf, mc = fine.mesh(), coarse.mesh()
+    check(L.gb_restrict_state(ctx.handle, ctypes.byref(fine.grid.c), ctypes.byref(sf), ctypes.byref(mf),
+                              ctypes.byref(coarse.grid.c), ctypes.byref(sc), ctypes.byref(mc), _ptr(om)))
+    return om
 
 
 def face_divergence(ctx, grid, ax, ay, az, J, fx, fy, fz, out=None):

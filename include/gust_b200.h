@@ -495,6 +495,19 @@ typedef struct gb_prolong_result {
 gb_status gb_simplec_prolong(gb_simplec* s, const gb_state* q, const gb_grid* gc, const gb_state* qc, double reltol,
                              gb_prolong_result* r);
 
+/* restrict_state (Source/Transfer.H:94-110, Transfer.cpp:199-286): the fine
+ * state qf on grid gf (mesh mf: detJ and the face areas) onto the coarse
+ * state qc on gc (mesh mc: its face areas; coarser by a power of two in x
+ * and y, the same layers and periodicity). theta, k, p': the detJ-weighted
+ * means of the fine cells; u, v: the fine face fluxes a q summed over the
+ * coarse face, per unit width, over the coarse area; w from the restricted
+ * vertical flux Omega (a_z Omega summed over r^2 fine z-faces, over the
+ * coarse a_z), the coarse u and v read with zero-gradient rows below the
+ * ground and above the top. qf's u and v need one ghost layer (the
+ * stage's ghost fill). omega_c (may be NULL) receives the coarse Omega. */
+gb_status gb_restrict_state(gb_ctx* ctx, const gb_grid* gf, const gb_state* qf, const gb_mesh_fields* mf,
+                            const gb_grid* gc, const gb_state* qc, const gb_mesh_fields* mc, double* omega_c);
+
 /* gust::local_dtau (Source/PseudoTime.H:32-33) with the stage's diffusivity nu. */
 gb_status gb_local_dtau(gb_simplec* s, const gb_state* q, double cfl, double* dtau);
 

@@ -253,6 +253,8 @@ def _declare_simplec(L):
     L.og_implicit_rows2.argtypes = [G, ctypes.POINTER(BC), ctypes.POINTER(Physics), i32, P, P, P, P, P,
                                     ctypes.POINTER(Diffusivities), PP, PP, P]
     L.og_prolong_fields.argtypes = [G, ctypes.POINTER(State), G, ctypes.POINTER(State), i32]
+    L.og_restrict_state.argtypes = [G, ctypes.POINTER(State), ctypes.POINTER(MeshFields), G, ctypes.POINTER(State),
+                                    ctypes.POINTER(MeshFields), i32, P]
     L.og_prolong_state.argtypes = [G, ctypes.POINTER(State), G, ctypes.POINTER(State), i32, ctypes.POINTER(BC),
                                    ctypes.POINTER(Physics), ctypes.POINTER(SimplecOptions), ctypes.POINTER(MeshFields),
                                    f64, ctypes.POINTER(f64)]
@@ -404,6 +406,18 @@ def prolong_fields(coarse, fine, r):
     coarse case's valid points, r the ratio of the cell sizes."""
     sc, sf = coarse.state(), fine.state()
     _L().og_prolong_fields(ctypes.byref(coarse.grid.c), ctypes.byref(sc), ctypes.byref(fine.grid.c), ctypes.byref(sf), int(r))
+
+
+def restrict_state(fine, coarse, r):
+    """restrict_state (Transfer.cpp:199-286) of the fine case's state into
+    the coarse case's; returns the coarse Omega. The fine u and v need one
+    ghost layer."""
+    om = coarse.grid.np_zeros()
+    sf, sc = fine.state(), coarse.state()
+    mf, mc = fine.mesh(), coarse.mesh()
+    _L().og_restrict_state(ctypes.byref(fine.grid.c), ctypes.byref(sf), ctypes.byref(mf), ctypes.byref(coarse.grid.c),
+                           ctypes.byref(sc), ctypes.byref(mc), int(r), _p(om))
+    return om
 
 
 def prolong_state(coarse, fine, r, bc, phys, opts, reltol=1e-10):

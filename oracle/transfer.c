@@ -1,6 +1,7 @@
 /*
  * ORACLE -- test infrastructure, not product code. FP64 C restatement of the
- * prolongation of grid sequencing (Source/Transfer.cpp): the locate/axis
+ * transfers of grid sequencing (Source/Transfer.cpp): the restriction
+ * (restrict_state, :150-286), and for the prolongation the locate/axis
  * arithmetic (:20-84), the bilinear interpolation per zeta-level (:86-108),
  * prolong_fields (:290-320) and prolong_state (:322-385): k clipped at the
  * floor, the fine level's ghost fill, the projection by the pressure
@@ -157,4 +158,100 @@ int og_prolong_state(const og_grid* gc, const gb_state* qc, const og_grid* gf, g
     for (int c = 0; c < 3; ++c) { free(dd[c]); }
     free(pkeep);
     return st;
+}
+
+void og_omega_from_w(const og_grid* g, const double* u, const double* v, const double* w, const double* z, double* om,
+                     int ngrow);
+void og_w_from_omega(const og_grid* g, const double* u, const double* v, const double* om, const double* z, double* w);
+
+/* restrict_state (Transfer.cpp:199-286): the fine state onto the coarse
+ * level r times coarser in x and y. Cell fields: the detJ-weighted means
+ * (restrict_cells, :112-132); u, v: the r fine face fluxes summed over r,
+ * over the coarse area (restrict_faces, :134-155); Omega: the r x r fine
+ * z-face fluxes over r^2, over the coarse a_z (restrict_zfaces, :157-175);
+ * w from it with the coarse u and v read with zero-gradient rows
+ * (zero_gradient_rows, :177-197). omega_c (may be NULL) receives the coarse
+ * Omega. */
+void og_restrict_state(const og_grid* gf, const gb_state* qf, const gb_mesh_fields* mf, const og_grid* gc, gb_state* qc,
+                       const gb_mesh_fields* mc, int r, double* omega_c)
+{
+    const double* src[3] = {qf->theta, qf->tke, qf->p};
+    double* dst[3] = {qc->theta, qc->tke, qc->p};
+    for (int n = 0; n < 3; ++n) {
+        for (int k = 0; k < gc->nz; ++k) {
+            for (int J = 0; J < gc->ny; ++J) {
+                for (int I = 0; I < gc->nx; ++I) {
+                    double sjq = 0, sj = 0;
+                    for (int b = 0; b < r; ++b) {
+                        for (int a = 0; a < r; ++a) {
+                            const double w = mf->detJ[IX(gf, r * I + a, r * J + b, k)];
+                            sjq += w * src[n][IX(gf, r * I + a, r * J + b, k)];
+                            sj += w;
+                        }
+                    }
+                    dst[n][IX(gc, I, J, k)] = sjq / sj;
+                }
+            }
+        }
+    }
+    const double rinv = 1.0 / (double)r;
+    for (int k = 0; k < gc->nz; ++k) {
+        for (int J = 0; J < gc->ny; ++J) {
+            for (int I = 0; I <= gc->nx; ++I) {
+                double s = 0;
+                for (int b = 0; b < r; ++b) { s += mf->ax[IX(gf, r * I, r * J + b, k)] * qf->u[IX(gf, r * I, r * J + b, k)]; }
+                const double c = s * rinv;
+                qc->u[IX(gc, I, J, k)] = c / mc->ax[IX(gc, I, J, k)];
+            }
+        }
+        for (int J = 0; J <= gc->ny; ++J) {
+            for (int I = 0; I < gc->nx; ++I) {
+                double s = 0;
+                for (int b = 0; b < r; ++b) { s += mf->ay[IX(gf, r * I + b, r * J, k)] * qf->v[IX(gf, r * I + b, r * J, k)]; }
+                const double c = s * rinv;
+                qc->v[IX(gc, I, J, k)] = c / mc->ay[IX(gc, I, J, k)];
+            }
+        }
+    }
+    const int64_t vf = VOL(gf), vc = VOL(gc);
+    double* omf = (double*)calloc(vf, sizeof(double));
+    og_omega_from_w(gf, qf->u, qf->v, qf->w, qf->z_nd, omf, 0);
+    double* omc = (double*)calloc(vc, sizeof(double));
+    const double r2inv = 1.0 / (double)(r * r);
+    for (int k = 0; k <= gc->nz; ++k) {
+        for (int J = 0; J < gc->ny; ++J) {
+            for (int I = 0; I < gc->nx; ++I) {
+                double s = 0;
+                for (int b = 0; b < r; ++b) {
+                    for (int a = 0; a < r; ++a) {
+                        s += mf->az[IX(gf, r * I + a, r * J + b, k)] * omf[IX(gf, r * I + a, r * J + b, k)];
+                    }
+                }
+                const double c = s * r2inv;
+                omc[IX(gc, I, J, k)] = c / mc->az[IX(gc, I, J, k)];
+            }
+        }
+    }
+    double* u1 = (double*)malloc(sizeof(double) * (size_t)vc);
+    double* v1 = (double*)malloc(sizeof(double) * (size_t)vc);
+    memcpy(u1, qc->u, sizeof(double) * (size_t)vc);
+    memcpy(v1, qc->v, sizeof(double) * (size_t)vc);
+    for (int j = 0; j < gc->ny; ++j) {
+        for (int i = 0; i <= gc->nx; ++i) {
+            u1[IX(gc, i, j, -1)] = u1[IX(gc, i, j, 0)];
+            u1[IX(gc, i, j, gc->nz)] = u1[IX(gc, i, j, gc->nz - 1)];
+        }
+    }
+    for (int j = 0; j <= gc->ny; ++j) {
+        for (int i = 0; i < gc->nx; ++i) {
+            v1[IX(gc, i, j, -1)] = v1[IX(gc, i, j, 0)];
+            v1[IX(gc, i, j, gc->nz)] = v1[IX(gc, i, j, gc->nz - 1)];
+        }
+    }
+    og_w_from_omega(gc, u1, v1, omc, qc->z_nd, qc->w);
+    if (omega_c) { memcpy(omega_c, omc, sizeof(double) * (size_t)vc); }
+    free(omf);
+    free(omc);
+    free(u1);
+    free(v1);
 }

@@ -289,6 +289,132 @@ def test_prolongation_and_projection_is_divergence_free(hill):
     assert np.array_equal(cf.q["theta"][v], ref.q["theta"][v])
 
 
+# ------------------------------------------------------------ restriction ---
+
+def _three_levels(hill):
+    faces = (abi.FACE_INFLOW, abi.FACE_PERIODIC, abi.FACE_SLIP_WALL, abi.FACE_OUTFLOW, abi.FACE_PERIODIC,
+             abi.FACE_SLIP_WALL)
+    inst = workloads.config1(16, 16, 6, turbulence=False)
+    if not hill:
+        inst.ground = np.zeros_like(inst.ground)
+    else:
+        inst.ground = workloads.node_ground(inst.grid, lambda x, y: 90.0 * math.exp(-((x - 200) ** 2 + (y - 210) ** 2) / 120.0 ** 2))
+    inst.z = workloads.btf_heights(inst.grid, inst.zlevels, inst.ground)
+    inst.bc = abi.BC.make(faces, theta_ref=((0.0, 1500.0), (300.0, 300.0)), ustar=inst.ustar, z0=inst.z0)
+    inst.physics = abi.Physics.make(1500.0)
+    return inst, hierarchy.build(inst, 3, 1)
+
+
+@pytest.mark.parametrize("hill", [False, True])
+def test_restriction_conserves_face_flux(hill):
+    """Each coarse face carries the sum of its fine faces' fluxes, each coarse
+    cell the detJ-weighted mean of its fine cells, and r^2 J_c D_c = sum J_f
+    D_f for the divergence (Transfer.RestrictionConservesFaceFlux)."""
+    inst, levels = _three_levels(hill)
+    for lf, lc in ((0, 1), (1, 2), (0, 2)):
+        r = 1 << (lc - lf)
+        cf, cc = case_from_instance(levels[lf].inst), case_from_instance(levels[lc].inst)
+        _smooth_state(cf, 20 + lf + lc)
+        oracle.fill_ghosts(cf, inst.bc, inst.physics)
+        om_c = oracle.restrict_state(cf, cc, r)
+        gf, gc = cf.grid, cc.grid
+        G = gf.ng
+        F = lambda a, i, j, k: a[k + G, j + G, i + G]        # noqa: E731
+        om_f = oracle.omega_from_w(gf, cf.q["u"], cf.q["v"], cf.q["w"], cf.z)
+        ex = sx = ey = ez = sz = 0.0
+        areas_differ = False
+        for k in range(gc.nz):
+            for J in range(gc.ny):
+                for I in range(gc.nx + 1):
+                    s = sum(F(cf.ax, r * I, r * J + b, k) * F(cf.q["u"], r * I, r * J + b, k) for b in range(r))
+                    sa = sum(F(cf.ax, r * I, r * J + b, k) for b in range(r))
+                    ex = max(ex, abs(F(cc.ax, I, J, k) * F(cc.q["u"], I, J, k) * r - s))
+                    sx = max(sx, abs(s))
+                    areas_differ |= abs(sa - r * F(cc.ax, I, J, k)) > 1e-3 * sa
+            for J in range(gc.ny + 1):
+                for I in range(gc.nx):
+                    s = sum(F(cf.ay, r * I + a, r * J, k) * F(cf.q["v"], r * I + a, r * J, k) for a in range(r))
+                    ey = max(ey, abs(F(cc.ay, I, J, k) * F(cc.q["v"], I, J, k) * r - s))
+        for k in range(gc.nz + 1):
+            for J in range(gc.ny):
+                for I in range(gc.nx):
+                    s = sum(F(cf.az, r * I + a, r * J + b, k) * F(om_f, r * I + a, r * J + b, k)
+                            for b in range(r) for a in range(r))
+                    ez = max(ez, abs(F(cc.az, I, J, k) * F(om_c, I, J, k) * r * r - s))
+                    sz = max(sz, abs(s))
+        assert ex < 1e-12 * sx and ey < 1e-12 * sx and ez < 1e-12 * sz
+        assert sz > 1e-3 * sx
+        assert areas_differ == hill
+        v = gc.valid(0)
+        Jf = cf.J[gf.valid(0)].reshape(gc.nz, gc.ny, r, gc.nx, r)
+        for f in ("theta", "tke", "p"):
+            qf = cf.q[f][gf.valid(0)].reshape(gc.nz, gc.ny, r, gc.nx, r)
+            mean = (Jf * qf).sum(axis=(2, 4)) / Jf.sum(axis=(2, 4))
+            assert np.abs(cc.q[f][v] - mean).max() < 4e-15 * np.abs(mean).max() * 10
+        Df = oracle.velocity_divergence(gf, cf.q["u"], cf.q["v"], cf.q["w"], cf.z, cf.ax, cf.ay, cf.az, cf.J)
+        Dc = oracle.face_divergence(gc, cc.ax, cc.ay, cc.az, cc.J, cc.q["u"], cc.q["v"], om_c)
+        sJD = (cf.J * Df)[gf.valid(0)].reshape(gc.nz, gc.ny, r, gc.nx, r).sum(axis=(2, 4))
+        ed = np.abs(r * r * cc.J[v] * Dc[v] - sJD).max()
+        dscale = sx / gc.dx * r
+        assert ed < 1e-12 * dscale and np.abs(sJD).max() > 1e-3 * dscale
+
+
+def _smooth1(c, I, N, periodic):
+    if not periodic and (I == 0 or I == N - 1):
+        return c(I)
+    im = (I - 1 + N) % N if periodic else I - 1
+    ip = (I + 1) % N if periodic else I + 1
+    return (c(im) + 6 * c(I) + c(ip)) / 8
+
+
+@pytest.mark.parametrize("px", [False, True])
+def test_round_trip_is_the_closed_form_smoother(px):
+    """restrict(prolong(c)) on flat ground for r = 2 is S_x S_y with
+    (S c)_I = (c_{I-1} + 6 c_I + c_{I+1}) / 8 in the interior and across a
+    periodic seam, c_I next to a non-periodic face, and 1 along a nodal
+    direction (Transfer.RoundTripIsTheClosedFormSmoother)."""
+    faces = (abi.FACE_PERIODIC if px else abi.FACE_INFLOW, abi.FACE_INFLOW if px else abi.FACE_PERIODIC,
+             abi.FACE_SLIP_WALL, abi.FACE_PERIODIC if px else abi.FACE_OUTFLOW,
+             abi.FACE_OUTFLOW if px else abi.FACE_PERIODIC, abi.FACE_SLIP_WALL)
+    inst = workloads.config1(16, 16, 4, turbulence=False)
+    inst.grid = Grid(16, 16, 4, inst.grid.dx, inst.grid.dy, inst.grid.dzeta, px, not px)
+    inst.ground = np.zeros((19, 19))
+    inst.z = workloads.btf_heights(inst.grid, inst.zlevels[:5] if len(inst.zlevels) > 5 else inst.zlevels, inst.ground)
+    inst.bc = abi.BC.make(faces, theta_ref=((0.0, 1500.0), (300.0, 300.0)))
+    l0, l1 = hierarchy.build(inst, 2, 1)
+    cc, cf, back = case_from_instance(l1.inst), case_from_instance(l0.inst), case_from_instance(l1.inst)
+    g = cc.grid
+    rng = np.random.default_rng(5)
+    for f in FIELDS:
+        v = g.valid(LOCS[f])
+        cc.q[f][v] = 1.0 + 1e-5 * rng.standard_normal(cc.q[f][v].shape)
+        seam_sync(g, LOCS[f], cc.q[f])
+    oracle.prolong_fields(cc, cf, 2)
+    for f in ("u", "v"):
+        seam_sync(cf.grid, LOCS[f], cf.q[f])
+        oracle.fill_periodic(cf.grid, LOCS[f], cf.q[f])
+    oracle.restrict_state(cf, back, 2)
+    G = g.ng
+    for f in FIELDS:
+        loc = LOCS[f]
+        nx_, ny_ = (loc & 1) == 1, (loc & 2) == 2
+        hc = cc.q[f]
+        err = change = scale = 0.0
+        for k in range(g.nz + ((loc >> 2) & 1)):
+            for J in range(g.ny + ny_):
+                for I in range(g.nx + nx_):
+                    def sx(jj):
+                        if nx_:
+                            return hc[k + G, jj + G, I + G]
+                        return _smooth1(lambda ii: hc[k + G, jj + G, ii + G], I, g.nx, px)
+                    ex = sx(J) if ny_ else _smooth1(sx, J, g.ny, not px)
+                    err = max(err, abs(back.q[f][k + G, J + G, I + G] - ex))
+                    change = max(change, abs(ex - hc[k + G, J + G, I + G]))
+                    scale = max(scale, abs(ex))
+        assert err < 2e-14 * scale, (f, err)
+        assert change > 1e-7, f
+
+
 # ------------------------------------------------------------------ GPU ---
 
 @pytest.mark.gpu
@@ -361,3 +487,27 @@ def test_gpu_sequencing_runs_coarse_to_fine(ctx):
     finally:
         driver.close()
         stage.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("hill", [False, True])
+def test_gpu_restrict_matches_oracle(ctx, hill):
+    """gb_restrict_state against the oracle's restrict_state, every field and
+    the coarse Omega."""
+    import ablsteadyrans_b200 as gb
+    from ablsteadyrans_b200.simplec import DeviceCase
+    inst, levels = _three_levels(hill)
+    for lf, lc in ((0, 1), (0, 2)):
+        cf, cc = case_from_instance(levels[lf].inst), case_from_instance(levels[lc].inst)
+        _smooth_state(cf, 30 + lc)
+        oracle.fill_ghosts(cf, inst.bc, inst.physics)
+        dcf, dcc = DeviceCase.from_oracle(cf), DeviceCase.from_oracle(cc)
+        om = gb.restrict_state(ctx, dcf, dcc).cpu().numpy()
+        om_ref = oracle.restrict_state(cf, cc, 1 << (lc - lf))
+        gc = cc.grid
+        for f in FIELDS:
+            v = gc.valid(LOCS[f])
+            ref, got = cc.q[f][v], dcc.host(f)[v]
+            assert np.abs(got - ref).max() <= 1e-13 * max(np.abs(ref).max(), 1e-300), (f, lf, lc)
+        v = gc.valid(4)
+        assert np.abs(om[v] - om_ref[v]).max() <= 1e-13 * np.abs(om_ref[v]).max()
