@@ -172,3 +172,92 @@ def sequencing_report(levels, finest_iterations, finest_status):
             lines.append(f"         prolonged into level {s.level}: divergence {p.divergence_before:.3e} -> "
                          f"{p.divergence_after:.3e}, {p.tke_clipped} k values clipped")
     return "\n".join(lines)
+
+
+def _finest(ctx, inst):
+    import torch
+
+    import ablsteadyrans_b200 as gb
+    from .simplec import DeviceCase, SimplecStage
+    g = inst.grid
+    z = torch.from_numpy(inst.z).cuda()
+    J, ax, ay, az, _ = gb.mesh_metrics(ctx, g, z)
+    case = DeviceCase(g, z, J, ax, ay, az, inst.nu, inst.gamma_theta, inst.gamma_tke, inst.q, inst.z0map)
+    return case, SimplecStage(ctx, case, inst.bc, inst.physics, inst.options)
+
+
+def compare(inst_fn, levels, max_iterations, seq=None):
+    """One steady solve of inst_fn() without and one with grid sequencing
+    over `levels` levels (the C++ driver on every level); returns a dict of
+    iterations, seconds and the per-field difference of the two solutions."""
+    import time
+
+    import numpy as np
+    import torch
+
+    import ablsteadyrans_b200 as gb
+    from .simplec import NativeDriver, run_drivers
+    seq = seq or abi.SequencingOptions.make(enabled=1)
+    out = {}
+    fields = {}
+    for mode in ("plain", "sequenced"):
+        inst = inst_fn()
+        ctx = gb.Context()
+        case, stage = _finest(ctx, inst)
+        driver = NativeDriver(stage)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        summary = None
+        if mode == "plain":
+            stage.initialize()
+        else:
+            summary = sequence_coarse_levels(ctx, inst, levels, seq, stage, driver, max_iterations=max_iterations)
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        (verdict, n), = run_drivers([driver], max_iterations, 1)
+        torch.cuda.synchronize()
+        t2 = time.perf_counter()
+        rec = {"verdict": verdict, "level0_iterations": n, "seconds": t2 - t0, "level0_seconds": t2 - t1}
+        if summary is not None:
+            rec["levels"] = [{"level": s.level, "cells": list(s.cells), "iterations": s.iterations, "stop": s.stop,
+                              "divergence": ([s.prolong.divergence_before, s.prolong.divergence_after]
+                                             if s.prolonged else None)} for s in summary]
+            rec["coarse_seconds"] = t1 - t0
+            # work in level-0 iterations: a level-l iteration costs 4^-l of one
+            rec["work_level0_iterations"] = n + sum(s.iterations / 4.0 ** s.level for s in summary if s.level > 0)
+        out[mode] = rec
+        fields[mode] = {f: t.cpu().numpy() for f, t in case.q.items()}
+        driver.close()
+        stage.close()
+        ctx.close()
+    g = inst.grid
+    valid = {"u": g.valid(1), "v": g.valid(2), "w": g.valid(4), "p": g.valid(0), "theta": g.valid(0),
+             "tke": g.valid(0)}
+    out["sequenced_vs_plain_rel_difference"] = {
+        f: float(np.abs(fields["sequenced"][f][sl] - fields["plain"][f][sl]).max()
+                 / max(np.abs(fields["plain"][f][sl]).max(), 1e-300)) for f, sl in valid.items()}
+    return out
+
+
+def main(argv=None):
+    """Grid sequencing against a plain solve on config 1 (the 150 m hill):
+    python -m ablsteadyrans_b200.sequencing --levels 3 --max-iterations 6000"""
+    import argparse
+    import json
+
+    from . import workloads
+    ap = argparse.ArgumentParser(description="grid sequencing against a plain steady solve")
+    ap.add_argument("--levels", type=int, default=3)
+    ap.add_argument("--max-iterations", type=int, default=6000)
+    ap.add_argument("--nx", type=int, default=128)
+    ap.add_argument("--nz", type=int, default=64)
+    args = ap.parse_args(argv)
+    out = {"workload": f"config 1: 150 m Gaussian hill {args.nx}x{args.nx}x{args.nz}, dx 25 m, the k-L closure and "
+                       "the surface layer", "levels": args.levels}
+    out.update(compare(lambda: workloads.config1(args.nx, args.nx, args.nz), args.levels, args.max_iterations))
+    print(json.dumps(out))
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())
