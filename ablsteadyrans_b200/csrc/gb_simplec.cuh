@@ -24,5 +24,12 @@ gb_ctx* simplec_ctx(const gb_simplec* S);
 const gb_physics& simplec_physics(const gb_simplec* S);
 //! Whether the ground is a surface-layer face (the wall model's state).
 bool simplec_has_wall(const gb_simplec* S);
+const gb_simplec_opts& simplec_options(const gb_simplec* S);
+//! theta_ref at the cell centres (the stage's reference profile).
+const double* simplec_theta_ref(const gb_simplec* S);
+//! The Dirichlet rows (1, else 0) of velocity component c on its valid faces.
+void simplec_dirichlet_rows(gb_simplec* S, int c, double* mask);
+//! dtau on the x-, y- and z-faces from the cell dtau (face_dtau, Predictor.H).
+void simplec_face_dtau(gb_simplec* S, const double* dtau, double** faces);
 
 }  // namespace gb

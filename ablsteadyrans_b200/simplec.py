@@ -151,6 +151,17 @@ class SimplecStage:
         check(self._L.gb_local_dtau(self._h, ctypes.byref(st), float(cfl), ctypes.c_void_p(dt.data_ptr())))
         return dt
 
+    def local_dtau_of(self, state, cfl, out):
+        """local_dtau at another state of this stage's grid (an abi.State)."""
+        from . import check
+        check(self._L.gb_local_dtau(self._h, ctypes.byref(state), float(cfl), ctypes.c_void_p(out.data_ptr())))
+        return out
+
+    def _fill_state(self, state):
+        """The ghost fill of another state of this stage's grid (an abi.State)."""
+        from . import check
+        check(self._L.gb_simplec_fill_ghosts(self._h, ctypes.byref(state)))
+
     def iterate(self, dtau):
         from . import check
         info = abi.IterInfo()

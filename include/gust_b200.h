@@ -527,6 +527,58 @@ typedef struct gb_driver_opts {
     int32_t monitor_window;          /* steady.monitor_window (>= 2) */
 } gb_driver_opts;
 
+/* ---- the Newton-Krylov finishing stage ---------------------------------- */
+
+/* steady.newton_* of the Newton-Krylov core (gust::NewtonOptions, Source/
+ * Newton.H:84-107) and the pressure scale of its scaled variables
+ * (JvpScales::pressure, Source/Residual.H:72-80). */
+typedef struct gb_newton_opts {
+    int32_t gmres_restart;           /* steady.newton_gmres_restart (5..200; 30) */
+    int32_t gmres_max_iters;         /* steady.newton_gmres_max_iters (>= 1; 2000) */
+    double fd_eps_scale;             /* steady.newton_fd_eps_scale (eps^(3/4) .. 1e-2; sqrt(eps)) */
+    double krylov_rtol;              /* steady.newton_krylov_rtol ((0, 1); 1e-2) */
+    double scale_pressure;           /* s_p (100 m^2/s^2) */
+} gb_newton_opts;
+/* What one Newton step did (gust::NewtonStepInfo, Source/Newton.H:230-248). */
+typedef struct gb_newton_step_info {
+    int32_t gmres_iterations;
+    int32_t gmres_status;            /* 0 converged, 1 the iteration cap */
+    double residual_norm;            /* |b| = |T^-1 R(q)|_2 before the step */
+    double krylov_residual;          /* FGMRES's final |b - A x|_2 (its Arnoldi estimate) */
+    double krylov_relative;          /* krylov_residual / residual_norm */
+    double eps_min, eps_max;         /* the jvp steps used */
+    int32_t jvp_calls;
+    int32_t applied;                 /* the update was usable (newton_update_usable) */
+} gb_newton_step_info;
+typedef struct gb_newton gb_newton;
+gb_status gb_newton_options_default(gb_newton_opts* o);
+/* check_newton_options (Source/Newton.cpp): each violation names its key. */
+gb_status gb_newton_check(const gb_newton_opts* o);
+/* gust::NewtonKrylov on a stage (its residual, ghost fill and scales;
+ * check_newton_options' range checks name their keys). Allocates
+ * 2 restart + 13 state-sized vectors. */
+gb_status gb_newton_create(gb_simplec* s, const gb_newton_opts* o, gb_newton** out);
+gb_status gb_newton_destroy(gb_newton* n);
+/* gust::jvp with the refill (Source/Residual.cpp:324-396): Jv = (R(fill(q +
+ * eps v)) - R(q)) / eps, eps = h (1 + mean |q~|) / rms(v~) over the owned
+ * points of the six fields; q's ghost cells are filled first. v and Jv: six
+ * device arrays each (u, v, w, p, theta, k) on the grid layout, v's ghost
+ * cells 0. */
+gb_status gb_newton_jvp(gb_newton* n, const gb_state* q, double* const* v, double* const* Jv, double* eps);
+/* NewtonKrylov::step (Source/Newton.H:292-298): q += dq from (D + J) dq =
+ * -R(q) (dtau NULL: plain Newton), skipped when the update is not usable;
+ * q's ghost cells filled before and after. */
+gb_status gb_newton_step(gb_newton* n, const gb_state* q, const double* dtau, gb_newton_step_info* info);
+/* NewtonKrylov::direction: the same solve, dq (six device arrays) = S x on
+ * the valid points (0 when not usable), q unchanged but its ghost fill. */
+gb_status gb_newton_direction(gb_newton* n, const gb_state* q, const double* dtau, double* const* dq,
+                              gb_newton_step_info* info);
+/* NewtonKrylov::residual_norm: |T^-1 R(fill(q))|_2 (the line search's norm). */
+gb_status gb_newton_residual_norm(gb_newton* n, const gb_state* q, double* norm);
+/* The continuation's trial point: out = q0 + lambda dq on the valid points
+ * (k clipped at the stage's tke_floor), q0's ghost cells copied. */
+gb_status gb_newton_trial(gb_newton* n, const gb_state* q0, double* const* dq, double lambda, const gb_state* out);
+
 /* ---- the steady criterion ------------------------------------------------ */
 
 /* gust::SteadyCriterion (Source/SteadyCriterion.H:81-150): residual

@@ -1,0 +1,230 @@
+"""The Newton-Krylov finishing stage: the continuation's line search, SER
+ramp and retries on known answers (test_Continuation.cpp), the option checks,
+and on the GPU the jvp against the oracle's residual difference, Poiseuille
+in one Newton step (test_Newton.cpp) and continuation steps that reduce |R|
+over a hill with the closure and the wall law."""
+import math
+import sys
+
+import numpy as np
+import pytest
+
+import oracle
+from ablsteadyrans_b200 import GustError
+from ablsteadyrans_b200.driver import ser_cfl
+from ablsteadyrans_b200.newton import (ContinuationOptions, ContinuationState, NewtonOptions, armijo_accepts,
+                                       armijo_line_search, check_continuation_options, check_newton_options,
+                                       continuation_after_accept, continuation_after_failure, line_search_growth)
+
+FIELDS = ("u", "v", "w", "p", "theta", "tke")
+LOCS = (1, 2, 4, 0, 0, 0)
+
+
+@pytest.mark.parametrize("K,c,beta,lmin,lam,nb,acc", [(3, 1e-4, 0.5, 1e-2, 0.25, 2, True),
+                                                      (3, 1e-4, 0.3, 1e-2, 0.3, 1, True),
+                                                      (0.5, 1e-4, 0.5, 1e-2, 1, 0, True),
+                                                      (1.5, 0.4, 0.5, 1e-2, 0.25, 2, True),
+                                                      (9, 1e-4, 0.5, 1e-2, 0.0625, 4, True),
+                                                      (100, 1e-4, 0.5, 0.05, 0.0625, 4, False)])
+def test_armijo_on_known_quadratic(K, c, beta, lmin, lam, nb, acc):
+    o = ContinuationOptions(armijo_c=c, backtrack=beta, lambda_min=lmin)
+    r = 7.0
+    calls = []
+    ls = armijo_line_search(lambda l: calls.append(l) or r * (1 - l + K * l * l), r, o)
+    lstar = (1 - c) / K
+    expect, n = 1.0, 0
+    while expect > lstar and expect * beta >= lmin:
+        expect *= beta
+        n += 1
+    assert ls.accepted == acc == (expect <= lstar)
+    assert abs(ls.lam - lam) < 1e-15 and abs(ls.lam - expect) < 1e-15
+    assert ls.backtracks == nb == n and len(calls) == n + 1
+
+
+def test_armijo_non_finite_trials_and_growth_bound():
+    o = ContinuationOptions()
+    nan, inf = float("nan"), float("inf")
+    ls = armijo_line_search(lambda l: nan if l > 0.3 else (inf if l > 0.2 else 1.0), 2.0, o)
+    assert ls.accepted and ls.lam == 0.125 and ls.backtracks == 3
+    assert not armijo_accepts(nan, 1, 1, 1e-4) and not armijo_accepts(inf, 1, 1, 1e-4)
+    assert armijo_accepts(0.5, 1, 1, 0.5) and not armijo_accepts(math.nextafter(0.5, 1), 1, 1, 0.5)
+    g = ContinuationOptions(lambda_min=0.05)
+    r = 2.0
+    for growth in (100.0, math.nextafter(100.0, 0.0), 1.0):
+        calls = []
+        lg = armijo_line_search(lambda l: calls.append(l) or r * (1 - l + 100 * l * l), r, g, growth)
+        accept = growth >= 100.0
+        assert lg.accepted == accept and lg.by_growth == accept and lg.backtracks == 4
+        assert len(calls) == (6 if accept else 5) and calls[-1] == (1.0 if accept else 0.0625)
+        if accept:
+            assert lg.lam == 1 and lg.residual == 100 * r
+    assert not armijo_line_search(lambda l: nan, r, g, 1e30).accepted
+
+
+def test_dtau_ramp_follows_ser():
+    """continuation_after_accept: the SER law from |R_n| / |R_0|, growth
+    capped, the switch to infinite dtau at cfl_max (and cfl_max as the base
+    while infinite); a failure cuts the CFL and leaves infinite dtau."""
+    o = ContinuationOptions(cfl0=1.0, cfl_max=50.0, ser_exponent=1.0, ser_max_growth=2.0)
+    st = ContinuationState(o.cfl0)
+    st.r0 = 1.0
+    cfl = o.cfl0
+    for n, rn in enumerate([0.9, 0.5, 0.2, 0.05, 0.01, 1e-3, 1e-4]):
+        expect = ser_cfl(cfl, rn, o.cfl0, o.cfl_max, o.ser_exponent, o.ser_max_growth)
+        st = continuation_after_accept(o, st, rn)
+        assert st.steps == n + 1 and st.r_last == rn and st.cfl == expect
+        assert st.infinite == (expect >= o.cfl_max)
+        cfl = expect
+    assert st.infinite
+    f = continuation_after_failure(o, st)
+    assert not f.infinite and f.cfl == o.cfl_cut * o.cfl_max
+    st2 = ContinuationState(1e-307)
+    for _ in range(5):
+        st2 = continuation_after_failure(o, st2)
+    assert st2.cfl == sys.float_info.min
+    assert line_search_growth(ContinuationOptions(ptc_growth=3.0), st) == 1.0
+    assert line_search_growth(ContinuationOptions(ptc_growth=3.0), f) == 3.0
+
+
+@pytest.mark.parametrize("key,kw", [("steady.newton_armijo_c", {"armijo_c": 0.5}),
+                                    ("steady.newton_backtrack", {"backtrack": 1.0}),
+                                    ("steady.newton_lambda_min", {"lambda_min": float("nan")}),
+                                    ("steady.newton_cfl_cut", {"cfl_cut": 0.0}),
+                                    ("steady.newton_max_retries", {"max_retries": 0}),
+                                    ("steady.newton_dtau_inf_at_cap", {"dtau_inf_at_cap": 2}),
+                                    ("steady.newton_ptc_growth", {"ptc_growth": 0.5}),
+                                    ("steady.cfl_max", {"cfl_max": 0.5})])
+def test_continuation_range_checks_name_their_keys(key, kw):
+    assert check_continuation_options(ContinuationOptions()) == []
+    err = check_continuation_options(ContinuationOptions(**kw))
+    assert len(err) == 1 and key in err[0]
+
+
+@pytest.mark.parametrize("key,kw", [("steady.newton_gmres_restart", {"gmres_restart": 4}),
+                                    ("steady.newton_gmres_restart", {"gmres_restart": 201}),
+                                    ("steady.newton_gmres_max_iters", {"gmres_max_iters": 0}),
+                                    ("steady.newton_fd_eps_scale", {"fd_eps_scale": 1e-13}),
+                                    ("steady.newton_fd_eps_scale", {"fd_eps_scale": 0.02}),
+                                    ("steady.newton_krylov_rtol", {"krylov_rtol": 1.0})])
+def test_newton_option_checks_name_their_keys(key, kw):
+    check_newton_options(NewtonOptions.make())
+    with pytest.raises(GustError, match=key.replace(".", r"\.")):
+        check_newton_options(NewtonOptions.make(**kw))
+
+
+# ------------------------------------------------------------------ GPU ---
+
+def _hill():
+    from test_turbulence import _hill_case
+    return _hill_case()
+
+
+@pytest.mark.gpu
+def test_gpu_jvp_matches_the_oracle_difference(ctx):
+    """J v on the GPU equals the oracle's (R(fill(q + eps v)) - R(fill(q))) /
+    eps at the GPU's eps (the closure and the wall law, refilled ghosts)."""
+    import torch
+    from ablsteadyrans_b200.abi import SimplecOptions
+    from ablsteadyrans_b200.newton import NewtonKrylov
+    from ablsteadyrans_b200.simplec import DeviceCase, SimplecStage
+    from helpers import seam_sync
+    case, bc, ph = _hill()
+    g = case.grid
+    rng = np.random.default_rng(3)
+    v = []
+    for f, loc in zip(FIELDS, LOCS):
+        a = g.np_zeros()
+        a[g.valid(loc)] = rng.standard_normal(a[g.valid(loc)].shape) * (0.3 if f != "p" else 3.0)
+        seam_sync(g, loc, a)
+        v.append(a)
+    dc = DeviceCase.from_oracle(case)
+    st = SimplecStage(ctx, dc, bc, ph, SimplecOptions.make())
+    nk = NewtonKrylov(st)
+    try:
+        Jv, eps = nk.jvp([torch.from_numpy(a).cuda() for a in v])
+        assert eps > 0
+        oracle.fill_ghosts(case, bc, ph)
+        R0 = oracle.residual(case, bc, ph)
+        qp = case.copy()
+        for n, f in enumerate(FIELDS):
+            qp.q[f] = case.q[f] + eps * v[n]
+        oracle.fill_ghosts(qp, bc, ph)
+        Rp = oracle.residual(qp, bc, ph)
+        for n, loc in enumerate(LOCS):
+            vv = g.valid(loc)
+            ref = (Rp[n][vv] - R0[n][vv]) / eps
+            got = Jv[n].cpu().numpy()[vv]
+            scale = max(np.abs(ref).max(), 1e-300)
+            assert np.abs(got - ref).max() <= 1e-4 * scale, (FIELDS[n], np.abs(got - ref).max() / scale)
+    finally:
+        nk.close()
+        st.close()
+
+
+@pytest.mark.gpu
+def test_gpu_poiseuille_in_one_newton_step(ctx):
+    """Laminar Poiseuille flow (R linear in the column): one plain Newton
+    step from rest with GMRES to 1e-12 gives the discrete solution to 1e-9 of
+    the peak; v and w stay 0 and theta unchanged (Newton.PoiseuilleInOneStep)."""
+    from ablsteadyrans_b200.abi import (BC, FACE_NO_SLIP_WALL, FACE_PERIODIC, Physics, SimplecOptions)
+    from ablsteadyrans_b200.newton import NewtonKrylov
+    from ablsteadyrans_b200.simplec import DeviceCase, SimplecStage
+    from helpers import flat_case
+    H, F, nu, nz = 500.0, 1e-4, 10.0, 16
+    case = flat_case(2, 2, nz, 1000.0, 1000.0, H, True, True, nu)
+    bc = BC.make((FACE_PERIODIC, FACE_PERIODIC, FACE_NO_SLIP_WALL, FACE_PERIODIC, FACE_PERIODIC, FACE_NO_SLIP_WALL),
+                 theta_ref=((-1000.0, 5000.0), (300.0, 300.0)))
+    ph = Physics.make(H, gravity=0.0, pressure_gradient=(F, 0.0, 0.0))
+    case.q["theta"][...] = 300.0
+    case.q["tke"][...] = 0.5
+    dc = DeviceCase.from_oracle(case)
+    st = SimplecStage(ctx, dc, bc, ph, SimplecOptions.make())
+    nk = NewtonKrylov(st, NewtonOptions.make(gmres_restart=100, krylov_rtol=1e-12))
+    try:
+        info = nk.step(None)
+        assert info.gmres_status == 0 and info.jvp_calls > 0 and info.applied
+        G = case.grid.ng
+        dz = H / nz
+        zc = (np.arange(nz) + 0.5) * dz
+        exact = F / (2 * nu) * (zc * (H - zc) + dz * dz / 4)
+        umax = F * H * H / (8 * nu)
+        u = dc.host("u")[G:G + nz, G:G + 2, G:G + 3]
+        assert np.abs(u - exact[:, None, None]).max() < 1e-9 * umax
+        assert np.abs(dc.host("v")[case.grid.valid(2)]).max() < 1e-12 * umax
+        assert np.abs(dc.host("w")[case.grid.valid(4)]).max() < 1e-12 * umax
+        th = dc.host("theta")[case.grid.valid(0)]
+        assert th.min() == 300.0 and th.max() == 300.0
+    finally:
+        nk.close()
+        st.close()
+
+
+@pytest.mark.gpu
+def test_gpu_continuation_reduces_the_residual(ctx):
+    """Over the hill with the closure and the wall law, after SIMPLEC
+    iterations: every accepted continuation step lowers |R| (the Armijo
+    condition), and five steps take it well below where they started."""
+    from ablsteadyrans_b200.abi import SimplecOptions
+    from ablsteadyrans_b200.newton import Continuation
+    from ablsteadyrans_b200.simplec import DeviceCase, SimplecStage
+    case, bc, ph = _hill()
+    dc = DeviceCase.from_oracle(case)
+    st = SimplecStage(ctx, dc, bc, ph, SimplecOptions.make(pressure_reltol=1e-6))
+    st.fill_ghosts()
+    for _ in range(40):
+        st.iterate(st.local_dtau(2.0))
+    cont = Continuation(st, ContinuationOptions(cfl0=2.0, cfl_max=50.0),
+                        NewtonOptions.make(gmres_restart=60, krylov_rtol=1e-3))
+    try:
+        r_start = cont.nk.residual_norm()
+        status, converged, steps = cont.run(5, 1e-12)
+        acc = [r for r in cont.records if r["outcome"] == "accepted"]
+        assert status == "accepted" and steps == 5 and len(acc) == 5
+        for r in acc:
+            assert r["residual_new"] <= (1 - 1e-4 * r["lam"]) * r["residual"]
+        assert cont.st.r_last < 0.5 * r_start
+        for f, loc in zip(FIELDS, LOCS):
+            assert np.isfinite(dc.host(f)[case.grid.valid(loc)]).all(), f
+    finally:
+        cont.close()
+        st.close()
