@@ -342,6 +342,16 @@ gb_status gb_simplec_prolong(gb_simplec* s, const gb_state* q, const gb_grid* gc
     return gb::simplec_prolong(s, *q, *gc, *qc, reltol, r);
 }
 
+gb_status gb_simplec_norms(gb_simplec* s, const gb_state* q, double* residual_norms, double* monitors)
+{
+    gb::clear_error();
+    if (s == nullptr || q == nullptr || residual_norms == nullptr || monitors == nullptr) {
+        gb::set_error("gust: stage_norms: null argument");
+        return GB_BAD_ARG;
+    }
+    return gb::simplec_norms(s, *q, residual_norms, monitors);
+}
+
 gb_status gb_simplec_implicit_rows(gb_simplec* s, const gb_state* q, int32_t eq, double* A)
 {
     gb::clear_error();

@@ -1800,6 +1800,43 @@ gb_status simplec_iterate(gb_simplec* S, const gb_state& q, const double* dtau, 
     return check_cuda("SimplecStage::iterate");
 }
 
+//! stage_norms (Simplec.cpp:385-409) at q with no iteration: the ghost fill
+//! (the wall state), the residual, the six scaled RMS norms and the monitors
+//! (max speed, mean k, mean u* with the surface layer).
+gb_status simplec_norms(gb_simplec* S, const gb_state& q, double* res, double* mon)
+{
+    gb_ctx* ctx = S->ctx;
+    const gb_grid g = S->g;
+    SimplecWork& w = S->w;
+    cudaMemsetAsync(dword(ctx, 0), 0, sizeof(unsigned long long) * W_COUNT, ctx->stream);
+    fill_ghosts_into(S, q, S->ss);
+    simplec_residual(S, q, w.R);
+    for (int n = 0; n < 6; ++n) { dsum(S, valid_box(g, kLoc[n]), w.R[n], 0, SUM_R0 + n); }
+    dsum(S, valid_box(g, CC), q.tke, 1, SUM_TKE);
+    if (S->wall) { dsum(S, Box{{0, 0, -g.ng}, {g.nx - 1, g.ny - 1, -g.ng}}, S->ss[kSsUstar], 1, SUM_USTAR); }
+    dmax(S, valid_box(g, XF), q.u, nullptr, W_MON_U);
+    dmax(S, valid_box(g, YF), q.v, nullptr, W_MON_V);
+    dmax(S, valid_box(g, ZF), q.w, nullptr, W_MON_W);
+    unsigned long long words[W_COUNT];
+    gb_status st = read_words(ctx, 0, W_COUNT, words);
+    if (st != GB_OK) { return st; }
+    double sums[8];
+    cudaMemcpyAsync(S->h_words, w.sums, sizeof(double) * 8, cudaMemcpyDeviceToHost, ctx->stream);
+    if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) { return check_cuda("stage_norms"); }
+    std::memcpy(sums, S->h_words, sizeof(double) * 8);
+    const gb_physics& ph = S->ph;
+    const double U = ph.scale_velocity, H = ph.scale_height;
+    const double scale[6] = {U * U / H, U * U / H, U * U / H, U / H, U * ph.scale_theta / H, U * ph.scale_tke / H};
+    for (int n = 0; n < 6; ++n) {
+        const Box b = valid_box(g, kLoc[n]);
+        res[n] = std::sqrt(sums[n]) / std::sqrt(static_cast<double>(b.count())) / scale[n];
+    }
+    mon[0] = std::max(std::max(bits_to_double(words[W_MON_U]), bits_to_double(words[W_MON_V])), bits_to_double(words[W_MON_W]));
+    mon[1] = sums[SUM_TKE] / (static_cast<double>(g.nx) * g.ny * g.nz);
+    mon[2] = S->wall ? sums[SUM_USTAR] / (static_cast<double>(g.nx) * g.ny) : 0.0;
+    return check_cuda("stage_norms");
+}
+
 // ------------------------------------------------------ pseudo-time step ---
 
 gb_status simplec_local_dtau(gb_simplec* S, const gb_state& q, double cfl, double* dtau)

@@ -355,3 +355,120 @@ class Continuation:
 
     def close(self):
         self.nk.close()
+
+
+# ------------------------------------------------------------ the stage ---
+
+class SwitchOptions:
+    """steady.switch_* and newton_fallback_failures of the two-stage driver
+    (Source/Driver.H:60-80): forward to Newton after switch_window
+    iterations with r_n <= switch_residual; back to SIMPLEC after
+    fallback_failures consecutive failed continuation steps."""
+
+    def __init__(self, switch_residual=1e-4, switch_window=20, fallback_failures=2):
+        self.switch_residual, self.switch_window, self.fallback_failures = switch_residual, switch_window, fallback_failures
+
+
+def solve_simplec_newton(stage, max_iterations, driver_options=None, switch=None, newton_options=None,
+                         continuation_options=None):
+    """steady.stage = simplec_newton on one stage: the native SIMPLEC driver
+    until the switch rule holds, then one continuation step per iteration
+    (started afresh at cfl_max, as the reference's Newton stage starts its
+    continuation), the run's norms and monitors at each new state into the
+    driver's criterion, back to SIMPLEC after the failures. Returns
+    (verdict, iterations, newton_iterations)."""
+    from .simplec import NativeDriver
+    d = NativeDriver(stage, driver_options)
+    crit = d.criterion
+    sw = switch or SwitchOptions()
+    o = d.options
+    copt = continuation_options or ContinuationOptions(cfl0=o.cfl_max, cfl_max=o.cfl_max,
+                                                       ser_exponent=o.ser_exponent, ser_max_growth=o.ser_max_growth)
+    mode, below, failures, newton_its = "simplec", 0, 0, 0
+    cont = None
+    n_mon = 3 if stage.bc.face[2] == abi.FACE_SURFACE_LAYER else 2
+    try:
+        for it in range(max_iterations):
+            if mode == "simplec":
+                verdict, _, _ = d.step()
+                if verdict != "running":
+                    return verdict, it + 1, newton_its
+                _, _, r = d.status()
+                below = below + 1 if r <= sw.switch_residual else 0
+                if below >= sw.switch_window:
+                    mode, failures = "newton", 0
+                    if cont is not None:
+                        cont.close()
+                    cont = Continuation(stage, copt, newton_options)
+                continue
+            status = cont.step()
+            newton_its += 1
+            failures = failures + 1 if status == "failed" else 0
+            res, mon = stage.norms()
+            crit.add(res, mon[:n_mon])
+            v = crit.verdict()
+            if v.status == abi.DIVERGED:
+                return "diverged", it + 1, newton_its
+            if v.status == abi.STEADY:
+                return "steady", it + 1, newton_its
+            if failures >= sw.fallback_failures:
+                mode, below = "simplec", 0
+        return "running", max_iterations, newton_its
+    finally:
+        if cont is not None:
+            cont.close()
+        d.close()
+
+
+def main(argv=None):
+    """SIMPLEC alone against SIMPLEC with the Newton finishing stage on the
+    config-1 hill, both to the strict criterion:
+    python -m ablsteadyrans_b200.newton --nx 64 --nz 32"""
+    import argparse
+    import json
+    import time
+
+    import torch
+
+    import ablsteadyrans_b200 as gb
+    from . import workloads
+    from .sequencing import _finest
+    from .simplec import NativeDriver, run_drivers
+    ap = argparse.ArgumentParser(description="the Newton finishing stage against SIMPLEC alone")
+    ap.add_argument("--nx", type=int, default=64)
+    ap.add_argument("--nz", type=int, default=32)
+    ap.add_argument("--max-iterations", type=int, default=4000)
+    ap.add_argument("--switch-residual", type=float, default=1e-4)
+    ap.add_argument("--switch-window", type=int, default=20)
+    ap.add_argument("--restart", type=int, default=60)
+    args = ap.parse_args(argv)
+    out = {"workload": f"config 1: 150 m Gaussian hill {args.nx}x{args.nx}x{args.nz}, dx 25 m, the k-L closure and "
+                       "the surface layer; the Newton stage's preconditioner: identity"}
+    for mode in ("simplec", "simplec_newton"):
+        inst = workloads.config1(args.nx, args.nx, args.nz)
+        ctx = gb.Context()
+        case, stage = _finest(ctx, inst)
+        stage.initialize()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        if mode == "simplec":
+            d = NativeDriver(stage)
+            (verdict, n), = run_drivers([d], args.max_iterations, 1)
+            nn = 0
+            d.close()
+        else:
+            verdict, n, nn = solve_simplec_newton(
+                stage, args.max_iterations, switch=SwitchOptions(args.switch_residual, args.switch_window),
+                newton_options=NewtonOptions.make(gmres_restart=args.restart))
+        torch.cuda.synchronize()
+        out[mode] = {"verdict": verdict, "iterations": n, "newton_iterations": nn, "seconds": time.perf_counter() - t0}
+        res, _ = stage.norms()
+        out[mode]["final_residual_norms"] = res
+        stage.close()
+        ctx.close()
+    print(json.dumps(out))
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

@@ -29,6 +29,8 @@ def _declare(L):
                                         ctypes.POINTER(abi.InitResult)]
     L.gb_simplec_turbulence.argtypes = [P, ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_void_p)]
     L.gb_simplec_implicit_rows.argtypes = [P, ctypes.POINTER(abi.State), ctypes.c_int32, P]
+    L.gb_simplec_norms.argtypes = [P, ctypes.POINTER(abi.State), ctypes.POINTER(ctypes.c_double),
+                                   ctypes.POINTER(ctypes.c_double)]
     L.gb_driver_criterion.argtypes = [P, ctypes.POINTER(P)]
     L.gb_driver_seed_reference.argtypes = [P, ctypes.POINTER(ctypes.c_double)]
     L.gb_driver_release_hold.argtypes = [P]
@@ -150,6 +152,14 @@ class SimplecStage:
         st = self.case.state()
         check(self._L.gb_local_dtau(self._h, ctypes.byref(st), float(cfl), ctypes.c_void_p(dt.data_ptr())))
         return dt
+
+    def norms(self):
+        """stage_norms at the stage's state: (six residual norms, three monitors)."""
+        from . import check
+        res, mon = (ctypes.c_double * 6)(), (ctypes.c_double * 3)()
+        st = self.case.state()
+        check(self._L.gb_simplec_norms(self._h, ctypes.byref(st), res, mon))
+        return list(res), list(mon)
 
     def local_dtau_of(self, state, cfl, out):
         """local_dtau at another state of this stage's grid (an abi.State)."""

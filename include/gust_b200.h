@@ -508,6 +508,11 @@ gb_status gb_simplec_prolong(gb_simplec* s, const gb_state* q, const gb_grid* gc
 gb_status gb_restrict_state(gb_ctx* ctx, const gb_grid* gf, const gb_state* qf, const gb_mesh_fields* mf,
                             const gb_grid* gc, const gb_state* qc, const gb_mesh_fields* mc, double* omega_c);
 
+/* stage_norms (Source/Simplec.cpp:385-409) at q with no iteration: the ghost
+ * fill, the residual, residual_norms[6] (the scaled RMS of R_u .. R_k) and
+ * monitors[3] (max speed, mean k, mean u* with a surface-layer ground, else 0). */
+gb_status gb_simplec_norms(gb_simplec* s, const gb_state* q, double* residual_norms, double* monitors);
+
 /* gust::local_dtau (Source/PseudoTime.H:32-33) with the stage's diffusivity nu. */
 gb_status gb_local_dtau(gb_simplec* s, const gb_state* q, double cfl, double* dtau);
 

@@ -228,3 +228,26 @@ def test_gpu_continuation_reduces_the_residual(ctx):
     finally:
         cont.close()
         st.close()
+
+
+@pytest.mark.gpu
+def test_gpu_simplec_newton_reaches_the_strict_criterion(ctx):
+    """steady.stage = simplec_newton over the hill: SIMPLEC until r_n has
+    stayed at or below the switch residual, then the continuation; the run
+    ends steady by the driver's own criterion, with Newton iterations."""
+    from ablsteadyrans_b200.abi import SimplecOptions
+    from ablsteadyrans_b200.newton import SwitchOptions, solve_simplec_newton
+    from ablsteadyrans_b200.simplec import DeviceCase, SimplecStage
+    case, bc, ph = _hill()
+    dc = DeviceCase.from_oracle(case)
+    st = SimplecStage(ctx, dc, bc, ph, SimplecOptions.make(pressure_reltol=1e-6))
+    st.fill_ghosts()
+    try:
+        verdict, its, newton_its = solve_simplec_newton(st, 3000, switch=SwitchOptions(1e-2, 5),
+                                                        newton_options=NewtonOptions.make(gmres_restart=60))
+        assert verdict == "steady", (verdict, its, newton_its)
+        assert newton_its > 0
+        res, _ = st.norms()
+        assert max(res) < 5e-5
+    finally:
+        st.close()
