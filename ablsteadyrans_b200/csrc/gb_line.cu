@@ -222,11 +222,14 @@ __global__ void __launch_bounds__(128) zline_pipe_kernel(LineArgs<T> a)
 //! e_k = (r_k + a_ZM,k e_{k-1}) / m_k as a multiply by the stored 1/m_k:
 //! no division on the k chain. Inputs are staged R levels ahead with cp.async
 //! as in zline_pipe_kernel.
-//! BG: the forward sweep's c' and e' stay in global memory for the back
-//! substitution (c' in its stored array, e' in the output array, which the
-//! back substitution overwrites level by level), so shared memory holds the
-//! ring alone and more warps fit on an SM; otherwise both go to shared memory.
-template <typename T, bool FIRST, int R, bool BG = false>
+//! BACK, where the back substitution finds c' and e': 0 both in shared
+//! memory; 1 both in global memory (c' in its stored array, e' in the output
+//! array, which the back substitution overwrites level by level), so shared
+//! memory holds the ring alone; 2 e' in shared memory and c' read again from
+//! its stored array (this sweep's reads or writes of it, still in L2), which
+//! halves the column's shared memory without e''s extra traffic. Less shared
+//! memory per column puts more warps on an SM.
+template <typename T, bool FIRST, int R, int BACK = 0>
 __device__ __forceinline__ void zline_fact_body(const LineArgs<T>& a, T* __restrict__ im_out,
                                                 const T* __restrict__ im_in, T* __restrict__ cp_out,
                                                 const T* __restrict__ cp_in)
@@ -241,7 +244,7 @@ __device__ __forceinline__ void zline_fact_body(const LineArgs<T>& a, T* __restr
     const gb_grid& g = a.g;
     T* ring = reinterpret_cast<T*>(smem_raw);
     T* cs = ring + R * NV * nthr;
-    T* es = cs + static_cast<int64_t>(a.nk) * nthr;
+    T* es = (BACK == 2) ? cs : cs + static_cast<int64_t>(a.nk) * nthr;
     int64_t o0 = 0, oxm = -1, oxp = -1, oym = -1, oyp = -1;
     if (active) {
         const int im = lateral_image(i - 1, a.ni, g.nx, g.periodic_x != 0);
@@ -309,17 +312,17 @@ __device__ __forceinline__ void zline_fact_body(const LineArgs<T>& a, T* __restr
             }
             cprev = c;
             eprev = ((k == 0) ? rk : rk - lower * eprev) * inv;
-            if (BG) {
+            if (BACK == 1) {
                 a.dnew[o0 + static_cast<int64_t>(k) * g.sz] = eprev;
             } else {
-                cs[k * nthr + tid] = c;
+                if (BACK == 0) { cs[k * nthr + tid] = c; }
                 es[k * nthr + tid] = eprev;
             }
         }
     }
     cp_async_wait<0>();
     T chg = T(0);
-    if (BG && active) {
+    if (BACK == 1 && active) {
         // x_k = e'_k - c'_k x_{k+1} in place over e' (this thread's own writes)
         const T* cpk = FIRST ? cp_out : cp_in;
         T x = eprev;
@@ -336,7 +339,8 @@ __device__ __forceinline__ void zline_fact_body(const LineArgs<T>& a, T* __restr
             }
         }
     }
-    if (!BG && active) {
+    if (BACK != 1 && active) {
+        const T* cpk = FIRST ? cp_out : cp_in;
         T x = eprev;
         int64_t ko = static_cast<int64_t>(a.nk - 1) * g.sz;
         a.dnew[o0 + ko] = x;
@@ -344,7 +348,8 @@ __device__ __forceinline__ void zline_fact_body(const LineArgs<T>& a, T* __restr
 #pragma unroll 4
         for (int k = a.nk - 2; k >= 0; --k) {
             ko -= g.sz;
-            x = es[k * nthr + tid] - cs[k * nthr + tid] * x;
+            const T ck = (BACK == 2) ? cpk[o0 + ko] : cs[k * nthr + tid];
+            x = es[k * nthr + tid] - ck * x;
             a.dnew[o0 + ko] = x;
             if (a.change) {
                 const T d = fabs(x - (FIRST ? T(0) : a.dold[o0 + ko]));
@@ -379,24 +384,24 @@ struct MultiLineArgs {
     T* cp[kMaxLineSystems];
 };
 
-template <typename T, bool FIRST, int R, int S, bool BG>
+template <typename T, bool FIRST, int R, int S, int BACK>
 __device__ __forceinline__ void zline_fact_system(const MultiLineArgs<T>& m)
 {
     if (FIRST) {
-        zline_fact_body<T, true, R, BG>(m.a[S], m.inv[S], nullptr, m.cp[S], nullptr);
+        zline_fact_body<T, true, R, BACK>(m.a[S], m.inv[S], nullptr, m.cp[S], nullptr);
     } else {
-        zline_fact_body<T, false, R, BG>(m.a[S], nullptr, m.inv[S], nullptr, m.cp[S]);
+        zline_fact_body<T, false, R, BACK>(m.a[S], nullptr, m.inv[S], nullptr, m.cp[S]);
     }
 }
 
-template <typename T, bool FIRST, int R, bool BG>
+template <typename T, bool FIRST, int R, int BACK>
 __global__ void __launch_bounds__(128) zline_fact_multi_kernel(MultiLineArgs<T> m)
 {
     // constant indices into the parameter block (no dynamic parameter indexing)
     switch (blockIdx.z) {
-    case 0: zline_fact_system<T, FIRST, R, 0, BG>(m); break;
-    case 1: zline_fact_system<T, FIRST, R, 1, BG>(m); break;
-    default: zline_fact_system<T, FIRST, R, 2, BG>(m); break;
+    case 0: zline_fact_system<T, FIRST, R, 0, BACK>(m); break;
+    case 1: zline_fact_system<T, FIRST, R, 1, BACK>(m); break;
+    default: zline_fact_system<T, FIRST, R, 2, BACK>(m); break;
     }
 }
 
@@ -598,15 +603,21 @@ gb_status zline_sweeps_multi(gb_ctx* ctx, const gb_grid& g, int n, const int* lo
     static std::atomic<bool> attr_done[2];  // set once per process (one device per process)
     const int ti = sizeof(T) == 8 ? 1 : 0;
     if (!attr_done[ti].load()) {
-        cudaFuncSetAttribute(zline_fact_multi_kernel<T, true, R, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaFuncSetAttribute(zline_fact_multi_kernel<T, true, R, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              200 * 1024);
-        cudaFuncSetAttribute(zline_fact_multi_kernel<T, false, R, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaFuncSetAttribute(zline_fact_multi_kernel<T, false, R, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             200 * 1024);
+        cudaFuncSetAttribute(zline_fact_multi_kernel<T, true, R, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             200 * 1024);
+        cudaFuncSetAttribute(zline_fact_multi_kernel<T, false, R, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              200 * 1024);
         attr_done[ti].store(true);
     }
-    // c' and e' of the back substitution in shared memory (1) or in the global arrays (2)
-    const bool bg = ctx->tune[GB_TUNE_LINE_BACK] == 2;
-    const size_t back = bg ? 0 : static_cast<size_t>(2 * max_nk);
+    // where the back substitution finds c' and e' (zline_fact_body's BACK):
+    // GB_TUNE_LINE_BACK 1 -> 0 (shared), 2 -> 1 (global), 3 -> 2 (e' shared, c' again from L2)
+    const int knob = ctx->tune[GB_TUNE_LINE_BACK];
+    const int back_mode = (knob == 2) ? 1 : (knob == 3) ? 2 : 0;
+    const size_t back = (back_mode == 1) ? 0 : (back_mode == 2) ? static_cast<size_t>(max_nk) : static_cast<size_t>(2 * max_nk);
     const size_t smem_first = static_cast<size_t>(R * 4 + back) * kThr * sizeof(T);
     const size_t smem = static_cast<size_t>(R * 12 + back) * kThr * sizeof(T);
     const dim3 grid((max_ni + kThr - 1) / kThr, max_nj, n);
@@ -633,16 +644,19 @@ gb_status zline_sweeps_multi(gb_ctx* ctx, const gb_grid& g, int n, const int* lo
             m.cp[s] = cpr[s];
         }
         Span span(ctx, GB_KERNEL_LINE_SWEEP);
+        const size_t sm = (k == 0) ? smem_first : smem;
         if (k == 0) {
-            if (bg) {
-                zline_fact_multi_kernel<T, true, R, true><<<grid, kThr, smem_first, ctx->stream>>>(m);
-            } else {
-                zline_fact_multi_kernel<T, true, R, false><<<grid, kThr, smem_first, ctx->stream>>>(m);
+            switch (back_mode) {
+            case 1: zline_fact_multi_kernel<T, true, R, 1><<<grid, kThr, sm, ctx->stream>>>(m); break;
+            case 2: zline_fact_multi_kernel<T, true, R, 2><<<grid, kThr, sm, ctx->stream>>>(m); break;
+            default: zline_fact_multi_kernel<T, true, R, 0><<<grid, kThr, sm, ctx->stream>>>(m); break;
             }
-        } else if (bg) {
-            zline_fact_multi_kernel<T, false, R, true><<<grid, kThr, smem, ctx->stream>>>(m);
         } else {
-            zline_fact_multi_kernel<T, false, R, false><<<grid, kThr, smem, ctx->stream>>>(m);
+            switch (back_mode) {
+            case 1: zline_fact_multi_kernel<T, false, R, 1><<<grid, kThr, sm, ctx->stream>>>(m); break;
+            case 2: zline_fact_multi_kernel<T, false, R, 2><<<grid, kThr, sm, ctx->stream>>>(m); break;
+            default: zline_fact_multi_kernel<T, false, R, 0><<<grid, kThr, sm, ctx->stream>>>(m); break;
+            }
         }
         ++ctx->launches;
     }

@@ -107,7 +107,8 @@ enum {
                                    2 twice that */
     GB_TUNE_LINE_BACK,          /* where the batched factored sweep keeps c' and e' for the back substitution:
                                    0 auto (= 1), 1 shared memory, 2 the global arrays (c' stored, e' in the
-                                   output array): less shared memory per warp, more warps per SM */
+                                   output array), 3 e' in shared memory and c' read again from its stored
+                                   array (L2): less shared memory per warp, more warps per SM */
     GB_N_TUNE
 };
 gb_status gb_ctx_tune(gb_ctx* ctx, int32_t key, int32_t value);

@@ -198,14 +198,15 @@ def test_gpu_zline_lusgs_refusals(ctx):
 @pytest.mark.parametrize("precision", [0, 1])
 def test_gpu_batched_sweep_back_substitution_placement_is_bitwise_neutral(ctx, precision):
     """The batched factored sweeps keep c' and e' for the back substitution in
-    shared memory (TUNE_LINE_BACK = 1) or in the global arrays (2): the same
-    arithmetic in the same order, so three SIMPLEC iterations (u, v, w and
-    theta, k swept in batched launches) give identical fields."""
+    shared memory (TUNE_LINE_BACK = 1), in the global arrays (2), or e' in
+    shared memory with c' read again (3): the same arithmetic in the same
+    order, so three SIMPLEC iterations (u, v, w and theta, k swept in batched
+    launches) give identical fields."""
     import ablsteadyrans_b200 as gb
     from ablsteadyrans_b200 import workloads
     from ablsteadyrans_b200.simplec import DeviceCase, SimplecStage
     out = []
-    for back in (1, 2):
+    for back in (1, 2, 3):
         inst = workloads.tile(40, 24, 3, precision=precision)
         ctx.tune(gb.TUNE_LINE_BACK, back)
         J, ax, ay, az, _ = oracle.metrics(inst.grid, inst.z)
@@ -219,3 +220,4 @@ def test_gpu_batched_sweep_back_substitution_placement_is_bitwise_neutral(ctx, p
     ctx.tune(gb.TUNE_LINE_BACK, 0)
     for f in out[0]:
         assert np.array_equal(out[0][f], out[1][f]), f
+        assert np.array_equal(out[0][f], out[2][f]), f
