@@ -225,6 +225,22 @@ class SimplecWorkload:
         return rc
 
 
+def max_over_ranks(dist, x, device):
+    """The job's time: the largest of every rank's (x itself on one rank)."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([float(x)], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(cells_per_rank, world, steps, ms):
+    """Cell updates per second of the whole job: every rank's instance, every
+    step, over the slowest rank's time."""
+    return cells_per_rank * world * steps / (ms / 1e3)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -311,10 +327,7 @@ def main():
         ms, n = ctx.profile_read(fam)
         families[name] = {"ms_per_step": ms / nb, "launches_per_step": n / nb}
     ctx.profile(False)
-    if dist is not None:
-        t = torch.tensor([total_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = max_over_ranks(dist, total_ms, "cuda")
 
     # end to end through the public API: one solve of K steps from host memory
     wl.e2e_setup(args.steps)
@@ -329,14 +342,10 @@ def main():
     e1.record()
     torch.cuda.synchronize()
     e2e_ms = e0.elapsed_time(e1)
-    if dist is not None:
-        t = torch.tensor([e2e_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(dist, e2e_ms, "cuda")
 
-    cells_per_step = wl.cells * world
-    value = cells_per_step * args.steps / (total_ms / 1e3)
-    e2e_value = cells_per_step * args.steps / (e2e_ms / 1e3)
+    value = whole_job_rate(wl.cells, world, args.steps, total_ms)
+    e2e_value = whole_job_rate(wl.cells, world, args.steps, e2e_ms)
     peak, peak_kind = hbm_peak()
     line_bytes = wl.line_bytes_per_step() * args.steps
     achieved = (line_bytes / (sweep_ms / 1e3)) / 1e9 if sweep_ms > 0 else None
