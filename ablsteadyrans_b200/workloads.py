@@ -108,6 +108,22 @@ def fractal_field(n, seed, rms, slope=3.0, dx=None, max_slope=None):
     return f - f.min()
 
 
+def edge_taper(f, margin):
+    """The field brought down to its minimum over the outer `margin` fraction
+    of each side with a raised-cosine weight (flat ground at the lateral
+    faces, so that the inflow profile and the zero-gradient outflow meet
+    level terrain)."""
+    if margin <= 0:
+        return f
+    ny, nx = f.shape
+
+    def w(n):
+        s = np.minimum(np.arange(n), np.arange(n)[::-1]) / max((n - 1) * margin, 1e-300)
+        return np.where(s < 1.0, 0.5 * (1.0 - np.cos(np.pi * np.minimum(s, 1.0))), 1.0)
+    base = f.min()
+    return base + (f - base) * w(ny)[:, None] * w(nx)[None, :]
+
+
 def log_law(h, ustar, z0):
     return ustar / KAPPA * np.log((np.maximum(h, 0.0) + z0) / z0)
 
@@ -247,6 +263,9 @@ def config1(nx=128, ny=128, nz=64, precision=0, zline_sweeps=4, turbulence=True)
 #: The steepest node-to-node terrain slope of a generated tile (the fractal
 #: field is scaled down to it where steeper).
 MAX_TILE_SLOPE = 1.0
+#: The outer fraction of each side of a tile over which its terrain is
+#: tapered to flat (edge_taper).
+TILE_EDGE_TAPER = 0.15
 
 
 def tile(n, nz, seed, rms=None, ustar=None, z0=None, met=None, dx=30.0, precision=1, zline_sweeps=4, turbulence=True):
@@ -254,7 +273,10 @@ def tile(n, nz, seed, rms=None, ustar=None, z0=None, met=None, dx=30.0, precisio
     seeded fractal terrain (|k|^-3, rms uniform 20-150 m unless given), a
     random wind direction, u* and z0 (seed-derived); inflow on the upwind x
     and y faces of the wind's quadrant, outflow on the others. The terrain
-    is scaled down where its slope would exceed MAX_TILE_SLOPE."""
+    is scaled down where its slope would exceed MAX_TILE_SLOPE and tapered
+    to flat over the outer TILE_EDGE_TAPER of each side: without the taper,
+    ridges at the outflow faces turn the flow back into the domain there,
+    where the zero-gradient outflow is ill-posed, and the solve stalls."""
     rng = np.random.default_rng(1000 + seed)
     rms = rms if rms is not None else rng.uniform(20, 150)
     ustar = ustar if ustar is not None else rng.uniform(0.2, 0.6)
@@ -263,7 +285,7 @@ def tile(n, nz, seed, rms=None, ustar=None, z0=None, met=None, dx=30.0, precisio
     direction = (270.0 - met) % 360.0
     zl, _ = geometric_zlevels(nz)
     g = Grid(n, n, nz, dx, dx, 1500.0 / nz, False, False)
-    terrain = fractal_field(n + 1, seed, rms, dx=dx, max_slope=MAX_TILE_SLOPE)
+    terrain = edge_taper(fractal_field(n + 1, seed, rms, dx=dx, max_slope=MAX_TILE_SLOPE), TILE_EDGE_TAPER)
     ground = node_ground(g, lambda x, y: float(terrain[int(round(y / dx)) % (n + 1), int(round(x / dx)) % (n + 1)]))
     ground_face, surface, turb = _turbulence(turbulence, z0)
     bc = abi.BC.make(_faces_for(direction, periodic_y=False, ground=ground_face), theta_ref=((0.0, 1500.0), (300.0, 300.0)),
