@@ -124,6 +124,14 @@ def edge_taper(f, margin):
     return base + (f - base) * w(ny)[:, None] * w(nx)[None, :]
 
 
+def cap_slope(f, dx, max_slope):
+    """f scaled about its minimum so that no node-to-node slope exceeds max_slope."""
+    steepest = max(np.abs(np.diff(f, axis=0)).max(), np.abs(np.diff(f, axis=1)).max()) / dx
+    if steepest <= max_slope:
+        return f
+    return f.min() + (f - f.min()) * (max_slope / steepest)
+
+
 def log_law(h, ustar, z0):
     return ustar / KAPPA * np.log((np.maximum(h, 0.0) + z0) / z0)
 
@@ -285,7 +293,8 @@ def tile(n, nz, seed, rms=None, ustar=None, z0=None, met=None, dx=30.0, precisio
     direction = (270.0 - met) % 360.0
     zl, _ = geometric_zlevels(nz)
     g = Grid(n, n, nz, dx, dx, 1500.0 / nz, False, False)
-    terrain = edge_taper(fractal_field(n + 1, seed, rms, dx=dx, max_slope=MAX_TILE_SLOPE), TILE_EDGE_TAPER)
+    terrain = cap_slope(edge_taper(fractal_field(n + 1, seed, rms, dx=dx, max_slope=MAX_TILE_SLOPE), TILE_EDGE_TAPER),
+                        dx, MAX_TILE_SLOPE)
     ground = node_ground(g, lambda x, y: float(terrain[int(round(y / dx)) % (n + 1), int(round(x / dx)) % (n + 1)]))
     ground_face, surface, turb = _turbulence(turbulence, z0)
     bc = abi.BC.make(_faces_for(direction, periodic_y=False, ground=ground_face), theta_ref=((0.0, 1500.0), (300.0, 300.0)),
