@@ -401,8 +401,12 @@ def solve_simplec_newton(stage, max_iterations, driver_options=None, switch=None
                         cont.close()
                     cont = Continuation(stage, copt, newton_options)
                 continue
-            status = cont.step()
-            newton_its += 1
+            # once the continuation has converged on the run's equations
+            # (|R| <= 10^-residual_drop_orders |R_0|) no step is taken: the
+            # norms fill the criterion's monitor window (NewtonStage.H)
+            done = cont.st.steps > 0 and cont.st.r_last <= 10.0 ** (-o.residual_drop_orders) * cont.st.r0
+            status = "accepted" if done else cont.step()
+            newton_its += 0 if done else 1
             failures = failures + 1 if status == "failed" else 0
             res, mon = stage.norms()
             crit.add(res, mon[:n_mon])
