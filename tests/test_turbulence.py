@@ -438,3 +438,33 @@ def test_gpu_implicit_rows_match_oracle(ctx, damping):
             ref, got = A_ref[c][v], A[c][v]
             assert np.abs(got - ref).max() <= 1e-11 * max(np.abs(ref).max(), 1e-300), (eq, c, np.abs(got - ref).max())
     st.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("seed", [0, 3])
+def test_gpu_tile_layout_iterations_match_oracle(ctx, seed):
+    """The served tiles' layout (inflow on the upwind x and y faces, outflow
+    on the others, fractal terrain tapered at the edges, the closure and the
+    wall law with the tile's u* and z0): three SIMPLEC iterations on the GPU
+    equal the oracle's."""
+    from ablsteadyrans_b200 import workloads
+    from helpers import case_from_instance
+    inst = workloads.tile(16, 12, seed, precision=0, zline_sweeps=3)
+    case = case_from_instance(inst)
+    bc, ph, so = inst.bc, inst.physics, inst.options
+    so.pressure_reltol = 1e-11
+    dc, st = _stage(ctx, case, bc, ph, pressure_reltol=1e-11, zline_sweeps=3)
+    oracle.fill_ghosts(case, bc, ph)
+    st.fill_ghosts()
+    try:
+        for it in range(3):
+            dt_ref = oracle.local_dtau(case, 2.0, phys=ph)
+            rc, _, _ = oracle.simplec_iterate(case, bc, ph, so, dt_ref)
+            assert rc == 0
+            st.iterate(st.local_dtau(2.0))
+            for f, loc in zip(FIELDS, LOCS):
+                v = case.grid.valid(loc)
+                ref, got = case.q[f][v], dc.host(f)[v]
+                assert np.abs(got - ref).max() <= 1e-9 * max(np.abs(ref).max(), 1e-300), (it, f)
+    finally:
+        st.close()
