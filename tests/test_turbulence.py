@@ -446,13 +446,16 @@ def test_gpu_tile_layout_iterations_match_oracle(ctx, seed):
     """The served tiles' layout (inflow on the upwind x and y faces, outflow
     on the others, fractal terrain tapered at the edges, the closure and the
     wall law with the tile's u* and z0): three SIMPLEC iterations on the GPU
-    equal the oracle's."""
+    equal the oracle's, from the oracle's mass-consistent initial state."""
     from ablsteadyrans_b200 import workloads
     from helpers import case_from_instance
     inst = workloads.tile(16, 12, seed, precision=0, zline_sweeps=3)
     case = case_from_instance(inst)
     bc, ph, so = inst.bc, inst.physics, inst.options
     so.pressure_reltol = 1e-11
+    from ablsteadyrans_b200.abi import InitOptions
+    rc, _ = oracle.initialize(case, bc, InitOptions.make())
+    assert rc == 0
     dc, st = _stage(ctx, case, bc, ph, pressure_reltol=1e-11, zline_sweeps=3)
     oracle.fill_ghosts(case, bc, ph)
     st.fill_ghosts()
