@@ -243,8 +243,10 @@ def test_gpu_simplec_newton_reaches_the_strict_criterion(ctx):
     st = SimplecStage(ctx, dc, bc, ph, SimplecOptions.make(pressure_reltol=1e-6))
     st.fill_ghosts()
     try:
-        verdict, its, newton_its = solve_simplec_newton(st, 3000, switch=SwitchOptions(1e-2, 5),
-                                                        newton_options=NewtonOptions.make(gmres_restart=60))
+        from ablsteadyrans_b200.abi import DriverOptions
+        verdict, its, newton_its = solve_simplec_newton(
+            st, 3000, driver_options=DriverOptions.make(monitor_window=5), switch=SwitchOptions(1e-2, 5),
+            newton_options=NewtonOptions.make(gmres_restart=60, gmres_max_iters=300))
         assert verdict == "steady", (verdict, its, newton_its)
         assert newton_its > 0
         res, _ = st.norms()
