@@ -564,6 +564,10 @@ gb_status gb_newton_create(gb_simplec* s, const gb_newton_opts* o, gb_newton** o
     }
     gb_status st = check_newton(o);
     if (st != GB_OK) { return st; }
+    if (gb::volume(gb::simplec_grid(s)) >= (static_cast<int64_t>(1) << 31)) {
+        gb::set_error("gust: NewtonKrylov: the padded grid has 2^31 points or more (one flat launch per field)");
+        return GB_BAD_ARG;
+    }
     gb_newton* n = new (std::nothrow) gb_newton;
     if (n == nullptr) {
         gb::set_error("gust: NewtonKrylov: out of host memory");
