@@ -519,6 +519,72 @@ __global__ void __launch_bounds__(32) k_color_solve_staged(gb_grid g, int color,
     }
 }
 
+//! One colour's relaxation in ONE launch: a block owns up to kFusedCols
+//! columns of the colour along one row; its threads compute the residual
+//! r = b - A x of every cell of those columns into shared memory (with the
+//! columns' x and line factors), a block barrier, then one thread per column
+//! runs the factored Thomas solve of k_color_solve_staged and writes x. The
+//! arithmetic and its order are those of k_color_residual followed by
+//! k_color_solve_staged; r never goes to global memory and the colour costs
+//! one launch. The lateral neighbours of a column are of the other colour,
+//! and only this block updates its own columns, so every read sees the
+//! values from before the colour's update (a periodic direction of odd
+//! extent pairs a column with a same-colour image: the caller then uses the
+//! two-launch form). Shared memory: [array][k][column] for r, D, 1/m, c', x.
+constexpr int kFusedCols = 32;
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_color_relax_fused(gb_grid g, PBC b, int color, T* x, const T* __restrict__ bv,
+                                                           const T* __restrict__ AX, const T* __restrict__ AY,
+                                                           const T* __restrict__ AZ, const T* __restrict__ J,
+                                                           MeshRatios<T> m, const T* __restrict__ TD,
+                                                           const T* __restrict__ TC, const T* __restrict__ TU)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    constexpr int C = kFusedCols;
+    const int nz = g.nz;
+    const int plane = nz * C;
+    T* sr = reinterpret_cast<T*>(smem_raw);
+    T* sd = sr + plane;
+    T* sm = sd + plane;
+    T* sc = sm + plane;
+    T* sx = sc + plane;
+    const int j = blockIdx.y;
+    const int c0 = blockIdx.x * C;
+    for (int n = threadIdx.x; n < plane; n += blockDim.x) {
+        const int col = n % C, k = n / C;
+        const int i = 2 * (c0 + col) + ((j + color) & 1);
+        if (i >= g.nx) { continue; }
+        const int64_t o = at(g, i, j, k);
+        sx[n] = x[o];
+        sd[n] = TD[o];
+        sm[n] = TC[o];
+        sc[n] = TU[o];
+        sr[n] = bv[o] - adotx_cell<T>(g, b, i, j, k, x, AX, AY, AZ, J, m);
+    }
+    __syncthreads();
+    const int col = threadIdx.x;
+    if (col >= C) { return; }
+    const int i = 2 * (c0 + col) + ((j + color) & 1);
+    if (i >= g.nx) { return; }
+    T ep = sr[col] * sm[col];
+    sr[col] = ep;
+    for (int k = 1; k < nz; ++k) {
+        const int s = k * C + col;
+        ep = (sr[s] - sd[s] * ep) * sm[s];
+        sr[s] = ep;
+    }
+    T xk = ep;
+    int64_t o = at(g, i, j, nz - 1);
+    x[o] = sx[(nz - 1) * C + col] + xk;
+    for (int k = nz - 2; k >= 0; --k) {
+        const int s = k * C + col;
+        o -= g.sz;
+        xk = sr[s] - sc[s] * xk;
+        x[o] = sx[s] + xk;
+    }
+}
+
 //! Coarse right-hand side at coarse cell (I, J2, k): the J-weighted sum of
 //! the four fine residuals over 4 J_c (a coarse cell's flux balance is the sum
 //! of its fine cells').
@@ -830,6 +896,27 @@ void mg_smooth(gb_poisson* P, PoissonLevels<T>& L, int l)
         attr_done[ti].store(true);
     }
     const int half = (g.nx + 1) / 2;
+    // one launch per colour (k_color_relax_fused) unless a periodic direction
+    // has an odd extent or the columns' arrays do not fit shared memory
+    const size_t smem_fused = static_cast<size_t>(5) * g.nz * kFusedCols * sizeof(T);
+    const bool fused = ctx->tune[GB_TUNE_MG_FUSED_RELAX] != 1 && smem_fused <= kSmoothSmemMax
+                       && !(g.periodic_x && (g.nx & 1)) && !(g.periodic_y && (g.ny & 1));
+    if (fused) {
+        static std::atomic<bool> fused_attr[2];
+        if (!fused_attr[ti].load()) {
+            cudaFuncSetAttribute(k_color_relax_fused<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmoothSmemMax);
+            fused_attr[ti].store(true);
+        }
+        const dim3 fgrid((half + kFusedCols - 1) / kFusedCols, g.ny);
+        for (int color = 0; color < 2; ++color) {
+            Span span(ctx, GB_KERNEL_MG_SMOOTH);
+            k_color_relax_fused<T><<<fgrid, 256, smem_fused, ctx->stream>>>(g, b, color, L.x[l], L.bv[l], L.AX[l], L.AY[l],
+                                                                           L.AZ[l], L.J[l], L.ratios(l), L.TD[l],
+                                                                           L.TC[l], L.TU[l]);
+            ++ctx->launches;
+        }
+        return;
+    }
     for (int color = 0; color < 2; ++color) {
         Span span(ctx, GB_KERNEL_MG_SMOOTH);
         const dim3 rgrid((half + 31) / 32, (g.ny + 3) / 4, g.nz);

@@ -109,6 +109,8 @@ enum {
                                    0 auto (= 1), 1 shared memory, 2 the global arrays (c' stored, e' in the
                                    output array), 3 e' in shared memory and c' read again from its stored
                                    array (L2): less shared memory per warp, more warps per SM */
+    GB_TUNE_MG_FUSED_RELAX,     /* one launch per colour of the zebra line relaxation (the residual in shared
+                                   memory): 0 auto (where it applies), 1 the residual and the solve as two launches */
     GB_N_TUNE
 };
 gb_status gb_ctx_tune(gb_ctx* ctx, int32_t key, int32_t value);

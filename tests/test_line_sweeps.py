@@ -221,3 +221,30 @@ def test_gpu_batched_sweep_back_substitution_placement_is_bitwise_neutral(ctx, p
     for f in out[0]:
         assert np.array_equal(out[0][f], out[1][f]), f
         assert np.array_equal(out[0][f], out[2][f]), f
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", [0, 1])
+def test_gpu_fused_zebra_relaxation_is_bitwise_neutral(ctx, precision):
+    """The multigrid's zebra relaxation as one launch per colour (the
+    residual kept in shared memory) or as the residual and the solve in two
+    launches: the same arithmetic in the same order, so three SIMPLEC
+    iterations give identical fields."""
+    import ablsteadyrans_b200 as gb
+    from ablsteadyrans_b200 import workloads
+    from ablsteadyrans_b200.simplec import DeviceCase, SimplecStage
+    out = []
+    for mode in (0, 1):
+        inst = workloads.tile(40, 24, 3, precision=precision)
+        ctx.tune(gb.TUNE_MG_FUSED_RELAX, mode)
+        J, ax, ay, az, _ = oracle.metrics(inst.grid, inst.z)
+        dc = DeviceCase(inst.grid, inst.z, J, ax, ay, az, inst.nu, inst.gamma_theta, inst.gamma_tke, inst.q, inst.z0map)
+        st = SimplecStage(ctx, dc, inst.bc, inst.physics, inst.options)
+        st.fill_ghosts()
+        for _ in range(3):
+            st.iterate(st.local_dtau(2.0))
+        out.append({f: dc.host(f) for f in ("u", "v", "w", "p", "theta", "tke")})
+        st.close()
+    ctx.tune(gb.TUNE_MG_FUSED_RELAX, 0)
+    for f in out[0]:
+        assert np.array_equal(out[0][f], out[1][f]), f
