@@ -896,15 +896,15 @@ void mg_smooth(gb_poisson* P, PoissonLevels<T>& L, int l)
         attr_done[ti].store(true);
     }
     const int half = (g.nx + 1) / 2;
-    // one launch per colour (k_color_relax_fused) on the levels of at most
-    // kFusedMaxColumns columns, where a launch is latency (on the finer levels
-    // the two-launch form is faster: its residual runs one thread per cell),
-    // unless a periodic direction has an odd extent or the columns' arrays do
-    // not fit shared memory; GB_TUNE_MG_FUSED_RELAX 2 forces it on every level
+    // one launch per colour (k_color_relax_fused) only on request
+    // (GB_TUNE_MG_FUSED_RELAX 2: every level, 3: levels of at most
+    // kFusedMaxColumns columns): on config 1 it measured slower than the two
+    // launches on every level (the residual of the two-launch form runs one
+    // thread per cell; the fused block serialises its columns' solves)
     constexpr int kFusedMaxColumns = 1024;
     const size_t smem_fused = static_cast<size_t>(5) * g.nz * kFusedCols * sizeof(T);
     const int fknob = ctx->tune[GB_TUNE_MG_FUSED_RELAX];
-    const bool fused = fknob != 1 && (fknob == 2 || g.nx * g.ny <= kFusedMaxColumns) && smem_fused <= kSmoothSmemMax
+    const bool fused = (fknob == 2 || (fknob == 3 && g.nx * g.ny <= kFusedMaxColumns)) && smem_fused <= kSmoothSmemMax
                        && !(g.periodic_x && (g.nx & 1)) && !(g.periodic_y && (g.ny & 1));
     if (fused) {
         static std::atomic<bool> fused_attr[2];

@@ -110,8 +110,8 @@ enum {
                                    output array), 3 e' in shared memory and c' read again from its stored
                                    array (L2): less shared memory per warp, more warps per SM */
     GB_TUNE_MG_FUSED_RELAX,     /* one launch per colour of the zebra line relaxation (the residual in shared
-                                   memory): 0 auto (levels of at most 1024 columns), 1 never (the residual and
-                                   the solve as two launches), 2 on every level */
+                                   memory): 0 auto (= 1), 1 never (the residual and the solve as two launches),
+                                   2 on every level, 3 on the levels of at most 1024 columns */
     GB_N_TUNE
 };
 gb_status gb_ctx_tune(gb_ctx* ctx, int32_t key, int32_t value);
