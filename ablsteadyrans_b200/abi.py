@@ -234,14 +234,15 @@ class DriverOptions(ctypes.Structure):
     _fields_ = [("cfl0", ctypes.c_double), ("cfl_max", ctypes.c_double), ("ser_exponent", ctypes.c_double),
                 ("ser_max_growth", ctypes.c_double), ("residual_tol", ctypes.c_double),
                 ("residual_drop_orders", ctypes.c_double), ("residual_ref_iterations", ctypes.c_int32),
-                ("monitor_rel_tol", ctypes.c_double), ("monitor_window", ctypes.c_int32)]
+                ("monitor_rel_tol", ctypes.c_double), ("monitor_window", ctypes.c_int32),
+                ("confidence", ctypes.c_double), ("confidence_height", ctypes.c_double)]
 
     @classmethod
     def make(cls, line_sweep=0, **kw):
         """The reference's defaults (cfl_max 8 with steady.sweep = lusgs, else 10)."""
         o = cls(cfl0=1.0, cfl_max=8.0 if line_sweep == 1 else 10.0, ser_exponent=1.0, ser_max_growth=2.0,
                 residual_tol=5e-5, residual_drop_orders=4.0, residual_ref_iterations=5, monitor_rel_tol=1e-3,
-                monitor_window=50)
+                monitor_window=50, confidence=0.0, confidence_height=0.0)
         for k, v in kw.items():
             setattr(o, k, v)
         return o

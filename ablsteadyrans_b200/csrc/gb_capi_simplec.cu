@@ -352,6 +352,16 @@ gb_status gb_simplec_norms(gb_simplec* s, const gb_state* q, double* residual_no
     return gb::simplec_norms(s, *q, residual_norms, monitors);
 }
 
+gb_status gb_simplec_confidence(gb_simplec* s, const double* thresholds, double* share, double* height)
+{
+    gb::clear_error();
+    if (s == nullptr || thresholds == nullptr || share == nullptr || height == nullptr) {
+        gb::set_error("gust: SimplecStage::confidence: null argument");
+        return GB_BAD_ARG;
+    }
+    return gb::simplec_confidence(s, thresholds, share, height);
+}
+
 gb_status gb_simplec_implicit_rows(gb_simplec* s, const gb_state* q, int32_t eq, double* A)
 {
     gb::clear_error();

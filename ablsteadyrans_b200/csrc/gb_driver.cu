@@ -91,9 +91,24 @@ gb_status driver_step(gb_driver* d, int32_t* verdict, gb_iter_info* info_out, do
     }
     d->r_last = r;
     bool rm = false, mm = false;
-    if (gb::criterion_verdict(d->crit, &rm, &mm, nullptr) == GB_STEADY) {
+    const int v = gb::criterion_verdict(d->crit, &rm, &mm, nullptr);
+    if (v == GB_STEADY) {
         *verdict = GB_DRIVER_STEADY;
         return GB_OK;
+    }
+    // the confidence stop (Driver.cpp:453-477): the residual criterion met
+    // cell by cell on steady.confidence of the cells (and, with
+    // confidence_height, on every cell above it), every monitor met
+    if (o.confidence > 0 && v == GB_NOT_STEADY && h.count > d->hold_iterations() && mm) {
+        const double drop = std::pow(10.0, -o.residual_drop_orders);
+        double t[6];
+        for (int n = 0; n < 6; ++n) { t[n] = std::min(o.residual_tol, std::max(h.res_ref[n], o.residual_tol) * drop); }
+        double share = 0, height = 0;
+        if ((st = gb_simplec_confidence(d->stage, t, &share, &height)) != GB_OK) { return st; }
+        if (share >= o.confidence && (o.confidence_height == 0 || height <= o.confidence_height)) {
+            *verdict = GB_DRIVER_STEADY;
+            return GB_OK;
+        }
     }
     d->cfl = (h.count <= d->hold_iterations()) ? o.cfl0 : ser_cfl(d->cfl, r, o);
     *verdict = GB_DRIVER_RUNNING;
@@ -129,6 +144,8 @@ gb_status gb_driver_options_default(gb_driver_opts* o, int32_t line_sweep)
     o->residual_ref_iterations = 5;
     o->monitor_rel_tol = 1.0e-3;
     o->monitor_window = 50;
+    o->confidence = 0.0;
+    o->confidence_height = 0.0;
     return GB_OK;
 }
 
@@ -152,6 +169,19 @@ gb_status gb_driver_create(gb_simplec* s, const gb_state* q, const gb_driver_opt
     }
     if (bad(o->ser_max_growth, o->ser_max_growth >= 1)) {
         gb::set_error("gust: invalid inputs:\n  steady.ser_max_growth = %g: must be finite and >= 1", o->ser_max_growth);
+        return GB_BAD_ARG;
+    }
+    if (bad(o->confidence, o->confidence == 0 || (o->confidence > 0 && o->confidence <= 1))) {
+        gb::set_error("gust: invalid inputs:\n  steady.confidence = %g: must be 0 (off) or finite, > 0 and <= 1", o->confidence);
+        return GB_BAD_ARG;
+    }
+    if (bad(o->confidence_height, o->confidence_height >= 0)) {
+        gb::set_error("gust: invalid inputs:\n  steady.confidence_height = %g: must be 0 (anywhere) or finite and > 0 (m)",
+                      o->confidence_height);
+        return GB_BAD_ARG;
+    }
+    if (o->confidence == 0 && o->confidence_height > 0) {
+        gb::set_error("gust: invalid inputs:\n  steady.confidence_height has no effect without steady.confidence > 0");
         return GB_BAD_ARG;
     }
     // the criterion's residuals and monitors (stage_residual_names,

@@ -30,6 +30,7 @@ enum { F_U = 0, F_V, F_W, F_P, F_THETA, F_TKE };
 constexpr int kRedBlocks = 512;
 //! The result word that counts the ground columns without a positive, finite u*.
 constexpr int W_SURFACE_BAD = 40;
+constexpr int W_CONF_BAD = 41, W_CONF_TOP = 42;   // the confidence test's count and height
 
 // ------------------------------------------------------------- heights ---
 
@@ -280,6 +281,7 @@ struct gb_simplec {
     // nu the next local dtau reads: the closure's of the last iteration's
     // residual (SimplecStage::nu, Simplec.H:214; 0 before the first)
     double* nu_dtau{nullptr};
+    double* agl{nullptr};                // height above the ground for the confidence test (made on first use)
     double* ss[gb::kSsPlanes]{};         // the surface state of the iteration's first fill
     double* ssr[gb::kSsPlanes]{};        // the residual's own surface state
     double* sst[gb::kSsPlanes]{};        // the later fills' surface state
@@ -1835,6 +1837,53 @@ gb_status simplec_norms(gb_simplec* S, const gb_state& q, double* res, double* m
     mon[1] = sums[SUM_TKE] / (static_cast<double>(g.nx) * g.ny * g.nz);
     mon[2] = S->wall ? sums[SUM_USTAR] / (static_cast<double>(g.nx) * g.ny) : 0.0;
     return check_cuda("stage_norms");
+}
+
+//! SimplecStage::confidence (Simplec.cpp:411-445) on the residual of the last
+//! iteration's start: the share of cells whose six residuals (both faces of
+//! a velocity, the cell's p, theta and k) are within the thresholds (the
+//! criterion's, per equation, times the residual scales), and the largest
+//! height above the ground of a cell that is not.
+gb_status simplec_confidence(gb_simplec* S, const double* thresholds, double* share, double* height)
+{
+    gb_ctx* ctx = S->ctx;
+    const gb_grid g = S->g;
+    if (S->agl == nullptr) {
+        if ((S->agl = dbuf(S, volume(g))) == nullptr) {
+            set_error("gust: SimplecStage::confidence: cannot allocate the height above the ground");
+            return GB_OOM;
+        }
+        turb_height_above_ground(ctx, g, S->z, S->agl);
+    }
+    const gb_physics& ph = S->ph;
+    const double U = ph.scale_velocity, H = ph.scale_height;
+    const double scale[6] = {U * U / H, U * U / H, U * U / H, U / H, U * ph.scale_theta / H, U * ph.scale_tke / H};
+    double t[6];
+    for (int n = 0; n < 6; ++n) { t[n] = thresholds[n] * scale[n]; }
+    const double t0 = t[0], t1 = t[1], t2 = t[2], t3 = t[3], t4 = t[4], t5 = t[5];
+    const double *ru = S->w.R[0], *rv = S->w.R[1], *rw = S->w.R[2], *rp = S->w.R[3], *rt = S->w.R[4], *rk = S->w.R[5];
+    const double* d = S->agl;
+    unsigned long long* bad = dword(ctx, W_CONF_BAD);
+    unsigned long long* top = dword(ctx, W_CONF_TOP);
+    cudaMemsetAsync(bad, 0, 2 * sizeof(unsigned long long), ctx->stream);
+    for_box(ctx, valid_box(g, CC), [=] __device__(int i, int j, int k) {
+        const int64_t o = at(g, i, j, k);
+        const bool ok = fmax(fabs(ru[o]), fabs(ru[at(g, i + 1, j, k)])) <= t0
+                        && fmax(fabs(rv[o]), fabs(rv[at(g, i, j + 1, k)])) <= t1
+                        && fmax(fabs(rw[o]), fabs(rw[at(g, i, j, k + 1)])) <= t2 && fabs(rp[o]) <= t3
+                        && fabs(rt[o]) <= t4 && fabs(rk[o]) <= t5;
+        if (!ok) {
+            atomicAdd(bad, 1ull);
+            atomic_max_nonneg(top, d[o]);
+        }
+    }, GB_KERNEL_VECTOR);
+    unsigned long long words[2];
+    gb_status st = read_words(ctx, W_CONF_BAD, 2, words);
+    if (st != GB_OK) { return st; }
+    const double cells = static_cast<double>(g.nx) * g.ny * g.nz;
+    *share = 1.0 - static_cast<double>(words[0]) / cells;
+    *height = bits_to_double(words[1]);
+    return check_cuda("SimplecStage::confidence");
 }
 
 // ------------------------------------------------------ pseudo-time step ---

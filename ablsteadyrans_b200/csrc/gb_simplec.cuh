@@ -15,6 +15,7 @@ void simplec_implicit_rows(gb_simplec* S, int eq, double* const* F, double* A);
 void simplec_implicit_rows_at(gb_simplec* S, const gb_state& q, int eq, double* A);
 gb_status simplec_iterate(gb_simplec* S, const gb_state& q, const double* dtau, gb_iter_info* info);
 gb_status simplec_norms(gb_simplec* S, const gb_state& q, double* res, double* mon);
+gb_status simplec_confidence(gb_simplec* S, const double* thresholds, double* share, double* height);
 gb_status simplec_local_dtau(gb_simplec* S, const gb_state& q, double cfl, double* dtau);
 gb_status simplec_initialize(gb_simplec* S, const gb_state& q, const gb_init_opts& o, gb_init_result* r);
 gb_status simplec_turbulence(gb_simplec* S, double* const* closure, double* const* surface);

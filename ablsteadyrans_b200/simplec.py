@@ -31,6 +31,8 @@ def _declare(L):
     L.gb_simplec_implicit_rows.argtypes = [P, ctypes.POINTER(abi.State), ctypes.c_int32, P]
     L.gb_simplec_norms.argtypes = [P, ctypes.POINTER(abi.State), ctypes.POINTER(ctypes.c_double),
                                    ctypes.POINTER(ctypes.c_double)]
+    L.gb_simplec_confidence.argtypes = [P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
+                                        ctypes.POINTER(ctypes.c_double)]
     L.gb_driver_criterion.argtypes = [P, ctypes.POINTER(P)]
     L.gb_driver_seed_reference.argtypes = [P, ctypes.POINTER(ctypes.c_double)]
     L.gb_driver_release_hold.argtypes = [P]
@@ -160,6 +162,16 @@ class SimplecStage:
         st = self.case.state()
         check(self._L.gb_simplec_norms(self._h, ctypes.byref(st), res, mon))
         return list(res), list(mon)
+
+    def confidence(self, thresholds):
+        """SimplecStage::confidence on the last iteration's residual: (share
+        of the cells within the six thresholds, largest height above the
+        ground of a cell that is not)."""
+        from . import check
+        share, height = ctypes.c_double(), ctypes.c_double()
+        t = (ctypes.c_double * 6)(*[float(x) for x in thresholds])
+        check(self._L.gb_simplec_confidence(self._h, t, ctypes.byref(share), ctypes.byref(height)))
+        return share.value, height.value
 
     def local_dtau_of(self, state, cfl, out):
         """local_dtau at another state of this stage's grid (an abi.State)."""

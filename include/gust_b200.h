@@ -534,6 +534,10 @@ typedef struct gb_driver_opts {
     int32_t residual_ref_iterations; /* steady.residual_ref_iterations */
     double monitor_rel_tol;          /* steady.monitor_rel_tol */
     int32_t monitor_window;          /* steady.monitor_window (>= 2) */
+    double confidence;               /* steady.confidence: 0 off, or (0, 1]: steady once that share of the
+                                        cells meets the residual criterion cell by cell with every monitor met */
+    double confidence_height;        /* steady.confidence_height: 0 anywhere, or the height above the ground
+                                        (m) every failing cell must be below */
 } gb_driver_opts;
 
 /* ---- the Newton-Krylov finishing stage ---------------------------------- */
@@ -677,6 +681,11 @@ gb_status gb_driver_criterion(gb_driver* d, gb_criterion** c);
 gb_status gb_driver_seed_reference(gb_driver* d, const double* ref);
 gb_status gb_driver_release_hold(gb_driver* d);
 gb_status gb_driver_start_cfl(gb_driver* d, double cfl);
+/* SimplecStage::confidence (Source/Simplec.cpp:411-445) on the residual of the
+ * last iteration's start: the share of cells whose six residuals are within
+ * thresholds[6] (the criterion's per equation, in the scaled units of the
+ * norms) and the largest height above the ground of a cell that is not. */
+gb_status gb_simplec_confidence(gb_simplec* s, const double* thresholds, double* share, double* height);
 /* Driver::hold_iterations, the CFL of the next step and r_n of the last. */
 gb_status gb_driver_status(const gb_driver* d, int32_t* hold_iterations, double* next_cfl, double* relative_residual);
 /* Many drivers at once: each steps until its verdict is not RUNNING or it

@@ -471,3 +471,28 @@ def test_gpu_tile_layout_iterations_match_oracle(ctx, seed):
                 assert np.abs(got - ref).max() <= 1e-9 * max(np.abs(ref).max(), 1e-300), (it, f)
     finally:
         st.close()
+
+
+@pytest.mark.gpu
+def test_gpu_confidence_share_and_height(ctx):
+    """SimplecStage::confidence on the last iteration's residual: every cell
+    passes thresholds far above the residuals (share 1, no failing height),
+    no cell passes zero thresholds (share 0, the failing height is the
+    highest cell's height above the ground), and the share grows with the
+    thresholds."""
+    case, bc, ph = _hill_case()
+    dc, st = _stage(ctx, case, bc, ph)
+    st.fill_ghosts()
+    try:
+        info = st.iterate(st.local_dtau(2.0))
+        s1, h1 = st.confidence([1e30] * 6)
+        assert s1 == 1.0 and h1 == 0.0
+        s0, h0 = st.confidence([0.0] * 6)
+        assert s0 == 0.0
+        agl = oracle.height_above_ground(case)
+        assert abs(h0 - agl[case.grid.valid(0)].max()) <= 1e-9 * h0
+        norms = list(info.residual_norms)
+        shares = [st.confidence([f * n for n in norms])[0] for f in (0.3, 1.0, 3.0, 10.0)]
+        assert shares == sorted(shares) and 0.0 < shares[1] < 1.0
+    finally:
+        st.close()
