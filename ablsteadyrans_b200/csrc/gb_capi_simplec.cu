@@ -233,6 +233,11 @@ gb_status check_closure(const gb_physics& ph)
         {"nu_molecular", ph.turb_nu_molecular, ph.turb_nu_molecular >= 0, "finite and >= 0 (m^2/s)"},
         {"alpha_molecular", ph.turb_alpha_molecular, ph.turb_alpha_molecular >= 0, "finite and >= 0 (m^2/s)"},
         {"kappa", ph.turb_kappa, ph.turb_kappa > 0, "finite and > 0"},
+        {"ri_gate", ph.turb_ri_gate, ph.turb_ri_gate == 0 || (ph.turb_ri_gate >= 1e-6 && ph.turb_ri_gate <= 1),
+         "0 (off) or finite, >= 1e-6 and <= 1"},
+        {"realizability", ph.turb_realizability,
+         ph.turb_realizability == 0 || (ph.turb_realizability >= 0.01 && ph.turb_realizability <= 10),
+         "0 (off) or finite, >= 0.01 and <= 10"},
     };
     for (const Rule& r : rules) {
         if (bad(r.x) || !r.ok) {

@@ -234,6 +234,10 @@ void turb_closure(gb_ctx* ctx, const gb_grid& g, const gb_bc& bc, const gb_physi
     const double g_over_theta0 = ph.gravity / ph.theta0;
     const double nu_mol = ph.turb_nu_molecular, alpha_mol = ph.turb_alpha_molecular;
     const double inv_sigma = 1 / ph.turb_sigma_k;
+    // turb.ri_gate (gate_stratification, Closure.cpp:337-354) and
+    // turb.realizability (nut_cap_field, ClosureWake.cpp:8-29)
+    const double ri0 = ph.turb_ri_gate, r2 = ri0 * ri0, cr = ph.turb_realizability;
+    const bool gate = ri0 > 0, capped = cr > 0;
     // the ground's roughness in kappa (d + z0): a map, the uniform value, or 0
     // without a surface layer (ground_roughness, SurfaceLayer.H:176-181)
     const bool wall = bc.face[2] == GB_FACE_SURFACE_LAYER;
@@ -268,10 +272,21 @@ void turb_closure(gb_ctx* ctx, const gb_grid& g, const gb_bc& bc, const gb_physi
         const double z0 = zmap ? zmap[plane_at(gg, i, j)] : z0u;
         const double lraw = c.kappa * (dist[o] + z0);
         const double l_g = c.l_g_max * lraw / (c.l_g_max + lraw);
-        const Switches sw = switches_for(tk[o], N2, l_g, c);
-        const Point p = closure_point(tk[o], N2, l_g, c, sw);
+        // the length and Rt see the gated N^2; P_b keeps N^2
+        double N2c = N2;
+        if (gate) {
+            const double a = N2 * N2, b = S2 * S2;
+            N2c *= a / (a + r2 * b + DBL_MIN);
+        }
+        const Switches sw = switches_for(tk[o], N2c, l_g, c);
+        const Point p = closure_point(tk[o], N2c, l_g, c, sw);
         const double ratio = p.cmu_prime / p.cmu;
-        const double nt = 1.0 * fmin(p.nut, DBL_MAX) + (1.0 - 1.0) * tk[o];
+        double cap = DBL_MAX;
+        if (capped) {
+            const double sr = sqrt(S2);
+            cap = (sr > DBL_MIN) ? cr * fmax(tk[o], c.tke_floor) / sr : DBL_MAX;
+        }
+        const double nt = 1.0 * fmin(p.nut, cap) + (1.0 - 1.0) * tk[o];
         O.p[kClosureNut][o] = nt;
         O.p[kClosureNu][o] = nu_mol + nt;
         O.p[kClosureGammaTheta][o] = alpha_mol + ratio * nt;

@@ -347,6 +347,9 @@ typedef struct gb_physics {
     double turb_sigma_k;                          /* turb.sigma_k */
     double turb_nu_molecular, turb_alpha_molecular; /* turb.nu_molecular, turb.alpha_molecular (m^2/s) */
     double turb_kappa;                            /* turb.kappa */
+    double turb_ri_gate;                          /* turb.ri_gate: 0 off, or Ri_0 in [1e-6, 1] (the stratification
+                                                     gate of the length and Rt; P_b keeps N^2) */
+    double turb_realizability;                    /* turb.realizability: 0 off, or C_r in [0.01, 10] (nu_t <= C_r k / S) */
 } gb_physics;
 
 /* simplec.* and steady.zline_sweeps (gust::SimplecOptions, Source/Simplec.H:80-90). */

@@ -185,7 +185,11 @@ static double column_z0(const og_grid* g, const gb_bc* bc, const double* z0map, 
 }
 
 /* Closure::evaluate (Closure.cpp:365-460) with the weight 1 (no nu_t
- * history), no cap and no gate: nu, gamma_theta, gamma_tke and nu_t on the
+ * history), the stratification gate of turb.ri_gate (gate_stratification,
+ * Closure.cpp:337-354: the length and Rt see N^2 N^4 / (N^4 + Ri_0^2 S^4),
+ * P_b keeps N^2) and the realizability cap of turb.realizability
+ * (nut_cap_field, ClosureWake.cpp:8-29: nu_t <= C_r max(k, floor) / S):
+ * nu, gamma_theta, gamma_tke and nu_t on the
  * cells -1..nx, -1..ny (their vertical ghosts copied), the length, Rt, P_s,
  * P_b, eps and the Patankar diagonal on the valid cells. out: 10 arrays in
  * that order (nu, gth, gk, nut, L, Rt, Ps, Pb, eps, dSdk). */
@@ -203,6 +207,7 @@ void og_closure_evaluate(const og_grid* g, const gb_bc* bc, const gb_physics* ph
     const double nu_mol = ph->turb_nu_molecular, alpha_mol = ph->turb_alpha_molecular;
     const double inv_sigma = 1 / ph->turb_sigma_k;
     const double wgt = 1.0;
+    const double ri0 = ph->turb_ri_gate, r2 = ri0 * ri0, cr = ph->turb_realizability;
     double *nu = out[0], *gth = out[1], *gk = out[2], *nut = out[3];
     for (int k = 0; k < g->nz; ++k) {
         for (int j = -1; j <= g->ny; ++j) {
@@ -211,10 +216,20 @@ void og_closure_evaluate(const og_grid* g, const gb_bc* bc, const gb_physics* ph
                 /* kappa (d + z0): with a map the sum d + z0(i, j) is formed
                  * first and the kernel adds z0 = 0, the same value */
                 const double l_g = geom_length(c.kappa * (dist[o] + column_z0(g, bc, z0map, i, j)), c.l_g_max);
-                const switches s = switches_for(tk[o], N2[o], l_g, &c);
-                const cpoint p = closure_point(tk[o], N2[o], S2[o], l_g, &c, s);
+                double N2c = N2[o];
+                if (ri0 > 0) {
+                    const double a = N2[o] * N2[o], b = S2[o] * S2[o];
+                    N2c *= a / (a + r2 * b + DBL_MIN);
+                }
+                const switches s = switches_for(tk[o], N2c, l_g, &c);
+                const cpoint p = closure_point(tk[o], N2c, S2[o], l_g, &c, s);
                 const double ratio = p.cmu_prime / p.cmu;
-                const double nt = wgt * fmin(p.nut, DBL_MAX) + (1 - wgt) * tk[o];
+                double cap = DBL_MAX;
+                if (cr > 0) {
+                    const double sr = sqrt(S2[o]);
+                    cap = (sr > DBL_MIN) ? cr * fmax(tk[o], c.tke_floor) / sr : DBL_MAX;
+                }
+                const double nt = wgt * fmin(p.nut, cap) + (1 - wgt) * tk[o];
                 nut[o] = nt;
                 nu[o] = nu_mol + nt;
                 gth[o] = alpha_mol + ratio * nt;

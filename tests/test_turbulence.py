@@ -496,3 +496,91 @@ def test_gpu_confidence_share_and_height(ctx):
         assert shares == sorted(shares) and 0.0 < shares[1] < 1.0
     finally:
         st.close()
+
+
+@pytest.mark.parametrize("dtdz", [0.02, -0.02])
+def test_oracle_closure_gate_and_cap(dtdz):
+    """turb.ri_gate: the length, Rt, nu_t and the heat diffusivity follow the
+    AL01 relations at N^2 N^4 / (N^4 + Ri_0^2 S^4) while P_b keeps the ungated
+    N^2 (gate_stratification, Closure.cpp:337-354); a neutral column is the
+    same bits with the gate on. turb.realizability: nu_t = min(nu_t,
+    C_r max(k, floor) / S) (ClosureWake.cpp:8-29)."""
+    case, bc, ph = closure_column_case()
+    g = case.grid
+    G = g.ng
+    zc = (np.arange(-G, g.nz + 1 + G) + 0.5) * g.dzeta
+    case.q["theta"][...] = (300.0 + dtdz * zc)[:, None, None]
+    ph.turb_max_geom_lscale = 30.0
+    case.q["tke"][...] = 0.05
+    oracle.fill_ghosts(case, bc, ph)
+    plain = oracle.closure_fields(case, bc, ph)
+    ri0 = 0.25
+    ph.turb_ri_gate = ri0
+    gated = oracle.closure_fields(case, bc, ph)
+    N2 = 9.81 / 300.0 * dtdz
+    kk = 0.05
+    changed = 0
+    for k in range(1, g.nz - 1):
+        o = (G + k, G + 3, G + 4)
+        S2 = plain["Ps"][o] / plain["nut"][o]
+        N2c = N2 * (N2 * N2) / (N2 * N2 + ri0 * ri0 * S2 * S2 + np.finfo(float).tiny)
+        d = (k + 0.5) * g.dzeta
+        lraw = KAPPA * (d + 0.1)
+        l_g = 30.0 * lraw / (30.0 + lraw)
+        L, rt, nut, nutp, eps = _al01(kk, N2c, l_g)
+        assert gated["length"][o] == pytest.approx(L, rel=1e-11)
+        assert gated["nut"][o] == pytest.approx(nut, rel=1e-10)
+        assert gated["gamma_theta"][o] == pytest.approx(nutp, rel=1e-10)
+        assert gated["Pb"][o] == pytest.approx(-nutp * N2, rel=1e-10)
+        changed += abs(gated["nut"][o] - plain["nut"][o]) > 1e-6 * plain["nut"][o]
+    assert changed > 0
+    # neutral: the gate changes nothing
+    case.q["theta"][...] = 300.0
+    oracle.fill_ghosts(case, bc, ph)
+    ph.turb_ri_gate = 0.0
+    n0 = oracle.closure_fields(case, bc, ph)
+    ph.turb_ri_gate = ri0
+    n1 = oracle.closure_fields(case, bc, ph)
+    for f in ("nu", "nut", "length", "Rt", "eps"):
+        assert np.array_equal(n0[f], n1[f]), f
+    # the realizability cap on the neutral column
+    ph.turb_ri_gate = 0.0
+    cr = 0.2
+    ph.turb_realizability = cr
+    capped = oracle.closure_fields(case, bc, ph)
+    floor = max(ph.turb_tke_floor, np.finfo(float).eps)
+    n_capped = 0
+    for k in range(0, g.nz - 1):
+        o = (G + k, G + 3, G + 4)
+        S2 = n0["Ps"][o] / n0["nut"][o]
+        cap = cr * max(case.q["tke"][o], floor) / math.sqrt(S2)
+        assert capped["nut"][o] == pytest.approx(min(n0["nut"][o], cap), rel=1e-12)
+        n_capped += cap < n0["nut"][o]
+    assert n_capped > 0
+
+
+@pytest.mark.gpu
+def test_gpu_closure_gate_and_cap_match_oracle(ctx):
+    """The stratification gate and the realizability cap on the GPU over a
+    stratified hill: the closure's fields and the residuals equal the
+    oracle's (1e-11 relative)."""
+    case, bc, ph = _hill_case()
+    g = case.grid
+    G = g.ng
+    case.q["theta"][...] = 300.0 + 0.01 * np.arange(case.q["theta"].shape[0])[:, None, None] * 40.0
+    ph.turb_ri_gate, ph.turb_realizability = 0.25, 0.3
+    dc, st = _stage(ctx, case, bc, ph)
+    try:
+        oracle.fill_ghosts(case, bc, ph)
+        R_ref, cf_ref, _ = oracle.residual(case, bc, ph, fields=True)
+        st.fill_ghosts()
+        R = [r.cpu().numpy() for r in st.residual()]
+        cf, _ = st.turbulence()
+        for f in ("nu", "gamma_theta", "gamma_tke", "nut", "length", "Ps", "Pb", "eps", "dSdk"):
+            ref, got = _cells(g, cf_ref[f]), _cells(g, cf[f])
+            assert np.abs(got - ref).max() <= 1e-11 * max(np.abs(ref).max(), 1e-300), f
+        for n, loc in enumerate(LOCS):
+            v = g.valid(loc)
+            assert np.abs(R[n][v] - R_ref[n][v]).max() <= 1e-10 * max(np.abs(R_ref[n][v]).max(), 1e-300), n
+    finally:
+        st.close()
