@@ -95,7 +95,7 @@ class Physics(ctypes.Structure):
                 ("turb_tke_floor", ctypes.c_double), ("turb_sigma_k", ctypes.c_double),
                 ("turb_nu_molecular", ctypes.c_double), ("turb_alpha_molecular", ctypes.c_double),
                 ("turb_kappa", ctypes.c_double), ("turb_ri_gate", ctypes.c_double),
-                ("turb_realizability", ctypes.c_double)]
+                ("turb_realizability", ctypes.c_double), ("turb_nut_relax", ctypes.c_double)]
 
     @classmethod
     def make(cls, scale_height, **kw):
@@ -110,7 +110,7 @@ class Physics(ctypes.Structure):
                 scale_height=scale_height, closure=0, turb_Cmu0=0.5562, turb_Cb=0.35, turb_Rt_crit=-1.0,
                 turb_Rt_min=-3.0, turb_max_geom_lscale=30.0, turb_tke_floor=0.0, turb_sigma_k=1.0,
                 turb_nu_molecular=0.0, turb_alpha_molecular=0.0, turb_kappa=0.41, turb_ri_gate=0.0,
-                turb_realizability=0.0)
+                turb_realizability=0.0, turb_nut_relax=1.0)
         for k, v in kw.items():
             if k == "pressure_gradient":
                 for d in range(3):

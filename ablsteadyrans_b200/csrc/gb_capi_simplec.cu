@@ -235,6 +235,7 @@ gb_status check_closure(const gb_physics& ph)
         {"kappa", ph.turb_kappa, ph.turb_kappa > 0, "finite and > 0"},
         {"ri_gate", ph.turb_ri_gate, ph.turb_ri_gate == 0 || (ph.turb_ri_gate >= 1e-6 && ph.turb_ri_gate <= 1),
          "0 (off) or finite, >= 1e-6 and <= 1"},
+        {"nut_relax", ph.turb_nut_relax, ph.turb_nut_relax > 0 && ph.turb_nut_relax <= 1, "finite, > 0 and <= 1"},
         {"realizability", ph.turb_realizability,
          ph.turb_realizability == 0 || (ph.turb_realizability >= 0.01 && ph.turb_realizability <= 10),
          "0 (off) or finite, >= 0.01 and <= 10"},

@@ -282,6 +282,10 @@ struct gb_simplec {
     // residual (SimplecStage::nu, Simplec.H:214; 0 before the first)
     double* nu_dtau{nullptr};
     double* agl{nullptr};                // height above the ground for the confidence test (made on first use)
+    // the closure's nu_t history (Closure::accept, Closure.cpp:471-479): the
+    // nu_t of the last iteration's residual, blended by turb.nut_relax < 1
+    double* nut_hist{nullptr};
+    bool has_hist{false};
     double* ss[gb::kSsPlanes]{};         // the surface state of the iteration's first fill
     double* ssr[gb::kSsPlanes]{};        // the residual's own surface state
     double* sst[gb::kSsPlanes]{};        // the later fills' surface state
@@ -1094,7 +1098,9 @@ void simplec_residual(gb_simplec* S, const gb_state& q, double** R)
     const int64_t vol = volume(g);
     for (int n = 0; n < 6; ++n) { cudaMemsetAsync(R[n], 0, sizeof(double) * vol, ctx->stream); }
     // the closure's fields and the wall state at q (Residual.cpp:166-176, 205-208)
-    if (S->ph.closure) { turb_closure(ctx, g, S->bc, S->ph, q, S->z, S->dist, S->mesh.z0, S->cf); }
+    if (S->ph.closure) {
+        turb_closure(ctx, g, S->bc, S->ph, q, S->z, S->dist, S->mesh.z0, S->cf, S->has_hist ? S->nut_hist : nullptr);
+    }
     if (S->wall) { turb_surface_state(ctx, g, S->bc, S->ph, q, S->z, S->mesh.z0, S->ssr, dword(ctx, W_SURFACE_BAD)); }
     double** F = S->w.F;
     transport_fluxes(S, q, F[0], F[1], F[2]);
@@ -1754,6 +1760,11 @@ gb_status simplec_iterate(gb_simplec* S, const gb_state& q, const double* dtau, 
         });
     }
     if ((st = scalar_sweeps(S, q, dtau)) != GB_OK) { return st; }
+    // 6. the nu_t history (Closure::accept): the fields of this iteration's residual
+    if (S->ph.closure) {
+        cudaMemcpyAsync(S->nut_hist, S->cf[kClosureNut], sizeof(double) * volume(g), cudaMemcpyDeviceToDevice, ctx->stream);
+        S->has_hist = true;
+    }
     // read every result of the iteration at once
     unsigned long long words[W_COUNT];
     if ((st = read_words(ctx, 0, W_COUNT, words)) != GB_OK) { return st; }
@@ -2345,6 +2356,7 @@ gb_status simplec_build(gb_simplec* S)
         for (int n = 0; n < kClosureFields; ++n) { turb_ok = (S->cf[n] = dbuf(S, vol)) && turb_ok; }
         turb_ok = (S->dist = dbuf(S, vol)) && turb_ok;
         turb_ok = (S->nu_dtau = dbuf(S, vol)) && turb_ok;
+        turb_ok = (S->nut_hist = dbuf(S, vol)) && turb_ok;
         S->dfe = gb_diffusivities{S->cf[kClosureNu], S->cf[kClosureGammaTheta], S->cf[kClosureGammaTke]};
     }
     if (S->wall) {

@@ -227,7 +227,7 @@ void turb_height_above_ground(gb_ctx* ctx, const gb_grid& g, const double* z, do
 }
 
 void turb_closure(gb_ctx* ctx, const gb_grid& g, const gb_bc& bc, const gb_physics& ph, const gb_state& q,
-                  const double* z, const double* dist, const double* z0map, double* const* cf)
+                  const double* z, const double* dist, const double* z0map, double* const* cf, const double* nut_prev)
 {
     const gb_grid gg = g;
     const ClosureConst c = closure_constants(ph);
@@ -238,6 +238,9 @@ void turb_closure(gb_ctx* ctx, const gb_grid& g, const gb_bc& bc, const gb_physi
     // turb.realizability (nut_cap_field, ClosureWake.cpp:8-29)
     const double ri0 = ph.turb_ri_gate, r2 = ri0 * ri0, cr = ph.turb_realizability;
     const bool gate = ri0 > 0, capped = cr > 0;
+    // the nu_t relaxation (Closure.cpp:407-411): the history when there is
+    // one, else k with the weight 1 - w = 0
+    const double wgt = nut_prev ? ph.turb_nut_relax : 1.0;
     // the ground's roughness in kappa (d + z0): a map, the uniform value, or 0
     // without a surface layer (ground_roughness, SurfaceLayer.H:176-181)
     const bool wall = bc.face[2] == GB_FACE_SURFACE_LAYER;
@@ -248,6 +251,7 @@ void turb_closure(gb_ctx* ctx, const gb_grid& g, const gb_bc& bc, const gb_physi
     const double* w = q.w;
     const double* th = q.theta;
     const double* tk = q.tke;
+    const double* prev = nut_prev ? nut_prev : q.tke;
     ClosureOut O{};
     for (int n = 0; n < kClosureFields; ++n) { O.p[n] = cf[n]; }
     for_box(ctx, Box{{-1, -1, 0}, {g.nx, g.ny, g.nz - 1}}, [=] __device__(int i, int j, int k) {
@@ -286,7 +290,7 @@ void turb_closure(gb_ctx* ctx, const gb_grid& g, const gb_bc& bc, const gb_physi
             const double sr = sqrt(S2);
             cap = (sr > DBL_MIN) ? cr * fmax(tk[o], c.tke_floor) / sr : DBL_MAX;
         }
-        const double nt = 1.0 * fmin(p.nut, cap) + (1.0 - 1.0) * tk[o];
+        const double nt = wgt * fmin(p.nut, cap) + (1 - wgt) * prev[o];
         O.p[kClosureNut][o] = nt;
         O.p[kClosureNu][o] = nu_mol + nt;
         O.p[kClosureGammaTheta][o] = alpha_mol + ratio * nt;

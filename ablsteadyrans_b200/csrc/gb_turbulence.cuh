@@ -69,8 +69,11 @@ void turb_height_above_ground(gb_ctx* ctx, const gb_grid& g, const double* z, do
 
 //! Closure::evaluate (Closure.cpp:365-460) with the weight 1, no cap and no
 //! gate, at the state q (ghosts filled): cf[kClosure*].
+//! nut_prev: the nu_t of the last accepted iteration (turb.nut_relax < 1
+//! blends with it), or null (no history yet: the weight is 1).
 void turb_closure(gb_ctx* ctx, const gb_grid& g, const gb_bc& bc, const gb_physics& ph, const gb_state& q,
-                  const double* z, const double* dist, const double* z0map, double* const* cf);
+                  const double* z, const double* dist, const double* z0map, double* const* cf,
+                  const double* nut_prev = nullptr);
 
 //! compute_surface_state's columns (SurfaceLayer.cpp:97-230) into ss; the
 //! columns without a positive, finite u* (or with a non-finite k_w) are

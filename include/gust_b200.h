@@ -350,6 +350,8 @@ typedef struct gb_physics {
     double turb_ri_gate;                          /* turb.ri_gate: 0 off, or Ri_0 in [1e-6, 1] (the stratification
                                                      gate of the length and Rt; P_b keeps N^2) */
     double turb_realizability;                    /* turb.realizability: 0 off, or C_r in [0.01, 10] (nu_t <= C_r k / S) */
+    double turb_nut_relax;                        /* turb.nut_relax in (0, 1]: nu_t = w nu_t,new + (1 - w) nu_t of the
+                                                     last iteration (1: no history) */
 } gb_physics;
 
 /* simplec.* and steady.zline_sweeps (gust::SimplecOptions, Source/Simplec.H:80-90). */

@@ -253,6 +253,7 @@ def _declare_simplec(L):
     L.og_implicit_rows2.argtypes = [G, ctypes.POINTER(BC), ctypes.POINTER(Physics), i32, P, P, P, P, P,
                                     ctypes.POINTER(Diffusivities), PP, PP, P]
     L.og_prolong_fields.argtypes = [G, ctypes.POINTER(State), G, ctypes.POINTER(State), i32]
+    L.og_set_nut_history.argtypes = [P]
     L.og_restrict_state.argtypes = [G, ctypes.POINTER(State), ctypes.POINTER(MeshFields), G, ctypes.POINTER(State),
                                     ctypes.POINTER(MeshFields), i32, P]
     L.og_prolong_state.argtypes = [G, ctypes.POINTER(State), G, ctypes.POINTER(State), i32, ctypes.POINTER(BC),
@@ -300,6 +301,7 @@ class Case:
         self.q = {f: grid.np_zeros() for f in self.FIELDS}
         self.cf = None                     # the closure's fields of the last iteration (with turbulence)
         self.closure_nu = None             # nu the next local dtau reads (0 before the first iteration)
+        self.nut_hist = None               # the closure's nu_t history (Closure::accept), None before the first
 
     def state(self):
         from ablsteadyrans_b200.abi import State
@@ -317,6 +319,7 @@ class Case:
     def copy(self):
         c = Case(self.grid, self.z, self.J, self.ax, self.ay, self.az, self.nu, self.gt, self.gk, self.z0map)
         c.q = {f: a.copy() for f, a in self.q.items()}
+        c.nut_hist = None if self.nut_hist is None else self.nut_hist.copy()
         return c
 
     def plane(self):
@@ -355,6 +358,7 @@ def fill_ghosts(case, bc, phys=None):
 def residual(case, bc, phys, fields=False):
     """Residual.cpp:159-256 at the case's state (ghosts filled by the caller);
     with fields=True also (closure fields, surface state) as dicts."""
+    _history(case)
     R = [case.grid.np_zeros() for _ in range(6)]
     cf = [case.grid.np_zeros() for _ in CLOSURE_FIELDS]
     ss = [case.plane() for _ in SURFACE_FIELDS]
@@ -368,6 +372,7 @@ def residual(case, bc, phys, fields=False):
 
 def closure_fields(case, bc, phys):
     """Closure::evaluate at the case's state (ghosts filled): dict of volumes."""
+    _history(case)
     q = case.q
     cf = [case.grid.np_zeros() for _ in CLOSURE_FIELDS]
     _L().og_closure_evaluate(ctypes.byref(case.grid.c), ctypes.byref(bc), ctypes.byref(phys), _p(q["u"]), _p(q["v"]),
@@ -453,9 +458,18 @@ def local_dtau(case, cfl, use_nu=True, nu=None, phys=None):
     return dt
 
 
+def _history(case):
+    """The closure's nu_t history of the case for the next evaluations."""
+    h = getattr(case, "nut_hist", None)
+    _L().og_set_nut_history(_p(h) if h is not None else None)
+
+
 def simplec_iterate(case, bc, phys, opts, dtau):
-    """One SimplecStage::iterate (Simplec.cpp:452-506); returns (status, IterInfo, R)."""
+    """One SimplecStage::iterate (Simplec.cpp:452-506); returns (status, IterInfo, R).
+    With the closure the iteration's nu_t becomes the case's history
+    (Closure::accept)."""
     from ablsteadyrans_b200.abi import IterInfo
+    _history(case)
     R = [case.grid.np_zeros() for _ in range(6)]
     arr = (ctypes.c_void_p * 6)(*[r.ctypes.data for r in R])
     info = IterInfo()
@@ -467,6 +481,7 @@ def simplec_iterate(case, bc, phys, opts, dtau):
                                   ctypes.byref(info), None if case.cf is None else _arrays(case.cf), None)
     if phys.closure:
         case.closure_nu = case.cf[0]
+        case.nut_hist = case.cf[3].copy()
     return int(rc), info, R
 
 

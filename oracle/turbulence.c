@@ -184,8 +184,9 @@ static double column_z0(const og_grid* g, const gb_bc* bc, const double* z0map, 
     return z0map ? z0map[(int64_t)(i + g->ng) + (int64_t)(j + g->ng) * g->sy] : bc->surface_z0;
 }
 
-/* Closure::evaluate (Closure.cpp:365-460) with the weight 1 (no nu_t
- * history), the stratification gate of turb.ri_gate (gate_stratification,
+/* Closure::evaluate (Closure.cpp:365-460) with the nu_t relaxation against
+ * the history og_set_nut_history gave (weight 1 without one), the
+ * stratification gate of turb.ri_gate (gate_stratification,
  * Closure.cpp:337-354: the length and Rt see N^2 N^4 / (N^4 + Ri_0^2 S^4),
  * P_b keeps N^2) and the realizability cap of turb.realizability
  * (nut_cap_field, ClosureWake.cpp:8-29: nu_t <= C_r max(k, floor) / S):
@@ -193,6 +194,12 @@ static double column_z0(const og_grid* g, const gb_bc* bc, const double* z0map, 
  * cells -1..nx, -1..ny (their vertical ghosts copied), the length, Rt, P_s,
  * P_b, eps and the Patankar diagonal on the valid cells. out: 10 arrays in
  * that order (nu, gth, gk, nut, L, Rt, Ps, Pb, eps, dSdk). */
+/* The nu_t history of Closure::accept (Closure.cpp:471-479) that
+ * og_closure_evaluate blends with (turb.nut_relax < 1); NULL: none. The
+ * Python side sets it from the case before each evaluation. */
+static const double* g_nut_prev = NULL;
+void og_set_nut_history(const double* prev) { g_nut_prev = prev; }
+
 void og_closure_evaluate(const og_grid* g, const gb_bc* bc, const gb_physics* ph, const double* u, const double* v,
                          const double* w, const double* th, const double* tk, const double* z, const double* z0map,
                          double** out)
@@ -206,7 +213,8 @@ void og_closure_evaluate(const og_grid* g, const gb_bc* bc, const gb_physics* ph
     og_stratification_and_strain(g, ph, u, v, w, th, z, N2, S2);
     const double nu_mol = ph->turb_nu_molecular, alpha_mol = ph->turb_alpha_molecular;
     const double inv_sigma = 1 / ph->turb_sigma_k;
-    const double wgt = 1.0;
+    const double wgt = g_nut_prev ? ph->turb_nut_relax : 1.0;
+    const double* prev = g_nut_prev ? g_nut_prev : tk;
     const double ri0 = ph->turb_ri_gate, r2 = ri0 * ri0, cr = ph->turb_realizability;
     double *nu = out[0], *gth = out[1], *gk = out[2], *nut = out[3];
     for (int k = 0; k < g->nz; ++k) {
@@ -229,7 +237,7 @@ void og_closure_evaluate(const og_grid* g, const gb_bc* bc, const gb_physics* ph
                     const double sr = sqrt(S2[o]);
                     cap = (sr > DBL_MIN) ? cr * fmax(tk[o], c.tke_floor) / sr : DBL_MAX;
                 }
-                const double nt = wgt * fmin(p.nut, cap) + (1 - wgt) * tk[o];
+                const double nt = wgt * fmin(p.nut, cap) + (1 - wgt) * prev[o];
                 nut[o] = nt;
                 nu[o] = nu_mol + nt;
                 gth[o] = alpha_mol + ratio * nt;

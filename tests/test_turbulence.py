@@ -584,3 +584,55 @@ def test_gpu_closure_gate_and_cap_match_oracle(ctx):
             assert np.abs(R[n][v] - R_ref[n][v]).max() <= 1e-10 * max(np.abs(R_ref[n][v]).max(), 1e-300), n
     finally:
         st.close()
+
+
+def test_oracle_nut_relaxation_blends_with_the_history():
+    """turb.nut_relax = w: after an iteration the closure's nu_t is w times
+    the new one plus 1 - w times the last iteration's (Closure.cpp:407-436),
+    and the diffusivities follow it; before the first iteration there is no
+    history and the weight is 1."""
+    from ablsteadyrans_b200.abi import SimplecOptions
+    case, bc, ph = _hill_case()
+    ph.turb_nut_relax = 0.4
+    oracle.fill_ghosts(case, bc, ph)
+    first = oracle.closure_fields(case, bc, ph)
+    ph.turb_nut_relax = 1.0
+    plain = oracle.closure_fields(case, bc, ph)
+    assert np.array_equal(first["nut"], plain["nut"])      # no history yet
+    ph.turb_nut_relax = 0.4
+    oracle.simplec_iterate(case, bc, ph, SimplecOptions.make(), oracle.local_dtau(case, 2.0, phys=ph))
+    hist = case.nut_hist.copy()
+    oracle.fill_ghosts(case, bc, ph)
+    relaxed = oracle.closure_fields(case, bc, ph)
+    ph.turb_nut_relax = 1.0
+    case.nut_hist = None
+    new = oracle.closure_fields(case, bc, ph)
+    v = case.grid.valid(0)
+    expect = 0.4 * new["nut"][v] + (1 - 0.4) * hist[v]
+    assert np.abs(relaxed["nut"][v] - expect).max() <= 1e-14 * np.abs(expect).max()
+    assert np.abs(relaxed["nu"][v] - (ph.turb_nu_molecular + relaxed["nut"][v])).max() == 0
+
+
+@pytest.mark.gpu
+def test_gpu_nut_relaxation_iterations_match_oracle(ctx):
+    """turb.nut_relax = 0.5 on the GPU: three SIMPLEC iterations (each
+    blending the closure's nu_t with the last one's) equal the oracle's."""
+    from ablsteadyrans_b200.abi import SimplecOptions
+    case, bc, ph = _hill_case()
+    ph.turb_nut_relax = 0.5
+    opts = dict(pressure_reltol=1e-11, zline_sweeps=3)
+    dc, st = _stage(ctx, case, bc, ph, **opts)
+    oracle.fill_ghosts(case, bc, ph)
+    st.fill_ghosts()
+    so = SimplecOptions.make(**opts)
+    try:
+        for it in range(3):
+            rc, _, _ = oracle.simplec_iterate(case, bc, ph, so, oracle.local_dtau(case, 2.0, phys=ph))
+            assert rc == 0
+            st.iterate(st.local_dtau(2.0))
+            for f, loc in zip(FIELDS, LOCS):
+                v = case.grid.valid(loc)
+                ref, got = case.q[f][v], dc.host(f)[v]
+                assert np.abs(got - ref).max() <= 1e-9 * max(np.abs(ref).max(), 1e-300), (it, f)
+    finally:
+        st.close()
