@@ -44,7 +44,10 @@ class BC(ctypes.Structure):
                 ("surface_wall_k", ctypes.c_int32), ("surface_denominator_floor", ctypes.c_int32),
                 ("rayleigh_zdamp", ctypes.c_double), ("rayleigh_dampcoef", ctypes.c_double),
                 ("rayleigh_fields", ctypes.c_int32), ("rayleigh_above_ground", ctypes.c_int32),
-                ("sponge_width", ctypes.c_double), ("sponge_strength", ctypes.c_double)]
+                ("sponge_width", ctypes.c_double), ("sponge_strength", ctypes.c_double),
+                ("surface_qnse", ctypes.c_int32), ("surface_qnse_am", ctypes.c_double),
+                ("surface_qnse_bm", ctypes.c_double), ("surface_qnse_ah", ctypes.c_double),
+                ("surface_qnse_bh", ctypes.c_double)]
 
     @classmethod
     def make(cls, faces, theta_ref=((0.0,), (300.0,)), ustar=0.4, z0=0.1, direction=0.0, kappa=0.41, Cmu0=0.5562,
@@ -61,6 +64,7 @@ class BC(ctypes.Structure):
             setattr(b, ("sponge_" if k in ("width", "strength") else "rayleigh_") + k, v)
         b.surface_z0, b.surface_zref, b.surface_stability = 0.1, 0.0, SURFACE_NEUTRAL
         b.surface_heat_flux, b.surface_wall_k, b.surface_denominator_floor = 0.0, WALL_K_DIRICHLET, DENOMINATOR_LOG_LAW
+        b.surface_qnse, b.surface_qnse_am, b.surface_qnse_bm, b.surface_qnse_ah, b.surface_qnse_bh = 0, 2.5, 0.2, 2.5, 0.2
         for k, v in (surface or {}).items():
             setattr(b, "surface_" + k, v)
         for n, f in enumerate(faces):

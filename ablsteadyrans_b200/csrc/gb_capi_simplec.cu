@@ -144,6 +144,27 @@ gb_status check_bc(const gb_grid& g, const gb_bc& bc)
             gb::set_error("gust: invalid inputs:\n  bc.surface_wall_k must be dirichlet or source");
             return GB_BAD_ARG;
         }
+        // check_surface_layer_options (SurfaceLayer.cpp:250-292): QNSE's b > 0 and a >= b
+        if (bc.surface_qnse != 0 && bc.surface_qnse != 1) {
+            gb::set_error("gust: invalid inputs:\n  bc.surface_stable_functions must be businger_dyer or qnse");
+            return GB_BAD_ARG;
+        }
+        if (bc.surface_qnse) {
+            const double a[2] = {bc.surface_qnse_am, bc.surface_qnse_ah}, b[2] = {bc.surface_qnse_bm, bc.surface_qnse_bh};
+            const char* an[2] = {"qnse_am", "qnse_ah"};
+            const char* bn[2] = {"qnse_bm", "qnse_bh"};
+            for (int n = 0; n < 2; ++n) {
+                if (std::isnan(b[n]) || !(b[n] > 0 && std::isfinite(b[n]))) {
+                    gb::set_error("gust: invalid inputs:\n  surface layer %s = %g: must be finite and > 0", bn[n], b[n]);
+                    return GB_BAD_ARG;
+                }
+                if (!(std::isfinite(a[n]) && a[n] >= b[n])) {
+                    gb::set_error("gust: invalid inputs:\n  surface layer %s = %g: must be finite and >= %s = %g", an[n], a[n],
+                                  bn[n], b[n]);
+                    return GB_BAD_ARG;
+                }
+            }
+        }
         if (bc.surface_denominator_floor != GB_DENOMINATOR_LOG_LAW && bc.surface_denominator_floor != GB_DENOMINATOR_ONE) {
             gb::set_error("gust: invalid inputs:\n  bc.surface_denominator_floor must be log_law or one");
             return GB_BAD_ARG;

@@ -143,21 +143,35 @@ __device__ __forceinline__ void tangential_wind_ground(const double* u, const do
     for (int d = 0; d < 3; ++d) { ut[d] = U[d] - un * n[d]; }
 }
 
-//! Businger-Dyer psi_m (ERF's calc_psi_m, StabilityFunctions.H most_psi_m).
-__device__ __forceinline__ double psi_m(double zeta)
+//! The stable side's coefficients (StabilityFunctions.H StableCoefficients):
+//! Businger-Dyer (5, 0, 5, 0) or QNSE's from the options.
+struct Stable {
+    bool qnse;
+    double am, bm, ah, bh;
+};
+
+__host__ Stable stable_of(const gb_bc& bc)
+{
+    if (bc.surface_qnse) { return {true, bc.surface_qnse_am, bc.surface_qnse_bm, bc.surface_qnse_ah, bc.surface_qnse_bh}; }
+    return {false, 5.0, 0.0, 5.0, 0.0};
+}
+
+//! psi_m (StabilityFunctions.H most_psi_m): the Businger-Dyer unstable side
+//! (ERF's calc_psi_m), the stable side -5 zeta or QNSE's -((a - b)/b) ln(1 + b zeta).
+__device__ __forceinline__ double psi_m(double zeta, const Stable& sc)
 {
     const double az = fabs(zeta);
     const double zs = 0.5 * (az + zeta), zu = 0.5 * (zeta - az);
-    if (zeta > 0) { return -5.0 * zs; }
+    if (zeta > 0) { return sc.qnse ? -((sc.am - sc.bm) / sc.bm) * log(1.0 + sc.bm * zs) : -5.0 * zs; }
     const double x = sqrt(sqrt(1.0 - 16.0 * zu));
     const double pi = 3.14159265358979323846264338327950288;
     return 2.0 * log(0.5 * (1.0 + x)) + log(0.5 * (1.0 + x * x)) - 2.0 * atan(x) + pi / 2.0;
 }
 
-//! most_phi (StabilityFunctions.H) with the Businger-Dyer stable side.
-__device__ __forceinline__ void most_phi(double zeta, double& phi_m, double& phi_h)
+//! most_phi (StabilityFunctions.H) with the stable side's coefficients.
+__device__ __forceinline__ void most_phi(double zeta, const Stable& sc, double& phi_m, double& phi_h)
 {
-    const double one = 1, gamma = 16, am = 5, bm = 0, ah = 5, bh = 0;
+    const double one = 1, gamma = 16, am = sc.am, bm = sc.bm, ah = sc.ah, bh = sc.bh;
     const double az = fabs(zeta);
     const double zs = 0.5 * (az + zeta);
     const double zu = 0.5 * (zeta - az);
@@ -169,6 +183,7 @@ __device__ __forceinline__ void most_phi(double zeta, double& phi_m, double& phi
 //! u - kappa U / max(ln((d + z0)/z0) - psi_m(d/L(u)), m) (MostRelation, SurfaceLayer.cpp:78-95).
 struct MostRelation {
     double kappa, U, d, lz, den_min, gq, ustar_min;
+    Stable sc;
     __device__ double inv_L(double u) const
     {
         const double uf = fmax(u, ustar_min);
@@ -177,7 +192,7 @@ struct MostRelation {
     __device__ double operator()(double u) const
     {
         const double zeta = fmax(fmin(d * inv_L(u), 100.0), -100.0);
-        return u - kappa * U / fmax(lz - psi_m(zeta), den_min);
+        return u - kappa * U / fmax(lz - psi_m(zeta, sc), den_min);
     }
 };
 
@@ -323,6 +338,7 @@ void turb_surface_state(gb_ctx* ctx, const gb_grid& g, const gb_bc& bc, const gb
     const double eps = DBL_EPSILON, tol = 64 * eps, hrel = std::sqrt(eps);
     const double z0u = bc.surface_z0;
     const double dxinv = 1.0 / g.dx, dyinv = 1.0 / g.dy;
+    const Stable sc = stable_of(bc);
     const double* u = q.u;
     const double* v = q.v;
     const double* w = q.w;
@@ -359,7 +375,7 @@ void turb_surface_state(gb_ctx* ctx, const gb_grid& g, const gb_bc& bc, const gb
         double ustar = kappa * U / fmax(lz, den_min);
         double invL = 0;
         if (heat) {
-            const MostRelation F{kappa, U, d, lz, den_min, gq, 0.001};
+            const MostRelation F{kappa, U, d, lz, den_min, gq, 0.001, sc};
             bool converged = false;
             for (int it = 0; it < 50 && !converged; ++it) {
                 const double fu = F(ustar);
@@ -398,6 +414,7 @@ void turb_ground_gradients(gb_ctx* ctx, const gb_grid& g, const gb_bc& bc, const
 {
     const gb_grid gg = g;
     const double unset = DBL_MAX;
+    const Stable sc = stable_of(bc);
     const double kappa = bc.kappa;
     const double qs = (bc.surface_stability == GB_SURFACE_HEAT_FLUX) ? bc.surface_heat_flux : 0.0;
     const double z0u = bc.surface_z0;
@@ -413,7 +430,7 @@ void turb_ground_gradients(gb_ctx* ctx, const gb_grid& g, const gb_bc& bc, const
         }
         const double zeta = fmax(fmin(S.p[kSsD0][p] * S.p[kSsInvL][p], 100.0), -100.0);
         double phi_m, phi_h;
-        most_phi(zeta, phi_m, phi_h);
+        most_phi(zeta, sc, phi_m, phi_h);
         const double z0 = z0map ? z0map[p] : z0u;
         const double s = kappa * (S.p[kSsD0][p] + z0);
         const double tx = S.p[kSsTauX][p], ty = S.p[kSsTauY][p], tz = S.p[kSsTauZ][p];

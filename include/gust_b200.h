@@ -322,6 +322,11 @@ typedef struct gb_bc {
     int32_t rayleigh_above_ground;   /* bc.rayleigh_height: 0 absolute, 1 above_ground */
     double sponge_width;             /* bc.sponge_width (m; 0: off) */
     double sponge_strength;          /* bc.sponge_strength (1/s) */
+    /* bc.surface_stable_functions: 0 businger_dyer, 1 qnse (the stable side
+     * phi = (1 + a zeta)/(1 + b zeta), psi = -((a - b)/b) ln(1 + b zeta) with
+     * bc.surface_qnse_am, _bm, _ah, _bh; StabilityFunctions.H) */
+    int32_t surface_qnse;
+    double surface_qnse_am, surface_qnse_bm, surface_qnse_ah, surface_qnse_bh;
 } gb_bc;
 
 /* The residual's physics inputs (gust::ResidualInputs, Source/Residual.H:61-128;

@@ -292,21 +292,42 @@ static void tangential_wind_ground(const og_grid* g, const double* u, const doub
     for (int d = 0; d < 3; ++d) { ut[d] = U[d] - un * n[d]; }
 }
 
-/* Businger-Dyer psi_m (ERF_MOSTUtils.H:102-111, StabilityFunctions.H most_psi_m). */
-static double psi_m(double zeta)
+/* The stable side (StabilityFunctions.H StableCoefficients): Businger-Dyer
+ * (5, 0, 5, 0) or QNSE's coefficients from bc.surface_qnse_*. */
+typedef struct {
+    int qnse;
+    double am, bm, ah, bh;
+} stable_c;
+
+static stable_c stable_of(const gb_bc* bc)
+{
+    stable_c s = {0, 5.0, 0.0, 5.0, 0.0};
+    if (bc->surface_qnse) {
+        s.qnse = 1;
+        s.am = bc->surface_qnse_am;
+        s.bm = bc->surface_qnse_bm;
+        s.ah = bc->surface_qnse_ah;
+        s.bh = bc->surface_qnse_bh;
+    }
+    return s;
+}
+
+/* psi_m (ERF_MOSTUtils.H:102-111 unstable side, StabilityFunctions.H
+ * most_psi_m): the stable side -5 zeta or -((a - b)/b) ln(1 + b zeta). */
+static double psi_m(double zeta, const stable_c* sc)
 {
     const double az = fabs(zeta);
     const double zs = 0.5 * (az + zeta), zu = 0.5 * (zeta - az);
-    if (zeta > 0) { return -5.0 * zs; }
+    if (zeta > 0) { return sc->qnse ? -((sc->am - sc->bm) / sc->bm) * log(1.0 + sc->bm * zs) : -5.0 * zs; }
     const double x = sqrt(sqrt(1.0 - 16.0 * zu));
     const double pi = 3.14159265358979323846264338327950288;
     return 2.0 * log(0.5 * (1.0 + x)) + log(0.5 * (1.0 + x * x)) - 2.0 * atan(x) + pi / 2.0;
 }
 
-/* most_phi (StabilityFunctions.H) with the Businger-Dyer stable side. */
-static void most_phi(double zeta, double* phi_m, double* phi_h)
+/* most_phi (StabilityFunctions.H) with the stable side's coefficients. */
+static void most_phi(double zeta, const stable_c* sc, double* phi_m, double* phi_h)
 {
-    const double one = 1, gamma = 16, am = 5, bm = 0, ah = 5, bh = 0;
+    const double one = 1, gamma = 16, am = sc->am, bm = sc->bm, ah = sc->ah, bh = sc->bh;
     const double az = fabs(zeta);
     const double zs = 0.5 * (az + zeta);
     const double zu = 0.5 * (zeta - az);
@@ -317,6 +338,7 @@ static void most_phi(double zeta, double* phi_m, double* phi_h)
 
 typedef struct {
     double kappa, U, d, lz, den_min, gq, ustar_min;
+    stable_c sc;
 } most_rel;
 
 static double most_inv_L(const most_rel* F, double u)
@@ -328,7 +350,7 @@ static double most_inv_L(const most_rel* F, double u)
 static double most_F(const most_rel* F, double u)
 {
     const double zeta = fmax(fmin(F->d * most_inv_L(F, u), 100.0), -100.0);
-    return u - F->kappa * F->U / fmax(F->lz - psi_m(zeta), F->den_min);
+    return u - F->kappa * F->U / fmax(F->lz - psi_m(zeta, &F->sc), F->den_min);
 }
 
 static int reference_interval(const og_grid* g, const double* z, int i, int j, int n, double zr)
@@ -389,7 +411,7 @@ int og_surface_state(const og_grid* g, const gb_bc* bc, const gb_physics* ph, co
             double ustar = kappa * U / fmax(lz, den_min);
             double invL = 0;
             if (heat) {
-                const most_rel F = {kappa, U, d, lz, den_min, gq, 0.001};
+                const most_rel F = {kappa, U, d, lz, den_min, gq, 0.001, stable_of(bc)};
                 int converged = 0;
                 for (int it = 0; it < 50 && !converged; ++it) {
                     const double fu = most_F(&F, ustar);
@@ -429,6 +451,7 @@ int og_surface_state(const og_grid* g, const gb_bc* bc, const gb_physics* ph, co
  * column for the rest (:614-648). gg: 3 planes. */
 void og_ground_gradients(const og_grid* g, const gb_bc* bc, const double* const* ss, const double* z0map, double** gg)
 {
+    const stable_c sc = stable_of(bc);
     const double unset = DBL_MAX;
     const double kappa = bc->kappa;
     const double qs = (bc->surface_stability == GB_SURFACE_HEAT_FLUX) ? bc->surface_heat_flux : 0.0;
@@ -442,7 +465,7 @@ void og_ground_gradients(const og_grid* g, const gb_bc* bc, const double* const*
             const int64_t p = PX(g, i, j);
             const double zeta = fmax(fmin(ss[3][p] * ss[4][p], 100.0), -100.0);
             double phi_m, phi_h;
-            most_phi(zeta, &phi_m, &phi_h);
+            most_phi(zeta, &sc, &phi_m, &phi_h);
             const double z0 = z0map ? z0map[p] : bc->surface_z0;
             const double s = kappa * (ss[3][p] + z0);
             const double tx = ss[5][p], ty = ss[6][p], tz = ss[7][p];

@@ -636,3 +636,56 @@ def test_gpu_nut_relaxation_iterations_match_oracle(ctx):
                 assert np.abs(got - ref).max() <= 1e-9 * max(np.abs(ref).max(), 1e-300), (it, f)
     finally:
         st.close()
+
+
+def test_oracle_surface_layer_qnse_stable_side():
+    """bc.surface_stable_functions = qnse under a downward heat flux: u*
+    solves the MOST relation with QNSE's stable psi_m = -((a - b)/b)
+    ln(1 + b zeta) (StabilityFunctions.H), which lowers u* less than
+    Businger-Dyer's -5 zeta; the range checks refuse b <= 0 and a < b."""
+    from ablsteadyrans_b200.abi import SURFACE_HEAT_FLUX
+    case, bc, ph = closure_column_case()
+    bc.surface_stability, bc.surface_heat_flux = SURFACE_HEAT_FLUX, -0.02
+    oracle.fill_ghosts(case, bc, ph)
+    bd, _ = oracle.surface_state(case, bc, ph)
+    bc.surface_qnse = 1
+    ss, bad = oracle.surface_state(case, bc, ph)
+    assert bad == 0
+    g = case.grid
+    p = (g.ng + 2) * int(g.c.sy) + g.ng + 3
+    us, U, d0, invL = ss["ustar"][p], ss["speed"][p], ss["d0"][p], ss["inv_L"][p]
+    zeta = max(min(d0 * invL, 100.0), -100.0)
+    assert zeta > 0
+    am, bm = bc.surface_qnse_am, bc.surface_qnse_bm
+    psi = -((am - bm) / bm) * math.log(1 + bm * zeta)
+    lz = math.log((d0 + 0.1) / 0.1)
+    assert us == pytest.approx(KAPPA * U / max(lz - psi, min(lz, 1.0)), rel=1e-12)
+    assert us > bd["ustar"][p]
+
+
+@pytest.mark.gpu
+def test_gpu_qnse_wall_model_matches_oracle(ctx):
+    """QNSE's stable side under a downward heat flux on the GPU: the surface
+    state, the wall law's ghost fill and the residuals equal the oracle's."""
+    from ablsteadyrans_b200.abi import SURFACE_HEAT_FLUX
+    case, bc, ph = _hill_case()
+    bc.surface_stability, bc.surface_heat_flux, bc.surface_qnse = SURFACE_HEAT_FLUX, -0.02, 1
+    dc, st = _stage(ctx, case, bc, ph)
+    try:
+        ss_ref = oracle.fill_ghosts(case, bc, ph)
+        R_ref = oracle.residual(case, bc, ph)
+        st.fill_ghosts()
+        R = [r.cpu().numpy() for r in st.residual()]
+        _, ss = st.turbulence()
+        g = case.grid
+        for f in FIELDS:
+            ref, got = case.q[f], dc.host(f)
+            assert np.abs(got - ref).max() <= 1e-11 * np.abs(ref).max(), f
+        for f in ("ustar", "inv_L", "tau_x", "tau_y", "kwall"):
+            ref, got = _columns(g, ss_ref[f]), _columns(g, ss[f])
+            assert np.abs(got - ref).max() <= 1e-11 * max(np.abs(ref).max(), 1e-300), f
+        for n, loc in enumerate(LOCS):
+            v = g.valid(loc)
+            assert np.abs(R[n][v] - R_ref[n][v]).max() <= 1e-10 * max(np.abs(R_ref[n][v]).max(), 1e-300), n
+    finally:
+        st.close()
