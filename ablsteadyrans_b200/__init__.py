@@ -30,7 +30,8 @@ _lib = None
 GB_OK = 0
 KERNEL_LINE_SWEEP, KERNEL_POISSON_APPLY, KERNEL_MG_SMOOTH, KERNEL_MG_TRANSFER, KERNEL_RESIDUAL, \
     KERNEL_MASSFLUX, KERNEL_COEFS, KERNEL_VECTOR, KERNEL_BC = range(9)
-TUNE_LINE_VARIANT, TUNE_LINE_BLOCK, TUNE_MG_COARSE_KERNEL, TUNE_LINE_DEPTH, TUNE_LINE_BACK, TUNE_MG_FUSED_RELAX = range(6)
+(TUNE_LINE_VARIANT, TUNE_LINE_BLOCK, TUNE_MG_COARSE_KERNEL, TUNE_LINE_DEPTH, TUNE_LINE_BACK, TUNE_MG_FUSED_RELAX,
+ TUNE_LINE_SEGMENT) = range(7)
 STATUS_NAMES = {0: "OK", 1: "BAD_ARG", 2: "NONFINITE", 3: "NOT_CONVERGED", 4: "TIMEOUT", 5: "OOM", 6: "CUDA"}
 
 
@@ -168,6 +169,15 @@ def zline_jacobi(ctx, grid, loc, A, ap, rhs, sweeps, delta):
     return float(out.value)
 
 
+def implicit_coefficients(ctx, grid, loc, F, gamma, z, J, log_mean, A):
+    """gust::implicit_coefficients (Source/ImplicitOperator.H:65-67) at loc:
+    the upwind transport of F (three face tensors) and the principal
+    diffusion of gamma into A (7 x grid, FP64)."""
+    check(_lib_full().gb_implicit_coefficients(ctx.handle, ctypes.byref(grid.c), int(loc), *[_ptr(f) for f in F],
+                                         _ptr(gamma), _ptr(z), _ptr(J), int(bool(log_mean)), _ptr(A)))
+    return A
+
+
 def zline_lusgs(ctx, grid, loc, A, ap, rhs, sweeps, delta, alternate=0):
     """gust::zline_lusgs with line_ghosts = lagged (Source/LineSweeps.H:
     159-161): symmetric line LU-SGS passes into delta (FP64); returns max
@@ -219,6 +229,7 @@ def _declare_poisson(L):
     P = ctypes.c_void_p
     G = ctypes.POINTER(GbGrid)
     L.gb_mesh_metrics.argtypes = [P, G, P, P, P, P, P, P]
+    L.gb_implicit_coefficients.argtypes = [P, G, ctypes.c_int32, P, P, P, P, P, P, ctypes.c_int32, P]
     L.gb_face_divergence.argtypes = [P, G, P, P, P, P, P, P, P, P]
     from .abi import MeshFields, State
     L.gb_restrict_state.argtypes = [P, G, ctypes.POINTER(State), ctypes.POINTER(MeshFields), G, ctypes.POINTER(State),

@@ -203,6 +203,26 @@ class IterInfo(ctypes.Structure):
         return d
 
 
+class PredictorResult(ctypes.Structure):
+    """gb_predictor_result (gust::MomentumPredictorResult)."""
+    _fields_ = [("max_du", ctypes.c_double), ("max_dv", ctypes.c_double), ("max_dw", ctypes.c_double),
+                ("last_sweep_du", ctypes.c_double), ("last_sweep_dv", ctypes.c_double),
+                ("last_sweep_dw", ctypes.c_double)]
+
+
+class PressureResult(ctypes.Structure):
+    """gb_pressure_result (gust::PressureCorrectionResult)."""
+    _fields_ = [("poisson_iterations", ctypes.c_int32), ("poisson_removed_mean", ctypes.c_double),
+                ("divergence_before", ctypes.c_double), ("divergence_after", ctypes.c_double),
+                ("max_dp", ctypes.c_double), ("max_du", ctypes.c_double), ("max_dv", ctypes.c_double),
+                ("max_dw", ctypes.c_double)]
+
+
+class ScalarResult(ctypes.Structure):
+    """gb_scalar_result (gust::ScalarSweepResult)."""
+    _fields_ = [("max_dq", ctypes.c_double), ("last_sweep", ctypes.c_double), ("clipped", ctypes.c_int64)]
+
+
 CRITERION_MAX_RESIDUALS, CRITERION_MAX_MONITORS = 8, 4
 NOT_STEADY, STEADY, DIVERGED = 0, 1, 2
 LOOSE_NONE, LOOSE_RESIDUALS, LOOSE_MONITORS = 0, 1, 2

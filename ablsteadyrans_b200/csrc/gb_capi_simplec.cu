@@ -164,6 +164,20 @@ gb_status check_bc(const gb_grid& g, const gb_bc& bc)
                     return GB_BAD_ARG;
                 }
             }
+        } else {
+            // With Businger-Dyer a QNSE coefficient other than its default would be
+            // ignored, which the reference refuses (SurfaceLayer.cpp:282-288). A zero
+            // reads as "not set", so a zero-initialised gb_bc stays valid.
+            const double qc[4] = {bc.surface_qnse_am, bc.surface_qnse_bm, bc.surface_qnse_ah, bc.surface_qnse_bh};
+            const double qd[4] = {2.5, 0.2, 2.5, 0.2};
+            const char* qn[4] = {"qnse_am", "qnse_bm", "qnse_ah", "qnse_bh"};
+            for (int n = 0; n < 4; ++n) {
+                if (qc[n] != 0.0 && qc[n] != qd[n]) {
+                    gb::set_error("gust: invalid inputs:\n  surface layer %s is set but stable_functions is "
+                                  "businger_dyer; it would be ignored", qn[n]);
+                    return GB_BAD_ARG;
+                }
+            }
         }
         if (bc.surface_denominator_floor != GB_DENOMINATOR_LOG_LAW && bc.surface_denominator_floor != GB_DENOMINATOR_ONE) {
             gb::set_error("gust: invalid inputs:\n  bc.surface_denominator_floor must be log_law or one");
@@ -417,6 +431,77 @@ gb_status gb_simplec_residual(gb_simplec* s, const gb_state* q, double* const* R
     }
     gb::simplec_residual(s, *q, r);
     return gb::check_cuda("residual");
+}
+
+gb_status gb_momentum_predictor(gb_simplec* s, const gb_state* q, double* const* R, const double* dtau,
+                                double* const* ap, double* const* d, gb_predictor_result* res)
+{
+    gb::clear_error();
+    if (s == nullptr || q == nullptr || R == nullptr || dtau == nullptr || res == nullptr) {
+        gb::set_error("gust: momentum_predictor: the stage, the state, R, dtau and the result are needed");
+        return GB_BAD_ARG;
+    }
+    for (int n = 0; n < 6; ++n) {
+        if (R[n] == nullptr) {
+            gb::set_error("gust: momentum_predictor: R needs six device arrays (u, v, w, p, theta, tke)");
+            return GB_BAD_ARG;
+        }
+    }
+    return gb::simplec_predictor_step(s, *q, R, dtau, ap, d, res);
+}
+
+gb_status gb_pressure_correction(gb_simplec* s, const gb_state* q, const double* const* d, gb_pressure_result* res)
+{
+    gb::clear_error();
+    if (s == nullptr || q == nullptr || res == nullptr) {
+        gb::set_error("gust: pressure_correction: the stage, the state and the result are needed");
+        return GB_BAD_ARG;
+    }
+    if (d != nullptr && (d[0] == nullptr || d[1] == nullptr || d[2] == nullptr)) {
+        gb::set_error("gust: pressure_correction: d needs three device arrays (the u, v, w faces) or none");
+        return GB_BAD_ARG;
+    }
+    return gb::simplec_pressure_step(s, *q, d, res);
+}
+
+gb_status gb_scalar_sweep(gb_simplec* s, const gb_state* q, int32_t eq, const double* R_eq, const double* dtau,
+                          int32_t clip, gb_scalar_result* res)
+{
+    gb::clear_error();
+    if (eq != 4 && eq != 5) {
+        gb::set_error("gust: scalar_sweep: eq must be theta or tke");
+        return GB_BAD_ARG;
+    }
+    if (s == nullptr || q == nullptr || R_eq == nullptr || dtau == nullptr || res == nullptr) {
+        gb::set_error("gust: scalar_sweep: the stage, the state, R, dtau and the result are needed");
+        return GB_BAD_ARG;
+    }
+    return gb::simplec_scalar_step(s, *q, eq, R_eq, dtau, clip, res);
+}
+
+gb_status gb_implicit_coefficients(gb_ctx* ctx, const gb_grid* g, int32_t loc, const double* F0, const double* F1,
+                                   const double* F2, const double* gamma, const double* z_nd, const double* detJ,
+                                   int32_t log_mean, double* A)
+{
+    gb::clear_error();
+    const char* op = "implicit_coefficients";
+    if (ctx == nullptr) {
+        gb::set_error("gust: %s: ctx is null", op);
+        return GB_BAD_ARG;
+    }
+    gb_status st = gb::check_grid(op, g);
+    if (st != GB_OK) { return st; }
+    if (loc != GB_LOC_CELL && loc != GB_LOC_XFACE && loc != GB_LOC_YFACE && loc != GB_LOC_ZFACE) {
+        gb::set_error("gust: implicit_coefficients: loc must be the cells or a face");
+        return GB_BAD_ARG;
+    }
+    if (F0 == nullptr || F1 == nullptr || F2 == nullptr || gamma == nullptr || z_nd == nullptr || detJ == nullptr
+        || A == nullptr) {
+        gb::set_error("gust: implicit_coefficients: F, gamma, z_nd, detJ and A must be device arrays of the grid");
+        return GB_BAD_ARG;
+    }
+    double* F[3] = {const_cast<double*>(F0), const_cast<double*>(F1), const_cast<double*>(F2)};
+    return gb::implicit_coefficients_at(ctx, *g, loc, F, gamma, z_nd, detJ, log_mean != 0, A);
 }
 
 gb_status gb_simplec_iterate(gb_simplec* s, const gb_state* q, const double* dtau, gb_iter_info* info)

@@ -405,6 +405,287 @@ __global__ void __launch_bounds__(128) zline_fact_multi_kernel(MultiLineArgs<T> 
     }
 }
 
+//! The segmented sweep: the column's levels split among the warps of a block.
+//! A block holds 32 columns (consecutive i of one j) and ceil(nk / L) warps;
+//! warp w owns levels [w L, w L + L) of every column, loads all of them at
+//! once into registers (every load of a thread is independent, so the memory
+//! latency is paid once per segment, not once per level) and runs the Thomas
+//! recurrences of gust::solve_column (Source/LineSolve_K.H:22-45) over its
+//! own levels. What crosses a segment boundary is one value per recurrence
+//! (c' on the first sweep, e' and x on every sweep): each warp composes its
+//! segment into one map of that value (a 2x2 projective map for c', which
+//! is a continued fraction; an affine map for e' and x), the maps go through
+//! shared memory, and each warp applies the maps of the segments before it
+//! to find its own starting value. Inside a segment the recurrences are the
+//! sequential ones, in the sequential operation order; only the values
+//! carried in across a boundary are evaluated through the composed maps, so
+//! the results agree with the sequential solve to rounding.
+//! FIRST: the first sweep of a solve (zero iterate, no lateral terms): it
+//! also stores the column factors 1/m and c' for the later sweeps, which read
+//! them in place of a_P and a_ZP (as zline_fact_body).
+template <typename T>
+__device__ __forceinline__ void seg_pow2_normalise(T& a, T& b, T& c, T& d)
+{
+    const T s = fmax(fmax(fabs(a), fabs(b)), fmax(fabs(c), fabs(d)));
+    if (s > T(0) && s == s && s < T(INFINITY)) {
+        int e;
+        frexp(s, &e);
+        const T f = ldexp(T(1), -e);  // a power of two: the scaling is exact
+        a *= f;
+        b *= f;
+        c *= f;
+        d *= f;
+    }
+}
+
+template <typename T, bool FIRST, int L>
+__device__ __forceinline__ void zline_seg_body(const LineArgs<T>& a, T* __restrict__ inv_io, T* __restrict__ cp_io)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int lane = threadIdx.x;
+    const int w = threadIdx.y;
+    const int W = blockDim.y;
+    const int i = blockIdx.x * 32 + lane;
+    const int j = blockIdx.y;
+    const bool col = (i < a.ni) && (j < a.nj);
+    const int k0 = w * L;
+    const int nk = a.nk;
+    const gb_grid& g = a.g;
+    T* carry_c = reinterpret_cast<T*>(smem_raw);      // [4][W][32]: the projective map of c'
+    T* carry_e = carry_c + 4 * W * 32;                 // [2][W][32]: the affine map of e'
+    T* carry_x = carry_e + 2 * W * 32;                 // [2][W][32]: the affine map of x
+    const int cs = W * 32;
+    const int me = w * 32 + lane;
+    int64_t o0 = 0, oxm = -1, oxp = -1, oym = -1, oyp = -1;
+    if (col) {
+        const int im = lateral_image(i - 1, a.ni, g.nx, g.periodic_x != 0);
+        const int ip = lateral_image(i + 1, a.ni, g.nx, g.periodic_x != 0);
+        const int jm = lateral_image(j - 1, a.nj, g.ny, g.periodic_y != 0);
+        const int jp = lateral_image(j + 1, a.nj, g.ny, g.periodic_y != 0);
+        o0 = at(g, i, j, 0);
+        oxm = (im >= 0) ? at(g, im, j, 0) : -1;
+        oxp = (ip >= 0) ? at(g, ip, j, 0) : -1;
+        oym = (jm >= 0) ? at(g, i, jm, 0) : -1;
+        oyp = (jp >= 0) ? at(g, i, jp, 0) : -1;
+    }
+    const T* __restrict__ azm = a.A + GB_COEF_ZM * a.cs;
+    const T* __restrict__ azp = a.A + GB_COEF_ZP * a.cs;
+    const T* __restrict__ axm = a.A + GB_COEF_XM * a.cs;
+    const T* __restrict__ axp = a.A + GB_COEF_XP * a.cs;
+    const T* __restrict__ aym = a.A + GB_COEF_YM * a.cs;
+    const T* __restrict__ ayp = a.A + GB_COEF_YP * a.cs;
+    // r: the right-hand side with the lagged lateral terms; lo: a_ZM; dg: a_P
+    // (FIRST) or 1/m; up: a_ZP (FIRST) or c'
+    T r[L], lo[L], dg[L], up[L];
+#pragma unroll
+    for (int q = 0; q < L; ++q) {
+        const int k = k0 + q;
+        r[q] = T(0);
+        lo[q] = T(0);
+        dg[q] = T(1);
+        up[q] = T(0);
+        if (col && k < nk) {
+            const int64_t ko = static_cast<int64_t>(k) * g.sz;
+            const int64_t o = o0 + ko;
+            r[q] = a.rhs[o];
+            lo[q] = azm[o];
+            if (FIRST) {
+                dg[q] = a.ap[o];
+                up[q] = azp[o];
+            } else {
+                dg[q] = inv_io[o];
+                up[q] = cp_io[o];
+                const T dxm = (oxm >= 0) ? a.dold[oxm + ko] : T(0);
+                const T dxp = (oxp >= 0) ? a.dold[oxp + ko] : T(0);
+                const T dym = (oym >= 0) ? a.dold[oym + ko] : T(0);
+                const T dyp = (oyp >= 0) ? a.dold[oyp + ko] : T(0);
+                r[q] = r[q] + axm[o] * dxm + axp[o] * dxp + aym[o] * dym + ayp[o] * dyp;
+            }
+        }
+    }
+    if (FIRST) {
+        // c'_k = -a_ZP,k / (a_P,k + a_ZM,k c'_{k-1}): the segment's map of c' as
+        // the product of [[0, -a_ZP], [a_ZM, a_P]] acting on (numerator, denominator)
+        T p00 = T(1), p01 = T(0), p10 = T(0), p11 = T(1);
+#pragma unroll
+        for (int q = 0; q < L; ++q) {
+            const int k = k0 + q;
+            if (k < nk) {
+                const T l = (k == 0) ? T(0) : lo[q];
+                const T n00 = -up[q] * p10, n01 = -up[q] * p11;
+                const T n10 = l * p00 + dg[q] * p10, n11 = l * p01 + dg[q] * p11;
+                p00 = n00;
+                p01 = n01;
+                p10 = n10;
+                p11 = n11;
+                seg_pow2_normalise(p00, p01, p10, p11);
+            }
+        }
+        carry_c[me] = p00;
+        carry_c[cs + me] = p01;
+        carry_c[2 * cs + me] = p10;
+        carry_c[3 * cs + me] = p11;
+        __syncthreads();
+        // c' at the level below this segment: the maps of the segments below applied to c' = 0
+        T num = T(0), den = T(1);
+        for (int s = 0; s < w; ++s) {
+            const int m = s * 32 + lane;
+            const T n2 = carry_c[m] * num + carry_c[cs + m] * den;
+            const T d2 = carry_c[2 * cs + m] * num + carry_c[3 * cs + m] * den;
+            num = n2;
+            den = d2;
+            T z0 = T(0), z1 = T(0);
+            seg_pow2_normalise(num, den, z0, z1);
+        }
+        T cprev = (w == 0) ? T(0) : num / den;
+        // the sequential factorisation over the segment (zline_fact_body's order)
+#pragma unroll
+        for (int q = 0; q < L; ++q) {
+            const int k = k0 + q;
+            if (k < nk) {
+                const T lower = -lo[q];
+                const T m = (k == 0) ? dg[q] : dg[q] - lower * cprev;
+                const T inv = T(1) / m;
+                const T c = -up[q] * inv;
+                dg[q] = inv;
+                up[q] = c;
+                cprev = c;
+                if (col) {
+                    const int64_t o = o0 + static_cast<int64_t>(k) * g.sz;
+                    inv_io[o] = inv;
+                    cp_io[o] = c;
+                }
+            }
+        }
+    }
+    // forward substitution e_k = (r_k + a_ZM,k e_{k-1}) / m_k: the segment's affine map
+    {
+        T al = T(0), be = T(1);
+#pragma unroll
+        for (int q = 0; q < L; ++q) {
+            const int k = k0 + q;
+            if (k < nk) {
+                if (k == 0) {
+                    al = r[q] * dg[q];
+                    be = T(0);
+                } else {
+                    al = (r[q] + lo[q] * al) * dg[q];
+                    be = (lo[q] * be) * dg[q];
+                }
+            }
+        }
+        carry_e[me] = al;
+        carry_e[cs + me] = be;
+    }
+    __syncthreads();
+    {
+        T eprev = T(0);
+        for (int s = 0; s < w; ++s) {
+            const int m = s * 32 + lane;
+            eprev = carry_e[m] + carry_e[cs + m] * eprev;
+        }
+#pragma unroll
+        for (int q = 0; q < L; ++q) {
+            const int k = k0 + q;
+            if (k < nk) {
+                const T lower = -lo[q];
+                eprev = ((k == 0) ? r[q] : r[q] - lower * eprev) * dg[q];
+                r[q] = eprev;  // e' in place of r
+            }
+        }
+    }
+    // back substitution x_k = e'_k - c'_k x_{k+1} (x_{nk-1} = e'_{nk-1}): the
+    // segment's affine map of x from the level above it
+    {
+        T ga = T(0), de = T(1);
+#pragma unroll
+        for (int q = L - 1; q >= 0; --q) {
+            const int k = k0 + q;
+            if (k < nk) {
+                if (k == nk - 1) {
+                    ga = r[q];
+                    de = T(0);
+                } else {
+                    ga = r[q] - up[q] * ga;
+                    de = -up[q] * de;
+                }
+            }
+        }
+        carry_x[me] = ga;
+        carry_x[cs + me] = de;
+    }
+    __syncthreads();
+    T chg = T(0);
+    {
+        T x = T(0);
+        for (int s = W - 1; s > w; --s) {
+            const int m = s * 32 + lane;
+            x = carry_x[m] + carry_x[cs + m] * x;
+        }
+#pragma unroll
+        for (int q = L - 1; q >= 0; --q) {
+            const int k = k0 + q;
+            if (k < nk) {
+                x = (k == nk - 1) ? r[q] : r[q] - up[q] * x;
+                if (col) {
+                    const int64_t o = o0 + static_cast<int64_t>(k) * g.sz;
+                    a.dnew[o] = x;
+                    if (a.change) {
+                        const T d = fabs(x - (FIRST ? T(0) : a.dold[o]));
+                        chg = (d > chg || d != d) ? d : chg;
+                    }
+                }
+            }
+        }
+    }
+    if (a.change != nullptr) {
+        chg = warp_max(chg);
+        if (lane == 0) { atomic_max_nonneg(a.change, chg); }
+    }
+}
+
+template <typename T, bool FIRST, int L>
+__global__ void __launch_bounds__(512) zline_seg_kernel(LineArgs<T> a, T* __restrict__ inv_io, T* __restrict__ cp_io)
+{
+    zline_seg_body<T, FIRST, L>(a, inv_io, cp_io);
+}
+
+//! The segmented sweep over several systems (MultiLineArgs; blockIdx.z picks
+//! the system, with constant indices into the parameter block).
+template <typename T, bool FIRST, int L>
+__global__ void __launch_bounds__(512) zline_seg_multi_kernel(MultiLineArgs<T> m)
+{
+    switch (blockIdx.z) {
+    case 0: zline_seg_body<T, FIRST, L>(m.a[0], m.inv[0], m.cp[0]); break;
+    case 1: zline_seg_body<T, FIRST, L>(m.a[1], m.inv[1], m.cp[1]); break;
+    default: zline_seg_body<T, FIRST, L>(m.a[2], m.inv[2], m.cp[2]); break;
+    }
+}
+
+//! Shared memory of the segmented sweep's carries: 8 values per thread.
+template <typename T>
+constexpr size_t seg_smem_bytes(int warps)
+{
+    return static_cast<size_t>(8) * warps * 32 * sizeof(T);
+}
+
+//! Levels per segment of the segmented sweep (GB_TUNE_LINE_SEGMENT: 4 or 8,
+//! default 8) and its warps per block for nk levels; 0 when the column is too
+//! tall (more than 16 segments), which the callers then sweep with the
+//! factored kernel.
+constexpr int kSegMaxWarps = 16;
+
+inline int seg_levels(const gb_ctx* ctx)
+{
+    return (ctx->tune[GB_TUNE_LINE_SEGMENT] == 4) ? 4 : 8;
+}
+
+inline int seg_warps(int nk, int L)
+{
+    const int w = (nk + L - 1) / L;
+    return (w >= 1 && w <= kSegMaxWarps) ? w : 0;
+}
+
 //! The two copies of a periodic seam face take the low copy's value.
 template <typename T>
 __global__ void seam_sync_kernel(gb_grid g, int loc, T* __restrict__ f)
@@ -454,12 +735,58 @@ gb_status zline_sweeps(gb_ctx* ctx, const gb_grid& g, int loc, const T* A, const
     T* tmp = static_cast<T*>(scratch(ctx, kSlotLineNext, sizeof(T) * vol));
     if (tmp == nullptr) { return GB_OOM; }
     const size_t smem = line_smem_bytes<T>(nk);
+    const int segL = seg_levels(ctx);
+    const int segW = seg_warps(nk, segL);
     if (scratch_kind == LineScratch::automatic) {
         const int v = ctx->tune[GB_TUNE_LINE_VARIANT];
         scratch_kind = (v == 1)   ? LineScratch::pipelined
                        : (v == 2) ? LineScratch::shared
                        : (v == 3) ? LineScratch::global
-                                  : LineScratch::factored;
+                       : (v == 4) ? LineScratch::factored
+                                  : LineScratch::segmented;
+    }
+    if (scratch_kind == LineScratch::segmented && segW == 0) { scratch_kind = LineScratch::factored; }
+    if (scratch_kind == LineScratch::segmented) {
+        T* inv = static_cast<T*>(scratch(ctx, kSlotLineInv, sizeof(T) * vol));
+        T* cpr = static_cast<T*>(scratch(ctx, kSlotLineCp, sizeof(T) * vol));
+        if (inv == nullptr || cpr == nullptr) { return GB_OOM; }
+        T* buf[2] = {delta, tmp};
+        if (change_word != nullptr) { cudaMemsetAsync(change_word, 0, sizeof(unsigned long long), ctx->stream); }
+        const dim3 block(32, segW);
+        const dim3 grid((ni + 31) / 32, nj);
+        const size_t sm = seg_smem_bytes<T>(segW);
+        for (int s = 0; s < sweeps; ++s) {
+            LineArgs<T> a{};
+            a.g = g;
+            a.ni = ni;
+            a.nj = nj;
+            a.nk = nk;
+            a.A = A;
+            a.cs = vol;
+            a.ap = ap;
+            a.rhs = rhs;
+            a.dold = buf[(sweeps - s) & 1];
+            a.dnew = buf[(sweeps - 1 - s) & 1];
+            a.first = (s == 0) ? 1 : 0;
+            a.change = (s == sweeps - 1) ? change_word : nullptr;
+            Span span(ctx, GB_KERNEL_LINE_SWEEP);
+            if (segL == 4) {
+                if (a.first) {
+                    zline_seg_kernel<T, true, 4><<<grid, block, sm, ctx->stream>>>(a, inv, cpr);
+                } else {
+                    zline_seg_kernel<T, false, 4><<<grid, block, sm, ctx->stream>>>(a, inv, cpr);
+                }
+            } else {
+                if (a.first) {
+                    zline_seg_kernel<T, true, 8><<<grid, block, sm, ctx->stream>>>(a, inv, cpr);
+                } else {
+                    zline_seg_kernel<T, false, 8><<<grid, block, sm, ctx->stream>>>(a, inv, cpr);
+                }
+            }
+            ++ctx->launches;
+        }
+        seam_sync<T>(ctx, g, loc, delta);
+        return check_cuda("zline_jacobi");
     }
     const bool factored = (scratch_kind == LineScratch::factored);
     const bool pipelined = factored || (scratch_kind == LineScratch::pipelined);
@@ -600,6 +927,52 @@ gb_status zline_sweeps_multi(gb_ctx* ctx, const gb_grid& g, int n, const int* lo
             cudaMemsetAsync(change_words[s], 0, sizeof(unsigned long long), ctx->stream);
         }
     }
+    // the segmented sweep (the default; GB_TUNE_LINE_VARIANT 4 selects the factored one below)
+    const int segL = seg_levels(ctx);
+    const int segW = seg_warps(max_nk, segL);
+    if (ctx->tune[GB_TUNE_LINE_VARIANT] != 4 && segW > 0) {
+        const dim3 block(32, segW);
+        const dim3 grid((max_ni + 31) / 32, max_nj, n);
+        const size_t sm = seg_smem_bytes<T>(segW);
+        for (int k = 0; k < sweeps; ++k) {
+            MultiLineArgs<T> m{};
+            for (int s = 0; s < n; ++s) {
+                T* buf[2] = {delta[s], tmp[s]};
+                LineArgs<T>& a = m.a[s];
+                a.g = g;
+                a.ni = ni[s];
+                a.nj = nj[s];
+                a.nk = nk[s];
+                a.A = A[s];
+                a.cs = vol;
+                a.ap = ap[s];
+                a.rhs = rhs[s];
+                a.dold = buf[(sweeps - k) & 1];
+                a.dnew = buf[(sweeps - 1 - k) & 1];
+                a.first = (k == 0) ? 1 : 0;
+                a.change = (k == sweeps - 1 && change_words != nullptr) ? change_words[s] : nullptr;
+                m.inv[s] = inv[s];
+                m.cp[s] = cpr[s];
+            }
+            Span span(ctx, GB_KERNEL_LINE_SWEEP);
+            if (segL == 4) {
+                if (k == 0) {
+                    zline_seg_multi_kernel<T, true, 4><<<grid, block, sm, ctx->stream>>>(m);
+                } else {
+                    zline_seg_multi_kernel<T, false, 4><<<grid, block, sm, ctx->stream>>>(m);
+                }
+            } else {
+                if (k == 0) {
+                    zline_seg_multi_kernel<T, true, 8><<<grid, block, sm, ctx->stream>>>(m);
+                } else {
+                    zline_seg_multi_kernel<T, false, 8><<<grid, block, sm, ctx->stream>>>(m);
+                }
+            }
+            ++ctx->launches;
+        }
+        for (int s = 0; s < n; ++s) { seam_sync<T>(ctx, g, locs[s], delta[s]); }
+        return check_cuda("zline_sweeps_multi");
+    }
     static std::atomic<bool> attr_done[2];  // set once per process (one device per process)
     const int ti = sizeof(T) == 8 ? 1 : 0;
     if (!attr_done[ti].load()) {
@@ -732,9 +1105,10 @@ gb_status gb_zline_jacobi_f32(gb_ctx* ctx, const gb_grid* g, int32_t loc, const 
 
 // ---- The allocation-free z-line solve ------------------------------------
 //
-// gb_zline_jacobi_noalloc runs the same FP64 sweeps as gb_zline_jacobi (the
-// pipelined kernel with one-warp blocks, which is what a context with default
-// tuning runs) for a caller that may not allocate device memory at all: no
+// gb_zline_jacobi_noalloc runs the same FP64 column solves as gb_zline_jacobi
+// (the pipelined kernel with one-warp blocks; the context path also keeps the
+// column factors between sweeps, so the two agree to rounding) for a caller
+// that may not allocate device memory at all: no
 // gb_ctx (creating one allocates), no cudaMalloc or cudaFree behind its back.
 // Its only scratch, the ping-pong iterate and the change word, live in the
 // fixed array below, which the CUDA runtime reserves on each device when it
@@ -758,7 +1132,9 @@ std::mutex g_noalloc_mutex;
 double* g_noalloc_addr[kNoAllocMaxDevices] = {};
 
 //! Per-device set-up, once, with that device current: the array's device
-//! address and the shared-memory limit of the two sweep kernels.
+//! address and the shared-memory limit of the two sweep kernels. The address
+//! is kept for the life of the process, so a cudaDeviceReset of the device
+//! after its first call is not supported (the address would be stale).
 gb_status noalloc_setup(int dev, double** out)
 {
     std::lock_guard<std::mutex> lock(g_noalloc_mutex);

@@ -17,7 +17,7 @@ enum ScratchSlot : int {
     kSlotMultiBase = 24  // 3 slots (next, 1/m, c') per system of zline_sweeps_multi
 };
 
-enum class LineScratch { automatic, pipelined, shared, global, factored };
+enum class LineScratch { automatic, pipelined, shared, global, factored, segmented };
 
 //! `sweeps` z-line Jacobi sweeps into delta (which must hold 0 on entry,
 //! ghosts included). change_word (device, may be null) receives the bit

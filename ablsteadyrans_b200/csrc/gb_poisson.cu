@@ -585,6 +585,130 @@ __global__ void __launch_bounds__(256) k_color_relax_fused(gb_grid g, PBC b, int
     }
 }
 
+//! One colour's relaxation in ONE launch with every level of a column in
+//! flight: a block holds 32 columns of the colour along one row and
+//! ceil(nz / L) warps; warp w owns levels [w L, w L + L) of every column. Each
+//! thread evaluates r = b - A x at its levels (adotx_cell, as
+//! k_color_residual) and loads the columns' line factors (D, 1/m, c') and x;
+//! then the factored Thomas solve of k_color_solve_staged runs over the
+//! segment with its sequential recurrences, and what crosses a segment
+//! boundary (e' upwards, the correction downwards) goes through shared memory
+//! as each segment's affine map, applied by the segments above (below) it. The
+//! results agree with the two-launch form to rounding (the values carried
+//! across a boundary are evaluated through the composed maps). All reads of x
+//! precede the block's first barrier and all writes follow its last; the
+//! lateral neighbours of a column are of the other colour and only this block
+//! writes its columns, so every read sees the values from before the
+//! colour's update (a periodic direction of odd extent pairs a column with a
+//! same-colour image: the caller then uses the two-launch form).
+template <typename T, int L>
+__global__ void __launch_bounds__(512) k_color_relax_seg(gb_grid g, PBC b, int color, T* x, const T* __restrict__ bv,
+                                                         const T* __restrict__ AX, const T* __restrict__ AY,
+                                                         const T* __restrict__ AZ, const T* __restrict__ J,
+                                                         MeshRatios<T> m, const T* __restrict__ TD,
+                                                         const T* __restrict__ TC, const T* __restrict__ TU)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int lane = threadIdx.x;
+    const int w = threadIdx.y;
+    const int W = blockDim.y;
+    const int j = blockIdx.y;
+    const int i = 2 * (blockIdx.x * 32 + lane) + ((j + color) & 1);
+    const bool col = i < g.nx;
+    const int nz = g.nz;
+    const int k0 = w * L;
+    const int cs = W * 32;
+    const int me = w * 32 + lane;
+    T* carry_e = reinterpret_cast<T*>(smem_raw);  // [2][W][32]
+    T* carry_x = carry_e + 2 * cs;                // [2][W][32]
+    T r[L], D[L], im[L], cp[L], x0[L];
+#pragma unroll
+    for (int q = 0; q < L; ++q) {
+        const int k = k0 + q;
+        r[q] = T(0);
+        D[q] = T(0);
+        im[q] = T(0);
+        cp[q] = T(0);
+        x0[q] = T(0);
+        if (col && k < nz) {
+            const int64_t o = at(g, i, j, k);
+            r[q] = bv[o] - adotx_cell<T>(g, b, i, j, k, x, AX, AY, AZ, J, m);
+            D[q] = TD[o];
+            im[q] = TC[o];
+            cp[q] = TU[o];
+            x0[q] = x[o];
+        }
+    }
+    // forward: e_k = (r_k - D_k e_{k-1}) / m_k, the segment's affine map of e'
+    {
+        T al = T(0), be = T(1);
+#pragma unroll
+        for (int q = 0; q < L; ++q) {
+            const int k = k0 + q;
+            if (k < nz) {
+                if (k == 0) {
+                    al = r[q] * im[q];
+                    be = T(0);
+                } else {
+                    al = (r[q] - D[q] * al) * im[q];
+                    be = (-D[q] * be) * im[q];
+                }
+            }
+        }
+        carry_e[me] = al;
+        carry_e[cs + me] = be;
+    }
+    __syncthreads();
+    {
+        T ep = T(0);
+        for (int s = 0; s < w; ++s) {
+            const int n = s * 32 + lane;
+            ep = carry_e[n] + carry_e[cs + n] * ep;
+        }
+#pragma unroll
+        for (int q = 0; q < L; ++q) {
+            const int k = k0 + q;
+            if (k < nz) {
+                ep = (k == 0) ? r[q] * im[q] : (r[q] - D[q] * ep) * im[q];
+                r[q] = ep;
+            }
+        }
+    }
+    // back: x_k = e_k - c'_k x_{k+1} (x_{nz-1} = e_{nz-1}), the segment's affine map
+    {
+        T ga = T(0), de = T(1);
+#pragma unroll
+        for (int q = L - 1; q >= 0; --q) {
+            const int k = k0 + q;
+            if (k < nz) {
+                if (k == nz - 1) {
+                    ga = r[q];
+                    de = T(0);
+                } else {
+                    ga = r[q] - cp[q] * ga;
+                    de = -cp[q] * de;
+                }
+            }
+        }
+        carry_x[me] = ga;
+        carry_x[cs + me] = de;
+    }
+    __syncthreads();
+    T xk = T(0);
+    for (int s = W - 1; s > w; --s) {
+        const int n = s * 32 + lane;
+        xk = carry_x[n] + carry_x[cs + n] * xk;
+    }
+#pragma unroll
+    for (int q = L - 1; q >= 0; --q) {
+        const int k = k0 + q;
+        if (k < nz) {
+            xk = (k == nz - 1) ? r[q] : r[q] - cp[q] * xk;
+            if (col) { x[at(g, i, j, k)] = x0[q] + xk; }
+        }
+    }
+}
+
 //! Coarse right-hand side at coarse cell (I, J2, k): the J-weighted sum of
 //! the four fine residuals over 4 J_c (a coarse cell's flux balance is the sum
 //! of its fine cells').
@@ -904,6 +1028,33 @@ void mg_smooth(gb_poisson* P, PoissonLevels<T>& L, int l)
     constexpr int kFusedMaxColumns = 1024;
     const size_t smem_fused = static_cast<size_t>(5) * g.nz * kFusedCols * sizeof(T);
     const int fknob = ctx->tune[GB_TUNE_MG_FUSED_RELAX];
+    // the segmented one-launch relaxation (GB_TUNE_MG_FUSED_RELAX 0 or 4, the
+    // default): every level of a column in flight, at most 16 segments of 4
+    // levels (8 for taller columns, or as GB_TUNE_LINE_SEGMENT asks)
+    const int sknob = ctx->tune[GB_TUNE_LINE_SEGMENT];
+    const int segL = (sknob == 4 || sknob == 8) ? sknob : ((g.nz + 3) / 4 <= 16 ? 4 : 8);
+    const int segW = (g.nz + segL - 1) / segL;
+    const bool seg = (fknob == 0 || fknob == 4) && segW <= 16 && !(g.periodic_x && (g.nx & 1))
+                     && !(g.periodic_y && (g.ny & 1));
+    if (seg) {
+        const dim3 block(32, segW);
+        const dim3 grid((half + 31) / 32, g.ny);
+        const size_t sm = static_cast<size_t>(4) * segW * 32 * sizeof(T);
+        for (int color = 0; color < 2; ++color) {
+            Span span(ctx, GB_KERNEL_MG_SMOOTH);
+            if (segL == 4) {
+                k_color_relax_seg<T, 4><<<grid, block, sm, ctx->stream>>>(g, b, color, L.x[l], L.bv[l], L.AX[l], L.AY[l],
+                                                                         L.AZ[l], L.J[l], L.ratios(l), L.TD[l],
+                                                                         L.TC[l], L.TU[l]);
+            } else {
+                k_color_relax_seg<T, 8><<<grid, block, sm, ctx->stream>>>(g, b, color, L.x[l], L.bv[l], L.AX[l], L.AY[l],
+                                                                         L.AZ[l], L.J[l], L.ratios(l), L.TD[l],
+                                                                         L.TC[l], L.TU[l]);
+            }
+            ++ctx->launches;
+        }
+        return;
+    }
     const bool fused = (fknob == 2 || (fknob == 3 && g.nx * g.ny <= kFusedMaxColumns)) && smem_fused <= kSmoothSmemMax
                        && !(g.periodic_x && (g.nx & 1)) && !(g.periodic_y && (g.ny & 1));
     if (fused) {

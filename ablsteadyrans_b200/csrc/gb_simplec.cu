@@ -1155,21 +1155,19 @@ __device__ __forceinline__ double face_weight(int side, int i, int j, int k, con
     return (dif + inflow) * dxinv[D];
 }
 
-//! ImplicitOperator.cpp:39-74 coefficients<C> (C = -1: a cell scalar).
+//! ImplicitOperator.cpp:39-74 coefficients<C> (C = -1: a cell scalar) on
+//! the grid g with node heights z and detJ J.
 template <int C>
-void implicit_coefficients(gb_simplec* S, double* const* F, const double* gm, double* A)
+void implicit_coefficients_on(gb_ctx* ctx, const gb_grid g, const double* z, const double* J, int logz,
+                              double* const* F, const double* gm, double* A)
 {
-    const gb_grid g = S->g;
-    const double* z = S->z;
-    const double* J = S->mesh.detJ;
-    const int logz = S->ph.log_mean;
     constexpr int T = (C < 0) ? CC : (1 << C);
     constexpr int lx = flux_lo(T, 0), ly = flux_lo(T, 1), lz = flux_lo(T, 2);
     const int64_t cs = volume(g);
     const double* F0 = F[0];
     const double* F1 = F[1];
     const double* F2 = F[2];
-    for_box(S->ctx, valid_box(g, T), [=] __device__(int i, int j, int k) {
+    for_box(ctx, valid_box(g, T), [=] __device__(int i, int j, int k) {
         const double Jinv = 1.0 / interp<CC, T>(J, g, i, j, k);
         const double xm = face_weight<T, C, 0>(0, i + lx, j, k, F0, gm, z, g, logz) * Jinv;
         const double xp = face_weight<T, C, 0>(1, i + lx + 1, j, k, F0, gm, z, g, logz) * Jinv;
@@ -1186,6 +1184,12 @@ void implicit_coefficients(gb_simplec* S, double* const* F, const double* gm, do
         A[GB_COEF_ZP * cs + o] = zp;
         A[GB_COEF_P * cs + o] = ((xm + xp) + (ym + yp)) + (zm + zp);
     }, GB_KERNEL_COEFS);
+}
+
+template <int C>
+void implicit_coefficients(gb_simplec* S, double* const* F, const double* gm, double* A)
+{
+    implicit_coefficients_on<C>(S->ctx, S->g, S->z, S->mesh.detJ, S->ph.log_mean, F, gm, A);
 }
 
 //! apply_to_implicit (BoundaryConditions.cpp:885-941): the damping first,
@@ -1816,6 +1820,139 @@ gb_status simplec_iterate(gb_simplec* S, const gb_state& q, const double* dtau, 
 //! stage_norms (Simplec.cpp:385-409) at q with no iteration: the ghost fill
 //! (the wall state), the residual, the six scaled RMS norms and the monitors
 //! (max speed, mean k, mean u* with the surface layer).
+// ------------------------------------------- the stage's steps alone ---
+//
+// The predictor, the pressure correction and the scalar sweep as the
+// reference's callers outside SimplecStage::iterate use them
+// (NewtonPreconditioner, Transfer's prolong_state): each is the same code
+// the iteration runs, on the stage's workspace, with its result words read
+// back at the end.
+
+gb_status simplec_predictor_step(gb_simplec* S, const gb_state& q, double* const* R, const double* dtau,
+                                 double* const* ap_out, double* const* d_out, gb_predictor_result* res)
+{
+    gb_ctx* ctx = S->ctx;
+    const gb_grid g = S->g;
+    SimplecWork& w = S->w;
+    *res = gb_predictor_result{};
+    cudaMemsetAsync(dword(ctx, 0), 0, sizeof(unsigned long long) * W_COUNT, ctx->stream);
+    transport_fluxes(S, q, w.F[0], w.F[1], w.F[2]);
+    face_dtau(S, dtau, w.dtf);
+    double* Rl[6];
+    for (int n = 0; n < 6; ++n) { Rl[n] = R[n]; }
+    gb_status st = momentum_predictor(S, q, Rl);
+    if (st != GB_OK) { return st; }
+    for (int c = 0; c < 3; ++c) {
+        if (ap_out != nullptr && ap_out[c] != nullptr) {
+            cudaMemcpyAsync(ap_out[c], w.ap[c], sizeof(double) * volume(g), cudaMemcpyDeviceToDevice, ctx->stream);
+        }
+        if (d_out != nullptr && d_out[c] != nullptr) {
+            cudaMemcpyAsync(d_out[c], w.dd[c], sizeof(double) * volume(g), cudaMemcpyDeviceToDevice, ctx->stream);
+        }
+    }
+    unsigned long long words[W_COUNT];
+    if ((st = read_words(ctx, 0, W_COUNT, words)) != GB_OK) { return st; }
+    res->max_du = bits_to_double(words[W_MAX_DU]);
+    res->max_dv = bits_to_double(words[W_MAX_DV]);
+    res->max_dw = bits_to_double(words[W_MAX_DW]);
+    res->last_sweep_du = bits_to_double(words[W_LAST_U]);
+    res->last_sweep_dv = bits_to_double(words[W_LAST_V]);
+    res->last_sweep_dw = bits_to_double(words[W_LAST_W]);
+    return check_cuda("momentum_predictor");
+}
+
+gb_status simplec_pressure_step(gb_simplec* S, const gb_state& q, const double* const* d, gb_pressure_result* res)
+{
+    gb_ctx* ctx = S->ctx;
+    const gb_grid g = S->g;
+    SimplecWork& w = S->w;
+    *res = gb_pressure_result{};
+    if (d != nullptr) {
+        for (int c = 0; c < 3; ++c) {
+            cudaMemcpyAsync(w.dd[c], d[c], sizeof(double) * volume(g), cudaMemcpyDeviceToDevice, ctx->stream);
+        }
+    }
+    cudaMemsetAsync(dword(ctx, 0), 0, sizeof(unsigned long long) * W_COUNT, ctx->stream);
+    // the ghosts of u* refilled first (Simplec.cpp:486), without the wall
+    // state the iteration's first fill keeps for the scalar sweeps
+    fill_ghosts_into(S, q, S->sst);
+    gb_iter_info info{};
+    gb_status st = pressure_correction(S, q, &info);
+    if (st != GB_OK) { return st; }
+    unsigned long long words[W_COUNT];
+    if ((st = read_words(ctx, 0, W_COUNT, words)) != GB_OK) { return st; }
+    res->poisson_iterations = info.poisson_iterations;
+    res->poisson_removed_mean = info.poisson_removed_mean;
+    res->divergence_before = bits_to_double(words[W_DIV_BEFORE]);
+    res->divergence_after = bits_to_double(words[W_DIV_AFTER]);
+    res->max_dp = S->opt.alpha_p * bits_to_double(words[W_MAX_PHI]);
+    res->max_du = bits_to_double(words[W_MAX_FU]);
+    res->max_dv = bits_to_double(words[W_MAX_FV]);
+    res->max_dw = bits_to_double(words[W_MAX_FW]);
+    return check_cuda("pressure_correction");
+}
+
+gb_status simplec_scalar_step(gb_simplec* S, const gb_state& q, int eq, const double* R_eq, const double* dtau,
+                              int clip, gb_scalar_result* res)
+{
+    gb_ctx* ctx = S->ctx;
+    const gb_grid g = S->g;
+    SimplecWork& w = S->w;
+    const int64_t cs = volume(g);
+    *res = gb_scalar_result{};
+    cudaMemsetAsync(dword(ctx, 0), 0, sizeof(unsigned long long) * W_COUNT, ctx->stream);
+    // the ghosts and the transport fluxes of the current (corrected) state, as
+    // the iteration refills them before the sweeps (Simplec.cpp:494-495)
+    fill_ghosts_into(S, q, S->sst);
+    transport_fluxes(S, q, w.F[0], w.F[1], w.F[2]);
+    simplec_implicit_rows(S, eq, w.F, w.Am[0]);
+    double* rhs = w.rhsm[0];
+    double* ap = w.ap[0];
+    const double* A = w.Am[0];
+    for_box(ctx, valid_box(g, CC), [=] __device__(int i, int j, int k) {
+        const int64_t o = at(g, i, j, k);
+        rhs[o] = -R_eq[o];
+        ap[o] = 1.0 / dtau[o] + A[GB_COEF_P * cs + o];
+    }, GB_KERNEL_COEFS);
+    const int word = (eq == F_THETA) ? W_LAST_TH : W_LAST_K;
+    gb_status st = line_solve(S, CC, w.Am[0], w.ap[0], w.rhsm[0], w.deltam[0], word);
+    if (st != GB_OK) { return st; }
+    const int wmax = (eq == F_THETA) ? W_MAX_DTH : W_MAX_DK;
+    dmax(S, valid_box(g, CC), w.deltam[0], nullptr, wmax);
+    unsigned long long* count = dword(ctx, W_CLIPPED);
+    const double* delta = w.deltam[0];
+    double* field = (eq == F_THETA) ? q.theta : q.tke;
+    const bool do_clip = (eq == F_TKE) && clip;
+    const double floor = S->opt.tke_floor;
+    for_box(ctx, valid_box(g, CC), [=] __device__(int i, int j, int k) {
+        const int64_t o = at(g, i, j, k);
+        double v = field[o] + delta[o];
+        if (do_clip && v < floor) {
+            v = floor;
+            atomicAdd(count, 1ull);
+        }
+        field[o] = v;
+    });
+    unsigned long long words[W_COUNT];
+    if ((st = read_words(ctx, 0, W_COUNT, words)) != GB_OK) { return st; }
+    res->max_dq = bits_to_double(words[wmax]);
+    res->last_sweep = bits_to_double(words[word]);
+    res->clipped = static_cast<int64_t>(words[W_CLIPPED]);
+    return check_cuda("scalar_sweep");
+}
+
+gb_status implicit_coefficients_at(gb_ctx* ctx, const gb_grid& g, int loc, double* const* F, const double* gamma,
+                                   const double* z, const double* J, int logz, double* A)
+{
+    switch (loc) {
+    case CC: implicit_coefficients_on<-1>(ctx, g, z, J, logz, F, gamma, A); break;
+    case XF: implicit_coefficients_on<0>(ctx, g, z, J, logz, F, gamma, A); break;
+    case YF: implicit_coefficients_on<1>(ctx, g, z, J, logz, F, gamma, A); break;
+    default: implicit_coefficients_on<2>(ctx, g, z, J, logz, F, gamma, A); break;
+    }
+    return check_cuda("implicit_coefficients");
+}
+
 gb_status simplec_norms(gb_simplec* S, const gb_state& q, double* res, double* mon)
 {
     gb_ctx* ctx = S->ctx;
@@ -1966,6 +2103,9 @@ gb_status simplec_initialize(gb_simplec* S, const gb_state& q, const gb_init_opt
     const int64_t vol = volume(g);
     SimplecWork& w = S->w;
     *r = gb_init_result{};
+    // A new initial state starts without a nu_t history: in the reference each
+    // level's closure is new when its state is initialized (Closure::has_history).
+    S->has_hist = false;
     // 1. u, v at every point; w = 0 but the ground faces, which carry no flux
     fill_from_profile(S, XF, F_U, o.z_agl_min, 0.0, q.u);
     fill_from_profile(S, YF, F_V, o.z_agl_min, 0.0, q.v);
@@ -2230,6 +2370,8 @@ gb_status simplec_prolong(gb_simplec* S, const gb_state& q, const gb_grid& gc, c
     const gb_grid g = S->g;
     SimplecWork& w = S->w;
     const int r = g.nx / gc.nx;
+    // the prolonged state is a new level's: no nu_t history (a fresh Closure)
+    S->has_hist = false;
     // prolong_fields (Transfer.cpp:290-320)
     interpolate(ctx, g, gc, CC, qc.theta, q.theta, r);
     interpolate(ctx, g, gc, CC, qc.tke, q.tke, r);

@@ -15,6 +15,13 @@ void simplec_implicit_rows(gb_simplec* S, int eq, double* const* F, double* A);
 void simplec_implicit_rows_at(gb_simplec* S, const gb_state& q, int eq, double* A);
 gb_status simplec_iterate(gb_simplec* S, const gb_state& q, const double* dtau, gb_iter_info* info);
 gb_status simplec_norms(gb_simplec* S, const gb_state& q, double* res, double* mon);
+gb_status simplec_predictor_step(gb_simplec* S, const gb_state& q, double* const* R, const double* dtau,
+                                 double* const* ap_out, double* const* d_out, gb_predictor_result* res);
+gb_status simplec_pressure_step(gb_simplec* S, const gb_state& q, const double* const* d, gb_pressure_result* res);
+gb_status simplec_scalar_step(gb_simplec* S, const gb_state& q, int eq, const double* R_eq, const double* dtau,
+                              int clip, gb_scalar_result* res);
+gb_status implicit_coefficients_at(gb_ctx* ctx, const gb_grid& g, int loc, double* const* F, const double* gamma,
+                                   const double* z, const double* J, int logz, double* A);
 gb_status simplec_confidence(gb_simplec* S, const double* thresholds, double* share, double* height);
 gb_status simplec_local_dtau(gb_simplec* S, const gb_state& q, double cfl, double* dtau);
 gb_status simplec_initialize(gb_simplec* S, const gb_state& q, const gb_init_opts& o, gb_init_result* r);

@@ -369,13 +369,32 @@ class SwitchOptions:
         self.switch_residual, self.switch_window, self.fallback_failures = switch_residual, switch_window, fallback_failures
 
 
+def newton_equations_differ(stage):
+    """NewtonStage::differs (NewtonStage.cpp:196-205) for what this build
+    has: with the closure and turb.nut_relax < 1 the residual blends nu_t with
+    the history of the last SIMPLEC iteration, which the Newton stage does not
+    update, so the stage's equations are not the steady ones. (The smooth
+    limiter and the frozen k-floor switches, the reference's other two
+    reasons, are not built: the Newton stage runs the run's own limiter and
+    live decisions.) The stage always has a history here: SIMPLEC iterated
+    for the switch window before the Newton stage began."""
+    ph = stage.physics
+    return bool(ph.closure) and ph.turb_nut_relax < 1.0
+
+
 def solve_simplec_newton(stage, max_iterations, driver_options=None, switch=None, newton_options=None,
-                         continuation_options=None):
+                         continuation_options=None, events=None):
     """steady.stage = simplec_newton on one stage: the native SIMPLEC driver
     until the switch rule holds, then one continuation step per iteration
     (started afresh at cfl_max, as the reference's Newton stage starts its
     continuation), the run's norms and monitors at each new state into the
-    driver's criterion, back to SIMPLEC after the failures. Returns
+    driver's criterion, back to SIMPLEC after the failures. As the reference's
+    NewtonStage::iterate (NewtonStage.cpp:127-178), the stage hands the run
+    back to SIMPLEC for good (no later switch, so the run ends on SIMPLEC)
+    when it has converged on equations that differ from the run's
+    (newton_equations_differ), or when it has converged but the criterion
+    has not held for steady.monitor_window further iterations. `events`, a
+    list, receives (iteration, from, to, reason) per switch. Returns
     (verdict, iterations, newton_iterations)."""
     from .simplec import NativeDriver
     d = NativeDriver(stage, driver_options)
@@ -385,8 +404,16 @@ def solve_simplec_newton(stage, max_iterations, driver_options=None, switch=None
     copt = continuation_options or ContinuationOptions(cfl0=o.cfl_max, cfl_max=o.cfl_max,
                                                        ser_exponent=o.ser_exponent, ser_max_growth=o.ser_max_growth)
     mode, below, failures, newton_its = "simplec", 0, 0, 0
+    handed_back, idle = False, 0
     cont = None
     n_mon = 3 if stage.bc.face[2] == abi.FACE_SURFACE_LAYER else 2
+    drop = 10.0 ** (-o.residual_drop_orders)
+
+    def switch_to(it, to, reason):
+        if events is not None:
+            events.append((it + 1, mode, to, reason))
+        return to
+
     try:
         for it in range(max_iterations):
             if mode == "simplec":
@@ -395,8 +422,8 @@ def solve_simplec_newton(stage, max_iterations, driver_options=None, switch=None
                     return verdict, it + 1, newton_its
                 _, _, r = d.status()
                 below = below + 1 if r <= sw.switch_residual else 0
-                if below >= sw.switch_window:
-                    mode, failures = "newton", 0
+                if below >= sw.switch_window and not handed_back:
+                    mode, failures, idle = switch_to(it, "newton", "switch_residual held"), 0, 0
                     if cont is not None:
                         cont.close()
                     cont = Continuation(stage, copt, newton_options)
@@ -404,9 +431,16 @@ def solve_simplec_newton(stage, max_iterations, driver_options=None, switch=None
             # once the continuation has converged on the run's equations
             # (|R| <= 10^-residual_drop_orders |R_0|) no step is taken: the
             # norms fill the criterion's monitor window (NewtonStage.H)
-            done = cont.st.steps > 0 and cont.st.r_last <= 10.0 ** (-o.residual_drop_orders) * cont.st.r0
-            status = "accepted" if done else cont.step()
-            newton_its += 0 if done else 1
+            done = cont.st.steps > 0 and cont.st.r0 > 0 and cont.st.r_last <= drop * cont.st.r0
+            hand_back = None
+            if done:
+                idle += 1
+                status = "accepted"
+                if idle > o.monitor_window:
+                    hand_back = "Newton converged but the steady criterion did not hold for steady.monitor_window iterations"
+            else:
+                status = cont.step()
+                newton_its += 1
             failures = failures + 1 if status == "failed" else 0
             res, mon = stage.norms()
             crit.add(res, mon[:n_mon])
@@ -415,8 +449,16 @@ def solve_simplec_newton(stage, max_iterations, driver_options=None, switch=None
                 return "diverged", it + 1, newton_its
             if v.status == abi.STEADY:
                 return "steady", it + 1, newton_its
-            if failures >= sw.fallback_failures:
-                mode, below = "simplec", 0
+            converged_now = (not done and status == "accepted" and cont.st.steps > 0 and cont.st.r0 > 0
+                             and cont.st.r_last <= drop * cont.st.r0)
+            if hand_back is None and converged_now and newton_equations_differ(stage):
+                hand_back = ("Newton converged on its own equations, which differ from the run's (turb.nut_relax < 1): "
+                             "the final SIMPLEC pass")
+            if hand_back is not None:
+                handed_back = True
+                mode, below = switch_to(it, "simplec", hand_back), 0
+            elif failures >= sw.fallback_failures:
+                mode, below = switch_to(it, "simplec", f"{failures} consecutive failed Newton steps"), 0
         return "running", max_iterations, newton_its
     finally:
         if cont is not None:

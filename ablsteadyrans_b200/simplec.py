@@ -41,6 +41,12 @@ def _declare(L):
                                    ctypes.POINTER(ctypes.c_double)]
     L.gb_simplec_prolong.argtypes = [P, ctypes.POINTER(abi.State), G, ctypes.POINTER(abi.State), ctypes.c_double,
                                      ctypes.POINTER(abi.ProlongResult)]
+    L.gb_momentum_predictor.argtypes = [P, ctypes.POINTER(abi.State), ctypes.POINTER(P), P, ctypes.POINTER(P),
+                                        ctypes.POINTER(P), ctypes.POINTER(abi.PredictorResult)]
+    L.gb_pressure_correction.argtypes = [P, ctypes.POINTER(abi.State), ctypes.POINTER(P),
+                                         ctypes.POINTER(abi.PressureResult)]
+    L.gb_scalar_sweep.argtypes = [P, ctypes.POINTER(abi.State), ctypes.c_int32, P, P, ctypes.c_int32,
+                                  ctypes.POINTER(abi.ScalarResult)]
 
 
 # The closure's fields and the surface state's planes, in the ABI's order.
@@ -190,6 +196,48 @@ class SimplecStage:
         st = self.case.state()
         check(self._L.gb_simplec_iterate(self._h, ctypes.byref(st), ctypes.c_void_p(dtau.data_ptr()), ctypes.byref(info)))
         return info
+
+    def momentum_predictor(self, R, dtau, with_fields=False):
+        """gust::momentum_predictor (Predictor.H:242-252) on the stage's state
+        with R the residual at it (gb_simplec_residual's, after
+        fill_ghosts): returns the PredictorResult, and with with_fields also
+        (ap, d) as three device tensors each."""
+        import torch
+        from . import check
+        res = abi.PredictorResult()
+        st = self.case.state()
+        Ra = (ctypes.c_void_p * 6)(*[r.data_ptr() for r in R])
+        ap = d = None
+        apa = da = None
+        if with_fields:
+            ap = [torch.zeros(self.case.grid.shape, dtype=torch.float64, device="cuda") for _ in range(3)]
+            d = [torch.zeros(self.case.grid.shape, dtype=torch.float64, device="cuda") for _ in range(3)]
+            apa = (ctypes.c_void_p * 3)(*[t.data_ptr() for t in ap])
+            da = (ctypes.c_void_p * 3)(*[t.data_ptr() for t in d])
+        check(self._L.gb_momentum_predictor(self._h, ctypes.byref(st), Ra, ctypes.c_void_p(dtau.data_ptr()), apa, da,
+                                            ctypes.byref(res)))
+        return (res, ap, d) if with_fields else res
+
+    def pressure_correction(self, d=None):
+        """gust::pressure_correction (Simplec.H:139-141) on the stage's state
+        with the denominators d (three device tensors; None: the last
+        predictor's). Returns the PressureResult."""
+        from . import check
+        res = abi.PressureResult()
+        st = self.case.state()
+        da = None if d is None else (ctypes.c_void_p * 3)(*[t.data_ptr() for t in d])
+        check(self._L.gb_pressure_correction(self._h, ctypes.byref(st), da, ctypes.byref(res)))
+        return res
+
+    def scalar_sweep(self, eq, R_eq, dtau, clip=True):
+        """gust::scalar_sweep (Simplec.H:156-163) of eq (4 theta, 5 k) on the
+        stage's state. Returns the ScalarResult."""
+        from . import check
+        res = abi.ScalarResult()
+        st = self.case.state()
+        check(self._L.gb_scalar_sweep(self._h, ctypes.byref(st), int(eq), ctypes.c_void_p(R_eq.data_ptr()),
+                                      ctypes.c_void_p(dtau.data_ptr()), int(bool(clip)), ctypes.byref(res)))
+        return res
 
     def initialize(self, options=None):
         """gust::initialize_state with init.first_guess = profile: the

@@ -245,6 +245,25 @@ def lognormal_z0(grid, seed, median, sigma):
     return plane.reshape(-1)
 
 
+def config0(nx=32, ny=32, nz=48, precision=0, zline_sweeps=4, turbulence=True):
+    """Plain FP64 over flat ground, the neutral ABL of the oracle case:
+    32 x 32 x 48 cells, dx = dy = 40 m, the stretched layers to a 1500 m lid
+    (ratio 1.0927); log-law inflow u* = 0.4 m/s, z0 = 0.1 m from the west
+    (270 deg), outflow east, periodic in y; the k-L closure and a neutral
+    Monin-Obukhov surface layer (turbulence); no Coriolis."""
+    dx = 40.0
+    zl, _ = geometric_zlevels(nz)
+    g = Grid(nx, ny, nz, dx, dx, 1500.0 / nz, False, True)
+    ground = np.zeros((ny + 3, nx + 3))
+    ustar, z0, direction = 0.4, 0.1, 270.0 - 270.0
+    ground_face, surface, turb = _turbulence(turbulence, z0)
+    bc = abi.BC.make(_faces_for(direction, ground=ground_face), theta_ref=((0.0, 1500.0), (300.0, 300.0)), ustar=ustar,
+                     z0=z0, direction=direction, kappa=KAPPA, Cmu0=CMU0, l_max=LMAX, surface=surface)
+    ph = abi.Physics.make(1500.0, gravity=9.81, **turb)
+    opts = abi.SimplecOptions.make(zline_sweeps=zline_sweeps, precision=precision)
+    return Instance(f"config0-flat-{nx}x{ny}x{nz}", g, zl, ground, bc, ph, opts, ustar, z0, direction)
+
+
 def config1(nx=128, ny=128, nz=64, precision=0, zline_sweeps=4, turbulence=True):
     """Plain FP64 on the GPU over a single Gaussian hill h = 150 exp(-(r/300)^2)
     centred in a 128 x 128 x 64 grid, dx = dy = 25 m, the stretched layers to a

@@ -98,8 +98,10 @@ gb_status gb_ctx_profile_read(gb_ctx* ctx, int32_t family, double* total_ms, int
 gb_status gb_ctx_profile_mask(gb_ctx* ctx, uint32_t mask);
 /* Tuning knobs of a context (the in-project autotuner sets them per shape). */
 enum {
-    GB_TUNE_LINE_VARIANT = 0,   /* z-line sweep kernel: 0 auto (= 4), 1 pipelined (cp.async ring), 2 shared,
-                                   3 global scratch, 4 pipelined with the column factors kept between sweeps */
+    GB_TUNE_LINE_VARIANT = 0,   /* z-line sweep kernel: 0 auto (= 5), 1 pipelined (cp.async ring), 2 shared,
+                                   3 global scratch, 4 pipelined with the column factors kept between sweeps,
+                                   5 segmented: the column's levels split among the warps of a block, the
+                                   factors kept between sweeps (columns of more than 128 levels: 4) */
     GB_TUNE_LINE_BLOCK,         /* threads per block of the pipelined sweep (32, 64 or 128; 0 = default) */
     GB_TUNE_MG_COARSE_KERNEL,   /* the coarsest level's relaxations: 0 auto (one single-block launch when the
                                    level has at most 64 columns), 1 the per-relaxation launches */
@@ -109,9 +111,14 @@ enum {
                                    0 auto (= 1), 1 shared memory, 2 the global arrays (c' stored, e' in the
                                    output array), 3 e' in shared memory and c' read again from its stored
                                    array (L2): less shared memory per warp, more warps per SM */
-    GB_TUNE_MG_FUSED_RELAX,     /* one launch per colour of the zebra line relaxation (the residual in shared
-                                   memory): 0 auto (= 1), 1 never (the residual and the solve as two launches),
-                                   2 on every level, 3 on the levels of at most 1024 columns */
+    GB_TUNE_MG_FUSED_RELAX,     /* one launch per colour of the zebra line relaxation: 0 auto (= 4), 1 never
+                                   (the residual and the solve as two launches), 2 the residual in shared memory
+                                   and one thread per column's solve, on every level, 3 that on the levels of at
+                                   most 1024 columns, 4 segmented (the column's levels split among the warps of
+                                   a block, the residual in registers; columns of more than 128 levels: 1) */
+    GB_TUNE_LINE_SEGMENT,       /* levels per warp of the segmented z-line sweep (default 8) and of the
+                                   segmented zebra relaxation (default 4, 8 for columns of more than 64
+                                   levels): 0 default, 4 or 8 */
     GB_N_TUNE
 };
 gb_status gb_ctx_tune(gb_ctx* ctx, int32_t key, int32_t value);
@@ -163,6 +170,8 @@ gb_status gb_zline_lusgs(gb_ctx* ctx, const gb_grid* g, int32_t loc, const doubl
  * - Set-up: the first call on each device (that device current) looks up the
  *   array's address and sets the kernels' shared-memory limit; later calls on
  *   that device reuse it. Make that first call before any stream capture.
+ *   A cudaDeviceReset of that device after its first call is not supported:
+ *   the kept address would belong to the destroyed context.
  * - Sharing: every call on a device uses the same array. Calls issued one
  *   after another on one stream are safe; calls that may overlap (other
  *   streams, other threads) race on it. The iterate needs no initial value
@@ -171,7 +180,8 @@ gb_status gb_zline_lusgs(gb_ctx* ctx, const gb_grid* g, int32_t loc, const doubl
  * - stream: the caller's cudaStream_t (NULL: the default stream). With change
  *   non-NULL the call waits for the stream to read max |change|; with change
  *   NULL it returns as soon as the work is queued.
- * Results equal those of gb_zline_jacobi on a context with default tuning. */
+ * Results agree with those of gb_zline_jacobi to rounding (the same column
+ * solves; the context path keeps the column factors between sweeps). */
 gb_status gb_zline_jacobi_noalloc(const gb_grid* g, int32_t loc, const double* A, const double* ap,
                                   const double* rhs, int32_t sweeps, double* delta, double* change, void* stream);
 
@@ -462,6 +472,82 @@ gb_status gb_simplec_implicit_rows(gb_simplec* s, const gb_state* q, int32_t eq,
 /* SimplecStage::iterate (Source/Simplec.cpp:452-506): one SIMPLEC outer
  * iteration of q with the local pseudo-time step dtau (cells). */
 gb_status gb_simplec_iterate(gb_simplec* s, const gb_state* q, const double* dtau, gb_iter_info* info);
+
+/* ---- the iteration's steps alone ---------------------------------------
+ * The pieces of gb_simplec_iterate that the reference also calls from outside
+ * SimplecStage::iterate (the Newton preconditioner and the grid-sequencing
+ * transfer reuse the predictor, the pressure correction and the scalar
+ * sweep). Each runs the iteration's own code on the stage's workspace, in the
+ * iteration's order: gb_simplec_fill_ghosts(q), gb_simplec_residual(q, R),
+ * gb_momentum_predictor(q, R, dtau), gb_pressure_correction(q),
+ * gb_scalar_sweep(theta), gb_scalar_sweep(k). */
+
+/* gust::MomentumPredictorResult (Source/Predictor.H:214-220). */
+typedef struct gb_predictor_result {
+    double max_du, max_dv, max_dw;                     /* max |correction| applied per component */
+    double last_sweep_du, last_sweep_dv, last_sweep_dw; /* max |change over the last sweep| */
+} gb_predictor_result;
+
+/* gust::PressureCorrectionResult (Source/Simplec.H:117-124), with the
+ * Poisson solve's iterations and removed mean (gust::PoissonResult). */
+typedef struct gb_pressure_result {
+    int32_t poisson_iterations;
+    double poisson_removed_mean;
+    double divergence_before, divergence_after; /* max |div u| before and after */
+    double max_dp;                              /* max |alpha_p p'| */
+    double max_du, max_dv, max_dw;              /* max |velocity correction| per component */
+} gb_pressure_result;
+
+/* gust::ScalarSweepResult (Source/Simplec.H:149-154). */
+typedef struct gb_scalar_result {
+    double max_dq;      /* max |dq| applied */
+    double last_sweep;  /* max |change over the last sweep| */
+    int64_t clipped;    /* cells raised to the floor (k only) */
+} gb_scalar_result;
+
+/* gust::momentum_predictor (Source/Predictor.H:242-252, Predictor.cpp:129-405)
+ * on q's u, v, w: R the residual at q as gb_simplec_residual returned it (the
+ * closure's fields of that evaluation and the wall state of the last
+ * gb_simplec_fill_ghosts are the ones used, as the reference's caller passes
+ * its residual's fields and surface state), dtau the cell pseudo-time step
+ * (face_dtau is taken here), the transport fluxes of q. ap and d (three
+ * device arrays each, u, v, w faces, or NULL) receive PredictorFields' a_P
+ * and the SIMPLEC denominators; the stage also keeps d for
+ * gb_pressure_correction. q's ghosts are not refilled. */
+gb_status gb_momentum_predictor(gb_simplec* s, const gb_state* q, double* const* R, const double* dtau,
+                                double* const* ap, double* const* d, gb_predictor_result* res);
+
+/* gust::pressure_correction (Source/Simplec.H:139-141, Simplec.cpp:134-220)
+ * on q's u, v, w and p: d the SIMPLEC denominators on the u, v, w faces
+ * (three device arrays, finite and >= 0; NULL: those of the last
+ * gb_momentum_predictor). The ghosts of q are filled first, as the iteration
+ * refills them after the predictor, without touching the wall state kept for
+ * the scalar sweeps. The Poisson solve uses the stage's solver and
+ * simplec.pressure_reltol; a predicted velocity with a net source the
+ * boundaries cannot carry is refused (GB_BAD_ARG) with the reference's
+ * message. */
+gb_status gb_pressure_correction(gb_simplec* s, const gb_state* q, const double* const* d, gb_pressure_result* res);
+
+/* gust::scalar_sweep (Source/Simplec.H:156-163, Simplec.cpp:222-281) of eq
+ * (4 theta, 5 k) in delta form on q's field: (1/dtau + A1) dq = -R_eq with
+ * the implicit rows of the transport fluxes of q (its ghosts filled first, as
+ * the iteration refills them before the sweeps), the closure's fields of the
+ * last residual and the wall state of the last gb_simplec_fill_ghosts;
+ * `simplec.zline_sweeps` sweeps; k clipped at simplec.tke_floor (counted)
+ * unless clip is 0. */
+gb_status gb_scalar_sweep(gb_simplec* s, const gb_state* q, int32_t eq, const double* R_eq, const double* dtau,
+                          int32_t clip, gb_scalar_result* res);
+
+/* gust::implicit_coefficients (Source/ImplicitOperator.H:65-67,
+ * ImplicitOperator.cpp:96-121): the 7 coefficients at loc (GB_LOC_CELL or a
+ * face) of the upwind transport F (x-, y-, z-face fluxes, one ghost) and the
+ * principal diffusion with the metric of the cell diffusivity gamma (one
+ * ghost), the node heights z_nd and detJ; the face means of gamma are
+ * arithmetic, or logarithmic with log_mean = 1 (FaceMean). A: GB_N_COEFS
+ * device arrays of the grid, component-major (valid points written). */
+gb_status gb_implicit_coefficients(gb_ctx* ctx, const gb_grid* g, int32_t loc, const double* F0, const double* F1,
+                                   const double* F2, const double* gamma, const double* z_nd, const double* detJ,
+                                   int32_t log_mean, double* A);
 
 /* SimplecStage::closure_fields (Source/Simplec.H:216) and the wall model's
  * state: the closure's fields at the last residual (nu, gamma_theta,

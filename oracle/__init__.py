@@ -267,6 +267,10 @@ def _declare_simplec(L):
                                       ctypes.POINTER(State), ctypes.POINTER(MeshFields), ctypes.POINTER(Diffusivities),
                                       P, PP, ctypes.POINTER(IterInfo), PP, PP]
     L.og_simplec_iterate2.restype = i32
+    L.og_stage_steps.argtypes = [G, ctypes.POINTER(BC), ctypes.POINTER(Physics), ctypes.POINTER(SimplecOptions),
+                                 ctypes.POINTER(State), ctypes.POINTER(MeshFields), ctypes.POINTER(Diffusivities),
+                                 P, PP, PP, PP, PP, P, P, P]
+    L.og_stage_steps.restype = i32
     L.og_closure_evaluate.argtypes = [G, ctypes.POINTER(BC), ctypes.POINTER(Physics), P, P, P, P, P, P, P, PP]
     L.og_surface_state.argtypes = [G, ctypes.POINTER(BC), ctypes.POINTER(Physics), P, P, P, P, P, PP]
     L.og_surface_state.restype = i32
@@ -429,6 +433,7 @@ def prolong_state(coarse, fine, r, bc, phys, opts, reltol=1e-10):
     """prolong_state (Transfer.cpp:322-385) into the fine case: returns
     (status, [divergence before, after, Poisson iterations, k cells raised])."""
     info = (ctypes.c_double * 4)()
+    fine.nut_hist = None   # the prolonged state is a new level's: no nu_t history
     sc, sf, m = coarse.state(), fine.state(), fine.mesh()
     rc = _L().og_prolong_state(ctypes.byref(coarse.grid.c), ctypes.byref(sc), ctypes.byref(fine.grid.c),
                                ctypes.byref(sf), int(r), ctypes.byref(bc), ctypes.byref(phys), ctypes.byref(opts),
@@ -485,12 +490,40 @@ def simplec_iterate(case, bc, phys, opts, dtau):
     return int(rc), info, R
 
 
+def stage_steps(case, bc, phys, opts, dtau):
+    """The predictor, the pressure correction and the scalar sweeps of one
+    SimplecStage::iterate (Simplec.cpp:452-506) taken one at a time
+    (og_stage_steps) on the case's state, which ends as the iteration leaves
+    it without theta's convection update. Returns a dict: status, R (the
+    residual at the start), ap and d (the predictor's), the snapshots u, v, w
+    after the predictor ("pred") and u, v, w, p after the correction ("pc"),
+    and the infos: pred (max |du|, |dv|, |dw|, last sweeps), pc (divergence
+    before, after, max |dp|, max |du|, |dv|, |dw|, removed mean, Poisson
+    iterations), scalar (max |dtheta|, its last sweep, max |dk|, its last
+    sweep, clipped)."""
+    _history(case)
+    g = case.grid
+    R = [g.np_zeros() for _ in range(6)]
+    ap = [g.np_zeros() for _ in range(3)]
+    dd = [g.np_zeros() for _ in range(3)]
+    snap = [g.np_zeros() for _ in range(7)]
+    pinfo, cinfo, sinfo = np.zeros(6), np.zeros(8), np.zeros(5)
+    st, m, d = case.state(), case.mesh(), case.diffusivities()
+    rc = _L().og_stage_steps(ctypes.byref(g.c), ctypes.byref(bc), ctypes.byref(phys), ctypes.byref(opts),
+                             ctypes.byref(st), ctypes.byref(m), ctypes.byref(d), _p(dtau), _arrays(R), _arrays(ap),
+                             _arrays(dd), _arrays(snap), _p(pinfo), _p(cinfo), _p(sinfo))
+    return {"status": int(rc), "R": R, "ap": ap, "d": dd,
+            "pred": dict(zip(("u", "v", "w"), snap[:3])), "pc": dict(zip(("u", "v", "w", "p"), snap[3:])),
+            "pred_info": pinfo, "pc_info": cinfo, "scalar_info": sinfo}
+
+
 def initialize(case, bc, init_opts):
     """gust::initialize_state with init.first_guess = profile
     (Source/Initializer.cpp:281-430) on the case's state; returns (status,
     [divergence before, after, Poisson iterations, final residual, O'Brien's
     top residual])."""
     info = np.zeros(5)
+    case.nut_hist = None   # a new initial state has no nu_t history
     st, m = case.state(), case.mesh()
     rc = _L().og_initialize(ctypes.byref(case.grid.c), ctypes.byref(bc), ctypes.byref(init_opts), ctypes.byref(st),
                             ctypes.byref(m), _p(info))

@@ -1577,3 +1577,76 @@ int og_initialize(const og_grid* g, const gb_bc* bc, const gb_init_opts* io, gb_
     free(om);
     return status;
 }
+
+/* The first steps of SimplecStage::iterate (Simplec.cpp:452-506) one at a
+ * time, for the tests of the stage's stand-alone entry points
+ * (momentum_predictor, pressure_correction, scalar_sweep): the ghost fill
+ * with the wall state and the residual at q (into R), the momentum predictor
+ * (Predictor.cpp:129-405; pinfo[6], ap[3], dd[3]), the ghost fill and the
+ * pressure correction with the predictor's denominators (Simplec.cpp:134-220;
+ * cinfo[8]), then the scalar sweeps (Simplec.cpp:222-281) of theta with
+ * R_theta as the residual left it and of k, each after a ghost fill, with the
+ * transport fluxes of the corrected state (sinfo: max |dtheta|, its last
+ * sweep, max |dk|, its last sweep, cells clipped). snap (7 arrays, or NULL)
+ * receives u, v, w after the predictor and u, v, w, p after the correction. */
+int og_stage_steps(const og_grid* g, const gb_bc* bc, const gb_physics* ph, const gb_simplec_opts* so, gb_state* q,
+                   const gb_mesh_fields* m, const gb_diffusivities* df, const double* dtau, double** R, double** ap,
+                   double** dd, double** snap, double* pinfo, double* cinfo, double* sinfo)
+{
+    const int64_t vol = VOL(g);
+    double* cfl[N_CF] = {0};
+    double* ssl[N_SS] = {0};
+    og_turb tcv = {NULL, NULL};
+    if (ph->closure) {
+        for (int n = 0; n < N_CF; ++n) { cfl[n] = zalloc(g); }
+        tcv.cf = cfl;
+    }
+    if (bc->face[2] == GB_FACE_SURFACE_LAYER) {
+        for (int n = 0; n < N_SS; ++n) { ssl[n] = palloc(g); }
+        tcv.ss = ssl;
+    }
+    const og_turb* tc = &tcv;
+    og_fill_ghosts2(g, bc, ph, m->z0, q->u, q->v, q->w, q->p, q->theta, q->tke, q->z_nd, (double**)tc->ss);
+    residual_t(g, bc, ph, q, m, df, R, tc);
+    double* F[3] = {zalloc(g), zalloc(g), zalloc(g)};
+    og_transport_fluxes(g, q->u, q->v, q->w, q->z_nd, m->ax, m->ay, F[0], F[1], F[2]);
+    double* dcc = zalloc(g);
+    memcpy(dcc, dtau, sizeof(double) * vol);
+    double* dtf[3] = {zalloc(g), zalloc(g), zalloc(g)};
+    og_face_dtau(g, dcc, dtf[0], dtf[1], dtf[2]);
+    og_momentum_predictor(g, bc, ph, so, q, R, F[0], F[1], F[2], dtf, m, df, tc, ap, dd, pinfo);
+    if (snap) {
+        memcpy(snap[0], q->u, sizeof(double) * vol);
+        memcpy(snap[1], q->v, sizeof(double) * vol);
+        memcpy(snap[2], q->w, sizeof(double) * vol);
+    }
+    og_fill_ghosts2(g, bc, ph, m->z0, q->u, q->v, q->w, q->p, q->theta, q->tke, q->z_nd, NULL);
+    const int st = og_pressure_correction(g, bc, so, q, dd, m, cinfo);
+    if (snap) {
+        memcpy(snap[3], q->u, sizeof(double) * vol);
+        memcpy(snap[4], q->v, sizeof(double) * vol);
+        memcpy(snap[5], q->w, sizeof(double) * vol);
+        memcpy(snap[6], q->p, sizeof(double) * vol);
+    }
+    og_fill_ghosts2(g, bc, ph, m->z0, q->u, q->v, q->w, q->p, q->theta, q->tke, q->z_nd, NULL);
+    og_transport_fluxes(g, q->u, q->v, q->w, q->z_nd, m->ax, m->ay, F[0], F[1], F[2]);
+    double last;
+    int64_t clipped = 0;
+    sinfo[0] = og_scalar_sweep(g, bc, ph, so, F_THETA, q->theta, R[4], F[0], F[1], F[2], q->z_nd, m->detJ, df, tc,
+                               dtau, 0, 0, &last, &clipped);
+    sinfo[1] = last;
+    og_fill_ghosts2(g, bc, ph, m->z0, q->u, q->v, q->w, q->p, q->theta, q->tke, q->z_nd, NULL);
+    og_transport_fluxes(g, q->u, q->v, q->w, q->z_nd, m->ax, m->ay, F[0], F[1], F[2]);
+    sinfo[2] = og_scalar_sweep(g, bc, ph, so, F_TKE, q->tke, R[5], F[0], F[1], F[2], q->z_nd, m->detJ, df, tc, dtau,
+                               so->tke_floor, 1, &last, &clipped);
+    sinfo[3] = last;
+    sinfo[4] = (double)clipped;
+    for (int c = 0; c < 3; ++c) {
+        free(F[c]);
+        free(dtf[c]);
+    }
+    free(dcc);
+    for (int n = 0; n < N_CF; ++n) { free(cfl[n]); }
+    for (int n = 0; n < N_SS; ++n) { free(ssl[n]); }
+    return st;
+}

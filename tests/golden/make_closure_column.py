@@ -13,7 +13,7 @@ length, R_u, R_v, R_w (face means), R_theta, R_tke, Ps, eps and, on the
 ground cells, ustar. This script, run once in a container that holds the
 reference, writes them as (64, 8, 8) arrays [k, j, i].
 
-Usage: python tests/golden/make_closure_column.py /root/reference
+Usage: python tests/golden/make_closure_column.py REFERENCE_ROOT
 """
 import os
 import sys
@@ -38,4 +38,6 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        raise SystemExit(__doc__)
+    main(sys.argv[1])

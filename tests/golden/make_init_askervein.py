@@ -15,7 +15,7 @@ reference, writes:
                            before and after, extrema).
 The mesh comes from tests/golden/poisson_askervein.npz (zlevels, ground).
 
-Usage: python tests/golden/make_init_askervein.py /root/reference
+Usage: python tests/golden/make_init_askervein.py REFERENCE_ROOT
 """
 import json
 import os
@@ -43,4 +43,6 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        raise SystemExit(__doc__)
+    main(sys.argv[1])

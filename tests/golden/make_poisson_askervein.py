@@ -19,7 +19,7 @@ The gold is AMReX's plotfile format: an ASCII FAB header per box, then the
 box's doubles in Fortran order, little-endian (the header's byte order
 "8 7 6 5 4 3 2 1").
 
-Usage: python tests/golden/make_poisson_askervein.py /root/reference
+Usage: python tests/golden/make_poisson_askervein.py REFERENCE_ROOT
 """
 import json
 import os
@@ -129,4 +129,6 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        raise SystemExit(__doc__)
+    main(sys.argv[1])

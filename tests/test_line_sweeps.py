@@ -96,6 +96,33 @@ def test_gpu_zline_jacobi_matches_oracle_fp64(ctx, loc, case, sweeps):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("variant,segment", [(4, 0), (5, 4), (5, 8)], ids=["factored", "segmented4", "segmented8"])
+@pytest.mark.parametrize("loc", LOCS)
+@pytest.mark.parametrize("case", [(37, 29, 17, True, False), (64, 48, 65, False, True), (33, 20, 128, True, True)])
+def test_gpu_zline_jacobi_kernels_match_oracle(ctx, variant, segment, loc, case):
+    """The sequential factored sweep (GB_TUNE_LINE_VARIANT 4) and the
+    segmented one with 4 or 8 levels per warp (5, the default) agree with the
+    oracle's column solves to 1e-12, on columns of 17 to 129 levels."""
+    import torch
+    import ablsteadyrans_b200 as gb
+    nx, ny, nz, px, py = case
+    g = Grid(nx, ny, nz, 30.0, 30.0, 10.0, px, py)
+    A, ap, rhs = random_system(g, loc, seed=5 + loc, extra=0.2, xscale=3.0)
+    d_ref = g.np_zeros()
+    ch_ref = oracle.zline_jacobi(g, loc, A, ap, rhs, 3, d_ref)
+    ctx.tune(gb.TUNE_LINE_VARIANT, variant)
+    ctx.tune(gb.TUNE_LINE_SEGMENT, segment)
+    try:
+        dd = torch.full(g.shape, 7.0, dtype=torch.float64, device="cuda")
+        ch = gb.zline_jacobi(ctx, g, loc, to_dev(A), to_dev(ap), to_dev(rhs), 3, dd)
+    finally:
+        ctx.tune(gb.TUNE_LINE_VARIANT, 0)
+        ctx.tune(gb.TUNE_LINE_SEGMENT, 0)
+    assert rel_err(to_host(dd), d_ref, g.valid(loc)) < 1e-12
+    assert abs(ch - ch_ref) <= 1e-12 * max(abs(ch_ref), 1e-300)
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("loc", LOCS)
 def test_gpu_zline_jacobi_fp32(ctx, loc):
     import torch
@@ -206,6 +233,7 @@ def test_gpu_batched_sweep_back_substitution_placement_is_bitwise_neutral(ctx, p
     from ablsteadyrans_b200 import workloads
     from ablsteadyrans_b200.simplec import DeviceCase, SimplecStage
     out = []
+    ctx.tune(gb.TUNE_LINE_VARIANT, 4)   # the factored kernel, where the placement applies
     for back in (1, 2, 3):
         inst = workloads.tile(40, 24, 3, precision=precision)
         ctx.tune(gb.TUNE_LINE_BACK, back)
@@ -218,6 +246,7 @@ def test_gpu_batched_sweep_back_substitution_placement_is_bitwise_neutral(ctx, p
         out.append({f: dc.host(f) for f in ("u", "v", "w", "p", "theta", "tke")})
         st.close()
     ctx.tune(gb.TUNE_LINE_BACK, 0)
+    ctx.tune(gb.TUNE_LINE_VARIANT, 0)
     for f in out[0]:
         assert np.array_equal(out[0][f], out[1][f]), f
         assert np.array_equal(out[0][f], out[2][f]), f

@@ -253,3 +253,36 @@ def test_gpu_simplec_newton_reaches_the_strict_criterion(ctx):
         assert max(res) < 5e-5
     finally:
         st.close()
+
+
+@pytest.mark.gpu
+def test_gpu_newton_hands_back_when_nut_relax_blends_the_history(ctx):
+    """With turb.nut_relax < 1 the Newton stage's equations blend nu_t with a
+    frozen SIMPLEC history, so they are not the run's: once the continuation
+    has converged on them the stage hands the run back to SIMPLEC for good
+    (NewtonStage::differs, NewtonStage.cpp:196-205 and 169-177), and the run
+    ends on SIMPLEC, steady by the driver's criterion."""
+    from ablsteadyrans_b200.abi import DriverOptions, SimplecOptions
+    from ablsteadyrans_b200.newton import SwitchOptions, newton_equations_differ, solve_simplec_newton
+    from ablsteadyrans_b200.simplec import DeviceCase, SimplecStage
+    case, bc, ph = _hill()
+    ph.turb_nut_relax = 0.5
+    dc = DeviceCase.from_oracle(case)
+    st = SimplecStage(ctx, dc, bc, ph, SimplecOptions.make(pressure_reltol=1e-6))
+    st.fill_ghosts()
+    assert newton_equations_differ(st)
+    events = []
+    try:
+        verdict, its, newton_its = solve_simplec_newton(
+            st, 4000, driver_options=DriverOptions.make(monitor_window=5), switch=SwitchOptions(1e-2, 5),
+            newton_options=NewtonOptions.make(gmres_restart=60, gmres_max_iters=300), events=events)
+        assert verdict == "steady", (verdict, its, events)
+        assert newton_its > 0
+        to_newton = [e for e in events if e[2] == "newton"]
+        back = [e for e in events if e[2] == "simplec" and "differ" in e[3]]
+        assert len(back) == 1, events
+        # no switch to Newton after the hand-back: the run ends on SIMPLEC
+        assert all(e[0] < back[0][0] for e in to_newton), events
+        assert events[-1] == back[0], events
+    finally:
+        st.close()

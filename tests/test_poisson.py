@@ -137,14 +137,18 @@ def test_gpu_apply_and_fluxes_match_oracle(ctx, per):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("relax", [0, 1])
 @pytest.mark.parametrize("kernel", [0, 1])
 @pytest.mark.parametrize("per", [(True, True), (False, False), (True, False)])
-def test_gpu_vcycle_matches_oracle_fp64(ctx, per, kernel):
+def test_gpu_vcycle_matches_oracle_fp64(ctx, per, kernel, relax):
     """One V-cycle of the FP64 multigrid agrees with the oracle's to 1e-12,
     with the coarsest level's relaxations in one single-block launch (kernel
-    0, the default) and launched one by one (kernel 1)."""
+    0, the default) and launched one by one (kernel 1), and the zebra
+    relaxation as one segmented launch per colour (relax 0, the default) or
+    as the residual and the column solves in two launches (relax 1)."""
     import ablsteadyrans_b200 as gb
     ctx.tune(gb.TUNE_MG_COARSE_KERNEL, kernel)
+    ctx.tune(gb.TUNE_MG_FUSED_RELAX, relax)
     g, z, J, ax, ay, az, _ = smooth_terrain_case(32, 24, 16, *per, hill=150.0)
     bc = (PERIODIC if per[0] else NEUMANN, PERIODIC if per[1] else NEUMANN, NEUMANN,
           PERIODIC if per[0] else DIRICHLET, PERIODIC if per[1] else NEUMANN, DIRICHLET)
@@ -159,6 +163,7 @@ def test_gpu_vcycle_matches_oracle_fp64(ctx, per, kernel):
     ps.set_coeffs(dax, day, daz)
     e = to_host(ps.vcycle(to_dev(r)))
     ctx.tune(gb.TUNE_MG_COARSE_KERNEL, 0)
+    ctx.tune(gb.TUNE_MG_FUSED_RELAX, 0)
     assert rel_err(e, e_ref, g.valid(0)) < 1e-12
     ps.close()
 

@@ -310,7 +310,9 @@ def test_gpu_turbulence_refusals(ctx):
                         (lambda b, p: b.face.__setitem__(5, FACE_SURFACE_LAYER), "the ground's only"),
                         (lambda b, p: setattr(b, "surface_heat_flux", 0.1), "stability is neutral"),
                         (lambda b, p: setattr(p, "turb_Rt_min", -4.0), "turb.Rt_min"),
-                        (lambda b, p: setattr(p, "turb_Cb", 0.0), "turb.Cb")):
+                        (lambda b, p: setattr(p, "turb_Cb", 0.0), "turb.Cb"),
+                        # a QNSE coefficient set under Businger-Dyer would be ignored (SurfaceLayer.cpp:282-288)
+                        (lambda b, p: setattr(b, "surface_qnse_bm", 0.3), "qnse_bm is set but stable_functions")):
         case, bc, ph = _hill_case()
         mutate(bc, ph)
         with pytest.raises(gb.GustError, match=msg):
@@ -636,6 +638,38 @@ def test_gpu_nut_relaxation_iterations_match_oracle(ctx):
                 assert np.abs(got - ref).max() <= 1e-9 * max(np.abs(ref).max(), 1e-300), (it, f)
     finally:
         st.close()
+
+
+@pytest.mark.gpu
+def test_gpu_initialize_clears_the_nut_history(ctx):
+    """A stage that iterated with turb.nut_relax < 1 and is then initialized
+    again starts without a nu_t history, as a fresh stage does (each level's
+    closure is new when its state is initialized in the reference): its next
+    iteration equals a fresh stage's bit for bit."""
+    import torch
+    from ablsteadyrans_b200.abi import InitOptions
+    case, bc, ph = _hill_case()
+    ph.turb_nut_relax = 0.5
+    opts = dict(pressure_reltol=1e-8, zline_sweeps=2)
+    q0 = {f: a.copy() for f, a in case.q.items()}
+    dc1, st1 = _stage(ctx, case, bc, ph, **opts)
+    dc2, st2 = _stage(ctx, case, bc, ph, **opts)
+    try:
+        st1.fill_ghosts()
+        for _ in range(2):
+            st1.iterate(st1.local_dtau(2.0))
+        for dc, st in ((dc1, st1), (dc2, st2)):
+            for f in q0:
+                dc.q[f].copy_(torch.from_numpy(q0[f]))
+            st.initialize(InitOptions.make())
+            st.fill_ghosts()
+            st.iterate(st.local_dtau(2.0))
+        for f, loc in zip(FIELDS, LOCS):
+            v = case.grid.valid(loc)
+            assert np.array_equal(dc1.host(f)[v], dc2.host(f)[v]), f
+    finally:
+        st1.close()
+        st2.close()
 
 
 def test_oracle_surface_layer_qnse_stable_side():
