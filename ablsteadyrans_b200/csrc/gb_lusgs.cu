@@ -7,16 +7,28 @@
 //
 // B200 mapping. Within a pass a column depends on the two columns before it
 // in both directions, so the pass walks the wavefront planes
-// (i - ilo) + (j - jlo) = s (the reference's diagonal order, bit-identical to
-// its sequential order): one block, one thread per column of a plane, a block
-// barrier between planes (a plane is at most min(ni, nj) columns). The
-// system is the same in every pass of a solve, so its column factors (1/m,
-// c') are computed once, in parallel over all columns, and each column solve
-// is division-free; the pass keeps only e in scratch. Loads of 8 levels are
-// issued together ahead of each column's recurrence.
+// (i - ilo) + (j - jlo) = s (the reference's diagonal order, which gives the
+// values of its sequential order): no two columns of a plane are neighbours,
+// so a plane's columns are solved in parallel, and the planes follow one
+// another. The system is the same in every pass of a solve, so its column
+// factors (1/m, c') are computed once, in parallel over all columns, and each
+// column solve is division-free.
+//
+// The pass is ONE launch of one thread-block cluster (up to 8 CTAs, on as
+// many SMs): each CTA takes 32 columns of the plane at a time, its warps
+// splitting the column's levels into segments (the segmented recurrences of
+// the z-line sweep: each warp's levels loaded at once, the values crossing a
+// segment boundary carried through shared memory as composed affine maps),
+// and the cluster's hardware barrier (barrier.cluster, release/acquire)
+// separates the planes. The iterate is read through L2 (ld.global.cg), since
+// other CTAs of the cluster wrote it on other SMs.
 #include "gb_line.cuh"
 
+#include <cooperative_groups.h>
+
 #include <algorithm>
+
+namespace cg = cooperative_groups;
 
 namespace gb {
 
@@ -160,6 +172,120 @@ __global__ void __launch_bounds__(256) k_lusgs_pass(LusgsArgs a, int forward)
     }
 }
 
+//! One pass as one cluster launch (see the file's header): planes in order
+//! (ascending forward, descending backward), 32 columns per CTA at a time,
+//! L levels per warp, a cluster barrier between planes. JREV: the j-reversed
+//! pair. Shared memory: the carries of e' and x, [4][W][32].
+template <bool JREV, int L>
+__global__ void __launch_bounds__(512) k_lusgs_pass_cluster(LusgsArgs a, int forward)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cg::cluster_group cluster = cg::this_cluster();
+    const int C = static_cast<int>(cluster.num_blocks());
+    const int cta = static_cast<int>(cluster.block_rank());
+    const gb_grid& g = a.g;
+    const int lane = threadIdx.x, w = threadIdx.y, W = blockDim.y;
+    const int cs = W * 32;
+    const int me = w * 32 + lane;
+    double* carry_e = reinterpret_cast<double*>(smem_raw);
+    double* carry_x = carry_e + 2 * cs;
+    const int k0 = w * L;
+    const int nk = a.nk;
+    const int last = a.ni + a.nj - 2;
+    const double* axm = a.A + GB_COEF_XM * a.cs;
+    const double* axp = a.A + GB_COEF_XP * a.cs;
+    const double* aym = a.A + GB_COEF_YM * a.cs;
+    const double* ayp = a.A + GB_COEF_YP * a.cs;
+    const double* azm = a.A + GB_COEF_ZM * a.cs;
+    const int64_t sy = g.sy;
+    for (int q = 0; q <= last; ++q) {
+        const int s = forward ? q : last - q;
+        const int amin = max(0, s - (a.nj - 1)), amax = min(s, a.ni - 1);
+        const int count = amax - amin + 1;
+        for (int base = cta * 32; base < count; base += C * 32) {   // the same trip count for every thread of a CTA
+            const int m = base + lane;
+            const bool col = m < count;
+            const int i = amin + m;
+            const int j = JREV ? a.nj - 1 - (s - i) : s - i;
+            const int64_t o0 = col ? at(g, i, j, 0) : 0;
+            double R[L], LO[L], IM[L], CP[L];
+#pragma unroll
+            for (int r = 0; r < L; ++r) {
+                const int k = k0 + r;
+                R[r] = 0.0;
+                LO[r] = 0.0;
+                IM[r] = 0.0;
+                CP[r] = 0.0;
+                if (col && k < nk) {
+                    const int64_t o = o0 + static_cast<int64_t>(k) * g.sz;
+                    R[r] = a.rhs[o] + axm[o] * __ldcg(a.d + o - 1) + axp[o] * __ldcg(a.d + o + 1)
+                         + aym[o] * __ldcg(a.d + o - sy) + ayp[o] * __ldcg(a.d + o + sy);
+                    LO[r] = -azm[o];
+                    IM[r] = a.inv[o];
+                    CP[r] = a.cp[o];
+                }
+            }
+            // e_k = (R_k - L_k e_{k-1}) / m_k: the segment's affine map
+            double al = 0.0, be = 1.0;
+#pragma unroll
+            for (int r = 0; r < L; ++r) {
+                const int k = k0 + r;
+                if (k < nk) {
+                    if (k == 0) {
+                        al = R[r] * IM[r];
+                        be = 0.0;
+                    } else {
+                        al = (R[r] - LO[r] * al) * IM[r];
+                        be = (-LO[r] * be) * IM[r];
+                    }
+                }
+            }
+            carry_e[me] = al;
+            carry_e[cs + me] = be;
+            __syncthreads();
+            double ep = 0.0;
+            for (int t = 0; t < w; ++t) { ep = carry_e[t * 32 + lane] + carry_e[cs + t * 32 + lane] * ep; }
+#pragma unroll
+            for (int r = 0; r < L; ++r) {
+                const int k = k0 + r;
+                if (k < nk) {
+                    ep = ((k == 0) ? R[r] : R[r] - LO[r] * ep) * IM[r];
+                    R[r] = ep;
+                }
+            }
+            // x_k = e_k - c'_k x_{k+1} (x_{nk-1} = e_{nk-1}): the segment's affine map from above
+            double ga = 0.0, de = 1.0;
+#pragma unroll
+            for (int r = L - 1; r >= 0; --r) {
+                const int k = k0 + r;
+                if (k < nk) {
+                    if (k == nk - 1) {
+                        ga = R[r];
+                        de = 0.0;
+                    } else {
+                        ga = R[r] - CP[r] * ga;
+                        de = -CP[r] * de;
+                    }
+                }
+            }
+            carry_x[me] = ga;
+            carry_x[cs + me] = de;
+            __syncthreads();
+            double x = 0.0;
+            for (int t = W - 1; t > w; --t) { x = carry_x[t * 32 + lane] + carry_x[cs + t * 32 + lane] * x; }
+#pragma unroll
+            for (int r = L - 1; r >= 0; --r) {
+                const int k = k0 + r;
+                if (k < nk) {
+                    x = (k == nk - 1) ? R[r] : R[r] - CP[r] * x;
+                    if (col) { a.d[o0 + static_cast<int64_t>(k) * g.sz] = x; }
+                }
+            }
+        }
+        cluster.sync();
+    }
+}
+
 //! max |b - d| over the valid points into a result word (rows of the box
 //! over the warps, one atomic per block).
 __global__ void __launch_bounds__(256) k_lusgs_change(gb_grid g, int ni, int nj, int nk, const double* __restrict__ b,
@@ -209,6 +335,11 @@ gb_status zline_lusgs(gb_ctx* ctx, const gb_grid& g, int loc, const double* A, c
     const int plane = std::min(ni, nj);
     const int nthr = std::min(256, std::max(32, (plane + 31) / 32 * 32));
     const int ext = std::max(ni, nj);
+    // the cluster pass: 8 levels per warp (columns of at most 128 levels), a
+    // CTA per 32 columns of the widest plane, at most 8 CTAs (the portable
+    // cluster size); taller columns take the single-block pass
+    const int cl_warps = ((nk + 7) / 8 <= 16 && ctx->tune[GB_TUNE_LINE_VARIANT] != 4) ? (nk + 7) / 8 : 0;
+    const int cl_ctas = std::min(8, std::max(1, (plane + 31) / 32));
     if (change_word != nullptr) { cudaMemsetAsync(change_word, 0, sizeof(unsigned long long), ctx->stream); }
     for (int s = 0; s < sweeps; ++s) {
         const bool jrev = alternate && (s % 2 == 1);
@@ -222,7 +353,25 @@ gb_status zline_lusgs(gb_ctx* ctx, const gb_grid& g, int loc, const double* A, c
                                                                                      delta);
                 ++ctx->launches;
             }
-            if (jrev) {
+            if (cl_warps > 0) {
+                cudaLaunchConfig_t cfg{};
+                cfg.gridDim = dim3(cl_ctas, 1, 1);
+                cfg.blockDim = dim3(32, cl_warps, 1);
+                cfg.dynamicSmemBytes = static_cast<size_t>(4) * cl_warps * 32 * sizeof(double);
+                cfg.stream = ctx->stream;
+                cudaLaunchAttribute attr[1];
+                attr[0].id = cudaLaunchAttributeClusterDimension;
+                attr[0].val.clusterDim.x = cl_ctas;
+                attr[0].val.clusterDim.y = 1;
+                attr[0].val.clusterDim.z = 1;
+                cfg.attrs = attr;
+                cfg.numAttrs = 1;
+                if (jrev) {
+                    cudaLaunchKernelEx(&cfg, k_lusgs_pass_cluster<true, 8>, a, static_cast<int>(forward));
+                } else {
+                    cudaLaunchKernelEx(&cfg, k_lusgs_pass_cluster<false, 8>, a, static_cast<int>(forward));
+                }
+            } else if (jrev) {
                 k_lusgs_pass<true><<<1, nthr, 0, ctx->stream>>>(a, forward);
             } else {
                 k_lusgs_pass<false><<<1, nthr, 0, ctx->stream>>>(a, forward);

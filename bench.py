@@ -2,22 +2,32 @@
 """Benchmark of the B200 SIMPLEC hot path (one JSON line on rank 0).
 
 python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                [--precision 0|1] [--workload config1]
+                [--precision 0|1] [--no-cpu] [--no-steady] [--no-batch]
 
 A step is one SIMPLEC outer iteration of config 1 (a single Gaussian hill,
 128 x 128 x 64 cells, dx = 25 m, stretched layers to a 1500 m lid, log-law
-inflow from the west, Coriolis, neutral): the local pseudo-time step, the
-iteration (ghost fills, FP64 residual, momentum predictor with z-line sweeps,
-the terrain pressure correction, theta and k sweeps, norms) and the host
-driver's criterion and SER CFL. The metric is cell-updates/s (cells x
-iterations / s). Under torchrun (N > 1) every rank iterates its own
-independent instance (the path shards by instance: no collective on the data
-path); the timed region is bracketed by a barrier and a device synchronise and
-the max over ranks is reported.
+inflow from the west, Coriolis, neutral, the k-L closure and the surface
+layer): the local pseudo-time step, the iteration (ghost fills, FP64
+residual, momentum predictor with z-line sweeps, the terrain pressure
+correction, theta and k sweeps, norms) and the host driver's criterion and
+SER CFL. The metric is cell-updates/s (cells x iterations / s). Under
+torchrun (N > 1) every rank iterates its own independent instance (the path
+shards by instance: no collective on the data path); the timed region is
+bracketed by a barrier and a device synchronise and the max over ranks is
+reported.
+
+Beside the headline, on one GPU (N = 1): the Poisson kernels' rooflines
+(the fine-level terrain operator, one V-cycle in FP64 and FP32), config 1
+solved to the steady criterion in plain FP64 and with FP32 inner solves
+(steady solves/s, iterations and the per-field difference of the two
+steady states), and the batched form on a sample of the batched
+configuration's uneven tiles (FP32 inner solves on concurrent streams
+against plain FP64 one by one, cell-updates/s).
 
 --impl reference times the reference's CPU implementation of the path, here
-the oracle (the FP64 C restatement; the reference itself needs AMReX, which
-is not available), on every host thread, on the same workload and metric.
+the FP64 C restatement of it (the reference itself needs AMReX, which is not
+available), built for speed on the host that runs it, on every host thread,
+on the same workload and metric.
 """
 import argparse
 import ctypes
@@ -241,6 +251,206 @@ def whole_job_rate(cells_per_rank, world, steps, ms):
     return cells_per_rank * world * steps / (ms / 1e3)
 
 
+def bench_config(wl):
+    """The `config` object of both arms' lines (the same workload)."""
+    return {"workload": wl.name, "cells": wl.cells,
+            "l2": "flushed between timed steps (256 MB write); the CPU arm has no flush to make"}
+
+
+# ------------------------------------------------- the Poisson rooflines ---
+# Algorithmic words per cell: the terrain operator apply reads phi, the
+# three a beta, J and z_nd and writes y (7); a z-line zebra relaxation of a
+# level reads phi, rhs, the three areas, J and z_nd and writes phi (8); the
+# residual of a level is an apply (7); restriction reads the fine residual
+# and writes a quarter coarse value (1.25 per fine cell), prolongation reads
+# a quarter coarse value and phi and writes phi (2.25 per fine cell).
+APPLY_WORDS, RELAX_WORDS, RESTRICT_WORDS, PROLONG_WORDS = 7, 8, 1.25, 2.25
+
+
+def mg_levels(nx, ny, max_levels, min_coarse):
+    """The multigrid's levels (nx, ny): x and y halved while both stay even
+    and at least min_coarse, at most max_levels."""
+    out = [(nx, ny)]
+    while len(out) < max_levels:
+        cx, cy = out[-1]
+        if cx % 2 or cy % 2 or cx // 2 < min_coarse or cy // 2 < min_coarse:
+            break
+        out.append((cx // 2, cy // 2))
+    return out
+
+
+def vcycle_words(nx, ny, nz, opts):
+    """Algorithmic words of one V-cycle per the table above."""
+    levels = mg_levels(nx, ny, opts.max_levels, opts.min_coarse)
+    words = 0.0
+    for n, (lx, ly) in enumerate(levels):
+        cells = lx * ly * nz
+        if n == len(levels) - 1:
+            words += opts.nu_coarse * RELAX_WORDS * cells
+        else:
+            words += ((opts.nu1 + opts.nu2) * RELAX_WORDS + APPLY_WORDS + RESTRICT_WORDS + PROLONG_WORDS) * cells
+    return words, len(levels)
+
+
+def poisson_rooflines(ctx, wl, flush, peak, reps=12):
+    """The fine-level terrain operator (FP64) and one V-cycle (FP64, FP32)
+    on config 1's mesh, each launch timed alone by CUDA events on the
+    context's stream with a 256 MB L2 flush before it (the level's arrays
+    would otherwise sit in the 126 MB L2)."""
+    import torch
+
+    import ablsteadyrans_b200 as gb
+    from ablsteadyrans_b200.abi import FACE_INFLOW, FACE_OUTFLOW, FACE_PERIODIC
+    g = wl.inst.grid
+    case = wl.case
+    face = list(wl.inst.bc.face)
+
+    def pbc(t):
+        if t == FACE_PERIODIC:
+            return gb.POISSON_PERIODIC
+        return gb.POISSON_DIRICHLET if t == FACE_OUTFLOW else gb.POISSON_NEUMANN
+    bc = tuple(pbc(t) for t in face)
+    assert FACE_INFLOW in face
+    rng = np.random.default_rng(1)
+    r = torch.from_numpy(g.np_zeros()).cuda()
+    v = g.valid(0)
+    r_host = g.np_zeros()
+    r_host[v] = rng.standard_normal(r_host[v].shape)
+    r.copy_(torch.from_numpy(r_host))
+    out = []
+    cells = g.nx * g.ny * g.nz
+    stream = ctx.stream
+    for prec in (0, 1):
+        opts = gb.PoissonOptions.default(precision=prec)
+        ps = gb.PoissonSolver(ctx, g, case.z, case.J, bc, opts)
+        ps.set_coeffs(case.ax, case.ay, case.az)
+        y = torch.zeros_like(r)
+        kinds = [("apply", None)] if prec == 0 else []
+        kinds.append(("vcycle", None))
+        for kind, _ in kinds:
+            fn = (lambda: ps.apply(r, out=y)) if kind == "apply" else (lambda: ps.vcycle(r, out=y))
+            for _ in range(3):
+                fn()
+            ms = []
+            for _ in range(reps):
+                with torch.cuda.stream(stream):
+                    flush.zero_()
+                    e0 = torch.cuda.Event(enable_timing=True)
+                    e1 = torch.cuda.Event(enable_timing=True)
+                    e0.record(stream)
+                    fn()
+                    e1.record(stream)
+                torch.cuda.synchronize()
+                ms.append(e0.elapsed_time(e1))
+            t = statistics.median(ms)
+            if kind == "apply":
+                words, what = APPLY_WORDS * cells, ("k_apply: the terrain operator on the fine level "
+                                                   f"({g.nx}x{g.ny}x{g.nz}), FP64; 7 words per cell")
+                word = 8
+            else:
+                words, nlev = vcycle_words(g.nx, g.ny, g.nz, opts)
+                word = 8 if prec == 0 else 4
+                what = (f"one multigrid V-cycle ({nlev} levels, nu1 = nu2 = {opts.nu1}, {opts.nu_coarse} coarsest "
+                        f"relaxations), {'FP64' if prec == 0 else 'FP32'}; 8 words per cell and relaxation, 7 per "
+                        "residual, 1.25 restriction, 2.25 prolongation")
+            nbytes = words * word
+            achieved = nbytes / (t / 1e3) / 1e9
+            out.append({"kernel": what, "bound": "hbm", "bytes_per_launch": nbytes, "launch_ms": t,
+                        "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak})
+        ps.close()
+    return out
+
+
+# ------------------------------------------------------------ steady solves ---
+
+def steady_solves(max_iterations=3000):
+    """Config 1 from the mass-consistent initial field to the steady
+    criterion (the C++ driver), in plain FP64 and with FP32 inner solves:
+    iterations, device seconds, steady solves/s, and the difference of the
+    two steady states per field (max |mixed - FP64| / max |FP64|)."""
+    import torch
+
+    import ablsteadyrans_b200 as gb
+    from ablsteadyrans_b200 import workloads
+    from ablsteadyrans_b200.sequencing import _finest
+    from ablsteadyrans_b200.simplec import NativeDriver, run_drivers
+    res = {}
+    fields = {}
+    for prec in (0, 1):
+        inst = workloads.config1(precision=prec)
+        ctx = gb.Context()
+        case, stage = _finest(ctx, inst)
+        stage.initialize()
+        stage.fill_ghosts()
+        d = NativeDriver(stage)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(ctx.stream)
+        (verdict, n), = run_drivers([d], max_iterations, 1)
+        e1.record(ctx.stream)
+        torch.cuda.synchronize()
+        sec = e0.elapsed_time(e1) / 1e3
+        key = "fp64" if prec == 0 else "fp32_inner"
+        res[key] = {"verdict": verdict, "iterations": n, "seconds": sec, "solves_per_s": 1.0 / sec,
+                    "cell_updates_per_s": inst.cells * n / sec}
+        g = inst.grid
+        fields[key] = {f: (case.q[f].cpu().numpy(), loc) for f, loc in zip(("u", "v", "w", "p", "theta", "tke"),
+                                                                           (1, 2, 4, 0, 0, 0))}
+        fields[key]["grid"] = g
+        d.close()
+        stage.close()
+        ctx.close()
+    g = fields["fp64"]["grid"]
+    err = {}
+    for f in ("u", "v", "w", "p", "theta", "tke"):
+        a, loc = fields["fp32_inner"][f]
+        b, _ = fields["fp64"][f]
+        vv = g.valid(loc)
+        scale = float(np.abs(b[vv]).max())
+        err[f] = float(np.abs(a[vv] - b[vv]).max()) / (scale if scale > 0 else 1.0)
+    res["fp32_inner_vs_fp64_rel_err"] = err
+    res["speedup_fp32_inner"] = res["fp64"]["seconds"] / res["fp32_inner"]["seconds"]
+    res["workload"] = ("config 1 (128x128x64 hill) from the mass-consistent initial field to the steady criterion "
+                       "(4 orders, monitors settled), the C++ driver; device time")
+    return res
+
+
+def batched_leg(count=16, iterations=10, warmup=2):
+    """A sample of the batched configuration (its first `count` uneven tiles
+    of the 48, drawn as config 3): every tile's outer iterations with FP32
+    inner solves on concurrent streams (the batched form), against the same
+    tiles in plain FP64 one by one; cell-updates/s of each (device time)."""
+    import torch
+
+    from ablsteadyrans_b200.batch import Batch, config3
+    out = {}
+    insts = config3(count, 0, precision=1)
+    cells = sum(i.cells for i in insts)
+    batch = Batch(insts)
+    batch.run_native(warmup, threads=0)
+    ms, _ = batch.run_native(iterations, threads=0)
+    out["batched_fp32_inner"] = cells * iterations / (ms / 1e3)
+    ms1, _ = batch.run_native(iterations, threads=1)
+    out["one_by_one_fp32_inner"] = cells * iterations / (ms1 / 1e3)
+    batch.close()
+    del batch
+    torch.cuda.empty_cache()
+    total = 0.0
+    for inst in config3(count, 0, precision=0):
+        b = Batch([inst])
+        b.run_native(warmup, threads=1)
+        t, _ = b.run_native(iterations, threads=1)
+        total += t
+        b.close()
+        torch.cuda.empty_cache()
+    out["one_by_one_fp64"] = cells * iterations / (total / 1e3)
+    out["speedup_batched_fp32_inner_vs_fp64_one_by_one"] = out["batched_fp32_inner"] / out["one_by_one_fp64"]
+    out["workload"] = (f"the first {count} of config 3's 48 uneven tiles (n in 64..192, nz in 48..96; {cells} cells), "
+                       f"{iterations} outer iterations each after {warmup}; cell-updates/s")
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -250,6 +460,8 @@ def main():
     ap.add_argument("--precision", type=int, default=0, choices=[0, 1])
     ap.add_argument("--sweeps", type=int, default=4)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
+    ap.add_argument("--no-steady", action="store_true", help="skip the steady-solve leg")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched leg")
     ap.add_argument("--tune", action="append", default=[], metavar="KEY=VALUE",
                     help="a context tuning knob (GB_TUNE_*, by number or name without the prefix), repeatable")
     args = ap.parse_args()
@@ -368,58 +580,82 @@ def main():
                  "MOST surface layer)" if wl.inst.physics.closure else
                  "synthetic (config 1 generated in-project: Gaussian hill, log-law inflow; frozen mixing-length "
                  "diffusivities, no-slip ground)"),
-        "config": {"workload": wl.name, "cells": wl.cells, "l2": "flushed between timed steps (256 MB write)",
-                   "parallelism": f"independent instances x{world}", "driver_status_last": statuses[-1],
-                   **({"tune": args.tune} if args.tune else {})},
+        "config": bench_config(wl),
+        "parallelism": f"independent instances x{world}",
+        "driver_status_last": statuses[-1],
         "e2e": {"value": e2e_value, "unit": "cell-updates/s", "h2d_bytes_per_step": wl.h2d,
                 "d2h_bytes_per_step": wl.d2h},
         "gpu_launches": launches,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None, "traffic": traffic,
-                     "kernel": "zline_fact_multi_kernel (z-line Thomas sweeps: u, v, w in one launch, theta and k in one)",
+                     "kernel": "zline_seg_multi_kernel (segmented z-line Thomas sweeps: u, v, w in one launch, "
+                               "theta and k in one)",
                      "peak_kind": peak_kind,
                      "bytes_per_launch": line_bytes / max(sweep_n, 1), "launch_ms": sweep_ms / max(sweep_n, 1)},
         "breakdown": families,
         "clocks": clocks,
     }
+    if args.tune:
+        line["tune"] = args.tune
+    if world == 1:
+        line["rooflines"] = poisson_rooflines(ctx, wl, flush, peak)
+    wl.stage.close()
+    ctx.close()
+    del flush
+    torch.cuda.empty_cache()
+    if world == 1 and not args.no_steady:
+        line["steady"] = steady_solves()
+    if world == 1 and not args.no_batch:
+        line["batched"] = batched_leg()
     if rank == 0 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(wl)
     if rank == 0:
         print(json.dumps(line))
-    wl.stage.close()
-    ctx.close()
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
     return 0
 
 
-def cpu_baseline(wl):
-    """The oracle on a bounded sample of the same workload: one or two
-    iterations of config 1 on every host thread."""
+def cpu_baseline(wl, budget=30.0):
+    """The FP64 C restatement built for speed on this host, on a bounded
+    sample of the same workload: config 1's iterations on every host thread
+    (at least one, until `budget` seconds), and one iteration on one thread."""
     import oracle
+    path = oracle.use_fast_build()
     threads = os.cpu_count() or 1
     oracle.set_threads(threads)
     wl.cpu_setup()
+    wl.cpu_step()   # untimed: first touch of the arrays
     t0 = time.perf_counter()
     n = 0
     while True:
         wl.cpu_step()
         n += 1
-        if time.perf_counter() - t0 > 20.0 or n >= 2:
+        if time.perf_counter() - t0 > budget or n >= 3:
             break
     dt = time.perf_counter() - t0
+    oracle.set_threads(1)
+    t1 = time.perf_counter()
+    wl.cpu_step()
+    dt1 = time.perf_counter() - t1
+    oracle.set_threads(threads)
     return {"value": wl.cells * n / dt, "unit": "cell-updates/s", "cores": threads, "kind": "port",
-            "sample": f"{n} SIMPLEC iteration(s) of config 1 ({dt:.1f} s), oracle = FP64 C restatement"}
+            "sample": f"{n} SIMPLEC iteration(s) of config 1 ({dt:.1f} s) on {threads} threads, after one untimed",
+            "single_thread": {"value": wl.cells / dt1, "unit": "cell-updates/s", "cores": 1,
+                              "sample": f"1 SIMPLEC iteration of config 1 ({dt1:.1f} s) on one thread"},
+            "cpu_model": oracle.cpu_model(), "nproc": threads,
+            "build": "the oracle's C sources, gcc -O3 -march=native -fopenmp (" + os.path.basename(path) + ")"}
 
 
 def run_reference(args):
     wl = SimplecWorkload(precision=0, sweeps=args.sweeps)
     import oracle
+    oracle.use_fast_build()
     threads = os.cpu_count() or 1
     oracle.set_threads(threads)
     wl.cpu_setup()
-    for _ in range(max(0, min(args.warmup, 3))):   # untimed warm-up iterations
+    for _ in range(max(0, args.warmup)):   # untimed warm-up iterations
         wl.cpu_step()
     t0 = time.perf_counter()
     n = 0
@@ -434,13 +670,16 @@ def run_reference(args):
     line = {
         "impl": "reference",
         "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": 0,
-        "steps": n, "warmup": max(0, min(args.warmup, 3)), "ms_per_step": dt / n * 1e3, "higher_is_better": True,
+        "steps": n, "warmup": max(0, args.warmup), "ms_per_step": dt / n * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic (config 1 generated in-project)",
-        "config": {"workload": wl.name, "cells": wl.cells},
+        "data": ("synthetic (config 1 generated in-project: Gaussian hill, log-law inflow; k-L closure, neutral "
+                 "MOST surface layer)"),
+        "config": bench_config(wl),
+        "parallelism": f"host threads x{threads}",
         "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": threads, "kind": "port",
-                         "sample": f"{n} SIMPLEC iteration(s) of config 1 ({dt:.1f} s); the oracle, the FP64 C "
-                                   "restatement of the reference (the reference needs AMReX)"},
+                         "sample": f"{n} SIMPLEC iteration(s) of config 1 ({dt:.1f} s); the FP64 C restatement of "
+                                   "the reference (the reference needs AMReX), gcc -O3 -march=native",
+                         "cpu_model": oracle.cpu_model(), "nproc": threads},
         "e2e": {"value": value, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))

@@ -37,6 +37,40 @@ def lib():
     return _lib
 
 
+def cpu_model():
+    """The host CPU's model name (/proc/cpuinfo), or the machine type."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+    return platform.machine()
+
+
+def use_fast_build():
+    """Switch this process's oracle calls to the speed build of the same
+    sources (-O3 -march=native, contraction allowed; results differ from the
+    parity build by rounding), compiled on this host into a directory named
+    by the CPU model. Only the timed CPU baseline uses it. Returns the
+    library's path."""
+    import hashlib
+    global _lib
+    d = os.path.join(HERE, "_fast", hashlib.sha1(cpu_model().encode()).hexdigest()[:12])
+    r = subprocess.run(["make", "-C", HERE, "fast", f"FAST_DIR={d}"], stdout=subprocess.PIPE, stderr=subprocess.STDOUT)
+    if r.returncode != 0:
+        raise RuntimeError("oracle speed build failed:\n" + r.stdout.decode(errors="replace"))
+    path = os.path.join(d, "liboracle_fast.so")
+    L = ctypes.CDLL(path)
+    _declare(L)
+    _declare_simplec(L)
+    L._og_simplec = True
+    _lib = L
+    return path
+
+
 def _declare(L):
     from ablsteadyrans_b200.grid import GbGrid
     G = ctypes.POINTER(GbGrid)
