@@ -988,6 +988,10 @@ void PoissonLevels<T>::release()
 
 gb_poisson::~gb_poisson()
 {
+    for (int n = 0; n < 2; ++n) {
+        if (vc_exec[n] != nullptr) { cudaGraphExecDestroy(vc_exec[n]); }
+    }
+    if (capture_stream != nullptr) { cudaStreamDestroy(capture_stream); }
     for (void* p : owned) { cudaFree(p); }
     dl.release();
     fl.release();
@@ -1160,6 +1164,72 @@ void vcycle(gb_poisson* P, PoissonLevels<T>& L, int l)
     for (int s = 0; s < P->opt.nu2; ++s) { mg_smooth(P, L, l); }
 }
 
+//! A key of the tuning knobs that choose the V-cycle's kernels.
+uint64_t tune_key(const gb_ctx* ctx)
+{
+    uint64_t k = 1469598103934665603ull;
+    for (int n = 0; n < GB_N_TUNE; ++n) { k = (k ^ static_cast<uint64_t>(static_cast<uint32_t>(ctx->tune[n]))) * 1099511628211ull; }
+    return k;
+}
+
+//! One V-cycle of the level hierarchy L from L.bv[0] into L.x[0]. The V-cycle
+//! has no host synchronisation and its arguments are fixed per solver, so
+//! from its second call on it runs as a CUDA graph, captured once on the
+//! solver's own stream and launched on the context's: one launch in place of
+//! the ~8 per level (the coarse levels' kernels last a few microseconds, so
+//! launch overhead, not their work, set their cost). Profiling (per-family
+//! events) and GB_TUNE_GRAPHS = 1 run it eagerly; the kernels and their
+//! order are the same either way.
+template <typename T>
+void run_vcycle(gb_poisson* P, PoissonLevels<T>& L, int ti)
+{
+    gb_ctx* ctx = P->ctx;
+    const bool graph = ctx->tune[GB_TUNE_GRAPHS] != 1 && !ctx->profiling;
+    if (!graph || P->vc_calls[ti]++ == 0) {
+        vcycle(P, L, 0);
+        return;
+    }
+    const uint64_t key = tune_key(ctx);
+    if (P->vc_exec[ti] != nullptr && P->vc_tune_key[ti] != key) {
+        cudaGraphExecDestroy(P->vc_exec[ti]);
+        P->vc_exec[ti] = nullptr;
+    }
+    if (P->vc_exec[ti] == nullptr) {
+        if (P->capture_stream == nullptr
+            && cudaStreamCreateWithFlags(&P->capture_stream, cudaStreamNonBlocking) != cudaSuccess) {
+            cudaGetLastError();
+            P->capture_stream = nullptr;
+            vcycle(P, L, 0);
+            return;
+        }
+        // the capture stream starts after the work queued so far on the context's
+        cudaStream_t own = ctx->stream;
+        const int64_t launches0 = ctx->launches;
+        cudaGraph_t g = nullptr;
+        ctx->stream = P->capture_stream;
+        bool ok = cudaStreamBeginCapture(P->capture_stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+        if (ok) {
+            vcycle(P, L, 0);
+            ok = cudaStreamEndCapture(P->capture_stream, &g) == cudaSuccess && g != nullptr;
+        }
+        ctx->stream = own;
+        const int64_t n = ctx->launches - launches0;
+        ctx->launches = launches0;
+        if (ok) { ok = cudaGraphInstantiate(&P->vc_exec[ti], g, 0) == cudaSuccess; }
+        if (g != nullptr) { cudaGraphDestroy(g); }
+        if (!ok) {
+            cudaGetLastError();
+            P->vc_exec[ti] = nullptr;
+            vcycle(P, L, 0);
+            return;
+        }
+        P->vc_launches[ti] = n;
+        P->vc_tune_key[ti] = key;
+    }
+    cudaGraphLaunch(P->vc_exec[ti], ctx->stream);
+    ctx->launches += P->vc_launches[ti];
+}
+
 //! e = one V-cycle for A e = r (FP64 vectors at the fine level).
 void precondition(gb_poisson* P, const double* r, double* e)
 {
@@ -1171,7 +1241,7 @@ void precondition(gb_poisson* P, const double* r, double* e)
         k_copy_valid<float, double><<<nblocks(ncell), kBlock, 0, ctx->stream>>>(g, L.bv[0], r);
         cudaMemsetAsync(L.x[0], 0, sizeof(float) * volume(g), ctx->stream);
         ctx->launches += 1;
-        vcycle(P, L, 0);
+        run_vcycle(P, L, 1);
         cudaMemsetAsync(e, 0, sizeof(double) * volume(g), ctx->stream);
         k_copy_valid<double, float><<<nblocks(ncell), kBlock, 0, ctx->stream>>>(g, e, L.x[0]);
         ctx->launches += 1;
@@ -1179,7 +1249,7 @@ void precondition(gb_poisson* P, const double* r, double* e)
         auto& L = P->dl;
         cudaMemcpyAsync(L.bv[0], r, sizeof(double) * volume(g), cudaMemcpyDeviceToDevice, ctx->stream);
         cudaMemsetAsync(L.x[0], 0, sizeof(double) * volume(g), ctx->stream);
-        vcycle(P, L, 0);
+        run_vcycle(P, L, 0);
         cudaMemcpyAsync(e, L.x[0], sizeof(double) * volume(g), cudaMemcpyDeviceToDevice, ctx->stream);
     }
 }

@@ -67,6 +67,14 @@ struct gb_poisson {
     double* d_coef{nullptr};
     double* h_dots{nullptr};
     double J_sum{0};
+    // The V-cycle as a CUDA graph per precision (0 FP64, 1 FP32): captured on
+    // the solver's own stream on its second call (the first runs eagerly) and
+    // launched on the context's stream; rebuilt when the tuning knobs change.
+    cudaStream_t capture_stream{nullptr};
+    cudaGraphExec_t vc_exec[2]{nullptr, nullptr};
+    int64_t vc_launches[2]{0, 0};
+    int vc_calls[2]{0, 0};
+    uint64_t vc_tune_key[2]{0, 0};
     std::vector<void*> owned;
     ~gb_poisson();
 };
