@@ -298,6 +298,17 @@ struct gb_simplec {
     double jmin{0};
     std::vector<void*> owned;
     unsigned long long* h_words{nullptr};
+    // The iteration's two launch sequences without a host synchronisation
+    // (before and after the Krylov solve of the pressure correction) as CUDA
+    // graphs: captured on the stage's own stream on an iteration after the
+    // first, launched on the context's stream, rebuilt when what their kernels'
+    // arguments depend on changes (the state and dtau pointers, the nu_t
+    // history's presence, the tuning knobs).
+    cudaStream_t capture_stream{nullptr};
+    cudaGraphExec_t seg_exec[2]{nullptr, nullptr};
+    int64_t seg_launches[2]{0, 0};
+    uint64_t seg_key[2]{0, 0};
+    int iterations{0};
     ~gb_simplec();
 };
 
@@ -1574,7 +1585,9 @@ gb_status momentum_predictor(gb_simplec* S, const gb_state& q, double** R)
     return check_cuda("momentum_predictor");
 }
 
-gb_status pressure_correction(gb_simplec* S, const gb_state& q, gb_iter_info* info)
+//! pressure_correction's first part: beta = 1/d and the keep masks, div u*,
+//! the monitors, the solver's coefficients (no host synchronisation).
+gb_status pressure_prelude(gb_simplec* S, const gb_state& q)
 {
     gb_ctx* ctx = S->ctx;
     const gb_grid g = S->g;
@@ -1595,10 +1608,18 @@ gb_status pressure_correction(gb_simplec* S, const gb_state& q, gb_iter_info* in
     dmax(S, valid_box(g, XF), q.u, nullptr, W_SPEED_U);
     dmax(S, valid_box(g, YF), q.v, nullptr, W_SPEED_V);
     dmax(S, valid_box(g, ZF), q.w, nullptr, W_SPEED_W);
-    gb_status st = poisson_set_coeffs(S->poisson, S->mesh.ax, S->mesh.ay, S->mesh.az, w.beta[0], w.beta[1], w.beta[2]);
-    if (st != GB_OK) { return st; }
+    return poisson_set_coeffs(S->poisson, S->mesh.ax, S->mesh.ay, S->mesh.az, w.beta[0], w.beta[1], w.beta[2]);
+}
+
+//! pressure_correction's Krylov solve (host-synchronising) and the check of
+//! the singular case's removed mean.
+gb_status pressure_solve(gb_simplec* S, gb_iter_info* info)
+{
+    gb_ctx* ctx = S->ctx;
+    const gb_grid g = S->g;
+    SimplecWork& w = S->w;
     gb_poisson_result pr{};
-    st = poisson_solve(S->poisson, w.rhs, w.phi, &pr);
+    gb_status st = poisson_solve(S->poisson, w.rhs, w.phi, &pr);
     if (st != GB_OK) { return st; }
     info->poisson_iterations = pr.iterations;
     info->poisson_removed_mean = pr.removed_mean;
@@ -1614,6 +1635,17 @@ gb_status pressure_correction(gb_simplec* S, const gb_state& q, gb_iter_info* in
             return GB_BAD_ARG;
         }
     }
+    return GB_OK;
+}
+
+//! pressure_correction's last part: the fluxes, p, u, v, Omega and w, the
+//! divergence after (no host synchronisation).
+gb_status pressure_finish(gb_simplec* S, const gb_state& q)
+{
+    gb_ctx* ctx = S->ctx;
+    const gb_grid g = S->g;
+    SimplecWork& w = S->w;
+    gb_status st;
     double* F[3] = {w.G[0], w.G[1], w.G[2]};
     if ((st = poisson_fluxes(S->poisson, w.phi, w.beta[0], w.beta[1], w.beta[2], F[0], F[1], F[2])) != GB_OK) { return st; }
     const double alpha = S->opt.alpha_p;
@@ -1665,6 +1697,78 @@ gb_status pressure_correction(gb_simplec* S, const gb_state& q, gb_iter_info* in
     velocity_divergence(S, q.u, q.v, q.w, w.rhs);
     dmax(S, valid_box(g, CC), w.rhs, nullptr, W_DIV_AFTER);
     return check_cuda("pressure_correction");
+}
+
+//! Simplec.cpp:134-220 pressure_correction on q (its ghosts filled).
+gb_status pressure_correction(gb_simplec* S, const gb_state& q, gb_iter_info* info)
+{
+    gb_status st = pressure_prelude(S, q);
+    if (st == GB_OK) { st = pressure_solve(S, info); }
+    if (st == GB_OK) { st = pressure_finish(S, q); }
+    return st;
+}
+
+//! A key of what a captured iteration segment's kernel arguments depend on.
+uint64_t segment_key(const gb_simplec* S, const gb_state& q, const double* dtau)
+{
+    uint64_t k = 1469598103934665603ull;
+    auto mix = [&](uint64_t v) { k = (k ^ v) * 1099511628211ull; };
+    const double* ptrs[8] = {q.u, q.v, q.w, q.p, q.theta, q.tke, q.z_nd, dtau};
+    for (const double* p : ptrs) { mix(reinterpret_cast<uintptr_t>(p)); }
+    mix(S->has_hist ? 1 : 0);
+    for (int n = 0; n < GB_N_TUNE; ++n) { mix(static_cast<uint32_t>(S->ctx->tune[n])); }
+    return k;
+}
+
+//! body() (launches on the context's stream, no host synchronisation) run
+//! eagerly or as the stage's graph `id`: eagerly on the stage's first
+//! iteration (it sizes the scratch and sets the kernels' attributes), while
+//! profiling and with GB_TUNE_GRAPHS = 1; else the graph, captured on the
+//! stage's stream when its key changed, launched on the context's stream.
+//! The kernels and their order are the same either way.
+template <typename F>
+gb_status run_segment(gb_simplec* S, int id, uint64_t key, F&& body)
+{
+    gb_ctx* ctx = S->ctx;
+    if (ctx->tune[GB_TUNE_GRAPHS] == 1 || ctx->profiling || S->iterations == 0) { return body(); }
+    if (S->seg_exec[id] != nullptr && S->seg_key[id] != key) {
+        cudaGraphExecDestroy(S->seg_exec[id]);
+        S->seg_exec[id] = nullptr;
+    }
+    if (S->seg_exec[id] == nullptr) {
+        if (S->capture_stream == nullptr
+            && cudaStreamCreateWithFlags(&S->capture_stream, cudaStreamNonBlocking) != cudaSuccess) {
+            cudaGetLastError();
+            S->capture_stream = nullptr;
+            return body();
+        }
+        cudaStream_t own = ctx->stream;
+        const int64_t launches0 = ctx->launches;
+        cudaGraph_t graph = nullptr;
+        gb_status st = GB_OK;
+        ctx->stream = S->capture_stream;
+        bool ok = cudaStreamBeginCapture(S->capture_stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+        if (ok) {
+            st = body();
+            ok = cudaStreamEndCapture(S->capture_stream, &graph) == cudaSuccess && graph != nullptr && st == GB_OK;
+        }
+        ctx->stream = own;
+        const int64_t n = ctx->launches - launches0;
+        ctx->launches = launches0;
+        if (ok) { ok = cudaGraphInstantiate(&S->seg_exec[id], graph, 0) == cudaSuccess; }
+        if (graph != nullptr) { cudaGraphDestroy(graph); }
+        if (!ok) {
+            cudaGetLastError();
+            S->seg_exec[id] = nullptr;
+            if (st != GB_OK) { return st; }
+            return body();
+        }
+        S->seg_launches[id] = n;
+        S->seg_key[id] = key;
+    }
+    cudaGraphLaunch(S->seg_exec[id], ctx->stream);
+    ctx->launches += S->seg_launches[id];
+    return GB_OK;
 }
 
 //! Simplec.cpp:222-281 scalar_sweep for theta and for k: each system's rows
@@ -1727,6 +1831,9 @@ gb_status simplec_iterate(gb_simplec* S, const gb_state& q, const double* dtau, 
     const gb_grid g = S->g;
     SimplecWork& w = S->w;
     *info = gb_iter_info{};
+    const uint64_t key = segment_key(S, q, dtau);
+    // 1.-3. up to the Krylov solve of the pressure correction
+    gb_status st = run_segment(S, 0, key, [&]() -> gb_status {
     cudaMemsetAsync(dword(ctx, 0), 0, sizeof(unsigned long long) * W_COUNT, ctx->stream);
     cudaMemsetAsync(dword(ctx, W_SURFACE_BAD), 0, sizeof(unsigned long long), ctx->stream);
     // 1. ghosts and the wall state at q; 2. the residual (the closure at q)
@@ -1746,10 +1853,17 @@ gb_status simplec_iterate(gb_simplec* S, const gb_state& q, const double* dtau, 
     dmax(S, valid_box(g, ZF), q.w, nullptr, W_MON_W);
     transport_fluxes(S, q, w.F[0], w.F[1], w.F[2]);
     face_dtau(S, dtau, w.dtf);
-    gb_status st = momentum_predictor(S, q, w.R);
-    if (st != GB_OK) { return st; }
+    gb_status s1 = momentum_predictor(S, q, w.R);
+    if (s1 != GB_OK) { return s1; }
     fill_ghosts_into(S, q, S->sst);
-    if ((st = pressure_correction(S, q, info)) != GB_OK) { return st; }
+    return pressure_prelude(S, q);
+    });
+    if (st != GB_OK) { return st; }
+    if ((st = pressure_solve(S, info)) != GB_OK) { return st; }
+    // 4. the rest of the correction, 5. theta and k, 6. the nu_t history
+    st = run_segment(S, 1, key, [&]() -> gb_status {
+    gb_status s2 = pressure_finish(S, q);
+    if (s2 != GB_OK) { return s2; }
     convection<CC>(S, q.theta, w.F, S->ph.limiter, S->ph.smooth_eps_theta, false, w.conv0);
     fill_ghosts_into(S, q, S->sst);
     transport_fluxes(S, q, w.F[0], w.F[1], w.F[2]);
@@ -1763,12 +1877,16 @@ gb_status simplec_iterate(gb_simplec* S, const gb_state& q, const double* dtau, 
             Rt[o] += c1[o] - c0[o];
         });
     }
-    if ((st = scalar_sweeps(S, q, dtau)) != GB_OK) { return st; }
+    if ((s2 = scalar_sweeps(S, q, dtau)) != GB_OK) { return s2; }
     // 6. the nu_t history (Closure::accept): the fields of this iteration's residual
     if (S->ph.closure) {
         cudaMemcpyAsync(S->nut_hist, S->cf[kClosureNut], sizeof(double) * volume(g), cudaMemcpyDeviceToDevice, ctx->stream);
-        S->has_hist = true;
     }
+    return GB_OK;
+    });
+    if (st != GB_OK) { return st; }
+    if (S->ph.closure) { S->has_hist = true; }
+    ++S->iterations;
     // read every result of the iteration at once
     unsigned long long words[W_COUNT];
     if ((st = read_words(ctx, 0, W_COUNT, words)) != GB_OK) { return st; }
@@ -2601,6 +2719,10 @@ void simplec_delete(gb_simplec* S)
 {
     if (S == nullptr) { return; }
     cudaStreamSynchronize(S->ctx->stream);
+    for (int n = 0; n < 2; ++n) {
+        if (S->seg_exec[n] != nullptr) { cudaGraphExecDestroy(S->seg_exec[n]); }
+    }
+    if (S->capture_stream != nullptr) { cudaStreamDestroy(S->capture_stream); }
     if (S->h_words) { cudaFreeHost(S->h_words); }
     delete S;
 }

@@ -280,3 +280,37 @@ def test_gpu_initializer_obrien_matches_oracle(ctx):
         scale = max(np.abs(ref).max(), 1e-300)
         assert np.abs(got - ref).max() <= 1e-9 * scale, (f, np.abs(got - ref).max() / scale)
     st.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", [0, 1])
+def test_gpu_iteration_graphs_equal_eager_launches(ctx, precision):
+    """From its second iteration a stage runs the launch sequences before and
+    after the Krylov solve as CUDA graphs (and the V-cycle as one): the same
+    kernels in the same order, so five iterations with graphs give the eager
+    iterations' fields bit for bit (GB_TUNE_GRAPHS = 1 launches every kernel
+    alone); the nu_t history's appearance after the first iteration and a
+    new dtau array rebuild the graphs."""
+    import ablsteadyrans_b200 as gb
+    from ablsteadyrans_b200 import workloads
+    from ablsteadyrans_b200.simplec import DeviceCase, SimplecStage
+    out = []
+    for graphs in (1, 0):
+        ctx.tune(gb.TUNE_GRAPHS, graphs)
+        inst = workloads.tile(40, 24, 3, precision=precision)
+        inst.physics.coriolis, inst.physics.latitude, inst.physics.rotation_period = 1, 45.0, 86164.0
+        inst.physics.turb_nut_relax = 0.7
+        J, ax, ay, az, _ = oracle.metrics(inst.grid, inst.z)
+        dc = DeviceCase(inst.grid, inst.z, J, ax, ay, az, inst.nu, inst.gamma_theta, inst.gamma_tke, inst.q, inst.z0map)
+        st = SimplecStage(ctx, dc, inst.bc, inst.physics, inst.options)
+        st.fill_ghosts()
+        infos = []
+        for it in range(5):
+            dt = st.local_dtau(2.0)          # a new dtau array each iteration
+            infos.append(list(st.iterate(dt).residual_norms))
+        out.append(({f: dc.host(f) for f in FIELDS}, infos))
+        st.close()
+    ctx.tune(gb.TUNE_GRAPHS, 0)
+    for f in FIELDS:
+        assert np.array_equal(out[0][0][f], out[1][0][f]), f
+    assert out[0][1] == out[1][1]
