@@ -1758,9 +1758,9 @@ gb_status run_segment(gb_simplec* S, int id, uint64_t key, F&& body)
         if (ok) { ok = cudaGraphInstantiate(&S->seg_exec[id], graph, 0) == cudaSuccess; }
         if (graph != nullptr) { cudaGraphDestroy(graph); }
         if (!ok) {
+            // a capture that failed recorded nothing that ran: run the segment eagerly
             cudaGetLastError();
             S->seg_exec[id] = nullptr;
-            if (st != GB_OK) { return st; }
             return body();
         }
         S->seg_launches[id] = n;

@@ -235,3 +235,49 @@ def test_gpu_config1_full_size_vcycle_matches_oracle(ctx, precision):
     err = float(np.abs(e[v] - e_ref[v]).max()) / float(np.abs(e_ref[v]).max())
     print(f"config 1 V-cycle, precision {precision}: {err:.3e}")
     assert err <= (1e-12 if precision == 0 else 1e-5)
+
+
+CONVERGED_CASE = dict(nx=8, ny=8, nz=48)
+
+
+@pytest.mark.gpu
+def test_gpu_converged_states_match_oracle(ctx):
+    """The flat neutral ABL of config 0 on an 8 x 8 x 48 grid run to the
+    steady criterion on the GPU in plain FP64 and with FP32 inner solves
+    (mixed precision), and the oracle's FP64 iterations at the FP64 run's
+    CFL per iteration, as many: the converged U, V, W, p, k, theta and L of
+    the plain FP64 GPU run agree with the oracle's within 1e-6 relative;
+    the mixed-precision run's converged velocity within 1e-4 of the
+    oracle's (the per-field table is printed)."""
+    from ablsteadyrans_b200.driver import Driver
+    runs = {}
+    for prec in (0, 1):
+        inst = workloads.config0(precision=prec, **CONVERGED_CASE)
+        oc = oracle_case(inst)
+        dc, st = gpu_stage(ctx, oc, inst)
+        try:
+            drv = Driver(st)
+            status, n = drv.run(6000)
+            assert status == "steady", (prec, status, n)
+            runs[prec] = {"fields": {f: dc.host(f) for f in FIELDS}, "cfls": [h[0] for h in drv.history],
+                          "L": gpu_closure_length(st), "iterations": n}
+        finally:
+            st.close()
+    inst = workloads.config0(precision=0, **CONVERGED_CASE)
+    oc = oracle_case(inst)
+    oracle.set_threads(oracle.max_threads())
+    run_oracle(oc, inst, runs[0]["cfls"])
+    g = inst.grid
+    v = g.valid(0)
+    Lo = closure_length(oc, inst)
+    table = {}
+    for prec, name in ((0, "fp64"), (1, "fp32_inner")):
+        err = field_errors(g, runs[prec]["fields"], oc.q)
+        err["L"] = float(np.abs(runs[prec]["L"][v] - Lo[v]).max() / np.abs(Lo[v]).max())
+        table[name] = err
+    print("converged (config 0 at 8x8x48), GPU vs oracle, iterations", runs[0]["iterations"], runs[1]["iterations"],
+          table)
+    for f, e in table["fp64"].items():
+        assert e <= 1e-6, ("fp64", f, e)
+    for f in ("u", "v", "w"):
+        assert table["fp32_inner"][f] <= 1e-4, ("fp32_inner", f, table["fp32_inner"][f])
