@@ -996,6 +996,7 @@ gb_poisson::~gb_poisson()
     dl.release();
     fl.release();
     if (h_dots) { cudaFreeHost(h_dots); }
+    if (h_step) { cudaFreeHost(h_step); }
 }
 
 namespace gb {
@@ -1271,6 +1272,32 @@ void apply_fine(gb_poisson* P, const double* x, const double* rhs, double* y)
     }
 }
 
+//! Dots <w, V_q> for q < nq into out[0, nq) on the device (deterministic
+//! two-stage block sums; no host synchronisation).
+void multidot_device(gb_poisson* P, const double* w, const double* V, int64_t vstride, int nq, double* out)
+{
+    gb_ctx* ctx = P->ctx;
+    const int nblk = P->dot_blocks;
+    Span span(ctx, GB_KERNEL_VECTOR);
+    k_multidot<<<dim3(nblk, nq), kBlock, 0, ctx->stream>>>(P->g, w, V, vstride, nq, P->d_partial);
+    k_reduce_partials<<<nq, 256, 0, ctx->stream>>>(P->d_partial, nblk, nq, out);
+    ctx->launches += 2;
+}
+
+//! The next Arnoldi vector v = w / |w| (0 where |w| is not > 0), |w|^2 read
+//! from the device (the host's 1/sqrt in the same IEEE operations).
+__global__ void k_scale_by_norm(gb_grid g, const double* __restrict__ w, const double* __restrict__ n2,
+                                double* __restrict__ v)
+{
+    int i, j, k;
+    const int64_t n = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (!cell_of(g, n, i, j, k)) { return; }
+    const double hn = sqrt(*n2);
+    if (!(hn > 0)) { return; }
+    const int64_t o = at(g, i, j, k);
+    v[o] = (1.0 / hn) * w[o];
+}
+
 //! Dots <w, V_q> for q < nq (or <a, b> with V = b, nq = 1) into P->h_dots (host), deterministic.
 gb_status multidot(gb_poisson* P, const double* w, const double* V, int64_t vstride, int nq, double* host_out)
 {
@@ -1410,8 +1437,15 @@ gb_status poisson_build(gb_poisson* P)
     P->d_partial = dalloc<double>(ctx->stream, P->owned, static_cast<int64_t>(P->dot_blocks) * (m + 2));
     P->d_dots = dalloc<double>(ctx->stream, P->owned, m + 2);
     P->d_coef = dalloc<double>(ctx->stream, P->owned, m + 2);
+    P->d_step = dalloc<double>(ctx->stream, P->owned, 3 * (m + 2));
     if (!P->V || !P->Zv || !P->w || !P->t || !P->d_partial || !P->d_dots || !P->d_coef) {
         set_error("gust: PoissonSolver: cannot allocate the Krylov workspace");
+        return GB_OOM;
+    }
+    if (cudaMallocHost(&P->h_step, sizeof(double) * 3 * (m + 2)) != cudaSuccess) {
+        cudaGetLastError();
+        P->h_step = nullptr;
+        set_error("gust: PoissonSolver: out of pinned host memory");
         return GB_OOM;
     }
     if (cudaMallocHost(&P->h_dots, sizeof(double) * (m + 2)) != cudaSuccess) {
@@ -1584,7 +1618,7 @@ gb_status poisson_solve(gb_poisson* P, double* rhs, double* phi, gb_poisson_resu
     const double bnorm = std::sqrt(bn2);
     res->initial_residual = bnorm;
     const double tol = std::max(P->opt.reltol * bnorm, P->opt.abstol);
-    std::vector<double> H(static_cast<size_t>(m + 1) * m), cs(m), sn(m), s(m + 1), y(m), h(m + 1), h2(m + 1);
+    std::vector<double> H(static_cast<size_t>(m + 1) * m), cs(m), sn(m), s(m + 1), y(m), h(m + 1);
     int it = 0;
     bool converged = !(bnorm > tol);
     while (!converged && it < P->opt.max_iter) {
@@ -1613,24 +1647,29 @@ gb_status poisson_solve(gb_poisson* P, double* rhs, double* phi, gb_poisson_resu
             double* zj = P->Zv + vol * jj;
             precondition(P, vj, zj);
             apply_fine(P, zj, nullptr, P->w);
-            // classical Gram-Schmidt, twice (batched dots: one kernel, one sync per pass)
+            // classical Gram-Schmidt, twice, and the norm of what is left: the
+            // dots stay on the device (each projection reads its coefficients
+            // there) and come back to the host once per step, for the Givens
+            // rotations and the convergence test
             std::fill(h.begin(), h.end(), 0.0);
+            const int64_t st3 = m + 2;
             for (int pass = 0; pass < 2; ++pass) {
-                if ((st = multidot(P, P->w, P->V, vol, jj + 1, h2.data())) != GB_OK) { return st; }
-                cudaMemcpyAsync(P->d_coef, h2.data(), sizeof(double) * (jj + 1), cudaMemcpyHostToDevice, ctx->stream);
-                k_subtract_projection<<<nblocks(ncell), kBlock, 0, ctx->stream>>>(g, P->w, P->V, vol, jj + 1, P->d_coef);
+                double* dots = P->d_step + pass * st3;
+                multidot_device(P, P->w, P->V, vol, jj + 1, dots);
+                k_subtract_projection<<<nblocks(ncell), kBlock, 0, ctx->stream>>>(g, P->w, P->V, vol, jj + 1, dots);
                 ++ctx->launches;
-                for (int q = 0; q <= jj; ++q) { h[q] += h2[q]; }
             }
-            double hn2 = 0;
-            if ((st = multidot(P, P->w, P->w, 0, 1, &hn2)) != GB_OK) { return st; }
-            const double hn = std::sqrt(hn2);
+            multidot_device(P, P->w, P->w, 0, 1, P->d_step + 2 * st3);
             double* vn = P->V + vol * (jj + 1);
             cudaMemsetAsync(vn, 0, sizeof(double) * vol, ctx->stream);
-            if (hn > 0) {
-                k_axpby<<<nblocks(ncell), kBlock, 0, ctx->stream>>>(g, 1.0 / hn, P->w, 0.0, vn);
-                ++ctx->launches;
+            k_scale_by_norm<<<nblocks(ncell), kBlock, 0, ctx->stream>>>(g, P->w, P->d_step + 2 * st3, vn);
+            ++ctx->launches;
+            cudaMemcpyAsync(P->h_step, P->d_step, sizeof(double) * 3 * st3, cudaMemcpyDeviceToHost, ctx->stream);
+            if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) { return check_cuda("poisson dot"); }
+            for (int pass = 0; pass < 2; ++pass) {
+                for (int q = 0; q <= jj; ++q) { h[q] += P->h_step[pass * st3 + q]; }
             }
+            const double hn = std::sqrt(P->h_step[2 * st3]);
             for (int q = 0; q <= jj; ++q) { H[q * m + jj] = h[q]; }
             H[(jj + 1) * m + jj] = hn;
             for (int q = 0; q < jj; ++q) {

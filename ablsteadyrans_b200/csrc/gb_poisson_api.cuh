@@ -66,6 +66,10 @@ struct gb_poisson {
     double* d_dots{nullptr};
     double* d_coef{nullptr};
     double* h_dots{nullptr};
+    // one Arnoldi step's dots on the device and their one read-back:
+    // [0, m+2) the first Gram-Schmidt pass, [m+2, 2m+4) the second, [2m+4] |w|^2
+    double* d_step{nullptr};
+    double* h_step{nullptr};
     double J_sum{0};
     // The V-cycle as a CUDA graph per precision (0 FP64, 1 FP32): captured on
     // the solver's own stream on its second call (the first runs eagerly) and
