@@ -104,10 +104,19 @@ class Member:
 
 
 class Batch:
-    """Members stepped together (threads over members) or one by one."""
+    """Members stepped together (threads over members) or one by one. With
+    a tuner (autotune.Autotuner) each member's context takes the knob choice
+    of its shape (timed on the first member of each shape)."""
 
-    def __init__(self, instances, restart=8):
+    def __init__(self, instances, restart=8, tuner=None):
         self.members = [Member(inst, restart=restart) for inst in instances]
+        self.choices = {}
+        if tuner is not None:
+            from .autotune import shape_key
+            for m in self.members:
+                with __import__("torch").cuda.stream(m.stream):
+                    choice, _ = tuner.tune(m.stage)
+                self.choices[shape_key(m.inst.grid, m.inst.options, m.inst.physics)] = choice
 
     @property
     def cells(self):

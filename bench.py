@@ -424,10 +424,12 @@ def batched_leg(count=16, iterations=10, warmup=2):
     import torch
 
     from ablsteadyrans_b200.batch import Batch, config3
+    from ablsteadyrans_b200.autotune import Autotuner
     out = {}
     insts = config3(count, 0, precision=1)
     cells = sum(i.cells for i in insts)
-    batch = Batch(insts)
+    batch = Batch(insts, tuner=Autotuner(iterations=2))
+    out["autotuned"] = batch.choices
     batch.run_native(warmup, threads=0)
     ms, _ = batch.run_native(iterations, threads=0)
     out["batched_fp32_inner"] = cells * iterations / (ms / 1e3)
