@@ -146,6 +146,66 @@ class Server:
         return time.perf_counter() - t0
 
 
+def sequential_latencies(arrivals, services):
+    """FIFO one-at-a-time service of requests arriving at `arrivals` (sorted)
+    with service times `services`: each starts when it has arrived and the
+    one before it is done. Returns the latencies (done - arrival)."""
+    done = 0.0
+    out = []
+    for a, sv in zip(arrivals, services):
+        start = max(a, done)
+        done = start + sv
+        out.append(done - a)
+    return out
+
+
+def serve_vs_sequential(count=12, rate=2.0, seed=0, sizes=None, layers=None, max_iterations=1500, budget=150e9):
+    """The served form against the plain FP64 sequential path on the same
+    requests: (1) the server (continuous batching, FP32 inner solves),
+    latencies from arrival to completion; (2) the requests in plain FP64
+    served one at a time in arrival order: each one's service time measured
+    alone (the initializer, then the C++ driver to the criterion or the cap),
+    its latency from the FIFO queue over the same arrivals. Returns a dict of
+    p50/p99 latency and solves/s of each."""
+    import torch
+
+    from .batch import Member
+    from .simplec import run_drivers
+    model = calibrate_footprint()
+    served = requests_config4(count, rate, seed, precision=1, sizes=sizes, layers=layers)
+    srv = Server(budget, model, max_iterations=max_iterations)
+    wall = srv.run(served)
+    lat = np.array([r.latency for r in served])
+    seq = requests_config4(count, rate, seed, precision=0, sizes=sizes, layers=layers)
+    services = []
+    for req in seq:
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        m = Member(req.inst)
+        m.stage.initialize()
+        if req.kind == "rans":
+            (req.status, req.iterations), = run_drivers([m.native], max_iterations, 1)
+        m.stream.synchronize()
+        services.append(time.perf_counter() - t0)
+        m.close()
+        del m
+        torch.cuda.empty_cache()
+    slat = np.array(sequential_latencies([r.arrival for r in seq], services))
+    makespan = max(r.arrival + l for r, l in zip(seq, slat))
+    return {
+        "requests": count, "rate_per_s": rate, "full_solves": sum(1 for r in served if r.kind == "rans"),
+        "served_fp32_inner": {"p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+                              "solves_per_s": count / wall, "wall_s": wall,
+                              "steady": sum(1 for r in served if r.status == "steady"),
+                              "capped": sum(1 for r in served if r.kind == "rans" and r.status == "running"),
+                              "peak_concurrent": srv.peak_active},
+        "sequential_fp64": {"p50_s": float(np.percentile(slat, 50)), "p99_s": float(np.percentile(slat, 99)),
+                            "solves_per_s": count / makespan, "makespan_s": makespan,
+                            "service_s_total": float(sum(services)),
+                            "steady": sum(1 for r in seq if r.status == "steady")},
+    }
+
+
 def measure_peak_bytes(n, nz):
     """Peak device bytes of one request on an n x n x nz tile: the resident
     member plus the initializer's Poisson solver, which lives only while the

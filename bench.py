@@ -2,7 +2,7 @@
 """Benchmark of the B200 SIMPLEC hot path (one JSON line on rank 0).
 
 python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                [--precision 0|1] [--no-cpu] [--no-steady] [--no-batch]
+                [--precision 0|1] [--no-cpu] [--no-steady] [--no-batch] [--no-serve]
 
 A step is one SIMPLEC outer iteration of config 1 (a single Gaussian hill,
 128 x 128 x 64 cells, dx = 25 m, stretched layers to a 1500 m lid, log-law
@@ -22,7 +22,9 @@ solved to the steady criterion in plain FP64 and with FP32 inner solves
 (steady solves/s, iterations and the per-field difference of the two
 steady states), and the batched form on a sample of the batched
 configuration's uneven tiles (FP32 inner solves on concurrent streams
-against plain FP64 one by one, cell-updates/s).
+against plain FP64 one by one, cell-updates/s), and a bounded sample of the
+served configuration (continuous batching against plain FP64 served one at
+a time: p50/p99 latency and solves/s).
 
 --impl reference times the reference's CPU implementation of the path, here
 the FP64 C restatement of it (the reference itself needs AMReX, which is not
@@ -453,6 +455,21 @@ def batched_leg(count=16, iterations=10, warmup=2):
     return out
 
 
+def served_leg():
+    """A bounded sample of the served configuration: 12 requests at 2 per
+    second, tiles drawn as config 3 with n in {64, 96} and nz in {48, 64},
+    70 % mass-consistent only and 30 % full solves (capped at 1500
+    iterations); served with continuous batching and FP32 inner solves
+    against plain FP64 served one at a time over the same arrivals."""
+    from ablsteadyrans_b200.serve import serve_vs_sequential
+    out = serve_vs_sequential(count=12, rate=2.0, sizes=(64, 96), layers=(48, 64), max_iterations=1500)
+    out["speedup_solves_per_s"] = out["served_fp32_inner"]["solves_per_s"] / out["sequential_fp64"]["solves_per_s"]
+    out["workload"] = ("12 requests, Poisson arrivals at 2/s, tiles drawn as config 3 with n in {64, 96}, nz in "
+                       "{48, 64} (a bounded sample), 70 % mass-consistent only, 30 % full solves capped at 1500 "
+                       "iterations")
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -464,6 +481,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
     ap.add_argument("--no-steady", action="store_true", help="skip the steady-solve leg")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched leg")
+    ap.add_argument("--no-serve", action="store_true", help="skip the served leg")
     ap.add_argument("--tune", action="append", default=[], metavar="KEY=VALUE",
                     help="a context tuning knob (GB_TUNE_*, by number or name without the prefix), repeatable")
     args = ap.parse_args()
@@ -609,6 +627,8 @@ def main():
         line["steady"] = steady_solves()
     if world == 1 and not args.no_batch:
         line["batched"] = batched_leg()
+    if world == 1 and not args.no_serve:
+        line["served"] = served_leg()
     if rank == 0 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(wl)
     if rank == 0:

@@ -119,3 +119,12 @@ def test_gpu_native_batch_same_alone_and_in_the_mix():
     for r, g_ in zip(ref, got):
         for f in r:
             assert np.array_equal(r[f], g_[f]), f
+
+
+def test_sequential_latencies_are_a_fifo_queue():
+    """The plain FP64 sequential path's latencies: one request at a time in
+    arrival order, each starting when it has arrived and the previous one
+    is done."""
+    from ablsteadyrans_b200.serve import sequential_latencies
+    assert sequential_latencies([0.0, 1.0, 1.5, 10.0], [2.0, 2.0, 2.0, 1.0]) == [2.0, 3.0, 4.5, 1.0]
+    assert sequential_latencies([], []) == []
