@@ -479,6 +479,34 @@ gb_status gb_scalar_sweep(gb_simplec* s, const gb_state* q, int32_t eq, const do
     return gb::simplec_scalar_step(s, *q, eq, R_eq, dtau, clip, res);
 }
 
+gb_status gb_simplec_precondition(gb_simplec* s, const gb_state* q, const double* dtau, double inf_cfl,
+                                  int32_t denominators, double* const* r, double* const* dq)
+{
+    gb::clear_error();
+    if (s == nullptr || q == nullptr || r == nullptr || dq == nullptr) {
+        gb::set_error("gust: SimplecPreconditioner: the stage, the state, r and dq are needed");
+        return GB_BAD_ARG;
+    }
+    if (denominators != 1 && denominators != 2) {
+        gb::set_error("gust: SimplecPreconditioner: denominators must be 1 (diagonal) or 2 (stage)");
+        return GB_BAD_ARG;
+    }
+    if (dtau == nullptr && (!std::isfinite(inf_cfl) || !(inf_cfl > 0))) {
+        gb::set_error("gust: SimplecPreconditioner: inf_cfl = %g: must be finite and > 0 (steady.cfl_max)", inf_cfl);
+        return GB_BAD_ARG;
+    }
+    for (int f = 0; f < 6; ++f) {
+        if (r[f] == nullptr || dq[f] == nullptr) {
+            gb::set_error("gust: SimplecPreconditioner: r and dq need six device arrays (u, v, w, p, theta, tke)");
+            return GB_BAD_ARG;
+        }
+    }
+    gb_status st = gb::simplec_linear_setup(s, *q, dtau, inf_cfl);
+    if (st != GB_OK) { return st; }
+    const double* rr[6] = {r[0], r[1], r[2], r[3], r[4], r[5]};
+    return gb::simplec_linear_apply(s, *q, rr, dq, denominators == 1);
+}
+
 gb_status gb_implicit_coefficients(gb_ctx* ctx, const gb_grid* g, int32_t loc, const double* F0, const double* F1,
                                    const double* F2, const double* gamma, const double* z_nd, const double* detJ,
                                    int32_t log_mean, double* A)

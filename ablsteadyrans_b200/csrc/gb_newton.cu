@@ -19,9 +19,11 @@
 // skipped when |b| is not finite or the Krylov residual is above |b|
 // (newton_update_usable).
 //
-// The preconditioner is the identity (steady.newton_preconditioner =
-// identity); the reductions are block sums added on the host in a fixed
-// order, so a step is deterministic.
+// The preconditioner (steady.newton_preconditioner) is the identity or the
+// SIMPLEC preconditioner of the stage (simplec_linear_setup/apply, one
+// SIMPLEC iteration on the linearized system), applied in the unscaled
+// variables: z = S^-1 P (T v). The reductions are block sums added on the
+// host in a fixed order, so a step is deterministic.
 #include "gb_simplec.cuh"
 #include "gb_stencil.cuh"
 
@@ -117,6 +119,7 @@ struct gb_newton {
     std::vector<gb::Vec> V, Z;
     gb::Vec R0, Jv, dq, qp, inv_dtau, b, x, w, dir;
     gb::Vec dtf;                         // the face dtau (3)
+    gb::Vec pr, pz;                      // the preconditioner's r = T v and its dq (with a preconditioner)
     double* partial{nullptr};            // device block sums
     double* h_partial{nullptr};          // pinned copy
     std::vector<void*> owned_mem;
@@ -360,8 +363,50 @@ gb_status base(gb_newton* n, const gb_state& q, double* bnorm)
     return st;
 }
 
-//! Restarted right-preconditioned flexible GMRES (identity preconditioner)
-//! for A x = b from x = 0, to |b - A x| <= rtol |b|.
+//! z = M v, the right preconditioner in the scaled variables: v itself
+//! (identity), or S^-1 P (T v) with P one SIMPLEC iteration on the
+//! unscaled linearized system (gust::SimplecPreconditioner::apply).
+gb_status precondition(gb_newton* n, const gb_state& q, const Vec& v, const Vec& z)
+{
+    if (n->opt.preconditioner == 0) {
+        lincomb(n, z, 1.0, v, 0.0);
+        return GB_OK;
+    }
+    const gb_grid g = n->g;
+    for (int f = 0; f < kNF; ++f) {
+        double* r = n->pr[f];
+        const double* vf = v[f];
+        const double tf = n->t[f];
+        for_box(nctx(n), valid_box(g, kFieldLoc[f]), [=] __device__(int i, int j, int k) {
+            const int64_t o = at(g, i, j, k);
+            r[o] = tf * vf[o];
+        }, GB_KERNEL_VECTOR);
+    }
+    // the stage's wall state and closure fields at q (the jvp's evaluations
+    // in between left the perturbed state's), as the setup froze them
+    simplec_fill_ghosts(n->S, q);
+    if (simplec_physics(n->S).closure) {
+        double* R[kNF] = {n->Jv[0], n->Jv[1], n->Jv[2], n->Jv[3], n->Jv[4], n->Jv[5]};
+        simplec_residual(n->S, q, R);
+    }
+    const double* rr[kNF] = {n->pr[0], n->pr[1], n->pr[2], n->pr[3], n->pr[4], n->pr[5]};
+    double* zz[kNF] = {n->pz[0], n->pz[1], n->pz[2], n->pz[3], n->pz[4], n->pz[5]};
+    gb_status st = simplec_linear_apply(n->S, q, rr, zz, n->opt.preconditioner == 1);
+    if (st != GB_OK) { return st; }
+    for (int f = 0; f < kNF; ++f) {
+        double* zf = z[f];
+        const double* pf = n->pz[f];
+        const double sinv = 1.0 / n->s[f];
+        for_box(nctx(n), valid_box(g, kFieldLoc[f]), [=] __device__(int i, int j, int k) {
+            const int64_t o = at(g, i, j, k);
+            zf[o] = sinv * pf[o];
+        }, GB_KERNEL_VECTOR);
+    }
+    return check_cuda("NewtonPreconditioner::apply");
+}
+
+//! Restarted right-preconditioned flexible GMRES for A x = b from x = 0, to
+//! |b - A x| <= rtol |b|.
 gb_status fgmres(gb_newton* n, const gb_state& q, bool has_dtau, double bnorm, gb_newton_step_info* info)
 {
     const int m = n->opt.gmres_restart;
@@ -394,7 +439,7 @@ gb_status fgmres(gb_newton* n, const gb_state& q, bool has_dtau, double bnorm, g
         sv[0] = beta;
         int jj = 0;
         for (; jj < m && it < n->opt.gmres_max_iters; ++jj, ++it) {
-            lincomb(n, n->Z[jj], 1.0, n->V[jj], 0.0);   // the identity preconditioner
+            if ((st = precondition(n, q, n->V[jj], n->Z[jj])) != GB_OK) { return st; }
             if ((st = apply_op(n, q, n->Z[jj], n->w, has_dtau)) != GB_OK) { return st; }
             for (int i = 0; i <= jj; ++i) {
                 double h = 0;
@@ -464,6 +509,9 @@ gb_status solve(gb_newton* n, const gb_state& q, const double* dtau, gb_newton_s
         for (int f = 0; f < kNF; ++f) { cudaMemsetAsync(n->x[f], 0, sizeof(double) * n->vol, nctx(n)->stream); }
         return GB_OK;
     }
+    if (n->opt.preconditioner != 0 && (st = simplec_linear_setup(n->S, q, dtau, n->opt.inf_cfl)) != GB_OK) {
+        return st;
+    }
     if ((st = fgmres(n, q, has_dtau, bnorm, info)) != GB_OK) { return st; }
     info->krylov_relative = info->krylov_residual / bnorm;
     info->eps_min = n->eps_min;
@@ -519,6 +567,16 @@ gb_status check_newton(const gb_newton_opts* o)
         std::snprintf(b, sizeof(b), "the pressure scale = %.3e: must be finite and > 0", o->scale_pressure);
         err.emplace_back(b);
     }
+    if (o->preconditioner < 0 || o->preconditioner > 2) {
+        std::snprintf(b, sizeof(b), "steady.newton_preconditioner = %d: must be identity (0) or simplec (1, 2)",
+                      o->preconditioner);
+        err.emplace_back(b);
+    }
+    if (o->preconditioner != 0 && (!std::isfinite(o->inf_cfl) || !(o->inf_cfl > 0))) {
+        std::snprintf(b, sizeof(b), "steady.cfl_max = %.3e: the preconditioner's CFL must be finite and > 0",
+                      o->inf_cfl);
+        err.emplace_back(b);
+    }
     if (err.empty()) { return GB_OK; }
     std::string all = "gust: invalid inputs:";
     for (const auto& e : err) { all += "\n  " + e; }
@@ -542,6 +600,8 @@ gb_status gb_newton_options_default(gb_newton_opts* o)
     o->fd_eps_scale = std::sqrt(std::numeric_limits<double>::epsilon());
     o->krylov_rtol = 1.0e-2;
     o->scale_pressure = 100.0;
+    o->preconditioner = 1;
+    o->inf_cfl = 10.0;
     return GB_OK;
 }
 
@@ -593,6 +653,7 @@ gb_status gb_newton_create(gb_simplec* s, const gb_newton_opts* o, gb_newton** o
     ok = ok && gb::make_vec(n, n->R0) && gb::make_vec(n, n->Jv) && gb::make_vec(n, n->dq) && gb::make_vec(n, n->qp)
          && gb::make_vec(n, n->inv_dtau) && gb::make_vec(n, n->b) && gb::make_vec(n, n->x) && gb::make_vec(n, n->w)
          && gb::make_vec(n, n->dir, 3) && gb::make_vec(n, n->dtf, 3);
+    if (o->preconditioner != 0) { ok = ok && gb::make_vec(n, n->pr) && gb::make_vec(n, n->pz); }
     ok = ok && (n->partial = gb::nbuf(n, 3 * gb::kRedBlocksN * gb::kNF)) != nullptr;
     if (ok && cudaMallocHost(&n->h_partial, sizeof(double) * 3 * gb::kRedBlocksN * gb::kNF) != cudaSuccess) {
         cudaGetLastError();

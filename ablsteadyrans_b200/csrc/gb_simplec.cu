@@ -304,6 +304,17 @@ struct gb_simplec {
     // first, launched on the context's stream, rebuilt when what their kernels'
     // arguments depend on changes (the state and dtau pointers, the nu_t
     // history's presence, the tuning knobs).
+    // the Newton stage's SIMPLEC preconditioner (simplec_linear_setup/apply),
+    // allocated on first use: the increment state, q + sigma du, the transport
+    // at q and at q + sigma du, theta's convection at q, the setup's cell step
+    double* lin_d[6]{};
+    double* lin_qn[6]{};
+    double* lin_F0[3]{};
+    double* lin_F1[3]{};
+    double* lin_conv0{nullptr};
+    double* lin_dtau{nullptr};
+    double lin_speed{1};
+    bool lin_ready{false};
     cudaStream_t capture_stream{nullptr};
     cudaGraphExec_t seg_exec[2]{nullptr, nullptr};
     int64_t seg_launches[2]{0, 0};
@@ -436,8 +447,10 @@ void fill_periodic_all(gb_simplec* S, double* const* f, const int* t, int nf)
 }
 
 //! The face fills of every field along d on one side (fill_face / fill_gradient_z,
-//! BoundaryConditions.cpp:418-517), fields in the reference's order.
-void fill_side(gb_simplec* S, const gb_state& q, int d, bool lo)
+//! BoundaryConditions.cpp:418-517), fields in the reference's order. homog:
+//! the homogeneous fill of an increment (every boundary value, inflow
+//! profile and gradient taken as 0, BoundaryConditions.cpp:421-517).
+void fill_side(gb_simplec* S, const gb_state& q, int d, bool lo, bool homog = false)
 {
     const gb_grid g = S->g;
     const int ng = g.ng;
@@ -450,15 +463,17 @@ void fill_side(gb_simplec* S, const gb_state& q, int d, bool lo)
         FF[f].t = kLoc[f];
         FF[f].f = f;
         FF[f].rule = rule_for(f, ft, d, lo);
-        FF[f].V = (ft == GB_FACE_NO_SLIP_WALL && f <= F_W) ? S->bc.wall_velocity[face][f] : 0.0;
+        FF[f].V = (ft == GB_FACE_NO_SLIP_WALL && f <= F_W && !homog) ? S->bc.wall_velocity[face][f] : 0.0;
         FF[f].gg = nullptr;
-        if (ft == GB_FACE_SURFACE_LAYER && FF[f].rule == R_GRADIENT) { FF[f].gg = S->gg[f == F_U ? 0 : f == F_V ? 1 : 2]; }
+        if (ft == GB_FACE_SURFACE_LAYER && FF[f].rule == R_GRADIENT && !homog) {
+            FF[f].gg = S->gg[f == F_U ? 0 : f == F_V ? 1 : 2];
+        }
     }
     FillPack P;
     std::memcpy(P.F, FF, sizeof(FF));
     const Profile prof = S->prof;
     const double* z = S->z;
-    const double G = S->bc.zhi_theta_grad;
+    const double G = homog ? 0.0 : S->bc.zhi_theta_grad;
     const int per[3] = {g.periodic_x, g.periodic_y, 0};
     // union box over the slab: layers 0..ng along d, the grown extents elsewhere
     Box b{};
@@ -508,7 +523,7 @@ void fill_side(gb_simplec* S, const gb_state& q, int d, bool lo)
                 if (!(nod && (F.rule == R_VALUE || F.rule == R_PROFILE))) { continue; }
                 int p[3] = {i, j, k};
                 p[d] = edge;
-                a[at(g, p[0], p[1], p[2])] = (F.rule == R_PROFILE)
+                a[at(g, p[0], p[1], p[2])] = (F.rule == R_PROFILE && !homog)
                     ? prof.value(F.f, height_above_ground(z, g, t, p[0], p[1], p[2])) : F.V;
                 continue;
             }
@@ -519,7 +534,7 @@ void fill_side(gb_simplec* S, const gb_state& q, int d, bool lo)
             s[d] = mirror - gidx;
             double* dst = &a[at(g, p[0], p[1], p[2])];
             if (F.rule == R_PROFILE) {
-                *dst = prof.value(F.f, height_above_ground(z, g, t, p[0], p[1], p[2]));
+                *dst = homog ? 0.0 : prof.value(F.f, height_above_ground(z, g, t, p[0], p[1], p[2]));
             } else if (F.rule == R_VALUE) {
                 *dst = 2 * F.V - a[at(g, s[0], s[1], s[2])];
             } else {
@@ -559,18 +574,18 @@ void fill_no_flux_w(gb_simplec* S, const gb_state& q)
 //! BoundaryConditions::fill_ghosts (BoundaryConditions.cpp:597-663); a
 //! surface_layer ground: the surface state from the laterally filled state
 //! into ss and the wall law's gradient for the ground fills.
-void fill_ghosts_into(gb_simplec* S, const gb_state& q, double* const* ss)
+void fill_ghosts_into(gb_simplec* S, const gb_state& q, double* const* ss, bool homog = false)
 {
     double* f[6] = {q.u, q.v, q.w, q.p, q.theta, q.tke};
     fill_periodic_all(S, f, kLoc, 6);
     for (int d = 0; d < 3; ++d) {
-        if (d == 2 && S->wall) {
+        if (d == 2 && S->wall && !homog) {
             turb_surface_state(S->ctx, S->g, S->bc, S->ph, q, S->z, S->mesh.z0, ss, dword(S->ctx, W_SURFACE_BAD));
             turb_ground_gradients(S->ctx, S->g, S->bc, ss, S->mesh.z0, S->gg);
         }
         if (is_per(S->g, d)) { continue; }
-        fill_side(S, q, d, true);
-        fill_side(S, q, d, false);
+        fill_side(S, q, d, true, homog);
+        fill_side(S, q, d, false, homog);
         if (d == 2) {
             // the no-flux w faces after u, v, w (p, theta, k do not read w)
             fill_no_flux_w(S, q);
@@ -1587,7 +1602,7 @@ gb_status momentum_predictor(gb_simplec* S, const gb_state& q, double** R)
 
 //! pressure_correction's first part: beta = 1/d and the keep masks, div u*,
 //! the monitors, the solver's coefficients (no host synchronisation).
-gb_status pressure_prelude(gb_simplec* S, const gb_state& q)
+gb_status pressure_prelude(gb_simplec* S, const gb_state& q, const double* source = nullptr)
 {
     gb_ctx* ctx = S->ctx;
     const gb_grid g = S->g;
@@ -1604,6 +1619,15 @@ gb_status pressure_prelude(gb_simplec* S, const gb_state& q)
         }, GB_KERNEL_COEFS);
     }
     velocity_divergence(S, q.u, q.v, q.w, w.rhs);
+    if (source != nullptr) {
+        // the Newton preconditioner's continuity rows: div(du) = r_p
+        // (pressure_correction's source, Simplec.H:130-138)
+        double* rhs = w.rhs;
+        for_box(ctx, valid_box(g, CC), [=] __device__(int i, int j, int k) {
+            const int64_t o = at(g, i, j, k);
+            rhs[o] -= source[o];
+        }, GB_KERNEL_MASSFLUX);
+    }
     dmax(S, valid_box(g, CC), w.rhs, nullptr, W_DIV_BEFORE);
     dmax(S, valid_box(g, XF), q.u, nullptr, W_SPEED_U);
     dmax(S, valid_box(g, YF), q.v, nullptr, W_SPEED_V);
@@ -1613,7 +1637,7 @@ gb_status pressure_prelude(gb_simplec* S, const gb_state& q)
 
 //! pressure_correction's Krylov solve (host-synchronising) and the check of
 //! the singular case's removed mean.
-gb_status pressure_solve(gb_simplec* S, gb_iter_info* info)
+gb_status pressure_solve(gb_simplec* S, gb_iter_info* info, bool project_net_source = false)
 {
     gb_ctx* ctx = S->ctx;
     const gb_grid g = S->g;
@@ -1623,7 +1647,7 @@ gb_status pressure_solve(gb_simplec* S, gb_iter_info* info)
     if (st != GB_OK) { return st; }
     info->poisson_iterations = pr.iterations;
     info->poisson_removed_mean = pr.removed_mean;
-    if (pr.singular) {
+    if (pr.singular && !project_net_source) {
         unsigned long long sp[3];
         if ((st = read_words(ctx, W_SPEED_U, 3, sp)) != GB_OK) { return st; }
         const double speed = std::max(std::max(bits_to_double(sp[0]), bits_to_double(sp[1])), bits_to_double(sp[2]));
@@ -1775,7 +1799,7 @@ gb_status run_segment(gb_simplec* S, int id, uint64_t key, F&& body)
 //! (the A1 rows, a_P = 1/dtau + A_P, rhs = -R), the two solved by one batched
 //! line solve (the systems are independent), the increments added, k clipped
 //! at the floor with the clipped points counted.
-gb_status scalar_sweeps(gb_simplec* S, const gb_state& q, const double* dtau)
+gb_status scalar_sweeps(gb_simplec* S, const gb_state& q, const double* dtau, bool clip = true)
 {
     gb_ctx* ctx = S->ctx;
     const gb_grid g = S->g;
@@ -1806,7 +1830,7 @@ gb_status scalar_sweeps(gb_simplec* S, const gb_state& q, const double* dtau)
         dmax(S, valid_box(g, CC), w.deltam[e], nullptr, wmax[e]);
         const double* delta = w.deltam[e];
         double* field = fields[e];
-        const bool do_clip = (eqs[e] == F_TKE);
+        const bool do_clip = (eqs[e] == F_TKE) && clip;
         const double floor = S->opt.tke_floor;
         for_box(ctx, valid_box(g, CC), [=] __device__(int i, int j, int k) {
             const int64_t o = at(g, i, j, k);
@@ -2069,6 +2093,217 @@ gb_status implicit_coefficients_at(gb_ctx* ctx, const gb_grid& g, int loc, doubl
     default: implicit_coefficients_on<2>(ctx, g, z, J, logz, F, gamma, A); break;
     }
     return check_cuda("implicit_coefficients");
+}
+
+// ----------------------------------- the Newton stage's preconditioner ---
+//
+// gust::SimplecPreconditioner (Source/NewtonPreconditioner.H:1-108,
+// NewtonPreconditioner.cpp:113-219): one SIMPLEC iteration on the Newton
+// system linearized at q, (D + J) dq = r, from dq = 0, built from the stage's
+// own pieces.
+
+namespace {
+
+gb_status lin_alloc(gb_simplec* S)
+{
+    if (S->lin_d[0] != nullptr) { return GB_OK; }
+    const int64_t vol = volume(S->g);
+    for (int f = 0; f < 6; ++f) {
+        S->lin_d[f] = dbuf(S, vol);
+        S->lin_qn[f] = dbuf(S, vol);
+        if (!S->lin_d[f] || !S->lin_qn[f]) { return GB_OOM; }
+    }
+    for (int c = 0; c < 3; ++c) {
+        S->lin_F0[c] = dbuf(S, vol);
+        S->lin_F1[c] = dbuf(S, vol);
+        if (!S->lin_F0[c] || !S->lin_F1[c]) { return GB_OOM; }
+    }
+    S->lin_conv0 = dbuf(S, vol);
+    S->lin_dtau = dbuf(S, vol);
+    if (!S->lin_conv0 || !S->lin_dtau) { return GB_OOM; }
+    return GB_OK;
+}
+
+gb_state lin_state(double* const* f, const double* z)
+{
+    return gb_state{f[0], f[1], f[2], f[3], f[4], f[5], z};
+}
+
+}  // namespace
+
+//! SimplecPreconditioner::setup (NewtonPreconditioner.cpp:113-150) at q:
+//! the stage's fill with the wall state, the closure's fields at q (one
+//! residual), the step (dtau, or local_dtau at inf_cfl when dtau is null),
+//! the transport at q, the face steps, theta's convection at q and the
+//! velocity scale max(1, max |u|).
+gb_status simplec_linear_setup(gb_simplec* S, const gb_state& q, const double* dtau, double inf_cfl)
+{
+    gb_ctx* ctx = S->ctx;
+    const gb_grid g = S->g;
+    SimplecWork& w = S->w;
+    gb_status st = lin_alloc(S);
+    if (st != GB_OK) {
+        set_error("gust: SimplecPreconditioner: out of device memory");
+        return st;
+    }
+    fill_ghosts_into(S, q, S->ss);
+    if (S->ph.closure) {
+        simplec_residual(S, q, w.R);
+        cudaMemcpyAsync(S->nu_dtau, S->cf[kClosureNu], sizeof(double) * volume(g), cudaMemcpyDeviceToDevice, ctx->stream);
+    }
+    if (dtau != nullptr) {
+        cudaMemcpyAsync(S->lin_dtau, dtau, sizeof(double) * volume(g), cudaMemcpyDeviceToDevice, ctx->stream);
+    } else if ((st = simplec_local_dtau(S, q, inf_cfl, S->lin_dtau)) != GB_OK) {
+        return st;
+    }
+    transport_fluxes(S, q, S->lin_F0[0], S->lin_F0[1], S->lin_F0[2]);
+    face_dtau(S, S->lin_dtau, w.dtf);
+    convection<CC>(S, q.theta, S->lin_F0, S->ph.limiter, S->ph.smooth_eps_theta, false, S->lin_conv0);
+    cudaMemsetAsync(dword(ctx, W_SPEED_U), 0, sizeof(unsigned long long) * 3, ctx->stream);
+    dmax(S, valid_box(g, XF), q.u, nullptr, W_SPEED_U);
+    dmax(S, valid_box(g, YF), q.v, nullptr, W_SPEED_V);
+    dmax(S, valid_box(g, ZF), q.w, nullptr, W_SPEED_W);
+    unsigned long long sp[3];
+    if ((st = read_words(ctx, W_SPEED_U, 3, sp)) != GB_OK) { return st; }
+    S->lin_speed = std::max(1.0, std::max(bits_to_double(sp[0]), std::max(bits_to_double(sp[1]), bits_to_double(sp[2]))));
+    S->lin_ready = true;
+    return check_cuda("SimplecPreconditioner::setup");
+}
+
+//! SimplecPreconditioner::apply (NewtonPreconditioner.cpp:152-219): dq from
+//! r (six fields at the state's locations, valid points read). diagonal: the
+//! SIMPLE denominators d = a_P (the reference's default) and theta's coupling
+//! as the directional derivative along du with the scalar sweeps on q's
+//! transport (linear in r); else the stage's SIMPLEC denominators with the
+//! full du and the corrected transport (one iteration of the stage). The
+//! wall state and the closure's fields are the stage's current ones (the
+//! setup's, or the caller's refresh at q).
+gb_status simplec_linear_apply(gb_simplec* S, const gb_state& q, const double* const* r, double* const* dq,
+                               bool diagonal)
+{
+    gb_ctx* ctx = S->ctx;
+    const gb_grid g = S->g;
+    const int64_t vol = volume(g);
+    SimplecWork& w = S->w;
+    if (!S->lin_ready) {
+        set_error("gust: SimplecPreconditioner::apply: setup has not been called");
+        return GB_BAD_ARG;
+    }
+    // -r in place of the residual (the stage's R(q) for r = -R(q))
+    for (int f = 0; f < 6; ++f) {
+        cudaMemsetAsync(w.R[f], 0, sizeof(double) * vol, ctx->stream);
+        double* Rf = w.R[f];
+        const double* rf = r[f];
+        for_box(ctx, valid_box(g, kLoc[f]), [=] __device__(int i, int j, int k) {
+            const int64_t o = at(g, i, j, k);
+            Rf[o] = -rf[o];
+        }, GB_KERNEL_VECTOR);
+    }
+    // 1. the momentum predictor on the increment from zero, theta = q's for
+    // its buoyancy coupling, the transport, wall state and closure at q
+    for (int f = 0; f < 6; ++f) {
+        if (f == F_THETA) {
+            cudaMemcpyAsync(S->lin_d[f], q.theta, sizeof(double) * vol, cudaMemcpyDeviceToDevice, ctx->stream);
+        } else {
+            cudaMemsetAsync(S->lin_d[f], 0, sizeof(double) * vol, ctx->stream);
+        }
+    }
+    const gb_state d = lin_state(S->lin_d, q.z_nd);
+    for (int c = 0; c < 3; ++c) {
+        cudaMemcpyAsync(w.F[c], S->lin_F0[c], sizeof(double) * vol, cudaMemcpyDeviceToDevice, ctx->stream);
+    }
+    gb_status st = momentum_predictor(S, d, w.R);
+    if (st != GB_OK) { return st; }
+    // 2. the pressure correction of du*, r_p as the source, the homogeneous
+    // fill giving du*'s ghosts (theta back to 0 first)
+    cudaMemsetAsync(S->lin_d[F_THETA], 0, sizeof(double) * vol, ctx->stream);
+    fill_ghosts_into(S, d, nullptr, true);
+    if (diagonal) {
+        for (int c = 0; c < 3; ++c) {
+            double* dd = w.dd[c];
+            const double* ap = w.ap[c];
+            for_box(ctx, valid_box(g, kLoc[c]), [=] __device__(int i, int j, int k) {
+                const int64_t o = at(g, i, j, k);
+                dd[o] = (dd[o] > 0) ? ap[o] : 0.0;
+            }, GB_KERNEL_COEFS);
+        }
+    }
+    if ((st = pressure_prelude(S, d, r[3])) != GB_OK) { return st; }
+    gb_iter_info info{};
+    if ((st = pressure_solve(S, &info, true)) != GB_OK) { return st; }
+    if ((st = pressure_finish(S, d)) != GB_OK) { return st; }
+    // 3. theta's convection with the corrected velocity minus that at q:
+    // diagonal, the directional derivative along du with the step
+    // sigma = sqrt(eps) max(1, max|u|) / max|du|; else the full du
+    double sigma = 1.0;
+    if (diagonal) {
+        cudaMemsetAsync(dword(ctx, W_MAX_DU), 0, sizeof(unsigned long long) * 3, ctx->stream);
+        dmax(S, valid_box(g, XF), S->lin_d[F_U], nullptr, W_MAX_DU);
+        dmax(S, valid_box(g, YF), S->lin_d[F_V], nullptr, W_MAX_DV);
+        dmax(S, valid_box(g, ZF), S->lin_d[F_W], nullptr, W_MAX_DW);
+        unsigned long long md[3];
+        if ((st = read_words(ctx, W_MAX_DU, 3, md)) != GB_OK) { return st; }
+        const double dmx = std::max(bits_to_double(md[0]), std::max(bits_to_double(md[1]), bits_to_double(md[2])));
+        sigma = (dmx > 0) ? std::sqrt(std::numeric_limits<double>::epsilon()) * S->lin_speed / dmx : 1.0;
+    }
+    const double* qf[6] = {q.u, q.v, q.w, q.p, q.theta, q.tke};
+    for (int f = 0; f < 6; ++f) {
+        cudaMemcpyAsync(S->lin_qn[f], qf[f], sizeof(double) * vol, cudaMemcpyDeviceToDevice, ctx->stream);
+    }
+    for (int c = 0; c < 3; ++c) {
+        double* qn = S->lin_qn[c];
+        const double* dc = S->lin_d[c];
+        for_box(ctx, valid_box(g, kLoc[c]), [=] __device__(int i, int j, int k) {
+            const int64_t o = at(g, i, j, k);
+            qn[o] += sigma * dc[o];
+        }, GB_KERNEL_VECTOR);
+    }
+    const gb_state qn = lin_state(S->lin_qn, q.z_nd);
+    fill_ghosts_into(S, qn, S->sst);
+    transport_fluxes(S, qn, S->lin_F1[0], S->lin_F1[1], S->lin_F1[2]);
+    convection<CC>(S, qn.theta, S->lin_F1, S->ph.limiter, S->ph.smooth_eps_theta, false, w.conv1);
+    {
+        double* Rt = w.R[F_THETA];
+        const double* c0 = S->lin_conv0;
+        const double* c1 = w.conv1;
+        const double inv_sigma = 1.0 / sigma;
+        for_box(ctx, valid_box(g, CC), [=] __device__(int i, int j, int k) {
+            const int64_t o = at(g, i, j, k);
+            Rt[o] += inv_sigma * (c1[o] - c0[o]);
+        }, GB_KERNEL_VECTOR);
+    }
+    // 4. the theta and k steps on the increments (0, ghosts included), no
+    // floor on dk: diagonal, with q's transport; else the corrected one
+    cudaMemsetAsync(S->lin_d[F_THETA], 0, sizeof(double) * vol, ctx->stream);
+    cudaMemsetAsync(S->lin_d[F_TKE], 0, sizeof(double) * vol, ctx->stream);
+    double* const* Fs = diagonal ? S->lin_F0 : S->lin_F1;
+    for (int c = 0; c < 3; ++c) {
+        cudaMemcpyAsync(w.F[c], Fs[c], sizeof(double) * vol, cudaMemcpyDeviceToDevice, ctx->stream);
+    }
+    if ((st = scalar_sweeps(S, d, S->lin_dtau, false)) != GB_OK) { return st; }
+    // 5. dq: the increment's valid points; the Dirichlet rows of u, v, w are
+    // identity rows of the Newton system (dq = r there); seam copies synced
+    for (int f = 0; f < 6; ++f) {
+        cudaMemsetAsync(dq[f], 0, sizeof(double) * vol, ctx->stream);
+        double* o_ = dq[f];
+        const double* src = S->lin_d[f];
+        for_box(ctx, valid_box(g, kLoc[f]), [=] __device__(int i, int j, int k) {
+            const int64_t o = at(g, i, j, k);
+            o_[o] = src[o];
+        }, GB_KERNEL_VECTOR);
+    }
+    for (int c = 0; c < 3; ++c) {
+        dirichlet_rows(S, c, 1 << c, w.mask);
+        double* o_ = dq[c];
+        const double* rc = r[c];
+        const double* mask = w.mask;
+        for_box(ctx, valid_box(g, kLoc[c]), [=] __device__(int i, int j, int k) {
+            const int64_t o = at(g, i, j, k);
+            if (mask[o] > 0) { o_[o] = rc[o]; }
+        }, GB_KERNEL_VECTOR);
+        seam_sync<double>(ctx, g, kLoc[c], dq[c]);
+    }
+    return check_cuda("SimplecPreconditioner::apply");
 }
 
 gb_status simplec_norms(gb_simplec* S, const gb_state& q, double* res, double* mon)

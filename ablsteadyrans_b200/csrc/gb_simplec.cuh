@@ -20,6 +20,9 @@ gb_status simplec_predictor_step(gb_simplec* S, const gb_state& q, double* const
 gb_status simplec_pressure_step(gb_simplec* S, const gb_state& q, const double* const* d, gb_pressure_result* res);
 gb_status simplec_scalar_step(gb_simplec* S, const gb_state& q, int eq, const double* R_eq, const double* dtau,
                               int clip, gb_scalar_result* res);
+gb_status simplec_linear_setup(gb_simplec* S, const gb_state& q, const double* dtau, double inf_cfl);
+gb_status simplec_linear_apply(gb_simplec* S, const gb_state& q, const double* const* r, double* const* dq,
+                               bool diagonal);
 gb_status implicit_coefficients_at(gb_ctx* ctx, const gb_grid& g, int loc, double* const* F, const double* gamma,
                                    const double* z, const double* J, int logz, double* A);
 gb_status simplec_confidence(gb_simplec* S, const double* thresholds, double* share, double* height);

@@ -25,12 +25,16 @@ class NewtonOptions(ctypes.Structure):
     """gb_newton_opts: steady.newton_* of the Newton core."""
     _fields_ = [("gmres_restart", ctypes.c_int32), ("gmres_max_iters", ctypes.c_int32),
                 ("fd_eps_scale", ctypes.c_double), ("krylov_rtol", ctypes.c_double),
-                ("scale_pressure", ctypes.c_double)]
+                ("scale_pressure", ctypes.c_double), ("preconditioner", ctypes.c_int32),
+                ("inf_cfl", ctypes.c_double)]
+
+    #: steady.newton_preconditioner values
+    IDENTITY, SIMPLEC, SIMPLEC_STAGE = 0, 1, 2
 
     @classmethod
     def make(cls, **kw):
         o = cls(gmres_restart=30, gmres_max_iters=2000, fd_eps_scale=math.sqrt(sys.float_info.epsilon),
-                krylov_rtol=1e-2, scale_pressure=100.0)
+                krylov_rtol=1e-2, scale_pressure=100.0, preconditioner=1, inf_cfl=10.0)
         for k, v in kw.items():
             setattr(o, k, v)
         return o

@@ -47,6 +47,8 @@ def _declare(L):
                                          ctypes.POINTER(abi.PressureResult)]
     L.gb_scalar_sweep.argtypes = [P, ctypes.POINTER(abi.State), ctypes.c_int32, P, P, ctypes.c_int32,
                                   ctypes.POINTER(abi.ScalarResult)]
+    L.gb_simplec_precondition.argtypes = [P, ctypes.POINTER(abi.State), P, ctypes.c_double, ctypes.c_int32,
+                                          ctypes.POINTER(P), ctypes.POINTER(P)]
 
 
 # The closure's fields and the surface state's planes, in the ABI's order.
@@ -238,6 +240,21 @@ class SimplecStage:
         check(self._L.gb_scalar_sweep(self._h, ctypes.byref(st), int(eq), ctypes.c_void_p(R_eq.data_ptr()),
                                       ctypes.c_void_p(dtau.data_ptr()), int(bool(clip)), ctypes.byref(res)))
         return res
+
+    def precondition(self, r, dtau=None, inf_cfl=10.0, denominators=1):
+        """gust::SimplecPreconditioner setup at the stage's state and one
+        apply to r (six device tensors): dq for (D + J) dq = r by one SIMPLEC
+        iteration (denominators 1: d = a_P; 2: the stage's d)."""
+        import torch
+        from . import check
+        dq = [torch.zeros(self.case.grid.shape, dtype=torch.float64, device="cuda") for _ in range(6)]
+        st = self.case.state()
+        ra = (ctypes.c_void_p * 6)(*[t.data_ptr() for t in r])
+        da = (ctypes.c_void_p * 6)(*[t.data_ptr() for t in dq])
+        check(self._L.gb_simplec_precondition(self._h, ctypes.byref(st),
+                                              None if dtau is None else ctypes.c_void_p(dtau.data_ptr()),
+                                              float(inf_cfl), int(denominators), ra, da))
+        return dq
 
     def initialize(self, options=None):
         """gust::initialize_state with init.first_guess = profile: the

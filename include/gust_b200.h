@@ -540,6 +540,21 @@ gb_status gb_pressure_correction(gb_simplec* s, const gb_state* q, const double*
 gb_status gb_scalar_sweep(gb_simplec* s, const gb_state* q, int32_t eq, const double* R_eq, const double* dtau,
                           int32_t clip, gb_scalar_result* res);
 
+/* gust::SimplecPreconditioner (Source/NewtonPreconditioner.H:120-186):
+ * setup at q (the stage's fill with the wall state, the closure's fields at
+ * q, the step dtau, or local_dtau at inf_cfl when dtau is NULL, the transport
+ * and theta's convection at q), then one apply: dq for the Newton system
+ * linearized at q, (D + J) dq = r, by one SIMPLEC iteration from dq = 0 (the
+ * momentum predictor with -r as the residual, the pressure correction of du*
+ * with r_p as the source after the homogeneous fill, theta's coupling, the
+ * theta and k steps without the floor; dq = r on the Dirichlet rows of u, v,
+ * w). denominators: 1 the SIMPLE d = a_P (the reference's default), 2 the
+ * stage's SIMPLEC d = a_P - sum a_nb (then with r = -R(q) the result is the
+ * increment of one stage iteration from q, off the Dirichlet rows). r and dq:
+ * six device arrays of the grid (u, v, w, p, theta, k). */
+gb_status gb_simplec_precondition(gb_simplec* s, const gb_state* q, const double* dtau, double inf_cfl,
+                                  int32_t denominators, double* const* r, double* const* dq);
+
 /* gust::implicit_coefficients (Source/ImplicitOperator.H:65-67,
  * ImplicitOperator.cpp:96-121): the 7 coefficients at loc (GB_LOC_CELL or a
  * face) of the upwind transport F (x-, y-, z-face fluxes, one ghost) and the
@@ -649,6 +664,12 @@ typedef struct gb_newton_opts {
     double fd_eps_scale;             /* steady.newton_fd_eps_scale (eps^(3/4) .. 1e-2; sqrt(eps)) */
     double krylov_rtol;              /* steady.newton_krylov_rtol ((0, 1); 1e-2) */
     double scale_pressure;           /* s_p (100 m^2/s^2) */
+    int32_t preconditioner;          /* steady.newton_preconditioner: 0 identity, 1 simplec (one SIMPLEC
+                                        iteration on the linearized system with the SIMPLE denominators
+                                        d = a_P, the default; gust::SimplecPreconditioner,
+                                        Source/NewtonPreconditioner.H:1-108), 2 simplec with the stage's
+                                        SIMPLEC denominators (PressureDenominator::stage) */
+    double inf_cfl;                  /* the preconditioner's CFL when a step has no dtau (steady.cfl_max; 10) */
 } gb_newton_opts;
 /* What one Newton step did (gust::NewtonStepInfo, Source/Newton.H:230-248). */
 typedef struct gb_newton_step_info {
