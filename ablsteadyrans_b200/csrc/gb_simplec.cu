@@ -2456,9 +2456,12 @@ gb_status simplec_initialize(gb_simplec* S, const gb_state& q, const gb_init_opt
     const int64_t vol = volume(g);
     SimplecWork& w = S->w;
     *r = gb_init_result{};
-    // A new initial state starts without a nu_t history: in the reference each
-    // level's closure is new when its state is initialized (Closure::has_history).
+    // A new initial state starts without a nu_t history and with the first
+    // local dtau's viscosity 0: in the reference each level's closure and
+    // stage are new when its state is initialized (Closure::has_history,
+    // Simplec.cpp:328).
     S->has_hist = false;
+    if (S->ph.closure) { cudaMemsetAsync(S->nu_dtau, 0, sizeof(double) * volume(g), ctx->stream); }
     // 1. u, v at every point; w = 0 but the ground faces, which carry no flux
     fill_from_profile(S, XF, F_U, o.z_agl_min, 0.0, q.u);
     fill_from_profile(S, YF, F_V, o.z_agl_min, 0.0, q.v);
@@ -2724,7 +2727,9 @@ gb_status simplec_prolong(gb_simplec* S, const gb_state& q, const gb_grid& gc, c
     SimplecWork& w = S->w;
     const int r = g.nx / gc.nx;
     // the prolonged state is a new level's: no nu_t history (a fresh Closure)
+    // and the first local dtau's viscosity 0 (a fresh stage)
     S->has_hist = false;
+    if (S->ph.closure) { cudaMemsetAsync(S->nu_dtau, 0, sizeof(double) * volume(g), ctx->stream); }
     // prolong_fields (Transfer.cpp:290-320)
     interpolate(ctx, g, gc, CC, qc.theta, q.theta, r);
     interpolate(ctx, g, gc, CC, qc.tke, q.tke, r);
