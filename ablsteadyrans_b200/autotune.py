@@ -9,8 +9,9 @@ form runs, never what is computed:
     split among a block's warps) or the sequential factored sweep (one
     thread walks a column);
   * GB_TUNE_LINE_SEGMENT: levels per warp of the segmented sweeps (4 or 8);
-  * GB_TUNE_MG_FUSED_RELAX: the zebra relaxation as one segmented launch
-    per colour or as the residual and the column solves in two launches.
+  * GB_TUNE_MG_FUSED_RELAX: the zebra relaxation as the residual and the
+    column solves in two launches (the default) or as one segmented launch
+    per colour.
 
 Every candidate performs the same arithmetic up to rounding (the segmented
 and the sequential recurrences differ only in the values carried across a
@@ -29,7 +30,7 @@ import os
 CANDIDATES = {
     "LINE_VARIANT": (0, 4),
     "LINE_SEGMENT": (0, 4, 8),
-    "MG_FUSED_RELAX": (0, 1),
+    "MG_FUSED_RELAX": (0, 4),
 }
 
 
@@ -44,7 +45,7 @@ def candidates(space=None):
     for values in itertools.product(*[space[n] for n in names]):
         c = dict(zip(names, values))
         seg_default = space.get("LINE_SEGMENT", (0,))[0]
-        if c.get("LINE_VARIANT") == 4 and c.get("MG_FUSED_RELAX") == 1 and c.get("LINE_SEGMENT", seg_default) != seg_default:
+        if c.get("LINE_VARIANT") == 4 and c.get("MG_FUSED_RELAX") == 0 and c.get("LINE_SEGMENT", seg_default) != seg_default:
             continue
         out.append(c)
     return out

@@ -456,18 +456,22 @@ __device__ __forceinline__ void zline_seg_body(const LineArgs<T>& a, T* __restri
     T* carry_x = carry_e + 2 * W * 32;                 // [2][W][32]: the affine map of x
     const int cs = W * 32;
     const int me = w * 32 + lane;
-    int64_t o0 = 0, oxm = -1, oxp = -1, oym = -1, oyp = -1;
-    if (col) {
-        const int im = lateral_image(i - 1, a.ni, g.nx, g.periodic_x != 0);
-        const int ip = lateral_image(i + 1, a.ni, g.nx, g.periodic_x != 0);
-        const int jm = lateral_image(j - 1, a.nj, g.ny, g.periodic_y != 0);
-        const int jp = lateral_image(j + 1, a.nj, g.ny, g.periodic_y != 0);
-        o0 = at(g, i, j, 0);
-        oxm = (im >= 0) ? at(g, im, j, 0) : -1;
-        oxp = (ip >= 0) ? at(g, ip, j, 0) : -1;
-        oym = (jm >= 0) ? at(g, i, jm, 0) : -1;
-        oyp = (jp >= 0) ? at(g, i, jp, 0) : -1;
-    }
+    // Every lane reads an in-range column and level (a lane past the columns
+    // reads the last one, a level past the column its top; their results are
+    // discarded), so no load sits behind a branch and a segment's loads can
+    // all be in flight together; a missing lateral neighbour reads the
+    // column itself and its term is selected away.
+    const int ic = min(i, a.ni - 1), jc = min(j, a.nj - 1);
+    const int im = lateral_image(ic - 1, a.ni, g.nx, g.periodic_x != 0);
+    const int ip = lateral_image(ic + 1, a.ni, g.nx, g.periodic_x != 0);
+    const int jm = lateral_image(jc - 1, a.nj, g.ny, g.periodic_y != 0);
+    const int jp = lateral_image(jc + 1, a.nj, g.ny, g.periodic_y != 0);
+    const int64_t o0 = at(g, ic, jc, 0);
+    const bool hxm = im >= 0, hxp = ip >= 0, hym = jm >= 0, hyp = jp >= 0;
+    const int64_t oxm = hxm ? at(g, im, jc, 0) : o0;
+    const int64_t oxp = hxp ? at(g, ip, jc, 0) : o0;
+    const int64_t oym = hym ? at(g, ic, jm, 0) : o0;
+    const int64_t oyp = hyp ? at(g, ic, jp, 0) : o0;
     const T* __restrict__ azm = a.A + GB_COEF_ZM * a.cs;
     const T* __restrict__ azp = a.A + GB_COEF_ZP * a.cs;
     const T* __restrict__ axm = a.A + GB_COEF_XM * a.cs;
@@ -479,28 +483,23 @@ __device__ __forceinline__ void zline_seg_body(const LineArgs<T>& a, T* __restri
     T r[L], lo[L], dg[L], up[L];
 #pragma unroll
     for (int q = 0; q < L; ++q) {
-        const int k = k0 + q;
-        r[q] = T(0);
-        lo[q] = T(0);
-        dg[q] = T(1);
-        up[q] = T(0);
-        if (col && k < nk) {
-            const int64_t ko = static_cast<int64_t>(k) * g.sz;
-            const int64_t o = o0 + ko;
-            r[q] = a.rhs[o];
-            lo[q] = azm[o];
-            if (FIRST) {
-                dg[q] = a.ap[o];
-                up[q] = azp[o];
-            } else {
-                dg[q] = inv_io[o];
-                up[q] = cp_io[o];
-                const T dxm = (oxm >= 0) ? a.dold[oxm + ko] : T(0);
-                const T dxp = (oxp >= 0) ? a.dold[oxp + ko] : T(0);
-                const T dym = (oym >= 0) ? a.dold[oym + ko] : T(0);
-                const T dyp = (oyp >= 0) ? a.dold[oyp + ko] : T(0);
-                r[q] = r[q] + axm[o] * dxm + axp[o] * dxp + aym[o] * dym + ayp[o] * dyp;
-            }
+        const int k = min(k0 + q, nk - 1);
+        const int64_t ko = static_cast<int64_t>(k) * g.sz;
+        const int64_t o = o0 + ko;
+        r[q] = a.rhs[o];
+        lo[q] = azm[o];
+        if (FIRST) {
+            dg[q] = a.ap[o];
+            up[q] = azp[o];
+        } else {
+            dg[q] = inv_io[o];
+            up[q] = cp_io[o];
+            const T vxm = a.dold[oxm + ko], vxp = a.dold[oxp + ko], vym = a.dold[oym + ko], vyp = a.dold[oyp + ko];
+            const T dxm = hxm ? vxm : T(0);
+            const T dxp = hxp ? vxp : T(0);
+            const T dym = hym ? vym : T(0);
+            const T dyp = hyp ? vyp : T(0);
+            r[q] = r[q] + axm[o] * dxm + axp[o] * dxp + aym[o] * dym + ayp[o] * dyp;
         }
     }
     if (FIRST) {

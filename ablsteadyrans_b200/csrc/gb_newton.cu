@@ -112,6 +112,7 @@ __global__ void k_field_sums(gb_grid g, int t, int mode, const double* __restric
 
 struct gb_newton {
     gb_simplec* S{nullptr};
+    gb_ctx* ctx{nullptr};                // the stage's context (outlives the stage)
     gb_newton_opts opt{};
     gb_grid g{};
     int64_t vol{0};
@@ -634,6 +635,7 @@ gb_status gb_newton_create(gb_simplec* s, const gb_newton_opts* o, gb_newton** o
         return GB_OOM;
     }
     n->S = s;
+    n->ctx = gb::simplec_ctx(s);
     n->opt = *o;
     n->g = gb::simplec_grid(s);
     n->vol = gb::volume(n->g);
@@ -673,7 +675,8 @@ gb_status gb_newton_create(gb_simplec* s, const gb_newton_opts* o, gb_newton** o
 gb_status gb_newton_destroy(gb_newton* n)
 {
     gb::clear_error();
-    if (n) { cudaStreamSynchronize(gb::simplec_ctx(n->S)->stream); }
+    // the context's stream, kept at creation: the stage may be gone already
+    if (n) { cudaStreamSynchronize(n->ctx->stream); }
     delete n;
     return GB_OK;
 }

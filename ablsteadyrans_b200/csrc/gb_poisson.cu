@@ -1033,13 +1033,16 @@ void mg_smooth(gb_poisson* P, PoissonLevels<T>& L, int l)
     constexpr int kFusedMaxColumns = 1024;
     const size_t smem_fused = static_cast<size_t>(5) * g.nz * kFusedCols * sizeof(T);
     const int fknob = ctx->tune[GB_TUNE_MG_FUSED_RELAX];
-    // the segmented one-launch relaxation (GB_TUNE_MG_FUSED_RELAX 0 or 4, the
-    // default): every level of a column in flight, at most 16 segments of 4
-    // levels (8 for taller columns, or as GB_TUNE_LINE_SEGMENT asks)
+    // the segmented one-launch relaxation (GB_TUNE_MG_FUSED_RELAX 4): every
+    // level of a column in flight, at most 16 segments of 4 levels (8 for
+    // taller columns, or as GB_TUNE_LINE_SEGMENT asks). Measured slower than
+    // the two launches on config 1 and on every tile shape the autotuner
+    // timed (a coarse level's few blocks each walk 4 cells' stencils per
+    // thread), so it is not the default.
     const int sknob = ctx->tune[GB_TUNE_LINE_SEGMENT];
     const int segL = (sknob == 4 || sknob == 8) ? sknob : ((g.nz + 3) / 4 <= 16 ? 4 : 8);
     const int segW = (g.nz + segL - 1) / segL;
-    const bool seg = (fknob == 0 || fknob == 4) && segW <= 16 && !(g.periodic_x && (g.nx & 1))
+    const bool seg = fknob == 4 && segW <= 16 && !(g.periodic_x && (g.nx & 1))
                      && !(g.periodic_y && (g.ny & 1));
     if (seg) {
         const dim3 block(32, segW);

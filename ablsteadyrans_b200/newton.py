@@ -93,6 +93,7 @@ class NewtonKrylov:
         self._h = ctypes.c_void_p()
         check(self._L.gb_newton_create(stage._h, ctypes.byref(self.options), ctypes.byref(self._h)))
         stage.ctx.own(self)
+        stage.own(self)
 
     def _zeros(self):
         import torch

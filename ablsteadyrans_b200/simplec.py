@@ -277,8 +277,20 @@ class SimplecStage:
                                          float(reltol), ctypes.byref(res)))
         return res
 
+    def own(self, obj):
+        """Record a native object made on this stage (a Newton core): close()
+        destroys the live ones first."""
+        import weakref
+        deps = getattr(self, "_dependents", [])
+        self._dependents = [r for r in deps if r() is not None] + [weakref.ref(obj)]
+
     def close(self):
         from . import check
+        for r in reversed(getattr(self, "_dependents", [])):
+            obj = r()
+            if obj is not None:
+                obj.close()
+        self._dependents = []
         if self._h:
             check(self._L.gb_simplec_destroy(self._h))
             self._h = ctypes.c_void_p()

@@ -111,7 +111,7 @@ enum {
                                    0 auto (= 1), 1 shared memory, 2 the global arrays (c' stored, e' in the
                                    output array), 3 e' in shared memory and c' read again from its stored
                                    array (L2): less shared memory per warp, more warps per SM */
-    GB_TUNE_MG_FUSED_RELAX,     /* one launch per colour of the zebra line relaxation: 0 auto (= 4), 1 never
+    GB_TUNE_MG_FUSED_RELAX,     /* one launch per colour of the zebra line relaxation: 0 auto (= 1), 1 never
                                    (the residual and the solve as two launches), 2 the residual in shared memory
                                    and one thread per column's solve, on every level, 3 that on the levels of at
                                    most 1024 columns, 4 segmented (the column's levels split among the warps of

@@ -15,8 +15,8 @@ def test_candidates_start_with_the_defaults_and_drop_no_op_combinations():
     keys = [json.dumps(c, sort_keys=True) for c in cands]
     assert len(keys) == len(set(keys))
     # the segment length does nothing with the sequential sweep and the two-launch relaxation
-    assert {"LINE_VARIANT": 4, "LINE_SEGMENT": 4, "MG_FUSED_RELAX": 1} not in cands
-    assert {"LINE_VARIANT": 4, "LINE_SEGMENT": 0, "MG_FUSED_RELAX": 1} in cands
+    assert {"LINE_VARIANT": 4, "LINE_SEGMENT": 4, "MG_FUSED_RELAX": 0} not in cands
+    assert {"LINE_VARIANT": 4, "LINE_SEGMENT": 0, "MG_FUSED_RELAX": 0} in cands
     assert len(cands) == 2 * 3 * 2 - 2
 
 
