@@ -585,6 +585,109 @@ __global__ void __launch_bounds__(256) k_color_relax_fused(gb_grid g, PBC b, int
     }
 }
 
+//! Zebra relaxation, second half, with the column's levels split among the
+//! warps of a block: x += T^{-1} r on every column of the colour with the
+//! factors of k_line_factor (e_k = (r_k - D_k e_{k-1}) / m_k, then x_k = e_k
+//! - c'_k x_{k+1}). A block holds 32 columns of the colour along one row and
+//! ceil(nz / L) warps; each thread loads its L levels' r, D, 1/m, c' and x at
+//! once (in-range clamped indices: no load behind a branch), runs the
+//! recurrences over them in their sequential order and carries e' upwards and
+//! the correction downwards through shared memory as each segment's affine
+//! map (the segmented z-line sweep's carries). A coarse level's few columns
+//! then keep many warps busy, where one thread per column walks every level.
+template <typename T, int L>
+__global__ void __launch_bounds__(512) k_color_solve_seg(gb_grid g, int color, const T* __restrict__ r,
+                                                         const T* __restrict__ TD, const T* __restrict__ TC,
+                                                         const T* __restrict__ TU, T* __restrict__ x)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int lane = threadIdx.x;
+    const int w = threadIdx.y;
+    const int W = blockDim.y;
+    const int j = blockIdx.y;
+    const int half = (g.nx + 1) / 2;
+    const int c = blockIdx.x * 32 + lane;
+    const bool col = c < half && 2 * c + ((j + color) & 1) < g.nx;
+    const int i = col ? 2 * c + ((j + color) & 1) : ((j + color) & 1);   // an in-range column for every lane
+    const int nz = g.nz;
+    const int k0 = w * L;
+    const int cs = W * 32;
+    const int me = w * 32 + lane;
+    T* carry_e = reinterpret_cast<T*>(smem_raw);  // [2][W][32]
+    T* carry_x = carry_e + 2 * cs;                // [2][W][32]
+    const int64_t o0 = at(g, min(i, g.nx - 1), j, 0);
+    T R[L], D[L], IM[L], CP[L], X0[L];
+#pragma unroll
+    for (int q = 0; q < L; ++q) {
+        const int64_t o = o0 + static_cast<int64_t>(min(k0 + q, nz - 1)) * g.sz;
+        R[q] = r[o];
+        D[q] = TD[o];
+        IM[q] = TC[o];
+        CP[q] = TU[o];
+        X0[q] = x[o];
+    }
+    {
+        T al = T(0), be = T(1);
+#pragma unroll
+        for (int q = 0; q < L; ++q) {
+            const int k = k0 + q;
+            if (k < nz) {
+                if (k == 0) {
+                    al = R[q] * IM[q];
+                    be = T(0);
+                } else {
+                    al = (R[q] - D[q] * al) * IM[q];
+                    be = (-D[q] * be) * IM[q];
+                }
+            }
+        }
+        carry_e[me] = al;
+        carry_e[cs + me] = be;
+    }
+    __syncthreads();
+    {
+        T ep = T(0);
+        for (int s = 0; s < w; ++s) { ep = carry_e[s * 32 + lane] + carry_e[cs + s * 32 + lane] * ep; }
+#pragma unroll
+        for (int q = 0; q < L; ++q) {
+            const int k = k0 + q;
+            if (k < nz) {
+                ep = (k == 0) ? R[q] * IM[q] : (R[q] - D[q] * ep) * IM[q];
+                R[q] = ep;
+            }
+        }
+    }
+    {
+        T ga = T(0), de = T(1);
+#pragma unroll
+        for (int q = L - 1; q >= 0; --q) {
+            const int k = k0 + q;
+            if (k < nz) {
+                if (k == nz - 1) {
+                    ga = R[q];
+                    de = T(0);
+                } else {
+                    ga = R[q] - CP[q] * ga;
+                    de = -CP[q] * de;
+                }
+            }
+        }
+        carry_x[me] = ga;
+        carry_x[cs + me] = de;
+    }
+    __syncthreads();
+    T xk = T(0);
+    for (int s = W - 1; s > w; --s) { xk = carry_x[s * 32 + lane] + carry_x[cs + s * 32 + lane] * xk; }
+#pragma unroll
+    for (int q = L - 1; q >= 0; --q) {
+        const int k = k0 + q;
+        if (k < nz) {
+            xk = (k == nz - 1) ? R[q] : R[q] - CP[q] * xk;
+            if (col) { x[o0 + static_cast<int64_t>(k) * g.sz] = X0[q] + xk; }
+        }
+    }
+}
+
 //! One colour's relaxation in ONE launch with every level of a column in
 //! flight: a block holds 32 columns of the colour along one row and
 //! ceil(nz / L) warps; warp w owns levels [w L, w L + L) of every column. Each
@@ -1087,7 +1190,19 @@ void mg_smooth(gb_poisson* P, PoissonLevels<T>& L, int l)
         k_color_residual<T><<<rgrid, dim3(32, 4), 0, ctx->stream>>>(g, b, color, L.x[l], L.bv[l], L.AX[l], L.AY[l],
                                                                    L.AZ[l], L.J[l], L.ratios(l), L.r[l]);
         const dim3 sgrid((half + nthr - 1) / nthr, g.ny);
-        if (staged) {
+        const int sL = (g.nz + 7) / 8 <= 16 ? 8 : 16;
+        const int sW = (g.nz + sL - 1) / sL;
+        if (ctx->tune[GB_TUNE_MG_SOLVE] != 1 && sW <= 16) {
+            // the segmented column solves (the default; GB_TUNE_MG_SOLVE = 1: one thread per column)
+            const size_t sm = static_cast<size_t>(4) * sW * 32 * sizeof(T);
+            if (sL == 8) {
+                k_color_solve_seg<T, 8><<<dim3((half + 31) / 32, g.ny), dim3(32, sW), sm, ctx->stream>>>(
+                    g, color, L.r[l], L.TD[l], L.TC[l], L.TU[l], L.x[l]);
+            } else {
+                k_color_solve_seg<T, 16><<<dim3((half + 31) / 32, g.ny), dim3(32, sW), sm, ctx->stream>>>(
+                    g, color, L.r[l], L.TD[l], L.TC[l], L.TU[l], L.x[l]);
+            }
+        } else if (staged) {
             k_color_solve_staged<T><<<sgrid, nthr, smem_staged, ctx->stream>>>(g, color, L.r[l], L.TD[l], L.TC[l],
                                                                               L.TU[l], L.x[l]);
         } else {

@@ -118,6 +118,8 @@ enum {
                                    a block, the residual in registers; columns of more than 128 levels: 1) */
     GB_TUNE_GRAPHS,             /* CUDA graphs for launch sequences without a host synchronisation (the
                                    multigrid V-cycle): 0 default (on), 1 off (every kernel launched alone) */
+    GB_TUNE_MG_SOLVE,           /* the column solves of the two-launch zebra relaxation: 0 default (the
+                                   column's levels split among the warps of a block), 1 one thread per column */
     GB_TUNE_LINE_SEGMENT,       /* levels per warp of the segmented z-line sweep (default 8) and of the
                                    segmented zebra relaxation (default 4, 8 for columns of more than 64
                                    levels): 0 default, 4 or 8 */
