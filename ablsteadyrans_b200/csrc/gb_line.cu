@@ -35,6 +35,7 @@ struct LineArgs {
     T* __restrict__ ebuf;
     int first;  // dold == 0: no neighbour terms, change against 0
     unsigned long long* change;  // max |dnew - dold| (nullptr: not wanted)
+    const T* __restrict__ rfold;  // rhs with the lagged lateral terms folded in (the split sweep)
 };
 
 template <typename T, bool SMEM>
@@ -382,6 +383,7 @@ struct MultiLineArgs {
     LineArgs<T> a[kMaxLineSystems];
     T* inv[kMaxLineSystems];
     T* cp[kMaxLineSystems];
+    T* fold[kMaxLineSystems];  // the split sweep's folded right-hand sides
 };
 
 template <typename T, bool FIRST, int R, int S, int BACK>
@@ -438,7 +440,7 @@ __device__ __forceinline__ void seg_pow2_normalise(T& a, T& b, T& c, T& d)
     }
 }
 
-template <typename T, bool FIRST, int L>
+template <typename T, bool FIRST, int L, bool PREF = false>
 __device__ __forceinline__ void zline_seg_body(const LineArgs<T>& a, T* __restrict__ inv_io, T* __restrict__ cp_io)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -491,6 +493,10 @@ __device__ __forceinline__ void zline_seg_body(const LineArgs<T>& a, T* __restri
         if (FIRST) {
             dg[q] = a.ap[o];
             up[q] = azp[o];
+        } else if (PREF) {
+            r[q] = a.rfold[o];
+            dg[q] = inv_io[o];
+            up[q] = cp_io[o];
         } else {
             dg[q] = inv_io[o];
             up[q] = cp_io[o];
@@ -649,6 +655,53 @@ __global__ void __launch_bounds__(512) zline_seg_kernel(LineArgs<T> a, T* __rest
     zline_seg_body<T, FIRST, L>(a, inv_io, cp_io);
 }
 
+//! The split sweep's first half: the right-hand side with the lagged lateral
+//! terms, r' = rhs + a_XM d_XM + a_XP d_XP + a_YM d_YM + a_YP d_YP (the
+//! segmented sweep's fold, in its operation order), one thread per point,
+//! for every system of the launch (blockIdx.z = system * nk + k). The column
+//! solves then read r' in place of the nine values the fold needs: a fully
+//! parallel pass and a light one instead of one with a heavy load phase.
+template <typename T>
+__device__ __forceinline__ void line_fold_point(const LineArgs<T>& a, T* __restrict__ out, int i, int j, int k)
+{
+    if (i >= a.ni || j >= a.nj || k >= a.nk) { return; }
+    const gb_grid& g = a.g;
+    const int im = lateral_image(i - 1, a.ni, g.nx, g.periodic_x != 0);
+    const int ip = lateral_image(i + 1, a.ni, g.nx, g.periodic_x != 0);
+    const int jm = lateral_image(j - 1, a.nj, g.ny, g.periodic_y != 0);
+    const int jp = lateral_image(j + 1, a.nj, g.ny, g.periodic_y != 0);
+    const int64_t o = at(g, i, j, k);
+    const T dxm = (im >= 0) ? a.dold[at(g, im, j, k)] : T(0);
+    const T dxp = (ip >= 0) ? a.dold[at(g, ip, j, k)] : T(0);
+    const T dym = (jm >= 0) ? a.dold[at(g, i, jm, k)] : T(0);
+    const T dyp = (jp >= 0) ? a.dold[at(g, i, jp, k)] : T(0);
+    out[o] = a.rhs[o] + a.A[GB_COEF_XM * a.cs + o] * dxm + a.A[GB_COEF_XP * a.cs + o] * dxp
+           + a.A[GB_COEF_YM * a.cs + o] * dym + a.A[GB_COEF_YP * a.cs + o] * dyp;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(128) k_line_fold(MultiLineArgs<T> m, int nkmax)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y;
+    const int s = blockIdx.z / nkmax, k = blockIdx.z % nkmax;
+    switch (s) {
+    case 0: line_fold_point<T>(m.a[0], m.fold[0], i, j, k); break;
+    case 1: line_fold_point<T>(m.a[1], m.fold[1], i, j, k); break;
+    default: line_fold_point<T>(m.a[2], m.fold[2], i, j, k); break;
+    }
+}
+
+template <typename T, int L>
+__global__ void __launch_bounds__(512) zline_seg_pref_multi_kernel(MultiLineArgs<T> m)
+{
+    switch (blockIdx.z) {
+    case 0: zline_seg_body<T, false, L, true>(m.a[0], m.inv[0], m.cp[0]); break;
+    case 1: zline_seg_body<T, false, L, true>(m.a[1], m.inv[1], m.cp[1]); break;
+    default: zline_seg_body<T, false, L, true>(m.a[2], m.inv[2], m.cp[2]); break;
+    }
+}
+
 //! The segmented sweep over several systems (MultiLineArgs; blockIdx.z picks
 //! the system, with constant indices into the parameter block).
 template <typename T, bool FIRST, int L>
@@ -746,46 +799,15 @@ gb_status zline_sweeps(gb_ctx* ctx, const gb_grid& g, int loc, const T* A, const
     }
     if (scratch_kind == LineScratch::segmented && segW == 0) { scratch_kind = LineScratch::factored; }
     if (scratch_kind == LineScratch::segmented) {
-        T* inv = static_cast<T*>(scratch(ctx, kSlotLineInv, sizeof(T) * vol));
-        T* cpr = static_cast<T*>(scratch(ctx, kSlotLineCp, sizeof(T) * vol));
-        if (inv == nullptr || cpr == nullptr) { return GB_OOM; }
-        T* buf[2] = {delta, tmp};
-        if (change_word != nullptr) { cudaMemsetAsync(change_word, 0, sizeof(unsigned long long), ctx->stream); }
-        const dim3 block(32, segW);
-        const dim3 grid((ni + 31) / 32, nj);
-        const size_t sm = seg_smem_bytes<T>(segW);
-        for (int s = 0; s < sweeps; ++s) {
-            LineArgs<T> a{};
-            a.g = g;
-            a.ni = ni;
-            a.nj = nj;
-            a.nk = nk;
-            a.A = A;
-            a.cs = vol;
-            a.ap = ap;
-            a.rhs = rhs;
-            a.dold = buf[(sweeps - s) & 1];
-            a.dnew = buf[(sweeps - 1 - s) & 1];
-            a.first = (s == 0) ? 1 : 0;
-            a.change = (s == sweeps - 1) ? change_word : nullptr;
-            Span span(ctx, GB_KERNEL_LINE_SWEEP);
-            if (segL == 4) {
-                if (a.first) {
-                    zline_seg_kernel<T, true, 4><<<grid, block, sm, ctx->stream>>>(a, inv, cpr);
-                } else {
-                    zline_seg_kernel<T, false, 4><<<grid, block, sm, ctx->stream>>>(a, inv, cpr);
-                }
-            } else {
-                if (a.first) {
-                    zline_seg_kernel<T, true, 8><<<grid, block, sm, ctx->stream>>>(a, inv, cpr);
-                } else {
-                    zline_seg_kernel<T, false, 8><<<grid, block, sm, ctx->stream>>>(a, inv, cpr);
-                }
-            }
-            ++ctx->launches;
-        }
-        seam_sync<T>(ctx, g, loc, delta);
-        return check_cuda("zline_jacobi");
+        // one system through the batched form (the segmented kernels, and the
+        // split form with GB_TUNE_LINE_VARIANT 6)
+        const int locs[1] = {loc};
+        const T* As[1] = {A};
+        const T* aps[1] = {ap};
+        const T* rhss[1] = {rhs};
+        T* deltas[1] = {delta};
+        unsigned long long* words[1] = {change_word};
+        return zline_sweeps_multi<T>(ctx, g, 1, locs, As, aps, rhss, sweeps, deltas, words);
     }
     const bool factored = (scratch_kind == LineScratch::factored);
     const bool pipelined = factored || (scratch_kind == LineScratch::pipelined);
@@ -933,6 +955,15 @@ gb_status zline_sweeps_multi(gb_ctx* ctx, const gb_grid& g, int n, const int* lo
         const dim3 block(32, segW);
         const dim3 grid((max_ni + 31) / 32, max_nj, n);
         const size_t sm = seg_smem_bytes<T>(segW);
+        // GB_TUNE_LINE_VARIANT 6: the later sweeps split into the fold and light column solves
+        const bool split = ctx->tune[GB_TUNE_LINE_VARIANT] == 6 && sweeps > 1;
+        T* fold[kMaxLineSystems] = {};
+        if (split) {
+            for (int s = 0; s < n; ++s) {
+                fold[s] = static_cast<T*>(scratch(ctx, kSlotMultiBase + 3 * kMaxLineSystems + s, sizeof(T) * vol));
+                if (!fold[s]) { return GB_OOM; }
+            }
+        }
         for (int k = 0; k < sweeps; ++k) {
             MultiLineArgs<T> m{};
             for (int s = 0; s < n; ++s) {
@@ -950,10 +981,23 @@ gb_status zline_sweeps_multi(gb_ctx* ctx, const gb_grid& g, int n, const int* lo
                 a.dnew = buf[(sweeps - 1 - k) & 1];
                 a.first = (k == 0) ? 1 : 0;
                 a.change = (k == sweeps - 1 && change_words != nullptr) ? change_words[s] : nullptr;
+                a.rfold = fold[s];
                 m.inv[s] = inv[s];
                 m.cp[s] = cpr[s];
+                m.fold[s] = fold[s];
             }
             Span span(ctx, GB_KERNEL_LINE_SWEEP);
+            if (split && k > 0) {
+                const dim3 fgrid((max_ni + 127) / 128, max_nj, max_nk * n);
+                k_line_fold<T><<<fgrid, 128, 0, ctx->stream>>>(m, max_nk);
+                if (segL == 4) {
+                    zline_seg_pref_multi_kernel<T, 4><<<grid, block, sm, ctx->stream>>>(m);
+                } else {
+                    zline_seg_pref_multi_kernel<T, 8><<<grid, block, sm, ctx->stream>>>(m);
+                }
+                ctx->launches += 2;
+                continue;
+            }
             if (segL == 4) {
                 if (k == 0) {
                     zline_seg_multi_kernel<T, true, 4><<<grid, block, sm, ctx->stream>>>(m);

@@ -101,7 +101,9 @@ enum {
     GB_TUNE_LINE_VARIANT = 0,   /* z-line sweep kernel: 0 auto (= 5), 1 pipelined (cp.async ring), 2 shared,
                                    3 global scratch, 4 pipelined with the column factors kept between sweeps,
                                    5 segmented: the column's levels split among the warps of a block, the
-                                   factors kept between sweeps (columns of more than 128 levels: 4) */
+                                   factors kept between sweeps (columns of more than 128 levels: 4), 6 the
+                                   segmented sweep with each later sweep split into the fold of the lagged
+                                   lateral terms (one thread per point) and the column solves */
     GB_TUNE_LINE_BLOCK,         /* threads per block of the pipelined sweep (32, 64 or 128; 0 = default) */
     GB_TUNE_MG_COARSE_KERNEL,   /* the coarsest level's relaxations: 0 auto (one single-block launch when the
                                    level has at most 64 columns), 1 the per-relaxation launches */

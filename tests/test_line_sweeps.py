@@ -96,13 +96,16 @@ def test_gpu_zline_jacobi_matches_oracle_fp64(ctx, loc, case, sweeps):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("variant,segment", [(4, 0), (5, 4), (5, 8)], ids=["factored", "segmented4", "segmented8"])
+@pytest.mark.parametrize("variant,segment", [(4, 0), (5, 4), (5, 8), (6, 8)],
+                         ids=["factored", "segmented4", "segmented8", "split8"])
 @pytest.mark.parametrize("loc", LOCS)
 @pytest.mark.parametrize("case", [(37, 29, 17, True, False), (64, 48, 65, False, True), (33, 20, 128, True, True)])
 def test_gpu_zline_jacobi_kernels_match_oracle(ctx, variant, segment, loc, case):
-    """The sequential factored sweep (GB_TUNE_LINE_VARIANT 4) and the
-    segmented one with 4 or 8 levels per warp (5, the default) agree with the
-    oracle's column solves to 1e-12, on columns of 17 to 129 levels."""
+    """The sequential factored sweep (GB_TUNE_LINE_VARIANT 4), the segmented
+    one with 4 or 8 levels per warp (5, the default) and the segmented one
+    with the later sweeps split into the fold and the column solves (6)
+    agree with the oracle's column solves to 1e-12, on columns of 17 to 129
+    levels."""
     import torch
     import ablsteadyrans_b200 as gb
     nx, ny, nz, px, py = case
