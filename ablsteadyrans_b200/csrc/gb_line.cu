@@ -425,19 +425,37 @@ __global__ void __launch_bounds__(128) zline_fact_multi_kernel(MultiLineArgs<T> 
 //! FIRST: the first sweep of a solve (zero iterate, no lateral terms): it
 //! also stores the column factors 1/m and c' for the later sweeps, which read
 //! them in place of a_P and a_ZP (as zline_fact_body).
+//! 2^-e for a finite positive normal s = m 2^e (m in [1, 2)), from the
+//! exponent bits (1 for 0, a subnormal, inf or NaN): the scale that brings s
+//! into [1, 2) by an exact multiplication.
+__device__ __forceinline__ double pow2_inverse_scale(double s)
+{
+    const long long b = __double_as_longlong(s);
+    const int eb = static_cast<int>((b >> 52) & 0x7ff);
+    if (eb == 0 || eb == 0x7ff) { return 1.0; }
+    return __longlong_as_double(static_cast<long long>(2046 - eb) << 52);
+}
+
+__device__ __forceinline__ float pow2_inverse_scale(float s)
+{
+    const int b = __float_as_int(s);
+    const int eb = (b >> 23) & 0xff;
+    if (eb == 0 || eb == 0xff) { return 1.0f; }
+    return __int_as_float((254 - eb) << 23);
+}
+
+//! The four entries of a projective map scaled by one power of two (exact)
+//! so that the largest magnitude lies in [1, 2): the map is unchanged and
+//! the entries neither overflow nor underflow along a segment's product.
 template <typename T>
 __device__ __forceinline__ void seg_pow2_normalise(T& a, T& b, T& c, T& d)
 {
     const T s = fmax(fmax(fabs(a), fabs(b)), fmax(fabs(c), fabs(d)));
-    if (s > T(0) && s == s && s < T(INFINITY)) {
-        int e;
-        frexp(s, &e);
-        const T f = ldexp(T(1), -e);  // a power of two: the scaling is exact
-        a *= f;
-        b *= f;
-        c *= f;
-        d *= f;
-    }
+    const T f = pow2_inverse_scale(s);
+    a *= f;
+    b *= f;
+    c *= f;
+    d *= f;
 }
 
 template <typename T, bool FIRST, int L, bool PREF = false>

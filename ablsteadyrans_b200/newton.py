@@ -387,6 +387,30 @@ def newton_equations_differ(stage):
     return bool(ph.closure) and ph.turb_nut_relax < 1.0
 
 
+def newton_stage_action(verdict, idle, monitor_window, status, converged_now, differs, failures, fallback_failures):
+    """What the two-stage driver does after one Newton-stage iteration, in the
+    reference's order: the criterion's verdict first (Driver::step,
+    Driver.cpp:403-468: a steady or diverged verdict ends the run whatever
+    the stage asks), then the stage's requests (NewtonStage::iterate,
+    NewtonStage.cpp:127-178): a hand-back for good after sitting converged
+    for more than steady.monitor_window iterations (idle) or after
+    converging on equations that differ from the run's (differs), the
+    fall-back after steady.newton_fallback_failures failed steps. verdict:
+    "steady", "diverged" or "running"; status: the continuation step's
+    outcome. Returns (action, reason): action "steady", "diverged",
+    "hand_back", "fallback" or "continue"."""
+    if verdict in ("steady", "diverged"):
+        return verdict, ""
+    if idle > monitor_window:
+        return "hand_back", "Newton converged but the steady criterion did not hold for steady.monitor_window iterations"
+    if failures >= fallback_failures:
+        return "fallback", f"{failures} consecutive failed Newton steps"
+    if status == "accepted" and converged_now and differs:
+        return "hand_back", ("Newton converged on its own equations, which differ from the run's (turb.nut_relax < 1): "
+                             "the final SIMPLEC pass")
+    return "continue", ""
+
+
 def solve_simplec_newton(stage, max_iterations, driver_options=None, switch=None, newton_options=None,
                          continuation_options=None, events=None):
     """steady.stage = simplec_newton on one stage: the native SIMPLEC driver
@@ -437,12 +461,9 @@ def solve_simplec_newton(stage, max_iterations, driver_options=None, switch=None
             # (|R| <= 10^-residual_drop_orders |R_0|) no step is taken: the
             # norms fill the criterion's monitor window (NewtonStage.H)
             done = cont.st.steps > 0 and cont.st.r0 > 0 and cont.st.r_last <= drop * cont.st.r0
-            hand_back = None
             if done:
                 idle += 1
                 status = "accepted"
-                if idle > o.monitor_window:
-                    hand_back = "Newton converged but the steady criterion did not hold for steady.monitor_window iterations"
             else:
                 status = cont.step()
                 newton_its += 1
@@ -450,20 +471,18 @@ def solve_simplec_newton(stage, max_iterations, driver_options=None, switch=None
             res, mon = stage.norms()
             crit.add(res, mon[:n_mon])
             v = crit.verdict()
-            if v.status == abi.DIVERGED:
-                return "diverged", it + 1, newton_its
-            if v.status == abi.STEADY:
-                return "steady", it + 1, newton_its
+            verdict = "diverged" if v.status == abi.DIVERGED else ("steady" if v.status == abi.STEADY else "running")
             converged_now = (not done and status == "accepted" and cont.st.steps > 0 and cont.st.r0 > 0
                              and cont.st.r_last <= drop * cont.st.r0)
-            if hand_back is None and converged_now and newton_equations_differ(stage):
-                hand_back = ("Newton converged on its own equations, which differ from the run's (turb.nut_relax < 1): "
-                             "the final SIMPLEC pass")
-            if hand_back is not None:
+            action, reason = newton_stage_action(verdict, idle, o.monitor_window, status, converged_now,
+                                                 newton_equations_differ(stage), failures, sw.fallback_failures)
+            if action in ("steady", "diverged"):
+                return action, it + 1, newton_its
+            if action == "hand_back":
                 handed_back = True
-                mode, below = switch_to(it, "simplec", hand_back), 0
-            elif failures >= sw.fallback_failures:
-                mode, below = switch_to(it, "simplec", f"{failures} consecutive failed Newton steps"), 0
+                mode, below = switch_to(it, "simplec", reason), 0
+            elif action == "fallback":
+                mode, below = switch_to(it, "simplec", reason), 0
         return "running", max_iterations, newton_its
     finally:
         if cont is not None:

@@ -38,12 +38,16 @@ def gpu_stage(ctx, oc, inst, options=None):
 
 
 def field_errors(grid, got, ref):
-    """Per field: max |got - ref| over the valid points / max |ref| (the
-    field's scale; 1 for a field that is zero everywhere)."""
+    """Per field: max |got - ref| over the valid points over the field's
+    scale: the velocity magnitude max(|u|, |v|, |w|) for u, v and w (a
+    component that is zero up to rounding, such as v over flat ground with
+    a wind along x, has no scale of its own), max |ref| for the others (1
+    for a field that is zero everywhere)."""
+    vel = max(float(np.abs(ref[f][grid.valid(loc)]).max()) for f, loc in zip(FIELDS[:3], LOCS[:3]))
     out = {}
     for f, loc in zip(FIELDS, LOCS):
         v = grid.valid(loc)
-        scale = float(np.abs(ref[f][v]).max())
+        scale = vel if f in ("u", "v", "w") else float(np.abs(ref[f][v]).max())
         out[f] = float(np.abs(got[f][v] - ref[f][v]).max()) / (scale if scale > 0 else 1.0)
     return out
 
