@@ -975,6 +975,21 @@ gb_status zline_sweeps_multi(gb_ctx* ctx, const gb_grid& g, int n, const int* lo
         const size_t sm = seg_smem_bytes<T>(segW);
         // GB_TUNE_LINE_VARIANT 6: the later sweeps split into the fold and light column solves
         const bool split = ctx->tune[GB_TUNE_LINE_VARIANT] == 6 && sweeps > 1;
+        // GB_TUNE_LINE_FIRST 2: the first sweep (the factorisation) by the sequential factored kernel,
+        // which stores the same factors (1/m, c') the segmented later sweeps read
+        constexpr int RF = (sizeof(T) == 8) ? 4 : 8;
+        const bool fact_first = ctx->tune[GB_TUNE_LINE_FIRST] == 2;
+        const size_t fsm = static_cast<size_t>(RF * 4 + 2 * max_nk) * 32 * sizeof(T);
+        if (fact_first) {
+            static std::atomic<bool> ff_attr[2];
+            const int ti = sizeof(T) == 8 ? 1 : 0;
+            if (!ff_attr[ti].load()) {
+                cudaFuncSetAttribute(zline_fact_multi_kernel<T, true, RF, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     200 * 1024);
+                ff_attr[ti].store(true);
+            }
+            if (fsm > 200 * 1024) { return GB_BAD_ARG; }
+        }
         T* fold[kMaxLineSystems] = {};
         if (split) {
             for (int s = 0; s < n; ++s) {
@@ -1005,6 +1020,12 @@ gb_status zline_sweeps_multi(gb_ctx* ctx, const gb_grid& g, int n, const int* lo
                 m.fold[s] = fold[s];
             }
             Span span(ctx, GB_KERNEL_LINE_SWEEP);
+            if (fact_first && k == 0) {
+                const dim3 fgrid((max_ni + 31) / 32, max_nj, n);
+                zline_fact_multi_kernel<T, true, RF, 0><<<fgrid, 32, fsm, ctx->stream>>>(m);
+                ++ctx->launches;
+                continue;
+            }
             if (split && k > 0) {
                 const dim3 fgrid((max_ni + 127) / 128, max_nj, max_nk * n);
                 k_line_fold<T><<<fgrid, 128, 0, ctx->stream>>>(m, max_nk);

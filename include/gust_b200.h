@@ -122,6 +122,8 @@ enum {
                                    multigrid V-cycle): 0 default (on), 1 off (every kernel launched alone) */
     GB_TUNE_MG_SOLVE,           /* the column solves of the two-launch zebra relaxation: 0 default (the
                                    column's levels split among the warps of a block), 1 one thread per column */
+    GB_TUNE_LINE_FIRST,         /* the first sweep of a segmented solve (the column factorisation): 0 default
+                                   (= 1), 1 segmented, 2 the sequential factored kernel (the same factors) */
     GB_TUNE_LINE_SEGMENT,       /* levels per warp of the segmented z-line sweep (default 8) and of the
                                    segmented zebra relaxation (default 4, 8 for columns of more than 64
                                    levels): 0 default, 4 or 8 */

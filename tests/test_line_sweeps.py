@@ -96,16 +96,17 @@ def test_gpu_zline_jacobi_matches_oracle_fp64(ctx, loc, case, sweeps):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("variant,segment", [(4, 0), (5, 4), (5, 8), (6, 8)],
-                         ids=["factored", "segmented4", "segmented8", "split8"])
+@pytest.mark.parametrize("variant,segment,first", [(4, 0, 0), (5, 4, 0), (5, 8, 0), (6, 8, 0), (5, 8, 2), (6, 4, 2)],
+                         ids=["factored", "segmented4", "segmented8", "split8", "hybrid8", "hybrid-split4"])
 @pytest.mark.parametrize("loc", LOCS)
 @pytest.mark.parametrize("case", [(37, 29, 17, True, False), (64, 48, 65, False, True), (33, 20, 128, True, True)])
-def test_gpu_zline_jacobi_kernels_match_oracle(ctx, variant, segment, loc, case):
+def test_gpu_zline_jacobi_kernels_match_oracle(ctx, variant, segment, first, loc, case):
     """The sequential factored sweep (GB_TUNE_LINE_VARIANT 4), the segmented
-    one with 4 or 8 levels per warp (5, the default) and the segmented one
-    with the later sweeps split into the fold and the column solves (6)
-    agree with the oracle's column solves to 1e-12, on columns of 17 to 129
-    levels."""
+    one with 4 or 8 levels per warp (5, the default), the segmented one
+    with the later sweeps split into the fold and the column solves (6),
+    and either segmented form after a first sweep (the factorisation) by the
+    factored kernel (GB_TUNE_LINE_FIRST 2) agree with the oracle's column
+    solves to 1e-12, on columns of 17 to 129 levels."""
     import torch
     import ablsteadyrans_b200 as gb
     nx, ny, nz, px, py = case
@@ -115,12 +116,14 @@ def test_gpu_zline_jacobi_kernels_match_oracle(ctx, variant, segment, loc, case)
     ch_ref = oracle.zline_jacobi(g, loc, A, ap, rhs, 3, d_ref)
     ctx.tune(gb.TUNE_LINE_VARIANT, variant)
     ctx.tune(gb.TUNE_LINE_SEGMENT, segment)
+    ctx.tune(gb.TUNE_LINE_FIRST, first)
     try:
         dd = torch.full(g.shape, 7.0, dtype=torch.float64, device="cuda")
         ch = gb.zline_jacobi(ctx, g, loc, to_dev(A), to_dev(ap), to_dev(rhs), 3, dd)
     finally:
         ctx.tune(gb.TUNE_LINE_VARIANT, 0)
         ctx.tune(gb.TUNE_LINE_SEGMENT, 0)
+        ctx.tune(gb.TUNE_LINE_FIRST, 0)
     assert rel_err(to_host(dd), d_ref, g.valid(loc)) < 1e-12
     assert abs(ch - ch_ref) <= 1e-12 * max(abs(ch_ref), 1e-300)
 
@@ -259,9 +262,11 @@ def test_gpu_batched_sweep_back_substitution_placement_is_bitwise_neutral(ctx, p
 @pytest.mark.parametrize("precision", [0, 1])
 def test_gpu_fused_zebra_relaxation_is_bitwise_neutral(ctx, precision):
     """The multigrid's zebra relaxation as one launch per colour (the
-    residual kept in shared memory) or as the residual and the solve in two
-    launches: the same arithmetic in the same order, so three SIMPLEC
-    iterations give identical fields."""
+    residual kept in shared memory) or as the residual and the sequential
+    column solve (GB_TUNE_MG_SOLVE 1) in two launches: the same arithmetic
+    in the same order, so three SIMPLEC iterations give identical fields.
+    (The default segmented column solve carries e' and x across segments
+    and is held to the oracle's V-cycle with a tolerance instead.)"""
     import ablsteadyrans_b200 as gb
     from ablsteadyrans_b200 import workloads
     from ablsteadyrans_b200.simplec import DeviceCase, SimplecStage
@@ -269,6 +274,7 @@ def test_gpu_fused_zebra_relaxation_is_bitwise_neutral(ctx, precision):
     for mode in (2, 1):
         inst = workloads.tile(40, 24, 3, precision=precision)
         ctx.tune(gb.TUNE_MG_FUSED_RELAX, mode)
+        ctx.tune(gb.TUNE_MG_SOLVE, 1)
         J, ax, ay, az, _ = oracle.metrics(inst.grid, inst.z)
         dc = DeviceCase(inst.grid, inst.z, J, ax, ay, az, inst.nu, inst.gamma_theta, inst.gamma_tke, inst.q, inst.z0map)
         st = SimplecStage(ctx, dc, inst.bc, inst.physics, inst.options)
@@ -278,5 +284,6 @@ def test_gpu_fused_zebra_relaxation_is_bitwise_neutral(ctx, precision):
         out.append({f: dc.host(f) for f in ("u", "v", "w", "p", "theta", "tke")})
         st.close()
     ctx.tune(gb.TUNE_MG_FUSED_RELAX, 0)
+    ctx.tune(gb.TUNE_MG_SOLVE, 0)
     for f in out[0]:
         assert np.array_equal(out[0][f], out[1][f]), f
