@@ -16,11 +16,15 @@ namespace gb {
 
 // ---------------------------------------------------------------- layout ---
 
-//! Element offset of point (i, j, k) of any location type.
+//! Element offset of point (i, j, k) of any location type. The arithmetic is
+//! 32-bit (an accepted grid has fewer than 2^31 points, check_grid), widened
+//! once: the offsets of a stencil's points from one (i, j, k) then differ by
+//! constants the compiler folds, where 64-bit products of each point's
+//! indices cost several instructions per load.
 __host__ __device__ __forceinline__ int64_t at(const gb_grid& g, int i, int j, int k)
 {
-    return static_cast<int64_t>(i + g.ng) + static_cast<int64_t>(j + g.ng) * g.sy
-         + static_cast<int64_t>(k + g.ng) * g.sz;
+    return static_cast<int64_t>((i + g.ng) + (j + g.ng) * static_cast<int32_t>(g.sy)
+                                + (k + g.ng) * static_cast<int32_t>(g.sz));
 }
 
 __host__ __device__ __forceinline__ int64_t volume(const gb_grid& g)

@@ -118,6 +118,11 @@ gb_status check_grid(const char* op, const gb_grid* g)
         set_error("gust: %s: grid cell sizes must be > 0", op);
         return GB_BAD_ARG;
     }
+    if (volume(*g) > INT32_MAX) {
+        set_error("gust: %s: grid of %lld padded points (at most 2^31 - 1: 32-bit point offsets)", op,
+                  static_cast<long long>(volume(*g)));
+        return GB_BAD_ARG;
+    }
     return GB_OK;
 }
 

@@ -408,7 +408,7 @@ __global__ void __launch_bounds__(128) zline_fact_multi_kernel(MultiLineArgs<T> 
 }
 
 //! The segmented sweep: the column's levels split among the warps of a block.
-//! A block holds 32 columns (consecutive i of one j) and ceil(nk / L) warps;
+//! A block holds 32 consecutive columns in (j, i) order and ceil(nk / L) warps;
 //! warp w owns levels [w L, w L + L) of every column, loads all of them at
 //! once into registers (every load of a thread is independent, so the memory
 //! latency is paid once per segment, not once per level) and runs the Thomas
@@ -465,9 +465,12 @@ __device__ __forceinline__ void zline_seg_body(const LineArgs<T>& a, T* __restri
     const int lane = threadIdx.x;
     const int w = threadIdx.y;
     const int W = blockDim.y;
-    const int i = blockIdx.x * 32 + lane;
-    const int j = blockIdx.y;
-    const bool col = (i < a.ni) && (j < a.nj);
+    // 32 consecutive columns in (j, i) order: a block is never mostly past
+    // the end of a row (a face system's rows are one column longer than 32 k)
+    const int c = blockIdx.x * 32 + lane;
+    const int i = c % a.ni;
+    const int j = c / a.ni;
+    const bool col = c < a.ni * a.nj;
     const int k0 = w * L;
     const int nk = a.nk;
     const gb_grid& g = a.g;
@@ -721,9 +724,14 @@ __global__ void __launch_bounds__(512) zline_seg_pref_multi_kernel(MultiLineArgs
 }
 
 //! The segmented sweep over several systems (MultiLineArgs; blockIdx.z picks
-//! the system, with constant indices into the parameter block).
+//! the system, with constant indices into the parameter block). At most 96
+//! registers a thread (no spills at L = 8): an SM's register file is split
+//! among its 4 schedulers, and two blocks of 9 warps place 5 warps on one of
+//! them, which 96 registers a thread fit (5 x 96 x 32 <= 16 K) and the 104
+//! the compiler picks unbounded do not: a second block per SM then doubles
+//! the warps that hide the segment loads' latency.
 template <typename T, bool FIRST, int L>
-__global__ void __launch_bounds__(512) zline_seg_multi_kernel(MultiLineArgs<T> m)
+__global__ void __maxnreg__(96) zline_seg_multi_kernel(MultiLineArgs<T> m)
 {
     switch (blockIdx.z) {
     case 0: zline_seg_body<T, FIRST, L>(m.a[0], m.inv[0], m.cp[0]); break;
@@ -971,7 +979,9 @@ gb_status zline_sweeps_multi(gb_ctx* ctx, const gb_grid& g, int n, const int* lo
     const int segW = seg_warps(max_nk, segL);
     if (ctx->tune[GB_TUNE_LINE_VARIANT] != 4 && segW > 0) {
         const dim3 block(32, segW);
-        const dim3 grid((max_ni + 31) / 32, max_nj, n);
+        int max_cols = 0;
+        for (int s = 0; s < n; ++s) { max_cols = std::max(max_cols, ni[s] * nj[s]); }
+        const dim3 grid((max_cols + 31) / 32, 1, n);
         const size_t sm = seg_smem_bytes<T>(segW);
         // GB_TUNE_LINE_VARIANT 6: the later sweeps split into the fold and light column solves
         const bool split = ctx->tune[GB_TUNE_LINE_VARIANT] == 6 && sweeps > 1;

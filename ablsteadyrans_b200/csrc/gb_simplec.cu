@@ -665,7 +665,30 @@ __device__ __forceinline__ double slope_dp(const double* z, const double* p, con
     return s * dp * (1.0 / g.dzeta);
 }
 
-//! R_c += (G p)_c (MassFlux.cpp:138-179) fused into the residual.
+//! Component C of the pressure gradient (G p)_C at a valid point of its
+//! face type (MassFlux.cpp:138-179).
+template <int C>
+__device__ __forceinline__ double pressure_gradient_at(const double* __restrict__ p, const double* __restrict__ z,
+                                                       const double* __restrict__ J, const double* __restrict__ ax,
+                                                       const double* __restrict__ ay, const gb_grid& g, int i, int j,
+                                                       int k)
+{
+    if (C == 0) {
+        const double cross = 0.25 * ((slope_dp<0>(z, p, g, i - 1, j, k) + slope_dp<0>(z, p, g, i, j, k))
+                                     + (slope_dp<0>(z, p, g, i - 1, j, k + 1) + slope_dp<0>(z, p, g, i, j, k + 1)));
+        return (ax[at(g, i, j, k)] * (p[at(g, i, j, k)] - p[at(g, i - 1, j, k)]) * (1.0 / g.dx) - cross)
+             / interp<CC, XF>(J, g, i, j, k);
+    }
+    if (C == 1) {
+        const double cross = 0.25 * ((slope_dp<1>(z, p, g, i, j - 1, k) + slope_dp<1>(z, p, g, i, j, k))
+                                     + (slope_dp<1>(z, p, g, i, j - 1, k + 1) + slope_dp<1>(z, p, g, i, j, k + 1)));
+        return (ay[at(g, i, j, k)] * (p[at(g, i, j, k)] - p[at(g, i, j - 1, k)]) * (1.0 / g.dy) - cross)
+             / interp<CC, YF>(J, g, i, j, k);
+    }
+    return (p[at(g, i, j, k)] - p[at(g, i, j, k - 1)]) * (1.0 / g.dzeta) / interp<CC, ZF>(J, g, i, j, k);
+}
+
+//! R_c += (G p)_c (MassFlux.cpp:138-179) on the valid points of each component.
 void add_pressure_gradient(gb_simplec* S, const double* p, double* Ru, double* Rv, double* Rw)
 {
     const gb_grid g = S->g;
@@ -674,21 +697,9 @@ void add_pressure_gradient(gb_simplec* S, const double* p, double* Ru, double* R
     const double* ax = S->mesh.ax;
     const double* ay = S->mesh.ay;
     for_box(S->ctx, Box{{0, 0, 0}, {g.nx, g.ny, g.nz}}, [=] __device__(int i, int j, int k) {
-        if (j < g.ny && k < g.nz) {
-            const double cross = 0.25 * ((slope_dp<0>(z, p, g, i - 1, j, k) + slope_dp<0>(z, p, g, i, j, k))
-                                         + (slope_dp<0>(z, p, g, i - 1, j, k + 1) + slope_dp<0>(z, p, g, i, j, k + 1)));
-            Ru[at(g, i, j, k)] += (ax[at(g, i, j, k)] * (p[at(g, i, j, k)] - p[at(g, i - 1, j, k)]) * (1.0 / g.dx) - cross)
-                                / interp<CC, XF>(J, g, i, j, k);
-        }
-        if (i < g.nx && k < g.nz) {
-            const double cross = 0.25 * ((slope_dp<1>(z, p, g, i, j - 1, k) + slope_dp<1>(z, p, g, i, j, k))
-                                         + (slope_dp<1>(z, p, g, i, j - 1, k + 1) + slope_dp<1>(z, p, g, i, j, k + 1)));
-            Rv[at(g, i, j, k)] += (ay[at(g, i, j, k)] * (p[at(g, i, j, k)] - p[at(g, i, j - 1, k)]) * (1.0 / g.dy) - cross)
-                                / interp<CC, YF>(J, g, i, j, k);
-        }
-        if (i < g.nx && j < g.ny) {
-            Rw[at(g, i, j, k)] += (p[at(g, i, j, k)] - p[at(g, i, j, k - 1)]) * (1.0 / g.dzeta) / interp<CC, ZF>(J, g, i, j, k);
-        }
+        if (j < g.ny && k < g.nz) { Ru[at(g, i, j, k)] += pressure_gradient_at<0>(p, z, J, ax, ay, g, i, j, k); }
+        if (i < g.nx && k < g.nz) { Rv[at(g, i, j, k)] += pressure_gradient_at<1>(p, z, J, ax, ay, g, i, j, k); }
+        if (i < g.nx && j < g.ny) { Rw[at(g, i, j, k)] += pressure_gradient_at<2>(p, z, J, ax, ay, g, i, j, k); }
     }, GB_KERNEL_RESIDUAL);
 }
 
@@ -727,21 +738,28 @@ Box flux_box(const gb_grid& g, int D)
     return b;
 }
 
-//! Convection.cpp:17-43 flux_kernel<T, D, L>.
+//! The convective flux of q (at T) through its control volume's face along D
+//! at the flux point (i, j, k): Convection.cpp:17-43 flux_kernel<T, D, L>.
 template <int T, int D>
-void conv_fluxes(gb_simplec* S, const double* q, const double* F, int lim, double eps2, double* G)
+__device__ __forceinline__ double conv_face(const double* __restrict__ q, const double* __restrict__ F, int lim,
+                                            double eps2, const gb_grid& g, int i, int j, int k)
 {
-    const gb_grid g = S->g;
     constexpr int Sx = T ^ (1 << D);
     constexpr int TF = 1 << D;
     constexpr int l = lo_off(T, Sx, D);
     constexpr int ex = (D == 0), ey = (D == 1), ez = (D == 2);
+    const double tr = interp<TF, Sx>(F, g, i, j, k);
+    const int i0 = i + l * ex, j0 = j + l * ey, k0 = k + l * ez;
+    return tr * muscl_face(lim, tr, q[at(g, i0 - ex, j0 - ey, k0 - ez)], q[at(g, i0, j0, k0)],
+                           q[at(g, i0 + ex, j0 + ey, k0 + ez)], q[at(g, i0 + 2 * ex, j0 + 2 * ey, k0 + 2 * ez)], eps2);
+}
+
+template <int T, int D>
+void conv_fluxes(gb_simplec* S, const double* q, const double* F, int lim, double eps2, double* G)
+{
+    const gb_grid g = S->g;
     for_box(S->ctx, flux_box<T>(g, D), [=] __device__(int i, int j, int k) {
-        const double tr = interp<TF, Sx>(F, g, i, j, k);
-        const int i0 = i + l * ex, j0 = j + l * ey, k0 = k + l * ez;
-        G[at(g, i, j, k)] = tr * muscl_face(lim, tr, q[at(g, i0 - ex, j0 - ey, k0 - ez)], q[at(g, i0, j0, k0)],
-                                            q[at(g, i0 + ex, j0 + ey, k0 + ez)],
-                                            q[at(g, i0 + 2 * ex, j0 + 2 * ey, k0 + 2 * ez)], eps2);
+        G[at(g, i, j, k)] = conv_face<T, D>(q, F, lim, eps2, g, i, j, k);
     }, GB_KERNEL_RESIDUAL);
 }
 
@@ -826,18 +844,48 @@ __device__ __forceinline__ double area_dot(const Metric<double>& m, const double
     return v[2] - m.zx * v[0] - m.zy * v[1];
 }
 
+//! The diffusive flux of a cell scalar q through the face along D at the flux
+//! point (i, j, k) (Diffusion.cpp:10-57).
+template <int D>
+__device__ __forceinline__ double scalar_diff_face(const double* __restrict__ q, const double* __restrict__ gamma,
+                                                   const double* __restrict__ z, int logz, const gb_grid& g, int i,
+                                                   int j, int k)
+{
+    constexpr int Sx = 1 << D;
+    const Metric<double> m = metric_at<Sx>(z, g, i, j, k);
+    double gr[3];
+    grad_at<CC, Sx>(q, g, i, j, k, m, gr);
+    return face_gamma<Sx>(gamma, g, i, j, k, logz) * area_dot<D>(m, gr);
+}
+
+//! The diffusive flux of velocity component C through its control volume's
+//! face along D at the flux point (i, j, k) (Diffusion.cpp:59-127).
+template <int C, int D>
+__device__ __forceinline__ double momentum_diff_face(const double* __restrict__ u, const double* __restrict__ v,
+                                                     const double* __restrict__ w, const double* __restrict__ nu,
+                                                     const double* __restrict__ z, int logz, const gb_grid& g, int i,
+                                                     int j, int k)
+{
+    constexpr int T = 1 << C;
+    constexpr int Sx = T ^ (1 << D);
+    const Metric<double> m = metric_at<Sx>(z, g, i, j, k);
+    double gu[3], gv[3], gw[3];
+    grad_at<XF, Sx>(u, g, i, j, k, m, gu);
+    grad_at<YF, Sx>(v, g, i, j, k, m, gv);
+    grad_at<ZF, Sx>(w, g, i, j, k, m, gw);
+    const double* gc = (C == 0) ? gu : (C == 1) ? gv : gw;
+    const double tau[3] = {gc[0] + gu[C], gc[1] + gv[C], gc[2] + gw[C]};
+    return face_gamma<Sx>(nu, g, i, j, k, logz) * area_dot<D>(m, tau);
+}
+
 template <int D>
 void scalar_diffusive_flux(gb_simplec* S, const double* q, const double* gamma, double* G)
 {
     const gb_grid g = S->g;
     const double* z = S->z;
     const int logz = S->ph.log_mean;
-    constexpr int Sx = 1 << D;
     for_box(S->ctx, flux_box<CC>(g, D), [=] __device__(int i, int j, int k) {
-        const Metric<double> m = metric_at<Sx>(z, g, i, j, k);
-        double gr[3];
-        grad_at<CC, Sx>(q, g, i, j, k, m, gr);
-        G[at(g, i, j, k)] = face_gamma<Sx>(gamma, g, i, j, k, logz) * area_dot<D>(m, gr);
+        G[at(g, i, j, k)] = scalar_diff_face<D>(q, gamma, z, logz, g, i, j, k);
     }, GB_KERNEL_RESIDUAL);
 }
 
@@ -850,17 +898,8 @@ void momentum_diffusive_flux(gb_simplec* S, const gb_state& q, const double* nu,
     const double* v = q.v;
     const double* w = q.w;
     const int logz = S->ph.log_mean;
-    constexpr int T = 1 << C;
-    constexpr int Sx = T ^ (1 << D);
-    for_box(S->ctx, flux_box<T>(g, D), [=] __device__(int i, int j, int k) {
-        const Metric<double> m = metric_at<Sx>(z, g, i, j, k);
-        double gu[3], gv[3], gw[3];
-        grad_at<XF, Sx>(u, g, i, j, k, m, gu);
-        grad_at<YF, Sx>(v, g, i, j, k, m, gv);
-        grad_at<ZF, Sx>(w, g, i, j, k, m, gw);
-        const double* gc = (C == 0) ? gu : (C == 1) ? gv : gw;
-        const double tau[3] = {gc[0] + gu[C], gc[1] + gv[C], gc[2] + gw[C]};
-        G[at(g, i, j, k)] = face_gamma<Sx>(nu, g, i, j, k, logz) * area_dot<D>(m, tau);
+    for_box(S->ctx, flux_box<1 << C>(g, D), [=] __device__(int i, int j, int k) {
+        G[at(g, i, j, k)] = momentum_diff_face<C, D>(u, v, w, nu, z, logz, g, i, j, k);
     }, GB_KERNEL_RESIDUAL);
 }
 
@@ -888,6 +927,183 @@ void scalar_diffusion_subtract(gb_simplec* S, const double* q, const double* gam
     scalar_diffusive_flux<2>(S, q, gamma, G[2]);
     if (S->wall) { turb_ground_flux(S->ctx, S->g, S->bc, S->ssr, field, G[2]); }
     flux_divergence<CC>(S, G[0], G[1], G[2], R, 1);
+}
+
+// ------------------------------------------------------- fused residual ---
+//
+// The convection, diffusion and pressure-gradient terms of one equation in
+// one launch. A block holds 32 x 8 columns of the equation's points and
+// marches up kc levels of them. At each level every thread evaluates the
+// convective and diffusive fluxes through the low x, y faces of its control
+// volume into shared memory (the block's last row and column also the high
+// faces) and through its upper z face into registers (the lower one is the
+// level below's upper face), then takes the divergences from there. Each
+// face flux is evaluated once per block (twice on the block's edges and at
+// its first level), by the same device functions as the separate flux
+// launches, and no flux array goes through memory.
+
+constexpr int kFusedTx = 32, kFusedTy = 8;
+
+struct FusedResidualArgs {
+    gb_grid g;
+    int ni, nj, nk, kc;          // the equation's valid points; levels per block
+    const double* q;             // the transported field
+    const double* u;
+    const double* v;
+    const double* w;
+    const double* p;
+    const double* F0;            // the transport fluxes
+    const double* F1;
+    const double* F2;
+    const double* gamma;         // nu (momentum) or the scalar's diffusivity
+    const double* z;
+    const double* J;
+    const double* ax;
+    const double* ay;
+    int lim;
+    double eps2;
+    int logz;
+    int wall;                    // a surface_layer ground: its z faces carry the wall's flux
+    const double* plane;         // the wall stress (u, v) or the cell area (theta) per column
+    double qs;                   // the surface heat flux (theta)
+    const double* ps;            // k's shear and buoyancy production and dissipation (null: none)
+    const double* pb;
+    const double* eps;
+    double* R;
+};
+
+//! The convective and diffusive fluxes of equation E (0-2 the velocity
+//! components, 3 theta, 4 k) through the face along D at flux point (i, j, k),
+//! the ground faces of a surface_layer ground replaced by the wall's flux
+//! (set_ground_fluxes, SurfaceLayer.cpp:418-450).
+template <int E, int D>
+__device__ __forceinline__ void fused_face(const FusedResidualArgs& a, int i, int j, int k, double& gc, double& gd)
+{
+    constexpr int T = (E < 3) ? (1 << E) : CC;
+    const double* F = (D == 0) ? a.F0 : (D == 1) ? a.F1 : a.F2;
+    gc = conv_face<T, D>(a.q, F, a.lim, a.eps2, a.g, i, j, k);
+    if (D == 2 && E != 2 && a.wall && k == 0) {
+        if (E == 0) {
+            gd = 0.5 * (a.plane[plane_at(a.g, i - 1, j)] + a.plane[plane_at(a.g, i, j)]);
+        } else if (E == 1) {
+            gd = 0.5 * (a.plane[plane_at(a.g, i, j - 1)] + a.plane[plane_at(a.g, i, j)]);
+        } else if (E == 3) {
+            gd = -a.qs * a.plane[plane_at(a.g, i, j)];
+        } else {
+            gd = 0;
+        }
+        return;
+    }
+    if (E < 3) {
+        gd = momentum_diff_face<(E < 3 ? E : 0), D>(a.u, a.v, a.w, a.gamma, a.z, a.logz, a.g, i, j, k);
+    } else {
+        gd = scalar_diff_face<D>(a.q, a.gamma, a.z, a.logz, a.g, i, j, k);
+    }
+}
+
+//! R = div(convective flux) - div(diffusive flux) (+ the pressure gradient
+//! for a velocity component; for k the bounded form's - k div(transport) and
+//! the sources), in the operation order of the separate launches
+//! (Residual.cpp:159-256).
+template <int E>
+__global__ void __launch_bounds__(kFusedTx* kFusedTy) k_fused_residual(const FusedResidualArgs a)
+{
+    constexpr int T = (E < 3) ? (1 << E) : CC;
+    constexpr int lx = flux_lo(T, 0), ly = flux_lo(T, 1), lz = flux_lo(T, 2);
+    __shared__ double xc[kFusedTy][kFusedTx + 1], xd[kFusedTy][kFusedTx + 1];
+    __shared__ double yc[kFusedTy + 1][kFusedTx], yd[kFusedTy + 1][kFusedTx];
+    const gb_grid& g = a.g;
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int i = blockIdx.x * kFusedTx + tx, j = blockIdx.y * kFusedTy + ty;
+    const bool active = i < a.ni && j < a.nj;
+    const bool xhi = active && (tx == kFusedTx - 1 || i == a.ni - 1);
+    const bool yhi = active && (ty == kFusedTy - 1 || j == a.nj - 1);
+    const int kb = blockIdx.z * a.kc, ke = min(kb + a.kc, a.nk);
+    double zc_lo = 0, zd_lo = 0;
+    if (active && kb < ke) { fused_face<E, 2>(a, i, j, kb + lz, zc_lo, zd_lo); }
+    for (int k = kb; k < ke; ++k) {
+        double zc_hi = 0, zd_hi = 0;
+        if (active) {
+            fused_face<E, 0>(a, i + lx, j, k, xc[ty][tx], xd[ty][tx]);
+            if (xhi) { fused_face<E, 0>(a, i + lx + 1, j, k, xc[ty][tx + 1], xd[ty][tx + 1]); }
+            fused_face<E, 1>(a, i, j + ly, k, yc[ty][tx], yd[ty][tx]);
+            if (yhi) { fused_face<E, 1>(a, i, j + ly + 1, k, yc[ty + 1][tx], yd[ty + 1][tx]); }
+            fused_face<E, 2>(a, i, j, k + lz + 1, zc_hi, zd_hi);
+        }
+        __syncthreads();
+        if (active) {
+            const int64_t o = at(g, i, j, k);
+            const double Jt = interp<CC, T>(a.J, g, i, j, k);
+            double r = ((xc[ty][tx + 1] - xc[ty][tx]) * (1.0 / g.dx) + (yc[ty + 1][tx] - yc[ty][tx]) * (1.0 / g.dy)
+                        + (zc_hi - zc_lo) * (1.0 / g.dzeta))
+                     / Jt;
+            if (E == 4) {
+                constexpr int SX = T ^ XF, SY = T ^ YF, SZ = T ^ ZF;
+                const double div = (interp<XF, SX>(a.F0, g, i + lx + 1, j, k) - interp<XF, SX>(a.F0, g, i + lx, j, k)) * (1.0 / g.dx)
+                                 + (interp<YF, SY>(a.F1, g, i, j + ly + 1, k) - interp<YF, SY>(a.F1, g, i, j + ly, k)) * (1.0 / g.dy)
+                                 + (interp<ZF, SZ>(a.F2, g, i, j, k + lz + 1) - interp<ZF, SZ>(a.F2, g, i, j, k + lz)) * (1.0 / g.dzeta);
+                r -= a.q[o] * div / Jt;
+            }
+            r -= ((xd[ty][tx + 1] - xd[ty][tx]) * (1.0 / g.dx) + (yd[ty + 1][tx] - yd[ty][tx]) * (1.0 / g.dy)
+                  + (zd_hi - zd_lo) * (1.0 / g.dzeta))
+               / Jt;
+            if (E < 3) { r += pressure_gradient_at<(E < 3 ? E : 0)>(a.p, a.z, a.J, a.ax, a.ay, g, i, j, k); }
+            if (E == 4 && a.ps != nullptr) { r = ((r - a.ps[o]) - a.pb[o]) + a.eps[o]; }
+            a.R[o] = r;
+        }
+        zc_lo = zc_hi;
+        zd_lo = zd_hi;
+        __syncthreads();
+    }
+}
+
+//! One fused residual launch for equation E into R.
+template <int E>
+void fused_residual(gb_simplec* S, const gb_state& q, double* R)
+{
+    constexpr int T = (E < 3) ? (1 << E) : CC;
+    const gb_grid g = S->g;
+    const gb_physics& ph = S->ph;
+    FusedResidualArgs a{};
+    a.g = g;
+    a.ni = g.nx + (T & 1);
+    a.nj = g.ny + ((T >> 1) & 1);
+    a.nk = g.nz + ((T >> 2) & 1);
+    const int knob = S->ctx->tune[GB_TUNE_RESIDUAL];
+    a.kc = (knob >= 2) ? knob : 8;
+    const double* fields[5] = {q.u, q.v, q.w, q.theta, q.tke};
+    a.q = fields[E];
+    a.u = q.u;
+    a.v = q.v;
+    a.w = q.w;
+    a.p = q.p;
+    a.F0 = S->w.F[0];
+    a.F1 = S->w.F[1];
+    a.F2 = S->w.F[2];
+    a.gamma = (E < 3) ? S->dfe.nu : (E == 3) ? S->dfe.gamma_theta : S->dfe.gamma_tke;
+    a.z = S->z;
+    a.J = S->mesh.detJ;
+    a.ax = S->mesh.ax;
+    a.ay = S->mesh.ay;
+    a.lim = (E == 4) ? GB_LIMITER_UPWIND : ph.limiter;
+    const double eps = (E < 3) ? ph.smooth_eps_velocity : (E == 3) ? ph.smooth_eps_theta : 1e-5;
+    a.eps2 = eps * eps;
+    a.logz = ph.log_mean;
+    a.wall = S->wall ? 1 : 0;
+    a.plane = (E == 0) ? S->ssr[kSsTauX] : (E == 1) ? S->ssr[kSsTauY] : (E == 3) ? S->ssr[kSsArea] : nullptr;
+    a.qs = (S->bc.surface_stability == GB_SURFACE_HEAT_FLUX) ? S->bc.surface_heat_flux : 0.0;
+    if (E == 4 && ph.closure) {
+        a.ps = S->cf[kClosurePs];
+        a.pb = S->cf[kClosurePb];
+        a.eps = S->cf[kClosureEps];
+    }
+    a.R = R;
+    const dim3 block(kFusedTx, kFusedTy);
+    const dim3 grid((a.ni + kFusedTx - 1) / kFusedTx, (a.nj + kFusedTy - 1) / kFusedTy, (a.nk + a.kc - 1) / a.kc);
+    span_begin(S->ctx, GB_KERNEL_RESIDUAL);
+    k_fused_residual<E><<<grid, block, 0, S->ctx->stream>>>(a);
+    span_end(S->ctx);
+    ++S->ctx->launches;
 }
 
 // ------------------------------------------------------------- forcing ---
@@ -1131,20 +1347,32 @@ void simplec_residual(gb_simplec* S, const gb_state& q, double** R)
     double** F = S->w.F;
     transport_fluxes(S, q, F[0], F[1], F[2]);
     const gb_physics& ph = S->ph;
-    convection<XF>(S, q.u, F, ph.limiter, ph.smooth_eps_velocity, false, R[0]);
-    convection<YF>(S, q.v, F, ph.limiter, ph.smooth_eps_velocity, false, R[1]);
-    convection<ZF>(S, q.w, F, ph.limiter, ph.smooth_eps_velocity, false, R[2]);
-    momentum_diffusion_subtract<0>(S, q, R[0]);
-    momentum_diffusion_subtract<1>(S, q, R[1]);
-    momentum_diffusion_subtract<2>(S, q, R[2]);
-    add_pressure_gradient(S, q.p, R[0], R[1], R[2]);
+    const bool fused = ctx->tune[GB_TUNE_RESIDUAL] != 1;
+    if (fused) {
+        fused_residual<0>(S, q, R[0]);
+        fused_residual<1>(S, q, R[1]);
+        fused_residual<2>(S, q, R[2]);
+    } else {
+        convection<XF>(S, q.u, F, ph.limiter, ph.smooth_eps_velocity, false, R[0]);
+        convection<YF>(S, q.v, F, ph.limiter, ph.smooth_eps_velocity, false, R[1]);
+        convection<ZF>(S, q.w, F, ph.limiter, ph.smooth_eps_velocity, false, R[2]);
+        momentum_diffusion_subtract<0>(S, q, R[0]);
+        momentum_diffusion_subtract<1>(S, q, R[1]);
+        momentum_diffusion_subtract<2>(S, q, R[2]);
+        add_pressure_gradient(S, q.p, R[0], R[1], R[2]);
+    }
     forcing(S, q, R);
     velocity_divergence(S, q.u, q.v, q.w, R[3]);
-    convection<CC>(S, q.theta, F, ph.limiter, ph.smooth_eps_theta, false, R[4]);
-    scalar_diffusion_subtract(S, q.theta, S->dfe.gamma_theta, R[4], 2);
-    convection<CC>(S, q.tke, F, GB_LIMITER_UPWIND, 1e-5, true, R[5]);
-    scalar_diffusion_subtract(S, q.tke, S->dfe.gamma_tke, R[5], 3);
-    if (S->ph.closure) { turb_k_sources(ctx, g, S->cf, R[5]); }
+    if (fused) {
+        fused_residual<3>(S, q, R[4]);
+        fused_residual<4>(S, q, R[5]);
+    } else {
+        convection<CC>(S, q.theta, F, ph.limiter, ph.smooth_eps_theta, false, R[4]);
+        scalar_diffusion_subtract(S, q.theta, S->dfe.gamma_theta, R[4], 2);
+        convection<CC>(S, q.tke, F, GB_LIMITER_UPWIND, 1e-5, true, R[5]);
+        scalar_diffusion_subtract(S, q.tke, S->dfe.gamma_tke, R[5], 3);
+        if (S->ph.closure) { turb_k_sources(ctx, g, S->cf, R[5]); }
+    }
     if (S->wall) { turb_apply_wall_k(ctx, g, S->bc, S->ssr, q.tke, R[5]); }
     add_damping(S, q, R);
     apply_rows(S, q, R);
@@ -1157,16 +1385,18 @@ void simplec_residual(gb_simplec* S, const gb_state& q, double** R)
 
 namespace {
 
+//! The two parts of an implicit face weight shared by the control volumes on
+//! either side of the face (ImplicitOperator.cpp:13-37): the diffusive
+//! conductance and the transport flux at the face.
 template <int T, int C, int D>
-__device__ __forceinline__ double face_weight(int side, int i, int j, int k, const double* f, const double* gm,
-                                              const double* z, const gb_grid& g, int logz)
+__device__ __forceinline__ void face_parts(int i, int j, int k, const double* f, const double* gm, const double* z,
+                                           const gb_grid& g, int logz, double& dif, double& tr)
 {
     constexpr int Sx = T ^ (1 << D);
     const double dxinv[3] = {1.0 / g.dx, 1.0 / g.dy, 1.0 / g.dzeta};
     const Metric<double> m = metric_at<Sx>(z, g, i, j, k);
     const double gs = face_gamma<Sx>(gm, g, i, j, k, logz);
-    const double tr = interp<(1 << D), Sx>(f, g, i, j, k);
-    double dif;
+    tr = interp<(1 << D), Sx>(f, g, i, j, k);
     if (D < 2) {
         const double own = (C == D) ? 2.0 : 1.0;
         dif = gs * m.zz * own * dxinv[D];
@@ -1177,8 +1407,81 @@ __device__ __forceinline__ double face_weight(int side, int i, int j, int k, con
         if (C == 2) { nc2 = 1; }
         dif = gs * (1 + m.zx * m.zx + m.zy * m.zy + nc2) / m.zz * dxinv[2];
     }
+}
+
+//! The face weight of the control volume on side 0 (above the face: its low
+//! face) or side 1 (below: its high face): the conductance plus the inflow.
+__device__ __forceinline__ double weight_of(int side, double dif, double tr, double dxinv)
+{
     const double inflow = (side == 0) ? fmax(tr, 0.0) : fmax(-tr, 0.0);
-    return (dif + inflow) * dxinv[D];
+    return (dif + inflow) * dxinv;
+}
+
+template <int T, int C, int D>
+__device__ __forceinline__ double face_weight(int side, int i, int j, int k, const double* f, const double* gm,
+                                              const double* z, const gb_grid& g, int logz)
+{
+    double dif, tr;
+    face_parts<T, C, D>(i, j, k, f, gm, z, g, logz, dif, tr);
+    const double dxinv = (D == 0) ? 1.0 / g.dx : (D == 1) ? 1.0 / g.dy : 1.0 / g.dzeta;
+    return weight_of(side, dif, tr, dxinv);
+}
+
+//! The implicit coefficients with each face's parts evaluated once per block
+//! (the layout of k_fused_residual: 32 x 8 columns marching kc levels, the
+//! low x and y faces in shared memory, the z faces in registers).
+template <int C>
+__global__ void __launch_bounds__(kFusedTx* kFusedTy)
+    k_fused_coefficients(const gb_grid g, int ni, int nj, int nk, int kc, const double* __restrict__ z,
+                         const double* __restrict__ J, int logz, const double* __restrict__ F0,
+                         const double* __restrict__ F1, const double* __restrict__ F2, const double* __restrict__ gm,
+                         double* __restrict__ A)
+{
+    constexpr int T = (C < 0) ? CC : (1 << C);
+    constexpr int lx = flux_lo(T, 0), ly = flux_lo(T, 1), lz = flux_lo(T, 2);
+    __shared__ double xdif[kFusedTy][kFusedTx + 1], xtr[kFusedTy][kFusedTx + 1];
+    __shared__ double ydif[kFusedTy + 1][kFusedTx], ytr[kFusedTy + 1][kFusedTx];
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int i = blockIdx.x * kFusedTx + tx, j = blockIdx.y * kFusedTy + ty;
+    const bool active = i < ni && j < nj;
+    const bool xhi = active && (tx == kFusedTx - 1 || i == ni - 1);
+    const bool yhi = active && (ty == kFusedTy - 1 || j == nj - 1);
+    const int kb = blockIdx.z * kc, ke = min(kb + kc, nk);
+    const int64_t cs = volume(g);
+    const double dxinv = 1.0 / g.dx, dyinv = 1.0 / g.dy, dzinv = 1.0 / g.dzeta;
+    double zdif_lo = 0, ztr_lo = 0;
+    if (active && kb < ke) { face_parts<T, C, 2>(i, j, kb + lz, F2, gm, z, g, logz, zdif_lo, ztr_lo); }
+    for (int k = kb; k < ke; ++k) {
+        double zdif_hi = 0, ztr_hi = 0;
+        if (active) {
+            face_parts<T, C, 0>(i + lx, j, k, F0, gm, z, g, logz, xdif[ty][tx], xtr[ty][tx]);
+            if (xhi) { face_parts<T, C, 0>(i + lx + 1, j, k, F0, gm, z, g, logz, xdif[ty][tx + 1], xtr[ty][tx + 1]); }
+            face_parts<T, C, 1>(i, j + ly, k, F1, gm, z, g, logz, ydif[ty][tx], ytr[ty][tx]);
+            if (yhi) { face_parts<T, C, 1>(i, j + ly + 1, k, F1, gm, z, g, logz, ydif[ty + 1][tx], ytr[ty + 1][tx]); }
+            face_parts<T, C, 2>(i, j, k + lz + 1, F2, gm, z, g, logz, zdif_hi, ztr_hi);
+        }
+        __syncthreads();
+        if (active) {
+            const double Jinv = 1.0 / interp<CC, T>(J, g, i, j, k);
+            const double xm = weight_of(0, xdif[ty][tx], xtr[ty][tx], dxinv) * Jinv;
+            const double xp = weight_of(1, xdif[ty][tx + 1], xtr[ty][tx + 1], dxinv) * Jinv;
+            const double ym = weight_of(0, ydif[ty][tx], ytr[ty][tx], dyinv) * Jinv;
+            const double yp = weight_of(1, ydif[ty + 1][tx], ytr[ty + 1][tx], dyinv) * Jinv;
+            const double zm = weight_of(0, zdif_lo, ztr_lo, dzinv) * Jinv;
+            const double zp = weight_of(1, zdif_hi, ztr_hi, dzinv) * Jinv;
+            const int64_t o = at(g, i, j, k);
+            A[GB_COEF_XM * cs + o] = xm;
+            A[GB_COEF_XP * cs + o] = xp;
+            A[GB_COEF_YM * cs + o] = ym;
+            A[GB_COEF_YP * cs + o] = yp;
+            A[GB_COEF_ZM * cs + o] = zm;
+            A[GB_COEF_ZP * cs + o] = zp;
+            A[GB_COEF_P * cs + o] = ((xm + xp) + (ym + yp)) + (zm + zp);
+        }
+        zdif_lo = zdif_hi;
+        ztr_lo = ztr_hi;
+        __syncthreads();
+    }
 }
 
 //! ImplicitOperator.cpp:39-74 coefficients<C> (C = -1: a cell scalar) on
@@ -1193,6 +1496,18 @@ void implicit_coefficients_on(gb_ctx* ctx, const gb_grid g, const double* z, con
     const double* F0 = F[0];
     const double* F1 = F[1];
     const double* F2 = F[2];
+    const int knob = ctx->tune[GB_TUNE_RESIDUAL];
+    if (knob != 1) {
+        const int ni = g.nx + (T & 1), nj = g.ny + ((T >> 1) & 1), nk = g.nz + ((T >> 2) & 1);
+        const int kc = (knob >= 2) ? knob : 8;
+        const dim3 block(kFusedTx, kFusedTy);
+        const dim3 grid((ni + kFusedTx - 1) / kFusedTx, (nj + kFusedTy - 1) / kFusedTy, (nk + kc - 1) / kc);
+        span_begin(ctx, GB_KERNEL_COEFS);
+        k_fused_coefficients<C><<<grid, block, 0, ctx->stream>>>(g, ni, nj, nk, kc, z, J, logz, F0, F1, F2, gm, A);
+        span_end(ctx);
+        ++ctx->launches;
+        return;
+    }
     for_box(ctx, valid_box(g, T), [=] __device__(int i, int j, int k) {
         const double Jinv = 1.0 / interp<CC, T>(J, g, i, j, k);
         const double xm = face_weight<T, C, 0>(0, i + lx, j, k, F0, gm, z, g, logz) * Jinv;

@@ -47,7 +47,7 @@ inline int64_t plane_size(const gb_grid& g) { return g.sy * static_cast<int64_t>
 
 __host__ __device__ __forceinline__ int64_t plane_at(const gb_grid& g, int i, int j)
 {
-    return static_cast<int64_t>(i + g.ng) + static_cast<int64_t>(j + g.ng) * g.sy;
+    return static_cast<int64_t>((i + g.ng) + (j + g.ng) * static_cast<int32_t>(g.sy));
 }
 
 //! The wall law's gradient of column (i, j) for a point of type t on the

@@ -127,6 +127,11 @@ enum {
     GB_TUNE_LINE_SEGMENT,       /* levels per warp of the segmented z-line sweep (default 8) and of the
                                    segmented zebra relaxation (default 4, 8 for columns of more than 64
                                    levels): 0 default, 4 or 8 */
+    GB_TUNE_RESIDUAL,           /* the SIMPLEC residual's convection, diffusion and pressure gradient and
+                                   the implicit coefficients: 0 default (one launch per equation, each
+                                   face evaluated once per block, 8 levels per block), 1 one thread per
+                                   point (the residual's fluxes and divergences as separate launches),
+                                   N >= 2 the per-equation launch with N levels per block */
     GB_N_TUNE
 };
 gb_status gb_ctx_tune(gb_ctx* ctx, int32_t key, int32_t value);

@@ -77,6 +77,37 @@ def test_gpu_residual_matches_oracle(ctx, name, opts):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("name", list(CONFIGS))
+@pytest.mark.parametrize("levels", [0, 3, 64], ids=["8-levels", "3-levels", "one-block-column"])
+def test_gpu_fused_residual_matches_separate_launches(ctx, name, levels):
+    """The residual's convection, diffusion and pressure gradient as one
+    launch per equation (GB_TUNE_RESIDUAL 0, or N levels per block) equal
+    the separate flux and divergence launches (GB_TUNE_RESIDUAL 1) to 1e-13
+    relative per field: the same face fluxes by the same device functions
+    (the compiler's contractions may differ between the two kernels)."""
+    import ablsteadyrans_b200 as gb
+    from ablsteadyrans_b200.simplec import DeviceCase, SimplecStage
+    case, bc = make(name, nx=37, ny=19, nz=11, seed=3)
+    ph = physics(case, limiter=LIMITER_VAN_ALBADA, log_mean=1, coriolis=1, latitude=45.0)
+    oracle.fill_ghosts(case, bc, ph)
+    dc = DeviceCase.from_oracle(case)
+    st = SimplecStage(ctx, dc, bc, ph, SimplecOptions.make())
+    try:
+        ctx.tune(gb.TUNE_RESIDUAL, 1)
+        R1 = [r.cpu().numpy() for r in st.residual()]
+        ctx.tune(gb.TUNE_RESIDUAL, levels)
+        R0 = [r.cpu().numpy() for r in st.residual()]
+    finally:
+        ctx.tune(gb.TUNE_RESIDUAL, 0)
+        st.close()
+    g = case.grid
+    for n, (a, b) in enumerate(zip(R0, R1)):
+        v = g.valid(LOCS[n])
+        scale = max(np.abs(b[v]).max(), 1e-300)
+        assert np.abs(a[v] - b[v]).max() <= 1e-13 * scale, (FIELDS[n], np.abs(a[v] - b[v]).max(), scale)
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("sweep", [(0, 0), (1, 1)], ids=["zjacobi", "lusgs-alternate"])
 @pytest.mark.parametrize("name", list(CONFIGS))
 def test_gpu_iterations_match_oracle(ctx, name, sweep):

@@ -110,3 +110,35 @@ def test_gpu_implicit_coefficients_match_oracle(ctx, loc, log_mean):
     for n in range(7):
         scale = max(float(np.abs(ref[n][v]).max()), 1e-300)
         assert float(np.abs(got[n][v] - ref[n][v]).max()) <= 1e-13 * scale, n
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("levels", [0, 5])
+@pytest.mark.parametrize("loc", [0, 1, 2, 4])
+def test_gpu_implicit_coefficients_per_block_faces_match_per_point(ctx, loc, levels):
+    """The implicit coefficients with each face's conductance and transport
+    evaluated once per block (GB_TUNE_RESIDUAL 0, or N levels per block)
+    equal the one-thread-per-point form (GB_TUNE_RESIDUAL 1), which
+    evaluates every face from both sides, to 1e-14 relative."""
+    import torch
+    import ablsteadyrans_b200 as gb
+    from helpers import terrain_simplec_case
+    case = terrain_simplec_case(41, 13, 12, False, True, seed=4)
+    g = case.grid
+    rng = np.random.default_rng(11 + loc)
+    F = [g.np_zeros() + rng.standard_normal(g.shape) for _ in range(3)]
+    gamma = g.np_zeros() + rng.uniform(0.5, 3.0, g.shape)
+    dev = lambda a: torch.from_numpy(a).cuda()  # noqa: E731
+    out = []
+    try:
+        for knob in (1, levels):
+            ctx.tune(gb.TUNE_RESIDUAL, knob)
+            A = torch.zeros((7,) + tuple(g.shape), dtype=torch.float64, device="cuda")
+            gb.implicit_coefficients(ctx, g, loc, [dev(f) for f in F], dev(gamma), dev(case.z), dev(case.J), 1, A)
+            out.append(A.cpu().numpy())
+    finally:
+        ctx.tune(gb.TUNE_RESIDUAL, 0)
+    v = g.valid(loc)
+    for n in range(7):
+        scale = max(float(np.abs(out[0][n][v]).max()), 1e-300)
+        assert float(np.abs(out[1][n][v] - out[0][n][v]).max()) <= 1e-14 * scale, n

@@ -275,6 +275,36 @@ def test_gpu_wall_model_and_closure_match_oracle(ctx, heat):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("heat", [0.0, 0.05])
+def test_gpu_fused_residual_with_wall_and_closure(ctx, heat):
+    """With the closure's k sources and the wall's ground fluxes (stress on
+    u and v, the heat flux on theta, none on k), the fused residual
+    launches equal the separate flux and divergence launches to 1e-13."""
+    import ablsteadyrans_b200 as gb
+    from ablsteadyrans_b200.abi import SURFACE_HEAT_FLUX
+    case, bc, ph = _hill_case()
+    if heat:
+        bc.surface_stability, bc.surface_heat_flux = SURFACE_HEAT_FLUX, heat
+        rng = np.random.default_rng(3)
+        case.q["theta"][...] = 300.0 + rng.uniform(-0.5, 0.5, case.q["theta"].shape)
+    dc, st = _stage(ctx, case, bc, ph)
+    try:
+        st.fill_ghosts()
+        ctx.tune(gb.TUNE_RESIDUAL, 1)
+        R1 = [r.cpu().numpy() for r in st.residual()]
+        ctx.tune(gb.TUNE_RESIDUAL, 0)
+        R0 = [r.cpu().numpy() for r in st.residual()]
+    finally:
+        ctx.tune(gb.TUNE_RESIDUAL, 0)
+        st.close()
+    g = case.grid
+    for n, loc in enumerate(LOCS):
+        v = g.valid(loc)
+        scale = max(np.abs(R1[n][v]).max(), 1e-300)
+        assert np.abs(R0[n][v] - R1[n][v]).max() <= 1e-13 * scale, n
+
+
+@pytest.mark.gpu
 def test_gpu_iterations_with_closure_and_wall_model_match_oracle(ctx):
     """Five SIMPLEC iterations with the closure and the surface layer (the
     local dtau from the last iteration's nu, 0 at first) agree with the
