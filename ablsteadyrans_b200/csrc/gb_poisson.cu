@@ -12,6 +12,8 @@
 #include "gb_poisson.cuh"
 #include "gb_poisson_api.cuh"
 
+#include <cooperative_groups.h>
+
 #include <algorithm>
 #include <atomic>
 #include <cmath>
@@ -933,6 +935,225 @@ __global__ void __launch_bounds__(256) k_coarse_relax(gb_grid g, PBC b, int nrel
     }
 }
 
+// ------------------------------------------------------ coarse-level tail ---
+//
+// The V-cycle below a level of at most GB_TUNE_MG_TAIL columns in ONE launch
+// of one thread-block cluster (selectable; off by default, see tail_start).
+// Every level there costs a handful of launches of a few microseconds each
+// for little work, so the tail's levels run as
+// phases of one kernel separated by cluster barriers (hardware, no spin):
+// per level the pre-smoothing colours, the residual restricted to the next
+// level (with its correction zeroed), the level below, the prolongation and
+// the post-smoothing colours; on the coarsest level its nu_coarse
+// relaxations. A colour's relaxation is one phase: each warp takes whole
+// columns of the colour, each lane evaluates r = b - A x at its ceil(nz / 32)
+// levels (adotx_cell, the per-level kernels' residual) and the column's
+// factored Thomas solve runs as two warp scans of the recurrences' affine
+// maps (forward e', backward x), so a column costs a few shuffle steps
+// instead of nz dependent steps. A column's lateral neighbours are of the
+// other colour, which this phase does not write (levels with a periodic
+// direction of odd extent, where a column is its own colour's neighbour,
+// keep the per-level launches). The restriction evaluates the four fine
+// residuals of each coarse cell itself, so the residual never goes to memory.
+
+namespace cg = cooperative_groups;
+
+constexpr int kTailMaxLevels = 8;
+constexpr int kTailThreads = 512;
+
+template <typename T>
+struct TailLevel {
+    gb_grid g;
+    PBC b;
+    T* x;
+    T* bv;
+    const T* AX;
+    const T* AY;
+    const T* AZ;
+    const T* J;
+    MeshRatios<T> m;
+    const T* TD;
+    const T* TC;
+    const T* TU;
+};
+
+template <typename T>
+struct TailArgs {
+    TailLevel<T> lv[kTailMaxLevels];
+    int n;  // levels in the tail (the last is the coarsest)
+    int nu1, nu2, nu_coarse;
+};
+
+//! One colour's zebra relaxation of a tail level: a warp per column.
+template <typename T, int P>
+__device__ __forceinline__ void tail_relax(const TailLevel<T>& v, int color, int warp, int nwarps, int lane)
+{
+    constexpr unsigned kAll = 0xffffffffu;
+    const gb_grid& g = v.g;
+    const int half = (g.nx + 1) / 2;
+    const int ncc = half * g.ny;
+    const int nz = g.nz;
+    for (int cc = warp; cc < ncc; cc += nwarps) {
+        const int j = cc / half;
+        const int i = 2 * (cc % half) + ((j + color) & 1);
+        if (i >= g.nx) { continue; }
+        T R[P], D[P], IM[P], CP[P], X0[P];
+#pragma unroll
+        for (int q = 0; q < P; ++q) {
+            const int k = min(lane * P + q, nz - 1);
+            const int64_t o = at(g, i, j, k);
+            R[q] = v.bv[o] - adotx_cell<T>(g, v.b, i, j, k, v.x, v.AX, v.AY, v.AZ, v.J, v.m);
+            D[q] = v.TD[o];
+            IM[q] = v.TC[o];
+            CP[q] = v.TU[o];
+            X0[q] = v.x[o];
+        }
+        __syncwarp();
+        // e_k = (r_k - D_k e_{k-1}) / m_k over this lane's levels as e = al + be e_in
+        T al = T(0), be = T(1);
+#pragma unroll
+        for (int q = 0; q < P; ++q) {
+            const int k = lane * P + q;
+            if (k < nz) {
+                if (k == 0) {
+                    al = R[q] * IM[q];
+                    be = T(0);
+                } else {
+                    al = (R[q] - D[q] * al) * IM[q];
+                    be = (-D[q] * be) * IM[q];
+                }
+            }
+        }
+        for (int d = 1; d < 32; d <<= 1) {
+            const T al2 = __shfl_up_sync(kAll, al, d), be2 = __shfl_up_sync(kAll, be, d);
+            if (lane >= d) {
+                al = al + be * al2;
+                be = be * be2;
+            }
+        }
+        T ep = __shfl_up_sync(kAll, al, 1);
+        if (lane == 0) { ep = T(0); }
+#pragma unroll
+        for (int q = 0; q < P; ++q) {
+            const int k = lane * P + q;
+            if (k < nz) {
+                ep = (k == 0) ? R[q] * IM[q] : (R[q] - D[q] * ep) * IM[q];
+                R[q] = ep;
+            }
+        }
+        // x_k = e_k - c'_k x_{k+1} over this lane's levels as x = ga + de x_in
+        T ga = T(0), de = T(1);
+#pragma unroll
+        for (int q = P - 1; q >= 0; --q) {
+            const int k = lane * P + q;
+            if (k < nz) {
+                if (k == nz - 1) {
+                    ga = R[q];
+                    de = T(0);
+                } else {
+                    ga = R[q] - CP[q] * ga;
+                    de = -CP[q] * de;
+                }
+            }
+        }
+        for (int d = 1; d < 32; d <<= 1) {
+            const T ga2 = __shfl_down_sync(kAll, ga, d), de2 = __shfl_down_sync(kAll, de, d);
+            if (lane + d < 32) {
+                ga = ga + de * ga2;
+                de = de * de2;
+            }
+        }
+        T xk = __shfl_down_sync(kAll, ga, 1);
+        if (lane == 31) { xk = T(0); }
+#pragma unroll
+        for (int q = P - 1; q >= 0; --q) {
+            const int k = lane * P + q;
+            if (k < nz) {
+                xk = (k == nz - 1) ? R[q] : R[q] - CP[q] * xk;
+                v.x[at(g, i, j, k)] = X0[q] + xk;
+            }
+        }
+        __syncwarp();
+    }
+}
+
+//! The coarse right-hand side from the fine residual (restrict_cell with the
+//! four fine residuals evaluated in place, as k_apply does) and the coarse
+//! correction zeroed.
+template <typename T>
+__device__ __forceinline__ void tail_restrict(const TailLevel<T>& f, const TailLevel<T>& c, int t, int nt)
+{
+    const gb_grid& gf = f.g;
+    const gb_grid& gc = c.g;
+    const int n = gc.nx * gc.ny * gc.nz;
+    for (int e = t; e < n; e += nt) {
+        const int I = e % gc.nx, J2 = (e / gc.nx) % gc.ny, k = e / (gc.nx * gc.ny);
+        const int i = 2 * I, j = 2 * J2;
+        T r[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int ii = i + (q & 1), jj = j + (q >> 1);
+            r[q] = f.bv[at(gf, ii, jj, k)] - adotx_cell<T>(gf, f.b, ii, jj, k, f.x, f.AX, f.AY, f.AZ, f.J, f.m);
+        }
+        const T s = (f.J[at(gf, i, j, k)] * r[0] + f.J[at(gf, i + 1, j, k)] * r[1])
+                  + (f.J[at(gf, i, j + 1, k)] * r[2] + f.J[at(gf, i + 1, j + 1, k)] * r[3]);
+        c.bv[at(gc, I, J2, k)] = s / (T(4) * c.J[at(gc, I, J2, k)]);
+    }
+    const int vol = static_cast<int>(volume(gc));
+    for (int e = t; e < vol; e += nt) { c.x[e] = T(0); }
+}
+
+template <typename T>
+__device__ __forceinline__ void tail_prolong(const TailLevel<T>& c, const TailLevel<T>& f, int t, int nt)
+{
+    const gb_grid& gf = f.g;
+    const int n = gf.nx * gf.ny * gf.nz;
+    for (int e = t; e < n; e += nt) {
+        const int i = e % gf.nx, j = (e / gf.nx) % gf.ny, k = e / (gf.nx * gf.ny);
+        prolong_cell<T>(c.g, c.b, c.x, gf, f.x, i, j, k);
+    }
+}
+
+//! The tail of a V-cycle (TailArgs) as one cluster; P levels per lane.
+template <typename T, int P>
+__global__ void __launch_bounds__(kTailThreads) k_mg_tail(const __grid_constant__ TailArgs<T> a)
+{
+    cg::cluster_group cl = cg::this_cluster();
+    const int nb = static_cast<int>(cl.num_blocks());
+    const int rank = static_cast<int>(cl.block_rank());
+    const int wpb = static_cast<int>(blockDim.x) / 32;
+    const int warp = rank * wpb + static_cast<int>(threadIdx.x) / 32, nwarps = nb * wpb;
+    const int lane = static_cast<int>(threadIdx.x) & 31;
+    const int t = rank * static_cast<int>(blockDim.x) + static_cast<int>(threadIdx.x);
+    const int nt = nb * static_cast<int>(blockDim.x);
+    for (int l = 0; l < a.n - 1; ++l) {
+        for (int s = 0; s < a.nu1; ++s) {
+            for (int c = 0; c < 2; ++c) {
+                tail_relax<T, P>(a.lv[l], c, warp, nwarps, lane);
+                cl.sync();
+            }
+        }
+        tail_restrict<T>(a.lv[l], a.lv[l + 1], t, nt);
+        cl.sync();
+    }
+    for (int s = 0; s < a.nu_coarse; ++s) {
+        for (int c = 0; c < 2; ++c) {
+            tail_relax<T, P>(a.lv[a.n - 1], c, warp, nwarps, lane);
+            cl.sync();
+        }
+    }
+    for (int l = a.n - 2; l >= 0; --l) {
+        tail_prolong<T>(a.lv[l + 1], a.lv[l], t, nt);
+        cl.sync();
+        for (int s = 0; s < a.nu2; ++s) {
+            for (int c = 0; c < 2; ++c) {
+                tail_relax<T, P>(a.lv[l], c, warp, nwarps, lane);
+                cl.sync();
+            }
+        }
+    }
+}
+
 // --------------------------------------------------------- vector ops ---
 
 template <typename TD, typename TS>
@@ -1237,10 +1458,124 @@ void mg_residual(gb_poisson* P, PoissonLevels<T>& L, int l)
     ++ctx->launches;
 }
 
+//! The first level of the V-cycle's coarse tail (k_mg_tail), or -1: the
+//! levels from it down have at most GB_TUNE_MG_TAIL's columns, at most 128
+//! z-levels and no periodic direction of odd extent. Off by default: on
+//! config 1 the per-level launches measured as fast with the tail on the
+//! coarsest level alone and faster than any larger tail (0.464 ms per FP64
+//! V-cycle with the per-level launches or a tail of the 2 x 2 level, 0.488
+//! with the levels of at most 16 columns, 0.645 with those of at most 1024):
+//! the cluster's 16 SMs take longer over the levels' work than all SMs take
+//! over it plus the launches.
+template <typename T>
+int tail_start(const gb_poisson* P, const PoissonLevels<T>& L)
+{
+    const int knob = P->ctx->tune[GB_TUNE_MG_TAIL];
+    if (knob < 2) { return -1; }
+    const int maxcols = knob;
+    int start = -1;
+    for (int l = P->nlev - 1; l >= 0 && P->nlev - l <= kTailMaxLevels; --l) {
+        const gb_grid& g = L.g[l];
+        const bool ok = g.nx * g.ny <= maxcols && g.nz <= 128 && !(g.periodic_x && (g.nx & 1))
+                        && !(g.periodic_y && (g.ny & 1));
+        if (!ok) { break; }
+        start = l;
+    }
+    return start;
+}
+
+//! One launch of the tail kernel as a cluster of 16 blocks where the device
+//! schedules one (a non-portable size), else 8.
+template <typename T, int PL>
+cudaError_t launch_tail(gb_ctx* ctx, const TailArgs<T>& a)
+{
+    static std::atomic<int> csize{0};  // per instantiation, once per process (one device per process)
+    int nc = csize.load();
+    if (nc == 0) {
+        nc = 8;
+        if (cudaFuncSetAttribute(k_mg_tail<T, PL>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess) {
+            cudaLaunchConfig_t q{};
+            q.gridDim = dim3(16);
+            q.blockDim = dim3(kTailThreads);
+            cudaLaunchAttribute qa[1];
+            qa[0].id = cudaLaunchAttributeClusterDimension;
+            qa[0].val.clusterDim.x = 16;
+            qa[0].val.clusterDim.y = 1;
+            qa[0].val.clusterDim.z = 1;
+            q.attrs = qa;
+            q.numAttrs = 1;
+            int nclusters = 0;
+            if (cudaOccupancyMaxActiveClusters(&nclusters, k_mg_tail<T, PL>, &q) == cudaSuccess && nclusters > 0) {
+                nc = 16;
+            }
+        }
+        cudaGetLastError();
+        csize.store(nc);
+    }
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(nc);
+    cfg.blockDim = dim3(kTailThreads);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = ctx->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = nc;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, k_mg_tail<T, PL>, a);
+}
+
+//! The V-cycle from level l down (l = tail_start) in one cluster launch.
+template <typename T>
+bool mg_tail(gb_poisson* P, PoissonLevels<T>& L, int l)
+{
+    gb_ctx* ctx = P->ctx;
+    TailArgs<T> a{};
+    a.n = P->nlev - l;
+    a.nu1 = P->opt.nu1;
+    a.nu2 = P->opt.nu2;
+    a.nu_coarse = P->opt.nu_coarse;
+    for (int q = 0; q < a.n; ++q) {
+        const int m = l + q;
+        TailLevel<T>& v = a.lv[q];
+        v.g = L.g[m];
+        v.b = L.b[m];
+        v.x = L.x[m];
+        v.bv = L.bv[m];
+        v.AX = L.AX[m];
+        v.AY = L.AY[m];
+        v.AZ = L.AZ[m];
+        v.J = L.J[m];
+        v.m = L.ratios(m);
+        v.TD = L.TD[m];
+        v.TC = L.TC[m];
+        v.TU = L.TU[m];
+    }
+    const int pl = (L.g[l].nz + 31) / 32;
+    Span span(ctx, GB_KERNEL_MG_SMOOTH);
+    cudaError_t e = cudaErrorInvalidValue;
+    switch (pl) {
+    case 1: e = launch_tail<T, 1>(ctx, a); break;
+    case 2: e = launch_tail<T, 2>(ctx, a); break;
+    case 3: e = launch_tail<T, 3>(ctx, a); break;
+    case 4: e = launch_tail<T, 4>(ctx, a); break;
+    default: break;
+    }
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    ++ctx->launches;
+    return true;
+}
+
 template <typename T>
 void vcycle(gb_poisson* P, PoissonLevels<T>& L, int l)
 {
     gb_ctx* ctx = P->ctx;
+    if (l == tail_start(P, L) && mg_tail(P, L, l)) { return; }
     if (l == P->nlev - 1) {
         const gb_grid& g = L.g[l];
         const size_t smem = static_cast<size_t>(5) * g.nx * g.ny * g.nz * sizeof(T);

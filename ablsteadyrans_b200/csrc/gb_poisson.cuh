@@ -97,28 +97,24 @@ __device__ __forceinline__ T xoff(const T* x, const gb_grid& g, const PBC& b, in
     return ldc<T>(x, x, g, b, i + di, j + dj, k + dk);
 }
 
-//! The terrain operator at cell (i, j, k): terrpoisson_adotx
-//! (ERF_TerrainPoisson_3D_K.H:316-530) with the premultiplied areas a beta and
-//! the zero-flux mask, the mesh ratios precomputed (MeshRatios): the same
-//! operations in the same order on the same values, without its ~19 divisions
-//! per cell. INTERIOR:
-//! every neighbour read lies in the valid cells (no ghost resolution). x is
-//! not declared restrict: one kernel may update it between applications.
-template <typename T, bool INTERIOR>
-__device__ __forceinline__ T adotx_r(const gb_grid& g, const PBC& b, int i, int j, int k, const T* x,
-                                     const T* __restrict__ axa, const T* __restrict__ aya, const T* __restrict__ aza,
-                                     const T* __restrict__ Jc, const MeshRatios<T>& m)
+//! The terrain operator at cell (i, j, k) with the iterate's 15 values read by
+//! X(di, dj, dk): terrpoisson_adotx (ERF_TerrainPoisson_3D_K.H:316-530) with
+//! the premultiplied areas a beta and the zero-flux mask (MASKS: the cell may
+//! touch a boundary), the mesh ratios precomputed (MeshRatios): the same
+//! operations in the same order on the same values, without its ~19
+//! divisions per cell.
+template <typename T, bool MASKS, typename XA>
+__device__ __forceinline__ T adotx_body(const gb_grid& g, const PBC& b, int i, int j, int k, int64_t o, XA&& X,
+                                        const T* __restrict__ axa, const T* __restrict__ aya, const T* __restrict__ aza,
+                                        const T* __restrict__ Jc, const MeshRatios<T>& m)
 {
     const T dxinv = static_cast<T>(1.0 / g.dx), dyinv = static_cast<T>(1.0 / g.dy), dzinv = static_cast<T>(1.0 / g.dzeta);
     const T h = T(0.5);
-    const int64_t o = at(g, i, j, k);
-#define X(di, dj, dk) xoff<T, INTERIOR>(x, g, b, o, i, j, k, di, dj, dk)
     const T x000 = X(0, 0, 0), xp00 = X(1, 0, 0), xm00 = X(-1, 0, 0), x0p0 = X(0, 1, 0), x0m0 = X(0, -1, 0);
     const T x00p = X(0, 0, 1), x00m = X(0, 0, -1);
     const T xp0p = X(1, 0, 1), xp0m = X(1, 0, -1), xm0p = X(-1, 0, 1), xm0m = X(-1, 0, -1);
     const T x0pp = X(0, 1, 1), x0pm = X(0, 1, -1), x0mp = X(0, -1, 1), x0mm = X(0, -1, -1);
-#undef X
-    const int64_t sy = g.sy, sz = g.sz;
+    const int sy = static_cast<int>(g.sy), sz = static_cast<int>(g.sz);
     T px_hi = (xp00 - x000) * dxinv;
     T pz_hi_md_hi = h * (xp0p + x00p - xp00 - x000);
     pz_hi_md_hi *= m.rx[o + 1 + sz];
@@ -164,7 +160,7 @@ __device__ __forceinline__ T adotx_r(const gb_grid& g, const PBC& b, int i, int 
     const T py_md_lo_lo = h * (x000 - x0m0 + x00m - x0mm) * dyinv;
     pz_lo -= h * m.sx[o] * ((px_hi_md_lo + px_lo_md_lo) - (pz_hi_md_lo + pz_lo_md_lo));
     pz_lo -= h * m.sy[o] * ((py_md_hi_lo + py_md_lo_lo) - (pz_md_hi_lo + pz_md_lo_lo));
-    if (!INTERIOR) {
+    if (MASKS) {
         if (k == 0) { pz_lo = T(0); }
         if ((b.zf & TP_XLO) && i == 0) { px_lo = T(0); }
         if ((b.zf & TP_XHI) && i == g.nx - 1) { px_hi = T(0); }
@@ -178,15 +174,59 @@ __device__ __forceinline__ T adotx_r(const gb_grid& g, const PBC& b, int i, int 
     return y / Jc[o];
 }
 
-//! adotx_r at any valid cell: the direct form where all 18 neighbours are valid cells.
+//! The operator at (i, j, k) with the neighbours read directly (INTERIOR: all
+//! 18 lie in the valid cells) or through ldc's ghost resolution. x is not
+//! declared restrict: one kernel may update it between applications.
+template <typename T, bool INTERIOR>
+__device__ __forceinline__ T adotx_r(const gb_grid& g, const PBC& b, int i, int j, int k, const T* x,
+                                     const T* __restrict__ axa, const T* __restrict__ aya, const T* __restrict__ aza,
+                                     const T* __restrict__ Jc, const MeshRatios<T>& m)
+{
+    const int64_t o = at(g, i, j, k);
+    auto X = [&](int di, int dj, int dk) { return xoff<T, INTERIOR>(x, g, b, o, i, j, k, di, dj, dk); };
+    return adotx_body<T, !INTERIOR>(g, b, i, j, k, o, X, axa, aya, aza, Jc, m);
+}
+
+//! One direction's neighbour indices of index i (n cells) and their mirror
+//! signs: i - 1, i + 1 wrapped (periodic) or reflected into the cell itself
+//! with the face's sign (ldc's resolution for offsets of one).
+__device__ __forceinline__ void resolve_neighbours(int i, int n, int periodic, int s_lo, int s_hi, int& im, int& ip,
+                                                   int& sm, int& sp)
+{
+    const bool lo = (i == 0), hi = (i == n - 1);
+    im = lo ? (periodic ? n - 1 : 0) : i - 1;
+    ip = hi ? (periodic ? 0 : n - 1) : i + 1;
+    sm = (lo && !periodic) ? s_lo : 1;
+    sp = (hi && !periodic) ? s_hi : 1;
+}
+
+//! adotx at any valid cell, one code path for every cell (no divergence
+//! between a warp's interior and boundary lanes): each direction's neighbour
+//! indices and mirror signs resolved once, a neighbour's value the product of
+//! its directions' signs (+-1, exact) times one load at the resolved point,
+//! ldc's value (the composition of per-direction reflections and shifts).
 template <typename T>
 __device__ __forceinline__ T adotx_cell(const gb_grid& g, const PBC& b, int i, int j, int k, const T* x,
                                         const T* __restrict__ axa, const T* __restrict__ aya,
                                         const T* __restrict__ aza, const T* __restrict__ Jc, const MeshRatios<T>& m)
 {
-    const bool inside = i > 0 && i < g.nx - 1 && j > 0 && j < g.ny - 1 && k > 0 && k < g.nz - 1;
-    return inside ? adotx_r<T, true>(g, b, i, j, k, x, axa, aya, aza, Jc, m)
-                  : adotx_r<T, false>(g, b, i, j, k, x, axa, aya, aza, Jc, m);
+    int im, ip, sim, sip, jm, jp, sjm, sjp;
+    resolve_neighbours(i, g.nx, b.per_x, b.sxl, b.sxh, im, ip, sim, sip);
+    resolve_neighbours(j, g.ny, b.per_y, b.syl, b.syh, jm, jp, sjm, sjp);
+    const int km = (k == 0) ? 0 : k - 1, kp = (k == g.nz - 1) ? k : k + 1;
+    const int skm = (k == 0) ? b.szl : 1, skp = (k == g.nz - 1) ? b.szh : 1;
+    const int sy = static_cast<int>(g.sy), sz = static_cast<int>(g.sz);
+    const int ng = g.ng;
+    const int cx[3] = {im + ng, i + ng, ip + ng};
+    const int cy[3] = {(jm + ng) * sy, (j + ng) * sy, (jp + ng) * sy};
+    const int cz[3] = {(km + ng) * sz, (k + ng) * sz, (kp + ng) * sz};
+    const int sx3[3] = {sim, 1, sip}, sy3[3] = {sjm, 1, sjp}, sz3[3] = {skm, 1, skp};
+    auto X = [&](int di, int dj, int dk) {
+        const T v = x[cx[di + 1] + cy[dj + 1] + cz[dk + 1]];
+        return (sx3[di + 1] * sy3[dj + 1] * sz3[dk + 1] < 0) ? -v : v;
+    };
+    const int64_t o = at(g, i, j, k);
+    return adotx_body<T, true>(g, b, i, j, k, o, X, axa, aya, aza, Jc, m);
 }
 
 //! The principal tridiagonal of the operator on column (i, j) at level k

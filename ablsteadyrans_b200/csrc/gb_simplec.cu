@@ -171,21 +171,32 @@ __global__ void k_sum_partials(const double* __restrict__ partial, int n, double
 //! The mean of f over one k-plane of box b per block (block k: level k),
 //! summed in a fixed order (Predictor.cpp:286-306: the horizontal mean of the
 //! other component's residual per level, every face once).
-__global__ void k_level_mean(gb_grid g, Box b, const double* __restrict__ f, double npts_level, double* __restrict__ mean)
+//! One block per level (blockDim.x = kLevelThreads): each thread sums its
+//! points in four independent partial sums (loads in flight together, a
+//! fixed order), then the block reduces them in a fixed tree.
+constexpr int kLevelThreads = 1024;
+
+__global__ void __launch_bounds__(kLevelThreads) k_level_mean(gb_grid g, Box b, const double* __restrict__ f,
+                                                              double npts_level, double* __restrict__ mean)
 {
-    __shared__ double red[8];
+    __shared__ double red[kLevelThreads / 32];
     const int k = blockIdx.x;
     const int nx = b.hi[0] - b.lo[0] + 1, ny = b.hi[1] - b.lo[1] + 1;
-    double s = 0;
-    for (int n = threadIdx.x; n < nx * ny; n += blockDim.x) {
-        const int i = b.lo[0] + n % nx, j = b.lo[1] + n / nx;
-        s += f[at(g, i, j, k)];
+    const int np = nx * ny;
+    double s4[4] = {0, 0, 0, 0};
+    for (int n0 = threadIdx.x; n0 < np; n0 += 4 * kLevelThreads) {
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int n = n0 + u * kLevelThreads;
+            if (n < np) { s4[u] += f[at(g, b.lo[0] + n % nx, b.lo[1] + n / nx, k)]; }
+        }
     }
+    double s = (s4[0] + s4[1]) + (s4[2] + s4[3]);
     s = warp_sum(s);
     if ((threadIdx.x & 31) == 0) { red[threadIdx.x >> 5] = s; }
     __syncthreads();
     if (threadIdx.x < 32) {
-        double t = (threadIdx.x < 8) ? red[threadIdx.x] : 0.0;
+        double t = red[threadIdx.x];
         t = warp_sum(t);
         if (threadIdx.x == 0) { mean[k] = t / npts_level; }
     }
@@ -217,6 +228,97 @@ __global__ void __launch_bounds__(256) k_maxabs(gb_grid g, Box b, const double* 
         double t = (threadIdx.x < (blockDim.x >> 5)) ? red[threadIdx.x] : 0.0;
         t = warp_max_nan(t);
         if (threadIdx.x == 0) { atomic_max_nonneg(slot, t); }
+    }
+}
+
+//! Several reductions in one launch (blockIdx.y picks the item): each item
+//! reduces exactly as its single launch does (the same blocks, threads and
+//! order), so the sums are the same bits.
+constexpr int kMaxRed = 8;
+struct RedItem {
+    Box b;
+    const double* f;
+    const double* mul;
+    int mode;   // sums: 0 squares, 1 values
+    int slot;   // sums: the result slot; maxima: the result word
+};
+struct RedPack {
+    RedItem it[kMaxRed];
+    int n;
+};
+
+__global__ void k_sumsq_partial_many(gb_grid g, const __grid_constant__ RedPack P, double* __restrict__ partial)
+{
+    const RedItem& it = P.it[blockIdx.y];
+    const Box b = it.b;
+    const double* __restrict__ f = it.f;
+    const int mode = it.mode;
+    __shared__ double red[8];
+    double s = 0;
+    const int64_t n_tot = b.count();
+    const int nx = b.hi[0] - b.lo[0] + 1, ny = b.hi[1] - b.lo[1] + 1;
+    for (int64_t n = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; n < n_tot;
+         n += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int i = b.lo[0] + static_cast<int>(n % nx);
+        const int j = b.lo[1] + static_cast<int>((n / nx) % ny);
+        const int k = b.lo[2] + static_cast<int>(n / (static_cast<int64_t>(nx) * ny));
+        const double v = f[at(g, i, j, k)];
+        s += (mode == 0) ? v * v : v;
+    }
+    s = warp_sum(s);
+    if ((threadIdx.x & 31) == 0) { red[threadIdx.x >> 5] = s; }
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double t = (threadIdx.x < 8) ? red[threadIdx.x] : 0.0;
+        t = warp_sum(t);
+        if (threadIdx.x == 0) { partial[it.slot * gridDim.x + blockIdx.x] = t; }
+    }
+}
+
+__global__ void k_sum_partials_many(const __grid_constant__ RedPack P, const double* __restrict__ partial, int nb,
+                                    double* __restrict__ out)
+{
+    const int slot = P.it[blockIdx.x].slot;
+    __shared__ double red[8];
+    double s = 0;
+    for (int t = threadIdx.x; t < nb; t += blockDim.x) { s += partial[slot * nb + t]; }
+    s = warp_sum(s);
+    if ((threadIdx.x & 31) == 0) { red[threadIdx.x >> 5] = s; }
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double t = (threadIdx.x < 8) ? red[threadIdx.x] : 0.0;
+        t = warp_sum(t);
+        if (threadIdx.x == 0) { out[slot] = t; }
+    }
+}
+
+__global__ void __launch_bounds__(256) k_maxabs_many(gb_grid g, const __grid_constant__ RedPack P,
+                                                     unsigned long long* __restrict__ words)
+{
+    const RedItem& it = P.it[blockIdx.y];
+    const Box b = it.b;
+    const double* __restrict__ f = it.f;
+    const double* __restrict__ mul = it.mul;
+    __shared__ double red[8];
+    const int nx = b.hi[0] - b.lo[0] + 1, ny = b.hi[1] - b.lo[1] + 1, nz = b.hi[2] - b.lo[2] + 1;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int r = blockIdx.x * (blockDim.x >> 5) + warp;
+    double v = 0;
+    if (r < ny * nz) {
+        const int64_t o0 = at(g, b.lo[0], b.lo[1] + r % ny, b.lo[2] + r / ny);
+#pragma unroll 4
+        for (int i = lane; i < nx; i += 32) {
+            const double a = fabs(mul ? f[o0 + i] * mul[o0 + i] : f[o0 + i]);
+            v = (a > v || a != a) ? a : v;
+        }
+    }
+    v = warp_max_nan(v);
+    if (lane == 0) { red[warp] = v; }
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double t = (threadIdx.x < (blockDim.x >> 5)) ? red[threadIdx.x] : 0.0;
+        t = warp_max_nan(t);
+        if (threadIdx.x == 0) { atomic_max_nonneg(words + it.slot, t); }
     }
 }
 
@@ -382,6 +484,56 @@ void dmax(gb_simplec* S, const Box& b, const double* f, const double* mul, int w
     ++ctx->launches;
 }
 
+//! dsum of several arrays in two launches (the items' slots into w.sums).
+void dsum_many(gb_simplec* S, const RedPack& P)
+{
+    gb_ctx* ctx = S->ctx;
+    if (P.n <= 0) { return; }
+    Span span(ctx, GB_KERNEL_VECTOR);
+    k_sumsq_partial_many<<<dim3(kRedBlocks, P.n), 256, 0, ctx->stream>>>(S->g, P, S->w.partial);
+    k_sum_partials_many<<<P.n, 256, 0, ctx->stream>>>(P, S->w.partial, kRedBlocks, S->w.sums);
+    ctx->launches += 2;
+}
+
+//! dmax of several arrays in one launch (the items' slots are result words).
+void dmax_many(gb_simplec* S, const RedPack& P)
+{
+    gb_ctx* ctx = S->ctx;
+    if (P.n <= 0) { return; }
+    int rows = 1;
+    for (int q = 0; q < P.n; ++q) {
+        const Box& b = P.it[q].b;
+        rows = std::max(rows, (b.hi[1] - b.lo[1] + 1) * (b.hi[2] - b.lo[2] + 1));
+    }
+    Span span(ctx, GB_KERNEL_VECTOR);
+    k_maxabs_many<<<dim3((rows + 7) / 8, P.n), 256, 0, ctx->stream>>>(S->g, P, dword(ctx, 0));
+    ++ctx->launches;
+}
+
+//! A reduction item.
+RedItem red_item(const Box& b, const double* f, const double* mul, int mode, int slot)
+{
+    RedItem it{};
+    it.b = b;
+    it.f = f;
+    it.mul = mul;
+    it.mode = mode;
+    it.slot = slot;
+    return it;
+}
+
+//! The three velocity components' max |.| into words w0, w0 + 1, w0 + 2.
+void dmax_velocity(gb_simplec* S, const double* u, const double* v, const double* w, int w0)
+{
+    const gb_grid& g = S->g;
+    RedPack P{};
+    P.it[0] = red_item(valid_box(g, XF), u, nullptr, 0, w0);
+    P.it[1] = red_item(valid_box(g, YF), v, nullptr, 0, w0 + 1);
+    P.it[2] = red_item(valid_box(g, ZF), w, nullptr, 0, w0 + 2);
+    P.n = 3;
+    dmax_many(S, P);
+}
+
 // ---------------------------------------------------------- ghost fills ---
 
 struct FieldPtrs {
@@ -483,13 +635,19 @@ void fill_side(gb_simplec* S, const gb_state& q, int d, bool lo, bool homog = fa
         b.lo[e] = grow ? -ng : 0;
         b.hi[e] = ((e == 0) ? g.nx : (e == 1) ? g.ny : g.nz) + (grow ? ng : 0);
     }
+    // one thread per (point, field): the fields' fills are independent (each
+    // reads only its own array), so the six run side by side; the layer
+    // index along d carries the field (layer + (ng + 1) * field)
     b.lo[d] = 0;
-    b.hi[d] = ng;
+    b.hi[d] = 6 * (ng + 1) - 1;
     const int pe0 = per[0], pe1 = per[1];
-    for_box(S->ctx, b, [=] __device__(int i, int j, int k) {
-        int c[3] = {i, j, k};
+    for_box(S->ctx, b, [=] __device__(int i0, int j0, int k0) {
+        int c[3] = {i0, j0, k0};
+        const int n = c[d] / (ng + 1);
+        c[d] -= n * (ng + 1);
         const int layer = c[d];
-        for (int n = 0; n < 6; ++n) {
+        const int i = c[0], j = c[1], k = c[2];
+        {
             const FieldFill& F = P.F[n];
             const int t = F.t;
             // this field's slab extent in the other directions
@@ -501,13 +659,13 @@ void fill_side(gb_simplec* S, const gb_state& q, int d, bool lo, bool homog = fa
                 const int lo_e = grow ? -ng : 0, hi_e = nv - 1 + (grow ? ng : 0);
                 if (c[e] < lo_e || c[e] > hi_e) { inside = false; }
             }
-            if (!inside) { continue; }
+            if (!inside) { return; }
             const int nd = (d == 0) ? g.nx : (d == 1) ? g.ny : g.nz;
             const bool nod = nodal(t, d);
             double* a = F.a;
             if (F.rule == R_GRADIENT) {
                 // the top or a surface_layer ground (d == 2): one thread per column does both layers
-                if (layer != 1) { continue; }
+                if (layer != 1) { return; }
                 const int edge = lo ? 0 : nd - 1 + nod;
                 const int c1 = lo ? edge + 1 : edge - 1, g1 = lo ? edge - 1 : edge + 1, g2 = lo ? edge - 2 : edge + 2;
                 const double zc1 = point_z(z, g, t, i, j, c1), zg1 = point_z(z, g, t, i, j, g1),
@@ -516,16 +674,16 @@ void fill_side(gb_simplec* S, const gb_state& q, int d, bool lo, bool homog = fa
                 const double v1 = a[at(g, i, j, c1)] + (zg1 - zc1) * Gp;
                 a[at(g, i, j, g1)] = v1;
                 a[at(g, i, j, g2)] = v1 + (zg2 - zg1) * Gp;
-                continue;
+                return;
             }
             const int edge = lo ? 0 : (nod ? nd : nd - 1);
             if (layer == 0) {
-                if (!(nod && (F.rule == R_VALUE || F.rule == R_PROFILE))) { continue; }
+                if (!(nod && (F.rule == R_VALUE || F.rule == R_PROFILE))) { return; }
                 int p[3] = {i, j, k};
                 p[d] = edge;
                 a[at(g, p[0], p[1], p[2])] = (F.rule == R_PROFILE && !homog)
                     ? prof.value(F.f, height_above_ground(z, g, t, p[0], p[1], p[2])) : F.V;
-                continue;
+                return;
             }
             const int gidx = lo ? edge - layer : edge + layer;
             const int mirror = nod ? 2 * edge : (lo ? 2 * edge - 1 : 2 * edge + 1);
@@ -1757,6 +1915,23 @@ enum Word : int {
 };
 enum Sum : int { SUM_R0 = 0, SUM_TKE = 6, SUM_USTAR = 7, SUM_LEVEL = 8, SUM_COUNT = 8 };
 
+//! The six residuals' sums of squares, k's sum and (a surface_layer ground)
+//! the domain columns' u* sum (the u* plane is the k = -ng layer of the
+//! indexing) in two launches.
+void residual_sums(gb_simplec* S, const gb_state& q)
+{
+    const gb_grid& g = S->g;
+    RedPack P{};
+    for (int n = 0; n < 6; ++n) { P.it[n] = red_item(valid_box(g, kLoc[n]), S->w.R[n], nullptr, 0, SUM_R0 + n); }
+    P.it[6] = red_item(valid_box(g, CC), q.tke, nullptr, 1, SUM_TKE);
+    P.n = 7;
+    if (S->wall) {
+        P.it[7] = red_item(Box{{0, 0, -g.ng}, {g.nx - 1, g.ny - 1, -g.ng}}, S->ss[kSsUstar], nullptr, 1, SUM_USTAR);
+        P.n = 8;
+    }
+    dsum_many(S, P);
+}
+
 gb_status momentum_predictor(gb_simplec* S, const gb_state& q, double** R)
 {
     gb_ctx* ctx = S->ctx;
@@ -1823,7 +1998,7 @@ gb_status momentum_predictor(gb_simplec* S, const gb_state& q, double** R)
                 Box b = valid_box(g, to);
                 if (per_o) { b.hi[d_o] -= 1; }
                 Span span(ctx, GB_KERNEL_VECTOR);
-                k_level_mean<<<g.nz, 256, 0, ctx->stream>>>(g, b, other, npts_level, w.level_sum);
+                k_level_mean<<<g.nz, kLevelThreads, 0, ctx->stream>>>(g, b, other, npts_level, w.level_sum);
                 ++ctx->launches;
             }
             double* mean = w.level_sum;
@@ -1902,9 +2077,9 @@ gb_status momentum_predictor(gb_simplec* S, const gb_state& q, double** R)
     const int words[3] = {W_LAST_U, W_LAST_V, W_LAST_W};
     gb_status st = line_solve_multi(S, 3, locs, w.Am, w.ap, w.rhsm, w.deltam, words);
     if (st != GB_OK) { return st; }
+    dmax_velocity(S, w.deltam[0], w.deltam[1], w.deltam[2], W_MAX_DU);
     for (int c = 0; c < 3; ++c) {
         const int t = 1 << c;
-        dmax(S, valid_box(g, t), w.deltam[c], nullptr, W_MAX_DU + c);
         double* qc = comps[c];
         const double* delta = w.deltam[c];
         for_box(ctx, valid_box(g, t), [=] __device__(int i, int j, int k) {
@@ -1943,10 +2118,15 @@ gb_status pressure_prelude(gb_simplec* S, const gb_state& q, const double* sourc
             rhs[o] -= source[o];
         }, GB_KERNEL_MASSFLUX);
     }
-    dmax(S, valid_box(g, CC), w.rhs, nullptr, W_DIV_BEFORE);
-    dmax(S, valid_box(g, XF), q.u, nullptr, W_SPEED_U);
-    dmax(S, valid_box(g, YF), q.v, nullptr, W_SPEED_V);
-    dmax(S, valid_box(g, ZF), q.w, nullptr, W_SPEED_W);
+    {
+        RedPack P{};
+        P.it[0] = red_item(valid_box(g, CC), w.rhs, nullptr, 0, W_DIV_BEFORE);
+        P.it[1] = red_item(valid_box(g, XF), q.u, nullptr, 0, W_SPEED_U);
+        P.it[2] = red_item(valid_box(g, YF), q.v, nullptr, 0, W_SPEED_V);
+        P.it[3] = red_item(valid_box(g, ZF), q.w, nullptr, 0, W_SPEED_W);
+        P.n = 4;
+        dmax_many(S, P);
+    }
     return poisson_set_coeffs(S->poisson, S->mesh.ax, S->mesh.ay, S->mesh.az, w.beta[0], w.beta[1], w.beta[2]);
 }
 
@@ -1994,8 +2174,13 @@ gb_status pressure_finish(gb_simplec* S, const gb_state& q)
         const int64_t o = at(g, i, j, k);
         p[o] += alpha * phi[o];
     });
-    dmax(S, valid_box(g, CC), w.phi, nullptr, W_MAX_PHI);
-    for (int c = 0; c < 3; ++c) { dmax(S, valid_box(g, kLoc[c]), F[c], w.keep[c], W_MAX_FU + c); }
+    {
+        RedPack P{};
+        P.it[0] = red_item(valid_box(g, CC), w.phi, nullptr, 0, W_MAX_PHI);
+        for (int c = 0; c < 3; ++c) { P.it[1 + c] = red_item(valid_box(g, kLoc[c]), F[c], w.keep[c], 0, W_MAX_FU + c); }
+        P.n = 4;
+        dmax_many(S, P);
+    }
     omega_from_w(S, q.u, q.v, q.w, w.om);
     double* tgt[3] = {q.u, q.v, w.om};
     for (int c = 0; c < 3; ++c) {
@@ -2181,15 +2366,8 @@ gb_status simplec_iterate(gb_simplec* S, const gb_state& q, const double* dtau, 
     if (S->ph.closure) {
         cudaMemcpyAsync(S->nu_dtau, S->cf[kClosureNu], sizeof(double) * volume(g), cudaMemcpyDeviceToDevice, ctx->stream);
     }
-    for (int n = 0; n < 6; ++n) { dsum(S, valid_box(g, kLoc[n]), w.R[n], 0, SUM_R0 + n); }
-    dsum(S, valid_box(g, CC), q.tke, 1, SUM_TKE);
-    if (S->wall) {
-        // the u* plane of the domain columns (a plane is the k = -ng layer of the indexing)
-        dsum(S, Box{{0, 0, -g.ng}, {g.nx - 1, g.ny - 1, -g.ng}}, S->ss[kSsUstar], 1, SUM_USTAR);
-    }
-    dmax(S, valid_box(g, XF), q.u, nullptr, W_MON_U);
-    dmax(S, valid_box(g, YF), q.v, nullptr, W_MON_V);
-    dmax(S, valid_box(g, ZF), q.w, nullptr, W_MON_W);
+    residual_sums(S, q);
+    dmax_velocity(S, q.u, q.v, q.w, W_MON_U);
     transport_fluxes(S, q, w.F[0], w.F[1], w.F[2]);
     face_dtau(S, dtau, w.dtf);
     gb_status s1 = momentum_predictor(S, q, w.R);
@@ -2475,9 +2653,7 @@ gb_status simplec_linear_setup(gb_simplec* S, const gb_state& q, const double* d
     face_dtau(S, S->lin_dtau, w.dtf);
     convection<CC>(S, q.theta, S->lin_F0, S->ph.limiter, S->ph.smooth_eps_theta, false, S->lin_conv0);
     cudaMemsetAsync(dword(ctx, W_SPEED_U), 0, sizeof(unsigned long long) * 3, ctx->stream);
-    dmax(S, valid_box(g, XF), q.u, nullptr, W_SPEED_U);
-    dmax(S, valid_box(g, YF), q.v, nullptr, W_SPEED_V);
-    dmax(S, valid_box(g, ZF), q.w, nullptr, W_SPEED_W);
+    dmax_velocity(S, q.u, q.v, q.w, W_SPEED_U);
     unsigned long long sp[3];
     if ((st = read_words(ctx, W_SPEED_U, 3, sp)) != GB_OK) { return st; }
     S->lin_speed = std::max(1.0, std::max(bits_to_double(sp[0]), std::max(bits_to_double(sp[1]), bits_to_double(sp[2]))));
@@ -2553,9 +2729,7 @@ gb_status simplec_linear_apply(gb_simplec* S, const gb_state& q, const double* c
     double sigma = 1.0;
     if (diagonal) {
         cudaMemsetAsync(dword(ctx, W_MAX_DU), 0, sizeof(unsigned long long) * 3, ctx->stream);
-        dmax(S, valid_box(g, XF), S->lin_d[F_U], nullptr, W_MAX_DU);
-        dmax(S, valid_box(g, YF), S->lin_d[F_V], nullptr, W_MAX_DV);
-        dmax(S, valid_box(g, ZF), S->lin_d[F_W], nullptr, W_MAX_DW);
+        dmax_velocity(S, S->lin_d[F_U], S->lin_d[F_V], S->lin_d[F_W], W_MAX_DU);
         unsigned long long md[3];
         if ((st = read_words(ctx, W_MAX_DU, 3, md)) != GB_OK) { return st; }
         const double dmx = std::max(bits_to_double(md[0]), std::max(bits_to_double(md[1]), bits_to_double(md[2])));
@@ -2629,12 +2803,8 @@ gb_status simplec_norms(gb_simplec* S, const gb_state& q, double* res, double* m
     cudaMemsetAsync(dword(ctx, 0), 0, sizeof(unsigned long long) * W_COUNT, ctx->stream);
     fill_ghosts_into(S, q, S->ss);
     simplec_residual(S, q, w.R);
-    for (int n = 0; n < 6; ++n) { dsum(S, valid_box(g, kLoc[n]), w.R[n], 0, SUM_R0 + n); }
-    dsum(S, valid_box(g, CC), q.tke, 1, SUM_TKE);
-    if (S->wall) { dsum(S, Box{{0, 0, -g.ng}, {g.nx - 1, g.ny - 1, -g.ng}}, S->ss[kSsUstar], 1, SUM_USTAR); }
-    dmax(S, valid_box(g, XF), q.u, nullptr, W_MON_U);
-    dmax(S, valid_box(g, YF), q.v, nullptr, W_MON_V);
-    dmax(S, valid_box(g, ZF), q.w, nullptr, W_MON_W);
+    residual_sums(S, q);
+    dmax_velocity(S, q.u, q.v, q.w, W_MON_U);
     unsigned long long words[W_COUNT];
     gb_status st = read_words(ctx, 0, W_COUNT, words);
     if (st != GB_OK) { return st; }

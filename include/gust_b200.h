@@ -132,6 +132,9 @@ enum {
                                    face evaluated once per block, 8 levels per block), 1 one thread per
                                    point (the residual's fluxes and divergences as separate launches),
                                    N >= 2 the per-equation launch with N levels per block */
+    GB_TUNE_MG_TAIL,            /* the V-cycle's coarse levels as one thread-block-cluster launch: 0 default
+                                   and 1 off (per-level launches), N >= 2 the levels of at most N columns
+                                   (measured no faster: the cluster's 16 SMs do the levels' work) */
     GB_N_TUNE
 };
 gb_status gb_ctx_tune(gb_ctx* ctx, int32_t key, int32_t value);

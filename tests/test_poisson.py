@@ -168,8 +168,70 @@ def test_gpu_vcycle_matches_oracle_fp64(ctx, per, kernel, relax, solve):
     ctx.tune(gb.TUNE_MG_COARSE_KERNEL, 0)
     ctx.tune(gb.TUNE_MG_FUSED_RELAX, 0)
     ctx.tune(gb.TUNE_MG_SOLVE, 0)
+    ctx.tune(gb.TUNE_MG_TAIL, 0)
     assert rel_err(e, e_ref, g.valid(0)) < 1e-12
     ps.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("tail", [1024, 0, 64], ids=["tail-1024-columns", "per-level", "tail-64-columns"])
+@pytest.mark.parametrize("case", [(32, 24, 16, False, False), (64, 48, 24, True, False), (40, 32, 70, False, True),
+                                  (16, 16, 129, True, True)])
+def test_gpu_vcycle_tail_matches_oracle_fp64(ctx, case, tail):
+    """The V-cycle's coarse levels as one thread-block-cluster launch
+    (GB_TUNE_MG_TAIL N: the levels of at most N columns) agree with the
+    oracle's V-cycle to 1e-12, as the per-level launches (0, the default)
+    do: the whole hierarchy in the tail, part of it, 16 to 70
+    z-levels (one to three levels a lane), and a column of 129 levels,
+    which keeps the per-level launches."""
+    import ablsteadyrans_b200 as gb
+    nx, ny, nz, px, py = case
+    g, z, J, ax, ay, az, _ = smooth_terrain_case(nx, ny, nz, px, py, hill=150.0)
+    bc = (PERIODIC if px else NEUMANN, PERIODIC if py else NEUMANN, NEUMANN,
+          PERIODIC if px else DIRICHLET, PERIODIC if py else NEUMANN, DIRICHLET)
+    rng = np.random.default_rng(8)
+    r = g.np_zeros()
+    r[g.valid(0)] = rng.standard_normal(r[g.valid(0)].shape)
+    mg = oracle.Multigrid(g, bc, z, J, ax, ay, az, max_levels=12, min_coarse=2, nu1=1, nu2=1, nu_coarse=8)
+    e_ref = mg.vcycle(r)
+    dz, dJ, dax, day, daz = _gpu_case(g, z, J, ax, ay, az)
+    opts = gb.PoissonOptions.default(precision=0, nu1=1, nu2=1, nu_coarse=8, max_levels=12, min_coarse=2)
+    ctx.tune(gb.TUNE_MG_TAIL, tail)
+    try:
+        ps = gb.PoissonSolver(ctx, g, dz, dJ, bc, opts)
+        ps.set_coeffs(dax, day, daz)
+        es = [to_host(ps.vcycle(to_dev(r))) for _ in range(2)]
+        ps.close()
+    finally:
+        ctx.tune(gb.TUNE_MG_TAIL, 0)
+    for e in es:
+        assert rel_err(e, e_ref, g.valid(0)) < 1e-12
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("per", [(True, False), (False, True)])
+def test_gpu_vcycle_tail_fp32_tracks_per_level_launches(ctx, per):
+    """In FP32 the cluster tail and the per-level launches give the same
+    V-cycle to FP32 rounding (1e-5 relative)."""
+    import ablsteadyrans_b200 as gb
+    g, z, J, ax, ay, az, _ = smooth_terrain_case(64, 48, 24, *per, hill=150.0)
+    bc = (PERIODIC if per[0] else NEUMANN, PERIODIC if per[1] else NEUMANN, NEUMANN,
+          PERIODIC if per[0] else DIRICHLET, PERIODIC if per[1] else DIRICHLET, DIRICHLET)
+    rng = np.random.default_rng(9)
+    r = g.np_zeros()
+    r[g.valid(0)] = rng.standard_normal(r[g.valid(0)].shape)
+    out = []
+    try:
+        for tail in (1024, 0):
+            ctx.tune(gb.TUNE_MG_TAIL, tail)
+            dz, dJ, dax, day, daz = _gpu_case(g, z, J, ax, ay, az)
+            ps = gb.PoissonSolver(ctx, g, dz, dJ, bc, gb.PoissonOptions.default(precision=1))
+            ps.set_coeffs(dax, day, daz)
+            out.append(to_host(ps.vcycle(to_dev(r))))
+            ps.close()
+    finally:
+        ctx.tune(gb.TUNE_MG_TAIL, 0)
+    assert rel_err(out[0], out[1], g.valid(0)) < 1e-5
 
 
 @pytest.mark.gpu
@@ -197,6 +259,7 @@ def test_gpu_coarse_kernel_equals_per_relaxation_launches(ctx, precision, per):
         out.append(to_host(ps.vcycle(to_dev(r))))
         ps.close()
     ctx.tune(gb.TUNE_MG_COARSE_KERNEL, 0)
+    ctx.tune(gb.TUNE_MG_TAIL, 0)
     assert rel_err(out[0], out[1], g.valid(0)) < (1e-13 if precision == 0 else 1e-5)
 
 
