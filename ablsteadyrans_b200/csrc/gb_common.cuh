@@ -106,6 +106,77 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
+// ------------------------------------------ bulk copies (TMA) and mbarriers ---
+//
+// A bulk copy (cp.async.bulk, executed by the TMA unit) moves a contiguous
+// run of bytes from global to shared memory and reports its bytes to an
+// mbarrier of the block; the block waits on the barrier's phase. Both
+// addresses must be 16-byte aligned and the size a multiple of 16.
+
+__device__ __forceinline__ unsigned smem_addr(const void* p)
+{
+    return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+
+//! Makes the barriers' initialisation visible to the bulk-copy (async) proxy.
+__device__ __forceinline__ void fence_barrier_init()
+{
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+}
+
+//! Orders this thread's earlier generic accesses of shared memory before
+//! later bulk copies into it (a slot's readers, then its next fill).
+__device__ __forceinline__ void fence_proxy_async_shared()
+{
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+}
+
+//! The one arrival of a phase, announcing the bytes its copies will bring.
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, unsigned bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity)
+{
+    unsigned done;
+    asm volatile(
+        "{\n"
+        ".reg .pred p;\n"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        "selp.u32 %0, 1, 0, p;\n"
+        "}\n"
+        : "=r"(done)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return done != 0;
+}
+
+//! Waits for the barrier's phase of the given parity for at most `limit`
+//! polls (each poll may suspend the thread briefly); false: gave up.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity, int limit)
+{
+    for (int n = 0; n < limit; ++n) {
+        if (mbar_try_wait(bar, parity)) { return true; }
+    }
+    return false;
+}
+
+//! Bulk copy of `bytes` from global src to shared dst, completing on bar.
+__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, unsigned bytes, uint64_t* bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                     smem_addr(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_addr(bar))
+                 : "memory");
+}
+
 // ---------------------------------------------------------------- errors ---
 
 void set_error(const char* fmt, ...);

@@ -372,6 +372,140 @@ __global__ void k_color_residual(gb_grid g, PBC b, int color, const T* __restric
     r[o] = bv[o] - adotx_cell<T>(g, b, i, j, k, x, AX, AY, AZ, J, m);
 }
 
+// ------------------------------------------------ TMA-staged operator tiles ---
+//
+// The operator on a level as blocks of kTileI x kTileJ columns (COLOR: the
+// block's columns of one zebra colour, over 2 kTileI consecutive i) that
+// march up kTileK levels. The iterate's planes reach shared memory by bulk
+// copies (cp.async.bulk, the TMA unit): one copy per staged row, the rows
+// j0 - 1 .. j0 + kTileJ of columns i0 - 1 .. i0 + span, into a ring of
+// kTileRing plane slots, each slot's copies completing on its own mbarrier;
+// the plane two levels up streams in while a level is evaluated. A row's
+// copy starts at the 16-byte boundary at or below column i0 - 1 (a level's
+// row stride is an odd number of elements, so rows start on either
+// boundary) and the tile records the shift. Entries outside the valid cells
+// (the ghost rows, columns and planes a boundary block stages) are then
+// overwritten with their ghost-resolved values (ldc: periodic images and
+// mirrors with the face's sign), so every cell reads its 15 values from the
+// tile by one code path; the mesh ratios, areas and J, each read once or
+// twice a cell, stay direct loads.
+
+constexpr int kTileI = 32, kTileJ = 8, kTileK = 8, kTileRing = 4;
+constexpr int kTileWaitLimit = 1 << 22;
+
+template <typename T, bool COLOR>
+struct TileShape {
+    static constexpr int E = 16 / static_cast<int>(sizeof(T));    // elements per 16 bytes
+    static constexpr int SPAN = COLOR ? 2 * kTileI : kTileI;         // the block's i-span of cells
+    static constexpr int PITCH = ((SPAN + 2 + E - 1 + E - 1) / E) * E;  // staged row: shift + SPAN + 2, rounded
+    static constexpr int ROWS = kTileJ + 2;
+};
+
+//! y = rhs - A x (or A x with rhs null) on every cell (COLOR false) or on
+//! the cells of one colour (COLOR true), from TMA-staged tiles of x. err: a
+//! device word set when a wait for a tile gave up (the block then finishes
+//! with whatever the tile holds, and the caller reports the failure).
+template <typename T, bool COLOR>
+__global__ void __launch_bounds__(kTileI* kTileJ)
+    k_stencil_tile(gb_grid g, PBC b, int color, const T* __restrict__ x, const T* __restrict__ AX,
+                   const T* __restrict__ AY, const T* __restrict__ AZ, const T* __restrict__ J, MeshRatios<T> m,
+                   const T* __restrict__ rhs, T* __restrict__ y, unsigned long long* err)
+{
+    using S = TileShape<T, COLOR>;
+    __shared__ __align__(16) T tile[kTileRing][S::ROWS][S::PITCH];
+    __shared__ __align__(8) uint64_t bar[kTileRing];
+    __shared__ int shift[kTileRing][S::ROWS];
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * kTileI + tx;
+    const int i0 = blockIdx.x * S::SPAN, j0 = blockIdx.y * kTileJ;
+    const int kb = blockIdx.z * kTileK, ke = min(kb + kTileK, g.nz);
+    const int ilast = min(i0 + S::SPAN, g.nx);  // staged columns i0 - 1 .. ilast
+    const int jlast = min(j0 + kTileJ, g.ny);   // staged rows j0 - 1 .. jlast
+    const bool edge_block = (i0 == 0) || (ilast == g.nx) || (j0 == 0) || (jlast == g.ny);
+    const int j = j0 + ty;
+    const int i = COLOR ? i0 + 2 * tx + ((j + color) & 1) : i0 + tx;
+    const bool active = (i < g.nx) && (j < g.ny);
+    if (tid == 0) {
+        for (int q = 0; q < kTileRing; ++q) { mbar_init(&bar[q], 1); }
+        fence_barrier_init();
+    }
+    __syncthreads();
+    auto slot_of = [&](int kk) { return (kk + 1) & (kTileRing - 1); };
+    auto parity_of = [&](int kk) { return static_cast<unsigned>(((kk - (kb - 1)) / kTileRing) & 1); };
+    // one thread issues a plane's row copies (kk in -1 .. nz)
+    auto issue = [&](int kk) {
+        const int q = slot_of(kk);
+        unsigned total = 0;
+        int64_t ea[S::ROWS];
+        unsigned nb[S::ROWS];
+        for (int r = 0; r < S::ROWS; ++r) {
+            const int jj = j0 - 1 + r;
+            nb[r] = 0;
+            ea[r] = 0;
+            if (jj > jlast) { continue; }
+            const int64_t e0 = at(g, i0 - 1, jj, kk);
+            const int64_t e1 = at(g, ilast, jj, kk);
+            ea[r] = e0 & ~static_cast<int64_t>(S::E - 1);
+            const int64_t n = ((e1 - ea[r] + 1 + S::E - 1) / S::E) * S::E;
+            nb[r] = static_cast<unsigned>(n * sizeof(T));
+            shift[q][r] = static_cast<int>(e0 - ea[r]);
+            total += nb[r];
+        }
+        mbar_arrive_expect_tx(&bar[q], total);
+        for (int r = 0; r < S::ROWS; ++r) {
+            if (nb[r] != 0) { bulk_copy_g2s(&tile[q][r][0], x + ea[r], nb[r], &bar[q]); }
+        }
+    };
+    // after the copies landed: the entries outside the valid cells take their ghost-resolved values
+    auto fixup = [&](int kk) {
+        if (!edge_block && kk >= 0 && kk < g.nz) { return; }
+        const int q = slot_of(kk);
+        const int ncol = ilast - (i0 - 1) + 1;
+        const int nrow = jlast - (j0 - 1) + 1;
+        for (int e = tid; e < nrow * ncol; e += kTileI * kTileJ) {
+            const int r = e / ncol, c = e % ncol;
+            const int ii = i0 - 1 + c, jj = j0 - 1 + r;
+            if (ii < 0 || ii >= g.nx || jj < 0 || jj >= g.ny || kk < 0 || kk >= g.nz) {
+                tile[q][r][shift[q][r] + c] = ldc<T>(x, x, g, b, ii, jj, kk);
+            }
+        }
+    };
+    bool ok = true;
+    if (tid == 0) {
+        issue(kb - 1);
+        issue(kb);
+        if (kb + 1 <= ke) { issue(kb + 1); }
+    }
+    for (int kk = kb - 1; kk <= kb; ++kk) {
+        ok = mbar_wait_bounded(&bar[slot_of(kk)], parity_of(kk), kTileWaitLimit) && ok;
+        fixup(kk);
+    }
+    for (int k = kb; k < ke; ++k) {
+        if (tid == 0 && k + 2 <= ke) {
+            fence_proxy_async_shared();
+            issue(k + 2);
+        }
+        ok = mbar_wait_bounded(&bar[slot_of(k + 1)], parity_of(k + 1), kTileWaitLimit) && ok;
+        fixup(k + 1);
+        __syncthreads();
+        if (active) {
+            const int qm = slot_of(k - 1), q0 = slot_of(k), qp = slot_of(k + 1);
+            const int c = i - i0 + 1;
+            const int r = j - j0 + 1;
+            auto X = [&](int di, int dj, int dk) {
+                const int q = (dk < 0) ? qm : (dk > 0) ? qp : q0;
+                return tile[q][r + dj][shift[q][r + dj] + c + di];
+            };
+            const int64_t o = at(g, i, j, k);
+            const T v = adotx_body<T, true>(g, b, i, j, k, o, X, AX, AY, AZ, J, m);
+            y[o] = rhs ? rhs[o] - v : v;
+        }
+        // this thread's reads (and fix-up writes) of the slots before the next bulk copy into one
+        fence_proxy_async_shared();
+        __syncthreads();
+    }
+    if (!ok && tid == 0) { atomicOr(err, 1ull); }
+}
+
 //! The LU factors of every column's line tridiagonal T, once per coefficient
 //! set (T does not change between relaxations): in place of C and U the
 //! reciprocal pivots 1/m_k and the eliminated uppers c'_k = U_k / m_k, with
@@ -1327,6 +1461,32 @@ namespace gb {
 
 namespace {
 
+//! Whether the operator over the array x takes the TMA-staged tiles
+//! (GB_TUNE_MG_STENCIL = 2; never when x's base is not 16-byte aligned, as
+//! the bulk copies need). Not the default: on config 1's fine level the
+//! tiles measured 83 us per apply and 54 us per colour residual against 35
+//! and 24 us for one thread per cell (ncu, cold): staging the iterate
+//! leaves the other ten words of a cell as direct loads, whose latency is
+//! what bounds the operator, and adds two block barriers per level.
+template <typename T>
+bool use_tiles(const gb_poisson* P, const gb_grid& g, const T* x)
+{
+    (void)g;
+    if (P->ctx->tune[GB_TUNE_MG_STENCIL] != 2 || P->d_err == nullptr) { return false; }
+    return (reinterpret_cast<uintptr_t>(x) & 15u) == 0;
+}
+
+template <typename T, bool COLOR>
+void launch_tiles(gb_poisson* P, const gb_grid& g, const PBC& b, int color, const T* x, const T* AX, const T* AY,
+                  const T* AZ, const T* J, const MeshRatios<T>& m, const T* rhs, T* y)
+{
+    using S = TileShape<T, COLOR>;
+    const dim3 grid((g.nx + S::SPAN - 1) / S::SPAN, (g.ny + kTileJ - 1) / kTileJ, (g.nz + kTileK - 1) / kTileK);
+    k_stencil_tile<T, COLOR><<<grid, dim3(kTileI, kTileJ), 0, P->ctx->stream>>>(g, b, color, x, AX, AY, AZ, J, m, rhs,
+                                                                               y, P->d_err);
+    ++P->ctx->launches;
+}
+
 //! Largest dynamic shared memory a relaxation kernel asks for.
 constexpr size_t kSmoothSmemMax = 200 * 1024;
 
@@ -1407,9 +1567,15 @@ void mg_smooth(gb_poisson* P, PoissonLevels<T>& L, int l)
     }
     for (int color = 0; color < 2; ++color) {
         Span span(ctx, GB_KERNEL_MG_SMOOTH);
-        const dim3 rgrid((half + 31) / 32, (g.ny + 3) / 4, g.nz);
-        k_color_residual<T><<<rgrid, dim3(32, 4), 0, ctx->stream>>>(g, b, color, L.x[l], L.bv[l], L.AX[l], L.AY[l],
-                                                                   L.AZ[l], L.J[l], L.ratios(l), L.r[l]);
+        if (use_tiles(P, g, L.x[l])) {
+            launch_tiles<T, true>(P, g, b, color, L.x[l], L.AX[l], L.AY[l], L.AZ[l], L.J[l], L.ratios(l), L.bv[l],
+                                  L.r[l]);
+            --ctx->launches;  // counted with the solve below
+        } else {
+            const dim3 rgrid((half + 31) / 32, (g.ny + 3) / 4, g.nz);
+            k_color_residual<T><<<rgrid, dim3(32, 4), 0, ctx->stream>>>(g, b, color, L.x[l], L.bv[l], L.AX[l], L.AY[l],
+                                                                       L.AZ[l], L.J[l], L.ratios(l), L.r[l]);
+        }
         const dim3 sgrid((half + nthr - 1) / nthr, g.ny);
         const int sL = (g.nz + 7) / 8 <= 16 ? 8 : 16;
         const int sW = (g.nz + sL - 1) / sL;
@@ -1453,6 +1619,11 @@ void mg_residual(gb_poisson* P, PoissonLevels<T>& L, int l)
     gb_ctx* ctx = P->ctx;
     const gb_grid& g = L.g[l];
     Span span(ctx, GB_KERNEL_POISSON_APPLY);
+    if (use_tiles(P, g, L.x[l])) {
+        launch_tiles<T, false>(P, g, L.b[l], -1, L.x[l], L.AX[l], L.AY[l], L.AZ[l], L.J[l], L.ratios(l), L.bv[l],
+                               L.r[l]);
+        return;
+    }
     k_apply<T><<<cols_grid(g, g.nz), kColsBlock, 0, ctx->stream>>>(g, L.b[l], L.x[l], L.AX[l], L.AY[l], L.AZ[l],
                                                                    L.J[l], L.ratios(l), L.bv[l], L.r[l]);
     ++ctx->launches;
@@ -1713,9 +1884,15 @@ void apply_fine(gb_poisson* P, const double* x, const double* rhs, double* y)
     gb_ctx* ctx = P->ctx;
     const gb_grid& g = P->g;
     Span span(ctx, GB_KERNEL_POISSON_APPLY);
-    k_apply<double><<<cols_grid(g, g.nz), kColsBlock, 0, ctx->stream>>>(g, P->dl.b[0], x, P->dl.AX[0], P->dl.AY[0],
-                                                                        P->dl.AZ[0], P->dl.J[0], P->dl.ratios(0), rhs, y);
-    ++ctx->launches;
+    if (use_tiles(P, g, x)) {
+        launch_tiles<double, false>(P, g, P->dl.b[0], -1, x, P->dl.AX[0], P->dl.AY[0], P->dl.AZ[0], P->dl.J[0],
+                                    P->dl.ratios(0), rhs, y);
+    } else {
+        k_apply<double><<<cols_grid(g, g.nz), kColsBlock, 0, ctx->stream>>>(g, P->dl.b[0], x, P->dl.AX[0],
+                                                                            P->dl.AY[0], P->dl.AZ[0], P->dl.J[0],
+                                                                            P->dl.ratios(0), rhs, y);
+        ++ctx->launches;
+    }
     if (P->cross_ad != nullptr) {
         // PoissonSolver::Op::apply (Source/Poisson.cpp:148-156): the split
         // correction on top (subtracted when y is the residual rhs - A x)
@@ -1881,9 +2058,11 @@ gb_status poisson_build(gb_poisson* P)
     // Krylov workspace
     const int64_t vol = volume(P->g);
     const int m = P->opt.restart;
-    P->vstride = vol;
-    P->V = dalloc<double>(ctx->stream, P->owned, vol * (m + 1));
-    P->Zv = dalloc<double>(ctx->stream, P->owned, vol * m);
+    // the basis columns at a stride of whole 256-byte lines: every column's
+    // base is 16-byte aligned, as the TMA-staged operator tiles need
+    P->vstride = (vol + 31) / 32 * 32;
+    P->V = dalloc<double>(ctx->stream, P->owned, P->vstride * (m + 1));
+    P->Zv = dalloc<double>(ctx->stream, P->owned, P->vstride * m);
     P->w = dalloc<double>(ctx->stream, P->owned, vol);
     P->t = dalloc<double>(ctx->stream, P->owned, vol);
     P->dot_blocks = std::min(4 * ctx->num_sms, nblocks(static_cast<int64_t>(P->g.nx) * P->g.ny * P->g.nz));
@@ -1891,7 +2070,8 @@ gb_status poisson_build(gb_poisson* P)
     P->d_dots = dalloc<double>(ctx->stream, P->owned, m + 2);
     P->d_coef = dalloc<double>(ctx->stream, P->owned, m + 2);
     P->d_step = dalloc<double>(ctx->stream, P->owned, 3 * (m + 2));
-    if (!P->V || !P->Zv || !P->w || !P->t || !P->d_partial || !P->d_dots || !P->d_coef) {
+    P->d_err = dalloc<unsigned long long>(ctx->stream, P->owned, 1);
+    if (!P->V || !P->Zv || !P->w || !P->t || !P->d_partial || !P->d_dots || !P->d_coef || !P->d_err) {
         set_error("gust: PoissonSolver: cannot allocate the Krylov workspace");
         return GB_OOM;
     }
@@ -2096,8 +2276,8 @@ gb_status poisson_solve(gb_poisson* P, double* rhs, double* phi, gb_poisson_resu
         int jj = 0;
         for (; jj < m && it < P->opt.max_iter; ++jj) {
             ++it;
-            double* vj = P->V + vol * jj;
-            double* zj = P->Zv + vol * jj;
+            double* vj = P->V + P->vstride * jj;
+            double* zj = P->Zv + P->vstride * jj;
             precondition(P, vj, zj);
             apply_fine(P, zj, nullptr, P->w);
             // classical Gram-Schmidt, twice, and the norm of what is left: the
@@ -2108,12 +2288,13 @@ gb_status poisson_solve(gb_poisson* P, double* rhs, double* phi, gb_poisson_resu
             const int64_t st3 = m + 2;
             for (int pass = 0; pass < 2; ++pass) {
                 double* dots = P->d_step + pass * st3;
-                multidot_device(P, P->w, P->V, vol, jj + 1, dots);
-                k_subtract_projection<<<nblocks(ncell), kBlock, 0, ctx->stream>>>(g, P->w, P->V, vol, jj + 1, dots);
+                multidot_device(P, P->w, P->V, P->vstride, jj + 1, dots);
+                k_subtract_projection<<<nblocks(ncell), kBlock, 0, ctx->stream>>>(g, P->w, P->V, P->vstride, jj + 1,
+                                                                                   dots);
                 ++ctx->launches;
             }
             multidot_device(P, P->w, P->w, 0, 1, P->d_step + 2 * st3);
-            double* vn = P->V + vol * (jj + 1);
+            double* vn = P->V + P->vstride * (jj + 1);
             cudaMemsetAsync(vn, 0, sizeof(double) * vol, ctx->stream);
             k_scale_by_norm<<<nblocks(ncell), kBlock, 0, ctx->stream>>>(g, P->w, P->d_step + 2 * st3, vn);
             ++ctx->launches;
@@ -2149,7 +2330,7 @@ gb_status poisson_solve(gb_poisson* P, double* rhs, double* phi, gb_poisson_resu
             y[q] = acc / H[q * m + q];
         }
         cudaMemcpyAsync(P->d_coef, y.data(), sizeof(double) * jj, cudaMemcpyHostToDevice, ctx->stream);
-        k_add_combination<<<nblocks(ncell), kBlock, 0, ctx->stream>>>(g, phi, P->Zv, vol, jj, P->d_coef);
+        k_add_combination<<<nblocks(ncell), kBlock, 0, ctx->stream>>>(g, phi, P->Zv, P->vstride, jj, P->d_coef);
         ++ctx->launches;
         if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) { return check_cuda("poisson solve"); }
     }
@@ -2167,6 +2348,16 @@ gb_status poisson_solve(gb_poisson* P, double* rhs, double* phi, gb_poisson_resu
     if (!std::isfinite(res->final_residual)) {
         set_error("gust: the Poisson solve returned non-finite values");
         return GB_NONFINITE;
+    }
+    {
+        unsigned long long tile_err = 0;
+        cudaMemcpyAsync(&tile_err, P->d_err, sizeof(tile_err), cudaMemcpyDeviceToHost, ctx->stream);
+        if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) { return check_cuda("PoissonSolver::solve"); }
+        if (tile_err != 0) {
+            cudaMemsetAsync(P->d_err, 0, sizeof(tile_err), ctx->stream);
+            set_error("gust: the Poisson solve: a wait for a TMA-staged operator tile gave up");
+            return GB_TIMEOUT;
+        }
     }
     if (!(res->final_residual <= tol * (1 + 1e-7)) && !converged) {
         set_error("gust: the Poisson solve did not converge in solver.poisson_max_iter = %d iterations (residual %g of "

@@ -59,6 +59,7 @@ struct gb_poisson {
     int64_t vstride{0};
     double* V{nullptr};
     double* Zv{nullptr};
+    unsigned long long* d_err{nullptr};    // set when a TMA tile wait gave up
     double* w{nullptr};
     double* t{nullptr};
     int dot_blocks{0};

@@ -135,6 +135,10 @@ enum {
     GB_TUNE_MG_TAIL,            /* the V-cycle's coarse levels as one thread-block-cluster launch: 0 default
                                    and 1 off (per-level launches), N >= 2 the levels of at most N columns
                                    (measured no faster: the cluster's 16 SMs do the levels' work) */
+    GB_TUNE_MG_STENCIL,         /* the terrain operator of the Poisson apply and the zebra colour residual:
+                                   0 default and 1 one thread per cell, 2 TMA-staged tiles of the iterate
+                                   on every level (measured slower: the other ten words a cell stay
+                                   direct loads and each level costs two block barriers) */
     GB_N_TUNE
 };
 gb_status gb_ctx_tune(gb_ctx* ctx, int32_t key, int32_t value);
