@@ -1101,6 +1101,11 @@ void scalar_diffusion_subtract(gb_simplec* S, const double* q, const double* gam
 // launches, and no flux array goes through memory.
 
 constexpr int kFusedTx = 32, kFusedTy = 8;
+// levels per block: config 1's residual measured 0.856 ms with 2, 0.886 with
+// 4, 1.036 with 8 and 1.806 with 32 (one launch per flux direction: 1.017):
+// the face evaluations are latency-bound, and more, shorter blocks keep more
+// of them in flight than the z faces saved by longer ones are worth
+constexpr int kFusedLevels = 2;
 
 struct FusedResidualArgs {
     gb_grid g;
@@ -1228,7 +1233,7 @@ void fused_residual(gb_simplec* S, const gb_state& q, double* R)
     a.nj = g.ny + ((T >> 1) & 1);
     a.nk = g.nz + ((T >> 2) & 1);
     const int knob = S->ctx->tune[GB_TUNE_RESIDUAL];
-    a.kc = (knob >= 2) ? knob : 8;
+    a.kc = (knob >= 2) ? knob : kFusedLevels;
     const double* fields[5] = {q.u, q.v, q.w, q.theta, q.tke};
     a.q = fields[E];
     a.u = q.u;
@@ -1657,7 +1662,7 @@ void implicit_coefficients_on(gb_ctx* ctx, const gb_grid g, const double* z, con
     const int knob = ctx->tune[GB_TUNE_RESIDUAL];
     if (knob != 1) {
         const int ni = g.nx + (T & 1), nj = g.ny + ((T >> 1) & 1), nk = g.nz + ((T >> 2) & 1);
-        const int kc = (knob >= 2) ? knob : 8;
+        const int kc = (knob >= 2) ? knob : kFusedLevels;
         const dim3 block(kFusedTx, kFusedTy);
         const dim3 grid((ni + kFusedTx - 1) / kFusedTx, (nj + kFusedTy - 1) / kFusedTy, (nk + kc - 1) / kc);
         span_begin(ctx, GB_KERNEL_COEFS);
@@ -1691,46 +1696,106 @@ void implicit_coefficients(gb_simplec* S, double* const* F, const double* gm, do
     implicit_coefficients_on<C>(S->ctx, S->g, S->z, S->mesh.detJ, S->ph.log_mean, F, gm, A);
 }
 
+//! One boundary face's fold of the implicit rows (apply_to_implicit).
+struct FoldFace {
+    int d;              // the face's direction
+    int edge;           // its points' index along d
+    int dirichlet_pt;   // a Dirichlet point: the row becomes the identity
+    int ghost_coef;     // the coefficient towards the ghost
+    int other_coef;     // the opposite coefficient (to_other)
+    int to_other;       // the ghost coefficient moves to the opposite one
+    double fold;        // else a_P += fold a_ghost
+};
+struct FoldPack {
+    FoldFace f[6];
+    int n;
+    Box vb;               // the valid points of the rows' location
+    int64_t start[7];     // face q's points are [start[q], start[q + 1]) of the launch
+};
+
+__device__ __forceinline__ void apply_fold(const FoldFace& F, double* A, int64_t cs, int64_t o)
+{
+    if (F.dirichlet_pt) {
+        for (int n = 0; n < GB_N_COEFS; ++n) { A[n * cs + o] = 0; }
+        A[GB_COEF_P * cs + o] = 1;
+    } else {
+        const double ag = A[F.ghost_coef * cs + o];
+        A[F.ghost_coef * cs + o] = 0;
+        if (F.to_other) { A[F.other_coef * cs + o] += ag; } else { A[GB_COEF_P * cs + o] += F.fold * ag; }
+    }
+}
+
+//! Every face's folds in one launch: a thread per point of each face plane;
+//! a point on several faces (an edge or a corner) is taken by the thread of
+//! its first face in the order of the folds, which applies all of that
+//! point's folds in that order (the order of the per-face launches).
+__global__ void k_fold_rows(const gb_grid g, const __grid_constant__ FoldPack P, double* __restrict__ A)
+{
+    const int64_t n = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (n >= P.start[P.n]) { return; }
+    int q = 0;
+    while (n >= P.start[q + 1]) { ++q; }
+    // the point of face q's plane (the valid box with index d fixed at the edge), i fastest
+    Box b = P.vb;
+    b.lo[P.f[q].d] = b.hi[P.f[q].d] = P.f[q].edge;
+    const int64_t m = n - P.start[q];
+    const int nx = b.hi[0] - b.lo[0] + 1, ny = b.hi[1] - b.lo[1] + 1;
+    const int c[3] = {b.lo[0] + static_cast<int>(m % nx), b.lo[1] + static_cast<int>((m / nx) % ny),
+                      b.lo[2] + static_cast<int>(m / (static_cast<int64_t>(nx) * ny))};
+    for (int e = 0; e < q; ++e) {
+        if (c[P.f[e].d] == P.f[e].edge) { return; }  // an earlier face's thread takes it
+    }
+    const int64_t cs = volume(g);
+    const int64_t o = at(g, c[0], c[1], c[2]);
+    for (int e = 0; e < P.n; ++e) {
+        if (c[P.f[e].d] == P.f[e].edge) { apply_fold(P.f[e], A, cs, o); }
+    }
+}
+
 //! apply_to_implicit (BoundaryConditions.cpp:885-941): the damping first,
-//! then the folds (a Dirichlet face point's row becomes the identity).
+//! then the folds (a Dirichlet face point's row becomes the identity), the
+//! faces in the order d = x, y, z, low side then high side.
 void apply_to_implicit(gb_simplec* S, int f, int t, double* A)
 {
     add_damping_to_implicit(S, f, t, A);
     const gb_grid g = S->g;
-    const int64_t cs = volume(g);
+    FoldPack P{};
+    P.vb = valid_box(g, t);
+    P.n = 0;
+    P.start[0] = 0;
     for (int d = 0; d < 3; ++d) {
         if (is_per(g, d)) { continue; }
         for (int lo = 1; lo >= 0; --lo) {
             const int fc = d + (lo ? 0 : 3);
             const int rule = rule_for(f, S->bc.face[fc], d, lo);
             const bool nod = nodal(t, d);
-            const bool dirichlet_pt = nod && (rule == R_VALUE || rule == R_PROFILE);
             const int nd = (d == 0) ? g.nx : (d == 1) ? g.ny : g.nz;
-            const int edge = lo ? 0 : (nod ? nd : nd - 1);
+            FoldFace& F = P.f[P.n];
+            F.d = d;
+            F.edge = lo ? 0 : (nod ? nd : nd - 1);
+            F.dirichlet_pt = (nod && (rule == R_VALUE || rule == R_PROFILE)) ? 1 : 0;
             const int cm = (d == 0) ? GB_COEF_XM : (d == 1) ? GB_COEF_YM : GB_COEF_ZM;
             const int cp = (d == 0) ? GB_COEF_XP : (d == 1) ? GB_COEF_YP : GB_COEF_ZP;
-            const int ghost_coef = lo ? cm : cp, other_coef = lo ? cp : cm;
-            double fold = 0;
-            bool to_other = false;
-            if (nod) { to_other = true; }
-            else if (rule == R_EVEN) { fold = -1; }
-            else if (rule == R_ODD || rule == R_VALUE) { fold = 1; }
-            else if (rule == R_GRADIENT) { to_other = true; }
-            Box b = valid_box(g, t);
-            b.lo[d] = b.hi[d] = edge;
-            for_box(S->ctx, b, [=] __device__(int i, int j, int k) {
-                const int64_t o = at(g, i, j, k);
-                if (dirichlet_pt) {
-                    for (int n = 0; n < GB_N_COEFS; ++n) { A[n * cs + o] = 0; }
-                    A[GB_COEF_P * cs + o] = 1;
-                } else {
-                    const double ag = A[ghost_coef * cs + o];
-                    A[ghost_coef * cs + o] = 0;
-                    if (to_other) { A[other_coef * cs + o] += ag; } else { A[GB_COEF_P * cs + o] += fold * ag; }
-                }
-            }, GB_KERNEL_COEFS);
+            F.ghost_coef = lo ? cm : cp;
+            F.other_coef = lo ? cp : cm;
+            F.fold = 0;
+            F.to_other = 0;
+            if (nod) { F.to_other = 1; }
+            else if (rule == R_EVEN) { F.fold = -1; }
+            else if (rule == R_ODD || rule == R_VALUE) { F.fold = 1; }
+            else if (rule == R_GRADIENT) { F.to_other = 1; }
+            Box b = P.vb;
+            b.lo[d] = b.hi[d] = F.edge;
+            P.start[P.n + 1] = P.start[P.n] + b.count();
+            ++P.n;
         }
     }
+    const int64_t total = P.start[P.n];
+    if (total == 0) { return; }
+    span_begin(S->ctx, GB_KERNEL_COEFS);
+    k_fold_rows<<<static_cast<unsigned>((total + 255) / 256), 256, 0, S->ctx->stream>>>(g, P, A);
+    span_end(S->ctx);
+    ++S->ctx->launches;
 }
 
 void dirichlet_rows(gb_simplec* S, int f, int t, double* mask)

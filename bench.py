@@ -121,7 +121,7 @@ class ClockSampler:
 # the first sweep of a solve (zero initial iterate, no lateral terms) reads
 # a_P, a_ZM, a_ZP and rhs and writes the iterate (5)
 LINE_WORDS_FIRST, LINE_WORDS = 5, 10
-LINE_PROFILE = os.path.join(ROOT, "profiles", "zline_fact_multi_kernel_config1_fp64.txt")
+LINE_PROFILE = os.path.join(ROOT, "profiles", "zline_seg_multi_kernel_config1_fp64.txt")
 
 
 def line_traffic_per_point():

@@ -129,7 +129,7 @@ enum {
                                    levels): 0 default, 4 or 8 */
     GB_TUNE_RESIDUAL,           /* the SIMPLEC residual's convection, diffusion and pressure gradient and
                                    the implicit coefficients: 0 default (one launch per equation, each
-                                   face evaluated once per block, 8 levels per block), 1 one thread per
+                                   face evaluated once per block, 2 levels per block), 1 one thread per
                                    point (the residual's fluxes and divergences as separate launches),
                                    N >= 2 the per-equation launch with N levels per block */
     GB_TUNE_MG_TAIL,            /* the V-cycle's coarse levels as one thread-block-cluster launch: 0 default
