@@ -15,6 +15,7 @@
 #include "gb_turbulence.cuh"
 
 #include <algorithm>
+#include <type_traits>
 #include <cmath>
 #include <cstring>
 
@@ -330,6 +331,7 @@ struct SimplecWork {
     double* R[6];
     double* F[3];
     double* G[9];
+    double* Gd[9];   // the momentum diffusive fluxes, component C through its faces along D at [3 C + D]
     double* tmp;
     double* A;
     double* At;
@@ -1107,9 +1109,133 @@ constexpr int kFusedTx = 32, kFusedTy = 8;
 // of them in flight than the z faces saved by longer ones are worth
 constexpr int kFusedLevels = 2;
 
+//! The momentum diffusive fluxes at one location type L (a cell centre or
+//! an edge): the face flux of every velocity component C whose control
+//! volume has its faces along D at L (L = (1 << C) ^ (1 << D)), from one
+//! evaluation of the terrain metric, the face diffusivity and the
+//! gradients of u, v and w at the point (momentum_diff_face's operations,
+//! shared by the two or three fluxes that need them), each within its own
+//! flux box (CVFluxes.cpp:52-66); a surface_layer ground's u and v ground
+//! faces take the wall stress (set_ground_fluxes, SurfaceLayer.cpp:418-450).
+struct StressArgs {
+    gb_grid g;
+    Box b;                  // the union of the pairs' flux boxes
+    Box pb[3];              // each pair's flux box
+    double* G[3];           // each pair's flux array
+    const double* u;
+    const double* v;
+    const double* w;
+    const double* nu;
+    const double* z;
+    int logz;
+    int wall;
+    const double* taux;
+    const double* tauy;
+};
+
+template <int L>
+__global__ void __launch_bounds__(256) k_momentum_stress(const StressArgs a)
+{
+    // the (component, direction) pairs at L in increasing C
+    constexpr int C0 = (L == CC) ? 0 : (L == (XF ^ YF)) ? 0 : (L == (XF ^ ZF)) ? 0 : 1;
+    constexpr int D0 = (L == CC) ? 0 : (L == (XF ^ YF)) ? 1 : 2;
+    constexpr int C1 = (L == CC) ? 1 : (L == (XF ^ YF)) ? 1 : 2;
+    constexpr int D1 = (L == CC) ? 1 : (L == (XF ^ YF)) ? 0 : (L == (XF ^ ZF)) ? 0 : 1;
+    constexpr int NP = (L == CC) ? 3 : 2;
+    const Box& b = a.b;
+    const int64_t n = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (n >= b.count()) { return; }
+    const int nx = b.hi[0] - b.lo[0] + 1, ny = b.hi[1] - b.lo[1] + 1;
+    const int i = b.lo[0] + static_cast<int>(n % nx);
+    const int j = b.lo[1] + static_cast<int>((n / nx) % ny);
+    const int k = b.lo[2] + static_cast<int>(n / (static_cast<int64_t>(nx) * ny));
+    auto inside = [&](const Box& p) {
+        return i >= p.lo[0] && i <= p.hi[0] && j >= p.lo[1] && j <= p.hi[1] && k >= p.lo[2] && k <= p.hi[2];
+    };
+    bool in[3] = {inside(a.pb[0]), inside(a.pb[1]), NP == 3 ? inside(a.pb[2]) : false};
+    if (!in[0] && !in[1] && !in[2]) { return; }
+    const gb_grid& g = a.g;
+    const Metric<double> m = metric_at<L>(a.z, g, i, j, k);
+    double gu[3], gv[3], gw[3];
+    grad_at<XF, L>(a.u, g, i, j, k, m, gu);
+    grad_at<YF, L>(a.v, g, i, j, k, m, gv);
+    grad_at<ZF, L>(a.w, g, i, j, k, m, gw);
+    const double gam = face_gamma<L>(a.nu, g, i, j, k, a.logz);
+    const int64_t o = at(g, i, j, k);
+    auto flux = [&](auto Cc, auto Dc) {
+        constexpr int C = decltype(Cc)::value, D = decltype(Dc)::value;
+        const double* gc = (C == 0) ? gu : (C == 1) ? gv : gw;
+        const double tau[3] = {gc[0] + gu[C], gc[1] + gv[C], gc[2] + gw[C]};
+        return gam * area_dot<D>(m, tau);
+    };
+    using I2 = std::integral_constant<int, 2>;
+    if (in[0]) {
+        double f = flux(std::integral_constant<int, C0>{}, std::integral_constant<int, D0>{});
+        if (D0 == 2 && a.wall && k == 0) {
+            if (C0 == 0) { f = 0.5 * (a.taux[plane_at(g, i - 1, j)] + a.taux[plane_at(g, i, j)]); }
+            if (C0 == 1) { f = 0.5 * (a.tauy[plane_at(g, i, j - 1)] + a.tauy[plane_at(g, i, j)]); }
+        }
+        a.G[0][o] = f;
+    }
+    if (in[1]) {
+        double f = flux(std::integral_constant<int, C1>{}, std::integral_constant<int, D1>{});
+        if (D1 == 2 && a.wall && k == 0) {
+            if (C1 == 0) { f = 0.5 * (a.taux[plane_at(g, i - 1, j)] + a.taux[plane_at(g, i, j)]); }
+            if (C1 == 1) { f = 0.5 * (a.tauy[plane_at(g, i, j - 1)] + a.tauy[plane_at(g, i, j)]); }
+        }
+        a.G[1][o] = f;
+    }
+    if (NP == 3 && in[2]) { a.G[2][o] = flux(I2{}, I2{}); }
+}
+
+//! The nine momentum diffusive fluxes into w.Gd in four launches.
+void momentum_stress(gb_simplec* S, const gb_state& q)
+{
+    const gb_grid g = S->g;
+    double** Gd = S->w.Gd;
+    auto launch = [&](auto Lc, int c0, int d0, int c1, int d1, int c2, int d2) {
+        constexpr int L = decltype(Lc)::value;
+        StressArgs a{};
+        a.g = g;
+        const int cs[3] = {c0, c1, c2}, ds[3] = {d0, d1, d2};
+        const int np = (c2 >= 0) ? 3 : 2;
+        for (int p = 0; p < np; ++p) {
+            const int T = 1 << cs[p];
+            a.pb[p] = (T == XF) ? flux_box<XF>(g, ds[p]) : (T == YF) ? flux_box<YF>(g, ds[p]) : flux_box<ZF>(g, ds[p]);
+            a.G[p] = Gd[3 * cs[p] + ds[p]];
+        }
+        a.b = a.pb[0];
+        for (int p = 1; p < np; ++p) {
+            for (int e = 0; e < 3; ++e) {
+                a.b.lo[e] = std::min(a.b.lo[e], a.pb[p].lo[e]);
+                a.b.hi[e] = std::max(a.b.hi[e], a.pb[p].hi[e]);
+            }
+        }
+        a.u = q.u;
+        a.v = q.v;
+        a.w = q.w;
+        a.nu = S->dfe.nu;
+        a.z = S->z;
+        a.logz = S->ph.log_mean;
+        a.wall = S->wall ? 1 : 0;
+        a.taux = S->ssr[kSsTauX];
+        a.tauy = S->ssr[kSsTauY];
+        const int64_t n = a.b.count();
+        span_begin(S->ctx, GB_KERNEL_RESIDUAL);
+        k_momentum_stress<L><<<static_cast<unsigned>((n + 255) / 256), 256, 0, S->ctx->stream>>>(a);
+        span_end(S->ctx);
+        ++S->ctx->launches;
+    };
+    launch(std::integral_constant<int, CC>{}, 0, 0, 1, 1, 2, 2);
+    launch(std::integral_constant<int, XF ^ YF>{}, 0, 1, 1, 0, -1, -1);
+    launch(std::integral_constant<int, XF ^ ZF>{}, 0, 2, 2, 0, -1, -1);
+    launch(std::integral_constant<int, YF ^ ZF>{}, 1, 2, 2, 1, -1, -1);
+}
+
 struct FusedResidualArgs {
     gb_grid g;
     int ni, nj, nk, kc;          // the equation's valid points; levels per block
+    const double* gd[3];         // a velocity component's diffusive fluxes along x, y, z (momentum_stress)
     const double* q;             // the transported field
     const double* u;
     const double* v;
@@ -1145,7 +1271,11 @@ __device__ __forceinline__ void fused_face(const FusedResidualArgs& a, int i, in
     constexpr int T = (E < 3) ? (1 << E) : CC;
     const double* F = (D == 0) ? a.F0 : (D == 1) ? a.F1 : a.F2;
     gc = conv_face<T, D>(a.q, F, a.lim, a.eps2, a.g, i, j, k);
-    if (D == 2 && E != 2 && a.wall && k == 0) {
+    if (E < 3) {
+        gd = a.gd[D][at(a.g, i, j, k)];
+        return;
+    }
+    if (D == 2 && a.wall && k == 0) {
         if (E == 0) {
             gd = 0.5 * (a.plane[plane_at(a.g, i - 1, j)] + a.plane[plane_at(a.g, i, j)]);
         } else if (E == 1) {
@@ -1157,11 +1287,7 @@ __device__ __forceinline__ void fused_face(const FusedResidualArgs& a, int i, in
         }
         return;
     }
-    if (E < 3) {
-        gd = momentum_diff_face<(E < 3 ? E : 0), D>(a.u, a.v, a.w, a.gamma, a.z, a.logz, a.g, i, j, k);
-    } else {
-        gd = scalar_diff_face<D>(a.q, a.gamma, a.z, a.logz, a.g, i, j, k);
-    }
+    gd = scalar_diff_face<D>(a.q, a.gamma, a.z, a.logz, a.g, i, j, k);
 }
 
 //! R = div(convective flux) - div(diffusive flux) (+ the pressure gradient
@@ -1259,6 +1385,9 @@ void fused_residual(gb_simplec* S, const gb_state& q, double* R)
         a.ps = S->cf[kClosurePs];
         a.pb = S->cf[kClosurePb];
         a.eps = S->cf[kClosureEps];
+    }
+    if (E < 3) {
+        for (int d = 0; d < 3; ++d) { a.gd[d] = S->w.Gd[3 * E + d]; }
     }
     a.R = R;
     const dim3 block(kFusedTx, kFusedTy);
@@ -1512,6 +1641,7 @@ void simplec_residual(gb_simplec* S, const gb_state& q, double** R)
     const gb_physics& ph = S->ph;
     const bool fused = ctx->tune[GB_TUNE_RESIDUAL] != 1;
     if (fused) {
+        momentum_stress(S, q);
         fused_residual<0>(S, q, R[0]);
         fused_residual<1>(S, q, R[1]);
         fused_residual<2>(S, q, R[2]);
@@ -3358,6 +3488,7 @@ gb_status simplec_build(gb_simplec* S)
         w.keep[n] = dbuf(S, vol);
     }
     for (int n = 0; n < 3; ++n) { w.G[n] = dbuf(S, vol); }
+    for (int n = 0; n < 9; ++n) { w.Gd[n] = dbuf(S, vol); }
     w.tmp = dbuf(S, vol);
     w.A = dbuf(S, vol * GB_N_COEFS);
     w.At = dbuf(S, vol * GB_N_COEFS);
