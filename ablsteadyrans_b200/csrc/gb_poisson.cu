@@ -512,11 +512,24 @@ __global__ void __launch_bounds__(kTileI* kTileJ)
 //! m_0 = C_0, m_k = C_k - D_k c'_{k-1} (D, the lower diagonal, is kept). One
 //! thread per column; the loads of 8 levels are batched ahead of the chain.
 template <typename T>
+__device__ __forceinline__ void line_factor_column(const gb_grid& g, T* __restrict__ TD, T* __restrict__ TC,
+                                                   T* __restrict__ TU, int i, int j);
+
+template <typename T>
 __global__ void k_line_factor(gb_grid g, T* __restrict__ TD, T* __restrict__ TC, T* __restrict__ TU)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     if (i >= g.nx || j >= g.ny) { return; }
+    line_factor_column<T>(g, TD, TC, TU, i, j);
+}
+
+//! The factorisation of column (i, j): the reciprocal pivots and eliminated
+//! uppers in place of C and U (the loads of 8 levels batched ahead of the chain).
+template <typename T>
+__device__ __forceinline__ void line_factor_column(const gb_grid& g, T* __restrict__ TD, T* __restrict__ TC,
+                                                   T* __restrict__ TU, int i, int j)
+{
     const int64_t o0 = at(g, i, j, 0);
     T cp = T(0);
     for (int k0 = 0; k0 < g.nz; k0 += 8) {
@@ -543,6 +556,58 @@ __global__ void k_line_factor(gb_grid g, T* __restrict__ TD, T* __restrict__ TC,
             }
         }
     }
+}
+
+//! Every level's line tridiagonal (k_line_tridiag) in one launch and every
+//! level's column factorisation (k_line_factor) in another: the levels are
+//! independent, and one launch over all of them replaces two per level (the
+//! coarse levels' launches were latency for a few hundred cells).
+template <typename T>
+struct LineLevels {
+    gb_grid g[kMaxLevels];
+    PBC b[kMaxLevels];
+    const T* AX[kMaxLevels];
+    const T* AY[kMaxLevels];
+    const T* AZ[kMaxLevels];
+    const T* J[kMaxLevels];
+    const T* z[kMaxLevels];
+    T* TD[kMaxLevels];
+    T* TC[kMaxLevels];
+    T* TU[kMaxLevels];
+    int64_t cells[kMaxLevels + 1];  // prefix sums of the levels' cells
+    int64_t cols[kMaxLevels + 1];   // prefix sums of the levels' columns
+    int n;
+};
+
+template <typename T>
+__global__ void k_line_tridiag_all(const __grid_constant__ LineLevels<T> L)
+{
+    const int64_t n = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (n >= L.cells[L.n]) { return; }
+    int l = 0;
+    while (n >= L.cells[l + 1]) { ++l; }
+    const gb_grid& g = L.g[l];
+    const int64_t m = n - L.cells[l];
+    const int i = static_cast<int>(m % g.nx), j = static_cast<int>((m / g.nx) % g.ny);
+    const int k = static_cast<int>(m / (static_cast<int64_t>(g.nx) * g.ny));
+    T D, C, U;
+    line_tridiag<T>(g, L.b[l], L.AX[l], L.AY[l], L.AZ[l], L.J[l], L.z[l], i, j, k, D, C, U);
+    const int64_t o = at(g, i, j, k);
+    L.TD[l][o] = D;
+    L.TC[l][o] = C;
+    L.TU[l][o] = U;
+}
+
+template <typename T>
+__global__ void k_line_factor_all(const __grid_constant__ LineLevels<T> L)
+{
+    const int64_t n = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (n >= L.cols[L.n]) { return; }
+    int l = 0;
+    while (n >= L.cols[l + 1]) { ++l; }
+    const gb_grid& g = L.g[l];
+    const int64_t m = n - L.cols[l];
+    line_factor_column<T>(g, L.TD[l], L.TC[l], L.TU[l], static_cast<int>(m % g.nx), static_cast<int>(m / g.nx));
 }
 
 //! Zebra relaxation, second half: on every column of the colour x += T^{-1} r
@@ -997,75 +1062,146 @@ __global__ void k_prolong_add(gb_grid gc, PBC bcb, const T* __restrict__ xc, gb_
 
 //! All relaxations of the coarsest level in ONE block. On a level of a few
 //! columns every launch is latency, and the coarsest level takes nu_coarse
-//! relaxations: here the columns' line factors stay in shared memory for the
-//! whole kernel, each colour's residual goes to shared memory, and block
-//! barriers separate the phases. Operations and order are those of the
-//! per-level kernels (colour residual, then the factored Thomas solve).
-//! Shared memory: [k][column] arrays D, 1/m, c', r and x (5 * ncols * nz).
-template <typename T>
+//! relaxations: here the level's iterate and its columns' line factors stay
+//! in shared memory for the whole kernel. A colour's relaxation is one
+//! phase between block barriers: each warp takes whole columns of the
+//! colour, each lane evaluates r = b - A x at its P = ceil(nz / 32) levels
+//! (adotx_body with the neighbours read from the shared iterate through
+//! adotx_cell's resolved indices and mirror signs), and the factored Thomas
+//! solve runs as two warp scans of the recurrences' affine maps (forward
+//! e', backward x). The iterate returns to global memory at the end.
+//! Shared memory: the iterate and D, 1/m, c' ([k][j][i], 4 * nx ny nz).
+template <typename T, int P>
 __global__ void __launch_bounds__(256) k_coarse_relax(gb_grid g, PBC b, int nrelax, T* x, const T* __restrict__ bv,
                                                       const T* __restrict__ AX, const T* __restrict__ AY,
                                                       const T* __restrict__ AZ, const T* __restrict__ J,
                                                       MeshRatios<T> m, const T* __restrict__ TD,
                                                       const T* __restrict__ TC, const T* __restrict__ TU)
 {
+    constexpr unsigned kAll = 0xffffffffu;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int ncols = g.nx * g.ny, nz = g.nz;
-    const int plane = ncols * nz;
-    T* sd = reinterpret_cast<T*>(smem_raw);
+    const int nx = g.nx, ny = g.ny, nz = g.nz;
+    const int plane = nx * ny * nz;
+    T* xs = reinterpret_cast<T*>(smem_raw);
+    T* sd = xs + plane;
     T* sm = sd + plane;
     T* sc = sm + plane;
-    T* sr = sc + plane;
-    T* sx = sr + plane;
     for (int n = threadIdx.x; n < plane; n += blockDim.x) {
-        const int col = n % ncols, k = n / ncols;
-        const int64_t o = at(g, col % g.nx, col / g.nx, k);
-        cp_async_elem(sd + n, TD + o);
-        cp_async_elem(sm + n, TC + o);
-        cp_async_elem(sc + n, TU + o);
+        const int i = n % nx, j = (n / nx) % ny, k = n / (nx * ny);
+        const int64_t o = at(g, i, j, k);
+        xs[n] = x[o];
+        sd[n] = TD[o];
+        sm[n] = TC[o];
+        sc[n] = TU[o];
     }
-    cp_async_commit();
-    cp_async_wait<0>();
     __syncthreads();
-    const int half = (g.nx + 1) / 2;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const int half = (nx + 1) / 2;
+    const int ncc = half * ny;
     for (int s = 0; s < nrelax; ++s) {
         for (int color = 0; color < 2; ++color) {
-            const int ccols = half * g.ny;  // columns of the colour (some past nx when nx is odd)
-            for (int n = threadIdx.x; n < ccols * nz; n += blockDim.x) {
-                const int cc = n % ccols, k = n / ccols;
+            for (int cc = warp; cc < ncc; cc += nwarps) {
                 const int j = cc / half;
                 const int i = 2 * (cc % half) + ((j + color) & 1);
-                if (i >= g.nx) { continue; }
-                const int64_t o = at(g, i, j, k);
-                const int q = k * ncols + j * g.nx + i;
-                sx[q] = x[o];
-                sr[q] = bv[o] - adotx_cell<T>(g, b, i, j, k, x, AX, AY, AZ, J, m);
-            }
-            __syncthreads();
-            for (int cc = threadIdx.x; cc < ccols; cc += blockDim.x) {
-                const int j = cc / half;
-                const int i = 2 * (cc % half) + ((j + color) & 1);
-                if (i >= g.nx) { continue; }
-                const int col = j * g.nx + i;
-                T ep = sr[col] * sm[col];
-                sr[col] = ep;
-                for (int k = 1; k < nz; ++k) {
-                    const int q = k * ncols + col;
-                    ep = (sr[q] - sd[q] * ep) * sm[q];
-                    sr[q] = ep;
+                if (i >= nx) { continue; }
+                int im, ip, sim, sip, jm, jp, sjm, sjp;
+                resolve_neighbours(i, nx, b.per_x, b.sxl, b.sxh, im, ip, sim, sip);
+                resolve_neighbours(j, ny, b.per_y, b.syl, b.syh, jm, jp, sjm, sjp);
+                const int cx[3] = {im, i, ip}, cy[3] = {jm * nx, j * nx, jp * nx};
+                const int sx3[3] = {sim, 1, sip}, sy3[3] = {sjm, 1, sjp};
+                T R[P], D[P], IM[P], CP[P], X0[P];
+#pragma unroll
+                for (int q = 0; q < P; ++q) {
+                    const int k = min(lane * P + q, nz - 1);
+                    const int km = (k == 0) ? 0 : k - 1, kp = (k == nz - 1) ? k : k + 1;
+                    const int skm = (k == 0) ? b.szl : 1, skp = (k == nz - 1) ? b.szh : 1;
+                    const int cz[3] = {km * nx * ny, k * nx * ny, kp * nx * ny};
+                    const int sz3[3] = {skm, 1, skp};
+                    auto X = [&](int di, int dj, int dk) {
+                        const T v = xs[cx[di + 1] + cy[dj + 1] + cz[dk + 1]];
+                        return (sx3[di + 1] * sy3[dj + 1] * sz3[dk + 1] < 0) ? -v : v;
+                    };
+                    const int64_t o = at(g, i, j, k);
+                    const int n = cx[1] + cy[1] + cz[1];
+                    R[q] = bv[o] - adotx_body<T, true>(g, b, i, j, k, o, X, AX, AY, AZ, J, m);
+                    D[q] = sd[n];
+                    IM[q] = sm[n];
+                    CP[q] = sc[n];
+                    X0[q] = xs[n];
                 }
-                T xk = ep;
-                int64_t o = at(g, i, j, nz - 1);
-                x[o] = sx[(nz - 1) * ncols + col] + xk;
-                for (int k = nz - 2; k >= 0; --k) {
-                    const int q = k * ncols + col;
-                    o -= g.sz;
-                    xk = sr[q] - sc[q] * xk;
-                    x[o] = sx[q] + xk;
+                __syncwarp();
+                // e_k = (r_k - D_k e_{k-1}) / m_k over this lane's levels as e = al + be e_in, scanned over the lanes
+                T al = T(0), be = T(1);
+#pragma unroll
+                for (int q = 0; q < P; ++q) {
+                    const int k = lane * P + q;
+                    if (k < nz) {
+                        if (k == 0) {
+                            al = R[q] * IM[q];
+                            be = T(0);
+                        } else {
+                            al = (R[q] - D[q] * al) * IM[q];
+                            be = (-D[q] * be) * IM[q];
+                        }
+                    }
                 }
+                for (int d = 1; d < 32; d <<= 1) {
+                    const T al2 = __shfl_up_sync(kAll, al, d), be2 = __shfl_up_sync(kAll, be, d);
+                    if (lane >= d) {
+                        al = al + be * al2;
+                        be = be * be2;
+                    }
+                }
+                T ep = __shfl_up_sync(kAll, al, 1);
+                if (lane == 0) { ep = T(0); }
+#pragma unroll
+                for (int q = 0; q < P; ++q) {
+                    const int k = lane * P + q;
+                    if (k < nz) {
+                        ep = (k == 0) ? R[q] * IM[q] : (R[q] - D[q] * ep) * IM[q];
+                        R[q] = ep;
+                    }
+                }
+                // x_k = e_k - c'_k x_{k+1} over this lane's levels as x = ga + de x_in
+                T ga = T(0), de = T(1);
+#pragma unroll
+                for (int q = P - 1; q >= 0; --q) {
+                    const int k = lane * P + q;
+                    if (k < nz) {
+                        if (k == nz - 1) {
+                            ga = R[q];
+                            de = T(0);
+                        } else {
+                            ga = R[q] - CP[q] * ga;
+                            de = -CP[q] * de;
+                        }
+                    }
+                }
+                for (int d = 1; d < 32; d <<= 1) {
+                    const T ga2 = __shfl_down_sync(kAll, ga, d), de2 = __shfl_down_sync(kAll, de, d);
+                    if (lane + d < 32) {
+                        ga = ga + de * ga2;
+                        de = de * de2;
+                    }
+                }
+                T xk = __shfl_down_sync(kAll, ga, 1);
+                if (lane == 31) { xk = T(0); }
+#pragma unroll
+                for (int q = P - 1; q >= 0; --q) {
+                    const int k = lane * P + q;
+                    if (k < nz) {
+                        xk = (k == nz - 1) ? R[q] : R[q] - CP[q] * xk;
+                        xs[cx[1] + cy[1] + k * nx * ny] = X0[q] + xk;
+                    }
+                }
+                __syncwarp();
             }
             __syncthreads();
         }
+    }
+    for (int n = threadIdx.x; n < plane; n += blockDim.x) {
+        const int i = n % nx, j = (n / nx) % ny, k = n / (nx * ny);
+        x[at(g, i, j, k)] = xs[n];
     }
 }
 
@@ -1526,8 +1662,10 @@ void mg_smooth(gb_poisson* P, PoissonLevels<T>& L, int l)
     const int sknob = ctx->tune[GB_TUNE_LINE_SEGMENT];
     const int segL = (sknob == 4 || sknob == 8) ? sknob : ((g.nz + 3) / 4 <= 16 ? 4 : 8);
     const int segW = (g.nz + segL - 1) / segL;
-    const bool seg = fknob == 4 && segW <= 16 && !(g.periodic_x && (g.nx & 1))
-                     && !(g.periodic_y && (g.ny & 1));
+    // (GB_TUNE_MG_FUSED_RELAX 5: the segmented one-launch form on the levels
+    // of at least 4096 columns only, the two launches below)
+    const bool seg = (fknob == 4 || (fknob == 5 && g.nx * g.ny >= 4096)) && segW <= 16
+                     && !(g.periodic_x && (g.nx & 1)) && !(g.periodic_y && (g.ny & 1));
     if (seg) {
         const dim3 block(32, segW);
         const dim3 grid((half + 31) / 32, g.ny);
@@ -1604,13 +1742,28 @@ template <typename T>
 void build_line_tridiag(gb_poisson* P, PoissonLevels<T>& L)
 {
     gb_ctx* ctx = P->ctx;
+    LineLevels<T> A{};
+    A.n = P->nlev;
+    A.cells[0] = 0;
+    A.cols[0] = 0;
     for (int l = 0; l < P->nlev; ++l) {
         const gb_grid& g = L.g[l];
-        k_line_tridiag<T><<<cols_grid(g, g.nz), kColsBlock, 0, ctx->stream>>>(g, L.b[l], L.AX[l], L.AY[l], L.AZ[l],
-                                                                              L.J[l], L.z[l], L.TD[l], L.TC[l], L.TU[l]);
-        k_line_factor<T><<<cols_grid(g, 1), kColsBlock, 0, ctx->stream>>>(g, L.TD[l], L.TC[l], L.TU[l]);
-        ctx->launches += 2;
+        A.g[l] = g;
+        A.b[l] = L.b[l];
+        A.AX[l] = L.AX[l];
+        A.AY[l] = L.AY[l];
+        A.AZ[l] = L.AZ[l];
+        A.J[l] = L.J[l];
+        A.z[l] = L.z[l];
+        A.TD[l] = L.TD[l];
+        A.TC[l] = L.TC[l];
+        A.TU[l] = L.TU[l];
+        A.cells[l + 1] = A.cells[l] + static_cast<int64_t>(g.nx) * g.ny * g.nz;
+        A.cols[l + 1] = A.cols[l] + static_cast<int64_t>(g.nx) * g.ny;
     }
+    k_line_tridiag_all<T><<<static_cast<unsigned>((A.cells[A.n] + 255) / 256), 256, 0, ctx->stream>>>(A);
+    k_line_factor_all<T><<<static_cast<unsigned>((A.cols[A.n] + 127) / 128), 128, 0, ctx->stream>>>(A);
+    ctx->launches += 2;
 }
 
 template <typename T>
@@ -1749,20 +1902,30 @@ void vcycle(gb_poisson* P, PoissonLevels<T>& L, int l)
     if (l == tail_start(P, L) && mg_tail(P, L, l)) { return; }
     if (l == P->nlev - 1) {
         const gb_grid& g = L.g[l];
-        const size_t smem = static_cast<size_t>(5) * g.nx * g.ny * g.nz * sizeof(T);
+        const size_t smem = static_cast<size_t>(4) * g.nx * g.ny * g.nz * sizeof(T);
+        const int pl = (g.nz + 31) / 32;
         const bool one_block = ctx->tune[GB_TUNE_MG_COARSE_KERNEL] != 1 && g.nx * g.ny <= 64 && smem <= kSmoothSmemMax
-                               && !(g.periodic_x && (g.nx & 1)) && !(g.periodic_y && (g.ny & 1));
+                               && pl <= 4 && !(g.periodic_x && (g.nx & 1)) && !(g.periodic_y && (g.ny & 1));
         if (one_block && P->opt.nu_coarse > 0) {
             static std::atomic<bool> attr_done[2];  // set once per process (one device per process)
             const int ti = sizeof(T) == 8 ? 1 : 0;
             if (!attr_done[ti].load()) {
-                cudaFuncSetAttribute(k_coarse_relax<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmoothSmemMax);
+                cudaFuncSetAttribute(k_coarse_relax<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmoothSmemMax);
+                cudaFuncSetAttribute(k_coarse_relax<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmoothSmemMax);
+                cudaFuncSetAttribute(k_coarse_relax<T, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmoothSmemMax);
+                cudaFuncSetAttribute(k_coarse_relax<T, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmoothSmemMax);
                 attr_done[ti].store(true);
             }
             Span span(ctx, GB_KERNEL_MG_SMOOTH);
-            k_coarse_relax<T><<<1, 256, smem, ctx->stream>>>(g, L.b[l], P->opt.nu_coarse, L.x[l], L.bv[l], L.AX[l],
-                                                             L.AY[l], L.AZ[l], L.J[l], L.ratios(l), L.TD[l], L.TC[l],
-                                                             L.TU[l]);
+#define GB_COARSE_ARGS g, L.b[l], P->opt.nu_coarse, L.x[l], L.bv[l], L.AX[l], L.AY[l], L.AZ[l], L.J[l], L.ratios(l), \
+                       L.TD[l], L.TC[l], L.TU[l]
+            switch (pl) {
+            case 1: k_coarse_relax<T, 1><<<1, 256, smem, ctx->stream>>>(GB_COARSE_ARGS); break;
+            case 2: k_coarse_relax<T, 2><<<1, 256, smem, ctx->stream>>>(GB_COARSE_ARGS); break;
+            case 3: k_coarse_relax<T, 3><<<1, 256, smem, ctx->stream>>>(GB_COARSE_ARGS); break;
+            default: k_coarse_relax<T, 4><<<1, 256, smem, ctx->stream>>>(GB_COARSE_ARGS); break;
+            }
+#undef GB_COARSE_ARGS
             ++ctx->launches;
             return;
         }

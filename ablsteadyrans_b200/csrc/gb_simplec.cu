@@ -552,6 +552,9 @@ struct FieldFill {
 struct FillPack {
     FieldFill F[6];
 };
+struct FillPack2 {
+    FieldFill F[2][6];   // per side of the launch
+};
 
 //! FillBoundary of the lateral ghosts (two layers) of every field for the
 //! periodic directions: x over the valid y and z, then y over the x ghosts.
@@ -604,27 +607,37 @@ void fill_periodic_all(gb_simplec* S, double* const* f, const int* t, int nf)
 //! BoundaryConditions.cpp:418-517), fields in the reference's order. homog:
 //! the homogeneous fill of an increment (every boundary value, inflow
 //! profile and gradient taken as 0, BoundaryConditions.cpp:421-517).
-void fill_side(gb_simplec* S, const gb_state& q, int d, bool lo, bool homog = false)
+void fill_side(gb_simplec* S, const gb_state& q, int d, int sides, bool homog = false)
 {
     const gb_grid g = S->g;
     const int ng = g.ng;
-    const int face = d + (lo ? 0 : 3);
-    const int ft = S->bc.face[face];
-    FieldFill FF[6];
+    // the sides this launch fills: bit 0 the low side, bit 1 the high side
+    int nsides = 0;
+    bool side_lo[2] = {true, false};
+    FillPack2 P{};
     double* arr[6] = {q.u, q.v, q.w, q.p, q.theta, q.tke};
-    for (int f = 0; f < 6; ++f) {
-        FF[f].a = arr[f];
-        FF[f].t = kLoc[f];
-        FF[f].f = f;
-        FF[f].rule = rule_for(f, ft, d, lo);
-        FF[f].V = (ft == GB_FACE_NO_SLIP_WALL && f <= F_W && !homog) ? S->bc.wall_velocity[face][f] : 0.0;
-        FF[f].gg = nullptr;
-        if (ft == GB_FACE_SURFACE_LAYER && FF[f].rule == R_GRADIENT && !homog) {
-            FF[f].gg = S->gg[f == F_U ? 0 : f == F_V ? 1 : 2];
+    for (int sd = 0; sd < 2; ++sd) {
+        if (!(sides & (1 << sd))) { continue; }
+        const bool lo = (sd == 0);
+        const int face = d + (lo ? 0 : 3);
+        const int ft = S->bc.face[face];
+        for (int f = 0; f < 6; ++f) {
+            FieldFill& F = P.F[nsides][f];
+            F.a = arr[f];
+            F.t = kLoc[f];
+            F.f = f;
+            F.rule = rule_for(f, ft, d, lo);
+            F.V = (ft == GB_FACE_NO_SLIP_WALL && f <= F_W && !homog) ? S->bc.wall_velocity[face][f] : 0.0;
+            F.gg = nullptr;
+            if (ft == GB_FACE_SURFACE_LAYER && F.rule == R_GRADIENT && !homog) {
+                F.gg = S->gg[f == F_U ? 0 : f == F_V ? 1 : 2];
+            }
         }
+        side_lo[nsides] = lo;
+        ++nsides;
     }
-    FillPack P;
-    std::memcpy(P.F, FF, sizeof(FF));
+    if (nsides == 0) { return; }
+    const bool lo0 = side_lo[0], lo1 = side_lo[1];
     const Profile prof = S->prof;
     const double* z = S->z;
     const double G = homog ? 0.0 : S->bc.zhi_theta_grad;
@@ -637,20 +650,24 @@ void fill_side(gb_simplec* S, const gb_state& q, int d, bool lo, bool homog = fa
         b.lo[e] = grow ? -ng : 0;
         b.hi[e] = ((e == 0) ? g.nx : (e == 1) ? g.ny : g.nz) + (grow ? ng : 0);
     }
-    // one thread per (point, field): the fields' fills are independent (each
-    // reads only its own array), so the six run side by side; the layer
-    // index along d carries the field (layer + (ng + 1) * field)
+    // one thread per (point, field, side): the fields' fills are independent
+    // (each reads only its own array), and so are the two sides' (they write
+    // and read disjoint points: the caller merges them only when the extent
+    // along d is at least 2 ng + 2); the layer index along d carries the
+    // field and the side (layer + (ng + 1) (field + 6 side))
     b.lo[d] = 0;
-    b.hi[d] = 6 * (ng + 1) - 1;
+    b.hi[d] = nsides * 6 * (ng + 1) - 1;
     const int pe0 = per[0], pe1 = per[1];
     for_box(S->ctx, b, [=] __device__(int i0, int j0, int k0) {
         int c[3] = {i0, j0, k0};
-        const int n = c[d] / (ng + 1);
-        c[d] -= n * (ng + 1);
+        const int fs = c[d] / (ng + 1);
+        c[d] -= fs * (ng + 1);
+        const int sd = fs / 6, n = fs % 6;
+        const bool lo = (sd == 0) ? lo0 : lo1;
         const int layer = c[d];
         const int i = c[0], j = c[1], k = c[2];
         {
-            const FieldFill& F = P.F[n];
+            const FieldFill& F = P.F[sd][n];
             const int t = F.t;
             // this field's slab extent in the other directions
             bool inside = true;
@@ -744,8 +761,13 @@ void fill_ghosts_into(gb_simplec* S, const gb_state& q, double* const* ss, bool 
             turb_ground_gradients(S->ctx, S->g, S->bc, ss, S->mesh.z0, S->gg);
         }
         if (is_per(S->g, d)) { continue; }
-        fill_side(S, q, d, true, homog);
-        fill_side(S, q, d, false, homog);
+        const int nd = (d == 0) ? S->g.nx : (d == 1) ? S->g.ny : S->g.nz;
+        if (nd >= 2 * S->g.ng + 2) {
+            fill_side(S, q, d, 3, homog);
+        } else {
+            fill_side(S, q, d, 1, homog);
+            fill_side(S, q, d, 2, homog);
+        }
         if (d == 2) {
             // the no-flux w faces after u, v, w (p, theta, k do not read w)
             fill_no_flux_w(S, q);
