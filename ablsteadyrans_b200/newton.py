@@ -511,9 +511,14 @@ def main(argv=None):
     ap.add_argument("--switch-residual", type=float, default=1e-4)
     ap.add_argument("--switch-window", type=int, default=20)
     ap.add_argument("--restart", type=int, default=60)
+    N = NewtonOptions
+    ap.add_argument("--preconditioner", type=int, default=N.SIMPLEC, choices=[N.IDENTITY, N.SIMPLEC, N.SIMPLEC_STAGE],
+                    help="0 identity, 1 SIMPLEC (a_P denominators, the default), 2 SIMPLEC (the stage's)")
     args = ap.parse_args(argv)
+    names = {N.IDENTITY: "identity", N.SIMPLEC: "SIMPLEC (a_P denominators)",
+             N.SIMPLEC_STAGE: "SIMPLEC (stage denominators)"}
     out = {"workload": f"config 1: 150 m Gaussian hill {args.nx}x{args.nx}x{args.nz}, dx 25 m, the k-L closure and "
-                       "the surface layer; the Newton stage's preconditioner: identity"}
+                       f"the surface layer; the Newton stage's preconditioner: {names[args.preconditioner]}"}
     for mode in ("simplec", "simplec_newton"):
         inst = workloads.config1(args.nx, args.nx, args.nz)
         ctx = gb.Context()
@@ -529,7 +534,7 @@ def main(argv=None):
         else:
             verdict, n, nn = solve_simplec_newton(
                 stage, args.max_iterations, switch=SwitchOptions(args.switch_residual, args.switch_window),
-                newton_options=NewtonOptions.make(gmres_restart=args.restart))
+                newton_options=NewtonOptions.make(gmres_restart=args.restart, preconditioner=args.preconditioner))
         torch.cuda.synchronize()
         out[mode] = {"verdict": verdict, "iterations": n, "newton_iterations": nn, "seconds": time.perf_counter() - t0}
         res, _ = stage.norms()

@@ -365,8 +365,9 @@ def poisson_rooflines(ctx, wl, flush, peak, reps=12):
 
 # ------------------------------------------------------------ steady solves ---
 
-def steady_solves(max_iterations=3000):
-    """Config 1 from the mass-consistent initial field to the steady
+def steady_solves(max_iterations=3000, config=1):
+    """Config 1 (or config 2: the 256 x 256 x 96 fractal terrain, slopes
+    capped at 1) from the mass-consistent initial field to the steady
     criterion (the C++ driver), in plain FP64 and with FP32 inner solves:
     iterations, device seconds, steady solves/s, and the difference of the
     two steady states per field (max |mixed - FP64| / max |FP64|)."""
@@ -379,7 +380,7 @@ def steady_solves(max_iterations=3000):
     res = {}
     fields = {}
     for prec in (0, 1):
-        inst = workloads.config1(precision=prec)
+        inst = workloads.config1(precision=prec) if config == 1 else workloads.config2(precision=prec)
         ctx = gb.Context()
         case, stage = _finest(ctx, inst)
         stage.initialize()
@@ -394,7 +395,8 @@ def steady_solves(max_iterations=3000):
         torch.cuda.synchronize()
         sec = e0.elapsed_time(e1) / 1e3
         key = "fp64" if prec == 0 else "fp32_inner"
-        res[key] = {"verdict": verdict, "iterations": n, "seconds": sec, "solves_per_s": 1.0 / sec,
+        res[key] = {"verdict": verdict, "iterations": n, "seconds": sec,
+                    "solves_per_s": (1.0 / sec) if verdict == "steady" else None,
                     "cell_updates_per_s": inst.cells * n / sec}
         g = inst.grid
         fields[key] = {f: (case.q[f].cpu().numpy(), loc) for f, loc in zip(("u", "v", "w", "p", "theta", "tke"),
@@ -413,8 +415,15 @@ def steady_solves(max_iterations=3000):
         err[f] = float(np.abs(a[vv] - b[vv]).max()) / (scale if scale > 0 else 1.0)
     res["fp32_inner_vs_fp64_rel_err"] = err
     res["speedup_fp32_inner"] = res["fp64"]["seconds"] / res["fp32_inner"]["seconds"]
-    res["workload"] = ("config 1 (128x128x64 hill) from the mass-consistent initial field to the steady criterion "
-                       "(4 orders, monitors settled), the C++ driver; device time")
+    if config == 1:
+        res["workload"] = ("config 1 (128x128x64 hill) from the mass-consistent initial field to the steady criterion "
+                           "(4 orders, monitors settled), the C++ driver; device time")
+    else:
+        g = fields["fp64"]["grid"]
+        res["workload"] = (f"config 2 ({g.nx}x{g.ny}x{g.nz} fractal terrain, 120 m rms, node-to-node slopes capped at "
+                           f"{workloads.MAX_TILE_SLOPE:g}, u* 0.4 m/s from 225 deg, k-L closure, lognormal z0) from the "
+                           f"mass-consistent initial field to the steady criterion or {max_iterations} iterations; "
+                           f"device time")
     return res
 
 
@@ -479,7 +488,8 @@ def main():
     ap.add_argument("--precision", type=int, default=0, choices=[0, 1])
     ap.add_argument("--sweeps", type=int, default=4)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
-    ap.add_argument("--no-steady", action="store_true", help="skip the steady-solve leg")
+    ap.add_argument("--no-steady", action="store_true", help="skip the steady-solve legs")
+    ap.add_argument("--no-steady2", action="store_true", help="skip the config-2 steady-solve leg")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched leg")
     ap.add_argument("--no-serve", action="store_true", help="skip the served leg")
     ap.add_argument("--tune", action="append", default=[], metavar="KEY=VALUE",
@@ -625,6 +635,8 @@ def main():
     torch.cuda.empty_cache()
     if world == 1 and not args.no_steady:
         line["steady"] = steady_solves()
+        if not args.no_steady2:
+            line["steady_config2"] = steady_solves(max_iterations=3000, config=2)
     if world == 1 and not args.no_batch:
         line["batched"] = batched_leg()
     if world == 1 and not args.no_serve:
