@@ -32,7 +32,7 @@ KERNEL_LINE_SWEEP, KERNEL_POISSON_APPLY, KERNEL_MG_SMOOTH, KERNEL_MG_TRANSFER, K
     KERNEL_MASSFLUX, KERNEL_COEFS, KERNEL_VECTOR, KERNEL_BC = range(9)
 (TUNE_LINE_VARIANT, TUNE_LINE_BLOCK, TUNE_MG_COARSE_KERNEL, TUNE_LINE_DEPTH, TUNE_LINE_BACK, TUNE_MG_FUSED_RELAX,
  TUNE_GRAPHS, TUNE_MG_SOLVE, TUNE_LINE_FIRST, TUNE_LINE_SEGMENT, TUNE_RESIDUAL, TUNE_MG_TAIL,
- TUNE_MG_STENCIL) = range(13)
+ TUNE_MG_STENCIL, TUNE_PDL) = range(14)
 STATUS_NAMES = {0: "OK", 1: "BAD_ARG", 2: "NONFINITE", 3: "NOT_CONVERGED", 4: "TIMEOUT", 5: "OOM", 6: "CUDA"}
 
 

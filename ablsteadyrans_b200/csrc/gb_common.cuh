@@ -8,6 +8,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/gust_b200.h"
@@ -105,6 +106,44 @@ __device__ __forceinline__ void cp_async_elem(T* smem_dst, const T* gmem_src)
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// ------------------------------------------- programmatic dependent launch ---
+//
+// A kernel launched by launch_pdl may begin while the kernel before it on the
+// stream is finishing (its launch and block scheduling overlap the previous
+// kernel's tail). Such a kernel calls pdl_entry() first: griddepcontrol.wait
+// blocks until the previous grid has completed and its memory operations
+// are visible (it returns at once for a launch without that dependency),
+// then griddepcontrol.launch_dependents lets the next programmatic launch
+// be scheduled. Every access of global memory follows the wait, so a
+// kernel neither reads before its producer's writes land nor writes what
+// its predecessor may still read. Launches between other stream operations
+// (a memset, an event) are serialised as usual.
+
+__device__ __forceinline__ void pdl_entry()
+{
+    asm volatile("griddepcontrol.wait;\n" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
+}
+
+//! A launch with programmatic stream serialisation (the kernel must call
+//! pdl_entry() before touching global memory); a plain launch when pdl is false.
+template <typename... KArgs, typename... Args>
+cudaError_t launch_pdl(bool pdl, void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t stream,
+                       Args&&... args)
+{
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = pdl ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
 
 // ------------------------------------------ bulk copies (TMA) and mbarriers ---
 //

@@ -733,6 +733,7 @@ __global__ void __launch_bounds__(512) zline_seg_pref_multi_kernel(MultiLineArgs
 template <typename T, bool FIRST, int L>
 __global__ void __maxnreg__(96) zline_seg_multi_kernel(MultiLineArgs<T> m)
 {
+    pdl_entry();
     switch (blockIdx.z) {
     case 0: zline_seg_body<T, FIRST, L>(m.a[0], m.inv[0], m.cp[0]); break;
     case 1: zline_seg_body<T, FIRST, L>(m.a[1], m.inv[1], m.cp[1]); break;
@@ -1047,17 +1048,18 @@ gb_status zline_sweeps_multi(gb_ctx* ctx, const gb_grid& g, int n, const int* lo
                 ctx->launches += 2;
                 continue;
             }
+            const bool pdl = ctx->tune[GB_TUNE_PDL] != 1;
             if (segL == 4) {
                 if (k == 0) {
-                    zline_seg_multi_kernel<T, true, 4><<<grid, block, sm, ctx->stream>>>(m);
+                    launch_pdl(pdl, zline_seg_multi_kernel<T, true, 4>, grid, block, sm, ctx->stream, m);
                 } else {
-                    zline_seg_multi_kernel<T, false, 4><<<grid, block, sm, ctx->stream>>>(m);
+                    launch_pdl(pdl, zline_seg_multi_kernel<T, false, 4>, grid, block, sm, ctx->stream, m);
                 }
             } else {
                 if (k == 0) {
-                    zline_seg_multi_kernel<T, true, 8><<<grid, block, sm, ctx->stream>>>(m);
+                    launch_pdl(pdl, zline_seg_multi_kernel<T, true, 8>, grid, block, sm, ctx->stream, m);
                 } else {
-                    zline_seg_multi_kernel<T, false, 8><<<grid, block, sm, ctx->stream>>>(m);
+                    launch_pdl(pdl, zline_seg_multi_kernel<T, false, 8>, grid, block, sm, ctx->stream, m);
                 }
             }
             ++ctx->launches;

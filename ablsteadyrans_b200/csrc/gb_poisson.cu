@@ -84,6 +84,7 @@ __global__ void k_apply(gb_grid g, PBC b, const T* __restrict__ x, const T* __re
                         const T* __restrict__ AZ, const T* __restrict__ J, MeshRatios<T> m,
                         const T* __restrict__ rhs, T* __restrict__ y)
 {
+    pdl_entry();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     const int k = blockIdx.z;
@@ -364,6 +365,7 @@ __global__ void k_color_residual(gb_grid g, PBC b, int color, const T* __restric
                                  const T* __restrict__ AX, const T* __restrict__ AY, const T* __restrict__ AZ,
                                  const T* __restrict__ J, MeshRatios<T> m, T* __restrict__ r)
 {
+    pdl_entry();
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     const int i = 2 * (blockIdx.x * blockDim.x + threadIdx.x) + ((j + color) & 1);
     const int k = blockIdx.z;
@@ -620,6 +622,7 @@ __global__ void __launch_bounds__(64) k_color_solve(gb_grid g, int color, const 
                                                     const T* __restrict__ TD, const T* __restrict__ TC,
                                                     const T* __restrict__ TU, T* __restrict__ x)
 {
+    pdl_entry();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int tid = threadIdx.x;
     const int nthr = blockDim.x;
@@ -677,6 +680,7 @@ __global__ void __launch_bounds__(32) k_color_solve_staged(gb_grid g, int color,
                                                            const T* __restrict__ TD, const T* __restrict__ TC,
                                                            const T* __restrict__ TU, T* __restrict__ x)
 {
+    pdl_entry();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int tid = threadIdx.x;
     const int nthr = blockDim.x;
@@ -801,6 +805,7 @@ __global__ void __launch_bounds__(512) k_color_solve_seg(gb_grid g, int color, c
                                                          const T* __restrict__ TD, const T* __restrict__ TC,
                                                          const T* __restrict__ TU, T* __restrict__ x)
 {
+    pdl_entry();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x;
     const int w = threadIdx.y;
@@ -1041,18 +1046,23 @@ __device__ __forceinline__ void prolong_cell(const gb_grid& gc, const PBC& bcb, 
 
 template <typename T>
 __global__ void k_restrict(gb_grid gf, const T* __restrict__ Jf, const T* __restrict__ rf, gb_grid gc,
-                           const T* __restrict__ Jc, T* __restrict__ bc)
+                           const T* __restrict__ Jc, T* __restrict__ bc, T* __restrict__ xc)
 {
+    pdl_entry();
     const int I = blockIdx.x * blockDim.x + threadIdx.x;
     const int J2 = blockIdx.y * blockDim.y + threadIdx.y;
     const int k = blockIdx.z;
     if (I >= gc.nx || J2 >= gc.ny) { return; }
     restrict_cell<T>(gf, Jf, rf, gc, Jc, bc, I, J2, k);
+    // the coarse correction starts from zero (its ghosts are never read: every
+    // kernel resolves a level's ghosts by index)
+    if (xc != nullptr) { xc[at(gc, I, J2, k)] = T(0); }
 }
 
 template <typename T>
 __global__ void k_prolong_add(gb_grid gc, PBC bcb, const T* __restrict__ xc, gb_grid gf, T* __restrict__ xf)
 {
+    pdl_entry();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     const int k = blockIdx.z;
@@ -1078,6 +1088,7 @@ __global__ void __launch_bounds__(256) k_coarse_relax(gb_grid g, PBC b, int nrel
                                                       MeshRatios<T> m, const T* __restrict__ TD,
                                                       const T* __restrict__ TC, const T* __restrict__ TU)
 {
+    pdl_entry();
     constexpr unsigned kAll = 0xffffffffu;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int nx = g.nx, ny = g.ny, nz = g.nz;
@@ -1630,6 +1641,7 @@ template <typename T>
 void mg_smooth(gb_poisson* P, PoissonLevels<T>& L, int l)
 {
     gb_ctx* ctx = P->ctx;
+    const bool pdl = ctx->tune[GB_TUNE_PDL] != 1;
     const gb_grid& g = L.g[l];
     const PBC& b = L.b[l];
     constexpr int R = 4;
@@ -1711,8 +1723,8 @@ void mg_smooth(gb_poisson* P, PoissonLevels<T>& L, int l)
             --ctx->launches;  // counted with the solve below
         } else {
             const dim3 rgrid((half + 31) / 32, (g.ny + 3) / 4, g.nz);
-            k_color_residual<T><<<rgrid, dim3(32, 4), 0, ctx->stream>>>(g, b, color, L.x[l], L.bv[l], L.AX[l], L.AY[l],
-                                                                       L.AZ[l], L.J[l], L.ratios(l), L.r[l]);
+            launch_pdl(pdl, k_color_residual<T>, rgrid, dim3(32, 4), 0, ctx->stream, g, b, color, L.x[l], L.bv[l],
+                       L.AX[l], L.AY[l], L.AZ[l], L.J[l], L.ratios(l), L.r[l]);
         }
         const dim3 sgrid((half + nthr - 1) / nthr, g.ny);
         const int sL = (g.nz + 7) / 8 <= 16 ? 8 : 16;
@@ -1721,18 +1733,22 @@ void mg_smooth(gb_poisson* P, PoissonLevels<T>& L, int l)
             // the segmented column solves (the default; GB_TUNE_MG_SOLVE = 1: one thread per column)
             const size_t sm = static_cast<size_t>(4) * sW * 32 * sizeof(T);
             if (sL == 8) {
-                k_color_solve_seg<T, 8><<<dim3((half + 31) / 32, g.ny), dim3(32, sW), sm, ctx->stream>>>(
-                    g, color, L.r[l], L.TD[l], L.TC[l], L.TU[l], L.x[l]);
+                launch_pdl(pdl, k_color_solve_seg<T, 8>, dim3((half + 31) / 32, g.ny), dim3(32, sW), sm, ctx->stream, g,
+                           color, static_cast<const T*>(L.r[l]), static_cast<const T*>(L.TD[l]),
+                           static_cast<const T*>(L.TC[l]), static_cast<const T*>(L.TU[l]), L.x[l]);
             } else {
-                k_color_solve_seg<T, 16><<<dim3((half + 31) / 32, g.ny), dim3(32, sW), sm, ctx->stream>>>(
-                    g, color, L.r[l], L.TD[l], L.TC[l], L.TU[l], L.x[l]);
+                launch_pdl(pdl, k_color_solve_seg<T, 16>, dim3((half + 31) / 32, g.ny), dim3(32, sW), sm, ctx->stream,
+                           g, color, static_cast<const T*>(L.r[l]), static_cast<const T*>(L.TD[l]),
+                           static_cast<const T*>(L.TC[l]), static_cast<const T*>(L.TU[l]), L.x[l]);
             }
         } else if (staged) {
-            k_color_solve_staged<T><<<sgrid, nthr, smem_staged, ctx->stream>>>(g, color, L.r[l], L.TD[l], L.TC[l],
-                                                                              L.TU[l], L.x[l]);
+            launch_pdl(pdl, k_color_solve_staged<T>, sgrid, dim3(nthr), smem_staged, ctx->stream, g, color,
+                       static_cast<const T*>(L.r[l]), static_cast<const T*>(L.TD[l]), static_cast<const T*>(L.TC[l]),
+                       static_cast<const T*>(L.TU[l]), L.x[l]);
         } else {
-            k_color_solve<T, R><<<sgrid, nthr, smem_ring, ctx->stream>>>(g, color, L.r[l], L.TD[l], L.TC[l], L.TU[l],
-                                                                         L.x[l]);
+            launch_pdl(pdl, k_color_solve<T, R>, sgrid, dim3(nthr), smem_ring, ctx->stream, g, color,
+                       static_cast<const T*>(L.r[l]), static_cast<const T*>(L.TD[l]), static_cast<const T*>(L.TC[l]),
+                       static_cast<const T*>(L.TU[l]), L.x[l]);
         }
         ctx->launches += 2;
     }
@@ -1777,8 +1793,10 @@ void mg_residual(gb_poisson* P, PoissonLevels<T>& L, int l)
                                L.r[l]);
         return;
     }
-    k_apply<T><<<cols_grid(g, g.nz), kColsBlock, 0, ctx->stream>>>(g, L.b[l], L.x[l], L.AX[l], L.AY[l], L.AZ[l],
-                                                                   L.J[l], L.ratios(l), L.bv[l], L.r[l]);
+    launch_pdl(ctx->tune[GB_TUNE_PDL] != 1, k_apply<T>, cols_grid(g, g.nz), kColsBlock, 0, ctx->stream, g, L.b[l],
+               static_cast<const T*>(L.x[l]), static_cast<const T*>(L.AX[l]), static_cast<const T*>(L.AY[l]),
+               static_cast<const T*>(L.AZ[l]), static_cast<const T*>(L.J[l]), L.ratios(l),
+               static_cast<const T*>(L.bv[l]), L.r[l]);
     ++ctx->launches;
 }
 
@@ -1899,6 +1917,7 @@ template <typename T>
 void vcycle(gb_poisson* P, PoissonLevels<T>& L, int l)
 {
     gb_ctx* ctx = P->ctx;
+    const bool pdl = ctx->tune[GB_TUNE_PDL] != 1;
     if (l == tail_start(P, L) && mg_tail(P, L, l)) { return; }
     if (l == P->nlev - 1) {
         const gb_grid& g = L.g[l];
@@ -1917,13 +1936,15 @@ void vcycle(gb_poisson* P, PoissonLevels<T>& L, int l)
                 attr_done[ti].store(true);
             }
             Span span(ctx, GB_KERNEL_MG_SMOOTH);
-#define GB_COARSE_ARGS g, L.b[l], P->opt.nu_coarse, L.x[l], L.bv[l], L.AX[l], L.AY[l], L.AZ[l], L.J[l], L.ratios(l), \
-                       L.TD[l], L.TC[l], L.TU[l]
+#define GB_COARSE_ARGS g, L.b[l], P->opt.nu_coarse, L.x[l], static_cast<const T*>(L.bv[l]), \
+                       static_cast<const T*>(L.AX[l]), static_cast<const T*>(L.AY[l]), static_cast<const T*>(L.AZ[l]), \
+                       static_cast<const T*>(L.J[l]), L.ratios(l), static_cast<const T*>(L.TD[l]), \
+                       static_cast<const T*>(L.TC[l]), static_cast<const T*>(L.TU[l])
             switch (pl) {
-            case 1: k_coarse_relax<T, 1><<<1, 256, smem, ctx->stream>>>(GB_COARSE_ARGS); break;
-            case 2: k_coarse_relax<T, 2><<<1, 256, smem, ctx->stream>>>(GB_COARSE_ARGS); break;
-            case 3: k_coarse_relax<T, 3><<<1, 256, smem, ctx->stream>>>(GB_COARSE_ARGS); break;
-            default: k_coarse_relax<T, 4><<<1, 256, smem, ctx->stream>>>(GB_COARSE_ARGS); break;
+            case 1: launch_pdl(pdl, k_coarse_relax<T, 1>, dim3(1), dim3(256), smem, ctx->stream, GB_COARSE_ARGS); break;
+            case 2: launch_pdl(pdl, k_coarse_relax<T, 2>, dim3(1), dim3(256), smem, ctx->stream, GB_COARSE_ARGS); break;
+            case 3: launch_pdl(pdl, k_coarse_relax<T, 3>, dim3(1), dim3(256), smem, ctx->stream, GB_COARSE_ARGS); break;
+            default: launch_pdl(pdl, k_coarse_relax<T, 4>, dim3(1), dim3(256), smem, ctx->stream, GB_COARSE_ARGS); break;
             }
 #undef GB_COARSE_ARGS
             ++ctx->launches;
@@ -1938,15 +1959,16 @@ void vcycle(gb_poisson* P, PoissonLevels<T>& L, int l)
     const gb_grid& gc = L.g[l + 1];
     {
         Span span(ctx, GB_KERNEL_MG_TRANSFER);
-        k_restrict<T><<<cols_grid(gc, gc.nz), kColsBlock, 0, ctx->stream>>>(gf, L.J[l], L.r[l], gc, L.J[l + 1],
-                                                                            L.bv[l + 1]);
+        launch_pdl(pdl, k_restrict<T>, cols_grid(gc, gc.nz), kColsBlock, 0, ctx->stream, gf,
+                   static_cast<const T*>(L.J[l]), static_cast<const T*>(L.r[l]), gc, static_cast<const T*>(L.J[l + 1]),
+                   L.bv[l + 1], L.x[l + 1]);
         ++ctx->launches;
     }
-    cudaMemsetAsync(L.x[l + 1], 0, sizeof(T) * volume(gc), ctx->stream);
     vcycle(P, L, l + 1);
     {
         Span span(ctx, GB_KERNEL_MG_TRANSFER);
-        k_prolong_add<T><<<cols_grid(gf, gf.nz), kColsBlock, 0, ctx->stream>>>(gc, L.b[l + 1], L.x[l + 1], gf, L.x[l]);
+        launch_pdl(pdl, k_prolong_add<T>, cols_grid(gf, gf.nz), kColsBlock, 0, ctx->stream, gc, L.b[l + 1],
+                   static_cast<const T*>(L.x[l + 1]), gf, L.x[l]);
         ++ctx->launches;
     }
     for (int s = 0; s < P->opt.nu2; ++s) { mg_smooth(P, L, l); }
@@ -2051,9 +2073,10 @@ void apply_fine(gb_poisson* P, const double* x, const double* rhs, double* y)
         launch_tiles<double, false>(P, g, P->dl.b[0], -1, x, P->dl.AX[0], P->dl.AY[0], P->dl.AZ[0], P->dl.J[0],
                                     P->dl.ratios(0), rhs, y);
     } else {
-        k_apply<double><<<cols_grid(g, g.nz), kColsBlock, 0, ctx->stream>>>(g, P->dl.b[0], x, P->dl.AX[0],
-                                                                            P->dl.AY[0], P->dl.AZ[0], P->dl.J[0],
-                                                                            P->dl.ratios(0), rhs, y);
+        launch_pdl(ctx->tune[GB_TUNE_PDL] != 1, k_apply<double>, cols_grid(g, g.nz), kColsBlock, 0, ctx->stream, g,
+                   P->dl.b[0], x, static_cast<const double*>(P->dl.AX[0]), static_cast<const double*>(P->dl.AY[0]),
+                   static_cast<const double*>(P->dl.AZ[0]), static_cast<const double*>(P->dl.J[0]), P->dl.ratios(0),
+                   rhs, y);
         ++ctx->launches;
     }
     if (P->cross_ad != nullptr) {

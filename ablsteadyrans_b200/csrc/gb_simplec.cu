@@ -250,6 +250,7 @@ struct RedPack {
 
 __global__ void k_sumsq_partial_many(gb_grid g, const __grid_constant__ RedPack P, double* __restrict__ partial)
 {
+    pdl_entry();
     const RedItem& it = P.it[blockIdx.y];
     const Box b = it.b;
     const double* __restrict__ f = it.f;
@@ -279,6 +280,7 @@ __global__ void k_sumsq_partial_many(gb_grid g, const __grid_constant__ RedPack 
 __global__ void k_sum_partials_many(const __grid_constant__ RedPack P, const double* __restrict__ partial, int nb,
                                     double* __restrict__ out)
 {
+    pdl_entry();
     const int slot = P.it[blockIdx.x].slot;
     __shared__ double red[8];
     double s = 0;
@@ -296,6 +298,7 @@ __global__ void k_sum_partials_many(const __grid_constant__ RedPack P, const dou
 __global__ void __launch_bounds__(256) k_maxabs_many(gb_grid g, const __grid_constant__ RedPack P,
                                                      unsigned long long* __restrict__ words)
 {
+    pdl_entry();
     const RedItem& it = P.it[blockIdx.y];
     const Box b = it.b;
     const double* __restrict__ f = it.f;
@@ -492,8 +495,10 @@ void dsum_many(gb_simplec* S, const RedPack& P)
     gb_ctx* ctx = S->ctx;
     if (P.n <= 0) { return; }
     Span span(ctx, GB_KERNEL_VECTOR);
-    k_sumsq_partial_many<<<dim3(kRedBlocks, P.n), 256, 0, ctx->stream>>>(S->g, P, S->w.partial);
-    k_sum_partials_many<<<P.n, 256, 0, ctx->stream>>>(P, S->w.partial, kRedBlocks, S->w.sums);
+    const bool pdl = ctx->tune[GB_TUNE_PDL] != 1;
+    launch_pdl(pdl, k_sumsq_partial_many, dim3(kRedBlocks, P.n), dim3(256), 0, ctx->stream, S->g, P, S->w.partial);
+    launch_pdl(pdl, k_sum_partials_many, dim3(P.n), dim3(256), 0, ctx->stream, P,
+               static_cast<const double*>(S->w.partial), static_cast<int>(kRedBlocks), S->w.sums);
     ctx->launches += 2;
 }
 
@@ -508,7 +513,8 @@ void dmax_many(gb_simplec* S, const RedPack& P)
         rows = std::max(rows, (b.hi[1] - b.lo[1] + 1) * (b.hi[2] - b.lo[2] + 1));
     }
     Span span(ctx, GB_KERNEL_VECTOR);
-    k_maxabs_many<<<dim3((rows + 7) / 8, P.n), 256, 0, ctx->stream>>>(S->g, P, dword(ctx, 0));
+    launch_pdl(ctx->tune[GB_TUNE_PDL] != 1, k_maxabs_many, dim3((rows + 7) / 8, P.n), dim3(256), 0, ctx->stream,
+               S->g, P, dword(ctx, 0));
     ++ctx->launches;
 }
 
@@ -1158,6 +1164,7 @@ struct StressArgs {
 template <int L>
 __global__ void __launch_bounds__(256) k_momentum_stress(const StressArgs a)
 {
+    pdl_entry();
     // the (component, direction) pairs at L in increasing C
     constexpr int C0 = (L == CC) ? 0 : (L == (XF ^ YF)) ? 0 : (L == (XF ^ ZF)) ? 0 : 1;
     constexpr int D0 = (L == CC) ? 0 : (L == (XF ^ YF)) ? 1 : 2;
@@ -1244,7 +1251,8 @@ void momentum_stress(gb_simplec* S, const gb_state& q)
         a.tauy = S->ssr[kSsTauY];
         const int64_t n = a.b.count();
         span_begin(S->ctx, GB_KERNEL_RESIDUAL);
-        k_momentum_stress<L><<<static_cast<unsigned>((n + 255) / 256), 256, 0, S->ctx->stream>>>(a);
+        launch_pdl(S->ctx->tune[GB_TUNE_PDL] != 1, k_momentum_stress<L>, dim3(static_cast<unsigned>((n + 255) / 256)),
+                   dim3(256), 0, S->ctx->stream, a);
         span_end(S->ctx);
         ++S->ctx->launches;
     };
@@ -1319,6 +1327,7 @@ __device__ __forceinline__ void fused_face(const FusedResidualArgs& a, int i, in
 template <int E>
 __global__ void __launch_bounds__(kFusedTx* kFusedTy) k_fused_residual(const FusedResidualArgs a)
 {
+    pdl_entry();
     constexpr int T = (E < 3) ? (1 << E) : CC;
     constexpr int lx = flux_lo(T, 0), ly = flux_lo(T, 1), lz = flux_lo(T, 2);
     __shared__ double xc[kFusedTy][kFusedTx + 1], xd[kFusedTy][kFusedTx + 1];
@@ -1415,7 +1424,7 @@ void fused_residual(gb_simplec* S, const gb_state& q, double* R)
     const dim3 block(kFusedTx, kFusedTy);
     const dim3 grid((a.ni + kFusedTx - 1) / kFusedTx, (a.nj + kFusedTy - 1) / kFusedTy, (a.nk + a.kc - 1) / a.kc);
     span_begin(S->ctx, GB_KERNEL_RESIDUAL);
-    k_fused_residual<E><<<grid, block, 0, S->ctx->stream>>>(a);
+    launch_pdl(S->ctx->tune[GB_TUNE_PDL] != 1, k_fused_residual<E>, grid, block, 0, S->ctx->stream, a);
     span_end(S->ctx);
     ++S->ctx->launches;
 }
@@ -1752,6 +1761,7 @@ __global__ void __launch_bounds__(kFusedTx* kFusedTy)
                          const double* __restrict__ F1, const double* __restrict__ F2, const double* __restrict__ gm,
                          double* __restrict__ A)
 {
+    pdl_entry();
     constexpr int T = (C < 0) ? CC : (1 << C);
     constexpr int lx = flux_lo(T, 0), ly = flux_lo(T, 1), lz = flux_lo(T, 2);
     __shared__ double xdif[kFusedTy][kFusedTx + 1], xtr[kFusedTy][kFusedTx + 1];
@@ -1818,7 +1828,8 @@ void implicit_coefficients_on(gb_ctx* ctx, const gb_grid g, const double* z, con
         const dim3 block(kFusedTx, kFusedTy);
         const dim3 grid((ni + kFusedTx - 1) / kFusedTx, (nj + kFusedTy - 1) / kFusedTy, (nk + kc - 1) / kc);
         span_begin(ctx, GB_KERNEL_COEFS);
-        k_fused_coefficients<C><<<grid, block, 0, ctx->stream>>>(g, ni, nj, nk, kc, z, J, logz, F0, F1, F2, gm, A);
+        launch_pdl(ctx->tune[GB_TUNE_PDL] != 1, k_fused_coefficients<C>, grid, block, 0, ctx->stream, g, ni, nj, nk,
+                   kc, z, J, logz, F0, F1, F2, gm, A);
         span_end(ctx);
         ++ctx->launches;
         return;
@@ -1883,6 +1894,7 @@ __device__ __forceinline__ void apply_fold(const FoldFace& F, double* A, int64_t
 //! point's folds in that order (the order of the per-face launches).
 __global__ void k_fold_rows(const gb_grid g, const __grid_constant__ FoldPack P, double* __restrict__ A)
 {
+    pdl_entry();
     const int64_t n = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
     if (n >= P.start[P.n]) { return; }
     int q = 0;
@@ -1945,7 +1957,8 @@ void apply_to_implicit(gb_simplec* S, int f, int t, double* A)
     const int64_t total = P.start[P.n];
     if (total == 0) { return; }
     span_begin(S->ctx, GB_KERNEL_COEFS);
-    k_fold_rows<<<static_cast<unsigned>((total + 255) / 256), 256, 0, S->ctx->stream>>>(g, P, A);
+    launch_pdl(S->ctx->tune[GB_TUNE_PDL] != 1, k_fold_rows, dim3(static_cast<unsigned>((total + 255) / 256)),
+               dim3(256), 0, S->ctx->stream, g, P, A);
     span_end(S->ctx);
     ++S->ctx->launches;
 }

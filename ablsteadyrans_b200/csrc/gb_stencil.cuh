@@ -112,6 +112,7 @@ inline Box valid_box(const gb_grid& g, int t)
 template <typename F>
 __global__ void k_box(Box b, F f)
 {
+    pdl_entry();
     const int64_t n = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
     const int nx = b.hi[0] - b.lo[0] + 1, ny = b.hi[1] - b.lo[1] + 1;
     if (n >= b.count()) { return; }
@@ -128,7 +129,8 @@ void for_box(gb_ctx* ctx, const Box& b, F f, int family = -1)
     const int64_t n = b.count();
     if (n <= 0) { return; }
     if (family >= 0) { span_begin(ctx, family); }
-    k_box<<<static_cast<unsigned>((n + 255) / 256), 256, 0, ctx->stream>>>(b, f);
+    launch_pdl(ctx->tune[GB_TUNE_PDL] != 1, k_box<F>, dim3(static_cast<unsigned>((n + 255) / 256)), dim3(256), 0,
+               ctx->stream, b, f);
     if (family >= 0) { span_end(ctx); }
     ++ctx->launches;
 }

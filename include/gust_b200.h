@@ -139,6 +139,9 @@ enum {
                                    0 default and 1 one thread per cell, 2 TMA-staged tiles of the iterate
                                    on every level (measured slower: the other ten words a cell stay
                                    direct loads and each level costs two block barriers) */
+    GB_TUNE_PDL,                /* programmatic dependent launch of the multigrid's kernels and the stage's
+                                   one-thread-per-point kernels (each one's launch overlaps its predecessor's
+                                   tail): 0 default on, 1 off */
     GB_N_TUNE
 };
 gb_status gb_ctx_tune(gb_ctx* ctx, int32_t key, int32_t value);
