@@ -72,6 +72,7 @@ def _declare(L):
     L.gb_ctx_profile.argtypes = [P, i32]
     L.gb_ctx_profile_read.argtypes = [P, i32, ctypes.POINTER(f64), ctypes.POINTER(i64)]
     L.gb_ctx_profile_mask.argtypes = [P, ctypes.c_uint32]
+    L.gb_probe_fp64.argtypes = [P, i32, P, ctypes.POINTER(i64)]
     L.gb_zline_jacobi.argtypes = [P, G, i32, P, P, P, i32, P, ctypes.POINTER(f64)]
     L.gb_zline_jacobi_f32.argtypes = [P, G, i32, P, P, P, i32, P, ctypes.POINTER(ctypes.c_float)]
     L.gb_zline_jacobi_noalloc.argtypes = [G, i32, P, P, P, i32, P, ctypes.POINTER(f64), P]
@@ -170,6 +171,15 @@ def zline_jacobi(ctx, grid, loc, A, ap, rhs, sweeps, delta):
     return float(out.value)
 
 
+def probe_fp64(ctx, iters, sink):
+    """gb_probe_fp64: 8 chains of `iters` dependent FP64 FMAs per thread on the
+    context's stream (sink: 4 * SMs * 256 doubles); returns the FP64
+    operations it executes (2 per FMA)."""
+    threads = ctypes.c_int64()
+    check(lib().gb_probe_fp64(ctx.handle, int(iters), _ptr(sink), ctypes.byref(threads)))
+    return 2 * 8 * int(iters) * threads.value
+
+
 def implicit_coefficients(ctx, grid, loc, F, gamma, z, J, log_mean, A):
     """gust::implicit_coefficients (Source/ImplicitOperator.H:65-67) at loc:
     the upwind transport of F (three face tensors) and the principal
@@ -244,6 +254,7 @@ def _declare_poisson(L):
     L.gb_poisson_apply.argtypes = [P, P, P]
     L.gb_poisson_vcycle.argtypes = [P, P, P]
     L.gb_poisson_solve.argtypes = [P, P, P, ctypes.POINTER(PoissonResult)]
+    L.gb_tucker_wall_distance.argtypes = [P, G, P, ctypes.POINTER(PoissonOptions), P, ctypes.POINTER(PoissonResult)]
     L.gb_poisson_fluxes.argtypes = [P, P, P, P, P, P, P, P]
 
 
@@ -262,6 +273,18 @@ def _lib_full():
 def _zeros(grid, dtype=None):
     import torch
     return torch.zeros(grid.shape, dtype=dtype or torch.float64, device="cuda")
+
+
+def tucker_wall_distance(ctx, grid, z_nd, options=None):
+    """gust::tucker_wall_distance (Source/WallDistance.H:14-33): Tucker's
+    wall distance on the terrain mesh (a device volume of the grid with its
+    ghosts) and the Poisson solve's PoissonResult."""
+    L = _lib_full()
+    dist = _zeros(grid)
+    res = PoissonResult()
+    opt = ctypes.byref(options) if options is not None else None
+    check(L.gb_tucker_wall_distance(ctx.handle, ctypes.byref(grid.c), _ptr(z_nd), opt, _ptr(dist), ctypes.byref(res)))
+    return dist, res
 
 
 def mesh_metrics(ctx, grid, z_nd):

@@ -340,6 +340,16 @@ gb_status gb_simplec_turbulence(gb_simplec* s, double* const* closure, double* c
     return gb::simplec_turbulence(s, closure, surface);
 }
 
+gb_status gb_simplec_set_wall_distance(gb_simplec* s, const double* dist)
+{
+    gb::clear_error();
+    if (s == nullptr || dist == nullptr) {
+        gb::set_error("gust: SimplecStage::set_wall_distance: null argument");
+        return GB_BAD_ARG;
+    }
+    return gb::simplec_set_wall_distance(s, dist);
+}
+
 gb_status gb_simplec_destroy(gb_simplec* s)
 {
     gb::clear_error();

@@ -135,6 +135,30 @@ gb_status check_loc(const char* op, int loc)
 
 }  // namespace gb
 
+namespace gb {
+
+//! The FP64 pipe's rate: 8 independent chains of dependent fused
+//! multiply-adds per thread (a = a * b + c with b just below 1, so the
+//! values stay finite), the chains' sum written out.
+__global__ void __launch_bounds__(256) k_probe_fp64(int iters, double* __restrict__ sink)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    double a[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) { a[q] = 1.0 + 1e-3 * (t + q); }
+    const double b = 0.999999, c = 1e-7;
+    for (int n = 0; n < iters; ++n) {
+#pragma unroll
+        for (int q = 0; q < 8; ++q) { a[q] = fma(a[q], b, c); }
+    }
+    double s = 0;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) { s += a[q]; }
+    sink[t] = s;
+}
+
+}  // namespace gb
+
 extern "C" {
 
 gb_status gb_grid_init(gb_grid* g, int32_t nx, int32_t ny, int32_t nz, int32_t ng, double dx, double dy,
@@ -266,6 +290,19 @@ gb_status gb_ctx_profile_read(gb_ctx* ctx, int32_t family, double* total_ms, int
     *total_ms = t;
     *spans = n;
     return GB_OK;
+}
+
+gb_status gb_probe_fp64(gb_ctx* ctx, int32_t iters, double* sink, int64_t* threads)
+{
+    gb::clear_error();
+    if (ctx == nullptr || sink == nullptr || threads == nullptr || iters < 1) {
+        gb::set_error("gust: gb_probe_fp64: null argument or iters < 1");
+        return GB_BAD_ARG;
+    }
+    const int blocks = 4 * ctx->num_sms;
+    gb::k_probe_fp64<<<blocks, 256, 0, ctx->stream>>>(iters, sink);
+    *threads = static_cast<int64_t>(blocks) * 256;
+    return gb::check_cuda("gb_probe_fp64");
 }
 
 const char* gb_last_error(void) { return gb::g_error.c_str(); }

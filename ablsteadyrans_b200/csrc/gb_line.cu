@@ -723,15 +723,26 @@ __global__ void __launch_bounds__(512) zline_seg_pref_multi_kernel(MultiLineArgs
     }
 }
 
+//! The segmented sweep's register cap per thread for L levels a warp. Two
+//! blocks of nk / L warps share an SM; each of its 4 schedulers holds 16 K
+//! registers, so the warps one scheduler takes times 32 lanes times the cap
+//! must fit 16 K: 96 for L = 8 (9 warps a block on 65 levels), 64 for L = 5
+//! (13 warps), 56 for L = 4 (17 warps).
+constexpr int seg_reg_cap(int L)
+{
+    return L == 4 ? 56 : (L == 5 ? 64 : 96);
+}
+
 //! The segmented sweep over several systems (MultiLineArgs; blockIdx.z picks
-//! the system, with constant indices into the parameter block). At most 96
-//! registers a thread (no spills at L = 8): an SM's register file is split
-//! among its 4 schedulers, and two blocks of 9 warps place 5 warps on one of
-//! them, which 96 registers a thread fit (5 x 96 x 32 <= 16 K) and the 104
-//! the compiler picks unbounded do not: a second block per SM then doubles
-//! the warps that hide the segment loads' latency.
+//! the system, with constant indices into the parameter block). The register
+//! cap (seg_reg_cap, no spills at any L) lets two blocks share an SM: its
+//! register file is split among its 4 schedulers, and two blocks of W warps
+//! place ceil(W / 2) warps on one of them. At L = 5 (the default) a block of
+//! 13 warps at 64 registers gives 26 warps an SM to hide the segment loads'
+//! latency, against 18 at L = 8 and 96 registers (the 104 the compiler picks
+//! unbounded would fit one block only).
 template <typename T, bool FIRST, int L>
-__global__ void __maxnreg__(96) zline_seg_multi_kernel(MultiLineArgs<T> m)
+__global__ void __maxnreg__(seg_reg_cap(L)) zline_seg_multi_kernel(MultiLineArgs<T> m)
 {
     pdl_entry();
     switch (blockIdx.z) {
@@ -748,21 +759,32 @@ constexpr size_t seg_smem_bytes(int warps)
     return static_cast<size_t>(8) * warps * 32 * sizeof(T);
 }
 
-//! Levels per segment of the segmented sweep (GB_TUNE_LINE_SEGMENT: 4 or 8,
-//! default 8) and its warps per block for nk levels; 0 when the column is too
-//! tall (more than 16 segments), which the callers then sweep with the
-//! factored kernel.
+//! Levels per segment of the segmented sweep (GB_TUNE_LINE_SEGMENT: 4, 5 or 8,
+//! default 5) and its warps per block for nk levels; 0 when the column is too
+//! tall (more segments than seg_max_warps), which the callers then sweep with
+//! the factored kernel. The split form's solves (zline_seg_pref_multi_kernel,
+//! 512 threads a block) take at most kSegMaxWarps segments.
 constexpr int kSegMaxWarps = 16;
 
 inline int seg_levels(const gb_ctx* ctx)
 {
-    return (ctx->tune[GB_TUNE_LINE_SEGMENT] == 4) ? 4 : 8;
+    const int v = ctx->tune[GB_TUNE_LINE_SEGMENT];
+    return (v == 4 || v == 8) ? v : 5;
+}
+
+
+//! The segmented multi-system kernel's warps a block at most for L levels a
+//! warp: a block's registers (warps x 32 x the cap) within the SM's 64 K, and
+//! 32 warps.
+constexpr int seg_max_warps(int L)
+{
+    return (65536 / (32 * seg_reg_cap(L)) < 32) ? 65536 / (32 * seg_reg_cap(L)) : 32;
 }
 
 inline int seg_warps(int nk, int L)
 {
     const int w = (nk + L - 1) / L;
-    return (w >= 1 && w <= kSegMaxWarps) ? w : 0;
+    return (w >= 1 && w <= seg_max_warps(L)) ? w : 0;
 }
 
 //! The two copies of a periodic seam face take the low copy's value.
@@ -984,8 +1006,21 @@ gb_status zline_sweeps_multi(gb_ctx* ctx, const gb_grid& g, int n, const int* lo
         for (int s = 0; s < n; ++s) { max_cols = std::max(max_cols, ni[s] * nj[s]); }
         const dim3 grid((max_cols + 31) / 32, 1, n);
         const size_t sm = seg_smem_bytes<T>(segW);
+        if (sm > 48 * 1024) {
+            // more than 24 FP64 segments (tall columns at L = 4 or 5): the carries need the opt-in
+            static std::atomic<bool> big_attr[2];  // set once per process (one device per process)
+            const int ti = sizeof(T) == 8 ? 1 : 0;
+            if (!big_attr[ti].load()) {
+                const int big = static_cast<int>(seg_smem_bytes<T>(32));
+                cudaFuncSetAttribute(zline_seg_multi_kernel<T, true, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+                cudaFuncSetAttribute(zline_seg_multi_kernel<T, false, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+                cudaFuncSetAttribute(zline_seg_multi_kernel<T, true, 5>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+                cudaFuncSetAttribute(zline_seg_multi_kernel<T, false, 5>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+                big_attr[ti].store(true);
+            }
+        }
         // GB_TUNE_LINE_VARIANT 6: the later sweeps split into the fold and light column solves
-        const bool split = ctx->tune[GB_TUNE_LINE_VARIANT] == 6 && sweeps > 1;
+        const bool split = ctx->tune[GB_TUNE_LINE_VARIANT] == 6 && sweeps > 1 && segW <= kSegMaxWarps;
         // GB_TUNE_LINE_FIRST 2: the first sweep (the factorisation) by the sequential factored kernel,
         // which stores the same factors (1/m, c') the segmented later sweeps read
         constexpr int RF = (sizeof(T) == 8) ? 4 : 8;
@@ -1042,6 +1077,8 @@ gb_status zline_sweeps_multi(gb_ctx* ctx, const gb_grid& g, int n, const int* lo
                 k_line_fold<T><<<fgrid, 128, 0, ctx->stream>>>(m, max_nk);
                 if (segL == 4) {
                     zline_seg_pref_multi_kernel<T, 4><<<grid, block, sm, ctx->stream>>>(m);
+                } else if (segL == 5) {
+                    zline_seg_pref_multi_kernel<T, 5><<<grid, block, sm, ctx->stream>>>(m);
                 } else {
                     zline_seg_pref_multi_kernel<T, 8><<<grid, block, sm, ctx->stream>>>(m);
                 }
@@ -1054,6 +1091,12 @@ gb_status zline_sweeps_multi(gb_ctx* ctx, const gb_grid& g, int n, const int* lo
                     launch_pdl(pdl, zline_seg_multi_kernel<T, true, 4>, grid, block, sm, ctx->stream, m);
                 } else {
                     launch_pdl(pdl, zline_seg_multi_kernel<T, false, 4>, grid, block, sm, ctx->stream, m);
+                }
+            } else if (segL == 5) {
+                if (k == 0) {
+                    launch_pdl(pdl, zline_seg_multi_kernel<T, true, 5>, grid, block, sm, ctx->stream, m);
+                } else {
+                    launch_pdl(pdl, zline_seg_multi_kernel<T, false, 5>, grid, block, sm, ctx->stream, m);
                 }
             } else {
                 if (k == 0) {

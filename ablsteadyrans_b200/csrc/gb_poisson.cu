@@ -2152,7 +2152,7 @@ gb_status poisson_build(gb_poisson* P)
     for (int l = 0; l < P->nlev; ++l) {
         const gb_grid& g = grids[l];
         D.g[l] = g;
-        D.b[l] = make_pbc(g, P->bc, true);
+        D.b[l] = make_pbc(g, P->bc, P->bc[2] != PF_DIRICHLET);
         const int64_t vol = volume(g);
         if (l == 0) {
             D.z[l] = const_cast<double*>(P->z_fine);
@@ -2378,6 +2378,12 @@ gb_status poisson_fluxes(gb_poisson* P, const double* phi, const double* bx, con
 {
     gb_ctx* ctx = P->ctx;
     const gb_grid& g = P->g;
+    if (P->bc[2] == PF_DIRICHLET) {
+        // the pressure correction's fluxes have a zero-flux ground; a Dirichlet
+        // ground's one-sided flux is in the operator (the Tucker solve) only
+        set_error("gust: PoissonSolver::fluxes with a Dirichlet ground is not supported");
+        return GB_BAD_ARG;
+    }
     Span span(ctx, GB_KERNEL_POISSON_APPLY);
     k_fluxes<<<cols_grid(g, g.nz + 1, 1), kColsBlock, 0, ctx->stream>>>(g, P->dl.b[0], phi, P->dl.ratios(0), bx, by, bz, fx,
                                                                         fy, fz);

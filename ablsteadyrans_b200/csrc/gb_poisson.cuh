@@ -16,6 +16,9 @@ namespace gb {
 
 enum { PF_PERIODIC = 0, PF_NEUMANN = 1, PF_DIRICHLET = 2 };
 enum { TP_XLO = 1, TP_XHI = 2, TP_YLO = 4, TP_YHI = 8, TP_ZLO = 16, TP_ZHI = 32 };
+//! zf bit: a Dirichlet ground (phi = 0 on it: the odd ghost below the ground
+//! and the ground-face flux, Source/Poisson.cpp:158-189)
+enum { TP_DGROUND = 64 };
 
 //! Boundary description of one Poisson level: periodic flags, the mirror
 //! sign of each non-periodic face (+1 Neumann, -1 Dirichlet), and the
@@ -44,6 +47,7 @@ inline PBC make_pbc(const gb_grid& g, const int* bc, bool ground_even)
     if (!g.periodic_y && bc[1] == PF_NEUMANN) { b.zf |= TP_YLO; }
     if (!g.periodic_y && bc[4] == PF_NEUMANN) { b.zf |= TP_YHI; }
     if (bc[5] == PF_NEUMANN) { b.zf |= TP_ZHI; }
+    if (bc[2] == PF_DIRICHLET) { b.zf |= TP_DGROUND; }
     return b;
 }
 
@@ -85,6 +89,7 @@ struct MeshRatios {
     const T* __restrict__ hz;
     const T* __restrict__ sx;
     const T* __restrict__ sy;
+    const T* __restrict__ zn;  // the level's node heights (the Dirichlet ground's one-sided flux)
 };
 
 //! One value of the iterate at offset (di, dj, dk) from cell (i, j, k) at
@@ -95,6 +100,48 @@ __device__ __forceinline__ T xoff(const T* x, const gb_grid& g, const PBC& b, in
 {
     if (INTERIOR) { return x[o + di + dj * g.sy + dk * g.sz]; }
     return ldc<T>(x, x, g, b, i + di, j + dj, k + dk);
+}
+
+//! terrpoisson_flux_zlo_dir (ERF_TerrainPoisson_3D_K.H:214-275): the ground
+//! face's flux of column (i, j) with phi = 0 on the ground (one-sided), the
+//! iterate's values at the ground level read by X(di, dj, 0) (resolved
+//! lateral neighbours), the node heights from zn.
+template <typename T, typename XA>
+__device__ __forceinline__ T ground_flux_dir(const gb_grid& g, int i, int j, XA&& X, const T* __restrict__ zn)
+{
+    const int k = 0;
+    const T dxinv = static_cast<T>(1.0 / g.dx), dyinv = static_cast<T>(1.0 / g.dy);
+    const T h = T(0.5), q = T(0.25);
+#define ZN(a, b, c) zn[at(g, a, b, c)]
+    const T x00 = X(0, 0, 0);
+    T pz_lo = x00;
+    const T hzeta_inv_on_zlo = T(8) / ((ZN(i, j, k + 1) + ZN(i + 1, j, k + 1) + ZN(i, j + 1, k + 1) + ZN(i + 1, j + 1, k + 1))
+                                       - (ZN(i, j, k) + ZN(i + 1, j, k) + ZN(i, j + 1, k) + ZN(i + 1, j + 1, k)));
+    pz_lo *= hzeta_inv_on_zlo;
+    const T px_hi_md_lo = T(0), px_lo_md_lo = T(0), py_md_hi_lo = T(0), py_md_lo_lo = T(0);
+    T h_xi, h_eta, h_zeta;
+    T pz_hi_md_lo = h * (X(1, 0, 0) + x00);
+    h_xi = q * (ZN(i + 2, j, k) - ZN(i, j, k) + ZN(i + 2, j + 1, k) - ZN(i, j + 1, k)) * dxinv;
+    h_zeta = q * (ZN(i + 1, j, k + 1) - ZN(i + 1, j, k) + ZN(i + 1, j + 1, k + 1) - ZN(i + 1, j + 1, k));
+    pz_hi_md_lo *= h_xi / h_zeta;
+    T pz_lo_md_lo = h * (x00 + X(-1, 0, 0));
+    h_xi = q * (ZN(i + 1, j, k) - ZN(i - 1, j, k) + ZN(i + 1, j + 1, k) - ZN(i - 1, j + 1, k)) * dxinv;
+    h_zeta = q * (ZN(i, j, k + 1) - ZN(i, j, k) + ZN(i, j + 1, k + 1) - ZN(i, j + 1, k));
+    pz_lo_md_lo *= h_xi / h_zeta;
+    T pz_md_hi_lo = h * (X(0, 1, 0) + x00);
+    h_eta = q * (ZN(i, j + 2, k) - ZN(i, j, k) + ZN(i + 1, j + 2, k) - ZN(i + 1, j, k)) * dyinv;
+    h_zeta = q * (ZN(i, j + 1, k + 1) - ZN(i, j + 1, k) + ZN(i + 1, j + 1, k + 1) - ZN(i + 1, j + 1, k));
+    pz_md_hi_lo *= h_eta / h_zeta;
+    T pz_md_lo_lo = h * (x00 + X(0, -1, 0));
+    h_eta = q * (ZN(i, j + 1, k) - ZN(i, j - 1, k) + ZN(i + 1, j + 1, k) - ZN(i + 1, j - 1, k)) * dyinv;
+    h_zeta = q * (ZN(i, j, k + 1) - ZN(i, j, k) + ZN(i + 1, j, k + 1) - ZN(i + 1, j, k));
+    pz_md_lo_lo *= h_eta / h_zeta;
+    const T h_xi_on_zlo = h * (ZN(i + 1, j + 1, k) + ZN(i + 1, j, k) - ZN(i, j + 1, k) - ZN(i, j, k)) * dxinv;
+    const T h_eta_on_zlo = h * (ZN(i + 1, j + 1, k) + ZN(i, j + 1, k) - ZN(i + 1, j, k) - ZN(i, j, k)) * dyinv;
+#undef ZN
+    pz_lo -= h * h_xi_on_zlo * ((px_hi_md_lo + px_lo_md_lo) - (pz_hi_md_lo + pz_lo_md_lo));
+    pz_lo -= h * h_eta_on_zlo * ((py_md_hi_lo + py_md_lo_lo) - (pz_md_hi_lo + pz_md_lo_lo));
+    return -pz_lo;
 }
 
 //! The terrain operator at cell (i, j, k) with the iterate's 15 values read by
@@ -171,7 +218,12 @@ __device__ __forceinline__ T adotx_body(const gb_grid& g, const PBC& b, int i, i
     const T y = (axa[o + 1] * px_hi - axa[o] * px_lo) * dxinv
               + (aya[o + sy] * py_hi - aya[o] * py_lo) * dyinv
               + (aza[o + sz] * pz_hi - aza[o] * pz_lo) * dzinv;
-    return y / Jc[o];
+    T v = y / Jc[o];
+    if (MASKS && (b.zf & TP_DGROUND) && k == 0) {
+        // a Dirichlet ground: the ground-face flux ERF's kernel leaves out (Source/Poisson.cpp:162-189)
+        v += aza[o] * ground_flux_dir<T>(g, i, j, X, m.zn) * dzinv / Jc[o];
+    }
+    return v;
 }
 
 //! The operator at (i, j, k) with the neighbours read directly (INTERIOR: all
@@ -262,6 +314,14 @@ __device__ __forceinline__ void line_tridiag(const gb_grid& g, const PBC& b, con
     const T wh = mzh * AZ[at(g, i, j, k + 1)] * hzi_hi * dzinv;
     const T wl = mzl * AZ[at(g, i, j, k)] * hzi_lo * dzinv;
     c -= wh + wl;
+    if (k == 0 && (b.zf & TP_DGROUND)) {
+        // a Dirichlet ground: the ground face's principal part, one-sided
+        const T hzi_g = T(8) / ((zp[at(g, i, j, 1)] + zp[at(g, i + 1, j, 1)] + zp[at(g, i, j + 1, 1)]
+                                 + zp[at(g, i + 1, j + 1, 1)])
+                                - (zp[at(g, i, j, 0)] + zp[at(g, i + 1, j, 0)] + zp[at(g, i, j + 1, 0)]
+                                   + zp[at(g, i + 1, j + 1, 0)]));
+        c -= AZ[at(g, i, j, 0)] * hzi_g * dzinv;
+    }
     T u = wh, d = wl;
     if (k == g.nz - 1) {
         c += (b.szh < 0 ? T(-1) : T(1)) * u;

@@ -31,7 +31,7 @@ struct PoissonLevels {
     T* HZ[kMaxLevels] = {};
     T* SX[kMaxLevels] = {};
     T* SY[kMaxLevels] = {};
-    MeshRatios<T> ratios(int l) const { return MeshRatios<T>{RX[l], RY[l], HZ[l], SX[l], SY[l]}; }
+    MeshRatios<T> ratios(int l) const { return MeshRatios<T>{RX[l], RY[l], HZ[l], SX[l], SY[l], z[l]}; }
     std::vector<void*> owned;
     void release();
 };

@@ -3328,6 +3328,16 @@ void simplec_implicit_rows_at(gb_simplec* S, const gb_state& q, int eq, double* 
     simplec_implicit_rows(S, eq, S->w.F, A);
 }
 
+gb_status simplec_set_wall_distance(gb_simplec* S, const double* dist)
+{
+    if (!S->ph.closure || S->dist == nullptr) {
+        set_error("gust: SimplecStage::set_wall_distance: the stage has no closure (turb.model)");
+        return GB_BAD_ARG;
+    }
+    cudaMemcpyAsync(S->dist, dist, sizeof(double) * volume(S->g), cudaMemcpyDeviceToDevice, S->ctx->stream);
+    return check_cuda("SimplecStage::set_wall_distance");
+}
+
 gb_status simplec_turbulence(gb_simplec* S, double* const* closure, double* const* surface)
 {
     gb_ctx* ctx = S->ctx;

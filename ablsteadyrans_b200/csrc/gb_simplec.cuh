@@ -8,6 +8,7 @@ struct gb_simplec;
 namespace gb {
 
 gb_status simplec_build(gb_simplec* S);
+gb_status simplec_set_wall_distance(gb_simplec* S, const double* dist);
 void simplec_delete(gb_simplec* S);
 void simplec_fill_ghosts(gb_simplec* S, const gb_state& q);
 void simplec_residual(gb_simplec* S, const gb_state& q, double** R);

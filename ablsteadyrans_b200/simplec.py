@@ -28,6 +28,7 @@ def _declare(L):
     L.gb_simplec_initialize.argtypes = [P, ctypes.POINTER(abi.State), ctypes.POINTER(abi.InitOptions),
                                         ctypes.POINTER(abi.InitResult)]
     L.gb_simplec_turbulence.argtypes = [P, ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_void_p)]
+    L.gb_simplec_set_wall_distance.argtypes = [P, P]
     L.gb_simplec_implicit_rows.argtypes = [P, ctypes.POINTER(abi.State), ctypes.c_int32, P]
     L.gb_simplec_norms.argtypes = [P, ctypes.POINTER(abi.State), ctypes.POINTER(ctypes.c_double),
                                    ctypes.POINTER(ctypes.c_double)]
@@ -120,10 +121,12 @@ class SimplecStage:
         st = self.case.state()
         check(self._L.gb_simplec_fill_ghosts(self._h, ctypes.byref(st)))
 
-    def residual(self):
+    def residual(self, out=None):
+        """The six residuals at the state (into `out`, six grid tensors, when given)."""
         import torch
         from . import check
-        R = [torch.zeros(self.case.grid.shape, dtype=torch.float64, device="cuda") for _ in range(6)]
+        R = out if out is not None else [torch.zeros(self.case.grid.shape, dtype=torch.float64, device="cuda")
+                                         for _ in range(6)]
         arr = (ctypes.c_void_p * 6)(*[r.data_ptr() for r in R])
         st = self.case.state()
         check(self._L.gb_simplec_residual(self._h, ctypes.byref(st), arr))
@@ -137,6 +140,12 @@ class SimplecStage:
         st = self.case.state()
         check(self._L.gb_simplec_implicit_rows(self._h, ctypes.byref(st), int(eq), ctypes.c_void_p(A.data_ptr())))
         return A
+
+    def set_wall_distance(self, dist):
+        """The closure's wall distance from now on (a device volume of the
+        grid, e.g. gb.tucker_wall_distance's): turb.wall_distance = tucker."""
+        from . import check
+        check(self._L.gb_simplec_set_wall_distance(self._h, ctypes.c_void_p(dist.data_ptr())))
 
     def turbulence(self, closure=True, surface=True):
         """(closure fields, surface state) as dicts of host arrays: the

@@ -363,6 +363,99 @@ def poisson_rooflines(ctx, wl, flush, peak, reps=12):
     return out
 
 
+# ----------------------------------------------------------- the residual ---
+# algorithmic words of one residual evaluation per cell: the state (u, v, w,
+# p, theta, k), the mesh (z, J and the three areas) read, the six residuals
+# written; the closure's and the transport's fields are its intermediates
+RESIDUAL_WORDS = 17
+RESIDUAL_PROFILE = os.path.join(ROOT, "profiles", "k_fused_residual_fp64_flops_config1.txt")
+
+
+def residual_flops():
+    """FP64 operations of one residual evaluation of config 1 (ncu's FP64
+    instruction counters over every launch of one call; committed capture),
+    or None."""
+    try:
+        with open(RESIDUAL_PROFILE) as f:
+            for line in f:
+                if line.startswith("fp64_flops_per_residual:"):
+                    return float(line.split(":")[1])
+    except OSError:
+        return None
+    return None
+
+
+def fp64_peak(ctx, iters=4096, reps=5):
+    """The FP64 pipe's rate on this GPU, measured in-project (gb_probe_fp64:
+    chains of dependent FMAs on every SM), best of reps, TFLOP/s."""
+    import torch
+
+    import ablsteadyrans_b200 as gb
+    sink = torch.zeros(4 * torch.cuda.get_device_properties(0).multi_processor_count * 256, dtype=torch.float64,
+                       device="cuda")
+    best = 0.0
+    stream = ctx.stream
+    for _ in range(reps + 1):
+        with torch.cuda.stream(stream):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            flops = gb.probe_fp64(ctx, iters, sink)
+            e1.record(stream)
+        torch.cuda.synchronize()
+        best = max(best, flops / (e0.elapsed_time(e1) / 1e3) / 1e12)
+    return best
+
+
+def residual_roofline(ctx, wl, flush, hbm_peak, reps=12):
+    """One residual evaluation of config 1 (the closure and the surface
+    state at the state, the transport, the stresses, the per-equation
+    launches, the forcing, the boundary rows) timed alone by CUDA events on
+    the context's stream after a 256 MB L2 flush, against the HBM roofline
+    of its algorithmic bytes and the FP64 roofline of its counted FP64
+    operations (the FP64 peak measured in-project). One more evaluation runs
+    inside the NVTX range "gust_residual", which the ncu capture that counts
+    the operations selects."""
+    import torch
+    g = wl.inst.grid
+    cells = g.nx * g.ny * g.nz
+    R = [torch.zeros(g.shape, dtype=torch.float64, device="cuda") for _ in range(6)]
+    stream = ctx.stream
+    for _ in range(3):
+        wl.stage.residual(out=R)
+    ms = []
+    for _ in range(reps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            wl.stage.residual(out=R)
+            e1.record(stream)
+        torch.cuda.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    torch.cuda.nvtx.range_push("gust_residual")
+    wl.stage.residual(out=R)
+    torch.cuda.synchronize()
+    torch.cuda.nvtx.range_pop()
+    t = statistics.median(ms)
+    nbytes = RESIDUAL_WORDS * 8 * cells
+    peak64 = fp64_peak(ctx)
+    flops = residual_flops()
+    out = {"kernel": (f"one SIMPLEC residual evaluation of config 1 ({g.nx}x{g.ny}x{g.nz}, k-L closure and surface "
+                      f"layer), FP64; {RESIDUAL_WORDS} words per cell"),
+           "launch_ms": t, "bytes_per_launch": nbytes, "achieved_gbs": nbytes / (t / 1e3) / 1e9,
+           "hbm_peak_gbs": hbm_peak, "hbm_frac": nbytes / (t / 1e3) / 1e9 / hbm_peak,
+           "fp64_peak_tflops_measured": peak64, "fp64_flops_per_launch": flops}
+    if flops is not None:
+        tf = flops / (t / 1e3) / 1e12
+        out["achieved_tflops"] = tf
+        out["fp64_frac"] = tf / peak64
+        # the bound: the resource whose roofline time is the longer
+        out["bound"] = "fp64" if flops / (peak64 * 1e12) > nbytes / (hbm_peak * 1e9) else "hbm"
+    return out
+
+
 # ------------------------------------------------------------ steady solves ---
 
 def steady_solves(max_iterations=3000, config=1):
@@ -380,7 +473,11 @@ def steady_solves(max_iterations=3000, config=1):
     res = {}
     fields = {}
     for prec in (0, 1):
-        inst = workloads.config1(precision=prec) if config == 1 else workloads.config2(precision=prec)
+        # config 2 with frozen diffusivities: with the closure it is not steady
+        # within 3000 iterations (measured 57.6 s in FP64), so the two forms'
+        # difference would compare two transients
+        inst = (workloads.config1(precision=prec) if config == 1
+                else workloads.config2(precision=prec, turbulence=False))
         ctx = gb.Context()
         case, stage = _finest(ctx, inst)
         stage.initialize()
@@ -421,9 +518,9 @@ def steady_solves(max_iterations=3000, config=1):
     else:
         g = fields["fp64"]["grid"]
         res["workload"] = (f"config 2 ({g.nx}x{g.ny}x{g.nz} fractal terrain, 120 m rms, node-to-node slopes capped at "
-                           f"{workloads.MAX_TILE_SLOPE:g}, u* 0.4 m/s from 225 deg, k-L closure, lognormal z0) from the "
-                           f"mass-consistent initial field to the steady criterion or {max_iterations} iterations; "
-                           f"device time")
+                           f"{workloads.MAX_TILE_SLOPE:g}, u* 0.4 m/s from 225 deg, frozen diffusivities: the closure "
+                           f"and the surface layer off) from the mass-consistent initial field to the steady criterion "
+                           f"or {max_iterations} iterations; device time")
     return res
 
 
@@ -629,6 +726,7 @@ def main():
         line["tune"] = args.tune
     if world == 1:
         line["rooflines"] = poisson_rooflines(ctx, wl, flush, peak)
+        line["residual_roofline"] = residual_roofline(ctx, wl, flush, peak)
     wl.stage.close()
     ctx.close()
     del flush

@@ -96,6 +96,14 @@ gb_status gb_ctx_profile_read(gb_ctx* ctx, int32_t family, double* total_ms, int
 /* Which families profiling times: bit f set = family f (default: all). Timing
  * only the family of interest keeps the events' own cost out of a timed step. */
 gb_status gb_ctx_profile_mask(gb_ctx* ctx, uint32_t mask);
+/* A measurement probe, not part of the drop-in path: `iters` dependent FP64
+ * fused multiply-adds in each of 8 independent chains per thread, on 4
+ * blocks of 256 threads per SM, launched on the context's stream (the caller
+ * times it with events there). It executes 2 * 8 * iters * threads FP64
+ * operations and writes one value per thread to sink (4 * SMs * 256
+ * doubles), so that none of the arithmetic is removed. *threads receives the
+ * thread count. */
+gb_status gb_probe_fp64(gb_ctx* ctx, int32_t iters, double* sink, int64_t* threads);
 /* Tuning knobs of a context (the in-project autotuner sets them per shape). */
 enum {
     GB_TUNE_LINE_VARIANT = 0,   /* z-line sweep kernel: 0 auto (= 5), 1 pipelined (cp.async ring), 2 shared,
@@ -124,7 +132,8 @@ enum {
                                    column's levels split among the warps of a block), 1 one thread per column */
     GB_TUNE_LINE_FIRST,         /* the first sweep of a segmented solve (the column factorisation): 0 default
                                    (= 1), 1 segmented, 2 the sequential factored kernel (the same factors) */
-    GB_TUNE_LINE_SEGMENT,       /* levels per warp of the segmented z-line sweep (default 8) and of the
+    GB_TUNE_LINE_SEGMENT,       /* levels per warp of the segmented z-line sweep (0 default = 5; 4 or 8: more
+                                   or fewer warps per column at a lower or higher register cap) and of the
                                    segmented zebra relaxation (default 4, 8 for columns of more than 64
                                    levels): 0 default, 4 or 8 */
     GB_TUNE_RESIDUAL,           /* the SIMPLEC residual's convection, diffusion and pressure gradient and
@@ -287,6 +296,21 @@ gb_status gb_poisson_vcycle(gb_poisson* p, const double* r, double* e);
  * removes phi's mean when singular, reports the true residual.
  * GB_NOT_CONVERGED names solver.poisson_max_iter. */
 gb_status gb_poisson_solve(gb_poisson* p, double* rhs, double* phi, gb_poisson_result* res);
+
+/* gust::tucker_wall_distance (Source/WallDistance.H:14-33; Source/WallDistance.cpp:
+ * 78-94): Tucker's differential wall distance on the terrain mesh of node
+ * heights z_nd. One Poisson solve of laplacian(phi) = -1 with phi = 0 on the
+ * ground (tucker_bc, Source/WallDistance.cpp:65-76: periodic lateral
+ * directions stay periodic, the other lateral faces and the top carry no
+ * flux; opt: solver.poisson_*, null for the defaults), then in every valid
+ * cell d = -|grad phi| + sqrt(|grad phi|^2 + 2 phi) with ERF's cell-centred
+ * physical gradient (the first cell's vertical derivative from the
+ * quadratic through phi = 0 on the ground), and the ghosts of dist from the
+ * valid cells (extend_by_zero_gradient, Source/Sequencing.cpp:43-60: the
+ * periodic image, else the nearest valid cell). dist: a device volume of
+ * the grid. res: the Poisson solve's result. Needs nz >= 3. */
+gb_status gb_tucker_wall_distance(gb_ctx* ctx, const gb_grid* g, const double* z_nd, const gb_poisson_opts* opt,
+                                  double* dist, gb_poisson_result* res);
 
 /* The coefficient-weighted face fluxes F = -beta grad phi with the terrain
  * cross terms and the zero-flux faces (TerrainPoisson::getFluxes,
@@ -596,6 +620,13 @@ gb_status gb_implicit_coefficients(gb_ctx* ctx, const gb_grid* g, int32_t loc, c
  * null arrays (or entries) are skipped. GB_BAD_ARG when the stage has no
  * closure (closure) or no surface_layer ground (surface). */
 gb_status gb_simplec_turbulence(gb_simplec* s, double* const* closure, double* const* surface);
+/* ResidualInputs::wall_distance (Source/Residual.H:61-128) for
+ * turb.wall_distance = tucker: the closure's wall distance from now on is a
+ * copy of dist (a device volume of the grid with its ghosts, as
+ * gb_tucker_wall_distance writes it) in place of the height above the ground
+ * (turb.wall_distance = terrain_height, the default). GB_BAD_ARG when the
+ * stage has no closure. */
+gb_status gb_simplec_set_wall_distance(gb_simplec* s, const double* dist);
 
 /* The defaults of init.* (Source/Initializer.H: z_agl_min 0, alpha_h = alpha_v
  * = 1, k_decay_height 0, projection 1, obrien 0) and solver.poisson_*. */

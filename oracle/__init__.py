@@ -288,6 +288,8 @@ def _declare_simplec(L):
                                     ctypes.POINTER(Diffusivities), PP, PP, P]
     L.og_prolong_fields.argtypes = [G, ctypes.POINTER(State), G, ctypes.POINTER(State), i32]
     L.og_set_nut_history.argtypes = [P]
+    L.og_set_wall_distance.argtypes = [P]
+    L.og_tucker_distance.argtypes = [G, P, P, P]
     L.og_restrict_state.argtypes = [G, ctypes.POINTER(State), ctypes.POINTER(MeshFields), G, ctypes.POINTER(State),
                                     ctypes.POINTER(MeshFields), i32, P]
     L.og_prolong_state.argtypes = [G, ctypes.POINTER(State), G, ctypes.POINTER(State), i32, ctypes.POINTER(BC),
@@ -498,9 +500,40 @@ def local_dtau(case, cfl, use_nu=True, nu=None, phys=None):
 
 
 def _history(case):
-    """The closure's nu_t history of the case for the next evaluations."""
+    """The closure's nu_t history and wall distance of the case for the next
+    evaluations (the wall distance: case.wall_dist, or the height above the
+    ground when it is None)."""
     h = getattr(case, "nut_hist", None)
     _L().og_set_nut_history(_p(h) if h is not None else None)
+    d = getattr(case, "wall_dist", None)
+    _L().og_set_wall_distance(_p(d) if d is not None else None)
+
+
+def tucker_bc(grid):
+    """tucker_bc (Source/WallDistance.cpp:65-76): periodic lateral directions
+    stay periodic, other lateral faces zero flux, the ground Dirichlet, the
+    top zero flux."""
+    x = PERIODIC if grid.periodic_x else NEUMANN
+    y = PERIODIC if grid.periodic_y else NEUMANN
+    return (x, y, DIRICHLET, x, y, NEUMANN)
+
+
+def tucker_wall_distance(grid, z, reltol=1e-12, max_iter=400):
+    """tucker_wall_distance (Source/WallDistance.cpp:78-94): solve
+    laplacian(phi) = -1 with phi = 0 on the ground (tucker_bc) on the
+    terrain mesh, then Tucker's distance from phi and its ghosts
+    (og_tucker_distance). Returns (dist, Poisson iterations)."""
+    J, ax, ay, az, _ = metrics(grid, z)
+    bc = tucker_bc(grid)
+    mg = Multigrid(grid, bc, z, J, ax, ay, az)
+    rhs = grid.np_zeros()
+    rhs[grid.valid(0)] = -1.0
+    phi, it, _, _, _ = mg.solve(rhs, reltol=reltol, max_iter=max_iter)
+    mg.close()
+    poisson_fill_ghosts(grid, bc, phi, ground_even=False)
+    d = grid.np_zeros()
+    _L().og_tucker_distance(ctypes.byref(grid.c), _p(z), _p(phi), _p(d))
+    return d, it
 
 
 def simplec_iterate(case, bc, phys, opts, dtau):

@@ -27,6 +27,9 @@
 enum { PF_PERIODIC = 0, PF_NEUMANN = 1, PF_DIRICHLET = 2 };
 enum { FACE_XLO = 0, FACE_YLO = 1, FACE_ZLO = 2, FACE_XHI = 3, FACE_YHI = 4, FACE_ZHI = 5 };
 enum { TP_XLO = 1, TP_XHI = 2, TP_YLO = 4, TP_YHI = 8, TP_ZLO = 16, TP_ZHI = 32 };
+/* zf bit: a Dirichlet ground (phi = 0 on it: the odd ghost below and the
+ * ground-face flux, Source/Poisson.cpp:158-189) */
+enum { TP_DGROUND = 64 };
 
 /* ------------------------------------------------------------------ */
 /* mesh                                                                */
@@ -149,8 +152,13 @@ int og_poisson_zero_flux_faces(const og_grid* g, const int* bc)
     if (!g->periodic_y && bc[FACE_YLO] == PF_NEUMANN) { zf |= TP_YLO; }
     if (!g->periodic_y && bc[FACE_YHI] == PF_NEUMANN) { zf |= TP_YHI; }
     if (bc[FACE_ZHI] == PF_NEUMANN) { zf |= TP_ZHI; }
+    if (bc[FACE_ZLO] == PF_DIRICHLET) { zf |= TP_DGROUND; }
     return zf;
 }
+
+/* The ground's ghost parity of the solve: odd for a Dirichlet ground (fill_bc_ghosts,
+ * Source/Poisson.cpp:84-125), else even whatever bc says (TerrainPoisson::apply_bcs). */
+static int ground_even(const int* bc) { return bc[FACE_ZLO] != PF_DIRICHLET; }
 
 /* ------------------------------------------------------------------ */
 /* the operator                                                        */
@@ -159,7 +167,45 @@ int og_poisson_zero_flux_faces(const og_grid* g, const int* bc)
 #define X(a, b, c) x[IX(g, a, b, c)]
 #define Z(a, b, c) zp[IX(g, a, b, c)]
 
-/* ERF_TerrainPoisson_3D_K.H:316-530 (terrpoisson_adotx) at cell (i, j, k). */
+/* terrpoisson_flux_zlo_dir (ERF_TerrainPoisson_3D_K.H:214-275): the ground
+ * face's flux of column (i, j) with phi = 0 on the ground, one-sided (the
+ * ghosts of x filled). */
+static double ground_flux_dir(const og_grid* g, int i, int j, const double* x, const double* zp)
+{
+    const int k = 0;
+    const double dxinv = 1.0 / g->dx, dyinv = 1.0 / g->dy;
+    double pz_lo = X(i, j, k);
+    const double hzeta_inv_on_zlo = 8.0 / ((Z(i, j, k + 1) + Z(i + 1, j, k + 1) + Z(i, j + 1, k + 1) + Z(i + 1, j + 1, k + 1))
+                                           - (Z(i, j, k) + Z(i + 1, j, k) + Z(i, j + 1, k) + Z(i + 1, j + 1, k)));
+    pz_lo *= hzeta_inv_on_zlo;
+    const double px_hi_md_lo = 0, px_lo_md_lo = 0, py_md_hi_lo = 0, py_md_lo_lo = 0;
+    double h_xi, h_eta, h_zeta;
+    double pz_hi_md_lo = 0.5 * (X(i + 1, j, k) + X(i, j, k));
+    h_xi = 0.25 * (Z(i + 2, j, k) - Z(i, j, k) + Z(i + 2, j + 1, k) - Z(i, j + 1, k)) * dxinv;
+    h_zeta = 0.25 * (Z(i + 1, j, k + 1) - Z(i + 1, j, k) + Z(i + 1, j + 1, k + 1) - Z(i + 1, j + 1, k));
+    pz_hi_md_lo *= h_xi / h_zeta;
+    double pz_lo_md_lo = 0.5 * (X(i, j, k) + X(i - 1, j, k));
+    h_xi = 0.25 * (Z(i + 1, j, k) - Z(i - 1, j, k) + Z(i + 1, j + 1, k) - Z(i - 1, j + 1, k)) * dxinv;
+    h_zeta = 0.25 * (Z(i, j, k + 1) - Z(i, j, k) + Z(i, j + 1, k + 1) - Z(i, j + 1, k));
+    pz_lo_md_lo *= h_xi / h_zeta;
+    double pz_md_hi_lo = 0.5 * (X(i, j + 1, k) + X(i, j, k));
+    h_eta = 0.25 * (Z(i, j + 2, k) - Z(i, j, k) + Z(i + 1, j + 2, k) - Z(i + 1, j, k)) * dyinv;
+    h_zeta = 0.25 * (Z(i, j + 1, k + 1) - Z(i, j + 1, k) + Z(i + 1, j + 1, k + 1) - Z(i + 1, j + 1, k));
+    pz_md_hi_lo *= h_eta / h_zeta;
+    double pz_md_lo_lo = 0.5 * (X(i, j, k) + X(i, j - 1, k));
+    h_eta = 0.25 * (Z(i, j + 1, k) - Z(i, j - 1, k) + Z(i + 1, j + 1, k) - Z(i + 1, j - 1, k)) * dyinv;
+    h_zeta = 0.25 * (Z(i, j, k + 1) - Z(i, j, k) + Z(i + 1, j, k + 1) - Z(i + 1, j, k));
+    pz_md_lo_lo *= h_eta / h_zeta;
+    const double h_xi_on_zlo = 0.5 * (Z(i + 1, j + 1, k) + Z(i + 1, j, k) - Z(i, j + 1, k) - Z(i, j, k)) * dxinv;
+    const double h_eta_on_zlo = 0.5 * (Z(i + 1, j + 1, k) + Z(i, j + 1, k) - Z(i + 1, j, k) - Z(i, j, k)) * dyinv;
+    pz_lo -= 0.5 * h_xi_on_zlo * ((px_hi_md_lo + px_lo_md_lo) - (pz_hi_md_lo + pz_lo_md_lo));
+    pz_lo -= 0.5 * h_eta_on_zlo * ((py_md_hi_lo + py_md_lo_lo) - (pz_md_hi_lo + pz_md_lo_lo));
+    return -pz_lo;
+}
+
+/* ERF_TerrainPoisson_3D_K.H:316-530 (terrpoisson_adotx) at cell (i, j, k);
+ * with a Dirichlet ground the bottom row adds the ground-face flux
+ * (Source/Poisson.cpp:162-189). */
 static double adotx_cell(const og_grid* g, int i, int j, int k, const double* x, const double* axa, const double* aya,
                          const double* aza, const double* J, const double* zp, int zf)
 {
@@ -246,7 +292,9 @@ static double adotx_cell(const og_grid* g, int i, int j, int k, const double* x,
     double y = (axa[IX(g, i + 1, j, k)] * px_hi - axa[IX(g, i, j, k)] * px_lo) * dxinv
              + (aya[IX(g, i, j + 1, k)] * py_hi - aya[IX(g, i, j, k)] * py_lo) * dyinv
              + (aza[IX(g, i, j, k + 1)] * pz_hi - aza[IX(g, i, j, k)] * pz_lo) * dzinv;
-    return y / J[IX(g, i, j, k)];
+    double v = y / J[IX(g, i, j, k)];
+    if ((zf & TP_DGROUND) && k == 0) { v += aza[IX(g, i, j, k)] * ground_flux_dir(g, i, j, x, zp) * dzinv / J[IX(g, i, j, k)]; }
+    return v;
 }
 
 /* x-, y- and z-face fluxes (ERF_TerrainPoisson_3D_K.H:22-223: -grad phi on the
@@ -405,7 +453,7 @@ void og_poisson_cross_flux(const og_grid* g, const int* bc, const double* d, con
 void og_poisson_apply(const og_grid* g, const int* bc, const double* AX, const double* AY, const double* AZ,
                       const double* J, const double* z, double* phi, double* y)
 {
-    og_poisson_fill_ghosts(g, bc, phi, 1);
+    og_poisson_fill_ghosts(g, bc, phi, ground_even(bc));
     const int zf = og_poisson_zero_flux_faces(g, bc);
 #pragma omp parallel for collapse(2) schedule(static)
     for (int k = 0; k < g->nz; ++k) {
@@ -420,7 +468,7 @@ void og_poisson_apply(const og_grid* g, const int* bc, const double* AX, const d
 void og_poisson_fluxes(const og_grid* g, const int* bc, const double* z, double* phi, const double* bx,
                        const double* by, const double* bz, double* fx, double* fy, double* fz)
 {
-    og_poisson_fill_ghosts(g, bc, phi, 1);
+    og_poisson_fill_ghosts(g, bc, phi, ground_even(bc));
     const int zf = og_poisson_zero_flux_faces(g, bc);
     for (int k = 0; k < g->nz; ++k) {
         for (int j = 0; j < g->ny; ++j) {
@@ -701,6 +749,14 @@ void og_line_tridiag(const og_grid* g, const int* bc, int zf, const double* AX, 
     const double wh = mzh * AZ[IX(g, i, j, k + 1)] * hzi_hi * dzinv;
     const double wl = mzl * AZ[IX(g, i, j, k)] * hzi_lo * dzinv;
     C -= wh + wl;
+    if (k == 0 && (zf & TP_DGROUND)) {
+        /* the ground face's principal part (phi = 0 on it): one-sided */
+        const double hzi_g = 8.0 / ((zp[IX(g, i, j, 1)] + zp[IX(g, i + 1, j, 1)] + zp[IX(g, i, j + 1, 1)]
+                                     + zp[IX(g, i + 1, j + 1, 1)])
+                                    - (zp[IX(g, i, j, 0)] + zp[IX(g, i + 1, j, 0)] + zp[IX(g, i, j + 1, 0)]
+                                       + zp[IX(g, i + 1, j + 1, 0)]));
+        C -= AZ[IX(g, i, j, 0)] * hzi_g * dzinv;
+    }
     U = wh;
     D = wl;
     if (k == g->nz - 1) {
@@ -725,7 +781,7 @@ static void mg_smooth(og_mg* mg, og_level* L)
     const int zf = og_poisson_zero_flux_faces(g, mg->bc);
     const int nz = g->nz;
     for (int color = 0; color < 2; ++color) {
-        og_poisson_fill_ghosts(g, mg->bc, L->x, 1);
+        og_poisson_fill_ghosts(g, mg->bc, L->x, ground_even(mg->bc));
 #pragma omp parallel for collapse(2) schedule(static)
         for (int j = 0; j < g->ny; ++j) {
             for (int i = 0; i < g->nx; ++i) {
@@ -762,7 +818,7 @@ static void mg_smooth(og_mg* mg, og_level* L)
 static void mg_residual(og_mg* mg, og_level* L)
 {
     const og_grid* g = &L->g;
-    og_poisson_fill_ghosts(g, mg->bc, L->x, 1);
+    og_poisson_fill_ghosts(g, mg->bc, L->x, ground_even(mg->bc));
     const int zf = og_poisson_zero_flux_faces(g, mg->bc);
 #pragma omp parallel for collapse(2) schedule(static)
     for (int k = 0; k < g->nz; ++k) {
@@ -799,7 +855,7 @@ static void mg_prolong_add(og_mg* mg, og_level* C, og_level* F)
 {
     const og_grid* fg = &F->g;
     const og_grid* cg = &C->g;
-    og_poisson_fill_ghosts(cg, mg->bc, C->x, 1);
+    og_poisson_fill_ghosts(cg, mg->bc, C->x, ground_even(mg->bc));
     for (int k = 0; k < fg->nz; ++k) {
         for (int j = 0; j < fg->ny; ++j) {
             for (int i = 0; i < fg->nx; ++i) {

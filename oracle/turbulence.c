@@ -9,10 +9,14 @@
  *   (ground fluxes, wall k), :503-569 (the first cells' implicit rows);
  *   Source/StabilityFunctions.H (Businger-Dyer psi_m, phi_m, phi_h);
  *   Source/BoundaryConditions.cpp:549-593 (the wall law's ground gradient)
- *   and :614-648 (its ghost columns).
+ *   and :614-648 (its ghost columns);
+ *   Source/WallDistance.cpp:13-62 and Source/Sequencing.cpp:43-60 (Tucker's
+ *   wall distance from the Poisson solution, and its ghosts).
  * Only tests/, the smoke check and the benchmark's CPU legs use it.
  */
 #include <float.h>
+#include <math.h>
+#include <string.h>
 
 #include "og.h"
 
@@ -200,6 +204,74 @@ static double column_z0(const og_grid* g, const gb_bc* bc, const double* z0map, 
 static const double* g_nut_prev = NULL;
 void og_set_nut_history(const double* prev) { g_nut_prev = prev; }
 
+/* The closure's wall distance (ResidualInputs::wall_distance,
+ * Source/Residual.H:61-128): an array the Python side sets from the case
+ * (the Tucker distance of turb.wall_distance = tucker), or NULL: the
+ * height above the ground (turb.wall_distance = terrain_height). */
+static const double* g_wall_dist = NULL;
+void og_set_wall_distance(const double* d) { g_wall_dist = d; }
+
+/* distance_from_phi (Source/WallDistance.cpp:13-62): Tucker's
+ * d = -|grad phi| + sqrt(|grad phi|^2 + 2 phi) on the valid cells, with
+ * ERF's cell-centred physical gradient (centred differences, the cell-centre
+ * metrics) and, in the first cell, the quadratic through phi = 0 on the
+ * ground and the two lowest cell centres; phi's ghosts filled for the
+ * Tucker conditions. Then extend_by_zero_gradient (Source/Sequencing.cpp:
+ * 43-60): every ghost takes the value of the valid cell its periodic image
+ * or, across a non-periodic face, the nearest one. */
+void og_tucker_distance(const og_grid* g, const double* z, const double* p, double* d)
+{
+    const double dxinv = 1.0 / g->dx, dyinv = 1.0 / g->dy, dzinv = 1.0 / g->dzeta;
+#define P(a, b, c) p[IX(g, a, b, c)]
+#define ZN(a, b, c) z[IX(g, a, b, c)]
+    for (int k = 0; k < g->nz; ++k) {
+        for (int j = 0; j < g->ny; ++j) {
+            for (int i = 0; i < g->nx; ++i) {
+                const double dpdxi = 0.5 * (P(i + 1, j, k) - P(i - 1, j, k)) * dxinv;
+                const double dpdeta = 0.5 * (P(i, j + 1, k) - P(i, j - 1, k)) * dyinv;
+                const double dpdzeta = 0.5 * (P(i, j, k + 1) - P(i, j, k - 1)) * dzinv;
+                const double h_zeta = 0.25 * dzinv * (ZN(i + 1, j, k + 1) + ZN(i + 1, j + 1, k + 1) + ZN(i, j, k + 1)
+                                                      + ZN(i, j + 1, k + 1) - ZN(i + 1, j, k) - ZN(i + 1, j + 1, k)
+                                                      - ZN(i, j, k) - ZN(i, j + 1, k));
+                const double h_xi = 0.25 * dxinv * (ZN(i + 1, j, k) + ZN(i + 1, j + 1, k) + ZN(i + 1, j, k + 1)
+                                                    + ZN(i + 1, j + 1, k + 1) - ZN(i, j, k) - ZN(i, j + 1, k)
+                                                    - ZN(i, j, k + 1) - ZN(i, j + 1, k + 1));
+                const double h_eta = 0.25 * dyinv * (ZN(i, j + 1, k) + ZN(i + 1, j + 1, k) + ZN(i, j + 1, k + 1)
+                                                     + ZN(i + 1, j + 1, k + 1) - ZN(i, j, k) - ZN(i + 1, j, k)
+                                                     - ZN(i, j, k + 1) - ZN(i + 1, j, k + 1));
+                double dpdz = dpdzeta / h_zeta;
+                if (k == 0) {
+                    const double zw = 0.25 * (ZN(i, j, 0) + ZN(i + 1, j, 0) + ZN(i, j + 1, 0) + ZN(i + 1, j + 1, 0));
+                    const double c1 = 0.25 * (ZN(i, j, 1) + ZN(i + 1, j, 1) + ZN(i, j + 1, 1) + ZN(i + 1, j + 1, 1));
+                    const double c2 = 0.25 * (ZN(i, j, 2) + ZN(i + 1, j, 2) + ZN(i, j + 1, 2) + ZN(i + 1, j + 1, 2));
+                    const double a = 0.5 * (zw + c1) - zw;
+                    const double b = 0.5 * (c1 + c2) - zw;
+                    dpdz = (P(i, j, 0) * b * (b - 2.0 * a) + P(i, j, 1) * a * a) / (a * b * (b - a));
+                }
+                const double dpdx = dpdxi - h_xi * dpdz;
+                const double dpdy = dpdeta - h_eta * dpdz;
+                const double g2 = dpdx * dpdx + dpdy * dpdy + dpdz * dpdz;
+                d[IX(g, i, j, k)] = -sqrt(g2) + sqrt(g2 + 2.0 * P(i, j, k));
+            }
+        }
+    }
+#undef P
+#undef ZN
+    const int ng = g->ng;
+    for (int k = -ng; k <= g->nz + ng; ++k) {
+        for (int j = -ng; j <= g->ny + ng; ++j) {
+            for (int i = -ng; i <= g->nx + ng; ++i) {
+                if (i >= 0 && i < g->nx && j >= 0 && j < g->ny && k >= 0 && k < g->nz) { continue; }
+                int ii = i, jj = j;
+                if (g->periodic_x) { ii = ((i % g->nx) + g->nx) % g->nx; } else { ii = i < 0 ? 0 : (i >= g->nx ? g->nx - 1 : i); }
+                if (g->periodic_y) { jj = ((j % g->ny) + g->ny) % g->ny; } else { jj = j < 0 ? 0 : (j >= g->ny ? g->ny - 1 : j); }
+                const int kk = k < 0 ? 0 : (k >= g->nz ? g->nz - 1 : k);
+                d[IX(g, i, j, k)] = d[IX(g, ii, jj, kk)];
+            }
+        }
+    }
+}
+
 void og_closure_evaluate(const og_grid* g, const gb_bc* bc, const gb_physics* ph, const double* u, const double* v,
                          const double* w, const double* th, const double* tk, const double* z, const double* z0map,
                          double** out)
@@ -209,7 +281,11 @@ void og_closure_evaluate(const og_grid* g, const gb_bc* bc, const gb_physics* ph
     double* dist = (double*)calloc(vol, sizeof(double));
     double* N2 = (double*)calloc(vol, sizeof(double));
     double* S2 = (double*)calloc(vol, sizeof(double));
-    og_height_above_ground(g, z, dist);
+    if (g_wall_dist != NULL) {
+        memcpy(dist, g_wall_dist, sizeof(double) * vol);
+    } else {
+        og_height_above_ground(g, z, dist);
+    }
     og_stratification_and_strain(g, ph, u, v, w, th, z, N2, S2);
     const double nu_mol = ph->turb_nu_molecular, alpha_mol = ph->turb_alpha_molecular;
     const double inv_sigma = 1 / ph->turb_sigma_k;

@@ -96,13 +96,15 @@ def test_gpu_zline_jacobi_matches_oracle_fp64(ctx, loc, case, sweeps):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("variant,segment,first", [(4, 0, 0), (5, 4, 0), (5, 8, 0), (6, 8, 0), (5, 8, 2), (6, 4, 2)],
-                         ids=["factored", "segmented4", "segmented8", "split8", "hybrid8", "hybrid-split4"])
+@pytest.mark.parametrize("variant,segment,first", [(4, 0, 0), (5, 4, 0), (5, 5, 0), (5, 8, 0), (6, 8, 0), (6, 5, 0),
+                                                    (5, 8, 2), (6, 4, 2)],
+                         ids=["factored", "segmented4", "segmented5", "segmented8", "split8", "split5", "hybrid8",
+                              "hybrid-split4"])
 @pytest.mark.parametrize("loc", LOCS)
 @pytest.mark.parametrize("case", [(37, 29, 17, True, False), (64, 48, 65, False, True), (33, 20, 128, True, True)])
 def test_gpu_zline_jacobi_kernels_match_oracle(ctx, variant, segment, first, loc, case):
     """The sequential factored sweep (GB_TUNE_LINE_VARIANT 4), the segmented
-    one with 4 or 8 levels per warp (5, the default), the segmented one
+    one with 4, 5 or 8 levels per warp (5, the default), the segmented one
     with the later sweeps split into the fold and the column solves (6),
     and either segmented form after a first sweep (the factorisation) by the
     factored kernel (GB_TUNE_LINE_FIRST 2) agree with the oracle's column
