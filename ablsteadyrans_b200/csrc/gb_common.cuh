@@ -107,6 +107,12 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
+//! 1 / v rounded to nearest, the value IEEE division 1 / v gives, by the
+//! reciprocal intrinsic (which skips the general quotient's numerator
+//! handling).
+__device__ __forceinline__ double recip_rn(double v) { return __drcp_rn(v); }
+__device__ __forceinline__ float recip_rn(float v) { return __frcp_rn(v); }
+
 // ------------------------------------------- programmatic dependent launch ---
 //
 // A kernel launched by launch_pdl may begin while the kernel before it on the

@@ -300,7 +300,7 @@ __device__ __forceinline__ void zline_fact_body(const LineArgs<T>& a, T* __restr
             T inv, c;
             if (FIRST) {
                 const T m = (k == 0) ? s[nthr] : s[nthr] - lower * cprev;
-                inv = T(1) / m;
+                inv = recip_rn(m);
                 c = -s[3 * nthr] * inv;
                 const int64_t o = o0 + static_cast<int64_t>(k) * g.sz;
                 im_out[o] = inv;
@@ -544,9 +544,14 @@ __device__ __forceinline__ void zline_seg_body(const LineArgs<T>& a, T* __restri
                 p01 = n01;
                 p10 = n10;
                 p11 = n11;
-                seg_pow2_normalise(p00, p01, p10, p11);
+                if (sizeof(T) == 4) { seg_pow2_normalise(p00, p01, p10, p11); }
             }
         }
+        // Scaling by a power of two is exact, so the map normalised once per
+        // segment is the per-level normalised one times a power of two, and
+        // c' (its ratio) is bit for bit the same; FP64's range holds L levels'
+        // products of the coefficients, FP32's normalises every level.
+        if (sizeof(T) == 8) { seg_pow2_normalise(p00, p01, p10, p11); }
         carry_c[me] = p00;
         carry_c[cs + me] = p01;
         carry_c[2 * cs + me] = p10;
@@ -560,8 +565,12 @@ __device__ __forceinline__ void zline_seg_body(const LineArgs<T>& a, T* __restri
             const T d2 = carry_c[2 * cs + m] * num + carry_c[3 * cs + m] * den;
             num = n2;
             den = d2;
-            T z0 = T(0), z1 = T(0);
-            seg_pow2_normalise(num, den, z0, z1);
+            // (an exact common power of two: every 4th segment in FP64, whose
+            // range holds 4 normalised maps' growth; c' = num / den unchanged)
+            if (sizeof(T) == 4 || (s & 3) == 3) {
+                T z0 = T(0), z1 = T(0);
+                seg_pow2_normalise(num, den, z0, z1);
+            }
         }
         T cprev = (w == 0) ? T(0) : num / den;
         // the sequential factorisation over the segment (zline_fact_body's order)
@@ -571,7 +580,7 @@ __device__ __forceinline__ void zline_seg_body(const LineArgs<T>& a, T* __restri
             if (k < nk) {
                 const T lower = -lo[q];
                 const T m = (k == 0) ? dg[q] : dg[q] - lower * cprev;
-                const T inv = T(1) / m;
+                const T inv = recip_rn(m);
                 const T c = -up[q] * inv;
                 dg[q] = inv;
                 up[q] = c;
