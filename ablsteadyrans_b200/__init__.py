@@ -77,6 +77,8 @@ def _declare(L):
     L.gb_zline_jacobi_f32.argtypes = [P, G, i32, P, P, P, i32, P, ctypes.POINTER(ctypes.c_float)]
     L.gb_zline_jacobi_noalloc.argtypes = [G, i32, P, P, P, i32, P, ctypes.POINTER(f64), P]
     L.gb_zline_lusgs.argtypes = [P, G, i32, P, P, P, i32, i32, P, ctypes.POINTER(f64)]
+    L.gb_zline_jacobi_batch.argtypes = [P, i32, P, i32, P]
+    L.gb_zline_jacobi_batch_f32.argtypes = [P, i32, P, i32, P]
 
 
 def check(status):
@@ -169,6 +171,36 @@ def zline_jacobi(ctx, grid, loc, A, ap, rhs, sweeps, delta):
         check(L.gb_zline_jacobi_f32(ctx.handle, ctypes.byref(grid.c), loc, _ptr(A), _ptr(ap), _ptr(rhs), sweeps,
                                     _ptr(delta), ctypes.byref(out)))
     return float(out.value)
+
+
+def zline_jacobi_batch(ctx, systems, sweeps, want_change=True):
+    """gust::zline_jacobi over many systems of different grids at once
+    (gb_zline_jacobi_batch): systems is a list of (grid, loc, A, ap, rhs,
+    delta), all FP64 or all FP32; every delta gets the values
+    gb_zline_jacobi gives its system alone. Returns the list of each
+    system's max |change of the last sweep| (None when want_change is
+    false: nothing waits for the stream)."""
+    import torch
+    from .abi import LineSystem
+    n = len(systems)
+    arr = (LineSystem * n)()
+    f64 = None
+    for q, (grid, loc, A, ap, rhs, delta) in enumerate(systems):
+        is64 = A.dtype == torch.float64
+        if f64 is None:
+            f64 = is64
+        elif f64 != is64:
+            raise ValueError("zline_jacobi_batch: the systems mix FP64 and FP32")
+        arr[q].grid = grid.c
+        arr[q].loc = int(loc)
+        arr[q].A = A.data_ptr()
+        arr[q].ap = ap.data_ptr()
+        arr[q].rhs = rhs.data_ptr()
+        arr[q].delta = delta.data_ptr()
+    out = (ctypes.c_double * n)() if want_change else None
+    fn = lib().gb_zline_jacobi_batch if f64 else lib().gb_zline_jacobi_batch_f32
+    check(fn(ctx.handle, n, arr, int(sweeps), out))
+    return [float(v) for v in out] if want_change else None
 
 
 def probe_fp64(ctx, iters, sink):

@@ -14,6 +14,12 @@ LIMITER_VAN_LEER, LIMITER_VAN_ALBADA, LIMITER_UPWIND = range(3)
 MAX_PROFILE = 32
 
 
+class LineSystem(ctypes.Structure):
+    """gb_line_system / gb_line_system_f32 (the same layout: pointers by address)."""
+    _fields_ = [("grid", GbGrid), ("loc", ctypes.c_int32), ("A", ctypes.c_void_p), ("ap", ctypes.c_void_p),
+                ("rhs", ctypes.c_void_p), ("delta", ctypes.c_void_p)]
+
+
 class PoissonOptions(ctypes.Structure):
     """gb_poisson_opts: the solver.poisson_* inputs plus the multigrid settings."""
     _fields_ = [("reltol", ctypes.c_double), ("abstol", ctypes.c_double), ("max_iter", ctypes.c_int32),

@@ -130,3 +130,49 @@ class Autotuner:
         self.save()
         self.apply(stage.ctx, choice)
         return choice, timings
+
+
+#: Candidate levels per warp of the batched z-line sweep (GB_TUNE_LINE_SEGMENT).
+SWEEP_SEGMENTS = (0, 4, 8)
+
+
+def sweep_key(systems, sweeps):
+    """The cache key of a batched sweep: each system's extents at its
+    location, the precision and the sweep count."""
+    shapes = sorted(tuple(g.extents(loc)) for (g, loc, *_rest) in systems)
+    word = systems[0][2].element_size() if systems else 8
+    return f"batch-sweep:{word}:{sweeps}:" + ",".join(f"{a}x{b}x{c}" for a, b, c in shapes)
+
+
+def tune_batch_sweep(tuner, ctx, systems, sweeps, reps=2):
+    """The levels per warp of the batched z-line sweep (gb_zline_jacobi_batch)
+    over `systems`: each candidate of SWEEP_SEGMENTS timed on the systems
+    themselves (the sweep only writes its deltas, so timing changes no
+    input), the fastest applied to ctx and cached in `tuner` by sweep_key.
+    Returns (segment, {segment: ms} or None when cached)."""
+    import torch
+
+    import ablsteadyrans_b200 as gb
+    key = sweep_key(systems, sweeps)
+    if key in tuner.cache:
+        seg = tuner.cache[key]["choice"]["LINE_SEGMENT"]
+        ctx.tune(gb.TUNE_LINE_SEGMENT, seg)
+        return seg, None
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    timings = []
+    for seg in SWEEP_SEGMENTS:
+        ctx.tune(gb.TUNE_LINE_SEGMENT, seg)
+        gb.zline_jacobi_batch(ctx, systems, sweeps)        # untimed: the scratch at its size
+        torch.cuda.synchronize()
+        e0.record(ctx.stream)
+        for _ in range(reps):
+            gb.zline_jacobi_batch(ctx, systems, sweeps, want_change=False)
+        e1.record(ctx.stream)
+        torch.cuda.synchronize()
+        timings.append(({"LINE_SEGMENT": seg}, e0.elapsed_time(e1) / reps))
+    choice = best(timings)
+    tuner.cache[key] = {"choice": choice, "ms": {str(c["LINE_SEGMENT"]): ms for c, ms in timings}}
+    tuner.save()
+    ctx.tune(gb.TUNE_LINE_SEGMENT, choice["LINE_SEGMENT"])
+    return choice["LINE_SEGMENT"], {c["LINE_SEGMENT"]: ms for c, ms in timings}

@@ -15,7 +15,9 @@
 
 #include <algorithm>
 #include <atomic>
+#include <cstring>
 #include <mutex>
+#include <vector>
 
 namespace gb {
 
@@ -459,7 +461,8 @@ __device__ __forceinline__ void seg_pow2_normalise(T& a, T& b, T& c, T& d)
 }
 
 template <typename T, bool FIRST, int L, bool PREF = false>
-__device__ __forceinline__ void zline_seg_body(const LineArgs<T>& a, T* __restrict__ inv_io, T* __restrict__ cp_io)
+__device__ __forceinline__ void zline_seg_body(const LineArgs<T>& a, T* __restrict__ inv_io, T* __restrict__ cp_io,
+                                               int cblock)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x;
@@ -467,7 +470,7 @@ __device__ __forceinline__ void zline_seg_body(const LineArgs<T>& a, T* __restri
     const int W = blockDim.y;
     // 32 consecutive columns in (j, i) order: a block is never mostly past
     // the end of a row (a face system's rows are one column longer than 32 k)
-    const int c = blockIdx.x * 32 + lane;
+    const int c = cblock * 32 + lane;
     const int i = c % a.ni;
     const int j = c / a.ni;
     const bool col = c < a.ni * a.nj;
@@ -682,7 +685,7 @@ __device__ __forceinline__ void zline_seg_body(const LineArgs<T>& a, T* __restri
 template <typename T, bool FIRST, int L>
 __global__ void __launch_bounds__(512) zline_seg_kernel(LineArgs<T> a, T* __restrict__ inv_io, T* __restrict__ cp_io)
 {
-    zline_seg_body<T, FIRST, L>(a, inv_io, cp_io);
+    zline_seg_body<T, FIRST, L>(a, inv_io, cp_io, blockIdx.x);
 }
 
 //! The split sweep's first half: the right-hand side with the lagged lateral
@@ -726,9 +729,9 @@ template <typename T, int L>
 __global__ void __launch_bounds__(512) zline_seg_pref_multi_kernel(MultiLineArgs<T> m)
 {
     switch (blockIdx.z) {
-    case 0: zline_seg_body<T, false, L, true>(m.a[0], m.inv[0], m.cp[0]); break;
-    case 1: zline_seg_body<T, false, L, true>(m.a[1], m.inv[1], m.cp[1]); break;
-    default: zline_seg_body<T, false, L, true>(m.a[2], m.inv[2], m.cp[2]); break;
+    case 0: zline_seg_body<T, false, L, true>(m.a[0], m.inv[0], m.cp[0], blockIdx.x); break;
+    case 1: zline_seg_body<T, false, L, true>(m.a[1], m.inv[1], m.cp[1], blockIdx.x); break;
+    default: zline_seg_body<T, false, L, true>(m.a[2], m.inv[2], m.cp[2], blockIdx.x); break;
     }
 }
 
@@ -755,9 +758,9 @@ __global__ void __maxnreg__(seg_reg_cap(L)) zline_seg_multi_kernel(MultiLineArgs
 {
     pdl_entry();
     switch (blockIdx.z) {
-    case 0: zline_seg_body<T, FIRST, L>(m.a[0], m.inv[0], m.cp[0]); break;
-    case 1: zline_seg_body<T, FIRST, L>(m.a[1], m.inv[1], m.cp[1]); break;
-    default: zline_seg_body<T, FIRST, L>(m.a[2], m.inv[2], m.cp[2]); break;
+    case 0: zline_seg_body<T, FIRST, L>(m.a[0], m.inv[0], m.cp[0], blockIdx.x); break;
+    case 1: zline_seg_body<T, FIRST, L>(m.a[1], m.inv[1], m.cp[1], blockIdx.x); break;
+    default: zline_seg_body<T, FIRST, L>(m.a[2], m.inv[2], m.cp[2], blockIdx.x); break;
     }
 }
 
@@ -1183,6 +1186,223 @@ gb_status zline_sweeps_multi(gb_ctx* ctx, const gb_grid& g, int n, const int* lo
     return check_cuda("zline_sweeps_multi");
 }
 
+// ---- Sweeps of many uneven systems in one launch per sweep ----------------
+//
+// The batched form of the segmented sweep: systems of different grids (the
+// tiles of a batch, each with its own nx, ny, nz and location) are swept
+// together. The host lays out one column work-list for all of them: an entry
+// per 32-column block of a system, (system, block within the system). Each
+// launch is persistent: at most the blocks the SMs hold at once, each walking
+// the list with a stride of the grid size and running the segmented sweep's
+// body on the entry's columns. Systems whose columns need the same number of
+// warps share a launch (a block's warps are its segments; the warps above a
+// column's top are identity maps, so a block taller than a column gives the
+// same values bit for bit, but wastes its slots).
+
+template <typename T>
+struct BatchLineSys {
+    LineArgs<T> a;               // sweep-independent fields (dold, dnew, first, change set per sweep)
+    T* buf[2];                   // delta, its ping-pong partner
+    T* inv;                      // 1/m of the first sweep's factorisation
+    T* cp;                       // c'
+    unsigned long long* change;  // this system's max |change| word (null: not wanted)
+};
+
+//! Systems one batched launch takes: their descriptors travel in the launch's
+//! parameter block (the constant bank, read as instruction operands like a
+//! single system's arguments, not loaded into registers), 26 KB of the 32 KB
+//! a launch may carry.
+constexpr int kBatchLaunchSystems = 120;
+
+template <typename T>
+struct BatchLineParams {
+    BatchLineSys<T> sys[kBatchLaunchSystems];
+    //! The work-list: entry e is column block e - first_block[s] of the system
+    //! s with first_block[s] <= e < first_block[s + 1].
+    int first_block[kBatchLaunchSystems + 1];
+    int nsys;
+};
+
+//! The batched sweep's register cap: the segmented sweep's, but 72 at L = 5
+//! (the descriptors' fields taken from the constant bank by a runtime index
+//! need registers the single-system kernel folds into its instructions; 64
+//! spills). Two blocks of up to 14 warps still share an SM (7 warps x 32
+//! lanes x 72 within a scheduler's 16 K registers).
+constexpr int batch_reg_cap(int L)
+{
+    return L == 5 ? 72 : seg_reg_cap(L);
+}
+
+//! The batched sweep's warps a block at most (its registers within the SM's 64 K).
+constexpr int batch_max_warps(int L)
+{
+    return (65536 / (32 * batch_reg_cap(L)) < 32) ? 65536 / (32 * batch_reg_cap(L)) : 32;
+}
+
+template <typename T, bool FIRST, int L>
+__global__ void __maxnreg__(batch_reg_cap(L))
+    zline_seg_batch_kernel(const __grid_constant__ BatchLineParams<T> p, int sweep, int sweeps)
+{
+    const int items = p.first_block[p.nsys];
+    for (int it = blockIdx.x; it < items; it += gridDim.x) {
+        // the entry's system by bisection of the block offsets (values uniform
+        // over the block, so they stay out of the per-thread registers)
+        int lo = 0, hi = p.nsys - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (p.first_block[mid] <= it) {
+                lo = mid;
+            } else {
+                hi = mid - 1;
+            }
+        }
+        const BatchLineSys<T>& d = p.sys[lo];
+        LineArgs<T> a = d.a;
+        a.dold = d.buf[(sweeps - sweep) & 1];
+        a.dnew = d.buf[(sweeps - 1 - sweep) & 1];
+        a.first = FIRST ? 1 : 0;
+        a.change = (sweep == sweeps - 1) ? d.change : nullptr;
+        zline_seg_body<T, FIRST, L>(a, d.inv, d.cp, it - p.first_block[lo]);
+        // the next entry's carries reuse the shared memory
+        __syncthreads();
+    }
+}
+
+template <typename T, bool FIRST, int L>
+cudaError_t launch_seg_batch(const BatchLineParams<T>& sys, int warps, int sweep, int sweeps, cudaStream_t stream)
+{
+    auto kern = zline_seg_batch_kernel<T, FIRST, L>;
+    const size_t sm = seg_smem_bytes<T>(warps);
+    if (sm > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             static_cast<int>(seg_smem_bytes<T>(32)));
+        if (e != cudaSuccess) { return e; }
+    }
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32 * warps, sm);
+    const int resident = std::max(1, sms) * std::max(1, per_sm);
+    const int blocks = std::min(sys.first_block[sys.nsys], resident);
+    kern<<<blocks, dim3(32, warps), sm, stream>>>(sys, sweep, sweeps);
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_seg_batch_any(int L, bool first, const BatchLineParams<T>& sys, int warps, int sweep, int sweeps,
+                                 cudaStream_t stream)
+{
+    if (L == 4) {
+        return first ? launch_seg_batch<T, true, 4>(sys, warps, sweep, sweeps, stream)
+                     : launch_seg_batch<T, false, 4>(sys, warps, sweep, sweeps, stream);
+    }
+    if (L == 8) {
+        return first ? launch_seg_batch<T, true, 8>(sys, warps, sweep, sweeps, stream)
+                     : launch_seg_batch<T, false, 8>(sys, warps, sweep, sweeps, stream);
+    }
+    return first ? launch_seg_batch<T, true, 5>(sys, warps, sweep, sweeps, stream)
+                 : launch_seg_batch<T, false, 5>(sys, warps, sweep, sweeps, stream);
+}
+
+template <typename T>
+gb_status zline_sweeps_batch(gb_ctx* ctx, int n, const gb_grid* grids, const int* locs, const T* const* A,
+                             const T* const* ap, const T* const* rhs, int sweeps, T* const* delta, double* change)
+{
+    const int L = seg_levels(ctx);
+    // scratch: the ping-pong partners, 1/m and c' of every system (offsets in
+    // 256-byte units), then the change words
+    std::vector<int64_t> off(n + 1, 0);
+    std::vector<int> warps(n);
+    for (int s = 0; s < n; ++s) {
+        const int64_t vol = volume(grids[s]);
+        off[s + 1] = off[s] + ((vol * static_cast<int64_t>(sizeof(T)) + 255) / 256) * 256;
+        warps[s] = (ext_z(grids[s], locs[s]) + L - 1) / L;
+        if (warps[s] > batch_max_warps(L)) {
+            set_error("gust: zline_jacobi_batch: system %d has %d z-levels, more than the batched sweep's %d",
+                      s, ext_z(grids[s], locs[s]), batch_max_warps(L) * L);
+            return GB_BAD_ARG;
+        }
+    }
+    const size_t field_bytes = static_cast<size_t>(off[n]);
+    char* pool = static_cast<char*>(scratch(ctx, kSlotBatchBase, 3 * field_bytes + sizeof(unsigned long long) * n));
+    if (pool == nullptr) { return GB_OOM; }
+    unsigned long long* d_words = reinterpret_cast<unsigned long long*>(pool + 3 * field_bytes);
+
+    // One launch per run of systems with the same warps a block, at most
+    // kBatchLaunchSystems of them: its descriptors (indexed from 0 in the
+    // launch) and their column blocks' offsets in its work-list.
+    struct Launch {
+        int warps;
+    };
+    std::vector<Launch> launches;
+    std::vector<BatchLineParams<T>> params;
+    {
+        std::vector<int> order(n);
+        for (int s = 0; s < n; ++s) { order[s] = s; }
+        std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return warps[x] < warps[y]; });
+        for (int q = 0; q < n; ++q) {
+            const int s = order[q];
+            if (launches.empty() || launches.back().warps != warps[s] || params.back().nsys == kBatchLaunchSystems) {
+                launches.push_back(Launch{warps[s]});
+                params.emplace_back();
+                std::memset(static_cast<void*>(&params.back()), 0, sizeof(BatchLineParams<T>));
+            }
+            BatchLineParams<T>& pr = params.back();
+            const int local = pr.nsys;
+            BatchLineSys<T>& d = pr.sys[local];
+            LineArgs<T>& a = d.a;
+            a.g = grids[s];
+            a.ni = ext_x(grids[s], locs[s]);
+            a.nj = ext_y(grids[s], locs[s]);
+            a.nk = ext_z(grids[s], locs[s]);
+            a.A = A[s];
+            a.cs = volume(grids[s]);
+            a.ap = ap[s];
+            a.rhs = rhs[s];
+            d.buf[0] = delta[s];
+            d.buf[1] = reinterpret_cast<T*>(pool + off[s]);
+            d.inv = reinterpret_cast<T*>(pool + field_bytes + off[s]);
+            d.cp = reinterpret_cast<T*>(pool + 2 * field_bytes + off[s]);
+            d.change = d_words + s;
+            const int64_t blocks = (static_cast<int64_t>(a.ni) * a.nj + 31) / 32;
+            if (pr.first_block[local] + blocks > (int64_t(1) << 30)) {
+                set_error("gust: zline_jacobi_batch: more than 2^30 column blocks in one launch");
+                return GB_BAD_ARG;
+            }
+            pr.first_block[local + 1] = pr.first_block[local] + static_cast<int>(blocks);
+            pr.nsys = local + 1;
+        }
+    }
+    for (int s = 0; s < n; ++s) { cudaMemsetAsync(delta[s], 0, sizeof(T) * volume(grids[s]), ctx->stream); }
+    cudaMemsetAsync(d_words, 0, sizeof(unsigned long long) * n, ctx->stream);
+    for (int k = 0; k < sweeps; ++k) {
+        for (size_t q = 0; q < launches.size(); ++q) {
+            Span span(ctx, GB_KERNEL_LINE_SWEEP);
+            const cudaError_t e = launch_seg_batch_any<T>(L, k == 0, params[q], launches[q].warps, k, sweeps,
+                                                          ctx->stream);
+            if (e != cudaSuccess) {
+                set_error("gust: zline_jacobi_batch: launch failed: %s", cudaGetErrorString(e));
+                return GB_CUDA;
+            }
+            ++ctx->launches;
+        }
+    }
+    for (int s = 0; s < n; ++s) { seam_sync<T>(ctx, grids[s], locs[s], delta[s]); }
+    gb_status st = check_cuda("zline_jacobi_batch");
+    if (st != GB_OK || change == nullptr) { return st; }
+    std::vector<unsigned long long> w(n);
+    cudaMemcpyAsync(w.data(), d_words, sizeof(unsigned long long) * n, cudaMemcpyDeviceToHost, ctx->stream);
+    if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) { return check_cuda("zline_jacobi_batch"); }
+    for (int s = 0; s < n; ++s) { change[s] = bits_to_double(w[s]); }
+    return GB_OK;
+}
+
+template gb_status zline_sweeps_batch<double>(gb_ctx*, int, const gb_grid*, const int*, const double* const*,
+                                              const double* const*, const double* const*, int, double* const*,
+                                              double*);
+template gb_status zline_sweeps_batch<float>(gb_ctx*, int, const gb_grid*, const int*, const float* const*,
+                                             const float* const*, const float* const*, int, float* const*, double*);
+
 template gb_status zline_sweeps_multi<double>(gb_ctx*, const gb_grid&, int, const int*, const double* const*,
                                               const double* const*, const double* const*, int, double* const*,
                                               unsigned long long* const*);
@@ -1231,6 +1451,56 @@ gb_status zline_jacobi_api(gb_ctx* ctx, const gb_grid* g, int32_t loc, const T* 
     return GB_OK;
 }
 
+template <typename Sys>
+struct LineSystemOf;
+template <>
+struct LineSystemOf<double> { using type = gb_line_system; };
+template <>
+struct LineSystemOf<float> { using type = gb_line_system_f32; };
+
+template <typename T>
+gb_status zline_jacobi_batch_api(gb_ctx* ctx, int32_t n, const typename LineSystemOf<T>::type* systems,
+                                 int32_t sweeps, double* change)
+{
+    gb::clear_error();
+    const char* op = "zline_jacobi_batch";
+    if (ctx == nullptr) {
+        gb::set_error("gust: %s: ctx is null", op);
+        return GB_BAD_ARG;
+    }
+    if (n < 1 || systems == nullptr) {
+        gb::set_error("gust: zline_jacobi_batch: n must be >= 1 with a systems array (got %d)", n);
+        return GB_BAD_ARG;
+    }
+    if (sweeps < 1) {
+        gb::set_error("gust: zline_jacobi_batch: sweeps must be >= 1 (got %d)", sweeps);
+        return GB_BAD_ARG;
+    }
+    std::vector<gb_grid> grids(n);
+    std::vector<int> locs(n);
+    std::vector<const T*> A(n), ap(n), rhs(n);
+    std::vector<T*> delta(n);
+    for (int s = 0; s < n; ++s) {
+        const auto& y = systems[s];
+        gb_status st = gb::check_grid(op, &y.grid);
+        if (st != GB_OK) { return st; }
+        if ((st = gb::check_loc(op, y.loc)) != GB_OK) { return st; }
+        if (y.A == nullptr || y.ap == nullptr || y.rhs == nullptr || y.delta == nullptr) {
+            gb::set_error("gust: zline_jacobi_batch: system %d: A, ap, rhs and delta must be device arrays of its "
+                          "grid", s);
+            return GB_BAD_ARG;
+        }
+        grids[s] = y.grid;
+        locs[s] = y.loc;
+        A[s] = y.A;
+        ap[s] = y.ap;
+        rhs[s] = y.rhs;
+        delta[s] = y.delta;
+    }
+    return gb::zline_sweeps_batch<T>(ctx, n, grids.data(), locs.data(), A.data(), ap.data(), rhs.data(), sweeps,
+                                     delta.data(), change);
+}
+
 }  // namespace
 
 extern "C" {
@@ -1245,6 +1515,18 @@ gb_status gb_zline_jacobi_f32(gb_ctx* ctx, const gb_grid* g, int32_t loc, const 
                               const float* rhs, int32_t sweeps, float* delta, float* change)
 {
     return zline_jacobi_api<float>(ctx, g, loc, A, ap, rhs, sweeps, delta, change);
+}
+
+gb_status gb_zline_jacobi_batch(gb_ctx* ctx, int32_t n, const gb_line_system* systems, int32_t sweeps,
+                                double* change)
+{
+    return zline_jacobi_batch_api<double>(ctx, n, systems, sweeps, change);
+}
+
+gb_status gb_zline_jacobi_batch_f32(gb_ctx* ctx, int32_t n, const gb_line_system_f32* systems, int32_t sweeps,
+                                    double* change)
+{
+    return zline_jacobi_batch_api<float>(ctx, n, systems, sweeps, change);
 }
 
 }  // extern "C"

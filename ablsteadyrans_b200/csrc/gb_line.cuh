@@ -14,7 +14,8 @@ enum ScratchSlot : int {
     kSlotLineInv,  // 1/m of the factored sweeps
     kSlotLineCp,   // c' of the factored sweeps
     kSlotFirstFree,
-    kSlotMultiBase = 24  // 3 slots (next, 1/m, c') per system of zline_sweeps_multi
+    kSlotMultiBase = 24,  // 3 slots (next, 1/m, c') per system of zline_sweeps_multi
+    kSlotBatchBase = 48   // zline_sweeps_batch: its systems' fields, then its descriptors
 };
 
 enum class LineScratch { automatic, pipelined, shared, global, factored, segmented };
@@ -33,6 +34,16 @@ template <typename T>
 gb_status zline_sweeps_multi(gb_ctx* ctx, const gb_grid& g, int n, const int* locs, const T* const* A,
                              const T* const* ap, const T* const* rhs, int sweeps, T* const* delta,
                              unsigned long long* const* change_words);
+
+//! zline_sweeps for n systems of different grids (each at its own location,
+//! each into its own delta, which this sets to 0) by the segmented sweep over
+//! one column work-list: one launch per sweep for each number of warps a
+//! block the systems' columns need. change (host, n entries, may be null)
+//! receives each system's max |change over the last sweep|, after a wait for
+//! the stream; with change null nothing waits.
+template <typename T>
+gb_status zline_sweeps_batch(gb_ctx* ctx, int n, const gb_grid* grids, const int* locs, const T* const* A,
+                             const T* const* ap, const T* const* rhs, int sweeps, T* const* delta, double* change);
 
 //! The line LU-SGS passes (gb_zline_lusgs) into delta (0 on entry, ghosts
 //! included); change_word as for zline_sweeps. FP64.

@@ -159,24 +159,16 @@ def sequential_latencies(arrivals, services):
     return out
 
 
-def serve_vs_sequential(count=12, rate=2.0, seed=0, sizes=None, layers=None, max_iterations=1500, budget=150e9):
-    """The served form against the plain FP64 sequential path on the same
-    requests: (1) the server (continuous batching, FP32 inner solves),
-    latencies from arrival to completion; (2) the requests in plain FP64
-    served one at a time in arrival order: each one's service time measured
-    alone (the initializer, then the C++ driver to the criterion or the cap),
-    its latency from the FIFO queue over the same arrivals. Returns a dict of
-    p50/p99 latency and solves/s of each."""
+def sequential_services(count, seed=0, sizes=None, layers=None, max_iterations=1500):
+    """The plain FP64 sequential path's service time of each request (the
+    same tiles and kinds as requests_config4 at any rate: the arrival draws
+    do not move the tile draws), each one alone: the initializer, then the
+    C++ driver to the criterion or the cap. Returns (services, statuses)."""
     import torch
 
     from .batch import Member
     from .simplec import run_drivers
-    model = calibrate_footprint()
-    served = requests_config4(count, rate, seed, precision=1, sizes=sizes, layers=layers)
-    srv = Server(budget, model, max_iterations=max_iterations)
-    wall = srv.run(served)
-    lat = np.array([r.latency for r in served])
-    seq = requests_config4(count, rate, seed, precision=0, sizes=sizes, layers=layers)
+    seq = requests_config4(count, 1.0, seed, precision=0, sizes=sizes, layers=layers)
     services = []
     for req in seq:
         torch.cuda.synchronize()
@@ -190,20 +182,46 @@ def serve_vs_sequential(count=12, rate=2.0, seed=0, sizes=None, layers=None, max
         m.close()
         del m
         torch.cuda.empty_cache()
-    slat = np.array(sequential_latencies([r.arrival for r in seq], services))
-    makespan = max(r.arrival + l for r, l in zip(seq, slat))
-    return {
-        "requests": count, "rate_per_s": rate, "full_solves": sum(1 for r in served if r.kind == "rans"),
-        "served_fp32_inner": {"p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
-                              "solves_per_s": count / wall, "wall_s": wall,
-                              "steady": sum(1 for r in served if r.status == "steady"),
-                              "capped": sum(1 for r in served if r.kind == "rans" and r.status == "running"),
-                              "peak_concurrent": srv.peak_active},
-        "sequential_fp64": {"p50_s": float(np.percentile(slat, 50)), "p99_s": float(np.percentile(slat, 99)),
-                            "solves_per_s": count / makespan, "makespan_s": makespan,
-                            "service_s_total": float(sum(services)),
-                            "steady": sum(1 for r in seq if r.status == "steady")},
-    }
+    return services, [r.status for r in seq]
+
+
+def serve_sweep(rates, count=12, seed=0, sizes=None, layers=None, max_iterations=1500, budget=150e9):
+    """The served form against the plain FP64 sequential path on the same
+    requests, at each arrival rate of `rates`: (1) the server (continuous
+    batching, FP32 inner solves), latencies from arrival to completion;
+    (2) the requests in plain FP64 served one at a time in arrival order:
+    each one's service time measured alone once (sequential_services), its
+    latency from the FIFO queue over that rate's arrivals. Returns one dict
+    per rate with p50/p99 latency and solves/s of each form."""
+    model = calibrate_footprint()
+    services, statuses = sequential_services(count, seed, sizes, layers, max_iterations)
+    out = []
+    for rate in rates:
+        served = requests_config4(count, rate, seed, precision=1, sizes=sizes, layers=layers)
+        srv = Server(budget, model, max_iterations=max_iterations)
+        wall = srv.run(served)
+        lat = np.array([r.latency for r in served])
+        arrivals = [r.arrival for r in served]
+        slat = np.array(sequential_latencies(arrivals, services))
+        makespan = max(a + l for a, l in zip(arrivals, slat))
+        out.append({
+            "requests": count, "rate_per_s": rate, "full_solves": sum(1 for r in served if r.kind == "rans"),
+            "served_fp32_inner": {"p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+                                  "solves_per_s": count / wall, "wall_s": wall,
+                                  "steady": sum(1 for r in served if r.status == "steady"),
+                                  "capped": sum(1 for r in served if r.kind == "rans" and r.status == "running"),
+                                  "peak_concurrent": srv.peak_active},
+            "sequential_fp64": {"p50_s": float(np.percentile(slat, 50)), "p99_s": float(np.percentile(slat, 99)),
+                                "solves_per_s": count / makespan, "makespan_s": makespan,
+                                "service_s_total": float(sum(services)),
+                                "steady": sum(1 for st in statuses if st == "steady")},
+        })
+    return out
+
+
+def serve_vs_sequential(count=12, rate=2.0, seed=0, sizes=None, layers=None, max_iterations=1500, budget=150e9):
+    """serve_sweep at one rate."""
+    return serve_sweep([rate], count, seed, sizes, layers, max_iterations, budget)[0]
 
 
 def measure_peak_bytes(n, nz):

@@ -463,7 +463,8 @@ def steady_solves(max_iterations=3000, config=1):
     capped at 1) from the mass-consistent initial field to the steady
     criterion (the C++ driver), in plain FP64 and with FP32 inner solves:
     iterations, device seconds, steady solves/s, and the difference of the
-    two steady states per field (max |mixed - FP64| / max |FP64|)."""
+    two steady states per field (max |mixed - FP64| / max |FP64|) and of
+    the velocity vector in the 2-norm."""
     import torch
 
     import ablsteadyrans_b200 as gb
@@ -511,6 +512,16 @@ def steady_solves(max_iterations=3000, config=1):
         scale = float(np.abs(b[vv]).max())
         err[f] = float(np.abs(a[vv] - b[vv]).max()) / (scale if scale > 0 else 1.0)
     res["fp32_inner_vs_fp64_rel_err"] = err
+    # the velocity vector's relative error in the 2-norm over all valid points
+    # (u, v and w at their faces): ||mixed - FP64|| / ||FP64||
+    num = den = 0.0
+    for f in ("u", "v", "w"):
+        a, loc = fields["fp32_inner"][f]
+        b, _ = fields["fp64"][f]
+        vv = g.valid(loc)
+        num += float(np.sum((a[vv] - b[vv]) ** 2))
+        den += float(np.sum(b[vv] ** 2))
+    res["fp32_inner_vs_fp64_velocity_rel_l2"] = (num / den) ** 0.5 if den > 0 else None
     res["speedup_fp32_inner"] = res["fp64"]["seconds"] / res["fp32_inner"]["seconds"]
     if config == 1:
         res["workload"] = ("config 1 (128x128x64 hill) from the mass-consistent initial field to the steady criterion "
@@ -561,18 +572,117 @@ def batched_leg(count=16, iterations=10, warmup=2):
     return out
 
 
-def served_leg():
-    """A bounded sample of the served configuration: 12 requests at 2 per
-    second, tiles drawn as config 3 with n in {64, 96} and nz in {48, 64},
-    70 % mass-consistent only and 30 % full solves (capped at 1500
-    iterations); served with continuous batching and FP32 inner solves
-    against plain FP64 served one at a time over the same arrivals."""
-    from ablsteadyrans_b200.serve import serve_vs_sequential
-    out = serve_vs_sequential(count=12, rate=2.0, sizes=(64, 96), layers=(48, 64), max_iterations=1500)
-    out["speedup_solves_per_s"] = out["served_fp32_inner"]["solves_per_s"] / out["sequential_fp64"]["solves_per_s"]
-    out["workload"] = ("12 requests, Poisson arrivals at 2/s, tiles drawn as config 3 with n in {64, 96}, nz in "
-                       "{48, 64} (a bounded sample), 70 % mass-consistent only, 30 % full solves capped at 1500 "
-                       "iterations")
+def batched_sweep_leg(count=48, sweeps=4, reps=3, tune=True):
+    """The z-line sweeps of config 3's uneven tiles in one work-list (the
+    batched solve, gb_zline_jacobi_batch: one persistent launch per sweep
+    and column-height group) against the same systems one call each
+    (gb_zline_jacobi, each call reading its system's max |change| back, as
+    the batched call reads all of them once) on one stream: the u, v and w
+    systems of each of the
+    `count` tiles (n x n x nz drawn as config 3), seeded diagonally dominant
+    coefficients, `sweeps` sweeps, FP64 and FP32, both forms at the levels
+    per warp the autotuner picks for the batch (tune false: the default 5);
+    device time per pass, the
+    best of `reps` after one untimed pass, and the batched launches' HBM
+    rate on the sweep's algorithmic bytes (5 words a point in the first
+    sweep, 10 in each later one)."""
+    import torch
+
+    import ablsteadyrans_b200 as gb
+    from ablsteadyrans_b200.autotune import Autotuner, tune_batch_sweep
+    from ablsteadyrans_b200.batch import CONFIG3_LAYERS, CONFIG3_SIZES
+    rng = np.random.default_rng(0)
+    shapes = [(int(rng.choice(CONFIG3_SIZES)), int(rng.choice(CONFIG3_LAYERS))) for _ in range(count)]
+    peak = hbm_peak()[0]
+    out = {"workload": (f"z-line sweeps of the u, v and w systems of config 3's {count} uneven tiles (n in "
+                        f"{list(CONFIG3_SIZES)}, nz in {list(CONFIG3_LAYERS)}), {sweeps} sweeps, seeded "
+                        f"diagonally dominant coefficients; inputs resident, best of {reps}"), "systems": 3 * count}
+    for dtype, key in ((torch.float64, "fp64"), (torch.float32, "fp32")):
+        ctx = gb.Context()
+        gen = torch.Generator(device="cuda")
+        gen.manual_seed(7)
+        systems = []
+        points = 0
+        for n, nz in shapes:
+            g = gb.Grid(n, n, nz, 30.0, 30.0, 10.0, False, False)
+            for loc in (gb.LOC_XFACE, gb.LOC_YFACE, gb.LOC_ZFACE):
+                A = torch.rand((gb.N_COEFS,) + g.shape, dtype=dtype, device="cuda", generator=gen) * 0.9 + 0.1
+                ap = A.sum(0) + 0.2
+                rhs = torch.rand(g.shape, dtype=dtype, device="cuda", generator=gen) * 2.0 - 1.0
+                delta = torch.zeros(g.shape, dtype=dtype, device="cuda")
+                systems.append((g, loc, A, ap, rhs, delta))
+                ni, nj, nk = g.extents(loc)
+                points += ni * nj * nk
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+
+        def timed(fn):
+            fn()
+            best = float("inf")
+            for _ in range(reps):
+                torch.cuda.synchronize()
+                e0.record(ctx.stream)
+                fn()
+                e1.record(ctx.stream)
+                torch.cuda.synchronize()
+                best = min(best, e0.elapsed_time(e1))
+            return best
+
+        def batched():
+            gb.zline_jacobi_batch(ctx, systems, sweeps)
+
+        def one_by_one():
+            for (g, loc, A, ap, rhs, delta) in systems:
+                gb.zline_jacobi(ctx, g, loc, A, ap, rhs, sweeps, delta)
+
+        # the levels per warp for these systems (the in-project autotuner),
+        # used by both forms below
+        seg, seg_ms = tune_batch_sweep(Autotuner(), ctx, systems, sweeps) if tune else (0, None)
+        l0 = ctx.launches()
+        batched()
+        launches_batched = ctx.launches() - l0
+        l0 = ctx.launches()
+        one_by_one()
+        launches_single = ctx.launches() - l0
+        ms_b = timed(batched)
+        ms_1 = timed(one_by_one)
+        elt = torch.finfo(dtype).bits // 8
+        bytes_pass = points * (5 + 10 * (sweeps - 1)) * elt
+        out[key] = {"points": points, "batched_ms": ms_b, "one_by_one_ms": ms_1, "speedup": ms_1 / ms_b,
+                    "levels_per_warp": seg or 5, "autotune_ms": {str(k or 5): v for k, v in (seg_ms or {}).items()},
+                    "batched_point_sweeps_per_s": points * sweeps / (ms_b / 1e3),
+                    "launches_batched": launches_batched, "launches_one_by_one": launches_single,
+                    "hbm": {"achieved_gbs": bytes_pass / (ms_b / 1e3) / 1e9, "peak_gbs": peak,
+                            "frac": bytes_pass / (ms_b / 1e3) / 1e9 / peak, "bytes_per_pass": bytes_pass}}
+        del systems
+        ctx.close()
+        torch.cuda.empty_cache()
+    return out
+
+
+def served_leg(rates=(0.5, 2.0, 5.0, 20.0)):
+    """A bounded sample of the served configuration at each arrival rate of
+    `rates`: 12 requests, tiles drawn as config 3 with n in {64, 96} and nz
+    in {48, 64}, 70 % mass-consistent only and 30 % full solves (capped at
+    1500 iterations); served with continuous batching and FP32 inner solves
+    against plain FP64 served one at a time over the same arrivals (its
+    service times measured once, the FIFO queue replayed per rate)."""
+    from ablsteadyrans_b200.serve import serve_sweep
+    points = serve_sweep(rates, count=12, sizes=(64, 96), layers=(48, 64), max_iterations=1500)
+    for p in points:
+        p["speedup_solves_per_s"] = p["served_fp32_inner"]["solves_per_s"] / p["sequential_fp64"]["solves_per_s"]
+    out = dict(points[[p["rate_per_s"] for p in points].index(2.0)]) if 2.0 in rates else dict(points[0])
+    out["sweep"] = [{"rate_per_s": p["rate_per_s"], "speedup_solves_per_s": p["speedup_solves_per_s"],
+                     "served_p50_s": p["served_fp32_inner"]["p50_s"], "served_p99_s": p["served_fp32_inner"]["p99_s"],
+                     "served_solves_per_s": p["served_fp32_inner"]["solves_per_s"],
+                     "sequential_p50_s": p["sequential_fp64"]["p50_s"],
+                     "sequential_p99_s": p["sequential_fp64"]["p99_s"],
+                     "sequential_solves_per_s": p["sequential_fp64"]["solves_per_s"],
+                     "peak_concurrent": p["served_fp32_inner"]["peak_concurrent"]} for p in points]
+    out["workload"] = ("12 requests, Poisson arrivals at " + ", ".join(f"{r:g}" for r in rates) + " per s, tiles "
+                       "drawn as config 3 with n in {64, 96}, nz in {48, 64} (a bounded sample), 70 % "
+                       "mass-consistent only, 30 % full solves capped at 1500 iterations; the top-level figures "
+                       "are the 2/s point")
     return out
 
 
@@ -737,6 +847,7 @@ def main():
             line["steady_config2"] = steady_solves(max_iterations=3000, config=2)
     if world == 1 and not args.no_batch:
         line["batched"] = batched_leg()
+        line["batched_sweeps"] = batched_sweep_leg()
     if world == 1 and not args.no_serve:
         line["served"] = served_leg()
     if rank == 0 and not args.no_cpu:

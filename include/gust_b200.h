@@ -174,6 +174,41 @@ gb_status gb_zline_jacobi(gb_ctx* ctx, const gb_grid* g, int32_t loc, const doub
 /* The same in FP32 (the inner solver of the mixed-precision defect correction). */
 gb_status gb_zline_jacobi_f32(gb_ctx* ctx, const gb_grid* g, int32_t loc, const float* A, const float* ap,
                               const float* rhs, int32_t sweeps, float* delta, float* change);
+/* One system of a batched z-line solve: its own grid and location, and the
+ * arrays gb_zline_jacobi takes (device arrays of that grid). */
+typedef struct gb_line_system {
+    gb_grid grid;
+    int32_t loc;
+    const double* A;
+    const double* ap;
+    const double* rhs;
+    double* delta;
+} gb_line_system;
+typedef struct gb_line_system_f32 {
+    gb_grid grid;
+    int32_t loc;
+    const float* A;
+    const float* ap;
+    const float* rhs;
+    float* delta;
+} gb_line_system_f32;
+/* gust::zline_jacobi (Source/Predictor.cpp:87-127, the column solves of
+ * Source/LineSolve_K.H:22-45) over n systems of different grids at once, as
+ * a batch of terrain tiles and wind directions of uneven sizes brings them:
+ * every system's delta is set to 0 and gets `sweeps` sweeps, each value bit
+ * for bit the one gb_zline_jacobi gives that system alone on this context.
+ * The columns of all systems form one work-list of 32-column blocks, walked
+ * by persistent launches: one per sweep for each distinct number of
+ * segments (z-levels / the segment length, GB_TUNE_LINE_SEGMENT) the
+ * systems' columns have. change (host, n entries, or NULL) receives each
+ * system's max |change over the last sweep|; with change non-NULL the call
+ * waits for the context's stream. Columns taller than the segmented
+ * sweep's limit are refused (GB_BAD_ARG; use gb_zline_jacobi). */
+gb_status gb_zline_jacobi_batch(gb_ctx* ctx, int32_t n, const gb_line_system* systems, int32_t sweeps,
+                                double* change);
+/* The same in FP32. */
+gb_status gb_zline_jacobi_batch_f32(gb_ctx* ctx, int32_t n, const gb_line_system_f32* systems, int32_t sweeps,
+                                    double* change);
 /* The line LU-SGS solve, replacing gust::zline_lusgs with steady.line_ghosts =
  * lagged (Source/LineSweeps.H:159-161, Source/LineSweeps.cpp:183-210, 415-428):
  * `sweeps` symmetric passes of in-place column solves of the system of

@@ -70,3 +70,20 @@ def test_gpu_autotuner_picks_a_candidate_and_restores_the_state(ctx, tmp_path):
         for name in autotune.CANDIDATES:
             ctx.tune(getattr(gb, "TUNE_" + name), 0)
         st.close()
+
+
+def test_sweep_key_orders_systems_and_separates_precision_and_sweeps():
+    """The batched sweep's cache key lists the systems' extents in a fixed
+    order (the same batch in another order hits the same entry) and keeps
+    FP64 and FP32, and different sweep counts, apart."""
+    import torch
+    from helpers import Grid
+    from ablsteadyrans_b200.autotune import sweep_key
+    a, b = Grid(8, 6, 5, 1.0, 1.0, 1.0), Grid(4, 4, 9, 1.0, 1.0, 1.0)
+    d64, d32 = torch.zeros(1, dtype=torch.float64), torch.zeros(1, dtype=torch.float32)
+    s1 = [(a, 1, d64), (b, 4, d64)]
+    s2 = [(b, 4, d64), (a, 1, d64)]
+    assert sweep_key(s1, 4) == sweep_key(s2, 4)
+    assert sweep_key(s1, 4) != sweep_key(s1, 3)
+    assert sweep_key(s1, 4) != sweep_key([(a, 1, d32), (b, 4, d32)], 4)
+    assert "9x6x5" in sweep_key(s1, 4) and "4x4x10" in sweep_key(s1, 4)

@@ -144,6 +144,84 @@ def test_gpu_zline_jacobi_fp32(ctx, loc):
     assert rel_err(to_host(dd), d_ref, g.valid(loc)) < 2e-5
 
 
+BATCH = [
+    # nx, ny, nz, periodic_x, periodic_y, loc: uneven tiles, columns of 6 to 97
+    # levels (several warps-a-block groups), periodic seams
+    (37, 29, 17, True, False, 1),
+    (64, 48, 48, False, True, 0),
+    (5, 4, 6, False, False, 4),
+    (33, 20, 96, True, True, 4),
+    (40, 33, 64, False, False, 2),
+    (1, 1, 12, True, True, 0),
+    (24, 24, 48, False, False, 4),
+]
+
+
+def _batch_case(dtype, segment, seed0):
+    import torch
+    import ablsteadyrans_b200 as gb
+    systems, refs = [], []
+    for q, (nx, ny, nz, px, py, loc) in enumerate(BATCH):
+        g = Grid(nx, ny, nz, 30.0, 30.0, 10.0, px, py)
+        A, ap, rhs = random_system(g, loc, seed=seed0 + q, extra=0.2, xscale=3.0)
+        dA, dap, drhs = to_dev(A, dtype), to_dev(ap, dtype), to_dev(rhs, dtype)
+        dd = torch.full(g.shape, 7.0, dtype=dtype, device="cuda")  # overwritten: delta starts at 0
+        systems.append((g, loc, dA, dap, drhs, dd))
+        refs.append((g, loc, A, ap, rhs))
+    return gb, systems, refs
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("segment", [0, 4, 8])
+@pytest.mark.parametrize("sweeps", [1, 3])
+def test_gpu_zline_jacobi_batch_equals_single_systems(ctx, segment, sweeps):
+    """The batched solve (one column work-list over uneven systems, one
+    persistent launch per sweep and warps-a-block group) gives every system
+    the values of gb_zline_jacobi on that system alone, bit for bit (the same
+    segmented column solves; a block's warps above a column's top are
+    identity maps), in FP64 and FP32, with each system's max |change|; the
+    FP64 values are within 1e-12 of the oracle's."""
+    import torch
+    import ablsteadyrans_b200 as gb
+    ctx.tune(gb.TUNE_LINE_SEGMENT, segment)
+    try:
+        for dtype in (torch.float64, torch.float32):
+            gb, systems, refs = _batch_case(dtype, segment, 300 + sweeps)
+            changes = gb.zline_jacobi_batch(ctx, systems, sweeps)
+            for (g, loc, dA, dap, drhs, dd), (_, _, A, ap, rhs), ch in zip(systems, refs, changes):
+                alone = torch.full(g.shape, -3.0, dtype=dtype, device="cuda")
+                ch1 = gb.zline_jacobi(ctx, g, loc, dA, dap, drhs, sweeps, alone)
+                assert torch.equal(dd, alone), (g.nx, g.ny, g.nz, loc)
+                assert ch == pytest.approx(ch1, rel=1e-7 if dtype == torch.float32 else 0.0, abs=0.0)
+                if dtype == torch.float64:
+                    d_ref = g.np_zeros()
+                    ch_ref = oracle.zline_jacobi(g, loc, A, ap, rhs, sweeps, d_ref)
+                    assert rel_err(to_host(dd), d_ref, g.valid(loc)) < 1e-12
+                    assert abs(ch - ch_ref) <= 1e-12 * max(abs(ch_ref), 1e-300)
+    finally:
+        ctx.tune(gb.TUNE_LINE_SEGMENT, 0)
+
+
+@pytest.mark.gpu
+def test_gpu_zline_jacobi_batch_repeat_and_refusals(ctx):
+    """A second batched call on the same context (the scratch and work-list
+    reused) gives the same values; a system whose columns are taller than
+    the segmented sweep holds, and a bad sweep count, are refused."""
+    import torch
+    gb, systems, _ = _batch_case(torch.float64, 0, 500)
+    gb.zline_jacobi_batch(ctx, systems, 2, want_change=False)
+    first = [s[5].clone() for s in systems]
+    gb.zline_jacobi_batch(ctx, systems, 2)
+    for a, s in zip(first, systems):
+        assert torch.equal(a, s[5])
+    with pytest.raises(gb.GustError, match="sweeps must be >= 1"):
+        gb.zline_jacobi_batch(ctx, systems, 0)
+    tall = Grid(2, 2, 400, 1.0, 1.0, 1.0)
+    z = torch.zeros((7,) + tall.shape, dtype=torch.float64, device="cuda")
+    with pytest.raises(gb.GustError, match="z-levels"):
+        gb.zline_jacobi_batch(ctx, [(tall, 0, z, z[0], z[0], z[1])], 1)
+
+
 @pytest.mark.gpu
 def test_gpu_zline_jacobi_refusals(ctx):
     import torch
