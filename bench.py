@@ -48,6 +48,8 @@ sys.path.insert(0, ROOT)
 
 PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
+#: B200 HBM3e's nominal rate (DGX figure), beside which fractions are also given
+NOMINAL_HBM_GBS = 8000.0
 
 
 def hbm_peak():
@@ -653,14 +655,31 @@ def batched_sweep_leg(count=48, sweeps=4, reps=3, tune=True):
                     "batched_point_sweeps_per_s": points * sweeps / (ms_b / 1e3),
                     "launches_batched": launches_batched, "launches_one_by_one": launches_single,
                     "hbm": {"achieved_gbs": bytes_pass / (ms_b / 1e3) / 1e9, "peak_gbs": peak,
-                            "frac": bytes_pass / (ms_b / 1e3) / 1e9 / peak, "bytes_per_pass": bytes_pass}}
+                            "frac": bytes_pass / (ms_b / 1e3) / 1e9 / peak,
+                            "frac_of_nominal": bytes_pass / (ms_b / 1e3) / 1e9 / NOMINAL_HBM_GBS,
+                            "bytes_per_pass": bytes_pass}}
         del systems
         ctx.close()
         torch.cuda.empty_cache()
     return out
 
 
-def served_leg(rates=(0.5, 2.0, 5.0, 20.0)):
+def served_leg_isolated():
+    """served_leg in a child process of its own (bench.py --served-only): the
+    served form's latencies depend on the host threads and the device memory
+    it finds, so it starts from a fresh process, not after the other legs.
+    The parent's cached device memory is released first."""
+    import torch
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    proc = subprocess.run([sys.executable, os.path.abspath(__file__), "--served-only"], capture_output=True,
+                          text=True, cwd=ROOT)
+    if proc.returncode != 0:
+        raise RuntimeError(f"served leg failed ({proc.returncode}): {proc.stderr[-2000:]}")
+    return json.loads(proc.stdout.strip().splitlines()[-1])
+
+
+def served_leg(rates=(0.5, 1.0, 2.0, 5.0, 10.0, 20.0)):
     """A bounded sample of the served configuration at each arrival rate of
     `rates`: 12 requests, tiles drawn as config 3 with n in {64, 96} and nz
     in {48, 64}, 70 % mass-consistent only and 30 % full solves (capped at
@@ -699,6 +718,9 @@ def main():
     ap.add_argument("--no-steady2", action="store_true", help="skip the config-2 steady-solve leg")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched leg")
     ap.add_argument("--no-serve", action="store_true", help="skip the served leg")
+    ap.add_argument("--served-only", action="store_true",
+                    help="run the served leg alone and print its JSON (the main run's served leg runs this in a "
+                         "child process, so no earlier leg's device or host state is shared with it)")
     ap.add_argument("--tune", action="append", default=[], metavar="KEY=VALUE",
                     help="a context tuning knob (GB_TUNE_*, by number or name without the prefix), repeatable")
     args = ap.parse_args()
@@ -711,6 +733,9 @@ def main():
         if rank != 0:
             return 0
         return run_reference(args)
+    if args.served_only:
+        print(json.dumps(served_leg()))
+        return 0
 
     import torch
     torch.cuda.set_device(local_rank)
@@ -828,6 +853,8 @@ def main():
                      "kernel": "zline_seg_multi_kernel (segmented z-line Thomas sweeps: u, v, w in one launch, "
                                "theta and k in one)",
                      "peak_kind": peak_kind,
+                     "frac_of_nominal": (achieved / NOMINAL_HBM_GBS) if achieved else None,
+                     "nominal_peak": NOMINAL_HBM_GBS,
                      "bytes_per_launch": line_bytes / max(sweep_n, 1), "launch_ms": sweep_ms / max(sweep_n, 1)},
         "breakdown": families,
         "clocks": clocks,
@@ -849,7 +876,7 @@ def main():
         line["batched"] = batched_leg()
         line["batched_sweeps"] = batched_sweep_leg()
     if world == 1 and not args.no_serve:
-        line["served"] = served_leg()
+        line["served"] = served_leg_isolated()
     if rank == 0 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(wl)
     if rank == 0:
