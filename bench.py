@@ -674,9 +674,12 @@ def served_leg_isolated():
     torch.cuda.empty_cache()
     proc = subprocess.run([sys.executable, os.path.abspath(__file__), "--served-only"], capture_output=True,
                           text=True, cwd=ROOT)
-    if proc.returncode != 0:
-        raise RuntimeError(f"served leg failed ({proc.returncode}): {proc.stderr[-2000:]}")
-    return json.loads(proc.stdout.strip().splitlines()[-1])
+    try:
+        if proc.returncode != 0:
+            raise RuntimeError(f"exit status {proc.returncode}")
+        return json.loads(proc.stdout.strip().splitlines()[-1])
+    except Exception as e:  # the headline line still prints; the leg reports its failure
+        return {"error": f"served leg failed: {e}", "stderr_tail": proc.stderr[-2000:]}
 
 
 def served_leg(rates=(0.5, 1.0, 2.0, 5.0, 10.0, 20.0)):
