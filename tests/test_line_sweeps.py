@@ -216,10 +216,37 @@ def test_gpu_zline_jacobi_batch_repeat_and_refusals(ctx):
         assert torch.equal(a, s[5])
     with pytest.raises(gb.GustError, match="sweeps must be >= 1"):
         gb.zline_jacobi_batch(ctx, systems, 0)
+    with pytest.raises(gb.GustError, match="n must be >= 1"):
+        gb.zline_jacobi_batch(ctx, [], 1)
     tall = Grid(2, 2, 400, 1.0, 1.0, 1.0)
     z = torch.zeros((7,) + tall.shape, dtype=torch.float64, device="cuda")
     with pytest.raises(gb.GustError, match="z-levels"):
         gb.zline_jacobi_batch(ctx, [(tall, 0, z, z[0], z[0], z[1])], 1)
+
+
+@pytest.mark.gpu
+def test_gpu_zline_jacobi_batch_many_small_systems(ctx):
+    """More systems than one launch's parameter block holds (120): 130 small
+    uneven systems (1 to 5 columns a side, 3 to 14 levels, every location,
+    periodic seams) split over several launches per sweep, each system's
+    values still bit for bit those of gb_zline_jacobi alone."""
+    import torch
+    import ablsteadyrans_b200 as gb
+    rng = np.random.default_rng(77)
+    systems = []
+    for q in range(130):
+        nx, ny, nz = (int(v) for v in rng.integers((1, 1, 3), (6, 6, 15)))
+        px, py = bool(rng.integers(2)), bool(rng.integers(2))
+        loc = int(rng.choice(LOCS))
+        g = Grid(nx, ny, nz, 30.0, 30.0, 10.0, px, py)
+        A, ap, rhs = random_system(g, loc, seed=900 + q, extra=0.2, xscale=3.0)
+        systems.append((g, loc, to_dev(A), to_dev(ap), to_dev(rhs),
+                        torch.full(g.shape, 5.0, dtype=torch.float64, device="cuda")))
+    changes = gb.zline_jacobi_batch(ctx, systems, 3)
+    for (g, loc, dA, dap, drhs, dd), ch in zip(systems, changes):
+        alone = torch.zeros(g.shape, dtype=torch.float64, device="cuda")
+        assert gb.zline_jacobi(ctx, g, loc, dA, dap, drhs, 3, alone) == ch
+        assert torch.equal(dd, alone), (g.nx, g.ny, g.nz, loc)
 
 
 @pytest.mark.gpu
