@@ -664,8 +664,16 @@ void fill_side(gb_simplec* S, const gb_state& q, int d, int sides, bool homog = 
     b.lo[d] = 0;
     b.hi[d] = nsides * 6 * (ng + 1) - 1;
     const int pe0 = per[0], pe1 = per[1];
-    for_box(S->ctx, b, [=] __device__(int i0, int j0, int k0) {
-        int c[3] = {i0, j0, k0};
+    // launched with the (layer, field, side) index slowest: a warp then takes
+    // one field's rule on one side along a row of the slab (for d = 0 the
+    // rows run along y), not twelve rules in turn
+    const int q0 = (d == 0) ? 1 : 0, q1 = (d == 2) ? 1 : 2;
+    const Box pb{{b.lo[q0], b.lo[q1], b.lo[d]}, {b.hi[q0], b.hi[q1], b.hi[d]}};
+    for_box(S->ctx, pb, [=] __device__(int a0, int a1, int a2) {
+        int c[3];
+        c[q0] = a0;
+        c[q1] = a1;
+        c[d] = a2;
         const int fs = c[d] / (ng + 1);
         c[d] -= fs * (ng + 1);
         const int sd = fs / 6, n = fs % 6;

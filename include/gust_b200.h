@@ -200,7 +200,8 @@ typedef struct gb_line_system_f32 {
  * The columns of all systems form one work-list of 32-column blocks, walked
  * by persistent launches: one per sweep for each distinct number of
  * segments (z-levels / the segment length, GB_TUNE_LINE_SEGMENT) the
- * systems' columns have. change (host, n entries, or NULL) receives each
+ * systems' columns have, and one more per further 120 systems of one such
+ * group. change (host, n entries, or NULL) receives each
  * system's max |change over the last sweep|; with change non-NULL the call
  * waits for the context's stream. Columns taller than the segmented
  * sweep's limit are refused (GB_BAD_ARG; use gb_zline_jacobi). */
