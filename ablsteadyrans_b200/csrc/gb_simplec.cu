@@ -840,15 +840,27 @@ void velocity_divergence(gb_simplec* S, const double* u, const double* v, const 
     const double* ay = S->mesh.ay;
     const double* az = S->mesh.az;
     const double* J = S->mesh.detJ;
-    for_box(S->ctx, valid_box(g, CC), [=] __device__(int i, int j, int k) {
+    // a thread takes kDivLevels levels of a column: each z-face's Omega is
+    // evaluated once and serves the cells below and above it
+    constexpr int kDivLevels = 4;
+    const Box b{{0, 0, 0}, {g.nx - 1, g.ny - 1, (g.nz + kDivLevels - 1) / kDivLevels - 1}};
+    for_box(S->ctx, b, [=] __device__(int i, int j, int seg) {
         auto om = [&](int kk) {
             return w[at(g, i, j, kk)] - deriv<NODE, ZF, 0>(z, g, i, j, kk) * (1.0 / g.dx) * interp<XF, ZF>(u, g, i, j, kk)
                  - deriv<NODE, ZF, 1>(z, g, i, j, kk) * (1.0 / g.dy) * interp<YF, ZF>(v, g, i, j, kk);
         };
-        const int64_t o = at(g, i, j, k), ox = at(g, i + 1, j, k), oy = at(g, i, j + 1, k), oz = at(g, i, j, k + 1);
-        div[o] = ((ax[ox] * u[ox] - ax[o] * u[o]) * (1.0 / g.dx) + (ay[oy] * v[oy] - ay[o] * v[o]) * (1.0 / g.dy)
-                  + (az[oz] * om(k + 1) - az[o] * om(k)) * (1.0 / g.dzeta))
-               / J[o];
+        const int k0 = seg * kDivLevels;
+        double om_lo = om(k0);
+        for (int q = 0; q < kDivLevels; ++q) {
+            const int k = k0 + q;
+            if (k >= g.nz) { break; }
+            const double om_hi = om(k + 1);
+            const int64_t o = at(g, i, j, k), ox = at(g, i + 1, j, k), oy = at(g, i, j + 1, k), oz = at(g, i, j, k + 1);
+            div[o] = ((ax[ox] * u[ox] - ax[o] * u[o]) * (1.0 / g.dx) + (ay[oy] * v[oy] - ay[o] * v[o]) * (1.0 / g.dy)
+                      + (az[oz] * om_hi - az[o] * om_lo) * (1.0 / g.dzeta))
+                   / J[o];
+            om_lo = om_hi;
+        }
     }, GB_KERNEL_MASSFLUX);
 }
 
