@@ -587,6 +587,31 @@ gb_status check_newton(const gb_newton_opts* o)
 
 }  // namespace
 
+namespace {
+
+//! The Newton stage's residual inputs (Smoothness.cpp:54-67,
+//! newton_residual_inputs): the van Leer limiter's kink at every extremum
+//! spoils forward-difference Jacobian-vector products, so every residual the
+//! stage evaluates (its jvp, line search, norms and SIMPLEC preconditioner)
+//! takes the smooth counterpart, van Albada; van Albada and upwind stay.
+//! The stage's own limiter is restored when the call returns.
+class SmoothLimiter {
+public:
+    explicit SmoothLimiter(gb_simplec* S) : S_(S), saved_(gb::simplec_limiter(S))
+    {
+        if (saved_ == GB_LIMITER_VAN_LEER) { gb::simplec_set_limiter(S_, GB_LIMITER_VAN_ALBADA); }
+    }
+    ~SmoothLimiter() { gb::simplec_set_limiter(S_, saved_); }
+    SmoothLimiter(const SmoothLimiter&) = delete;
+    SmoothLimiter& operator=(const SmoothLimiter&) = delete;
+
+private:
+    gb_simplec* S_;
+    int saved_;
+};
+
+}  // namespace
+
 extern "C" {
 
 gb_status gb_newton_options_default(gb_newton_opts* o)
@@ -688,6 +713,7 @@ gb_status gb_newton_jvp(gb_newton* n, const gb_state* q, double* const* v, doubl
         gb::set_error("gust: jvp: null argument");
         return GB_BAD_ARG;
     }
+    const SmoothLimiter smooth(n->S);
     double bnorm = 0;
     gb_status st = gb::base(n, *q, &bnorm);
     if (st != GB_OK) { return st; }
@@ -704,6 +730,7 @@ gb_status gb_newton_direction(gb_newton* n, const gb_state* q, const double* dta
         gb::set_error("gust: NewtonKrylov::direction: null argument");
         return GB_BAD_ARG;
     }
+    const SmoothLimiter smooth(n->S);
     gb_status st = gb::solve(n, *q, dtau, info);
     if (st != GB_OK) { return st; }
     gb::Vec d(dq, dq + gb::kNF);
@@ -719,6 +746,7 @@ gb_status gb_newton_step(gb_newton* n, const gb_state* q, const double* dtau, gb
         gb::set_error("gust: NewtonKrylov::step: null argument");
         return GB_BAD_ARG;
     }
+    const SmoothLimiter smooth(n->S);
     gb_status st = gb::solve(n, *q, dtau, info);
     if (st != GB_OK) { return st; }
     if (info->applied) { gb::add_scaled(n, gb::vec_of(*q), n->x, 1.0); }
@@ -733,6 +761,7 @@ gb_status gb_newton_residual_norm(gb_newton* n, const gb_state* q, double* norm)
         gb::set_error("gust: NewtonKrylov::residual_norm: null argument");
         return GB_BAD_ARG;
     }
+    const SmoothLimiter smooth(n->S);
     return gb::base(n, *q, norm);
 }
 

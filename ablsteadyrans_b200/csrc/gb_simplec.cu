@@ -3534,6 +3534,8 @@ const gb_grid& simplec_grid(const gb_simplec* S) { return S->g; }
 gb_ctx* simplec_ctx(const gb_simplec* S) { return S->ctx; }
 const gb_physics& simplec_physics(const gb_simplec* S) { return S->ph; }
 const gb_simplec_opts& simplec_options(const gb_simplec* S) { return S->opt; }
+int simplec_limiter(const gb_simplec* S) { return S->ph.limiter; }
+void simplec_set_limiter(gb_simplec* S, int limiter) { S->ph.limiter = limiter; }
 const double* simplec_theta_ref(const gb_simplec* S) { return S->w.theta_ref; }
 void simplec_dirichlet_rows(gb_simplec* S, int c, double* mask) { dirichlet_rows(S, c, kLoc[c], mask); }
 void simplec_face_dtau(gb_simplec* S, const double* dtau, double** faces) { face_dtau(S, dtau, faces); }

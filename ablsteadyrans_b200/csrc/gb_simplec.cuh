@@ -38,6 +38,11 @@ const gb_physics& simplec_physics(const gb_simplec* S);
 //! Whether the ground is a surface-layer face (the wall model's state).
 bool simplec_has_wall(const gb_simplec* S);
 const gb_simplec_opts& simplec_options(const gb_simplec* S);
+//! The convection limiter of the stage's momentum and theta residuals, and
+//! its replacement for a while (the Newton stage's smooth counterpart); the
+//! stage's graphs never run while it is replaced.
+int simplec_limiter(const gb_simplec* S);
+void simplec_set_limiter(gb_simplec* S, int limiter);
 //! theta_ref at the cell centres (the stage's reference profile).
 const double* simplec_theta_ref(const gb_simplec* S);
 //! The Dirichlet rows (1, else 0) of velocity component c on its valid faces.

@@ -376,14 +376,19 @@ class SwitchOptions:
 
 def newton_equations_differ(stage):
     """NewtonStage::differs (NewtonStage.cpp:196-205) for what this build
-    has: with the closure and turb.nut_relax < 1 the residual blends nu_t with
-    the history of the last SIMPLEC iteration, which the Newton stage does not
-    update, so the stage's equations are not the steady ones. (The smooth
-    limiter and the frozen k-floor switches, the reference's other two
-    reasons, are not built: the Newton stage runs the run's own limiter and
-    live decisions.) The stage always has a history here: SIMPLEC iterated
-    for the switch window before the Newton stage began."""
+    has. (1) The Newton stage's residuals take the smooth counterpart of the
+    van Leer limiter, van Albada (gb_newton; Smoothness.cpp:54-67), so with
+    van Leer the stage solves other equations than the run's. (2) With the
+    closure and turb.nut_relax < 1 the residual blends nu_t with the history
+    of the last SIMPLEC iteration, which the Newton stage does not update.
+    (The frozen k-floor switches, the reference's third reason, are not
+    built: the Newton stage runs live floor decisions.) The stage always has
+    a history here: SIMPLEC iterated for the switch window before the Newton
+    stage began."""
+    from .abi import LIMITER_VAN_LEER
     ph = stage.physics
+    if int(ph.limiter) == LIMITER_VAN_LEER:
+        return True
     return bool(ph.closure) and ph.turb_nut_relax < 1.0
 
 
@@ -406,8 +411,8 @@ def newton_stage_action(verdict, idle, monitor_window, status, converged_now, di
     if failures >= fallback_failures:
         return "fallback", f"{failures} consecutive failed Newton steps"
     if status == "accepted" and converged_now and differs:
-        return "hand_back", ("Newton converged on its own equations, which differ from the run's (turb.nut_relax < 1): "
-                             "the final SIMPLEC pass")
+        return "hand_back", ("Newton converged on its own equations, which differ from the run's (the smooth limiter, "
+                             "or turb.nut_relax < 1): the final SIMPLEC pass")
     return "continue", ""
 
 

@@ -11,6 +11,7 @@ import pytest
 
 import oracle
 from ablsteadyrans_b200 import GustError
+from ablsteadyrans_b200.abi import LIMITER_VAN_ALBADA, LIMITER_VAN_LEER
 from ablsteadyrans_b200.driver import ser_cfl
 from ablsteadyrans_b200.newton import (ContinuationOptions, ContinuationState, NewtonOptions, armijo_accepts,
                                        armijo_line_search, check_continuation_options, check_newton_options,
@@ -140,6 +141,19 @@ def test_newton_stage_action_follows_the_reference_order(case, want):
         assert reason
 
 
+@pytest.mark.parametrize("limiter,closure,relax,want", [(0, 0, 1.0, True), (1, 0, 1.0, False), (2, 0, 1.0, False),
+                                                        (1, 1, 0.5, True), (1, 1, 1.0, False)])
+def test_newton_equations_differ_with_the_smooth_limiter(limiter, closure, relax, want):
+    """NewtonStage::differs (NewtonStage.cpp:196-205): van Leer's smooth
+    counterpart makes the Newton stage's equations differ from the run's;
+    van Albada and upwind are their own counterparts; turb.nut_relax < 1
+    with the closure differs too."""
+    from types import SimpleNamespace
+    from ablsteadyrans_b200.newton import newton_equations_differ
+    stage = SimpleNamespace(physics=SimpleNamespace(limiter=limiter, closure=closure, turb_nut_relax=relax))
+    assert newton_equations_differ(stage) is want
+
+
 def _hill():
     from test_turbulence import _hill_case
     return _hill_case()
@@ -148,7 +162,8 @@ def _hill():
 @pytest.mark.gpu
 def test_gpu_jvp_matches_the_oracle_difference(ctx):
     """J v on the GPU equals the oracle's (R(fill(q + eps v)) - R(fill(q))) /
-    eps at the GPU's eps (the closure and the wall law, refilled ghosts)."""
+    eps at the GPU's eps (the closure and the wall law, refilled ghosts),
+    R with the Newton stage's smooth limiter."""
     import torch
     from ablsteadyrans_b200.abi import SimplecOptions
     from ablsteadyrans_b200.newton import NewtonKrylov
@@ -169,13 +184,18 @@ def test_gpu_jvp_matches_the_oracle_difference(ctx):
     try:
         Jv, eps = nk.jvp([torch.from_numpy(a).cuda() for a in v])
         assert eps > 0
-        oracle.fill_ghosts(case, bc, ph)
-        R0 = oracle.residual(case, bc, ph)
+        # the Newton stage's residual inputs: van Leer's smooth counterpart
+        # (Smoothness.cpp:54-67)
+        phs = type(ph).from_buffer_copy(ph)
+        if phs.limiter == LIMITER_VAN_LEER:
+            phs.limiter = LIMITER_VAN_ALBADA
+        oracle.fill_ghosts(case, bc, phs)
+        R0 = oracle.residual(case, bc, phs)
         qp = case.copy()
         for n, f in enumerate(FIELDS):
             qp.q[f] = case.q[f] + eps * v[n]
-        oracle.fill_ghosts(qp, bc, ph)
-        Rp = oracle.residual(qp, bc, ph)
+        oracle.fill_ghosts(qp, bc, phs)
+        Rp = oracle.residual(qp, bc, phs)
         for n, loc in enumerate(LOCS):
             vv = g.valid(loc)
             ref = (Rp[n][vv] - R0[n][vv]) / eps
@@ -185,6 +205,40 @@ def test_gpu_jvp_matches_the_oracle_difference(ctx):
     finally:
         nk.close()
         st.close()
+
+
+@pytest.mark.gpu
+def test_gpu_newton_residuals_take_the_smooth_limiter(ctx):
+    """Every residual of the Newton stage takes van Leer's smooth counterpart
+    (Smoothness.cpp:54-67): its norm on a van Leer stage equals the norm on
+    the same state of a stage built with van Albada, bit for bit; the
+    stage's own residual afterwards is its van Leer residual again, which
+    differs from van Albada's on this hill."""
+    from ablsteadyrans_b200.abi import SimplecOptions
+    from ablsteadyrans_b200.newton import NewtonKrylov
+    from ablsteadyrans_b200.simplec import DeviceCase, SimplecStage
+    case, bc, ph = _hill()
+    assert ph.limiter == LIMITER_VAN_LEER
+    pha = type(ph).from_buffer_copy(ph)
+    pha.limiter = LIMITER_VAN_ALBADA
+    stages = []
+    try:
+        for p in (ph, pha, ph):
+            st = SimplecStage(ctx, DeviceCase.from_oracle(case), bc, p, SimplecOptions.make())
+            st.fill_ghosts()
+            stages.append(st)
+        leer, albada, fresh = stages
+        before, _ = leer.norms()
+        nk_leer, nk_albada = NewtonKrylov(leer), NewtonKrylov(albada)
+        assert nk_leer.residual_norm() == nk_albada.residual_norm()
+        after, _ = leer.norms()
+        own, _ = fresh.norms()
+        other, _ = albada.norms()
+        assert list(after) == list(before) == list(own)
+        assert list(after) != list(other)
+    finally:
+        for st in reversed(stages):
+            st.close()
 
 
 @pytest.mark.gpu
@@ -229,11 +283,14 @@ def test_gpu_poiseuille_in_one_newton_step(ctx):
 def test_gpu_continuation_reduces_the_residual(ctx):
     """Over the hill with the closure and the wall law, after SIMPLEC
     iterations: every accepted continuation step lowers |R| (the Armijo
-    condition), and five steps take it well below where they started."""
+    condition), and five steps take it well below where they started. The
+    run takes van Albada, so SIMPLEC and the Newton stage (which replaces
+    van Leer by it) iterate on the same equations."""
     from ablsteadyrans_b200.abi import SimplecOptions
     from ablsteadyrans_b200.newton import Continuation
     from ablsteadyrans_b200.simplec import DeviceCase, SimplecStage
     case, bc, ph = _hill()
+    ph.limiter = LIMITER_VAN_ALBADA
     dc = DeviceCase.from_oracle(case)
     st = SimplecStage(ctx, dc, bc, ph, SimplecOptions.make(pressure_reltol=1e-6))
     st.fill_ghosts()
