@@ -128,3 +128,17 @@ def test_sequential_latencies_are_a_fifo_queue():
     from ablsteadyrans_b200.serve import sequential_latencies
     assert sequential_latencies([0.0, 1.0, 1.5, 10.0], [2.0, 2.0, 2.0, 1.0]) == [2.0, 3.0, 4.5, 1.0]
     assert sequential_latencies([], []) == []
+
+
+def test_config4_tiles_do_not_depend_on_the_arrival_rate():
+    """The served sweep measures each request's sequential FP64 service time
+    once and replays the FIFO queue at every rate: that holds because the
+    same seed draws the same tiles and kinds at any rate (only the arrival
+    times scale, by 1 / rate)."""
+    a = serve.requests_config4(8, rate=0.5, seed=3, sizes=(32, 48), layers=(16, 24))
+    b = serve.requests_config4(8, rate=20.0, seed=3, sizes=(32, 48), layers=(16, 24))
+    for x, y in zip(a, b):
+        assert x.kind == y.kind
+        assert (x.inst.grid.nx, x.inst.grid.ny, x.inst.grid.nz) == (y.inst.grid.nx, y.inst.grid.ny, y.inst.grid.nz)
+        assert np.array_equal(x.inst.z, y.inst.z)
+        assert x.arrival * 0.5 == pytest.approx(y.arrival * 20.0, rel=1e-12)
