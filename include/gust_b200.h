@@ -776,7 +776,12 @@ gb_status gb_newton_options_default(gb_newton_opts* o);
 gb_status gb_newton_check(const gb_newton_opts* o);
 /* gust::NewtonKrylov on a stage (its residual, ghost fill and scales;
  * check_newton_options' range checks name their keys). Allocates
- * 2 restart + 13 state-sized vectors. */
+ * 2 restart + 13 state-sized vectors. Every residual the calls below
+ * evaluate (jvp, step, direction with its preconditioner, residual_norm)
+ * takes the Newton stage's residual inputs (Source/Smoothness.cpp:59-67,
+ * newton_residual_inputs): a stage with convection.limiter = van_leer is
+ * evaluated with van_albada for the duration of the call, and its own
+ * limiter is back when the call returns. */
 gb_status gb_newton_create(gb_simplec* s, const gb_newton_opts* o, gb_newton** out);
 gb_status gb_newton_destroy(gb_newton* n);
 /* gust::jvp with the refill (Source/Residual.cpp:324-396): Jv = (R(fill(q +
